@@ -1,0 +1,342 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 SIFT-and-stitching hot path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload NAME]
+
+Prints ONE JSON line on rank 0.  Workloads (synthetic, seeded inputs that
+stand in for the reference's datasets; see pysift_b200/synthetic.py):
+
+  detect_1280x960   detectAndCompute on one 1280x960 grayscale scene (the
+                    image size of the stitch-pair configuration)
+  detect_640x480    detectAndCompute on one 640x480 scene
+
+A step is one pass of the hot path over one input.  `value` is measured
+with CUDA events on the launching stream, inputs resident in HBM, L2
+flushed (256 MiB write) before every step outside the timed interval;
+`e2e` is the same metric through the public API with host buffers (pinned
+host->device copy of the input and device->host read of all outputs inside
+every timed step).  Multi-GPU runs are independent replicas (one process per
+GPU, each with its own input; scaling "weak"), timed as the max over ranks.
+"""
+import argparse
+import json
+import os
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "detect_1280x960": dict(kind="detect", H=960, W=1280, seed=0),
+    "detect_640x480": dict(kind="detect", H=480, W=640, seed=0),
+}
+DEFAULT_WORKLOAD = "detect_1280x960"
+METRIC = "SIFT Mpix/s + match-pairs/s on 1 B200: batched+BF16 vs plain, bit-exact"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", FALLBACK_HBM_GBS)), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def committed_traffic(workload):
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    return d.get(workload)
+
+
+class ClockSampler:
+    """Samples SM clock and clock-event reasons with NVML during the timed region."""
+    REASONS = {0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap",
+               0x8: "hw_slowdown", 0x10: "sync_boost", 0x20: "sw_thermal_slowdown",
+               0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting"}
+
+    def __init__(self, device_index):
+        self.samples = []
+        self.reasons = 0
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._thread = None
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            uuid = str(torch.cuda.get_device_properties(device_index).uuid)
+            if not uuid.startswith("GPU-"):
+                uuid = "GPU-" + uuid
+            self._h = pynvml.nvmlDeviceGetHandleByUUID(uuid.encode())
+            self._nv = pynvml
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self._nv = None
+
+    def _run(self):
+        nv = self._nv
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM))
+                self.reasons |= nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+            except Exception:
+                pass
+            time.sleep(0.1)
+
+    def __enter__(self):
+        if self._nv is not None:
+            self._thread = threading.Thread(target=self._run, daemon=True)
+            self._thread.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._thread:
+            self._thread.join()
+
+    def summary(self):
+        if self._nv is None or not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unavailable"]}
+        names = [n for b, n in self.REASONS.items() if self.reasons & b and n != "gpu_idle"]
+        return {"sm_mhz": float(np.median(self.samples)), "sm_max_mhz": self.max_mhz, "reasons": names,
+                "samples": len(self.samples)}
+
+
+def pyramid_alg_bytes(H, W, sift):
+    """Algorithmic bytes of pyramid + DoG + extrema for one image:
+    H*W (u8 in) + 4*P0 (upsampled base write) + 80*sum(P_o)."""
+    doubled = sift.double_image and H * W < sift._cfg.double_px_cap
+    h, w = (2 * H, 2 * W) if doubled else (H, W)
+    P = []
+    for _ in range(sift.n_octaves):
+        P.append(h * w)
+        h, w = (h + 1) // 2, (w + 1) // 2
+    return H * W + 4 * P[0] + 80 * sum(P)
+
+
+def detect_launches(sift, H, W):
+    """Kernel launches issued by one pysift_detect_and_compute call."""
+    doubled = sift.double_image and H * W < sift._cfg.double_px_cap
+    n_oct, S = sift.n_octaves, sift.n_scales
+    base = 3 if doubled else 1
+    blurs = 1 + n_oct * (S + 2)
+    detect = 2 * 5 + 1
+    return 1 + base + blurs + detect + 1 + 1 + 1 + 1 + 1 + 1
+
+
+def cpu_detect_baseline(img, budget_s=15.0):
+    """The oracle (a CPU port of the reference's path, OpenMP over the host
+    cores) on the same image, repeated until ~budget_s of work."""
+    from oracle import oracle
+    orc = oracle.OracleSIFT()
+    orc.detect_and_compute(img)  # warm-up (builds tables)
+    times = []
+    t_start = time.perf_counter()
+    while True:
+        t0 = time.perf_counter()
+        orc.detect_and_compute(img)
+        times.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_start > budget_s or len(times) >= 50:
+            break
+    med = float(np.median(times))
+    return med, len(times)
+
+
+def opencv_detect_baseline(img, runs=5):
+    try:
+        import cv2
+    except Exception:
+        return None
+    cv2.setNumThreads(os.cpu_count() or 1)
+    s = cv2.SIFT_create()
+    s.detectAndCompute(img, None)
+    t = []
+    for _ in range(runs):
+        t0 = time.perf_counter()
+        kps, _ = s.detectAndCompute(img, None)
+        t.append(time.perf_counter() - t0)
+    return float(np.median(t)), len(kps)
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference(args, wl, world, rank):
+    """--impl reference: the reference's path as the CPU oracle port, rank 0 only."""
+    if rank != 0:
+        return 0
+    from pysift_b200 import synthetic
+    img = synthetic.scene(wl["H"], wl["W"], seed=wl["seed"])
+    times = []
+    from oracle import oracle
+    orc = oracle.OracleSIFT()
+    for _ in range(args.warmup):
+        orc.detect_and_compute(img)
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        orc.detect_and_compute(img)
+        times.append(time.perf_counter() - t0)
+    sec = float(np.mean(times))
+    mpix = wl["H"] * wl["W"] / 1e6
+    value = mpix / sec
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Mpix/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "H": wl["H"], "W": wl["W"], "seed": wl["seed"]},
+        "cpu_baseline": {"value": value, "unit": "Mpix/s", "cores": os.cpu_count(), "kind": "port",
+                         "sample": f"one {wl['W']}x{wl['H']} image per step, full detectAndCompute"},
+        "e2e": {"value": value, "unit": "Mpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_detect(args, wl, world, rank, local):
+    import torch
+    import torch.distributed as dist
+    from pysift_b200 import PySIFT, synthetic
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    H, W = wl["H"], wl["W"]
+    img = synthetic.scene(H, W, seed=wl["seed"] + rank)
+    sift = PySIFT(device=dev)
+    g = torch.from_numpy(img).to(dev)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(7)]
+
+    for _ in range(args.warmup):
+        sift.run_device(g)
+    torch.cuda.synchronize(dev)
+    b = sift._bufs[(H, W)]
+    n_kp = int(b.stats.cpu()[0])
+
+    step_ms, pyr_ms = [], []
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            sift.run_device(g, stage_events=ev)
+            ev[6].synchronize()
+            step_ms.append(ev[0].elapsed_time(ev[6]))
+            pyr_ms.append(ev[0].elapsed_time(ev[3]))
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    total_ms = float(np.sum(step_ms))
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+
+    # end to end: pinned host image -> device -> pipeline -> host arrays
+    pinned = torch.from_numpy(img).pin_memory()
+    e2e_ms = []
+    h2d = img.nbytes
+    d2h = 0
+    for i in range(args.warmup + args.steps):
+        flush.zero_()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        b.gray.copy_(pinned, non_blocking=True)
+        sift.run_device(b.gray)
+        b.stats_host.copy_(b.stats, non_blocking=True)
+        stream.synchronize()
+        n = int(b.stats_host[0])
+        kp = b.kpts[:n].cpu()
+        rs = b.resp[:n].cpu()
+        oc = b.octv[:n].cpu()
+        ds = b.desc[:n].cpu()
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            e2e_ms.append(dt * 1e3)
+            d2h = b.stats.numel() * 4 + n * (4 * 4 + 4 + 4 + 128 * 4)
+    e2e_tot = torch.tensor([float(np.sum(e2e_ms))], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(e2e_tot, op=dist.ReduceOp.MAX)
+
+    if rank != 0:
+        return 0
+    mpix = H * W / 1e6
+    value = world * args.steps * mpix / (total_ms / 1e3)
+    e2e_value = world * args.steps * mpix / (float(e2e_tot.item()) / 1e3)
+    peak, peak_kind = measured_peaks()
+    alg = pyramid_alg_bytes(H, W, sift)
+    pyr_s = float(np.mean(pyr_ms)) / 1e3
+    achieved = alg / pyr_s / 1e9
+    if args.no_cpu_baseline:
+        cpu_med, cpu_n, ocv = float("nan"), 0, None
+    else:
+        cpu_med, cpu_n = cpu_detect_baseline(img)
+        ocv = opencv_detect_baseline(img)
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mpix/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "H": H, "W": W, "seed": wl["seed"], "keypoints": n_kp,
+                   "l2": "flushed (256 MiB write) before every step", "parallelism": f"replicas{world}"},
+        "roofline": {"bound": "hbm", "kernel": "pyramid+DoG+extrema (k_blur x%d + k_extrema_mask)"
+                     % (1 + sift.n_octaves * (sift.n_scales + 2)),
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_kind, "alg_bytes_per_launch": alg,
+                     "region_ms": pyr_s * 1e3, "traffic": committed_traffic(args.workload)},
+        "cpu_baseline": {"value": mpix / cpu_med, "unit": "Mpix/s", "cores": os.cpu_count(), "kind": "port",
+                         "sample": f"{cpu_n} runs of the oracle detectAndCompute on the same {W}x{H} image"},
+        "e2e": {"value": e2e_value, "unit": "Mpix/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": detect_launches(sift, H, W) * args.steps,
+        "clocks": clk.summary(),
+        "stage_ms": {"total": float(np.mean(step_ms))},
+    }
+    if ocv:
+        line["opencv_cpu"] = {"value": mpix / ocv[0], "unit": "Mpix/s", "cores": os.cpu_count(),
+                              "keypoints": ocv[1]}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU baseline legs (profiling runs)")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world, rank, local = dist_setup()
+    wl = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        return run_reference(args, wl, world, rank)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        return run_detect(args, wl, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

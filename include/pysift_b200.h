@@ -1,0 +1,142 @@
+/*
+ * pysift_b200.h -- C ABI of the B200 SIFT-and-stitching hot path.
+ *
+ * Every entry point takes device pointers, sizes and a cudaStream_t, returns
+ * an int status (PYSIFT_OK or a negative PYSIFT_ERR_*), never synchronises
+ * the device, and allocates no device memory: buffers (including the
+ * workspace) are owned by the caller.  pysift_last_error() returns a
+ * thread-local message for the last failing call on the calling thread.
+ *
+ * Reference interfaces replaced (paths in SivaIITM/PySIFT):
+ *   PySIFT.detectAndCompute           pysift/core.py:2021-2172
+ *   PySIFT._build_gaussian_pyramid    pysift/core.py:1234-1352
+ *   _fast_gaussian / gauss_h / gauss_v pysift/core.py:475-608
+ *   _adaptive_contrast_thresh         pysift/core.py:1129-1148
+ */
+#ifndef PYSIFT_B200_H
+#define PYSIFT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* pysift_stream_t; /* == cudaStream_t */
+
+#define PYSIFT_OK 0
+#define PYSIFT_ERR_INVALID_ARG (-1)
+#define PYSIFT_ERR_WORKSPACE (-2)    /* workspace too small */
+#define PYSIFT_ERR_CUDA (-3)         /* a launch or CUDA call failed */
+#define PYSIFT_ERR_UNSUPPORTED (-4)  /* configuration outside the supported range */
+#define PYSIFT_ERR_CAPACITY (-5)     /* an output buffer is too small */
+
+#define PYSIFT_MAX_OCTAVES 8
+#define PYSIFT_MAX_LEVELS 8          /* n_scales + 3 */
+#define PYSIFT_MAX_RADIUS 48
+#define PYSIFT_MAX_TAPS (2 * PYSIFT_MAX_RADIUS + 1)
+#define PYSIFT_DESC_DIM 128
+
+/* Detector configuration.  The host fills the tables the reference computes
+ * on the host (Gaussian weights in numpy float32, the per-scale sigma and
+ * patch-half-width tables, the keypoint size table); pysift_b200/core.py
+ * does this exactly as pysift/core.py:563-577, 1555, 1798-1810, 1512-1521. */
+typedef struct pysift_detect_config {
+    int32_t n_octaves;            /* 1..8 (reference: 5 on >= 12 GB GPUs)          */
+    int32_t n_scales;             /* S, 1..5                                        */
+    float sigma0;                 /* 1.6                                            */
+    double contrast_thresh;       /* base threshold before entropy scaling (0.04)   */
+    float edge_score;             /* float32((edge+1)^2/edge)                       */
+    int32_t double_image;         /* 2x cubic upsample when H*W < double_px_cap     */
+    int64_t double_px_cap;        /* 16,000,000 (>= 12 GB tier) or 4,194,304        */
+    int32_t fp16_pyramid;         /* store octaves >= 2 rounded to binary16         */
+    int32_t dsp;                  /* DSP-SIFT pooling                               */
+    int32_t n_dsp;                /* 3, 4 or 5                                      */
+    float dsp_scales[8];
+    int32_t rootsift;             /* RootSIFT post-normalisation                    */
+    int32_t max_cands_per_octave; /* 25000                                          */
+    int32_t keypoint_cap;         /* 8000                                           */
+    int32_t starvation_min;       /* 100: retry at half threshold below this        */
+    int32_t border;               /* 5                                              */
+    /* Gaussian kernels: [0] base blur when doubled, [1] base blur when not
+     * doubled, [2 + s] increment s -> s+1 for s = 0 .. n_scales+1.
+     * radius 0 means "no blur" (sigma < 0.01). */
+    int32_t blur_radius[2 + PYSIFT_MAX_LEVELS];
+    float blur_weights[2 + PYSIFT_MAX_LEVELS][PYSIFT_MAX_TAPS];
+    float ori_sigma[PYSIFT_MAX_LEVELS];           /* orientation sigma per scale index   */
+    float desc_ph[PYSIFT_MAX_LEVELS];             /* descriptor patch half-width per si  */
+    float kp_size[2][PYSIFT_MAX_OCTAVES][PYSIFT_MAX_LEVELS]; /* [doubled][o][si]     */
+} pysift_detect_config;
+
+/* Device-side counters written by pysift_detect_and_compute (int32 each). */
+#define PYSIFT_STAT_N_KEYPOINTS 0       /* oriented keypoints written             */
+#define PYSIFT_STAT_N_REFINED 1         /* refined keypoints before the cap       */
+#define PYSIFT_STAT_N_KEPT 2            /* after the keypoint cap                 */
+#define PYSIFT_STAT_RETRIED 3           /* 1 when the half-threshold retry ran    */
+#define PYSIFT_STAT_CAPPED 4            /* 1 when the keypoint cap applied        */
+#define PYSIFT_STAT_DOUBLED 5           /* 1 when the 2x upsample ran             */
+#define PYSIFT_STAT_CAND_OVERFLOW 6     /* octaves whose candidates were truncated */
+#define PYSIFT_STAT_CANDS 8             /* [8..15] extrema found per octave       */
+#define PYSIFT_STAT_REFINED_OCT 16      /* [16..23] refined per octave            */
+#define PYSIFT_STAT_THRESH_BITS 24      /* float bits of ct/S actually used       */
+#define PYSIFT_STAT_COUNT 32
+
+/* sizeof(pysift_detect_config), for bindings that mirror the struct. */
+size_t pysift_detect_config_size(void);
+
+/* Bytes of workspace pysift_detect_and_compute needs for an H x W image. */
+int pysift_detect_workspace_size(const pysift_detect_config* cfg, int32_t H, int32_t W, size_t* bytes);
+
+/* Largest number of keypoints the call can emit (4 orientations x cap). */
+int32_t pysift_detect_max_keypoints(const pysift_detect_config* cfg);
+
+/*
+ * Full detectAndCompute on a device-resident uint8 grayscale image
+ * (pysift/core.py:2021-2172).  Outputs, sorted by (x, y) like the reference:
+ *   kpts[i] = {x, y, size, angle}   (float32, the reference's gpu_output rows)
+ *   response[i] (float32), octave[i] (int32), desc[i][128] (float32;
+ *   RootSIFT when cfg->rootsift, else the L2/clip/L2 vector).
+ * stats (int32[PYSIFT_STAT_COUNT], device) receives the counters above;
+ * stats[PYSIFT_STAT_N_KEYPOINTS] is the number of rows written.
+ * max_out must be >= pysift_detect_max_keypoints(cfg).
+ * stage_events: NULL, or PYSIFT_DETECT_STAGE_EVENTS cudaEvent_t handles that
+ * are recorded on `stream` at the stage boundaries: 0 start, 1 base image
+ * ready, 2 Gaussian pyramid ready, 3 extrema bitmask ready, 4 keypoints
+ * refined and capped, 5 orientations ready, 6 end.
+ */
+#define PYSIFT_DETECT_STAGE_EVENTS 7
+int pysift_detect_and_compute(const pysift_detect_config* cfg, const uint8_t* gray, int32_t H, int32_t W,
+                              int64_t pitch_bytes, void* workspace, size_t workspace_bytes, float* kpts,
+                              float* response, int32_t* octave, float* desc, int32_t max_out, int32_t* stats,
+                              void* const* stage_events, pysift_stream_t stream);
+
+/* Locate an intermediate buffer of a run inside its workspace (for tests
+ * and tools).  what: 0 = Gaussian level (octave, level) as stored for the
+ * consumers (binary16-rounded in fp16 mode), 1 = the upsampled/converted
+ * base image before the first blur (octave, level ignored).  Returns the
+ * byte offset, rows, cols and row pitch (in floats). */
+int pysift_detect_workspace_view(const pysift_detect_config* cfg, int32_t H, int32_t W, int32_t what,
+                                 int32_t octave, int32_t level, size_t* offset, int32_t* rows, int32_t* cols,
+                                 int32_t* pitch_floats);
+
+/* Separable Gaussian blur of one float32 image (_fast_gaussian,
+ * pysift/core.py:552-608): horizontal then vertical FMA chain, reflect
+ * boundary.  in/out pitches in floats; weights has 2*radius+1 entries
+ * (host memory). */
+int pysift_gauss_blur(const float* in, int32_t in_pitch, float* out, int32_t out_pitch, int32_t H, int32_t W,
+                      const float* weights, int32_t radius, pysift_stream_t stream);
+
+/* 2x cubic B-spline zoom of a uint8 image scaled by 1/255
+ * (cupyx.scipy.ndimage.zoom(order=3) at pysift/core.py:1270-1275).
+ * coef: caller scratch of H*W doubles; out: 2H x 2W floats, pitch in floats. */
+int pysift_zoom2x_u8(const uint8_t* gray, int32_t H, int32_t W, int64_t pitch_bytes, int32_t fp16_round,
+                     double* coef, float* out, int32_t out_pitch, pysift_stream_t stream);
+
+const char* pysift_last_error(void);
+const char* pysift_b200_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,95 @@
+// Shared helpers for the pysift_b200 CUDA translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+#include "../../include/pysift_b200.h"
+
+namespace pysift {
+
+constexpr unsigned FULL_MASK = 0xffffffffu;
+
+// Thread-local error message behind pysift_last_error().
+void set_error(const char* fmt, ...);
+
+#define PYSIFT_CHECK_ARG(cond, ...)            \
+    do {                                       \
+        if (!(cond)) {                         \
+            ::pysift::set_error(__VA_ARGS__);  \
+            return PYSIFT_ERR_INVALID_ARG;     \
+        }                                      \
+    } while (0)
+
+#define PYSIFT_CUDA_TRY(call)                                                              \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess) {                                                           \
+            ::pysift::set_error("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_),    \
+                                __FILE__, __LINE__);                                       \
+            return PYSIFT_ERR_CUDA;                                                        \
+        }                                                                                  \
+    } while (0)
+
+#define PYSIFT_LAUNCH_CHECK(name)                                                          \
+    do {                                                                                   \
+        cudaError_t e_ = cudaGetLastError();                                               \
+        if (e_ != cudaSuccess) {                                                           \
+            ::pysift::set_error("launch of %s failed: %s", name, cudaGetErrorString(e_));  \
+            return PYSIFT_ERR_CUDA;                                                        \
+        }                                                                                  \
+    } while (0)
+
+inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+__host__ __device__ inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
+inline long long ceil_div_ll(long long a, long long b) { return (a + b - 1) / b; }
+
+__device__ __forceinline__ float round_half(float v) { return __half2float(__float2half_rn(v)); }
+
+// Exclusive scan of one int per thread across a block of blockDim.x
+// threads (multiple of 32, <= 1024).  sh must hold 33 ints.  Returns the
+// thread's exclusive prefix; *total receives the block total.
+__device__ __forceinline__ int block_excl_scan(int v, int* total, int* sh) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nwarps = blockDim.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        int y = __shfl_up_sync(FULL_MASK, x, d);
+        if (lane >= d) x += y;
+    }
+    if (lane == 31) sh[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        int w = (lane < nwarps) ? sh[lane] : 0;
+        int s = w;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            int y = __shfl_up_sync(FULL_MASK, s, d);
+            if (lane >= d) s += y;
+        }
+        sh[lane] = s - w;
+        if (lane == 31) sh[32] = s;
+    }
+    __syncthreads();
+    int res = sh[warp] + x - v;
+    *total = sh[32];
+    __syncthreads();
+    return res;
+}
+
+__device__ __forceinline__ int warp_excl_scan(int v, int* total) {
+    const int lane = threadIdx.x & 31;
+    int x = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        int y = __shfl_up_sync(FULL_MASK, x, d);
+        if (lane >= d) x += y;
+    }
+    *total = __shfl_sync(FULL_MASK, x, 31);
+    return x - v;
+}
+
+}  // namespace pysift

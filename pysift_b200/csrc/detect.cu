@@ -1,0 +1,1669 @@
+// detect.cu -- SIFT detection + description on one device-resident image.
+//
+// Pipeline (all launches on the caller's stream, no host synchronisation,
+// capturable into a CUDA graph):
+//   k_histogram          256-bin histogram + entropy threshold (pysift/core.py:1129-1148)
+//   k_prefilter_cols/rows, k_zoom_interp
+//                        2x cubic B-spline upsample (pysift/core.py:1270-1275)
+//   k_u8_to_f32          base image when not upsampled (pysift/core.py:1248-1261)
+//   k_blur<R>            fused H+V separable blur per level (pysift/core.py:475-608,
+//                        1288-1343); the first blur of octave o>0 reads the previous
+//                        octave's level S with stride 2 and also stores level 0
+//   k_extrema_mask       26-neighbour test on DoG computed on the fly from the Gaussian
+//                        levels (pysift/core.py:176-217); one bit per voxel + per-row
+//                        integer counts
+//   k_rowscan, k_scatter deterministic compaction in (s, r, c) order, cap per octave
+//   k_refine             Taylor refinement + contrast + edge (pysift/core.py:343-463)
+//   k_refine_compact     valid keypoints in candidate order
+//   k_retry_decide       starvation retry at half threshold (pysift/core.py:2066-2071)
+//   k_cap                top-cap by response, stable (pysift/core.py:2078-2080)
+//   k_orientation        36-bin histogram, peaks (pysift/core.py:228-333)
+//   k_expand             orientation expansion + (x, y) sort keys (pysift/core.py:1592-1598)
+//   k_rank               rank of each key = output row (pysift/core.py:2128-2134)
+//   k_descriptor         4x4x8 descriptor (+DSP) + L2/clip/L2 + RootSIFT, written at its
+//                        output row (pysift/core.py:693-997, 1870-1873)
+#include <cstdarg>
+#include <cstring>
+#include <mutex>
+
+#include "common.cuh"
+#include "sift_math.cuh"
+
+namespace pysift {
+
+static thread_local std::string g_last_error;
+
+void set_error(const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+}
+
+// ---------------------------------------------------------------------------
+// Device control block (one per run, inside the workspace).
+// ---------------------------------------------------------------------------
+struct Ctrl {
+    double ct;
+    float thr[2];
+    unsigned int hist[256];
+    unsigned int blocks_done;
+    int found[PYSIFT_MAX_OCTAVES];
+    int ncand[PYSIFT_MAX_OCTAVES];
+    int nref[PYSIFT_MAX_OCTAVES];
+    int retried;
+    int n_total_ref;
+    int n_kept;
+    int capped;
+    int n_oriented;
+    int overflow_octs;
+    int pad[2];
+};
+
+struct OctView {
+    const float* lev[PYSIFT_MAX_LEVELS];
+    int H, W, pitch;
+};
+
+// ---------------------------------------------------------------------------
+// Workspace layout.
+// ---------------------------------------------------------------------------
+struct Layout {
+    int n_oct, L, S;
+    bool doubled;
+    int H0, W0, pitch0;  // octave-0 / base image
+    int H[PYSIFT_MAX_OCTAVES], W[PYSIFT_MAX_OCTAVES], pitch[PYSIFT_MAX_OCTAVES], wpr[PYSIFT_MAX_OCTAVES];
+    size_t off_pyr[PYSIFT_MAX_OCTAVES], off_pyr_r[PYSIFT_MAX_OCTAVES];
+    size_t off_mask[PYSIFT_MAX_OCTAVES], off_rowcnt[PYSIFT_MAX_OCTAVES], off_rowoff[PYSIFT_MAX_OCTAVES];
+    size_t off_ctrl, off_coef, off_base;
+    size_t off_cand, off_rv_valid, off_rv_ri, off_rv_ci, off_rv_si, off_rv_resp;
+    size_t off_rf_ri, off_rf_ci, off_rf_si, off_rf_resp;
+    size_t off_kp_o, off_kp_si, off_kp_ri, off_kp_ci, off_kp_resp, off_kp_tb;
+    size_t off_ang, off_angcnt, off_ent_kp, off_ent_slot, off_keys, off_rank;
+    size_t rowcnt_bytes_total;
+    size_t off_rowcnt_base;
+    size_t total;
+};
+
+static int validate_cfg(const pysift_detect_config* c) {
+    PYSIFT_CHECK_ARG(c != nullptr, "config is NULL");
+    PYSIFT_CHECK_ARG(c->n_octaves >= 1 && c->n_octaves <= PYSIFT_MAX_OCTAVES, "n_octaves %d outside 1..%d",
+                     c->n_octaves, PYSIFT_MAX_OCTAVES);
+    PYSIFT_CHECK_ARG(c->n_scales >= 1 && c->n_scales + 3 <= PYSIFT_MAX_LEVELS, "n_scales %d outside 1..%d",
+                     c->n_scales, PYSIFT_MAX_LEVELS - 3);
+    PYSIFT_CHECK_ARG(c->max_cands_per_octave >= 1 && c->max_cands_per_octave <= (1 << 22),
+                     "max_cands_per_octave %d out of range", c->max_cands_per_octave);
+    PYSIFT_CHECK_ARG(c->keypoint_cap >= 1 && c->keypoint_cap <= (1 << 20), "keypoint_cap %d out of range",
+                     c->keypoint_cap);
+    PYSIFT_CHECK_ARG(c->border >= 1 && c->border < 64, "border %d out of range", c->border);
+    PYSIFT_CHECK_ARG(!c->dsp || (c->n_dsp >= 1 && c->n_dsp <= 8), "n_dsp %d out of range", c->n_dsp);
+    for (int i = 0; i < 2 + c->n_scales + 2; ++i)
+        PYSIFT_CHECK_ARG(c->blur_radius[i] >= 0 && c->blur_radius[i] <= PYSIFT_MAX_RADIUS,
+                         "blur radius %d outside 0..%d", c->blur_radius[i], PYSIFT_MAX_RADIUS);
+    for (int s = 1; s <= c->n_scales; ++s) {
+        PYSIFT_CHECK_ARG(c->desc_ph[s] >= 1.0f && c->desc_ph[s] <= 200.0f, "desc_ph[%d] out of range", s);
+        PYSIFT_CHECK_ARG(c->ori_sigma[s] > 0.0f && c->ori_sigma[s] < 64.0f, "ori_sigma[%d] out of range", s);
+    }
+    return PYSIFT_OK;
+}
+
+static Layout make_layout(const pysift_detect_config* c, int H, int W) {
+    Layout l;
+    memset(&l, 0, sizeof(l));
+    l.n_oct = c->n_octaves;
+    l.S = c->n_scales;
+    l.L = c->n_scales + 3;
+    l.doubled = c->double_image && ((int64_t)H * W < c->double_px_cap);
+    l.H0 = l.doubled ? 2 * H : H;
+    l.W0 = l.doubled ? 2 * W : W;
+    int h = l.H0, w = l.W0;
+    for (int o = 0; o < l.n_oct; ++o) {
+        l.H[o] = h;
+        l.W[o] = w;
+        l.pitch[o] = (int)align_up((size_t)w, 32);
+        l.wpr[o] = ceil_div(w, 32);
+        h = (h + 1) / 2;
+        w = (w + 1) / 2;
+    }
+    l.pitch0 = l.pitch[0];
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        size_t r = off;
+        off = align_up(off + bytes, 256);
+        return r;
+    };
+    const size_t cap = (size_t)c->max_cands_per_octave;
+    const size_t kc = (size_t)c->keypoint_cap;
+    l.off_ctrl = take(sizeof(Ctrl));
+    // row counts of all octaves are contiguous so one memset clears them
+    l.off_rowcnt_base = off;
+    size_t rc = 0;
+    for (int o = 0; o < l.n_oct; ++o) rc += (size_t)l.S * l.H[o];
+    size_t start = take(rc * sizeof(int));
+    l.rowcnt_bytes_total = rc * sizeof(int);
+    size_t acc = start;
+    for (int o = 0; o < l.n_oct; ++o) {
+        l.off_rowcnt[o] = acc;
+        acc += (size_t)l.S * l.H[o] * sizeof(int);
+    }
+    for (int o = 0; o < l.n_oct; ++o) l.off_rowoff[o] = take((size_t)l.S * l.H[o] * sizeof(int));
+    for (int o = 0; o < l.n_oct; ++o) l.off_mask[o] = take((size_t)l.S * l.H[o] * l.wpr[o] * sizeof(uint32_t));
+    l.off_cand = take(cap * l.n_oct * sizeof(int4));
+    l.off_rv_valid = take(cap * l.n_oct * sizeof(int));
+    l.off_rv_ri = take(cap * l.n_oct * sizeof(float));
+    l.off_rv_ci = take(cap * l.n_oct * sizeof(float));
+    l.off_rv_si = take(cap * l.n_oct * sizeof(int));
+    l.off_rv_resp = take(cap * l.n_oct * sizeof(float));
+    l.off_rf_ri = take(cap * l.n_oct * sizeof(float));
+    l.off_rf_ci = take(cap * l.n_oct * sizeof(float));
+    l.off_rf_si = take(cap * l.n_oct * sizeof(int));
+    l.off_rf_resp = take(cap * l.n_oct * sizeof(float));
+    l.off_kp_o = take(kc * sizeof(int));
+    l.off_kp_si = take(kc * sizeof(int));
+    l.off_kp_ri = take(kc * sizeof(float));
+    l.off_kp_ci = take(kc * sizeof(float));
+    l.off_kp_resp = take(kc * sizeof(float));
+    l.off_kp_tb = take(kc * sizeof(uint32_t));
+    l.off_ang = take(kc * 4 * sizeof(float));
+    l.off_angcnt = take(kc * sizeof(int));
+    l.off_ent_kp = take(kc * 4 * sizeof(int));
+    l.off_ent_slot = take(kc * 4 * sizeof(int));
+    l.off_keys = take(kc * 4 * sizeof(uint4));
+    l.off_rank = take(kc * 4 * sizeof(int));
+    if (l.doubled) l.off_coef = take((size_t)H * W * sizeof(double));
+    l.off_base = take((size_t)l.H0 * l.pitch0 * sizeof(float));
+    for (int o = 0; o < l.n_oct; ++o) l.off_pyr[o] = take((size_t)l.L * l.H[o] * l.pitch[o] * sizeof(float));
+    for (int o = 0; o < l.n_oct; ++o) {
+        if (c->fp16_pyramid && o >= 2)
+            l.off_pyr_r[o] = take((size_t)l.L * l.H[o] * l.pitch[o] * sizeof(float));
+        else
+            l.off_pyr_r[o] = l.off_pyr[o];
+    }
+    l.total = off;
+    return l;
+}
+
+// ---------------------------------------------------------------------------
+// A1: histogram + entropy threshold.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_histogram(const uint8_t* __restrict__ img, int H, int W, long long pitch,
+                                                   Ctrl* ctrl, double base, int S) {
+    __shared__ unsigned int sh[256];
+    __shared__ double terms[256];
+    __shared__ int is_last;
+    const int tid = threadIdx.x;
+    sh[tid] = 0;
+    __syncthreads();
+    const long long n = (long long)H * W;
+    for (long long i = (long long)blockIdx.x * blockDim.x + tid; i < n; i += (long long)gridDim.x * blockDim.x) {
+        long long r = i / W, c = i - r * W;
+        atomicAdd(&sh[img[r * pitch + c]], 1u);
+    }
+    __syncthreads();
+    if (sh[tid]) atomicAdd(&ctrl->hist[tid], sh[tid]);
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) is_last = (atomicAdd(&ctrl->blocks_done, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (!is_last) return;
+    __threadfence();
+    unsigned int h = atomicAdd(&ctrl->hist[tid], 0u);
+    double t = 0.0;
+    if (h) {
+        double p = (double)h / (double)n;
+        t = p * sm::log2d_(p);
+    }
+    terms[tid] = t;
+    sh[tid] = h;
+    __syncthreads();
+    if (tid == 0) {
+        double ent = 0.0;
+        for (int b = 0; b < 256; ++b)
+            if (sh[b]) ent = ent + terms[b];
+        ent = -ent;
+        double scale = 0.8 + ent / 40.0;
+        if (scale > 1.0) scale = 1.0;
+        double ct = base * scale;
+        ctrl->ct = ct;
+        ctrl->thr[0] = (float)(ct / (double)S);
+        ctrl->thr[1] = (float)((ct * 0.5) / (double)S);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// A2/A3: base image.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float u8_to_unit(uint8_t u, int fp16) {
+    float f = (float)u / 255.0f;
+    return fp16 ? round_half(f) : f;
+}
+
+__global__ void k_u8_to_f32(const uint8_t* __restrict__ img, int H, int W, long long pitch, int fp16,
+                            float* __restrict__ out, int out_pitch) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    int r = blockIdx.y;
+    if (c < W) out[(long long)r * out_pitch + c] = u8_to_unit(img[(long long)r * pitch + c], fp16);
+}
+
+// In-place B-spline prefilter of one line (scipy.ndimage spline_filter1d,
+// order 3, mirror boundary).  z^(n-1) by repeated multiplication.
+__device__ void prefilter_line(double* c, long long n, long long stride) {
+    if (n < 2) return;
+    const double z = sqrt(3.0) - 2.0;
+    const double gain = (1.0 - z) * (1.0 - 1.0 / z);
+    for (long long i = 0; i < n; ++i) c[i * stride] *= gain;
+    double z_i = z;
+    double z_n_1 = 1.0;
+    for (long long i = 0; i < n - 1; ++i) z_n_1 = z_n_1 * z;
+    double c0 = c[0] + z_n_1 * c[(n - 1) * stride];
+    for (long long i = 1; i < n - 1; ++i) {
+        c0 += z_i * (c[i * stride] + z_n_1 * c[(n - 1 - i) * stride]);
+        z_i *= z;
+    }
+    c0 /= 1.0 - z_n_1 * z_n_1;
+    c[0] = c0;
+    double prev = c0;
+    for (long long i = 1; i < n; ++i) {
+        prev = c[i * stride] + z * prev;
+        c[i * stride] = prev;
+    }
+    double last = (z * c[(n - 2) * stride] + c[(n - 1) * stride]) * z / (z * z - 1.0);
+    c[(n - 1) * stride] = last;
+    double nxt = last;
+    for (long long i = n - 2; i >= 0; --i) {
+        nxt = z * (nxt - c[i * stride]);
+        c[i * stride] = nxt;
+    }
+}
+
+__global__ void k_prefilter_cols(const uint8_t* __restrict__ img, int H, int W, long long pitch, int fp16,
+                                 double* __restrict__ coef) {
+    int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= W) return;
+    for (int r = 0; r < H; ++r) coef[(long long)r * W + x] = (double)u8_to_unit(img[(long long)r * pitch + x], fp16);
+    prefilter_line(coef + x, H, W);
+}
+
+__global__ void k_prefilter_rows(double* __restrict__ coef, int H, int W) {
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= H) return;
+    prefilter_line(coef + (long long)r * W, W, 1);
+}
+
+__device__ __forceinline__ long long mirror_index(long long idx, long long len) {
+    if (len <= 1) return 0;
+    long long s2 = 2 * len - 2;
+    if (idx < 0) {
+        idx = s2 * (long long)(-idx / s2) + idx;
+        idx = idx <= 1 - len ? idx + s2 : -idx;
+    } else if (idx >= len) {
+        idx -= s2 * (long long)(idx / s2);
+        if (idx >= len) idx = s2 - idx;
+    }
+    return idx;
+}
+
+__device__ __forceinline__ bool zoom_axis(long long k, long long in_len, long long out_len, long long idx[4],
+                                          double w[4]) {
+    double zoom = (out_len > 1) ? (double)(in_len - 1) / (double)(out_len - 1) : 1.0;
+    double cc = (double)k * zoom;
+    if (cc < 0.0 || cc > (double)(in_len - 1)) return false;
+    double fl = floor(cc);
+    long long start = (long long)fl - 1;
+    double y = cc - fl;
+    double z = 1.0 - y;
+    w[0] = z * z * z / 6.0;
+    w[1] = (y * y * (y - 2.0) * 3.0 + 4.0) / 6.0;
+    double y1 = 1.0 - y;
+    w[2] = (y1 * y1 * (y1 - 2.0) * 3.0 + 4.0) / 6.0;
+    w[3] = 1.0 - w[0] - w[1] - w[2];
+    for (int h = 0; h < 4; ++h) idx[h] = mirror_index(start + h, in_len);
+    return true;
+}
+
+__global__ void k_zoom_interp(const double* __restrict__ coef, int H, int W, int fp16, float* __restrict__ out,
+                              int out_pitch) {
+    const int OW = 2 * W, OH = 2 * H;
+    int x = blockIdx.x * blockDim.x + threadIdx.x;
+    int r = blockIdx.y;
+    if (x >= OW || r >= OH) return;
+    long long iy[4], ix[4];
+    double wy[4], wx[4];
+    bool vy = zoom_axis(r, H, OH, iy, wy);
+    bool vx = zoom_axis(x, W, OW, ix, wx);
+    float res = 0.0f;
+    if (vy && vx) {
+        double t = 0.0;
+        for (int i = 0; i < 4; ++i) {
+            const double* row = coef + iy[i] * (long long)W;
+            for (int j = 0; j < 4; ++j) {
+                double coeff = row[ix[j]];
+                coeff *= wy[i];
+                coeff *= wx[j];
+                t += coeff;
+            }
+        }
+        res = (float)t;
+        if (fp16) res = round_half(res);
+    }
+    out[(long long)r * out_pitch + x] = res;
+}
+
+// ---------------------------------------------------------------------------
+// A4/A5: fused separable blur.
+// ---------------------------------------------------------------------------
+struct BlurArgs {
+    const float* in;
+    long long in_pitch;
+    int step;  // 1, or 2 when reading level S of the previous octave
+    float* out;
+    float* out_r;  // binary16-rounded copy (fp16 mode), else null
+    float* copy0;  // stores the (subsampled) input tile interior, else null
+    float* copy0_r;
+    int out_pitch;
+    int H, W;
+    float w[PYSIFT_MAX_TAPS];
+};
+
+__device__ __forceinline__ int reflect_idx(int i, int n) {
+    int p = 2 * n;
+    i = i % p;
+    if (i < 0) i += p;
+    if (i >= n) i = 2 * n - 1 - i;
+    return i;
+}
+
+constexpr int BLUR_TW = 64, BLUR_TH = 32, BLUR_NT = 256;
+
+__device__ __forceinline__ void blur_load_tile(const BlurArgs& a, float* tile, int R, int TWP, int ROWS, int r0,
+                                               int c0) {
+    for (int i = threadIdx.x; i < ROWS * TWP; i += BLUR_NT) {
+        int rr = i / TWP, cc = i - rr * TWP;
+        int gr = reflect_idx(r0 - R + rr, a.H), gc = reflect_idx(c0 - R + cc, a.W);
+        float v = a.in[(long long)gr * a.step * a.in_pitch + (long long)gc * a.step];
+        tile[i] = v;
+        if (a.copy0 && rr >= R && rr < R + BLUR_TH && cc >= R && cc < R + BLUR_TW) {
+            int orow = r0 + rr - R, ocol = c0 + cc - R;
+            if (orow < a.H && ocol < a.W) {
+                a.copy0[(long long)orow * a.out_pitch + ocol] = v;
+                if (a.copy0_r) a.copy0_r[(long long)orow * a.out_pitch + ocol] = round_half(v);
+            }
+        }
+    }
+}
+
+template <int R>
+__global__ void __launch_bounds__(BLUR_NT) k_blur(const BlurArgs a) {
+    constexpr int TW = BLUR_TW, TH = BLUR_TH;
+    constexpr int TWP = TW + 2 * R, ROWS = TH + 2 * R;
+    extern __shared__ float smem[];
+    float* tile = smem;
+    float* hb = smem + ROWS * TWP;
+    const int c0 = blockIdx.x * TW, r0 = blockIdx.y * TH;
+    blur_load_tile(a, tile, R, TWP, ROWS, r0, c0);
+    __syncthreads();
+    constexpr int SPR = TW / 8;
+    for (int sidx = threadIdx.x; sidx < ROWS * SPR; sidx += BLUR_NT) {
+        int rr = sidx / SPR, x0 = (sidx - rr * SPR) * 8;
+        const float* src = tile + rr * TWP + x0;
+        float v[8 + 2 * R];
+#pragma unroll
+        for (int j = 0; j < 8 + 2 * R; ++j) v[j] = src[j];
+        float acc[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[j] = 0.0f;
+#pragma unroll
+        for (int k = 0; k <= 2 * R; ++k) {
+            const float wk = a.w[k];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) acc[j] = fmaf(v[j + k], wk, acc[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) hb[rr * TW + x0 + j] = acc[j];
+    }
+    __syncthreads();
+    {
+        const int col = threadIdx.x % TW, y0 = (threadIdx.x / TW) * 8;
+        float v[8 + 2 * R];
+#pragma unroll
+        for (int j = 0; j < 8 + 2 * R; ++j) v[j] = hb[(y0 + j) * TW + col];
+        float acc[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[j] = 0.0f;
+#pragma unroll
+        for (int k = 0; k <= 2 * R; ++k) {
+            const float wk = a.w[k];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) acc[j] = fmaf(v[j + k], wk, acc[j]);
+        }
+        const int gc = c0 + col;
+        if (gc < a.W) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                int gr = r0 + y0 + j;
+                if (gr < a.H) {
+                    a.out[(long long)gr * a.out_pitch + gc] = acc[j];
+                    if (a.out_r) a.out_r[(long long)gr * a.out_pitch + gc] = round_half(acc[j]);
+                }
+            }
+        }
+    }
+}
+
+// Any radius up to PYSIFT_MAX_RADIUS (no register blocking); radius 0 copies.
+__global__ void __launch_bounds__(BLUR_NT) k_blur_generic(const BlurArgs a, int R) {
+    const int TWP = BLUR_TW + 2 * R, ROWS = BLUR_TH + 2 * R;
+    extern __shared__ float smem[];
+    float* tile = smem;
+    float* hb = smem + ROWS * TWP;
+    const int c0 = blockIdx.x * BLUR_TW, r0 = blockIdx.y * BLUR_TH;
+    blur_load_tile(a, tile, R, TWP, ROWS, r0, c0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < ROWS * BLUR_TW; i += BLUR_NT) {
+        int rr = i / BLUR_TW, x = i - rr * BLUR_TW;
+        float acc = 0.0f;
+        if (R == 0) acc = tile[rr * TWP + x];
+        else
+            for (int k = 0; k <= 2 * R; ++k) acc = fmaf(tile[rr * TWP + x + k], a.w[k], acc);
+        hb[i] = acc;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < BLUR_TH * BLUR_TW; i += BLUR_NT) {
+        int y = i / BLUR_TW, x = i - y * BLUR_TW;
+        float acc = 0.0f;
+        if (R == 0) acc = hb[y * BLUR_TW + x];
+        else
+            for (int k = 0; k <= 2 * R; ++k) acc = fmaf(hb[(y + k) * BLUR_TW + x], a.w[k], acc);
+        int gr = r0 + y, gc = c0 + x;
+        if (gr < a.H && gc < a.W) {
+            a.out[(long long)gr * a.out_pitch + gc] = acc;
+            if (a.out_r) a.out_r[(long long)gr * a.out_pitch + gc] = round_half(acc);
+        }
+    }
+}
+
+static size_t blur_smem_bytes(int R) {
+    return (size_t)((BLUR_TH + 2 * R) * (BLUR_TW + 2 * R) + (BLUR_TH + 2 * R) * BLUR_TW) * sizeof(float);
+}
+
+typedef void (*BlurKernel)(const BlurArgs);
+
+template <int R>
+static BlurKernel blur_kernel_for() { return k_blur<R>; }
+
+static BlurKernel blur_table(int R) {
+    switch (R) {
+        case 1: return k_blur<1>;
+        case 2: return k_blur<2>;
+        case 3: return k_blur<3>;
+        case 4: return k_blur<4>;
+        case 5: return k_blur<5>;
+        case 6: return k_blur<6>;
+        case 7: return k_blur<7>;
+        case 8: return k_blur<8>;
+        case 9: return k_blur<9>;
+        case 10: return k_blur<10>;
+        case 11: return k_blur<11>;
+        case 12: return k_blur<12>;
+        case 13: return k_blur<13>;
+        case 14: return k_blur<14>;
+        case 15: return k_blur<15>;
+        case 16: return k_blur<16>;
+        default: return nullptr;
+    }
+}
+
+static int ensure_blur_attrs() {
+    static std::once_flag once;
+    static cudaError_t err = cudaSuccess;
+    std::call_once(once, [] {
+        cudaError_t e = cudaFuncSetAttribute(k_blur_generic, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)blur_smem_bytes(PYSIFT_MAX_RADIUS));
+        if (e != cudaSuccess) err = e;
+    });
+    if (err != cudaSuccess) {
+        set_error("cudaFuncSetAttribute(k_blur_generic): %s", cudaGetErrorString(err));
+        return PYSIFT_ERR_CUDA;
+    }
+    return PYSIFT_OK;
+}
+
+static int launch_blur(BlurArgs& a, int R, const float* w, cudaStream_t st) {
+    for (int k = 0; k <= 2 * R; ++k) a.w[k] = w[k];
+    dim3 grid(ceil_div(a.W, BLUR_TW), ceil_div(a.H, BLUR_TH));
+    BlurKernel kfn = (R >= 1) ? blur_table(R) : nullptr;
+    if (kfn) {
+        kfn<<<grid, BLUR_NT, blur_smem_bytes(R), st>>>(a);
+        PYSIFT_LAUNCH_CHECK("k_blur");
+    } else {
+        int rc = ensure_blur_attrs();
+        if (rc) return rc;
+        k_blur_generic<<<grid, BLUR_NT, blur_smem_bytes(R), st>>>(a, R);
+        PYSIFT_LAUNCH_CHECK("k_blur_generic");
+    }
+    return PYSIFT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// A7: extrema bitmask + per-row counts, then deterministic compaction.
+// ---------------------------------------------------------------------------
+struct ExtArgs {
+    OctView oct[PYSIFT_MAX_OCTAVES];
+    int n_oct, S, border, thr_idx, retry_mode, cap;
+    int blk_off[PYSIFT_MAX_OCTAVES + 1];
+    uint32_t* mask[PYSIFT_MAX_OCTAVES];
+    int* rowcnt[PYSIFT_MAX_OCTAVES];
+    int* rowoff[PYSIFT_MAX_OCTAVES];
+    int wpr[PYSIFT_MAX_OCTAVES];
+    int4* cand;
+};
+
+__device__ __forceinline__ float dog_at(const OctView& v, int s, int r, int c) {
+    long long off = (long long)r * v.pitch + c;
+    return v.lev[s + 1][off] - v.lev[s][off];
+}
+
+__device__ __forceinline__ int find_octave(const int* blk_off, int n_oct, int b) {
+    int o = 0;
+    while (o + 1 < n_oct && b >= blk_off[o + 1]) ++o;
+    return o;
+}
+
+__global__ void __launch_bounds__(256) k_extrema_mask(const ExtArgs a, Ctrl* ctrl) {
+    if (a.retry_mode && !ctrl->retried) return;
+    const float thr = ctrl->thr[a.thr_idx];
+    const int o = find_octave(a.blk_off, a.n_oct, blockIdx.x);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const OctView& v = a.oct[o];
+    const int wpr = a.wpr[o];
+    const int unit = (blockIdx.x - a.blk_off[o]) * 8 + warp;
+    if (unit >= v.H * wpr) return;
+    const int r = unit / wpr, wc = unit - r * wpr;
+    const int c = wc * 32 + lane;
+    const int B = a.border;
+    const bool inb = (r >= B && r < v.H - B && c >= B && c < v.W - B);
+    for (int s = 1; s <= a.S; ++s) {
+        bool ext = false;
+        if (inb) {
+            float val = dog_at(v, s, r, c);
+            if (fabsf(val) > thr) {
+                bool is_max = true, is_min = true;
+                for (int ds = -1; ds <= 1 && (is_max || is_min); ++ds)
+                    for (int dr = -1; dr <= 1; ++dr)
+                        for (int dc = -1; dc <= 1; ++dc) {
+                            if (ds == 0 && dr == 0 && dc == 0) continue;
+                            float nb = dog_at(v, s + ds, r + dr, c + dc);
+                            is_max = is_max && (val >= nb);
+                            is_min = is_min && (val <= nb);
+                        }
+                ext = is_max || is_min;
+            }
+        }
+        unsigned m = __ballot_sync(FULL_MASK, ext);
+        if (lane == 0) {
+            a.mask[o][((long long)(s - 1) * v.H + r) * wpr + wc] = m;
+            if (m) atomicAdd(&a.rowcnt[o][(s - 1) * v.H + r], __popc(m));
+        }
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_rowscan(const ExtArgs a, Ctrl* ctrl) {
+    if (a.retry_mode && !ctrl->retried) return;
+    __shared__ int sh[33];
+    const int o = blockIdx.x;
+    const int n = a.S * a.oct[o].H;
+    const int per = (n + (int)blockDim.x - 1) / (int)blockDim.x;
+    const int beg = threadIdx.x * per;
+    int local = 0;
+    for (int i = 0; i < per && beg + i < n; ++i) local += a.rowcnt[o][beg + i];
+    int total;
+    int off = block_excl_scan(local, &total, sh);
+    for (int i = 0; i < per && beg + i < n; ++i) {
+        int cnt = a.rowcnt[o][beg + i];
+        a.rowoff[o][beg + i] = off;
+        off += cnt;
+    }
+    if (threadIdx.x == 0) {
+        ctrl->found[o] = total;
+        ctrl->ncand[o] = total < a.cap ? total : a.cap;
+        if (total > a.cap) atomicAdd(&ctrl->overflow_octs, 1);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_scatter(const ExtArgs a, Ctrl* ctrl) {
+    if (a.retry_mode && !ctrl->retried) return;
+    const int o = find_octave(a.blk_off, a.n_oct, blockIdx.x);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int H = a.oct[o].H;
+    const int unit = (blockIdx.x - a.blk_off[o]) * 8 + warp;  // (s-1)*H + r
+    if (unit >= a.S * H) return;
+    if (a.rowcnt[o][unit] == 0) return;
+    const int s = unit / H + 1, r = unit - (s - 1) * H;
+    const int wpr = a.wpr[o];
+    int base = a.rowoff[o][unit];
+    const uint32_t* mrow = a.mask[o] + (long long)unit * wpr;
+    int4* out = a.cand + (long long)o * a.cap;
+    for (int w0 = 0; w0 < wpr; w0 += 32) {
+        uint32_t word = (w0 + lane < wpr) ? mrow[w0 + lane] : 0u;
+        int tot;
+        int pos = base + warp_excl_scan(__popc(word), &tot);
+        while (word) {
+            int b = __ffs(word) - 1;
+            word &= word - 1;
+            if (pos < a.cap) out[pos] = make_int4(s, r, (w0 + lane) * 32 + b, 0);
+            ++pos;
+        }
+        base += tot;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// A8: refinement.
+// ---------------------------------------------------------------------------
+struct RefArgs {
+    OctView oct[PYSIFT_MAX_OCTAVES];
+    int n_oct, S, border, cap, thr_idx, retry_mode;
+    float edge_score;
+    const int4* cand;
+    int* rv_valid;
+    float* rv_ri;
+    float* rv_ci;
+    int* rv_si;
+    float* rv_resp;
+    float* rf_ri;
+    float* rf_ci;
+    int* rf_si;
+    float* rf_resp;
+};
+
+__global__ void __launch_bounds__(256) k_refine(const RefArgs a, Ctrl* ctrl) {
+    if (a.retry_mode && !ctrl->retried) return;
+    const float cthr = ctrl->thr[a.thr_idx];
+    const long long nslots = (long long)a.n_oct * a.cap;
+    for (long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x; slot < nslots;
+         slot += (long long)gridDim.x * blockDim.x) {
+        const int o = (int)(slot / a.cap);
+        const int j = (int)(slot - (long long)o * a.cap);
+        if (j >= ctrl->ncand[o]) continue;
+        const OctView& v = a.oct[o];
+        const int4 cd = a.cand[slot];
+        int si = cd.x, row = cd.y, col = cd.z;
+        const int H = v.H, W = v.W, S = a.S, B = a.border;
+        float ox = 0.0f, oy = 0.0f, os_ = 0.0f;
+        bool converged = false;
+        for (int iter = 0; iter < 5; ++iter) {
+            if (si < 1 || si > S || row < B || row >= H - B || col < B || col >= W - B) break;
+            float cval = dog_at(v, si, row, col);
+            float cxp = dog_at(v, si, row, col + 1), cxm = dog_at(v, si, row, col - 1);
+            float cyp = dog_at(v, si, row + 1, col), cym = dog_at(v, si, row - 1, col);
+            float sp = dog_at(v, si + 1, row, col), smn = dog_at(v, si - 1, row, col);
+            float dx = (cxp - cxm) * 0.5f;
+            float dy = (cyp - cym) * 0.5f;
+            float ds = (sp - smn) * 0.5f;
+            float dxx = cxp - 2.0f * cval + cxm;
+            float dyy = cyp - 2.0f * cval + cym;
+            float dss = sp - 2.0f * cval + smn;
+            float dxy = (dog_at(v, si, row + 1, col + 1) - dog_at(v, si, row + 1, col - 1) -
+                         dog_at(v, si, row - 1, col + 1) + dog_at(v, si, row - 1, col - 1)) *
+                        0.25f;
+            float dxs = (dog_at(v, si + 1, row, col + 1) - dog_at(v, si + 1, row, col - 1) -
+                         dog_at(v, si - 1, row, col + 1) + dog_at(v, si - 1, row, col - 1)) *
+                        0.25f;
+            float dys = (dog_at(v, si + 1, row + 1, col) - dog_at(v, si + 1, row - 1, col) -
+                         dog_at(v, si - 1, row + 1, col) + dog_at(v, si - 1, row - 1, col)) *
+                        0.25f;
+            float det = dxx * (dyy * dss - dys * dys) - dxy * (dxy * dss - dys * dxs) + dxs * (dxy * dys - dyy * dxs);
+            if (fabsf(det) < 1e-12f) break;
+            float inv_det = 1.0f / det;
+            float p = -dx, q = -dy, rv = -ds;
+            ox = (p * (dyy * dss - dys * dys) - dxy * (q * dss - dys * rv) + dxs * (q * dys - dyy * rv)) * inv_det;
+            oy = (dxx * (q * dss - dys * rv) - p * (dxy * dss - dys * dxs) + dxs * (dxy * rv - q * dxs)) * inv_det;
+            os_ = (dxx * (dyy * rv - q * dys) - dxy * (dxy * rv - q * dxs) + p * (dxy * dys - dyy * dxs)) * inv_det;
+            if (fabsf(ox) < 0.5f && fabsf(oy) < 0.5f && fabsf(os_) < 0.5f) {
+                converged = true;
+                break;
+            }
+            col += (ox >= 0.0f) ? (int)(ox + 0.5f) : (int)(ox - 0.5f);
+            row += (oy >= 0.0f) ? (int)(oy + 0.5f) : (int)(oy - 0.5f);
+            si += (os_ >= 0.0f) ? (int)(os_ + 0.5f) : (int)(os_ - 0.5f);
+        }
+        int valid = 0;
+        float response = 0.0f;
+        if (converged && !(si < 1 || si > S || row < B || row >= H - B || col < B || col >= W - B)) {
+            float cval = dog_at(v, si, row, col);
+            float cxp = dog_at(v, si, row, col + 1), cxm = dog_at(v, si, row, col - 1);
+            float cyp = dog_at(v, si, row + 1, col), cym = dog_at(v, si, row - 1, col);
+            float dx_ = (cxp - cxm) * 0.5f;
+            float dy_ = (cyp - cym) * 0.5f;
+            float ds_ = (dog_at(v, si + 1, row, col) - dog_at(v, si - 1, row, col)) * 0.5f;
+            response = fabsf(cval + 0.5f * (dx_ * ox + dy_ * oy + ds_ * os_));
+            if (response >= cthr) {
+                float dxx = cxp - 2.0f * cval + cxm;
+                float dyy = cyp - 2.0f * cval + cym;
+                float dxy = (dog_at(v, si, row + 1, col + 1) - dog_at(v, si, row + 1, col - 1) -
+                             dog_at(v, si, row - 1, col + 1) + dog_at(v, si, row - 1, col - 1)) *
+                            0.25f;
+                float trace = dxx + dyy;
+                float det2d = dxx * dyy - dxy * dxy;
+                if (!(det2d <= 0.0f || (trace * trace / det2d) >= a.edge_score)) valid = 1;
+            }
+        }
+        a.rv_valid[slot] = valid;
+        if (valid) {
+            a.rv_ri[slot] = (float)row + oy;
+            a.rv_ci[slot] = (float)col + ox;
+            a.rv_si[slot] = si;
+            a.rv_resp[slot] = response;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_refine_compact(const RefArgs a, Ctrl* ctrl) {
+    if (a.retry_mode && !ctrl->retried) return;
+    __shared__ int sh[33];
+    const int o = blockIdx.x;
+    const int n = ctrl->ncand[o];
+    const long long base = (long long)o * a.cap;
+    int out_base = 0;
+    for (int c0 = 0; c0 < n; c0 += blockDim.x) {
+        int j = c0 + threadIdx.x;
+        int f = (j < n) ? a.rv_valid[base + j] : 0;
+        int tot;
+        int pos = out_base + block_excl_scan(f, &tot, sh);
+        if (f) {
+            a.rf_ri[base + pos] = a.rv_ri[base + j];
+            a.rf_ci[base + pos] = a.rv_ci[base + j];
+            a.rf_si[base + pos] = a.rv_si[base + j];
+            a.rf_resp[base + pos] = a.rv_resp[base + j];
+        }
+        out_base += tot;
+    }
+    if (threadIdx.x == 0) ctrl->nref[o] = out_base;
+}
+
+__global__ void k_retry_decide(Ctrl* ctrl, int n_oct, int starvation_min) {
+    int t = 0;
+    for (int o = 0; o < n_oct; ++o) t += ctrl->nref[o];
+    ctrl->retried = (t < starvation_min) ? 1 : 0;
+}
+
+// ---------------------------------------------------------------------------
+// A9: keypoint cap (top `cap` by response, stable).
+// ---------------------------------------------------------------------------
+struct CapArgs {
+    int n_oct, cap_cand, kp_cap;
+    const float* rf_ri;
+    const float* rf_ci;
+    const int* rf_si;
+    const float* rf_resp;
+    int* kp_o;
+    int* kp_si;
+    float* kp_ri;
+    float* kp_ci;
+    float* kp_resp;
+    uint32_t* kp_tb;
+};
+
+__device__ __forceinline__ void global_to_local(const int* nref_pref, int n_oct, int g, int* o, int* j) {
+    int oo = 0;
+    while (oo + 1 < n_oct && g >= nref_pref[oo + 1]) ++oo;
+    *o = oo;
+    *j = g - nref_pref[oo];
+}
+
+__global__ void __launch_bounds__(1024) k_cap(const CapArgs a, Ctrl* ctrl) {
+    __shared__ int sh[33];
+    __shared__ int pref[PYSIFT_MAX_OCTAVES + 1];
+    __shared__ unsigned int hist[256];
+    __shared__ unsigned int s_prefix, s_mask;
+    __shared__ int s_need;
+    if (threadIdx.x == 0) {
+        pref[0] = 0;
+        for (int o = 0; o < a.n_oct; ++o) pref[o + 1] = pref[o] + ctrl->nref[o];
+    }
+    __syncthreads();
+    const int total = pref[a.n_oct];
+    const bool capped = total > a.kp_cap;
+    auto load = [&](int g, int* o, int* j) {
+        global_to_local(pref, a.n_oct, g, o, j);
+        return (long long)(*o) * a.cap_cand + *j;
+    };
+    if (!capped) {
+        for (int g = threadIdx.x; g < total; g += blockDim.x) {
+            int o, j;
+            long long src = load(g, &o, &j);
+            a.kp_o[g] = o;
+            a.kp_si[g] = a.rf_si[src];
+            a.kp_ri[g] = a.rf_ri[src];
+            a.kp_ci[g] = a.rf_ci[src];
+            a.kp_resp[g] = a.rf_resp[src];
+            a.kp_tb[g] = 0u;
+        }
+        if (threadIdx.x == 0) {
+            ctrl->n_total_ref = total;
+            ctrl->n_kept = total;
+            ctrl->capped = 0;
+        }
+        return;
+    }
+    // radix select of the kp_cap-th largest response (non-negative float bits)
+    if (threadIdx.x == 0) {
+        s_prefix = 0u;
+        s_mask = 0u;
+        s_need = a.kp_cap;
+    }
+    __syncthreads();
+    for (int pass = 3; pass >= 0; --pass) {
+        for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0u;
+        __syncthreads();
+        const unsigned int prefix = s_prefix, mask = s_mask;
+        for (int g = threadIdx.x; g < total; g += blockDim.x) {
+            int o, j;
+            long long src = load(g, &o, &j);
+            unsigned int key = __float_as_uint(a.rf_resp[src]);
+            if ((key & mask) == prefix) atomicAdd(&hist[(key >> (8 * pass)) & 255u], 1u);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int need = s_need;
+            int cum = 0;
+            int d = 255;
+            for (; d > 0; --d) {
+                if (cum + (int)hist[d] >= need) break;
+                cum += (int)hist[d];
+            }
+            s_need = need - cum;
+            s_prefix = prefix | ((unsigned int)d << (8 * pass));
+            s_mask = mask | (255u << (8 * pass));
+        }
+        __syncthreads();
+    }
+    const unsigned int T = s_prefix;
+    const int need_eq = s_need;
+    int eq_base = 0, out_base = 0;
+    for (int c0 = 0; c0 < total; c0 += blockDim.x) {
+        int g = c0 + threadIdx.x;
+        unsigned int key = 0u;
+        long long src = 0;
+        int o = 0, j = 0;
+        if (g < total) {
+            src = load(g, &o, &j);
+            key = __float_as_uint(a.rf_resp[src]);
+        }
+        int is_eq = (g < total && key == T) ? 1 : 0;
+        int tot_eq;
+        int eq_rank = eq_base + block_excl_scan(is_eq, &tot_eq, sh);
+        eq_base += tot_eq;
+        int keep = (g < total) && (key > T || (is_eq && eq_rank < need_eq));
+        int tot_keep;
+        int pos = out_base + block_excl_scan(keep, &tot_keep, sh);
+        out_base += tot_keep;
+        if (keep) {
+            a.kp_o[pos] = o;
+            a.kp_si[pos] = a.rf_si[src];
+            a.kp_ri[pos] = a.rf_ri[src];
+            a.kp_ci[pos] = a.rf_ci[src];
+            a.kp_resp[pos] = a.rf_resp[src];
+            a.kp_tb[pos] = ~key;
+        }
+    }
+    if (threadIdx.x == 0) {
+        ctrl->n_total_ref = total;
+        ctrl->n_kept = out_base;
+        ctrl->capped = 1;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// A10: orientation.
+// ---------------------------------------------------------------------------
+struct OriArgs {
+    OctView oct[PYSIFT_MAX_OCTAVES];
+    float ori_sigma[PYSIFT_MAX_LEVELS];
+    const int* kp_o;
+    const int* kp_si;
+    const float* kp_ri;
+    const float* kp_ci;
+    float* ang;
+    int* angcnt;
+};
+
+constexpr int ORI_WARPS = 8;
+
+__global__ void __launch_bounds__(ORI_WARPS * 32) k_orientation(const OriArgs a, const Ctrl* ctrl) {
+    __shared__ float lh_all[ORI_WARPS][32 * 37];
+    __shared__ float hist_all[ORI_WARPS][36];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = blockIdx.x * ORI_WARPS + warp;
+    if (i >= ctrl->n_kept) return;
+    float* lh = lh_all[warp] + lane * 37;
+    for (int b = 0; b < 36; ++b) lh[b] = 0.0f;
+    const int o = a.kp_o[i], si = a.kp_si[i];
+    const float ri = a.kp_ri[i], ci = a.kp_ci[i];
+    const float sigma = a.ori_sigma[si];
+    const OctView& v = a.oct[o];
+    const int H = v.H, W = v.W;
+    int radius = (int)(4.5f * sigma + 0.5f);
+    if (radius < 1) radius = 1;
+    const float sigma_w = 1.5f * sigma;
+    const float inv_2sw2 = 1.0f / (2.0f * sigma_w * sigma_w + 1e-12f);
+    int r_min = (int)ri - radius;
+    if (r_min < 1) r_min = 1;
+    int r_max = (int)ri + radius;
+    if (r_max > H - 2) r_max = H - 2;
+    int c_min = (int)ci - radius;
+    if (c_min < 1) c_min = 1;
+    int c_max = (int)ci + radius;
+    if (c_max > W - 2) c_max = W - 2;
+    int n_cols = c_max - c_min + 1;
+    if (n_cols < 1) n_cols = 1;
+    int nr = r_max - r_min + 1;
+    if (nr < 0) nr = 0;
+    const int total = nr * n_cols;
+    const float* g = v.lev[si];
+    const long long P = v.pitch;
+    for (int pidx = lane; pidx < total; pidx += 32) {
+        int r = r_min + pidx / n_cols;
+        int c = c_min + pidx % n_cols;
+        float dx = g[r * P + c + 1] - g[r * P + c - 1];
+        float dy = g[(r + 1) * P + c] - g[(r - 1) * P + c];
+        float mag = sqrtf(dx * dx + dy * dy);
+        float ori = fmodf(sm::atan2f_(dy, dx) * 57.29577951f + 360.0f, 360.0f);
+        float fr = (float)r - ri, fc = (float)c - ci;
+        float wt = sm::expf_(-(fr * fr + fc * fc) * inv_2sw2);
+        float bin_f = ori * 0.1f;
+        int bin_i = ((int)bin_f) % 36;
+        int bin_r = (bin_i + 1) % 36;
+        float frac = bin_f - floorf(bin_f);
+        float mw = mag * wt;
+        lh[bin_i] = lh[bin_i] + mw * (1.0f - frac);
+        lh[bin_r] = lh[bin_r] + mw * frac;
+    }
+    __syncwarp();
+    float* hist = hist_all[warp];
+    for (int b = 0; b < 36; ++b) {
+        float val = lh[b];
+        val += __shfl_down_sync(FULL_MASK, val, 16);
+        val += __shfl_down_sync(FULL_MASK, val, 8);
+        val += __shfl_down_sync(FULL_MASK, val, 4);
+        val += __shfl_down_sync(FULL_MASK, val, 2);
+        val += __shfl_down_sync(FULL_MASK, val, 1);
+        if (lane == 0) hist[b] = val;
+    }
+    __syncwarp();
+    if (lane == 0) {
+        float h[36], smooth[36];
+        for (int b = 0; b < 36; ++b) h[b] = hist[b];
+        for (int it = 0; it < 2; ++it) {
+            for (int b = 0; b < 36; ++b)
+                smooth[b] = 0.25f * h[(b + 35) % 36] + 0.5f * h[b] + 0.25f * h[(b + 1) % 36];
+            for (int b = 0; b < 36; ++b) h[b] = smooth[b];
+        }
+        float peak = 0.0f;
+        for (int b = 0; b < 36; ++b)
+            if (h[b] > peak) peak = h[b];
+        const float thr = 0.8f * peak;
+        int out = 0;
+        for (int b = 0; b < 36; ++b) {
+            if (h[b] >= thr) {
+                float l = h[(b + 35) % 36], rv = h[(b + 1) % 36];
+                if (h[b] >= l && h[b] >= rv) {
+                    float denom = l - 2.0f * h[b] + rv;
+                    float fine = (float)b + (fabsf(denom) > 1e-12f ? 0.5f * (l - rv) / denom : 0.0f);
+                    float angle = fmodf(fine / 36.0f * 360.0f + 360.0f, 360.0f);
+                    if (out < 4) a.ang[i * 4 + (out++)] = angle;
+                }
+            }
+        }
+        a.angcnt[i] = out;
+        for (int k = out; k < 4; ++k) a.ang[i * 4 + k] = -1.0f;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Expansion into oriented keypoints + output sort keys.
+// ---------------------------------------------------------------------------
+struct ExpArgs {
+    const int* kp_o;
+    const int* kp_si;
+    const float* kp_ri;
+    const float* kp_ci;
+    const uint32_t* kp_tb;
+    const int* angcnt;
+    int* ent_kp;
+    int* ent_slot;
+    uint4* keys;
+    float coord_scale[PYSIFT_MAX_OCTAVES];  // 2^o * (0.5 if doubled else 1)
+};
+
+__global__ void __launch_bounds__(1024) k_expand(const ExpArgs a, Ctrl* ctrl) {
+    __shared__ int sh[33];
+    const int n = ctrl->n_kept;
+    int base = 0;
+    for (int c0 = 0; c0 < n; c0 += blockDim.x) {
+        int i = c0 + threadIdx.x;
+        int cnt = (i < n) ? a.angcnt[i] : 0;
+        int tot;
+        int pos = base + block_excl_scan(cnt, &tot, sh);
+        if (cnt) {
+            const int o = a.kp_o[i];
+            const float sc = a.coord_scale[o];
+            const float x = a.kp_ci[i] * sc, y = a.kp_ri[i] * sc;
+            for (int k = 0; k < cnt; ++k) {
+                a.ent_kp[pos + k] = i;
+                a.ent_slot[pos + k] = k;
+                a.keys[pos + k] = make_uint4(__float_as_uint(x), __float_as_uint(y), a.kp_tb[i],
+                                             (uint32_t)(i * 4 + k));
+            }
+        }
+        base += tot;
+    }
+    if (threadIdx.x == 0) ctrl->n_oriented = base;
+}
+
+__device__ __forceinline__ bool key_less(const uint4& p, const uint4& q) {
+    if (p.x != q.x) return p.x < q.x;
+    if (p.y != q.y) return p.y < q.y;
+    if (p.z != q.z) return p.z < q.z;
+    return p.w < q.w;
+}
+
+constexpr int RANK_TILE = 1024;
+
+__global__ void __launch_bounds__(256) k_rank(const uint4* __restrict__ keys, int* __restrict__ rank,
+                                              const Ctrl* ctrl) {
+    __shared__ uint4 tile[RANK_TILE];
+    const int n = ctrl->n_oriented;
+    if ((int)(blockIdx.x * blockDim.x) >= n) return;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    uint4 me = (e < n) ? keys[e] : make_uint4(0, 0, 0, 0);
+    int cnt = 0;
+    for (int t0 = 0; t0 < n; t0 += RANK_TILE) {
+        __syncthreads();
+        for (int k = threadIdx.x; k < RANK_TILE && t0 + k < n; k += blockDim.x) tile[k] = keys[t0 + k];
+        __syncthreads();
+        const int m = min(RANK_TILE, n - t0);
+        for (int k = 0; k < m; ++k) cnt += key_less(tile[k], me) ? 1 : 0;
+    }
+    if (e < n) rank[e] = cnt;
+}
+
+// ---------------------------------------------------------------------------
+// A11: descriptor.
+// ---------------------------------------------------------------------------
+struct DescArgs {
+    OctView oct[PYSIFT_MAX_OCTAVES];
+    float desc_ph[PYSIFT_MAX_LEVELS];
+    float kp_size[PYSIFT_MAX_OCTAVES][PYSIFT_MAX_LEVELS];
+    float coord_scale[PYSIFT_MAX_OCTAVES];
+    float dsp_scales[8];
+    int n_dsp;  // 0 = single scale
+    int rootsift;
+    const int* kp_o;
+    const int* kp_si;
+    const float* kp_ri;
+    const float* kp_ci;
+    const float* kp_resp;
+    const float* ang;
+    const int* ent_kp;
+    const int* ent_slot;
+    const int* rank;
+    float* out_kpts;
+    float* out_resp;
+    int* out_oct;
+    float* out_desc;
+};
+
+constexpr int DESC_WARPS = 2;
+constexpr int DESC_HSTRIDE = 129;
+
+__device__ __forceinline__ void desc_accumulate(const float* __restrict__ g, long long P, int H, int W, float ri,
+                                                float ci, float cos_a, float sin_a, float ang_rad, int ph,
+                                                float* __restrict__ part, int lane) {
+    const float scale_sp = 4.0f / (2.0f * (float)ph);
+    const float sigma_d = (float)ph * 0.5657f;
+    const float inv_2s2 = 1.0f / (2.0f * sigma_d * sigma_d + 1e-12f);
+    const int side = 2 * ph + 1;
+    const int total = side * side;
+    const int r0 = (int)ri, c0 = (int)ci;
+    for (int flat = lane; flat < total; flat += 32) {
+        int r_off = flat / side - ph;
+        int c_off = flat % side - ph;
+        int rr = r0 + r_off, cc = c0 + c_off;
+        if (rr < 1 || rr >= H - 1 || cc < 1 || cc >= W - 1) continue;
+        float fc = (float)c_off, fr = (float)r_off;
+        float xr = cos_a * fc - sin_a * fr;
+        float yr = sin_a * fc + cos_a * fr;
+        float xb = xr * scale_sp + 1.5f;
+        float yb = yr * scale_sp + 1.5f;
+        if (xb < -0.5f || xb >= 3.5f || yb < -0.5f || yb >= 3.5f) continue;
+        float dx = g[rr * P + cc + 1] - g[rr * P + cc - 1];
+        float dy = g[(rr + 1) * P + cc] - g[(rr - 1) * P + cc];
+        float mag = sqrtf(dx * dx + dy * dy);
+        float ori_deg = fmodf((sm::atan2f_(dy, dx) - ang_rad) * 57.29577951f + 360.0f, 360.0f);
+        float gw = sm::expf_(-(xr * xr + yr * yr) * inv_2s2);
+        float wmag = mag * gw;
+        float ob = ori_deg * 0.02222222f;
+        int oi0 = (int)floorf(ob);
+        float df = ob - (float)oi0;
+        int xi0 = (int)floorf(xb), yi0 = (int)floorf(yb);
+        float dx_b = xb - (float)xi0, dy_b = yb - (float)yi0;
+        int xi0c = max(0, min(xi0, 3));
+        int yi0c = max(0, min(yi0, 3));
+        int xi1c = max(0, min(xi0 + 1, 3));
+        int yi1c = max(0, min(yi0 + 1, 3));
+        int oi0w = ((oi0 % 8) + 8) % 8;
+        int oi1w = ((oi0 + 1) % 8 + 8) % 8;
+        float w_y0 = 1.0f - dy_b, w_y1 = dy_b;
+        float w_x0 = 1.0f - dx_b, w_x1 = dx_b;
+        float w_o0 = 1.0f - df, w_o1 = df;
+        part[yi0c * 32 + xi0c * 8 + oi0w] += w_y0 * w_x0 * w_o0 * wmag;
+        part[yi0c * 32 + xi0c * 8 + oi1w] += w_y0 * w_x0 * w_o1 * wmag;
+        part[yi0c * 32 + xi1c * 8 + oi0w] += w_y0 * w_x1 * w_o0 * wmag;
+        part[yi0c * 32 + xi1c * 8 + oi1w] += w_y0 * w_x1 * w_o1 * wmag;
+        part[yi1c * 32 + xi0c * 8 + oi0w] += w_y1 * w_x0 * w_o0 * wmag;
+        part[yi1c * 32 + xi0c * 8 + oi1w] += w_y1 * w_x0 * w_o1 * wmag;
+        part[yi1c * 32 + xi1c * 8 + oi0w] += w_y1 * w_x1 * w_o0 * wmag;
+        part[yi1c * 32 + xi1c * 8 + oi1w] += w_y1 * w_x1 * w_o1 * wmag;
+    }
+}
+
+__device__ __forceinline__ float warp_tree_sum(float v) {
+    v += __shfl_down_sync(FULL_MASK, v, 16);
+    v += __shfl_down_sync(FULL_MASK, v, 8);
+    v += __shfl_down_sync(FULL_MASK, v, 4);
+    v += __shfl_down_sync(FULL_MASK, v, 2);
+    v += __shfl_down_sync(FULL_MASK, v, 1);
+    return __shfl_sync(FULL_MASK, v, 0);
+}
+
+// Sum over the 128 bins in the reference's order: a warp tree per 32 bins,
+// then the four warp partials in order.  Lane j holds bins j + 32q.
+__device__ __forceinline__ float bins_sum_sq(const float v[4]) {
+    float w0 = warp_tree_sum(v[0] * v[0]), w1 = warp_tree_sum(v[1] * v[1]);
+    float w2 = warp_tree_sum(v[2] * v[2]), w3 = warp_tree_sum(v[3] * v[3]);
+    return w0 + w1 + w2 + w3;
+}
+
+__global__ void __launch_bounds__(DESC_WARPS * 32) k_descriptor(const DescArgs a, const Ctrl* ctrl) {
+    __shared__ float part_all[DESC_WARPS][32 * DESC_HSTRIDE];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int e = blockIdx.x * DESC_WARPS + warp;
+    if (e >= ctrl->n_oriented) return;
+    float* mine = part_all[warp] + lane * DESC_HSTRIDE;
+    for (int b = 0; b < 128; ++b) mine[b] = 0.0f;
+    const int kp = a.ent_kp[e], slot = a.ent_slot[e];
+    const int o = a.kp_o[kp], si = a.kp_si[kp];
+    const float ri = a.kp_ri[kp], ci = a.kp_ci[kp];
+    const float angle = a.ang[kp * 4 + slot];
+    const float ang_rad = angle * (float)(3.14159265358979323846 / 180.0);
+    const float phf = a.desc_ph[si];
+    const OctView& v = a.oct[o];
+    float sin_a, cos_a;
+    sm::sincosf_(ang_rad, &sin_a, &cos_a);
+    const float* g = v.lev[si];
+    if (a.n_dsp > 0) {
+        for (int d = 0; d < a.n_dsp; ++d) {
+            int ph = (int)(phf * a.dsp_scales[d] + 0.5f);
+            if (ph < 4) ph = 4;
+            desc_accumulate(g, v.pitch, v.H, v.W, ri, ci, cos_a, sin_a, ang_rad, ph, mine, lane);
+        }
+    } else {
+        desc_accumulate(g, v.pitch, v.H, v.W, ri, ci, cos_a, sin_a, ang_rad, (int)phf, mine, lane);
+    }
+    __syncwarp();
+    const float* base = part_all[warp];
+    float vq[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int b = q * 32 + lane;
+        float acc = base[b];
+        for (int l = 1; l < 32; ++l) acc = acc + base[l * DESC_HSTRIDE + b];
+        vq[q] = acc;
+    }
+    if (a.n_dsp > 0) {
+        const float inv_n = 1.0f / (float)a.n_dsp;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) vq[q] = vq[q] * inv_n;
+    }
+    float inv = 1.0f / sqrtf(bins_sum_sq(vq) + 1e-14f);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        float t = vq[q] * inv;
+        vq[q] = t > 0.2f ? 0.2f : t;
+    }
+    inv = 1.0f / sqrtf(bins_sum_sq(vq) + 1e-14f);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) vq[q] = vq[q] * inv;
+    if (a.rootsift) {
+        float l0 = warp_tree_sum(fabsf(vq[0])), l1 = warp_tree_sum(fabsf(vq[1]));
+        float l2 = warp_tree_sum(fabsf(vq[2])), l3 = warp_tree_sum(fabsf(vq[3]));
+        const float den = (l0 + l1 + l2 + l3) + 1e-7f;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            float t = vq[q] / den;
+            if (t < 0.0f) t = 0.0f;
+            vq[q] = sqrtf(t);
+        }
+    }
+    const int row = a.rank[e];
+    float* dst = a.out_desc + (long long)row * 128;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) dst[q * 32 + lane] = vq[q];
+    if (lane == 0) {
+        const float sc = a.coord_scale[o];
+        a.out_kpts[row * 4 + 0] = ci * sc;
+        a.out_kpts[row * 4 + 1] = ri * sc;
+        a.out_kpts[row * 4 + 2] = a.kp_size[o][si];
+        a.out_kpts[row * 4 + 3] = angle;
+        a.out_resp[row] = a.kp_resp[kp];
+        a.out_oct[row] = o;
+    }
+}
+
+__global__ void k_finalize(const Ctrl* ctrl, int32_t* stats, int n_oct, int doubled) {
+    int t = threadIdx.x;
+    if (t < PYSIFT_STAT_COUNT) stats[t] = 0;
+    __syncthreads();
+    if (t == 0) {
+        int nref = 0;
+        for (int o = 0; o < n_oct; ++o) nref += ctrl->nref[o];
+        stats[PYSIFT_STAT_N_KEYPOINTS] = ctrl->n_oriented;
+        stats[PYSIFT_STAT_N_REFINED] = nref;
+        stats[PYSIFT_STAT_N_KEPT] = ctrl->n_kept;
+        stats[PYSIFT_STAT_RETRIED] = ctrl->retried;
+        stats[PYSIFT_STAT_CAPPED] = ctrl->capped;
+        stats[PYSIFT_STAT_DOUBLED] = doubled;
+        stats[PYSIFT_STAT_CAND_OVERFLOW] = ctrl->overflow_octs;
+        for (int o = 0; o < n_oct; ++o) {
+            stats[PYSIFT_STAT_CANDS + o] = ctrl->found[o];
+            stats[PYSIFT_STAT_REFINED_OCT + o] = ctrl->nref[o];
+        }
+        stats[PYSIFT_STAT_THRESH_BITS] = (int32_t)__float_as_uint(ctrl->thr[ctrl->retried ? 1 : 0]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host side.
+// ---------------------------------------------------------------------------
+template <typename T>
+static T* at(void* ws, size_t off) {
+    return reinterpret_cast<T*>(static_cast<char*>(ws) + off);
+}
+
+static void fill_oct_views(const Layout& l, void* ws, bool rounded, OctView* out) {
+    for (int o = 0; o < l.n_oct; ++o) {
+        size_t off = rounded ? l.off_pyr_r[o] : l.off_pyr[o];
+        float* base = at<float>(ws, off);
+        for (int s = 0; s < PYSIFT_MAX_LEVELS; ++s)
+            out[o].lev[s] = (s < l.L) ? base + (size_t)s * l.H[o] * l.pitch[o] : nullptr;
+        out[o].H = l.H[o];
+        out[o].W = l.W[o];
+        out[o].pitch = l.pitch[o];
+    }
+}
+
+static int g_num_sms = 0;
+
+static int num_sms() {
+    if (g_num_sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        int n = 0;
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        g_num_sms = n > 0 ? n : 148;
+    }
+    return g_num_sms;
+}
+
+static int record_stage(void* const* ev, int i, cudaStream_t st) {
+    if (ev && ev[i]) PYSIFT_CUDA_TRY(cudaEventRecord(reinterpret_cast<cudaEvent_t>(ev[i]), st));
+    return PYSIFT_OK;
+}
+
+#define PYSIFT_STAGE(i)                              \
+    do {                                             \
+        int rc_ = record_stage(stage_events, i, st); \
+        if (rc_) return rc_;                         \
+    } while (0)
+
+static int run_detect(const pysift_detect_config* cfg, const uint8_t* gray, int H, int W, long long pitch,
+                      void* ws, const Layout& l, float* kpts, float* resp, int32_t* octv, float* desc,
+                      int32_t* stats, void* const* stage_events, cudaStream_t st) {
+    PYSIFT_STAGE(0);
+    const int S = l.S, n_oct = l.n_oct;
+    const int cap = cfg->max_cands_per_octave, kcap = cfg->keypoint_cap;
+    Ctrl* ctrl = at<Ctrl>(ws, l.off_ctrl);
+    PYSIFT_CUDA_TRY(cudaMemsetAsync(ctrl, 0, sizeof(Ctrl), st));
+    // A1
+    {
+        long long n = (long long)H * W;
+        int blocks = (int)std::min<long long>(ceil_div_ll(n, 256 * 16), (long long)num_sms() * 4);
+        if (blocks < 1) blocks = 1;
+        k_histogram<<<blocks, 256, 0, st>>>(gray, H, W, pitch, ctrl, cfg->contrast_thresh, S);
+        PYSIFT_LAUNCH_CHECK("k_histogram");
+    }
+    // A2/A3: base image
+    float* base = at<float>(ws, l.off_base);
+    if (l.doubled) {
+        double* coef = at<double>(ws, l.off_coef);
+        k_prefilter_cols<<<ceil_div(W, 128), 128, 0, st>>>(gray, H, W, pitch, cfg->fp16_pyramid, coef);
+        PYSIFT_LAUNCH_CHECK("k_prefilter_cols");
+        k_prefilter_rows<<<ceil_div(H, 128), 128, 0, st>>>(coef, H, W);
+        PYSIFT_LAUNCH_CHECK("k_prefilter_rows");
+        k_zoom_interp<<<dim3(ceil_div(2 * W, 256), 2 * H), 256, 0, st>>>(coef, H, W, cfg->fp16_pyramid, base,
+                                                                         l.pitch0);
+        PYSIFT_LAUNCH_CHECK("k_zoom_interp");
+    } else {
+        k_u8_to_f32<<<dim3(ceil_div(W, 256), H), 256, 0, st>>>(gray, H, W, pitch, cfg->fp16_pyramid, base,
+                                                               l.pitch0);
+        PYSIFT_LAUNCH_CHECK("k_u8_to_f32");
+    }
+    PYSIFT_STAGE(1);
+    // A4/A5: pyramid
+    {
+        static thread_local BlurArgs a;  // large (weights by value); not on the stack
+        for (int o = 0; o < n_oct; ++o) {
+            float* pyr = at<float>(ws, l.off_pyr[o]);
+            float* pyr_r = (l.off_pyr_r[o] != l.off_pyr[o]) ? at<float>(ws, l.off_pyr_r[o]) : nullptr;
+            const size_t lev = (size_t)l.H[o] * l.pitch[o];
+            // level 0
+            memset(&a, 0, sizeof(a));
+            a.H = l.H[o];
+            a.W = l.W[o];
+            a.out_pitch = l.pitch[o];
+            if (o == 0) {
+                int k = l.doubled ? 0 : 1;
+                a.in = base;
+                a.in_pitch = l.pitch0;
+                a.step = 1;
+                a.out = pyr;
+                a.out_r = pyr_r;
+                int rc = launch_blur(a, cfg->blur_radius[k], cfg->blur_weights[k], st);
+                if (rc) return rc;
+            }
+            for (int s = 0; s < S + 2; ++s) {
+                memset(&a, 0, sizeof(a));
+                a.H = l.H[o];
+                a.W = l.W[o];
+                a.out_pitch = l.pitch[o];
+                if (s == 0 && o > 0) {
+                    const float* prev = at<float>(ws, l.off_pyr[o - 1]) + (size_t)S * l.H[o - 1] * l.pitch[o - 1];
+                    a.in = prev;
+                    a.in_pitch = l.pitch[o - 1];
+                    a.step = 2;
+                    a.copy0 = pyr;
+                    a.copy0_r = pyr_r;
+                } else {
+                    a.in = pyr + (size_t)s * lev;
+                    a.in_pitch = l.pitch[o];
+                    a.step = 1;
+                }
+                a.out = pyr + (size_t)(s + 1) * lev;
+                a.out_r = pyr_r ? pyr_r + (size_t)(s + 1) * lev : nullptr;
+                int rc = launch_blur(a, cfg->blur_radius[2 + s], cfg->blur_weights[2 + s], st);
+                if (rc) return rc;
+            }
+        }
+    }
+    PYSIFT_STAGE(2);
+    // A7/A8 (+ retry)
+    static thread_local ExtArgs ea;
+    static thread_local RefArgs ra;
+    memset(&ea, 0, sizeof(ea));
+    memset(&ra, 0, sizeof(ra));
+    fill_oct_views(l, ws, true, ea.oct);
+    fill_oct_views(l, ws, true, ra.oct);
+    ea.n_oct = ra.n_oct = n_oct;
+    ea.S = ra.S = S;
+    ea.border = ra.border = cfg->border;
+    ea.cap = ra.cap = cap;
+    ea.cand = at<int4>(ws, l.off_cand);
+    ra.cand = ea.cand;
+    int mask_blocks = 0, row_blocks = 0;
+    int row_off[PYSIFT_MAX_OCTAVES + 1];
+    for (int o = 0; o < n_oct; ++o) {
+        ea.blk_off[o] = mask_blocks;
+        mask_blocks += ceil_div(l.H[o] * l.wpr[o], 8);
+        row_off[o] = row_blocks;
+        row_blocks += ceil_div(S * l.H[o], 8);
+        ea.mask[o] = at<uint32_t>(ws, l.off_mask[o]);
+        ea.rowcnt[o] = at<int>(ws, l.off_rowcnt[o]);
+        ea.rowoff[o] = at<int>(ws, l.off_rowoff[o]);
+        ea.wpr[o] = l.wpr[o];
+    }
+    ea.blk_off[n_oct] = mask_blocks;
+    row_off[n_oct] = row_blocks;
+    ra.edge_score = cfg->edge_score;
+    ra.rv_valid = at<int>(ws, l.off_rv_valid);
+    ra.rv_ri = at<float>(ws, l.off_rv_ri);
+    ra.rv_ci = at<float>(ws, l.off_rv_ci);
+    ra.rv_si = at<int>(ws, l.off_rv_si);
+    ra.rv_resp = at<float>(ws, l.off_rv_resp);
+    ra.rf_ri = at<float>(ws, l.off_rf_ri);
+    ra.rf_ci = at<float>(ws, l.off_rf_ci);
+    ra.rf_si = at<int>(ws, l.off_rf_si);
+    ra.rf_resp = at<float>(ws, l.off_rf_resp);
+    const int refine_blocks = (int)std::min<long long>(ceil_div_ll((long long)n_oct * cap, 256), num_sms() * 8);
+    for (int pass = 0; pass < 2; ++pass) {
+        ea.thr_idx = ra.thr_idx = pass;
+        ea.retry_mode = ra.retry_mode = pass;
+        PYSIFT_CUDA_TRY(cudaMemsetAsync(at<char>(ws, l.off_rowcnt_base), 0, l.rowcnt_bytes_total, st));
+        k_extrema_mask<<<mask_blocks, 256, 0, st>>>(ea, ctrl);
+        PYSIFT_LAUNCH_CHECK("k_extrema_mask");
+        if (pass == 0) PYSIFT_STAGE(3);
+        k_rowscan<<<n_oct, 1024, 0, st>>>(ea, ctrl);
+        PYSIFT_LAUNCH_CHECK("k_rowscan");
+        // k_scatter indexes blocks by (s, r) rows: reuse blk_off for its own table
+        ExtArgs& sa = ea;
+        int saved[PYSIFT_MAX_OCTAVES + 1];
+        memcpy(saved, sa.blk_off, sizeof(saved));
+        memcpy(sa.blk_off, row_off, sizeof(row_off));
+        k_scatter<<<row_blocks, 256, 0, st>>>(sa, ctrl);
+        PYSIFT_LAUNCH_CHECK("k_scatter");
+        memcpy(sa.blk_off, saved, sizeof(saved));
+        k_refine<<<refine_blocks, 256, 0, st>>>(ra, ctrl);
+        PYSIFT_LAUNCH_CHECK("k_refine");
+        k_refine_compact<<<n_oct, 1024, 0, st>>>(ra, ctrl);
+        PYSIFT_LAUNCH_CHECK("k_refine_compact");
+        if (pass == 0) {
+            k_retry_decide<<<1, 1, 0, st>>>(ctrl, n_oct, cfg->starvation_min);
+            PYSIFT_LAUNCH_CHECK("k_retry_decide");
+        }
+    }
+    // A9
+    CapArgs ca;
+    ca.n_oct = n_oct;
+    ca.cap_cand = cap;
+    ca.kp_cap = kcap;
+    ca.rf_ri = ra.rf_ri;
+    ca.rf_ci = ra.rf_ci;
+    ca.rf_si = ra.rf_si;
+    ca.rf_resp = ra.rf_resp;
+    ca.kp_o = at<int>(ws, l.off_kp_o);
+    ca.kp_si = at<int>(ws, l.off_kp_si);
+    ca.kp_ri = at<float>(ws, l.off_kp_ri);
+    ca.kp_ci = at<float>(ws, l.off_kp_ci);
+    ca.kp_resp = at<float>(ws, l.off_kp_resp);
+    ca.kp_tb = at<uint32_t>(ws, l.off_kp_tb);
+    k_cap<<<1, 1024, 0, st>>>(ca, ctrl);
+    PYSIFT_LAUNCH_CHECK("k_cap");
+    PYSIFT_STAGE(4);
+    // A10
+    static thread_local OriArgs oa;
+    memset(&oa, 0, sizeof(oa));
+    fill_oct_views(l, ws, true, oa.oct);
+    for (int s = 0; s < PYSIFT_MAX_LEVELS; ++s) oa.ori_sigma[s] = cfg->ori_sigma[s];
+    oa.kp_o = ca.kp_o;
+    oa.kp_si = ca.kp_si;
+    oa.kp_ri = ca.kp_ri;
+    oa.kp_ci = ca.kp_ci;
+    oa.ang = at<float>(ws, l.off_ang);
+    oa.angcnt = at<int>(ws, l.off_angcnt);
+    k_orientation<<<ceil_div(kcap, ORI_WARPS), ORI_WARPS * 32, 0, st>>>(oa, ctrl);
+    PYSIFT_LAUNCH_CHECK("k_orientation");
+    // expansion + keys + rank
+    ExpArgs xa;
+    memset(&xa, 0, sizeof(xa));
+    xa.kp_o = ca.kp_o;
+    xa.kp_si = ca.kp_si;
+    xa.kp_ri = ca.kp_ri;
+    xa.kp_ci = ca.kp_ci;
+    xa.kp_tb = ca.kp_tb;
+    xa.angcnt = oa.angcnt;
+    xa.ent_kp = at<int>(ws, l.off_ent_kp);
+    xa.ent_slot = at<int>(ws, l.off_ent_slot);
+    xa.keys = at<uint4>(ws, l.off_keys);
+    for (int o = 0; o < n_oct; ++o) xa.coord_scale[o] = (float)((double)(1 << o) * (l.doubled ? 0.5 : 1.0));
+    k_expand<<<1, 1024, 0, st>>>(xa, ctrl);
+    PYSIFT_LAUNCH_CHECK("k_expand");
+    int* rank = at<int>(ws, l.off_rank);
+    k_rank<<<ceil_div(4 * kcap, 256), 256, 0, st>>>(xa.keys, rank, ctrl);
+    PYSIFT_LAUNCH_CHECK("k_rank");
+    PYSIFT_STAGE(5);
+    // A11
+    static thread_local DescArgs da;
+    memset(&da, 0, sizeof(da));
+    fill_oct_views(l, ws, true, da.oct);
+    for (int s = 0; s < PYSIFT_MAX_LEVELS; ++s) da.desc_ph[s] = cfg->desc_ph[s];
+    for (int o = 0; o < n_oct; ++o) {
+        for (int s = 0; s < PYSIFT_MAX_LEVELS; ++s) da.kp_size[o][s] = cfg->kp_size[l.doubled ? 1 : 0][o][s];
+        da.coord_scale[o] = xa.coord_scale[o];
+    }
+    da.n_dsp = cfg->dsp ? cfg->n_dsp : 0;
+    for (int d = 0; d < 8; ++d) da.dsp_scales[d] = cfg->dsp_scales[d];
+    da.rootsift = cfg->rootsift;
+    da.kp_o = ca.kp_o;
+    da.kp_si = ca.kp_si;
+    da.kp_ri = ca.kp_ri;
+    da.kp_ci = ca.kp_ci;
+    da.kp_resp = ca.kp_resp;
+    da.ang = oa.ang;
+    da.ent_kp = xa.ent_kp;
+    da.ent_slot = xa.ent_slot;
+    da.rank = rank;
+    da.out_kpts = kpts;
+    da.out_resp = resp;
+    da.out_oct = octv;
+    da.out_desc = desc;
+    k_descriptor<<<ceil_div(4 * kcap, DESC_WARPS), DESC_WARPS * 32, 0, st>>>(da, ctrl);
+    PYSIFT_LAUNCH_CHECK("k_descriptor");
+    k_finalize<<<1, 32, 0, st>>>(ctrl, stats, n_oct, l.doubled ? 1 : 0);
+    PYSIFT_LAUNCH_CHECK("k_finalize");
+    PYSIFT_STAGE(6);
+    return PYSIFT_OK;
+}
+
+}  // namespace pysift
+
+using namespace pysift;
+
+extern "C" {
+
+const char* pysift_last_error(void) { return g_last_error.c_str(); }
+
+const char* pysift_b200_version(void) { return "pysift_b200 0.1.0 (sm_100a)"; }
+
+size_t pysift_detect_config_size(void) { return sizeof(pysift_detect_config); }
+
+int pysift_detect_workspace_size(const pysift_detect_config* cfg, int32_t H, int32_t W, size_t* bytes) {
+    int rc = validate_cfg(cfg);
+    if (rc) return rc;
+    PYSIFT_CHECK_ARG(H > 0 && W > 0, "image size %dx%d must be positive", H, W);
+    PYSIFT_CHECK_ARG(bytes != nullptr, "bytes is NULL");
+    Layout l = make_layout(cfg, H, W);
+    *bytes = l.total;
+    return PYSIFT_OK;
+}
+
+int32_t pysift_detect_max_keypoints(const pysift_detect_config* cfg) {
+    if (!cfg) return 0;
+    return 4 * cfg->keypoint_cap;
+}
+
+int pysift_detect_workspace_view(const pysift_detect_config* cfg, int32_t H, int32_t W, int32_t what, int32_t octave,
+                                 int32_t level, size_t* offset, int32_t* rows, int32_t* cols, int32_t* pitch_floats) {
+    int rc = validate_cfg(cfg);
+    if (rc) return rc;
+    PYSIFT_CHECK_ARG(H > 0 && W > 0, "image size %dx%d must be positive", H, W);
+    PYSIFT_CHECK_ARG(offset && rows && cols && pitch_floats, "NULL output pointer");
+    Layout l = make_layout(cfg, H, W);
+    if (what == 0) {
+        PYSIFT_CHECK_ARG(octave >= 0 && octave < l.n_oct && level >= 0 && level < l.L, "octave/level out of range");
+        *offset = l.off_pyr_r[octave] + (size_t)level * l.H[octave] * l.pitch[octave] * sizeof(float);
+        *rows = l.H[octave];
+        *cols = l.W[octave];
+        *pitch_floats = l.pitch[octave];
+    } else if (what == 1) {
+        *offset = l.off_base;
+        *rows = l.H0;
+        *cols = l.W0;
+        *pitch_floats = l.pitch0;
+    } else {
+        set_error("unknown view %d", what);
+        return PYSIFT_ERR_INVALID_ARG;
+    }
+    return PYSIFT_OK;
+}
+
+int pysift_detect_and_compute(const pysift_detect_config* cfg, const uint8_t* gray, int32_t H, int32_t W,
+                              int64_t pitch_bytes, void* workspace, size_t workspace_bytes, float* kpts,
+                              float* response, int32_t* octave, float* desc, int32_t max_out, int32_t* stats,
+                              void* const* stage_events, pysift_stream_t stream) {
+    int rc = validate_cfg(cfg);
+    if (rc) return rc;
+    PYSIFT_CHECK_ARG(H > 0 && W > 0, "image size %dx%d must be positive", H, W);
+    PYSIFT_CHECK_ARG(pitch_bytes >= W, "pitch %lld smaller than width %d", (long long)pitch_bytes, W);
+    PYSIFT_CHECK_ARG(gray && workspace && kpts && response && octave && desc && stats, "NULL pointer argument");
+    Layout l = make_layout(cfg, H, W);
+    if (workspace_bytes < l.total) {
+        set_error("workspace %zu bytes < required %zu", workspace_bytes, l.total);
+        return PYSIFT_ERR_WORKSPACE;
+    }
+    if (max_out < 4 * cfg->keypoint_cap) {
+        set_error("max_out %d < 4 * keypoint_cap (%d)", max_out, 4 * cfg->keypoint_cap);
+        return PYSIFT_ERR_CAPACITY;
+    }
+    if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0) {
+        set_error("workspace must be 256-byte aligned");
+        return PYSIFT_ERR_INVALID_ARG;
+    }
+    return run_detect(cfg, gray, H, W, pitch_bytes, workspace, l, kpts, response, octave, desc, stats,
+                      stage_events, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int pysift_gauss_blur(const float* in, int32_t in_pitch, float* out, int32_t out_pitch, int32_t H, int32_t W,
+                      const float* weights, int32_t radius, pysift_stream_t stream) {
+    PYSIFT_CHECK_ARG(in && out && weights, "NULL pointer argument");
+    PYSIFT_CHECK_ARG(H > 0 && W > 0 && in_pitch >= W && out_pitch >= W, "bad sizes");
+    PYSIFT_CHECK_ARG(radius >= 0 && radius <= PYSIFT_MAX_RADIUS, "radius %d outside 0..%d", radius,
+                     PYSIFT_MAX_RADIUS);
+    static thread_local BlurArgs a;
+    memset(&a, 0, sizeof(a));
+    a.in = in;
+    a.in_pitch = in_pitch;
+    a.step = 1;
+    a.out = out;
+    a.out_pitch = out_pitch;
+    a.H = H;
+    a.W = W;
+    return launch_blur(a, radius, weights, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int pysift_zoom2x_u8(const uint8_t* gray, int32_t H, int32_t W, int64_t pitch_bytes, int32_t fp16_round,
+                     double* coef, float* out, int32_t out_pitch, pysift_stream_t stream) {
+    PYSIFT_CHECK_ARG(gray && coef && out, "NULL pointer argument");
+    PYSIFT_CHECK_ARG(H > 0 && W > 0 && pitch_bytes >= W && out_pitch >= 2 * W, "bad sizes");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    k_prefilter_cols<<<ceil_div(W, 128), 128, 0, st>>>(gray, H, W, pitch_bytes, fp16_round, coef);
+    PYSIFT_LAUNCH_CHECK("k_prefilter_cols");
+    k_prefilter_rows<<<ceil_div(H, 128), 128, 0, st>>>(coef, H, W);
+    PYSIFT_LAUNCH_CHECK("k_prefilter_rows");
+    k_zoom_interp<<<dim3(ceil_div(2 * W, 256), 2 * H), 256, 0, st>>>(coef, H, W, fp16_round, out, out_pitch);
+    PYSIFT_LAUNCH_CHECK("k_zoom_interp");
+    return PYSIFT_OK;
+}
+
+}  // extern "C"

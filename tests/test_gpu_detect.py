@@ -1,0 +1,142 @@
+"""GPU parity of detectAndCompute against the CPU oracle (bit-exact).
+
+The CUDA path runs through the C ABI (pysift_detect_and_compute) via the
+PySIFT drop-in class; the oracle restates the reference's algorithm on the
+CPU.  Every output row -- x, y, size, angle, response, octave and all 128
+descriptor values -- must be identical, as must the Gaussian pyramid.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from pysift_b200 import synthetic
+
+pytestmark = pytest.mark.gpu
+
+
+def _run_both(img, oracle_lib, **kw):
+    import torch
+    from pysift_b200 import PySIFT
+    sift = PySIFT(**kw)
+    out = sift.detect_arrays(img)
+    okw = dict(kw)
+    hv = okw.pop("high_vram", True)
+    orc = oracle_lib.OracleSIFT(high_vram=hv, **okw)
+    ref = orc.detect_and_compute(img)
+    return sift, out, ref
+
+
+def _pyramid_equal(sift, img, ref):
+    import torch
+    from pysift_b200 import _lib
+    H, W = img.shape
+    b = sift._bufs[(H, W)]
+    lib = sift._lib
+    ws = b.ws
+    bad = []
+    for o, g in enumerate(ref["pyramid"]):
+        for s in range(g.shape[0]):
+            off, rows, cols, pitch = ctypes.c_size_t(), ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+            rc = lib.pysift_detect_workspace_view(ctypes.byref(sift._cfg), H, W, 0, o, s, ctypes.byref(off),
+                                                  ctypes.byref(rows), ctypes.byref(cols), ctypes.byref(pitch))
+            assert rc == 0
+            start = b.ws_off + off.value
+            n = rows.value * pitch.value * 4
+            arr = ws[start:start + n].view(torch.float32).view(rows.value, pitch.value)[:, :cols.value].cpu().numpy()
+            if not np.array_equal(arr, g[s]):
+                d = np.abs(arr - g[s])
+                bad.append((o, s, float(d.max()), int((d > 0).sum())))
+    return bad
+
+
+def _compare(out, ref):
+    n_gpu, n_ref = len(out["x"]), len(ref["x"])
+    assert n_gpu == n_ref, f"keypoint count {n_gpu} != oracle {n_ref}"
+    for k in ("x", "y", "size", "angle", "response", "octave"):
+        a, b = out[k], ref[k]
+        assert np.array_equal(a, b), f"{k}: {int(np.sum(a != b))} rows differ"
+    d = out["desc"]
+    assert np.array_equal(d, ref["desc"]), f"desc: max diff {np.abs(d - ref['desc']).max()}"
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_cfg1_scene_bit_exact(seed, oracle_lib):
+    img = synthetic.scene(480, 640, seed=seed)
+    sift, out, ref = _run_both(img, oracle_lib)
+    bad = _pyramid_equal(sift, img, ref)
+    assert not bad, f"pyramid levels differ (octave, level, max|d|, count): {bad[:6]}"
+    st = sift.last_stats
+    assert st[1] == ref["n_refined"] or ref["capped"]
+    _compare(out, ref)
+
+
+@pytest.mark.parametrize("shape", [(37, 53), (12, 16), (121, 90)])
+def test_odd_sizes(shape, oracle_lib):
+    img = synthetic.scene(shape[0], shape[1], seed=7)
+    sift, out, ref = _run_both(img, oracle_lib)
+    assert not _pyramid_equal(sift, img, ref)
+    _compare(out, ref)
+
+
+def test_no_doubling(oracle_lib):
+    img = synthetic.scene(480, 640, seed=3)
+    sift, out, ref = _run_both(img, oracle_lib, double_image=False)
+    assert sift.last_stats[5] == 0
+    _compare(out, ref)
+
+
+def test_fp16_dsp_low_vram_tier(oracle_lib):
+    """The configuration of the reference's golden dumps: 4 octaves, fp16
+    pyramid, DSP-5 descriptors, 4 MP doubling cap."""
+    img = synthetic.scene(300, 400, seed=4)
+    sift, out, ref = _run_both(img, oracle_lib, n_octaves=4, dsp=True, dsp_n_scales=5, fp16_pyramid=True,
+                               high_vram=False)
+    assert not _pyramid_equal(sift, img, ref)
+    _compare(out, ref)
+
+
+def test_starvation_retry(oracle_lib):
+    """Few keypoints -> the half-threshold retry runs (pysift/core.py:2066-2071)."""
+    H, W = 200, 240
+    yy, xx = np.mgrid[0:H, 0:W]
+    img = (128 + 60 * np.exp(-((yy - 100) ** 2 + (xx - 120) ** 2) / (2 * 20.0 ** 2))).astype(np.uint8)
+    sift, out, ref = _run_both(img, oracle_lib)
+    assert ref["retried"]
+    assert sift.last_stats[3] == 1
+    _compare(out, ref)
+
+
+def test_keypoint_cap(oracle_lib):
+    """More than 8000 refined keypoints -> top-8000 by response (pysift/core.py:2078-2080)."""
+    img = synthetic.dense_texture(800, 1000, seed=5, sigma=2.0)
+    sift, out, ref = _run_both(img, oracle_lib)
+    assert ref["capped"]
+    assert sift.last_stats[4] == 1
+    _compare(out, ref)
+
+
+def test_device_input_and_gpu_output(oracle_lib):
+    import torch
+    from pysift_b200 import PySIFT
+    img = synthetic.scene(240, 320, seed=9)
+    sift = PySIFT()
+    kp_t, desc_t = sift.detectAndCompute(torch.from_numpy(img).cuda(), gpu_output=True)
+    assert kp_t.is_cuda and desc_t.is_cuda and kp_t.shape[1] == 4 and desc_t.shape[1] == 128
+    ref = oracle_lib.OracleSIFT().detect_and_compute(img)
+    assert kp_t.shape[0] == len(ref["x"])
+    assert np.array_equal(kp_t[:, 0].cpu().numpy(), ref["x"])
+    assert np.array_equal(desc_t.cpu().numpy(), ref["desc"])
+    kps, desc = sift.detectAndCompute(img)
+    assert len(kps) == len(ref["x"]) and desc.shape == (len(ref["x"]), 128)
+    assert kps[0].pt == (float(ref["x"][0]), float(ref["y"][0]))
+
+
+def test_repeat_determinism():
+    from pysift_b200 import PySIFT
+    img = synthetic.scene(480, 640, seed=11)
+    sift = PySIFT()
+    a = sift.detect_arrays(img)
+    b = sift.detect_arrays(img)
+    for k in a:
+        assert np.array_equal(a[k], b[k])

@@ -1,0 +1,103 @@
+"""Pin the CPU oracle to the reference's own golden detectAndCompute dumps.
+
+determinism_reference/*.npz in the reference were produced by PySIFT itself
+on an RTX 3050 (n_octaves=4, DSP-5 descriptors, fp16 pyramid, 4 MP doubling
+cap; determinism_reference/manifest.json).  The reference's own check
+(tests/cross_determinism_test.py:50-121) calls two extractions EQUIVALENT at
+>= 95 % of keypoints within 0.5 px and mean descriptor cosine >= 0.99.
+
+Here the oracle, run with the same parameters on the same decoded images,
+must meet a stricter, duplicate-aware bar: >= 99 % of the reference rows
+have an oracle row within 1e-3 px whose angle agrees within 0.05 deg
+(>= 95 % with bit-identical x and y), those pairs have mean descriptor
+cosine >= 0.999, and the keypoint counts agree within 0.5 %.  The
+remaining differences come from the reference's fast-math refinement and
+atomic-order float sums.  The compact committed copy of one dump
+(tests/golden/, made by tests/golden/make_golden.py) always runs; the full
+dumps run when the reference tree is available.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF = "/root/reference"
+
+IMC_IMAGES = {
+    "imc_british_museum": "british_museum/set_100/images/00350405_2611802704.jpg",
+    "imc_florence_cathedral_side": "florence_cathedral_side/set_100/images/05246669_3774806731.jpg",
+    "imc_st_pauls_cathedral": "st_pauls_cathedral/21260922_4094863925.jpg",
+}
+
+
+def _oracle_for_fixture(oracle_lib):
+    return oracle_lib.OracleSIFT(n_octaves=4, n_scales=3, sigma0=1.6, contrast_thresh=0.04, edge_thresh=10.0,
+                                 dsp=True, dsp_n_scales=5, fp16_pyramid=True, high_vram=False)
+
+
+def pair_rows(ref_pts, ref_ang, pts, ang, tol=1e-3):
+    """For every reference row, the oracle row within `tol` px with the
+    nearest angle (-1 when none).  Returns (index, angle diff, bit-identical
+    position flag)."""
+    from scipy.spatial import cKDTree
+    tree = cKDTree(pts)
+    out = np.full(len(ref_pts), -1, np.int64)
+    dang = np.full(len(ref_pts), 360.0)
+    exact = np.zeros(len(ref_pts), bool)
+    for j, cand in enumerate(tree.query_ball_point(ref_pts, r=tol)):
+        if not cand:
+            continue
+        d = np.abs(ang[cand] - ref_ang[j])
+        d = np.minimum(d, 360 - d)
+        k = int(np.argmin(d))
+        out[j] = cand[k]
+        dang[j] = d[k]
+        exact[j] = pts[cand[k], 0] == ref_pts[j, 0] and pts[cand[k], 1] == ref_pts[j, 1]
+    return out, dang, exact
+
+
+def check_pin(r, ref_pts, ref_ang, ref_desc, desc_rows=None):
+    pts = np.stack([r["x"], r["y"]], 1)
+    n_ref = len(ref_pts)
+    assert abs(len(pts) - n_ref) <= max(2, 0.005 * n_ref), (len(pts), n_ref)
+    idx, dang, exact = pair_rows(ref_pts, ref_ang, pts, r["angle"])
+    good = (idx >= 0) & (dang < 0.05)
+    assert good.mean() >= 0.99, f"only {good.mean():.4f} of reference rows reproduced within tolerance"
+    assert (good & exact).mean() >= 0.95, f"only {(good & exact).mean():.4f} bit-identical positions"
+    rows = np.arange(n_ref) if desc_rows is None else desc_rows
+    sel = good[rows]
+    a = ref_desc[sel]
+    b = r["desc"][idx[rows][sel]]
+    cos = np.sum(a * b, 1) / (np.linalg.norm(a, axis=1) * np.linalg.norm(b, axis=1) + 1e-12)
+    assert cos.mean() >= 0.999, cos.mean()
+    # the reference's own criterion (tests/cross_determinism_test.py:112-119), position part
+    from scipy.spatial import cKDTree
+    d, _ = cKDTree(pts).query(ref_pts, k=1)
+    assert np.mean(d <= 0.5) >= 0.95
+    return good.mean(), (good & exact).mean(), cos.mean()
+
+
+def test_pin_committed_fixture(oracle_lib):
+    import cv2
+    gray = cv2.imread(os.path.join(HERE, "golden", "imc_st_pauls_cathedral_gray.png"), cv2.IMREAD_GRAYSCALE)
+    fx = np.load(os.path.join(HERE, "golden", "imc_st_pauls_cathedral.npz"))
+    assert gray.shape == tuple(fx["image_shape"][:2])
+    r = _oracle_for_fixture(oracle_lib).detect_and_compute(gray)
+    frac, frac_exact, cos = check_pin(r, fx["points"], fx["angles"], fx["descriptors"],
+                                      desc_rows=fx["desc_rows"])
+    assert cos > 0.9999
+
+
+@pytest.mark.skipif(not os.path.isdir(os.path.join(REF, "determinism_reference")), reason="reference tree absent")
+@pytest.mark.parametrize("name", sorted(IMC_IMAGES))
+def test_pin_reference_dumps(name, oracle_lib):
+    import cv2
+    with open(os.path.join(REF, "determinism_reference", "manifest.json")) as f:
+        params = json.load(f)["pysift_params"]
+    assert params["dsp"] and params["dsp_n_scales"] == 5 and params["fp16_pyramid"] and params["n_octaves"] == 4
+    gray = cv2.imread(os.path.join(REF, "test_images", "imc_phototourism", IMC_IMAGES[name]), cv2.IMREAD_GRAYSCALE)
+    fx = np.load(os.path.join(REF, "determinism_reference", name + ".npz"))
+    r = _oracle_for_fixture(oracle_lib).detect_and_compute(gray)
+    check_pin(r, fx["points"], fx["angles"], fx["descriptors"])
