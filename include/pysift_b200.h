@@ -133,6 +133,22 @@ int pysift_gauss_blur(const float* in, int32_t in_pitch, float* out, int32_t out
 int pysift_zoom2x_u8(const uint8_t* gray, int32_t H, int32_t W, int64_t pitch_bytes, int32_t fp16_round,
                      double* coef, float* out, int32_t out_pitch, pysift_stream_t stream);
 
+/* Allocation-free 2x zoom (no counterpart in the reference; it exists for
+ * callers that cannot allocate device memory at the call site, such as a
+ * plugin inside a host application that owns the device heap).  Same result
+ * as pysift_zoom2x_u8, but the coefficient scratch is a fixed file-scope
+ * device array of PYSIFT_ZOOM2X_NOALLOC_MAX_PIXELS doubles (8 MiB) that every
+ * GPU loading the library holds until exit.  Inputs larger than that
+ * (H*W > PYSIFT_ZOOM2X_NOALLOC_MAX_PIXELS) return PYSIFT_ERR_CAPACITY.
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture.  All calls share the one array: calls that
+ * overlap on the GPU (other streams, other host threads) race and must be
+ * serialised by the caller.  Allocates nothing. */
+#define PYSIFT_ZOOM2X_NOALLOC_MAX_PIXELS (1 << 20)
+int pysift_zoom2x_u8_noalloc(const uint8_t* gray, int32_t H, int32_t W, int64_t pitch_bytes, int32_t fp16_round,
+                             float* out, int32_t out_pitch, pysift_stream_t stream);
+
 const char* pysift_last_error(void);
 const char* pysift_b200_version(void);
 

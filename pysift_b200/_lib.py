@@ -87,7 +87,10 @@ EXPORTS = {
                                          c_void_p]),
     "pysift_zoom2x_u8": (ctypes.c_int, [c_void_p, c_int32, c_int32, c_int64, c_int32, c_void_p, c_void_p, c_int32,
                                         c_void_p]),
+    "pysift_zoom2x_u8_noalloc": (ctypes.c_int, [c_void_p, c_int32, c_int32, c_int64, c_int32, c_void_p, c_int32,
+                                                c_void_p]),
 }
+ZOOM2X_NOALLOC_MAX_PIXELS = 1 << 20
 
 
 def lib_path():

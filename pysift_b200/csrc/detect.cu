@@ -1667,3 +1667,77 @@ int pysift_zoom2x_u8(const uint8_t* gray, int32_t H, int32_t W, int64_t pitch_by
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of pysift_zoom2x_u8.
+//
+// Some callers cannot allocate device memory at the call site: for example a
+// plugin loaded into a host application that owns the whole device heap and
+// forbids cudaMalloc inside plugins, or code that runs under a fixed device
+// memory budget with no allocator handle to pass in.  For them this entry
+// point keeps the spline-coefficient scratch in a file-scope device array of
+// PYSIFT_ZOOM2X_NOALLOC_MAX_PIXELS doubles (8 MiB), which every GPU that
+// loads the library holds until the process exits.
+//
+// Host code cannot pass g_zoom2x_scratch to a kernel directly (in host code
+// the name is a host-side stand-in, not a device address), so the device
+// address is looked up with cudaGetSymbolAddress once per device, on the
+// first call made with that device current, and cached.
+// ---------------------------------------------------------------------------
+namespace pysift {
+
+static __device__ __align__(256) double g_zoom2x_scratch[PYSIFT_ZOOM2X_NOALLOC_MAX_PIXELS];
+
+static int zoom2x_scratch_ptr(double** out) {
+    constexpr int MAX_DEVICES = 64;
+    static std::mutex mu;
+    static double* ptrs[MAX_DEVICES] = {nullptr};
+    int dev = 0;
+    PYSIFT_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= MAX_DEVICES) {
+        set_error("device ordinal %d not supported by the allocation-free entry point", dev);
+        return PYSIFT_ERR_UNSUPPORTED;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    if (!ptrs[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_zoom2x_scratch);
+        if (e != cudaSuccess || p == nullptr) {
+            set_error("cudaGetSymbolAddress(g_zoom2x_scratch) on device %d failed: %s", dev,
+                      cudaGetErrorString(e));
+            return PYSIFT_ERR_CUDA;
+        }
+        ptrs[dev] = static_cast<double*>(p);
+    }
+    *out = ptrs[dev];
+    return PYSIFT_OK;
+}
+
+}  // namespace pysift
+
+extern "C" int pysift_zoom2x_u8_noalloc(const uint8_t* gray, int32_t H, int32_t W, int64_t pitch_bytes,
+                                        int32_t fp16_round, float* out, int32_t out_pitch,
+                                        pysift_stream_t stream) {
+    PYSIFT_CHECK_ARG(gray && out, "NULL pointer argument");
+    PYSIFT_CHECK_ARG(H > 0 && W > 0 && pitch_bytes >= W && out_pitch >= 2 * W, "bad sizes");
+    if ((int64_t)H * W > (int64_t)PYSIFT_ZOOM2X_NOALLOC_MAX_PIXELS) {
+        set_error("pysift_zoom2x_u8_noalloc: %dx%d = %lld pixels exceeds the fixed scratch of %d pixels; "
+                  "use pysift_zoom2x_u8 with caller-provided scratch",
+                  H, W, (long long)H * W, (int)PYSIFT_ZOOM2X_NOALLOC_MAX_PIXELS);
+        return PYSIFT_ERR_CAPACITY;
+    }
+    double* coef = nullptr;
+    int rc = zoom2x_scratch_ptr(&coef);
+    if (rc) return rc;
+    // Every scratch element the kernels read is written earlier in this same
+    // call (k_prefilter_cols fills all H*W coefficients), so nothing needs
+    // clearing between calls.
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    k_prefilter_cols<<<ceil_div(W, 128), 128, 0, st>>>(gray, H, W, pitch_bytes, fp16_round, coef);
+    PYSIFT_LAUNCH_CHECK("k_prefilter_cols");
+    k_prefilter_rows<<<ceil_div(H, 128), 128, 0, st>>>(coef, H, W);
+    PYSIFT_LAUNCH_CHECK("k_prefilter_rows");
+    k_zoom_interp<<<dim3(ceil_div(2 * W, 256), 2 * H), 256, 0, st>>>(coef, H, W, fp16_round, out, out_pitch);
+    PYSIFT_LAUNCH_CHECK("k_zoom_interp");
+    return PYSIFT_OK;
+}
