@@ -227,7 +227,7 @@ def run_detect(args, wl, world, rank, local):
     b = sift._bufs[(H, W)]
     n_kp = int(b.stats.cpu()[0])
 
-    step_ms, pyr_ms = [], []
+    step_ms, pyr_ms, stage = [], [], []
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize(dev)
@@ -238,6 +238,7 @@ def run_detect(args, wl, world, rank, local):
             ev[6].synchronize()
             step_ms.append(ev[0].elapsed_time(ev[6]))
             pyr_ms.append(ev[0].elapsed_time(ev[3]))
+            stage.append([ev[i].elapsed_time(ev[i + 1]) for i in range(6)])
     torch.cuda.synchronize(dev)
     if world > 1:
         dist.barrier()
@@ -303,7 +304,9 @@ def run_detect(args, wl, world, rank, local):
         "e2e": {"value": e2e_value, "unit": "Mpix/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": detect_launches(sift, H, W) * args.steps,
         "clocks": clk.summary(),
-        "stage_ms": {"total": float(np.mean(step_ms))},
+        "stage_ms": dict(zip(["base_image", "pyramid", "extrema_mask", "refine_cap", "orientation", "descriptor"],
+                             [round(float(x), 4) for x in np.mean(np.array(stage), 0)]),
+                         total=round(float(np.mean(step_ms)), 4)),
     }
     if ocv:
         line["opencv_cpu"] = {"value": mpix / ocv[0], "unit": "Mpix/s", "cores": os.cpu_count(),

@@ -11,9 +11,10 @@
  *   exp   : Cody-Waite reduction x = n*ln2 + r (ln2 split in two parts),
  *           Taylor series of exp(r) to degree 8 in Horner form (fmaf),
  *           exact scaling by 2^n.
- *   atan2 : octant reduction to t in [0,1], t > tan(pi/8) mapped through
- *           atan(t) = pi/4 + atan((t-1)/(t+1)), Taylor series of atan(u) to
- *           u^23, quadrant fix-up.
+ *   atan2 : t = min(|x|,|y|)/max(|x|,|y|) in [0,1], atan(t) = t*P(t^2)
+ *           with P a degree-9 polynomial (coefficients from a Chebyshev
+ *           interpolation of atan(sqrt(s))/sqrt(s) on [0,1], rounded to
+ *           float32; max error ~1.5 ulp), then octant/quadrant fix-up.
  *   sincos: Cody-Waite reduction by pi/2 (three float parts), Taylor series
  *           of sin (to r^9) and cos (to r^10), quadrant rotation.
  *   log2d : (double) m*2^e split with m in [sqrt(1/2), sqrt(2)),
@@ -68,22 +69,6 @@ static inline float orc_expf(float x) {
 #define ORC_PIO2_F 1.57079632679489661923f
 #define ORC_PIO4_F 0.78539816339744830962f
 
-static inline float orc_atan_poly(float u) {
-    float u2 = u * u;
-    float p = -4.34782608695652173913e-02f;      /* -1/23 */
-    p = fmaf(p, u2, 4.76190476190476190476e-02f);  /*  1/21 */
-    p = fmaf(p, u2, -5.26315789473684210526e-02f); /* -1/19 */
-    p = fmaf(p, u2, 5.88235294117647058824e-02f);  /*  1/17 */
-    p = fmaf(p, u2, -6.66666666666666666667e-02f); /* -1/15 */
-    p = fmaf(p, u2, 7.69230769230769230769e-02f);  /*  1/13 */
-    p = fmaf(p, u2, -9.09090909090909090909e-02f); /* -1/11 */
-    p = fmaf(p, u2, 1.11111111111111111111e-01f);  /*  1/9  */
-    p = fmaf(p, u2, -1.42857142857142857143e-01f); /* -1/7  */
-    p = fmaf(p, u2, 2.00000000000000000000e-01f);  /*  1/5  */
-    p = fmaf(p, u2, -3.33333333333333333333e-01f); /* -1/3  */
-    return fmaf(u * u2, p, u);
-}
-
 static inline float orc_atan2f(float y, float x) {
     float ax = fabsf(x), ay = fabsf(y);
     if (ax == 0.0f && ay == 0.0f) {
@@ -91,16 +76,21 @@ static inline float orc_atan2f(float y, float x) {
         return signbit(y) ? -a : a;
     }
     int swap = ay > ax;
-    float num = swap ? ax : ay;
-    float den = swap ? ay : ax;
-    float t = num / den;
-    float a;
-    if (t > 0.41421356237309504880f) {
-        float u = (t - 1.0f) / (t + 1.0f);
-        a = ORC_PIO4_F + orc_atan_poly(u);
-    } else {
-        a = orc_atan_poly(t);
-    }
+    float mn = swap ? ax : ay;
+    float mx = swap ? ay : ax;
+    float t = mn / mx;
+    float s = t * t;
+    float p = -0x1.c919cep-10f;
+    p = fmaf(p, s, 0x1.5dfc5ep-7f);
+    p = fmaf(p, s, -0x1.f74692p-6f);
+    p = fmaf(p, s, 0x1.d6bdd0p-5f);
+    p = fmaf(p, s, -0x1.56eb74p-4f);
+    p = fmaf(p, s, 0x1.c01c4cp-4f);
+    p = fmaf(p, s, -0x1.2413b8p-3f);
+    p = fmaf(p, s, 0x1.999052p-3f);
+    p = fmaf(p, s, -0x1.555534p-2f);
+    p = fmaf(p, s, 0x1.000000p+0f);
+    float a = t * p;
     if (swap) a = ORC_PIO2_F - a;
     if (signbit(x)) a = ORC_PI_F - a;
     if (signbit(y)) a = -a;

@@ -14,8 +14,9 @@
  *   - IEEE division / sqrt where the reference uses fast-math or rsqrtf;
  *   - elementary functions from orc_math.h;
  *   - candidate order (octave, s, r, c) instead of atomic-slot order;
- *   - descriptor histogram accumulated per lane (32 lanes, pixel stride 32)
- *     and merged lane 0..31 in order, instead of shared-memory atomics.
+ *   - orientation and descriptor histograms summed exactly in 64-bit fixed
+ *     point (2^-40 units), independent of summation order, instead of the
+ *     reference's per-lane float sums / shared-memory float atomics.
  */
 #include <math.h>
 #include <stdint.h>
@@ -60,31 +61,44 @@ EXPORT void orc_u8_to_f32(const uint8_t* img, long n, float* out) {
 /* boundary (pole sqrt(3)-2, gain 6), interpolation in float64, output  */
 /* rounded to float32.                                                   */
 /* ------------------------------------------------------------------ */
-static void spline_prefilter_1d(double* c, long n, long stride) {
-    if (n < 2) return;
+/* B-spline direct transform as a symmetric FIR: the impulse response of the
+ * cubic-spline prefilter on the mirror-extended line is
+ * h[k] = (-6 z / (1 - z^2)) z^|k|, z = sqrt(3) - 2 (h[0] = sqrt(3)); it is
+ * truncated at |k| <= 30 (|z|^31 < 2e-18).  Taps are applied k = -30..30 in
+ * order with one fma each, over whole-sample-symmetric (mirror) extension. */
+#define ORC_SPL_K 30
+static void spline_taps(double h[2 * ORC_SPL_K + 1]) {
     const double z = sqrt(3.0) - 2.0;
-    const double gain = (1.0 - z) * (1.0 - 1.0 / z);
-    for (long i = 0; i < n; ++i) c[i * stride] *= gain;
-    /* causal init, mirror boundary */
-    double z_i = z;
-    double z_n_1 = 1.0;  /* z^(n-1) by repeated multiplication (no libm pow) */
-    for (long i = 0; i < n - 1; ++i) z_n_1 = z_n_1 * z;
-    c[0] = c[0] + z_n_1 * c[(n - 1) * stride];
-    for (long i = 1; i < n - 1; ++i) {
-        c[0] += z_i * (c[i * stride] + z_n_1 * c[(n - 1 - i) * stride]);
-        z_i *= z;
+    const double c0 = -6.0 * z / (1.0 - z * z);
+    for (int k = -ORC_SPL_K; k <= ORC_SPL_K; ++k) {
+        int a = k < 0 ? -k : k;
+        double zk = 1.0;
+        for (int i = 0; i < a; ++i) zk = zk * z;
+        h[k + ORC_SPL_K] = c0 * zk;
     }
-    c[0] /= 1.0 - z_n_1 * z_n_1;
-    for (long i = 1; i < n; ++i) c[i * stride] += z * c[(i - 1) * stride];
-    /* anticausal init, mirror boundary */
-    c[(n - 1) * stride] = (z * c[(n - 2) * stride] + c[(n - 1) * stride]) * z / (z * z - 1.0);
-    for (long i = n - 2; i >= 0; --i) c[i * stride] = z * (c[(i + 1) * stride] - c[i * stride]);
+}
+
+static long mirror_index(long idx, long len);
+
+static void spline_prefilter_1d(const double* in, double* out, long n, long stride, const double* h) {
+    for (long i = 0; i < n; ++i) {
+        double acc = 0.0;
+        for (int k = -ORC_SPL_K; k <= ORC_SPL_K; ++k)
+            acc = fma(h[k + ORC_SPL_K], in[mirror_index(i + k, n) * stride], acc);
+        out[i * stride] = acc;
+    }
 }
 
 EXPORT void orc_spline_prefilter_2d(double* c, int H, int W) {
-    /* scipy filters axis 0 (columns) first, then axis 1 (rows) */
-    for (int x = 0; x < W; ++x) spline_prefilter_1d(c + x, H, W);
-    for (int r = 0; r < H; ++r) spline_prefilter_1d(c + (long)r * W, W, 1);
+    /* axis 0 (along columns) first, then axis 1 (along rows), as scipy */
+    double h[2 * ORC_SPL_K + 1];
+    spline_taps(h);
+    double* tmp = (double*)malloc(sizeof(double) * (size_t)H * W);
+    #pragma omp parallel for schedule(static)
+    for (int x = 0; x < W; ++x) spline_prefilter_1d(c + x, tmp + x, H, W, h);
+    #pragma omp parallel for schedule(static)
+    for (int r = 0; r < H; ++r) spline_prefilter_1d(tmp + (long)r * W, c + (long)r * W, W, 1, h);
+    free(tmp);
 }
 
 static void cubic_weights(double t, double w[4]) {
@@ -315,12 +329,22 @@ EXPORT void orc_refine(const float* dog, int S2, int H, int W, const int* cands,
 
 /* ------------------------------------------------------------------ */
 /* A10: orientation histogram (pysift/core.py:228-333).  gauss is       */
-/* (L,H,W); kpts (N,4) = [ri, ci, sigma, si].  36 bins, 32 per-lane     */
-/* partial histograms (pixel stride 32), warp shuffle-down tree         */
-/* 16,8,4,2,1 per bin, 2x [.25,.5,.25] circular smoothing, peaks >=     */
-/* 0.8*max, parabolic refinement, up to 4 angles (-1 = none).           */
-/* Canonical: orc_expf for __expf, orc_atan2f for atan2f.                */
+/* (L,H,W); kpts (N,4) = [ri, ci, sigma, si].  36 bins with linear bin  */
+/* split, 2x [.25,.5,.25] circular smoothing, peaks >= 0.8*max and >=    */
+/* both neighbours, parabolic refinement, up to 4 angles (-1 = none).   */
+/* Canonical: orc_expf for __expf, orc_atan2f for atan2f; the histogram */
+/* is an exact fixed-point sum (orc_fix) instead of per-lane float sums */
+/* merged by a warp tree, so its value does not depend on the order in  */
+/* which pixels are visited.                                            */
 /* ------------------------------------------------------------------ */
+/* Exact, order-independent histogram accumulation: every non-negative
+ * float32 contribution is rounded to a multiple of 2^-40 (round to nearest
+ * even) and summed as a 64-bit integer; the bin value is the sum rounded to
+ * float32 and scaled back.  Contributions are <= sqrt(2), so the sums stay
+ * far below 2^63 for any patch these kernels visit. */
+static inline long long orc_fix(float c) { return llrintf(c * 0x1p40f); }
+static inline float orc_unfix(long long s) { return (float)s * 0x1p-40f; }
+
 static float tree32(const float* v, int stride) {
     float a[32];
     for (int i = 0; i < 32; ++i) a[i] = v[i * stride];
@@ -333,8 +357,8 @@ EXPORT void orc_orientation(const float* gauss, int H, int W, const float* kpts,
     long HW = (long)H * W;
     #pragma omp parallel for schedule(dynamic, 16)
     for (long k = 0; k < N; ++k) {
-        float lh[32][36];
-        memset(lh, 0, sizeof(lh));
+        long long acc[36];
+        memset(acc, 0, sizeof(acc));
         float ri = kpts[k * 4 + 0], ci = kpts[k * 4 + 1], sigma = kpts[k * 4 + 2];
         int si = (int)kpts[k * 4 + 3];
         int radius = (int)(4.5f * sigma + 0.5f);
@@ -350,7 +374,6 @@ EXPORT void orc_orientation(const float* gauss, int H, int W, const float* kpts,
         int total = nr * n_cols;
         const float* g = gauss + si * HW;
         for (int pidx = 0; pidx < total; ++pidx) {
-            int lane = pidx & 31;
             int r = r_min + pidx / n_cols;
             int c = c_min + pidx % n_cols;
             float dx = g[(long)r * W + c + 1] - g[(long)r * W + c - 1];
@@ -364,11 +387,11 @@ EXPORT void orc_orientation(const float* gauss, int H, int W, const float* kpts,
             int bin_r = (bin_i + 1) % 36;
             float frac = bin_f - floorf(bin_f);
             float mw = mag * wt;
-            lh[lane][bin_i] = lh[lane][bin_i] + mw * (1.0f - frac);
-            lh[lane][bin_r] = lh[lane][bin_r] + mw * frac;
+            acc[bin_i] += orc_fix(mw * (1.0f - frac));
+            acc[bin_r] += orc_fix(mw * frac);
         }
         float hist[36], smooth[36];
-        for (int b = 0; b < 36; ++b) hist[b] = tree32(&lh[0][b], 36);
+        for (int b = 0; b < 36; ++b) hist[b] = orc_unfix(acc[b]);
         for (int it = 0; it < 2; ++it) {
             for (int b = 0; b < 36; ++b)
                 smooth[b] = 0.25f * hist[(b + 35) % 36] + 0.5f * hist[b] + 0.25f * hist[(b + 1) % 36];
@@ -399,12 +422,12 @@ EXPORT void orc_orientation(const float* gauss, int H, int W, const float* kpts,
 /* (N,5) = [ri, ci, ang_rad, ph, si]; dsp_scales NULL/n_dsp=0 for the   */
 /* single-scale descriptor.  Output: L2 -> clip 0.2 -> L2 vector (the   */
 /* kernel output before RootSIFT).                                      */
-/* Canonical: 32 per-lane partial histograms (pixel index stride 32),   */
-/* merged lane 0..31 in order; norms by the reference's warp tree then  */
-/* warp partials 0..3 in order; 1/sqrtf instead of rsqrtf; orc_* math.   */
+/* Canonical: exact fixed-point histogram (orc_fix) instead of shared-  */
+/* memory float atomics; norms by the reference's warp tree then warp   */
+/* partials 0..3 in order; 1/sqrtf instead of rsqrtf; orc_* math.        */
 /* ------------------------------------------------------------------ */
 static void desc_accumulate(const float* g, int H, int W, float ri, float ci, float cos_a, float sin_a,
-                            float ang_rad, int ph, float part[32][128]) {
+                            float ang_rad, int ph, long long acc[128]) {
     float scale_sp = 4.0f / (2.0f * (float)ph);
     float sigma_d = (float)ph * 0.5657f;
     float inv_2s2 = 1.0f / (2.0f * sigma_d * sigma_d + 1e-12f);
@@ -412,7 +435,6 @@ static void desc_accumulate(const float* g, int H, int W, float ri, float ci, fl
     int total = side * side;
     int r0 = (int)ri, c0 = (int)ci;
     for (int flat = 0; flat < total; ++flat) {
-        int lane = flat & 31;
         int r_off = flat / side - ph;
         int c_off = flat % side - ph;
         int rr = r0 + r_off, cc = c0 + c_off;
@@ -443,15 +465,14 @@ static void desc_accumulate(const float* g, int H, int W, float ri, float ci, fl
         float w_y0 = 1.0f - dy_b, w_y1 = dy_b;
         float w_x0 = 1.0f - dx_b, w_x1 = dx_b;
         float w_o0 = 1.0f - df, w_o1 = df;
-        float* p = part[lane];
-        p[yi0c * 32 + xi0c * 8 + oi0w] += w_y0 * w_x0 * w_o0 * wmag;
-        p[yi0c * 32 + xi0c * 8 + oi1w] += w_y0 * w_x0 * w_o1 * wmag;
-        p[yi0c * 32 + xi1c * 8 + oi0w] += w_y0 * w_x1 * w_o0 * wmag;
-        p[yi0c * 32 + xi1c * 8 + oi1w] += w_y0 * w_x1 * w_o1 * wmag;
-        p[yi1c * 32 + xi0c * 8 + oi0w] += w_y1 * w_x0 * w_o0 * wmag;
-        p[yi1c * 32 + xi0c * 8 + oi1w] += w_y1 * w_x0 * w_o1 * wmag;
-        p[yi1c * 32 + xi1c * 8 + oi0w] += w_y1 * w_x1 * w_o0 * wmag;
-        p[yi1c * 32 + xi1c * 8 + oi1w] += w_y1 * w_x1 * w_o1 * wmag;
+        acc[yi0c * 32 + xi0c * 8 + oi0w] += orc_fix(w_y0 * w_x0 * w_o0 * wmag);
+        acc[yi0c * 32 + xi0c * 8 + oi1w] += orc_fix(w_y0 * w_x0 * w_o1 * wmag);
+        acc[yi0c * 32 + xi1c * 8 + oi0w] += orc_fix(w_y0 * w_x1 * w_o0 * wmag);
+        acc[yi0c * 32 + xi1c * 8 + oi1w] += orc_fix(w_y0 * w_x1 * w_o1 * wmag);
+        acc[yi1c * 32 + xi0c * 8 + oi0w] += orc_fix(w_y1 * w_x0 * w_o0 * wmag);
+        acc[yi1c * 32 + xi0c * 8 + oi1w] += orc_fix(w_y1 * w_x0 * w_o1 * wmag);
+        acc[yi1c * 32 + xi1c * 8 + oi0w] += orc_fix(w_y1 * w_x1 * w_o0 * wmag);
+        acc[yi1c * 32 + xi1c * 8 + oi1w] += orc_fix(w_y1 * w_x1 * w_o1 * wmag);
     }
 }
 
@@ -467,8 +488,8 @@ EXPORT void orc_descriptor(const float* gauss, int n_slices, int H, int W, const
     long HW = (long)H * W;
     #pragma omp parallel for schedule(dynamic, 8)
     for (long k = 0; k < N; ++k) {
-        float part[32][128];
-        memset(part, 0, sizeof(part));
+        long long acc[128];
+        memset(acc, 0, sizeof(acc));
         float ri = kpts[k * 5 + 0], ci = kpts[k * 5 + 1], ang = kpts[k * 5 + 2];
         float phf = kpts[k * 5 + 3];
         int si = (int)kpts[k * 5 + 4];
@@ -486,17 +507,13 @@ EXPORT void orc_descriptor(const float* gauss, int n_slices, int H, int W, const
             for (int d = 0; d < n_dsp; ++d) {
                 int ph = (int)(phf * dsp_scales[d] + 0.5f);
                 if (ph < 4) ph = 4;
-                desc_accumulate(g, H, W, ri, ci, cos_a, sin_a, ang, ph, part);
+                desc_accumulate(g, H, W, ri, ci, cos_a, sin_a, ang, ph, acc);
             }
         } else {
-            desc_accumulate(g, H, W, ri, ci, cos_a, sin_a, ang, (int)phf, part);
+            desc_accumulate(g, H, W, ri, ci, cos_a, sin_a, ang, (int)phf, acc);
         }
         float v[128];
-        for (int b = 0; b < 128; ++b) {
-            float acc = part[0][b];
-            for (int l = 1; l < 32; ++l) acc = acc + part[l][b];
-            v[b] = acc;
-        }
+        for (int b = 0; b < 128; ++b) v[b] = orc_unfix(acc[b]);
         if (n_dsp > 0) {
             float inv_n = 1.0f / (float)n_dsp;
             for (int b = 0; b < 128; ++b) v[b] = v[b] * inv_n;

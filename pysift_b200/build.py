@@ -40,7 +40,7 @@ def build(verbose=False, force=False):
             return LIB_PATH
     tmp = LIB_PATH + ".tmp"
     cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "--fmad=false", "-std=c++17",
-           "-Xcompiler", "-fPIC", "-shared", "-o", tmp, *srcs]
+           "-Xcompiler", "-fPIC,-ffp-contract=off", "-shared", "-o", tmp, *srcs]
     if verbose:
         print(" ".join(cmd))
     subprocess.check_call(cmd)

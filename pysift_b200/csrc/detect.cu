@@ -3,7 +3,7 @@
 // Pipeline (all launches on the caller's stream, no host synchronisation,
 // capturable into a CUDA graph):
 //   k_histogram          256-bin histogram + entropy threshold (pysift/core.py:1129-1148)
-//   k_prefilter_cols/rows, k_zoom_interp
+//   k_prefilter_cols, k_zoom_rows_interp
 //                        2x cubic B-spline upsample (pysift/core.py:1270-1275)
 //   k_u8_to_f32          base image when not upsampled (pysift/core.py:1248-1261)
 //   k_blur<R>            fused H+V separable blur per level (pysift/core.py:475-608,
@@ -190,38 +190,40 @@ static Layout make_layout(const pysift_detect_config* c, int H, int W) {
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_histogram(const uint8_t* __restrict__ img, int H, int W, long long pitch,
                                                    Ctrl* ctrl, double base, int S) {
-    __shared__ unsigned int sh[256];
+    __shared__ unsigned int sh[8][256];
     __shared__ double terms[256];
     __shared__ int is_last;
-    const int tid = threadIdx.x;
-    sh[tid] = 0;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    for (int i = tid; i < 8 * 256; i += 256) (&sh[0][0])[i] = 0u;
     __syncthreads();
-    const long long n = (long long)H * W;
-    for (long long i = (long long)blockIdx.x * blockDim.x + tid; i < n; i += (long long)gridDim.x * blockDim.x) {
-        long long r = i / W, c = i - r * W;
-        atomicAdd(&sh[img[r * pitch + c]], 1u);
+    for (int r = blockIdx.y; r < H; r += gridDim.y) {
+        const uint8_t* row = img + (long long)r * pitch;
+        for (int c = blockIdx.x * 256 + tid; c < W; c += gridDim.x * 256) atomicAdd(&sh[warp][row[c]], 1u);
     }
     __syncthreads();
-    if (sh[tid]) atomicAdd(&ctrl->hist[tid], sh[tid]);
+    unsigned int mine = 0;
+    for (int w = 0; w < 8; ++w) mine += sh[w][tid];
+    if (mine) atomicAdd(&ctrl->hist[tid], mine);
     __threadfence();
     __syncthreads();
-    if (tid == 0) is_last = (atomicAdd(&ctrl->blocks_done, 1u) == gridDim.x - 1);
+    if (tid == 0) is_last = (atomicAdd(&ctrl->blocks_done, 1u) == gridDim.x * gridDim.y - 1);
     __syncthreads();
     if (!is_last) return;
     __threadfence();
+    const double n = (double)H * (double)W;
     unsigned int h = atomicAdd(&ctrl->hist[tid], 0u);
     double t = 0.0;
     if (h) {
-        double p = (double)h / (double)n;
+        double p = (double)h / n;
         t = p * sm::log2d_(p);
     }
     terms[tid] = t;
-    sh[tid] = h;
+    sh[0][tid] = h;
     __syncthreads();
     if (tid == 0) {
         double ent = 0.0;
         for (int b = 0; b < 256; ++b)
-            if (sh[b]) ent = ent + terms[b];
+            if (sh[0][b]) ent = ent + terms[b];
         ent = -ent;
         double scale = 0.8 + ent / 40.0;
         if (scale > 1.0) scale = 1.0;
@@ -247,49 +249,36 @@ __global__ void k_u8_to_f32(const uint8_t* __restrict__ img, int H, int W, long 
     if (c < W) out[(long long)r * out_pitch + c] = u8_to_unit(img[(long long)r * pitch + c], fp16);
 }
 
-// In-place B-spline prefilter of one line (scipy.ndimage spline_filter1d,
-// order 3, mirror boundary).  z^(n-1) by repeated multiplication.
-__device__ void prefilter_line(double* c, long long n, long long stride) {
-    if (n < 2) return;
-    const double z = sqrt(3.0) - 2.0;
-    const double gain = (1.0 - z) * (1.0 - 1.0 / z);
-    for (long long i = 0; i < n; ++i) c[i * stride] *= gain;
-    double z_i = z;
-    double z_n_1 = 1.0;
-    for (long long i = 0; i < n - 1; ++i) z_n_1 = z_n_1 * z;
-    double c0 = c[0] + z_n_1 * c[(n - 1) * stride];
-    for (long long i = 1; i < n - 1; ++i) {
-        c0 += z_i * (c[i * stride] + z_n_1 * c[(n - 1 - i) * stride]);
-        z_i *= z;
-    }
-    c0 /= 1.0 - z_n_1 * z_n_1;
-    c[0] = c0;
-    double prev = c0;
-    for (long long i = 1; i < n; ++i) {
-        prev = c[i * stride] + z * prev;
-        c[i * stride] = prev;
-    }
-    double last = (z * c[(n - 2) * stride] + c[(n - 1) * stride]) * z / (z * z - 1.0);
-    c[(n - 1) * stride] = last;
-    double nxt = last;
-    for (long long i = n - 2; i >= 0; --i) {
-        nxt = z * (nxt - c[i * stride]);
-        c[i * stride] = nxt;
-    }
-}
+// B-spline direct transform (scipy.ndimage.spline_filter, order 3, mirror
+// boundary) as a symmetric FIR: on the mirror-extended line the recursive
+// prefilter's impulse response is h[k] = (-6 z / (1 - z^2)) z^|k| with
+// z = sqrt(3) - 2, truncated at |k| <= SPL_K (|z|^31 < 2e-18).  Taps run
+// k = -SPL_K..SPL_K with one fma each.  Columns (axis 0) are filtered first,
+// then rows, as scipy does.
+constexpr int SPL_K = 30;
+constexpr int SPL_TAPS = 2 * SPL_K + 1;
 
-__global__ void k_prefilter_cols(const uint8_t* __restrict__ img, int H, int W, long long pitch, int fp16,
-                                 double* __restrict__ coef) {
-    int x = blockIdx.x * blockDim.x + threadIdx.x;
-    if (x >= W) return;
-    for (int r = 0; r < H; ++r) coef[(long long)r * W + x] = (double)u8_to_unit(img[(long long)r * pitch + x], fp16);
-    prefilter_line(coef + x, H, W);
-}
+// Taps computed once on the host with the same operation sequence as the
+// oracle (IEEE double, no contraction) and passed by value, so that fully
+// unrolled loops read them as constant-bank operands.
+struct SplTaps {
+    double h[SPL_TAPS];
+};
 
-__global__ void k_prefilter_rows(double* __restrict__ coef, int H, int W) {
-    int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= H) return;
-    prefilter_line(coef + (long long)r * W, W, 1);
+static const SplTaps& spline_taps() {
+    static const SplTaps taps = [] {
+        SplTaps t;
+        const double z = sqrt(3.0) - 2.0;
+        const double c0 = -6.0 * z / (1.0 - z * z);
+        for (int k = -SPL_K; k <= SPL_K; ++k) {
+            const int a = k < 0 ? -k : k;
+            double zk = 1.0;
+            for (int i = 0; i < a; ++i) zk = zk * z;
+            t.h[k + SPL_K] = c0 * zk;
+        }
+        return t;
+    }();
+    return taps;
 }
 
 __device__ __forceinline__ long long mirror_index(long long idx, long long len) {
@@ -305,6 +294,51 @@ __device__ __forceinline__ long long mirror_index(long long idx, long long len) 
     return idx;
 }
 
+constexpr int PC_TW = 32, PC_RB = 8, PC_TH = 8 * PC_RB;
+
+// Column FIR straight from the uint8 image: coef[r][x] = sum_k h[k] u[mirror(r+k)][x].
+// Each thread produces PC_RB consecutive rows of one column, streaming the
+// input window through registers (taps in ascending k for every output).
+__global__ void __launch_bounds__(256) k_prefilter_cols(const uint8_t* __restrict__ img, int H, int W,
+                                                        long long pitch, int fp16, double* __restrict__ coef,
+                                                        const SplTaps taps) {
+    __shared__ double tile[(PC_TH + 2 * SPL_K) * PC_TW];
+    const int x0 = blockIdx.x * PC_TW, r0 = blockIdx.y * PC_TH;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int x = x0 + tx;
+    for (int rr = ty; rr < PC_TH + 2 * SPL_K; rr += 8) {
+        double v = 0.0;
+        if (x < W) {
+            long long gr = mirror_index(r0 - SPL_K + rr, H);
+            v = (double)u8_to_unit(img[gr * pitch + x], fp16);
+        }
+        tile[rr * PC_TW + tx] = v;
+    }
+    __syncthreads();
+    if (x >= W) return;
+    const int y0 = ty * PC_RB;
+    double acc[PC_RB];
+#pragma unroll
+    for (int j = 0; j < PC_RB; ++j) acc[j] = 0.0;
+#pragma unroll
+    for (int m = 0; m < PC_RB + 2 * SPL_K; ++m) {
+        const double t = tile[(y0 + m) * PC_TW + tx];
+#pragma unroll
+        for (int j = 0; j < PC_RB; ++j) {
+            const int k = m - j;
+            if (k >= 0 && k < SPL_TAPS) acc[j] = fma(taps.h[k], t, acc[j]);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < PC_RB; ++j) {
+        const int r = r0 + y0 + j;
+        if (r < H) coef[(long long)r * W + x] = acc[j];
+    }
+}
+
+// Output-coordinate setup for one axis of scipy's zoom (grid_mode=False,
+// mode='constant'): input coordinate k*(in-1)/(out-1), cubic B-spline
+// weights, mirror-mapped support; false outside [0, in-1] (cval 0).
 __device__ __forceinline__ bool zoom_axis(long long k, long long in_len, long long out_len, long long idx[4],
                                           double w[4]) {
     double zoom = (out_len > 1) ? (double)(in_len - 1) / (double)(out_len - 1) : 1.0;
@@ -323,32 +357,151 @@ __device__ __forceinline__ bool zoom_axis(long long k, long long in_len, long lo
     return true;
 }
 
-__global__ void k_zoom_interp(const double* __restrict__ coef, int H, int W, int fp16, float* __restrict__ out,
-                              int out_pitch) {
-    const int OW = 2 * W, OH = 2 * H;
-    int x = blockIdx.x * blockDim.x + threadIdx.x;
-    int r = blockIdx.y;
-    if (x >= OW || r >= OH) return;
-    long long iy[4], ix[4];
-    double wy[4], wx[4];
-    bool vy = zoom_axis(r, H, OH, iy, wy);
-    bool vx = zoom_axis(x, W, OW, ix, wx);
-    float res = 0.0f;
-    if (vy && vx) {
-        double t = 0.0;
-        for (int i = 0; i < 4; ++i) {
-            const double* row = coef + iy[i] * (long long)W;
-            for (int j = 0; j < 4; ++j) {
-                double coeff = row[ix[j]];
-                coeff *= wy[i];
-                coeff *= wx[j];
-                t += coeff;
+constexpr int ZI_TW = 64, ZI_TH = 32;   // output tile
+constexpr int ZI_CR = 24, ZI_CC = 40;   // input rows / cols a tile can touch (span <= 20 x 36)
+constexpr int ZI_XB = 4;                // row-FIR outputs per thread
+
+// Row FIR of the column-filtered coefficients for the input window a tile
+// needs, then the 4x4 cubic interpolation t = sum_i sum_j (c*wy_i)*wx_j in
+// scipy's order, rounded to float32.
+__global__ void __launch_bounds__(256) k_zoom_rows_interp(const double* __restrict__ coef, int H, int W, int fp16,
+                                                          float* __restrict__ out, int out_pitch, const SplTaps taps) {
+    __shared__ int rvalid[ZI_TH], ridx[ZI_TH][4];
+    __shared__ double rw[ZI_TH][4];
+    __shared__ int cvalid[ZI_TW], cidx[ZI_TW][4];
+    __shared__ double cw[ZI_TW][4];
+    __shared__ int s_lo[2], s_hi[2];
+    __shared__ double c1[ZI_CR][ZI_CC + 2 * SPL_K + ZI_XB];
+    __shared__ double c2[ZI_CR][ZI_CC];
+    const int OH = 2 * H, OW = 2 * W;
+    const int ox0 = blockIdx.x * ZI_TW, oy0 = blockIdx.y * ZI_TH;
+    const int tid = threadIdx.x;
+    if (tid < 2) {
+        s_lo[tid] = 0x7fffffff;
+        s_hi[tid] = -1;
+    }
+    __syncthreads();
+    if (tid < ZI_TH) {
+        const int r = oy0 + tid;
+        long long idx[4];
+        double w[4];
+        bool v = (r < OH) && zoom_axis(r, H, OH, idx, w);
+        rvalid[tid] = v;
+        if (v) {
+            int lo = 0x7fffffff, hi = -1;
+            for (int q = 0; q < 4; ++q) {
+                ridx[tid][q] = (int)idx[q];
+                rw[tid][q] = w[q];
+                lo = min(lo, (int)idx[q]);
+                hi = max(hi, (int)idx[q]);
+            }
+            atomicMin(&s_lo[0], lo);
+            atomicMax(&s_hi[0], hi);
+        }
+    } else if (tid >= 32 && tid < 32 + ZI_TW) {
+        const int t = tid - 32;
+        const int x = ox0 + t;
+        long long idx[4];
+        double w[4];
+        bool v = (x < OW) && zoom_axis(x, W, OW, idx, w);
+        cvalid[t] = v;
+        if (v) {
+            int lo = 0x7fffffff, hi = -1;
+            for (int q = 0; q < 4; ++q) {
+                cidx[t][q] = (int)idx[q];
+                cw[t][q] = w[q];
+                lo = min(lo, (int)idx[q]);
+                hi = max(hi, (int)idx[q]);
+            }
+            atomicMin(&s_lo[1], lo);
+            atomicMax(&s_hi[1], hi);
+        }
+    }
+    __syncthreads();
+    const int ylo = s_lo[0], yhi = s_hi[0], xlo = s_lo[1], xhi = s_hi[1];
+    const bool any = (yhi >= 0 && xhi >= 0);
+    const int ny = any ? yhi - ylo + 1 : 0, nx = any ? xhi - xlo + 1 : 0;
+    const bool fits = ny <= ZI_CR && nx <= ZI_CC;
+    if (any && fits) {
+        const int nxw = nx + 2 * SPL_K;
+        for (int i = tid; i < ny * nxw; i += blockDim.x) {
+            const int yy = i / nxw, xx = i - yy * nxw;
+            const long long gx = mirror_index((long long)xlo - SPL_K + xx, W);
+            c1[yy][xx] = coef[(long long)(ylo + yy) * W + gx];
+        }
+        __syncthreads();
+        const int nxg = (nx + ZI_XB - 1) / ZI_XB;
+        for (int i = tid; i < ny * nxg; i += blockDim.x) {
+            const int yy = i / nxg, x0 = (i - yy * nxg) * ZI_XB;
+            double acc[ZI_XB];
+#pragma unroll
+            for (int j = 0; j < ZI_XB; ++j) acc[j] = 0.0;
+#pragma unroll
+            for (int m = 0; m < ZI_XB + 2 * SPL_K; ++m) {
+                const double t = c1[yy][x0 + m];
+#pragma unroll
+                for (int j = 0; j < ZI_XB; ++j) {
+                    const int k = m - j;
+                    if (k >= 0 && k < SPL_TAPS) acc[j] = fma(taps.h[k], t, acc[j]);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < ZI_XB; ++j)
+                if (x0 + j < nx) c2[yy][x0 + j] = acc[j];
+        }
+        __syncthreads();
+    }
+    // each thread: one output column, every 4th output row of the tile
+    const int tx = tid % ZI_TW;
+    const int x = ox0 + tx;
+    if (x >= OW) return;
+    const bool cv = cvalid[tx];
+    int cx[4];
+    double wx[4];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+        cx[b] = cv ? cidx[tx][b] - xlo : 0;
+        wx[b] = cv ? cw[tx][b] : 0.0;
+    }
+    for (int ty = tid / ZI_TW; ty < ZI_TH; ty += 256 / ZI_TW) {
+        const int r = oy0 + ty;
+        if (r >= OH) break;
+        float res = 0.0f;
+        if (rvalid[ty] && cv) {
+            if (fits) {
+                double t = 0.0;
+#pragma unroll
+                for (int a = 0; a < 4; ++a) {
+                    const double* row = c2[ridx[ty][a] - ylo];
+                    const double wy = rw[ty][a];
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) {
+                        double coeff = row[cx[b]];
+                        coeff *= wy;
+                        coeff *= wx[b];
+                        t += coeff;
+                    }
+                }
+                res = (float)t;
+                if (fp16) res = round_half(res);
+            } else {
+                res = __int_as_float(0x7fc00000);  // unreachable by construction; visible in parity tests
             }
         }
-        res = (float)t;
-        if (fp16) res = round_half(res);
+        out[(long long)r * out_pitch + x] = res;
     }
-    out[(long long)r * out_pitch + x] = res;
+}
+
+static int launch_zoom2x(const uint8_t* gray, int H, int W, long long pitch, int fp16, double* coef, float* out,
+                         int out_pitch, cudaStream_t st) {
+    const SplTaps& taps = spline_taps();
+    k_prefilter_cols<<<dim3(ceil_div(W, PC_TW), ceil_div(H, PC_TH)), 256, 0, st>>>(gray, H, W, pitch, fp16, coef,
+                                                                                  taps);
+    PYSIFT_LAUNCH_CHECK("k_prefilter_cols");
+    k_zoom_rows_interp<<<dim3(ceil_div(2 * W, ZI_TW), ceil_div(2 * H, ZI_TH)), 256, 0, st>>>(coef, H, W, fp16, out,
+                                                                                            out_pitch, taps);
+    PYSIFT_LAUNCH_CHECK("k_zoom_rows_interp");
+    return PYSIFT_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -367,25 +520,44 @@ struct BlurArgs {
     float w[PYSIFT_MAX_TAPS];
 };
 
+// Half-sample-symmetric reflection into [0, n) (period 2n), as the
+// reference's reflect() (pysift/core.py:477-483), without integer division.
 __device__ __forceinline__ int reflect_idx(int i, int n) {
-    int p = 2 * n;
-    i = i % p;
-    if (i < 0) i += p;
-    if (i >= n) i = 2 * n - 1 - i;
+    while (i < 0 || i >= n) {
+        if (i < 0) i = -i - 1;
+        if (i >= n) i = 2 * n - 1 - i;
+    }
     return i;
 }
 
 constexpr int BLUR_TW = 64, BLUR_TH = 32, BLUR_NT = 256;
 
-__device__ __forceinline__ void blur_load_tile(const BlurArgs& a, float* tile, int R, int TWP, int ROWS, int r0,
-                                               int c0) {
+// Loads input rows [r0-R, r0+TH+R) and columns [c0-RA, c0+TW+RA) (RA >= R,
+// a multiple of 4) into tile[ROWS][TWP] with reflection.  Tiles whose
+// window lies inside the image, read with stride 1 from a 16-byte aligned
+// base and pitch, use float4 loads.
+__device__ __forceinline__ void blur_load_tile(const BlurArgs& a, float* tile, int R, int RA, int TWP, int ROWS,
+                                               int r0, int c0) {
+    const bool interior = a.step == 1 && r0 - R >= 0 && r0 + BLUR_TH + R <= a.H && c0 - RA >= 0 &&
+                          c0 + BLUR_TW + RA <= a.W && ((a.in_pitch & 3) == 0) &&
+                          ((reinterpret_cast<uintptr_t>(a.in) & 15) == 0);
+    if (interior) {
+        const int q4 = TWP / 4;
+        for (int i = threadIdx.x; i < ROWS * q4; i += BLUR_NT) {
+            const int rr = i / q4, q = i - rr * q4;
+            const float4 v = *reinterpret_cast<const float4*>(a.in + (long long)(r0 - R + rr) * a.in_pitch + c0 - RA +
+                                                              4 * q);
+            *reinterpret_cast<float4*>(tile + rr * TWP + 4 * q) = v;
+        }
+        return;
+    }
     for (int i = threadIdx.x; i < ROWS * TWP; i += BLUR_NT) {
         int rr = i / TWP, cc = i - rr * TWP;
-        int gr = reflect_idx(r0 - R + rr, a.H), gc = reflect_idx(c0 - R + cc, a.W);
+        int gr = reflect_idx(r0 - R + rr, a.H), gc = reflect_idx(c0 - RA + cc, a.W);
         float v = a.in[(long long)gr * a.step * a.in_pitch + (long long)gc * a.step];
         tile[i] = v;
-        if (a.copy0 && rr >= R && rr < R + BLUR_TH && cc >= R && cc < R + BLUR_TW) {
-            int orow = r0 + rr - R, ocol = c0 + cc - R;
+        if (a.copy0 && rr >= R && rr < R + BLUR_TH && cc >= RA && cc < RA + BLUR_TW) {
+            int orow = r0 + rr - R, ocol = c0 + cc - RA;
             if (orow < a.H && ocol < a.W) {
                 a.copy0[(long long)orow * a.out_pitch + ocol] = v;
                 if (a.copy0_r) a.copy0_r[(long long)orow * a.out_pitch + ocol] = round_half(v);
@@ -397,17 +569,18 @@ __device__ __forceinline__ void blur_load_tile(const BlurArgs& a, float* tile, i
 template <int R>
 __global__ void __launch_bounds__(BLUR_NT) k_blur(const BlurArgs a) {
     constexpr int TW = BLUR_TW, TH = BLUR_TH;
-    constexpr int TWP = TW + 2 * R, ROWS = TH + 2 * R;
+    constexpr int RA = (R + 3) / 4 * 4;
+    constexpr int TWP = TW + 2 * RA, ROWS = TH + 2 * R;
     extern __shared__ float smem[];
     float* tile = smem;
     float* hb = smem + ROWS * TWP;
     const int c0 = blockIdx.x * TW, r0 = blockIdx.y * TH;
-    blur_load_tile(a, tile, R, TWP, ROWS, r0, c0);
+    blur_load_tile(a, tile, R, RA, TWP, ROWS, r0, c0);
     __syncthreads();
     constexpr int SPR = TW / 8;
     for (int sidx = threadIdx.x; sidx < ROWS * SPR; sidx += BLUR_NT) {
         int rr = sidx / SPR, x0 = (sidx - rr * SPR) * 8;
-        const float* src = tile + rr * TWP + x0;
+        const float* src = tile + rr * TWP + x0 + (RA - R);
         float v[8 + 2 * R];
 #pragma unroll
         for (int j = 0; j < 8 + 2 * R; ++j) v[j] = src[j];
@@ -454,12 +627,13 @@ __global__ void __launch_bounds__(BLUR_NT) k_blur(const BlurArgs a) {
 
 // Any radius up to PYSIFT_MAX_RADIUS (no register blocking); radius 0 copies.
 __global__ void __launch_bounds__(BLUR_NT) k_blur_generic(const BlurArgs a, int R) {
-    const int TWP = BLUR_TW + 2 * R, ROWS = BLUR_TH + 2 * R;
+    const int RA = (R + 3) / 4 * 4;
+    const int TWP = BLUR_TW + 2 * RA, ROWS = BLUR_TH + 2 * R;
     extern __shared__ float smem[];
-    float* tile = smem;
-    float* hb = smem + ROWS * TWP;
+    float* tile = smem + (RA - R);
+    float* hb = smem + ROWS * TWP + 4;
     const int c0 = blockIdx.x * BLUR_TW, r0 = blockIdx.y * BLUR_TH;
-    blur_load_tile(a, tile, R, TWP, ROWS, r0, c0);
+    blur_load_tile(a, smem, R, RA, TWP, ROWS, r0, c0);
     __syncthreads();
     for (int i = threadIdx.x; i < ROWS * BLUR_TW; i += BLUR_NT) {
         int rr = i / BLUR_TW, x = i - rr * BLUR_TW;
@@ -485,7 +659,8 @@ __global__ void __launch_bounds__(BLUR_NT) k_blur_generic(const BlurArgs a, int 
 }
 
 static size_t blur_smem_bytes(int R) {
-    return (size_t)((BLUR_TH + 2 * R) * (BLUR_TW + 2 * R) + (BLUR_TH + 2 * R) * BLUR_TW) * sizeof(float);
+    const int RA = (R + 3) / 4 * 4;
+    return (size_t)((BLUR_TH + 2 * R) * (BLUR_TW + 2 * RA) + (BLUR_TH + 2 * R) * BLUR_TW + 4) * sizeof(float);
 }
 
 typedef void (*BlurKernel)(const BlurArgs);
@@ -930,95 +1105,170 @@ struct OriArgs {
     int* angcnt;
 };
 
-constexpr int ORI_WARPS = 8;
+// Exact, order-independent histogram accumulation: each non-negative float32
+// contribution is rounded to a multiple of 2^-40 (round to nearest even) and
+// added as a 64-bit integer; a bin's value is the integer sum rounded to
+// float32 and scaled back.  Contributions are <= sqrt(2), so sums stay far
+// below 2^63.  This makes the histograms independent of which thread adds
+// what when, so any number of threads can share a keypoint.
+__device__ __forceinline__ unsigned long long fix40(float c) {
+    return (unsigned long long)__float2ll_rn(c * 0x1p40f);
+}
+__device__ __forceinline__ float unfix40(unsigned long long s) { return __ll2float_rn((long long)s) * 0x1p-40f; }
 
-__global__ void __launch_bounds__(ORI_WARPS * 32) k_orientation(const OriArgs a, const Ctrl* ctrl) {
-    __shared__ float lh_all[ORI_WARPS][32 * 37];
-    __shared__ float hist_all[ORI_WARPS][36];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int i = blockIdx.x * ORI_WARPS + warp;
-    if (i >= ctrl->n_kept) return;
-    float* lh = lh_all[warp] + lane * 37;
-    for (int b = 0; b < 36; ++b) lh[b] = 0.0f;
-    const int o = a.kp_o[i], si = a.kp_si[i];
-    const float ri = a.kp_ri[i], ci = a.kp_ci[i];
-    const float sigma = a.ori_sigma[si];
-    const OctView& v = a.oct[o];
-    const int H = v.H, W = v.W;
-    int radius = (int)(4.5f * sigma + 0.5f);
-    if (radius < 1) radius = 1;
-    const float sigma_w = 1.5f * sigma;
-    const float inv_2sw2 = 1.0f / (2.0f * sigma_w * sigma_w + 1e-12f);
-    int r_min = (int)ri - radius;
-    if (r_min < 1) r_min = 1;
-    int r_max = (int)ri + radius;
-    if (r_max > H - 2) r_max = H - 2;
-    int c_min = (int)ci - radius;
-    if (c_min < 1) c_min = 1;
-    int c_max = (int)ci + radius;
-    if (c_max > W - 2) c_max = W - 2;
-    int n_cols = c_max - c_min + 1;
-    if (n_cols < 1) n_cols = 1;
-    int nr = r_max - r_min + 1;
-    if (nr < 0) nr = 0;
-    const int total = nr * n_cols;
-    const float* g = v.lev[si];
-    const long long P = v.pitch;
-    for (int pidx = lane; pidx < total; pidx += 32) {
-        int r = r_min + pidx / n_cols;
-        int c = c_min + pidx % n_cols;
-        float dx = g[r * P + c + 1] - g[r * P + c - 1];
-        float dy = g[(r + 1) * P + c] - g[(r - 1) * P + c];
-        float mag = sqrtf(dx * dx + dy * dy);
-        float ori = fmodf(sm::atan2f_(dy, dx) * 57.29577951f + 360.0f, 360.0f);
-        float fr = (float)r - ri, fc = (float)c - ci;
-        float wt = sm::expf_(-(fr * fr + fc * fc) * inv_2sw2);
-        float bin_f = ori * 0.1f;
-        int bin_i = ((int)bin_f) % 36;
-        int bin_r = (bin_i + 1) % 36;
-        float frac = bin_f - floorf(bin_f);
-        float mw = mag * wt;
-        lh[bin_i] = lh[bin_i] + mw * (1.0f - frac);
-        lh[bin_r] = lh[bin_r] + mw * frac;
+// Warp-private fixed-point histograms with native 32-bit shared atomics.
+// A value q < 2^42 is added as two limbs, q mod 2^21 into lo[bin] and
+// q >> 21 into hi[bin]; every FOLD_STEPS warp steps (at most 4 values per
+// lane and bin per step) the limbs are folded into a 64-bit total and
+// cleared, so neither limb can overflow.  Integer sums keep the totals exact
+// and independent of the order of the atomics.
+constexpr int FOLD_STEPS = 8;
+
+struct WarpHist {
+    unsigned int* lo;
+    unsigned int* hi;
+    unsigned long long* tot;
+    int nbins;
+    __device__ __forceinline__ void add(int bin, unsigned long long q) const {
+        atomicAdd(lo + bin, (unsigned int)(q & 0x1fffffull));
+        atomicAdd(hi + bin, (unsigned int)(q >> 21));
     }
-    __syncwarp();
-    float* hist = hist_all[warp];
-    for (int b = 0; b < 36; ++b) {
-        float val = lh[b];
-        val += __shfl_down_sync(FULL_MASK, val, 16);
-        val += __shfl_down_sync(FULL_MASK, val, 8);
-        val += __shfl_down_sync(FULL_MASK, val, 4);
-        val += __shfl_down_sync(FULL_MASK, val, 2);
-        val += __shfl_down_sync(FULL_MASK, val, 1);
-        if (lane == 0) hist[b] = val;
-    }
-    __syncwarp();
-    if (lane == 0) {
-        float h[36], smooth[36];
-        for (int b = 0; b < 36; ++b) h[b] = hist[b];
-        for (int it = 0; it < 2; ++it) {
-            for (int b = 0; b < 36; ++b)
-                smooth[b] = 0.25f * h[(b + 35) % 36] + 0.5f * h[b] + 0.25f * h[(b + 1) % 36];
-            for (int b = 0; b < 36; ++b) h[b] = smooth[b];
+    // all lanes of the warp call fold() together
+    __device__ __forceinline__ void fold() const {
+        __syncwarp();
+        for (int b = (int)(threadIdx.x & 31); b < nbins; b += 32) {
+            tot[b] += ((unsigned long long)hi[b] << 21) + (unsigned long long)lo[b];
+            lo[b] = 0u;
+            hi[b] = 0u;
         }
-        float peak = 0.0f;
-        for (int b = 0; b < 36; ++b)
-            if (h[b] > peak) peak = h[b];
-        const float thr = 0.8f * peak;
-        int out = 0;
-        for (int b = 0; b < 36; ++b) {
-            if (h[b] >= thr) {
-                float l = h[(b + 35) % 36], rv = h[(b + 1) % 36];
-                if (h[b] >= l && h[b] >= rv) {
-                    float denom = l - 2.0f * h[b] + rv;
-                    float fine = (float)b + (fabsf(denom) > 1e-12f ? 0.5f * (l - rv) / denom : 0.0f);
-                    float angle = fmodf(fine / 36.0f * 360.0f + 360.0f, 360.0f);
-                    if (out < 4) a.ang[i * 4 + (out++)] = angle;
+        __syncwarp();
+    }
+};
+
+// fmodf(x, 360.0f) for x in (-360, 720): the remainder is exact in both forms
+// (Sterbenz), so this matches fmodf bit for bit on the ranges the orientation
+// (x in [180, 540]) and descriptor (x in (-180, 540]) formulas produce.
+__device__ __forceinline__ float mod360(float x) { return x >= 360.0f ? x - 360.0f : x; }
+
+constexpr int ORI_T = 64;
+constexpr int ORI_W = ORI_T / 32;
+
+__global__ void __launch_bounds__(ORI_T) k_orientation(const OriArgs a, const Ctrl* ctrl) {
+    __shared__ unsigned int wlo[ORI_W][36], whi[ORI_W][36];
+    __shared__ unsigned long long whist[ORI_W][36];
+    __shared__ float h0[36], h1[36];
+    __shared__ float s_peak;
+    __shared__ unsigned s_mask[2];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int n = ctrl->n_kept;
+    for (int i = blockIdx.x; i < n; i += gridDim.x) {
+        for (int b = tid; b < ORI_W * 36; b += ORI_T) {
+            (&whist[0][0])[b] = 0ull;
+            (&wlo[0][0])[b] = 0u;
+            (&whi[0][0])[b] = 0u;
+        }
+        __syncthreads();
+        const int o = a.kp_o[i], si = a.kp_si[i];
+        const float ri = a.kp_ri[i], ci = a.kp_ci[i];
+        const float sigma = a.ori_sigma[si];
+        const OctView& v = a.oct[o];
+        const int H = v.H, W = v.W;
+        int radius = (int)(4.5f * sigma + 0.5f);
+        if (radius < 1) radius = 1;
+        const float sigma_w = 1.5f * sigma;
+        const float inv_2sw2 = 1.0f / (2.0f * sigma_w * sigma_w + 1e-12f);
+        int r_min = (int)ri - radius;
+        if (r_min < 1) r_min = 1;
+        int r_max = (int)ri + radius;
+        if (r_max > H - 2) r_max = H - 2;
+        int c_min = (int)ci - radius;
+        if (c_min < 1) c_min = 1;
+        int c_max = (int)ci + radius;
+        if (c_max > W - 2) c_max = W - 2;
+        int n_cols = c_max - c_min + 1;
+        if (n_cols < 1) n_cols = 1;
+        int nr = r_max - r_min + 1;
+        if (nr < 0) nr = 0;
+        const float* g = v.lev[si];
+        const long long P = v.pitch;
+        const WarpHist hw{wlo[warp], whi[warp], whist[warp], 36};
+        // 8x4 pixel blocks per warp step
+        const int tcols = (n_cols + 7) >> 3, trows = (nr + 3) >> 2;
+        const int ntiles = tcols * trows;
+        int steps = 0;
+        for (int t = warp; t < ntiles; t += ORI_W) {
+            const int ty = t / tcols, tx = t - ty * tcols;
+            const int pr = ty * 4 + (lane >> 3), pc = tx * 8 + (lane & 7);
+            const bool act = pr < nr && pc < n_cols;
+            if (act) {
+                const int r = r_min + pr, c = c_min + pc;
+                const float* gp = g + r * P + c;
+                float dx = gp[1] - gp[-1];
+                float dy = gp[P] - gp[-P];
+                float mag = sqrtf(dx * dx + dy * dy);
+                float ori = mod360(sm::atan2f_(dy, dx) * 57.29577951f + 360.0f);
+                float fr = (float)r - ri, fc = (float)c - ci;
+                float wt = sm::expf_(-(fr * fr + fc * fc) * inv_2sw2);
+                float bin_f = ori * 0.1f;
+                const int b0 = ((int)bin_f) % 36;
+                const int b1 = (b0 + 1) % 36;
+                float frac = bin_f - floorf(bin_f);
+                float mw = mag * wt;
+                hw.add(b0, fix40(mw * (1.0f - frac)));
+                hw.add(b1, fix40(mw * frac));
+            }
+            if (++steps == FOLD_STEPS) {
+                hw.fold();
+                steps = 0;
+            }
+        }
+        hw.fold();
+        __syncthreads();
+        // smoothing and peaks, one bin per thread, same arithmetic per bin
+        if (tid < 36) {
+            unsigned long long s = 0ull;
+            for (int w = 0; w < ORI_W; ++w) s += whist[w][tid];
+            h0[tid] = unfix40(s);
+        }
+        __syncthreads();
+        if (tid < 36) h1[tid] = 0.25f * h0[(tid + 35) % 36] + 0.5f * h0[tid] + 0.25f * h0[(tid + 1) % 36];
+        __syncthreads();
+        if (tid < 36) h0[tid] = 0.25f * h1[(tid + 35) % 36] + 0.5f * h1[tid] + 0.25f * h1[(tid + 1) % 36];
+        __syncthreads();
+        if (tid == 0) {
+            float peak = 0.0f;
+            for (int b = 0; b < 36; ++b)
+                if (h0[b] > peak) peak = h0[b];
+            s_peak = peak;
+        }
+        __syncthreads();
+        bool is_peak = false;
+        float angle = 0.0f;
+        if (tid < 36) {
+            const float thr = 0.8f * s_peak;
+            const float hb = h0[tid];
+            if (hb >= thr) {
+                const float l = h0[(tid + 35) % 36], rv = h0[(tid + 1) % 36];
+                if (hb >= l && hb >= rv) {
+                    is_peak = true;
+                    const float denom = l - 2.0f * hb + rv;
+                    const float fine = (float)tid + (fabsf(denom) > 1e-12f ? 0.5f * (l - rv) / denom : 0.0f);
+                    angle = fmodf(fine / 36.0f * 360.0f + 360.0f, 360.0f);
                 }
             }
         }
-        a.angcnt[i] = out;
-        for (int k = out; k < 4; ++k) a.ang[i * 4 + k] = -1.0f;
+        const unsigned m = __ballot_sync(FULL_MASK, is_peak);
+        if (lane == 0) s_mask[warp] = m;
+        __syncthreads();
+        const unsigned m0 = s_mask[0], m1 = s_mask[1] & 0xfu;
+        const int before = warp == 0 ? __popc(m0 & ((1u << lane) - 1u)) : __popc(m0) + __popc(m1 & ((1u << lane) - 1u));
+        if (is_peak && before < 4) a.ang[i * 4 + before] = angle;
+        if (tid == 0) {
+            const int cnt = min(4, __popc(m0) + __popc(m1));
+            a.angcnt[i] = cnt;
+            for (int k = cnt; k < 4; ++k) a.ang[i * 4 + k] = -1.0f;
+        }
+        __syncthreads();
     }
 }
 
@@ -1070,24 +1320,32 @@ __device__ __forceinline__ bool key_less(const uint4& p, const uint4& q) {
     return p.w < q.w;
 }
 
-constexpr int RANK_TILE = 1024;
+constexpr int RANK_T = 256;
 
-__global__ void __launch_bounds__(256) k_rank(const uint4* __restrict__ keys, int* __restrict__ rank,
-                                              const Ctrl* ctrl) {
-    __shared__ uint4 tile[RANK_TILE];
+// rank[i] = #{j : key[j] < key[i]} over all (i-tile, j-tile) pairs; partial
+// counts are added with integer atomics (exact, order-independent).  rank
+// must be zeroed before the launch.
+__global__ void __launch_bounds__(RANK_T) k_rank(const uint4* __restrict__ keys, int* __restrict__ rank,
+                                                 const Ctrl* ctrl) {
+    __shared__ uint4 tile[RANK_T];
     const int n = ctrl->n_oriented;
-    if ((int)(blockIdx.x * blockDim.x) >= n) return;
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    uint4 me = (e < n) ? keys[e] : make_uint4(0, 0, 0, 0);
-    int cnt = 0;
-    for (int t0 = 0; t0 < n; t0 += RANK_TILE) {
+    const int nt = (n + RANK_T - 1) / RANK_T;
+    const long long pairs = (long long)nt * nt;
+    for (long long t = blockIdx.x; t < pairs; t += gridDim.x) {
+        const int ti = (int)(t / nt), tj = (int)(t - (long long)ti * nt);
         __syncthreads();
-        for (int k = threadIdx.x; k < RANK_TILE && t0 + k < n; k += blockDim.x) tile[k] = keys[t0 + k];
+        const int j = tj * RANK_T + threadIdx.x;
+        if (j < n) tile[threadIdx.x] = keys[j];
         __syncthreads();
-        const int m = min(RANK_TILE, n - t0);
-        for (int k = 0; k < m; ++k) cnt += key_less(tile[k], me) ? 1 : 0;
+        const int i = ti * RANK_T + threadIdx.x;
+        if (i < n) {
+            const uint4 me = keys[i];
+            const int m = min(RANK_T, n - tj * RANK_T);
+            int cnt = 0;
+            for (int k = 0; k < m; ++k) cnt += key_less(tile[k], me) ? 1 : 0;
+            if (cnt) atomicAdd(&rank[i], cnt);
+        }
     }
-    if (e < n) rank[e] = cnt;
 }
 
 // ---------------------------------------------------------------------------
@@ -1116,58 +1374,70 @@ struct DescArgs {
     float* out_desc;
 };
 
-constexpr int DESC_WARPS = 2;
-constexpr int DESC_HSTRIDE = 129;
+constexpr int DESC_T = 256;
+constexpr int DESC_W = DESC_T / 32;
 
 __device__ __forceinline__ void desc_accumulate(const float* __restrict__ g, long long P, int H, int W, float ri,
                                                 float ci, float cos_a, float sin_a, float ang_rad, int ph,
-                                                float* __restrict__ part, int lane) {
+                                                const WarpHist& hw, int tid) {
     const float scale_sp = 4.0f / (2.0f * (float)ph);
     const float sigma_d = (float)ph * 0.5657f;
     const float inv_2s2 = 1.0f / (2.0f * sigma_d * sigma_d + 1e-12f);
     const int side = 2 * ph + 1;
-    const int total = side * side;
     const int r0 = (int)ri, c0 = (int)ci;
-    for (int flat = lane; flat < total; flat += 32) {
-        int r_off = flat / side - ph;
-        int c_off = flat % side - ph;
-        int rr = r0 + r_off, cc = c0 + c_off;
-        if (rr < 1 || rr >= H - 1 || cc < 1 || cc >= W - 1) continue;
+    const int lane = tid & 31, warp = tid >> 5;
+    // the (2ph+1)^2 patch in 8x4 pixel blocks, one block per warp step
+    const int tcols = (side + 7) >> 3, trows = (side + 3) >> 2;
+    const int ntiles = tcols * trows;
+    int steps = 0;
+    for (int t = warp; t < ntiles; t += DESC_W) {
+        const int ty = t / tcols, tx = t - ty * tcols;
+        const int r_off = ty * 4 + (lane >> 3) - ph, c_off = tx * 8 + (lane & 7) - ph;
+        const int rr = r0 + r_off, cc = c0 + c_off;
+        bool act = r_off <= ph && c_off <= ph && !(rr < 1 || rr >= H - 1 || cc < 1 || cc >= W - 1);
         float fc = (float)c_off, fr = (float)r_off;
         float xr = cos_a * fc - sin_a * fr;
         float yr = sin_a * fc + cos_a * fr;
         float xb = xr * scale_sp + 1.5f;
         float yb = yr * scale_sp + 1.5f;
-        if (xb < -0.5f || xb >= 3.5f || yb < -0.5f || yb >= 3.5f) continue;
-        float dx = g[rr * P + cc + 1] - g[rr * P + cc - 1];
-        float dy = g[(rr + 1) * P + cc] - g[(rr - 1) * P + cc];
-        float mag = sqrtf(dx * dx + dy * dy);
-        float ori_deg = fmodf((sm::atan2f_(dy, dx) - ang_rad) * 57.29577951f + 360.0f, 360.0f);
-        float gw = sm::expf_(-(xr * xr + yr * yr) * inv_2s2);
-        float wmag = mag * gw;
-        float ob = ori_deg * 0.02222222f;
-        int oi0 = (int)floorf(ob);
-        float df = ob - (float)oi0;
-        int xi0 = (int)floorf(xb), yi0 = (int)floorf(yb);
-        float dx_b = xb - (float)xi0, dy_b = yb - (float)yi0;
-        int xi0c = max(0, min(xi0, 3));
-        int yi0c = max(0, min(yi0, 3));
-        int xi1c = max(0, min(xi0 + 1, 3));
-        int yi1c = max(0, min(yi0 + 1, 3));
-        int oi0w = ((oi0 % 8) + 8) % 8;
-        int oi1w = ((oi0 + 1) % 8 + 8) % 8;
-        float w_y0 = 1.0f - dy_b, w_y1 = dy_b;
-        float w_x0 = 1.0f - dx_b, w_x1 = dx_b;
-        float w_o0 = 1.0f - df, w_o1 = df;
-        part[yi0c * 32 + xi0c * 8 + oi0w] += w_y0 * w_x0 * w_o0 * wmag;
-        part[yi0c * 32 + xi0c * 8 + oi1w] += w_y0 * w_x0 * w_o1 * wmag;
-        part[yi0c * 32 + xi1c * 8 + oi0w] += w_y0 * w_x1 * w_o0 * wmag;
-        part[yi0c * 32 + xi1c * 8 + oi1w] += w_y0 * w_x1 * w_o1 * wmag;
-        part[yi1c * 32 + xi0c * 8 + oi0w] += w_y1 * w_x0 * w_o0 * wmag;
-        part[yi1c * 32 + xi0c * 8 + oi1w] += w_y1 * w_x0 * w_o1 * wmag;
-        part[yi1c * 32 + xi1c * 8 + oi0w] += w_y1 * w_x1 * w_o0 * wmag;
-        part[yi1c * 32 + xi1c * 8 + oi1w] += w_y1 * w_x1 * w_o1 * wmag;
+        act = act && !(xb < -0.5f || xb >= 3.5f || yb < -0.5f || yb >= 3.5f);
+        if (act) {
+            const float* gp = g + rr * P + cc;
+            float dx = gp[1] - gp[-1];
+            float dy = gp[P] - gp[-P];
+            float mag = sqrtf(dx * dx + dy * dy);
+            float ori_deg = mod360((sm::atan2f_(dy, dx) - ang_rad) * 57.29577951f + 360.0f);
+            float gw = sm::expf_(-(xr * xr + yr * yr) * inv_2s2);
+            const float wmag = mag * gw;
+            float ob = ori_deg * 0.02222222f;
+            int oi0 = (int)floorf(ob);
+            float df = ob - (float)oi0;
+            int xi0 = (int)floorf(xb), yi0 = (int)floorf(yb);
+            float dx_b = xb - (float)xi0, dy_b = yb - (float)yi0;
+            int xi0c = max(0, min(xi0, 3));
+            int yi0c = max(0, min(yi0, 3));
+            int xi1c = max(0, min(xi0 + 1, 3));
+            int yi1c = max(0, min(yi0 + 1, 3));
+            int oi0w = ((oi0 % 8) + 8) % 8;
+            int oi1w = ((oi0 + 1) % 8 + 8) % 8;
+            float w_y0 = 1.0f - dy_b, w_y1 = dy_b;
+            float w_x0 = 1.0f - dx_b, w_x1 = dx_b;
+            float w_o0 = 1.0f - df, w_o1 = df;
+            hw.add(yi0c * 32 + xi0c * 8 + oi0w, fix40(w_y0 * w_x0 * w_o0 * wmag));
+            hw.add(yi0c * 32 + xi0c * 8 + oi1w, fix40(w_y0 * w_x0 * w_o1 * wmag));
+            hw.add(yi0c * 32 + xi1c * 8 + oi0w, fix40(w_y0 * w_x1 * w_o0 * wmag));
+            hw.add(yi0c * 32 + xi1c * 8 + oi1w, fix40(w_y0 * w_x1 * w_o1 * wmag));
+            hw.add(yi1c * 32 + xi0c * 8 + oi0w, fix40(w_y1 * w_x0 * w_o0 * wmag));
+            hw.add(yi1c * 32 + xi0c * 8 + oi1w, fix40(w_y1 * w_x0 * w_o1 * wmag));
+            hw.add(yi1c * 32 + xi1c * 8 + oi0w, fix40(w_y1 * w_x1 * w_o0 * wmag));
+            hw.add(yi1c * 32 + xi1c * 8 + oi1w, fix40(w_y1 * w_x1 * w_o1 * wmag));
+        }
+        if (++steps == FOLD_STEPS) {
+            hw.fold();
+            steps = 0;
+        }
     }
+    hw.fold();
 }
 
 __device__ __forceinline__ float warp_tree_sum(float v) {
@@ -1176,90 +1446,89 @@ __device__ __forceinline__ float warp_tree_sum(float v) {
     v += __shfl_down_sync(FULL_MASK, v, 4);
     v += __shfl_down_sync(FULL_MASK, v, 2);
     v += __shfl_down_sync(FULL_MASK, v, 1);
-    return __shfl_sync(FULL_MASK, v, 0);
+    return v;
 }
 
-// Sum over the 128 bins in the reference's order: a warp tree per 32 bins,
-// then the four warp partials in order.  Lane j holds bins j + 32q.
-__device__ __forceinline__ float bins_sum_sq(const float v[4]) {
-    float w0 = warp_tree_sum(v[0] * v[0]), w1 = warp_tree_sum(v[1] * v[1]);
-    float w2 = warp_tree_sum(v[2] * v[2]), w3 = warp_tree_sum(v[3] * v[3]);
-    return w0 + w1 + w2 + w3;
+// Sum over the 128 bins (thread = bin) in the reference's order: a warp
+// shuffle tree per 32 bins, then the four warp partials in order.
+// Called by threads 0..127 only (named barrier 1 over those 4 warps).
+__device__ __forceinline__ float bins_sum(float x, float* part) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float w = warp_tree_sum(x);
+    if (lane == 0) part[warp] = w;
+    asm volatile("bar.sync 1, 128;" ::: "memory");
+    float s = part[0] + part[1] + part[2] + part[3];
+    asm volatile("bar.sync 1, 128;" ::: "memory");
+    return s;
 }
 
-__global__ void __launch_bounds__(DESC_WARPS * 32) k_descriptor(const DescArgs a, const Ctrl* ctrl) {
-    __shared__ float part_all[DESC_WARPS][32 * DESC_HSTRIDE];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int e = blockIdx.x * DESC_WARPS + warp;
-    if (e >= ctrl->n_oriented) return;
-    float* mine = part_all[warp] + lane * DESC_HSTRIDE;
-    for (int b = 0; b < 128; ++b) mine[b] = 0.0f;
-    const int kp = a.ent_kp[e], slot = a.ent_slot[e];
-    const int o = a.kp_o[kp], si = a.kp_si[kp];
-    const float ri = a.kp_ri[kp], ci = a.kp_ci[kp];
-    const float angle = a.ang[kp * 4 + slot];
-    const float ang_rad = angle * (float)(3.14159265358979323846 / 180.0);
-    const float phf = a.desc_ph[si];
-    const OctView& v = a.oct[o];
-    float sin_a, cos_a;
-    sm::sincosf_(ang_rad, &sin_a, &cos_a);
-    const float* g = v.lev[si];
-    if (a.n_dsp > 0) {
-        for (int d = 0; d < a.n_dsp; ++d) {
-            int ph = (int)(phf * a.dsp_scales[d] + 0.5f);
-            if (ph < 4) ph = 4;
-            desc_accumulate(g, v.pitch, v.H, v.W, ri, ci, cos_a, sin_a, ang_rad, ph, mine, lane);
+// One DESC_T-thread block per oriented keypoint (grid-stride).  Warps
+// accumulate into private fixed-point histograms; threads 0..127 then own one
+// bin each for the merge, normalisation and RootSIFT.
+__global__ void __launch_bounds__(DESC_T) k_descriptor(const DescArgs a, const Ctrl* ctrl) {
+    __shared__ unsigned int wlo[DESC_W][128], whi[DESC_W][128];
+    __shared__ unsigned long long whist[DESC_W][128];
+    __shared__ float part[4];
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int n = ctrl->n_oriented;
+    for (int e = blockIdx.x; e < n; e += gridDim.x) {
+        for (int b = tid; b < DESC_W * 128; b += DESC_T) {
+            (&whist[0][0])[b] = 0ull;
+            (&wlo[0][0])[b] = 0u;
+            (&whi[0][0])[b] = 0u;
         }
-    } else {
-        desc_accumulate(g, v.pitch, v.H, v.W, ri, ci, cos_a, sin_a, ang_rad, (int)phf, mine, lane);
-    }
-    __syncwarp();
-    const float* base = part_all[warp];
-    float vq[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const int b = q * 32 + lane;
-        float acc = base[b];
-        for (int l = 1; l < 32; ++l) acc = acc + base[l * DESC_HSTRIDE + b];
-        vq[q] = acc;
-    }
-    if (a.n_dsp > 0) {
-        const float inv_n = 1.0f / (float)a.n_dsp;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) vq[q] = vq[q] * inv_n;
-    }
-    float inv = 1.0f / sqrtf(bins_sum_sq(vq) + 1e-14f);
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        float t = vq[q] * inv;
-        vq[q] = t > 0.2f ? 0.2f : t;
-    }
-    inv = 1.0f / sqrtf(bins_sum_sq(vq) + 1e-14f);
-#pragma unroll
-    for (int q = 0; q < 4; ++q) vq[q] = vq[q] * inv;
-    if (a.rootsift) {
-        float l0 = warp_tree_sum(fabsf(vq[0])), l1 = warp_tree_sum(fabsf(vq[1]));
-        float l2 = warp_tree_sum(fabsf(vq[2])), l3 = warp_tree_sum(fabsf(vq[3]));
-        const float den = (l0 + l1 + l2 + l3) + 1e-7f;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            float t = vq[q] / den;
-            if (t < 0.0f) t = 0.0f;
-            vq[q] = sqrtf(t);
+        __syncthreads();
+        const int kp = a.ent_kp[e], slot = a.ent_slot[e];
+        const int o = a.kp_o[kp], si = a.kp_si[kp];
+        const float ri = a.kp_ri[kp], ci = a.kp_ci[kp];
+        const float angle = a.ang[kp * 4 + slot];
+        const float ang_rad = angle * (float)(3.14159265358979323846 / 180.0);
+        const float phf = a.desc_ph[si];
+        const OctView& v = a.oct[o];
+        float sin_a, cos_a;
+        sm::sincosf_(ang_rad, &sin_a, &cos_a);
+        const float* g = v.lev[si];
+        const WarpHist hw{wlo[warp], whi[warp], whist[warp], 128};
+        if (a.n_dsp > 0) {
+            for (int dd = 0; dd < a.n_dsp; ++dd) {
+                int ph = (int)(phf * a.dsp_scales[dd] + 0.5f);
+                if (ph < 4) ph = 4;
+                desc_accumulate(g, v.pitch, v.H, v.W, ri, ci, cos_a, sin_a, ang_rad, ph, hw, tid);
+            }
+        } else {
+            desc_accumulate(g, v.pitch, v.H, v.W, ri, ci, cos_a, sin_a, ang_rad, (int)phf, hw, tid);
         }
-    }
-    const int row = a.rank[e];
-    float* dst = a.out_desc + (long long)row * 128;
+        __syncthreads();
+        if (tid < 128) {
+            unsigned long long s = 0ull;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) dst[q * 32 + lane] = vq[q];
-    if (lane == 0) {
-        const float sc = a.coord_scale[o];
-        a.out_kpts[row * 4 + 0] = ci * sc;
-        a.out_kpts[row * 4 + 1] = ri * sc;
-        a.out_kpts[row * 4 + 2] = a.kp_size[o][si];
-        a.out_kpts[row * 4 + 3] = angle;
-        a.out_resp[row] = a.kp_resp[kp];
-        a.out_oct[row] = o;
+            for (int w = 0; w < DESC_W; ++w) s += whist[w][tid];
+            float val = unfix40(s);
+            if (a.n_dsp > 0) val = val * (1.0f / (float)a.n_dsp);
+            float inv = 1.0f / sqrtf(bins_sum(val * val, part) + 1e-14f);
+            float t = val * inv;
+            val = t > 0.2f ? 0.2f : t;
+            inv = 1.0f / sqrtf(bins_sum(val * val, part) + 1e-14f);
+            val = val * inv;
+            if (a.rootsift) {
+                const float den = bins_sum(fabsf(val), part) + 1e-7f;
+                float q = val / den;
+                if (q < 0.0f) q = 0.0f;
+                val = sqrtf(q);
+            }
+            const int row = a.rank[e];
+            a.out_desc[(long long)row * 128 + tid] = val;
+            if (tid == 0) {
+                const float sc = a.coord_scale[o];
+                a.out_kpts[row * 4 + 0] = ci * sc;
+                a.out_kpts[row * 4 + 1] = ri * sc;
+                a.out_kpts[row * 4 + 2] = a.kp_size[o][si];
+                a.out_kpts[row * 4 + 3] = angle;
+                a.out_resp[row] = a.kp_resp[kp];
+                a.out_oct[row] = o;
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -1339,23 +1608,17 @@ static int run_detect(const pysift_detect_config* cfg, const uint8_t* gray, int 
     PYSIFT_CUDA_TRY(cudaMemsetAsync(ctrl, 0, sizeof(Ctrl), st));
     // A1
     {
-        long long n = (long long)H * W;
-        int blocks = (int)std::min<long long>(ceil_div_ll(n, 256 * 16), (long long)num_sms() * 4);
-        if (blocks < 1) blocks = 1;
-        k_histogram<<<blocks, 256, 0, st>>>(gray, H, W, pitch, ctrl, cfg->contrast_thresh, S);
+        const int gx = ceil_div(W, 256);
+        int gy = std::max(1, std::min(H, (num_sms() * 4) / gx));
+        k_histogram<<<dim3(gx, gy), 256, 0, st>>>(gray, H, W, pitch, ctrl, cfg->contrast_thresh, S);
         PYSIFT_LAUNCH_CHECK("k_histogram");
     }
     // A2/A3: base image
     float* base = at<float>(ws, l.off_base);
     if (l.doubled) {
         double* coef = at<double>(ws, l.off_coef);
-        k_prefilter_cols<<<ceil_div(W, 128), 128, 0, st>>>(gray, H, W, pitch, cfg->fp16_pyramid, coef);
-        PYSIFT_LAUNCH_CHECK("k_prefilter_cols");
-        k_prefilter_rows<<<ceil_div(H, 128), 128, 0, st>>>(coef, H, W);
-        PYSIFT_LAUNCH_CHECK("k_prefilter_rows");
-        k_zoom_interp<<<dim3(ceil_div(2 * W, 256), 2 * H), 256, 0, st>>>(coef, H, W, cfg->fp16_pyramid, base,
-                                                                         l.pitch0);
-        PYSIFT_LAUNCH_CHECK("k_zoom_interp");
+        int rc = launch_zoom2x(gray, H, W, pitch, cfg->fp16_pyramid, coef, base, l.pitch0, st);
+        if (rc) return rc;
     } else {
         k_u8_to_f32<<<dim3(ceil_div(W, 256), H), 256, 0, st>>>(gray, H, W, pitch, cfg->fp16_pyramid, base,
                                                                l.pitch0);
@@ -1502,7 +1765,7 @@ static int run_detect(const pysift_detect_config* cfg, const uint8_t* gray, int 
     oa.kp_ci = ca.kp_ci;
     oa.ang = at<float>(ws, l.off_ang);
     oa.angcnt = at<int>(ws, l.off_angcnt);
-    k_orientation<<<ceil_div(kcap, ORI_WARPS), ORI_WARPS * 32, 0, st>>>(oa, ctrl);
+    k_orientation<<<std::min(kcap, num_sms() * 32), ORI_T, 0, st>>>(oa, ctrl);
     PYSIFT_LAUNCH_CHECK("k_orientation");
     // expansion + keys + rank
     ExpArgs xa;
@@ -1520,7 +1783,8 @@ static int run_detect(const pysift_detect_config* cfg, const uint8_t* gray, int 
     k_expand<<<1, 1024, 0, st>>>(xa, ctrl);
     PYSIFT_LAUNCH_CHECK("k_expand");
     int* rank = at<int>(ws, l.off_rank);
-    k_rank<<<ceil_div(4 * kcap, 256), 256, 0, st>>>(xa.keys, rank, ctrl);
+    PYSIFT_CUDA_TRY(cudaMemsetAsync(rank, 0, sizeof(int) * 4 * (size_t)kcap, st));
+    k_rank<<<num_sms() * 8, RANK_T, 0, st>>>(xa.keys, rank, ctrl);
     PYSIFT_LAUNCH_CHECK("k_rank");
     PYSIFT_STAGE(5);
     // A11
@@ -1548,7 +1812,7 @@ static int run_detect(const pysift_detect_config* cfg, const uint8_t* gray, int 
     da.out_resp = resp;
     da.out_oct = octv;
     da.out_desc = desc;
-    k_descriptor<<<ceil_div(4 * kcap, DESC_WARPS), DESC_WARPS * 32, 0, st>>>(da, ctrl);
+    k_descriptor<<<std::min(4 * kcap, num_sms() * (2048 / DESC_T)), DESC_T, 0, st>>>(da, ctrl);
     PYSIFT_LAUNCH_CHECK("k_descriptor");
     k_finalize<<<1, 32, 0, st>>>(ctrl, stats, n_oct, l.doubled ? 1 : 0);
     PYSIFT_LAUNCH_CHECK("k_finalize");
@@ -1657,13 +1921,7 @@ int pysift_zoom2x_u8(const uint8_t* gray, int32_t H, int32_t W, int64_t pitch_by
     PYSIFT_CHECK_ARG(gray && coef && out, "NULL pointer argument");
     PYSIFT_CHECK_ARG(H > 0 && W > 0 && pitch_bytes >= W && out_pitch >= 2 * W, "bad sizes");
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    k_prefilter_cols<<<ceil_div(W, 128), 128, 0, st>>>(gray, H, W, pitch_bytes, fp16_round, coef);
-    PYSIFT_LAUNCH_CHECK("k_prefilter_cols");
-    k_prefilter_rows<<<ceil_div(H, 128), 128, 0, st>>>(coef, H, W);
-    PYSIFT_LAUNCH_CHECK("k_prefilter_rows");
-    k_zoom_interp<<<dim3(ceil_div(2 * W, 256), 2 * H), 256, 0, st>>>(coef, H, W, fp16_round, out, out_pitch);
-    PYSIFT_LAUNCH_CHECK("k_zoom_interp");
-    return PYSIFT_OK;
+    return launch_zoom2x(gray, H, W, pitch_bytes, fp16_round, coef, out, out_pitch, st);
 }
 
 }  // extern "C"
@@ -1733,11 +1991,5 @@ extern "C" int pysift_zoom2x_u8_noalloc(const uint8_t* gray, int32_t H, int32_t 
     // call (k_prefilter_cols fills all H*W coefficients), so nothing needs
     // clearing between calls.
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    k_prefilter_cols<<<ceil_div(W, 128), 128, 0, st>>>(gray, H, W, pitch_bytes, fp16_round, coef);
-    PYSIFT_LAUNCH_CHECK("k_prefilter_cols");
-    k_prefilter_rows<<<ceil_div(H, 128), 128, 0, st>>>(coef, H, W);
-    PYSIFT_LAUNCH_CHECK("k_prefilter_rows");
-    k_zoom_interp<<<dim3(ceil_div(2 * W, 256), 2 * H), 256, 0, st>>>(coef, H, W, fp16_round, out, out_pitch);
-    PYSIFT_LAUNCH_CHECK("k_zoom_interp");
-    return PYSIFT_OK;
+    return launch_zoom2x(gray, H, W, pitch_bytes, fp16_round, coef, out, out_pitch, st);
 }

@@ -9,9 +9,10 @@
 //   sm_expf   Cody-Waite reduction x = n*ln2 + r (ln2 split in a 16-bit head
 //             and a tail), Taylor series of exp(r) to degree 8 (Horner/fmaf),
 //             exact power-of-two scaling.
-//   sm_atan2f octant reduction to t in [0,1]; t > tan(pi/8) is mapped through
-//             atan(t) = pi/4 + atan((t-1)/(t+1)); Taylor series of atan to
-//             u^23; quadrant fix-up from the operand signs.
+//   sm_atan2f t = min(|x|,|y|)/max(|x|,|y|) in [0,1], atan(t) = t*P(t^2) with
+//             P of degree 9 (coefficients from a Chebyshev interpolation of
+//             atan(sqrt(s))/sqrt(s) on [0,1], rounded to float32; max error
+//             ~1.5 ulp), then octant/quadrant fix-up from the operand signs.
 //   sm_sincosf Cody-Waite reduction by pi/2 in three float parts (the split
 //             used by the Cephes library), Taylor series of sin to r^9 and
 //             cos to r^10, quadrant rotation.
@@ -55,39 +56,28 @@ constexpr float PI_F = 3.14159265358979323846f;
 constexpr float PIO2_F = 1.57079632679489661923f;
 constexpr float PIO4_F = 0.78539816339744830962f;
 
-__device__ __forceinline__ float atan_poly(float u) {
-    float u2 = u * u;
-    float p = -4.34782608695652173913e-02f;
-    p = fmaf(p, u2, 4.76190476190476190476e-02f);
-    p = fmaf(p, u2, -5.26315789473684210526e-02f);
-    p = fmaf(p, u2, 5.88235294117647058824e-02f);
-    p = fmaf(p, u2, -6.66666666666666666667e-02f);
-    p = fmaf(p, u2, 7.69230769230769230769e-02f);
-    p = fmaf(p, u2, -9.09090909090909090909e-02f);
-    p = fmaf(p, u2, 1.11111111111111111111e-01f);
-    p = fmaf(p, u2, -1.42857142857142857143e-01f);
-    p = fmaf(p, u2, 2.00000000000000000000e-01f);
-    p = fmaf(p, u2, -3.33333333333333333333e-01f);
-    return fmaf(u * u2, p, u);
-}
-
 __device__ __forceinline__ float atan2f_(float y, float x) {
     float ax = fabsf(x), ay = fabsf(y);
     if (ax == 0.0f && ay == 0.0f) {
         float a = signbit(x) ? PI_F : 0.0f;
         return signbit(y) ? -a : a;
     }
-    bool swap = ay > ax;
-    float num = swap ? ax : ay;
-    float den = swap ? ay : ax;
-    float t = num / den;
-    float a;
-    if (t > 0.41421356237309504880f) {
-        float u = (t - 1.0f) / (t + 1.0f);
-        a = PIO4_F + atan_poly(u);
-    } else {
-        a = atan_poly(t);
-    }
+    const bool swap = ay > ax;
+    const float mn = swap ? ax : ay;
+    const float mx = swap ? ay : ax;
+    const float t = mn / mx;
+    const float s = t * t;
+    float p = -0x1.c919cep-10f;
+    p = fmaf(p, s, 0x1.5dfc5ep-7f);
+    p = fmaf(p, s, -0x1.f74692p-6f);
+    p = fmaf(p, s, 0x1.d6bdd0p-5f);
+    p = fmaf(p, s, -0x1.56eb74p-4f);
+    p = fmaf(p, s, 0x1.c01c4cp-4f);
+    p = fmaf(p, s, -0x1.2413b8p-3f);
+    p = fmaf(p, s, 0x1.999052p-3f);
+    p = fmaf(p, s, -0x1.555534p-2f);
+    p = fmaf(p, s, 0x1.000000p+0f);
+    float a = t * p;
     if (swap) a = PIO2_F - a;
     if (signbit(x)) a = PI_F - a;
     if (signbit(y)) a = -a;
