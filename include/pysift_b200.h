@@ -133,6 +133,29 @@ int pysift_gauss_blur(const float* in, int32_t in_pitch, float* out, int32_t out
 int pysift_zoom2x_u8(const uint8_t* gray, int32_t H, int32_t W, int64_t pitch_bytes, int32_t fp16_round,
                      double* coef, float* out, int32_t out_pitch, pysift_stream_t stream);
 
+/* ---- brute-force ratio-test matching (tcgen05 tensor cores) ----
+ * Replaces GPUPyStitch._match_symmetric / _match_one_direction and the
+ * mutual intersection of _match_features (pysift/core.py:2574-2701,
+ * 2930-2940).  Per direction: best index, ratio-test pass flag; the mutual
+ * pairs (i, j) in query order with distance sqrt(d1^2).  Ties between equal
+ * scores go to the lower index.  D must be 64 or 128. */
+int pysift_match_workspace_size(int32_t n1, int32_t n2, int32_t D, int32_t exact_u8, size_t* bytes);
+
+/* Reference semantics: fp16 operands (16-byte aligned rows), the fp32
+ * tensor-core tile rounded to fp16, d^2 = max(0, 2 - 2 s), pass iff
+ * d2^2 > 1e-10 and d1^2 < ratio^2 d2^2 (float32). pairs: int32[n1][2]. */
+int pysift_match_fp16(const uint16_t* d1, int32_t n1, const uint16_t* d2, int32_t n2, int32_t D, float ratio,
+                      void* workspace, size_t workspace_bytes, int32_t* fwd_best, int32_t* fwd_pass,
+                      int32_t* bwd_best, int32_t* bwd_pass, int32_t* pairs, float* pair_dist, int32_t* pair_count,
+                      pysift_stream_t stream);
+
+/* Exact squared L2 of uint8-valued descriptors via bf16 products (exact for
+ * D <= 128), pass iff d2^2 > 0 and d1^2 < ratio^2 d2^2. */
+int pysift_match_u8_exact(const uint8_t* d1, int32_t n1, const uint8_t* d2, int32_t n2, int32_t D, float ratio,
+                          void* workspace, size_t workspace_bytes, int32_t* fwd_best, int32_t* fwd_pass,
+                          int32_t* bwd_best, int32_t* bwd_pass, int32_t* pairs, float* pair_dist,
+                          int32_t* pair_count, pysift_stream_t stream);
+
 /* Allocation-free 2x zoom (no counterpart in the reference; it exists for
  * callers that cannot allocate device memory at the call site, such as a
  * plugin inside a host application that owns the device heap).  Same result

@@ -1,0 +1,77 @@
+"""CPU oracle for ratio-test matching -- TEST INFRASTRUCTURE ONLY.
+
+Restates pysift/core.py:2652-2701 (_match_symmetric) and 2840-2940
+(_match_features' mutual intersection) in numpy, with the canonical
+tie-break (equal scores: lower index first) that the reference leaves to
+torch.topk.
+
+* fp16 mode: the similarity is the fp16 rounding of the EXACT dot product
+  of the fp16 operands (float64 accumulation is exact for D <= 128 here up
+  to one final rounding); the GPU's fp32 tensor-core accumulation can
+  differ from it only when the exact value lies within ~1e-7 of an fp16
+  rounding boundary.
+* exact mode: int64 squared L2 distances of uint8 descriptors.
+"""
+import numpy as np
+
+
+def _top2(keys, larger_is_better):
+    """Per-row (best idx, best key, second key) with lower-index ties."""
+    n, m = keys.shape
+    k = keys if larger_is_better else -keys
+    # stable ordering: sort by (-key, index)
+    order = np.lexsort((np.broadcast_to(np.arange(m), keys.shape), -k), axis=1)
+    b1 = order[:, 0]
+    rows = np.arange(n)
+    k1 = keys[rows, b1]
+    k2 = keys[rows, order[:, 1]] if m > 1 else np.full(n, np.nan)
+    return b1, k1, k2
+
+
+def sim_fp16(d1h, d2h):
+    a = d1h.astype(np.float64)
+    b = d2h.astype(np.float64)
+    return (a @ b.T).astype(np.float16).astype(np.float32)
+
+
+def ratio_pass_fp16(s1, s2, ratio_sq=np.float32(0.5625)):
+    db = np.maximum(np.float32(2.0) - np.float32(2.0) * s1, np.float32(0.0))
+    ds = np.maximum(np.float32(2.0) - np.float32(2.0) * s2, np.float32(0.0))
+    ok = (ds > np.float32(1e-10)) & (db < ratio_sq * ds)
+    return ok, np.sqrt(db)
+
+
+def match_fp16(d1h, d2h, ratio=0.75):
+    S = sim_fp16(d1h, d2h)
+    rs = np.float32(ratio * ratio)
+    fb, f1, f2 = _top2(S, True)
+    fok, fdist = ratio_pass_fp16(f1, f2, rs)
+    bb, b1, b2 = _top2(S.T.copy(), True)
+    bok, _ = ratio_pass_fp16(b1, b2, rs)
+    return _mutual(fb, fok, fdist, bb, bok, S)
+
+
+def match_u8_exact(a, b, ratio=0.75):
+    A = a.astype(np.int64)
+    B = b.astype(np.int64)
+    D2 = (A * A).sum(1)[:, None] + (B * B).sum(1)[None, :] - 2 * (A @ B.T)
+    rs = ratio * ratio
+    fb, f1, f2 = _top2(D2, False)
+    fok = (f2 > 0) & (f1.astype(np.float64) < rs * f2.astype(np.float64))
+    bb, b1, b2 = _top2(D2.T.copy(), False)
+    bok = (b2 > 0) & (b1.astype(np.float64) < rs * b2.astype(np.float64))
+    return _mutual(fb, fok, np.sqrt(f1.astype(np.float32)), bb, bok, D2)
+
+
+def _mutual(fb, fok, fdist, bb, bok, S):
+    pairs = []
+    dist = []
+    for i in range(len(fb)):
+        if fok[i]:
+            j = int(fb[i])
+            if bok[j] and bb[j] == i:
+                pairs.append((i, j))
+                dist.append(fdist[i])
+    return dict(fwd_best=fb.astype(np.int32), fwd_pass=fok.astype(np.int32), bwd_best=bb.astype(np.int32),
+                bwd_pass=bok.astype(np.int32), pairs=np.array(pairs, np.int32).reshape(-1, 2),
+                dist=np.array(dist, np.float32), scores=S)

@@ -92,6 +92,16 @@ EXPORTS = {
 }
 ZOOM2X_NOALLOC_MAX_PIXELS = 1 << 20
 
+EXPORTS.update({
+    "pysift_match_workspace_size": (ctypes.c_int, [c_int32, c_int32, c_int32, c_int32, ctypes.POINTER(c_size_t)]),
+    "pysift_match_fp16": (ctypes.c_int, [c_void_p, c_int32, c_void_p, c_int32, c_int32, c_float, c_void_p, c_size_t,
+                                         c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                         c_void_p]),
+    "pysift_match_u8_exact": (ctypes.c_int, [c_void_p, c_int32, c_void_p, c_int32, c_int32, c_float, c_void_p,
+                                             c_size_t, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                             c_void_p, c_void_p]),
+})
+
 
 def lib_path():
     return _build.LIB_PATH

@@ -1,0 +1,66 @@
+"""Brute-force ratio-test matching on the tensor cores (C ABI: pysift_match_*).
+
+Two entry points:
+
+* ``match_fp16(d1, d2, ratio)``: the reference's stitch-path semantics
+  (pysift/core.py:2652-2701): fp16 operands, the similarity tile rounded to
+  fp16, top-2 per row and per column, ratio test on d^2 = max(0, 2 - 2 s),
+  mutual consistency.
+* ``match_u8_exact(a, b, ratio)``: exact squared-L2 matching of uint8-valued
+  descriptors through bf16 tensor-core products (exact for 128-d uint8).
+
+Both take CUDA tensors and return CUDA tensors; ties go to the lower index.
+"""
+import ctypes
+
+import torch
+
+from . import _lib
+
+
+def _ws(lib, n1, n2, D, exact, device):
+    sz = ctypes.c_size_t()
+    _lib.check(lib.pysift_match_workspace_size(n1, n2, D, 1 if exact else 0, ctypes.byref(sz)),
+               "pysift_match_workspace_size")
+    return torch.empty(int(sz.value) + 256, dtype=torch.uint8, device=device)
+
+
+def _aligned(t):
+    off = (-t.data_ptr()) % 256
+    return t.data_ptr() + off, t.numel() - off
+
+
+def _run(fn, name, d1, d2, ratio, exact, stream=None):
+    lib = _lib.load()
+    n1, D = d1.shape
+    n2 = d2.shape[0]
+    dev = d1.device
+    ws = _ws(lib, n1, n2, D, exact, dev)
+    wp, wn = _aligned(ws)
+    out = {k: torch.empty(n, dtype=torch.int32, device=dev) for k, n in
+           (("fwd_best", n1), ("fwd_pass", n1), ("bwd_best", n2), ("bwd_pass", n2))}
+    pairs = torch.empty((n1, 2), dtype=torch.int32, device=dev)
+    dist = torch.empty(n1, dtype=torch.float32, device=dev)
+    count = torch.zeros(1, dtype=torch.int32, device=dev)
+    st = (stream or torch.cuda.current_stream(dev)).cuda_stream
+    rc = fn(d1.data_ptr(), n1, d2.data_ptr(), n2, D, float(ratio), wp, wn, out["fwd_best"].data_ptr(),
+            out["fwd_pass"].data_ptr(), out["bwd_best"].data_ptr(), out["bwd_pass"].data_ptr(), pairs.data_ptr(),
+            dist.data_ptr(), count.data_ptr(), st)
+    _lib.check(rc, name)
+    out.update(pairs=pairs, dist=dist, count=count, workspace=ws)
+    return out
+
+
+def match_fp16(d1, d2, ratio=0.75, stream=None):
+    """d1 (N,D), d2 (M,D) float16 CUDA tensors, D in {64, 128}."""
+    assert d1.dtype == torch.float16 and d2.dtype == torch.float16
+    d1 = d1.contiguous()
+    d2 = d2.contiguous()
+    return _run(_lib.load().pysift_match_fp16, "pysift_match_fp16", d1, d2, ratio, False, stream)
+
+
+def match_u8_exact(a, b, ratio=0.75, stream=None):
+    """a (N,D), b (M,D) uint8 CUDA tensors, D in {64, 128}."""
+    assert a.dtype == torch.uint8 and b.dtype == torch.uint8
+    return _run(_lib.load().pysift_match_u8_exact, "pysift_match_u8_exact", a.contiguous(), b.contiguous(),
+                ratio, True, stream)
