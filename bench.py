@@ -7,8 +7,10 @@
 Prints ONE JSON line on rank 0.  Workloads (synthetic, seeded inputs that
 stand in for the reference's datasets; see pysift_b200/synthetic.py):
 
-  detect_1280x960   detectAndCompute on one 1280x960 grayscale scene (the
-                    image size of the stitch-pair configuration)
+  stitch_pair_1280x960  GPUPyStitch().stitch(img1, img2) on a seeded synthetic
+                    pair of 1280x960 BGR views (ratio 0.75, 2048 hypotheses,
+                    4 px, linear feather blend) -- the default
+  detect_1280x960   detectAndCompute on one 1280x960 grayscale scene
   detect_640x480    detectAndCompute on one 640x480 scene
 
 A step is one pass of the hot path over one input.  `value` is measured
@@ -32,10 +34,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOADS = {
+    "stitch_pair_1280x960": dict(kind="stitch", H=960, W=1280, seed=0, ransac_iters=2048, inlier_thresh=4.0),
     "detect_1280x960": dict(kind="detect", H=960, W=1280, seed=0),
     "detect_640x480": dict(kind="detect", H=480, W=640, seed=0),
 }
-DEFAULT_WORKLOAD = "detect_1280x960"
+DEFAULT_WORKLOAD = "stitch_pair_1280x960"
 METRIC = "SIFT Mpix/s + match-pairs/s on 1 B200: batched+BF16 vs plain, bit-exact"
 FALLBACK_HBM_GBS = 6650.0
 
@@ -124,16 +127,6 @@ def pyramid_alg_bytes(H, W, sift):
     return H * W + 4 * P[0] + 80 * sum(P)
 
 
-def detect_launches(sift, H, W):
-    """Kernel launches issued by one pysift_detect_and_compute call."""
-    doubled = sift.double_image and H * W < sift._cfg.double_px_cap
-    n_oct, S = sift.n_octaves, sift.n_scales
-    base = 3 if doubled else 1
-    blurs = 1 + n_oct * (S + 2)
-    detect = 2 * 5 + 1
-    return 1 + base + blurs + detect + 1 + 1 + 1 + 1 + 1 + 1
-
-
 def cpu_detect_baseline(img, budget_s=15.0):
     """The oracle (a CPU port of the reference's path, OpenMP over the host
     cores) on the same image, repeated until ~budget_s of work."""
@@ -180,6 +173,8 @@ def run_reference(args, wl, world, rank):
     if rank != 0:
         return 0
     from pysift_b200 import synthetic
+    if wl["kind"] == "stitch":
+        return run_reference_stitch(args, wl)
     img = synthetic.scene(wl["H"], wl["W"], seed=wl["seed"])
     times = []
     from oracle import oracle
@@ -201,6 +196,33 @@ def run_reference(args, wl, world, rank):
         "cpu_baseline": {"value": value, "unit": "Mpix/s", "cores": os.cpu_count(), "kind": "port",
                          "sample": f"one {wl['W']}x{wl['H']} image per step, full detectAndCompute"},
         "e2e": {"value": value, "unit": "Mpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_reference_stitch(args, wl):
+    from oracle import stitch_oracle as so
+    from pysift_b200 import synthetic
+    img1, img2, _ = synthetic.stitch_pair(wl["H"], wl["W"], seed=wl["seed"])
+    times = []
+    for i in range(args.warmup + args.steps):
+        orc = so.OracleStitch(ransac_iters=wl["ransac_iters"], inlier_thresh=wl["inlier_thresh"])
+        t0 = time.perf_counter()
+        orc.stitch(img1, img2)
+        if i >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    sec = float(np.mean(times))
+    value = 1.0 / sec
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "H": wl["H"], "W": wl["W"], "seed": wl["seed"],
+                   "ransac_iters": wl["ransac_iters"], "inlier_thresh": wl["inlier_thresh"]},
+        "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": os.cpu_count(), "kind": "port",
+                         "sample": "one full two-image stitch per step (oracle port, OpenMP over the host cores)"},
+        "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -231,6 +253,8 @@ def run_detect(args, wl, world, rank, local):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize(dev)
+    from pysift_b200 import _lib
+    launches0 = _lib.load().pysift_launch_count()
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             flush.zero_()
@@ -239,6 +263,7 @@ def run_detect(args, wl, world, rank, local):
             step_ms.append(ev[0].elapsed_time(ev[6]))
             pyr_ms.append(ev[0].elapsed_time(ev[3]))
             stage.append([ev[i].elapsed_time(ev[i + 1]) for i in range(6)])
+    launches = _lib.load().pysift_launch_count() - launches0
     torch.cuda.synchronize(dev)
     if world > 1:
         dist.barrier()
@@ -302,7 +327,7 @@ def run_detect(args, wl, world, rank, local):
         "cpu_baseline": {"value": mpix / cpu_med, "unit": "Mpix/s", "cores": os.cpu_count(), "kind": "port",
                          "sample": f"{cpu_n} runs of the oracle detectAndCompute on the same {W}x{H} image"},
         "e2e": {"value": e2e_value, "unit": "Mpix/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "gpu_launches": detect_launches(sift, H, W) * args.steps,
+        "gpu_launches": int(launches),
         "clocks": clk.summary(),
         "stage_ms": dict(zip(["base_image", "pyramid", "extrema_mask", "refine_cap", "orientation", "descriptor"],
                              [round(float(x), 4) for x in np.mean(np.array(stage), 0)]),
@@ -311,6 +336,127 @@ def run_detect(args, wl, world, rank, local):
     if ocv:
         line["opencv_cpu"] = {"value": mpix / ocv[0], "unit": "Mpix/s", "cores": os.cpu_count(),
                               "keypoints": ocv[1]}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def cpu_stitch_baseline(img1, img2, wl, budget_s=20.0):
+    """The oracle port of the stitch path on the host cores (bounded sample)."""
+    from oracle import stitch_oracle as so
+    times = []
+    t_start = time.perf_counter()
+    while True:
+        orc = so.OracleStitch(ransac_iters=wl["ransac_iters"], inlier_thresh=wl["inlier_thresh"])
+        t0 = time.perf_counter()
+        orc.stitch(img1, img2)
+        times.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_start > budget_s or len(times) >= 5:
+            break
+    return float(np.median(times)), len(times)
+
+
+def run_stitch(args, wl, world, rank, local):
+    import torch
+    import torch.distributed as dist
+    from pysift_b200 import _lib, synthetic
+    from pysift_b200.stitch import GPUPyStitch
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    H, W = wl["H"], wl["W"]
+    img1, img2, _ = synthetic.stitch_pair(H, W, seed=wl["seed"] + rank)
+    st = GPUPyStitch(ransac_iters=wl["ransac_iters"], inlier_thresh=wl["inlier_thresh"], save_output=False,
+                     verbose=False, device=dev)
+    g1 = torch.from_numpy(img1).to(dev)
+    g2 = torch.from_numpy(img2).to(dev)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    lib = _lib.load()
+    for _ in range(args.warmup):
+        st.stitch(g1, g2)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    step_ms = []
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    launches0 = lib.pysift_launch_count()
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            e0.record(stream)
+            pano = st.stitch(g1, g2)
+            e1.record(stream)
+            e1.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+    launches = lib.pysift_launch_count() - launches0
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    t = torch.tensor([float(np.sum(step_ms))], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    m = dict(st.last_metrics)
+    # end to end through the public API with host images
+    e2e_ms = []
+    for i in range(args.warmup + args.steps):
+        flush.zero_()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        pano = st.stitch(img1, img2)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            e2e_ms.append(dt * 1e3)
+    e2e_tot = torch.tensor([float(np.sum(e2e_ms))], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(e2e_tot, op=dist.ReduceOp.MAX)
+    # roofline of the dominant kernel region: pyramid + DoG + extrema of one view
+    sift = st._detector
+    gray = st._gray_clahe(g1, "img1")
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(7)]
+    pyr_ms = []
+    for _ in range(max(3, args.steps)):
+        flush.zero_()
+        sift.run_device(gray, stage_events=ev)
+        ev[6].synchronize()
+        pyr_ms.append(ev[0].elapsed_time(ev[3]))
+    if rank != 0:
+        return 0
+    pairs_s = world * args.steps / (total_ms / 1e3)
+    e2e_pairs_s = world * args.steps / (float(e2e_tot.item()) / 1e3)
+    peak, peak_kind = measured_peaks()
+    alg = pyramid_alg_bytes(H, W, sift)
+    pyr_s = float(np.median(pyr_ms)) / 1e3
+    achieved = alg / pyr_s / 1e9
+    if args.no_cpu_baseline:
+        cpu_s, cpu_n = float("nan"), 0
+    else:
+        cpu_s, cpu_n = cpu_stitch_baseline(img1, img2, wl)
+    mpix = 2 * H * W / 1e6
+    line = {
+        "metric": METRIC, "value": pairs_s, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "H": H, "W": W, "seed": wl["seed"],
+                   "ransac_iters": wl["ransac_iters"], "inlier_thresh": wl["inlier_thresh"], "match_ratio": 0.75,
+                   "blend": "linear feather", "keypoints": [m["kp1"], m["kp2"]], "matches": m["matches"],
+                   "inliers": m["inliers"], "canvas": [m["canvas_w"], m["canvas_h"]],
+                   "l2": "flushed (256 MiB write) before every step", "parallelism": f"replicas{world}"},
+        "mpix_per_s": pairs_s * mpix,
+        "roofline": {"bound": "hbm", "kernel": "pyramid+DoG+extrema of one 1280x960 view (k_blur x%d + "
+                     "k_extrema_mask)" % (1 + sift.n_octaves * (sift.n_scales + 2)),
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_kind, "alg_bytes_per_launch": alg, "region_ms": pyr_s * 1e3,
+                     "traffic": committed_traffic(args.workload)},
+        "cpu_baseline": {"value": 1.0 / cpu_s if cpu_s == cpu_s else None, "unit": "pairs/s",
+                         "cores": os.cpu_count(), "kind": "port",
+                         "sample": f"{cpu_n} full stitches of the same pair by the oracle port (OpenMP)"},
+        "e2e": {"value": e2e_pairs_s, "unit": "pairs/s", "h2d_bytes_per_step": int(img1.nbytes + img2.nbytes),
+                "d2h_bytes_per_step": int(pano.nbytes) + 72 + 16},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
     print(json.dumps(line), flush=True)
     return 0
 
@@ -334,6 +480,8 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
+        if wl["kind"] == "stitch":
+            return run_stitch(args, wl, world, rank, local)
         return run_detect(args, wl, world, rank, local)
     finally:
         if world > 1:

@@ -156,6 +156,67 @@ int pysift_match_u8_exact(const uint8_t* d1, int32_t n1, const uint8_t* d2, int3
                           int32_t* bwd_best, int32_t* bwd_pass, int32_t* pairs, float* pair_dist,
                           int32_t* pair_count, pysift_stream_t stream);
 
+/* ---- stitch path (GPUPyStitch) ---- */
+
+/* cv2.cvtColor(BGR2GRAY) for uint8 (pysift/core.py:2546). */
+int pysift_bgr2gray(const uint8_t* bgr, int32_t H, int32_t W, int64_t pitch_bytes, uint8_t* gray, int32_t gray_pitch,
+                    pysift_stream_t stream);
+
+/* cv2.createCLAHE(clip_limit, (tiles_x, tiles_y)).apply (pysift/core.py:2563-2565);
+ * lut: caller scratch of pysift_clahe_lut_bytes bytes. */
+int pysift_clahe_lut_bytes(int32_t tiles_x, int32_t tiles_y, size_t* bytes);
+int pysift_clahe(const uint8_t* src, int32_t H, int32_t W, int32_t pitch, double clip_limit, int32_t tiles_x,
+                 int32_t tiles_y, uint8_t* lut, uint8_t* dst, int32_t dst_pitch, pysift_stream_t stream);
+
+/* Indices of the k rows with the largest response, in the order of a
+ * stable descending sort (pysift/core.py:2566-2571); k <= n.  rank: caller
+ * scratch of n int32. */
+int pysift_topk_by_response(const float* response, int32_t n, int32_t k, int32_t* rank, int32_t* out_idx,
+                            pysift_stream_t stream);
+
+/* pts[m] = (double) kpts[pairs[m][col]][0:2] for m < count (device count). */
+int pysift_gather_points(const float* kpts, const int32_t* pairs, const int32_t* count, int32_t max_pairs, int32_t col,
+                         double* pts, pysift_stream_t stream);
+
+/* Matcher preparation (pysift/core.py:2877-2888, 2703-2743): row L2
+ * normalisation (+1e-7), PCA statistics (float32 mean, float64 covariance)
+ * of the stacked normalised sets, projection + normalisation to fp16. */
+int pysift_l2_normalize_rows(const float* in, int32_t n, int32_t D, float* out, pysift_stream_t stream);
+int pysift_pca_stats(const float* x, int32_t n, int32_t D, float* mean, double* cov, pysift_stream_t stream);
+int pysift_pca_project_f16(const float* x, int32_t n, int32_t D, const float* mean, const float* proj, int32_t P,
+                           uint16_t* out, pysift_stream_t stream);
+int pysift_to_f16(const float* in, int64_t n, uint16_t* out, pysift_stream_t stream);
+
+/* The raw 32-bit MT19937 stream of torch.Generator(device='cpu').manual_seed(seed):
+ * torch.randint(0, N, (B, 4), generator=g) equals out[0:4B] % N (host function). */
+void pysift_mt19937_u32(uint32_t seed, uint32_t* out, int64_t n);
+
+/* Batched RANSAC with MAGSAC++ (or classic) scoring and two LO refits
+ * (pysift/core.py:2272-2313, 3011-3097).  pts: n x 2 float64 on the device;
+ * rand_u32: 4*n_hyp raw MT19937 draws; outputs H (9 float64, row-major),
+ * inlier mask (n bytes) and info = {n_inliers, best hypothesis, LO stage}. */
+int pysift_ransac_workspace_size(int32_t n, int32_t n_hyp, size_t* bytes);
+int pysift_ransac(const double* pts1, const double* pts2, int32_t n, const uint32_t* rand_u32, int32_t n_hyp,
+                  double inlier_thresh, double sigma_max, int32_t magsac, int32_t min_inliers, void* workspace,
+                  size_t workspace_bytes, double* H_out, uint8_t* mask_out, int32_t* info, pysift_stream_t stream);
+
+/* Normalised DLT homography of all n correspondences (pysift/core.py:2959-2981). */
+int pysift_dlt_homography(const double* pts1, const double* pts2, int32_t n, int32_t* idx_scratch, double* H_out,
+                          pysift_stream_t stream);
+
+/* Warp of image 1 (BGR uint8) onto a cw x ch canvas through hinv9
+ * (float32 inverse homography) with grid_sample(bilinear, zeros,
+ * align_corners=True) semantics and uint8 truncation
+ * (pysift/core.py:3210-3239), placement of image 2 at (iox, ioy)
+ * (pysift/core.py:3794-3800) and, where both cover the canvas, a linear
+ * feather blend (weights 1 + distance to the image border).  Optional
+ * outputs: warped image 1, both masks, per-row/column coverage extents. */
+int pysift_warp_feather(const uint8_t* img1, int32_t hs, int32_t ws, int32_t pitch1, const uint8_t* img2, int32_t h2,
+                        int32_t w2, int32_t pitch2, int32_t cw, int32_t ch, const float* hinv9, float ox, float oy,
+                        int32_t iox, int32_t ioy, int32_t feather, uint8_t* out, uint8_t* warped, uint8_t* mask1,
+                        uint8_t* mask2, int32_t* row_lo, int32_t* row_hi, int32_t* col_lo, int32_t* col_hi,
+                        pysift_stream_t stream);
+
 /* Allocation-free 2x zoom (no counterpart in the reference; it exists for
  * callers that cannot allocate device memory at the call site, such as a
  * plugin inside a host application that owns the device heap).  Same result
@@ -171,6 +232,10 @@ int pysift_match_u8_exact(const uint8_t* d1, int32_t n1, const uint8_t* d2, int3
 #define PYSIFT_ZOOM2X_NOALLOC_MAX_PIXELS (1 << 20)
 int pysift_zoom2x_u8_noalloc(const uint8_t* gray, int32_t H, int32_t W, int64_t pitch_bytes, int32_t fp16_round,
                              float* out, int32_t out_pitch, pysift_stream_t stream);
+
+/* Number of kernel launches the library has issued in this process
+ * (monotonic, all threads and devices). */
+int64_t pysift_launch_count(void);
 
 const char* pysift_last_error(void);
 const char* pysift_b200_version(void);

@@ -7,4 +7,4 @@ here="$(cd "$(dirname "$0")" && pwd)"
 mkdir -p "$here/_build"
 gcc -O2 -std=c11 -fPIC -shared -fopenmp -ffp-contract=off -fno-fast-math \
     -fvisibility=hidden -o "$here/_build/liboracle.so" \
-    "$here/sift_oracle.c" -lm
+    "$here/sift_oracle.c" "$here/stitch_oracle.c" -lm

@@ -16,15 +16,22 @@ import numpy as np
 
 
 def _top2(keys, larger_is_better):
-    """Per-row (best idx, best key, second key) with lower-index ties."""
+    """Per-row (best idx, best key, second key) with lower-index ties:
+    np.argmax/argmin return the first extremum, and the second key is the
+    extremum of the row with the winner masked out."""
     n, m = keys.shape
-    k = keys if larger_is_better else -keys
-    # stable ordering: sort by (-key, index)
-    order = np.lexsort((np.broadcast_to(np.arange(m), keys.shape), -k), axis=1)
-    b1 = order[:, 0]
     rows = np.arange(n)
+    b1 = np.argmax(keys, axis=1) if larger_is_better else np.argmin(keys, axis=1)
     k1 = keys[rows, b1]
-    k2 = keys[rows, order[:, 1]] if m > 1 else np.full(n, np.nan)
+    if m < 2:
+        return b1, k1, np.full(n, np.nan)
+    masked = keys.copy()
+    if np.issubdtype(keys.dtype, np.floating):
+        masked[rows, b1] = -np.inf if larger_is_better else np.inf
+    else:
+        info = np.iinfo(keys.dtype)
+        masked[rows, b1] = info.min if larger_is_better else info.max
+    k2 = masked.max(axis=1) if larger_is_better else masked.min(axis=1)
     return b1, k1, k2
 
 

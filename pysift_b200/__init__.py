@@ -9,5 +9,6 @@ include/pysift_b200.h.
 __version__ = "0.1.0"
 
 from .core import PySIFT  # noqa: E402
+from .stitch import GPUPyStitch  # noqa: E402
 
-__all__ = ["PySIFT"]
+__all__ = ["PySIFT", "GPUPyStitch"]

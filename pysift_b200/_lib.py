@@ -74,6 +74,7 @@ EXPORTS = {
     # name: (restype, argtypes)
     "pysift_last_error": (ctypes.c_char_p, []),
     "pysift_b200_version": (ctypes.c_char_p, []),
+    "pysift_launch_count": (c_int64, []),
     "pysift_detect_config_size": (c_size_t, []),
     "pysift_detect_workspace_size": (ctypes.c_int, [c_void_p, c_int32, c_int32, ctypes.POINTER(c_size_t)]),
     "pysift_detect_max_keypoints": (c_int32, [c_void_p]),
@@ -133,3 +134,26 @@ def check(rc, what):
         if rc == ERR_INVALID_ARG:
             raise ValueError(f"{what}: {msg}")
         raise PySiftError(f"{what} failed ({rc}): {msg}")
+
+EXPORTS.update({
+    "pysift_bgr2gray": (ctypes.c_int, [c_void_p, c_int32, c_int32, c_int64, c_void_p, c_int32, c_void_p]),
+    "pysift_clahe_lut_bytes": (ctypes.c_int, [c_int32, c_int32, ctypes.POINTER(c_size_t)]),
+    "pysift_clahe": (ctypes.c_int, [c_void_p, c_int32, c_int32, c_int32, c_double, c_int32, c_int32, c_void_p,
+                                    c_void_p, c_int32, c_void_p]),
+    "pysift_topk_by_response": (ctypes.c_int, [c_void_p, c_int32, c_int32, c_void_p, c_void_p, c_void_p]),
+    "pysift_gather_points": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_void_p, c_void_p]),
+    "pysift_l2_normalize_rows": (ctypes.c_int, [c_void_p, c_int32, c_int32, c_void_p, c_void_p]),
+    "pysift_pca_stats": (ctypes.c_int, [c_void_p, c_int32, c_int32, c_void_p, c_void_p, c_void_p]),
+    "pysift_pca_project_f16": (ctypes.c_int, [c_void_p, c_int32, c_int32, c_void_p, c_void_p, c_int32, c_void_p,
+                                              c_void_p]),
+    "pysift_to_f16": (ctypes.c_int, [c_void_p, c_int64, c_void_p, c_void_p]),
+    "pysift_mt19937_u32": (None, [ctypes.c_uint32, c_void_p, c_int64]),
+    "pysift_ransac_workspace_size": (ctypes.c_int, [c_int32, c_int32, ctypes.POINTER(c_size_t)]),
+    "pysift_ransac": (ctypes.c_int, [c_void_p, c_void_p, c_int32, c_void_p, c_int32, c_double, c_double, c_int32,
+                                     c_int32, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "pysift_dlt_homography": (ctypes.c_int, [c_void_p, c_void_p, c_int32, c_void_p, c_void_p, c_void_p]),
+    "pysift_warp_feather": (ctypes.c_int, [c_void_p, c_int32, c_int32, c_int32, c_void_p, c_int32, c_int32, c_int32,
+                                           c_int32, c_int32, c_void_p, c_float, c_float, c_int32, c_int32, c_int32,
+                                           c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                           c_void_p, c_void_p]),
+})

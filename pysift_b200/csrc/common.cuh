@@ -33,8 +33,13 @@ void set_error(const char* fmt, ...);
         }                                                                                  \
     } while (0)
 
+// Every kernel launch of the library is followed by exactly one
+// PYSIFT_LAUNCH_CHECK, which also counts it (pysift_launch_count()).
+void count_launch();
+
 #define PYSIFT_LAUNCH_CHECK(name)                                                          \
     do {                                                                                   \
+        ::pysift::count_launch();                                                          \
         cudaError_t e_ = cudaGetLastError();                                               \
         if (e_ != cudaSuccess) {                                                           \
             ::pysift::set_error("launch of %s failed: %s", name, cudaGetErrorString(e_));  \

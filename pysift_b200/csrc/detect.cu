@@ -24,6 +24,7 @@
 //                        output row (pysift/core.py:693-997, 1870-1873)
 #include <cstdarg>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 
 #include "common.cuh"
@@ -32,6 +33,9 @@
 namespace pysift {
 
 static thread_local std::string g_last_error;
+static std::atomic<long long> g_launches{0};
+
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 void set_error(const char* fmt, ...) {
     char buf[512];
@@ -1831,6 +1835,8 @@ const char* pysift_last_error(void) { return g_last_error.c_str(); }
 const char* pysift_b200_version(void) { return "pysift_b200 0.1.0 (sm_100a)"; }
 
 size_t pysift_detect_config_size(void) { return sizeof(pysift_detect_config); }
+
+int64_t pysift_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
 int pysift_detect_workspace_size(const pysift_detect_config* cfg, int32_t H, int32_t W, size_t* bytes) {
     int rc = validate_cfg(cfg);

@@ -384,10 +384,12 @@ static int run_match(int mode, const uint16_t* a, int n1, const uint16_t* b, int
     const int ntb = ceil_div(n2, NT), nta = ceil_div(n1, MT);
     if (mode == SIM_F16) {
         k_match_merge<SIM_F16><<<ceil_div(n1, 256), 256, 0, st>>>(ta.row_part, n1, ntb, ratio_sq, fbest, fpass, fdist);
+        PYSIFT_LAUNCH_CHECK("k_match_merge");
         k_match_merge<SIM_F16><<<ceil_div(n2, 256), 256, 0, st>>>(ta.col_part, n2, nta, ratio_sq, bbest, bpass, bdist);
     } else {
         k_match_merge<DIST_BF16><<<ceil_div(n1, 256), 256, 0, st>>>(ta.row_part, n1, ntb, ratio_sq, fbest, fpass,
                                                                     fdist);
+        PYSIFT_LAUNCH_CHECK("k_match_merge");
         k_match_merge<DIST_BF16><<<ceil_div(n2, 256), 256, 0, st>>>(ta.col_part, n2, nta, ratio_sq, bbest, bpass,
                                                                     bdist);
     }
@@ -444,6 +446,7 @@ int pysift_match_u8_exact(const uint8_t* d1, int32_t n1, const uint8_t* d2, int3
     uint16_t* bfa = wsp<uint16_t>(workspace, l.off_bfa);
     uint16_t* bfb = wsp<uint16_t>(workspace, l.off_bfb);
     k_row_norms_u8<<<ceil_div(n1, 8), dim3(32, 8), 0, st>>>(d1, n1, D, wsp<int>(workspace, l.off_na), bfa);
+    PYSIFT_LAUNCH_CHECK("k_row_norms_u8");
     k_row_norms_u8<<<ceil_div(n2, 8), dim3(32, 8), 0, st>>>(d2, n2, D, wsp<int>(workspace, l.off_nb), bfb);
     PYSIFT_LAUNCH_CHECK("k_row_norms_u8");
     const float ratio_sq = (float)((double)ratio * (double)ratio);

@@ -1,0 +1,686 @@
+// ransac.cu -- batched RANSAC / MAGSAC++ scoring with LO refits, all on the GPU,
+// and the descriptor preparation of the stitch matcher.
+//
+// Reference: GPUPyStitch._ransac / _ransac_batch_eval / _compute_homography /
+// _normalize_points (pysift/core.py:2272-2313, 2946-2981, 3011-3097) and
+// _match_features / _pca_compress (pysift/core.py:2703-2743, 2877-2888).
+//
+// Canonical arithmetic (the CPU oracle implements the same definition):
+//   * sums over points use a fixed order: contiguous chunks per thread,
+//     sequential inside a chunk, then a pairwise tree over the partials;
+//   * a hypothesis' null vector is found by Gaussian elimination with partial
+//     pivoting on its 8x9 system (the reference takes the last right singular
+//     vector of a batched SVD); degenerate samples get score -inf;
+//   * the least-squares refit takes the eigenvector of A^T A for the smallest
+//     eigenvalue by cyclic Jacobi (15 sweeps) instead of the SVD of A;
+//   * T2^-1 is formed analytically, H^-1 by the adjugate; 3x3 products sum
+//     k = 0, 1, 2 in order; exp is computed by ransac_exp (below);
+//   * RANSAC samples are the reference's: torch.randint on a CPU generator
+//     seeded 42 draws raw 32-bit MT19937 outputs r and returns r % N, so the
+//     caller passes the raw stream and the kernel reduces it modulo N.
+#include <cstdint>
+#include <cstring>
+
+#include "common.cuh"
+
+namespace pysift {
+
+constexpr int RT = 256;  // threads of the single-CTA kernels
+
+// exp(x), x <= 0, float64: Cody-Waite reduction with ln2 split in a 32-bit
+// head and a tail, Taylor series of exp(r) to degree 13, exact 2^n scaling.
+__device__ __forceinline__ double ransac_exp(double x) {
+    if (x < -745.0) return 0.0;
+    const double LOG2E = 1.4426950408889634;
+    const double LN2_HI = 0x1.62e42ffp-1;
+    const double LN2_LO = -0x1.718432a1b0e26p-35;
+    const double n = rint(x * LOG2E);
+    double r = fma(-n, LN2_HI, x);
+    r = fma(-n, LN2_LO, r);
+    double p = 1.0 / 6227020800.0;  // 1/13!
+    p = fma(p, r, 1.0 / 479001600.0);
+    p = fma(p, r, 1.0 / 39916800.0);
+    p = fma(p, r, 1.0 / 3628800.0);
+    p = fma(p, r, 1.0 / 362880.0);
+    p = fma(p, r, 1.0 / 40320.0);
+    p = fma(p, r, 1.0 / 5040.0);
+    p = fma(p, r, 1.0 / 720.0);
+    p = fma(p, r, 1.0 / 120.0);
+    p = fma(p, r, 1.0 / 24.0);
+    p = fma(p, r, 1.0 / 6.0);
+    p = fma(p, r, 0.5);
+    p = fma(p, r, 1.0);
+    p = fma(p, r, 1.0);
+    const int ni = (int)n;
+    if (ni >= -1022) return p * __longlong_as_double((long long)(ni + 1023) << 52);
+    return (p * __longlong_as_double((long long)(ni + 600 + 1023) << 52)) *
+           __longlong_as_double((long long)(1023 - 600) << 52);
+}
+
+// Fixed-order block sum of per-thread partials (RT threads): pairwise tree.
+__device__ double block_tree_sum(double v, double* sh) {
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (int s = RT / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) sh[threadIdx.x] = sh[threadIdx.x] + sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    const double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+struct Norm {
+    double s, cx, cy;
+};
+
+// Hartley normalisation of the points listed in idx (or 0..n-1), pysift/core.py:2946-2957:
+// c = mean, md = mean |p - c|, s = sqrt(2) / (md + 1e-10).
+__device__ Norm hartley(const double* pts, const int* idx, int n, double* sh) {
+    const int chunk = (n + RT - 1) / RT;
+    const int b = threadIdx.x * chunk, e = min(n, b + chunk);
+    double sx = 0.0, sy = 0.0;
+    for (int i = b; i < e; ++i) {
+        const int k = idx ? idx[i] : i;
+        sx = sx + pts[2 * k];
+        sy = sy + pts[2 * k + 1];
+    }
+    const double tx = block_tree_sum(sx, sh), ty = block_tree_sum(sy, sh);
+    Norm r;
+    r.cx = tx / (double)n;
+    r.cy = ty / (double)n;
+    double sd = 0.0;
+    for (int i = b; i < e; ++i) {
+        const int k = idx ? idx[i] : i;
+        const double dx = pts[2 * k] - r.cx, dy = pts[2 * k + 1] - r.cy;
+        sd = sd + sqrt(dx * dx + dy * dy);
+    }
+    const double md = block_tree_sum(sd, sh) / (double)n;
+    r.s = sqrt(2.0) / (md + 1e-10);
+    return r;
+}
+
+__device__ __forceinline__ void mat3_mul(const double* A, const double* B, double* C) {
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) C[3 * i + j] = (A[3 * i] * B[j] + A[3 * i + 1] * B[3 + j]) + A[3 * i + 2] * B[6 + j];
+}
+
+__device__ __forceinline__ void norm_mats(const Norm& n1, const Norm& n2, double* T1, double* T2inv) {
+    T1[0] = n1.s; T1[1] = 0.0; T1[2] = -n1.s * n1.cx;
+    T1[3] = 0.0; T1[4] = n1.s; T1[5] = -n1.s * n1.cy;
+    T1[6] = 0.0; T1[7] = 0.0; T1[8] = 1.0;
+    T2inv[0] = 1.0 / n2.s; T2inv[1] = 0.0; T2inv[2] = n2.cx;
+    T2inv[3] = 0.0; T2inv[4] = 1.0 / n2.s; T2inv[5] = n2.cy;
+    T2inv[6] = 0.0; T2inv[7] = 0.0; T2inv[8] = 1.0;
+}
+
+// Normalised coordinate: (s*x + 0*y) + (-s*c)
+__device__ __forceinline__ double nrm(double s, double c, double v) { return s * v + (-s * c); }
+
+// H = T2inv * Hn * T1, divided by H[2][2] when |H[2][2]| > 1e-10 (pysift/core.py:2290-2293)
+__device__ __forceinline__ void denormalise(const double* Hn, const double* T1, const double* T2inv, double* H) {
+    double t[9];
+    mat3_mul(T2inv, Hn, t);
+    mat3_mul(t, T1, H);
+    const double s = H[8];
+    const double ss = fabs(s) > 1e-10 ? s : 1.0;
+    for (int i = 0; i < 9; ++i) H[i] = H[i] / ss;
+}
+
+// Adjugate inverse with the reference's determinant guard (pysift/core.py:2298-2307).
+__device__ __forceinline__ void inv3_guarded(const double* a, double* inv, double guard) {
+    const double det = a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) +
+                       a[2] * (a[3] * a[7] - a[4] * a[6]);
+    const double d = (guard > 0.0 && !(fabs(det) > guard)) ? 1.0 : det;
+    inv[0] = (a[4] * a[8] - a[5] * a[7]) / d;
+    inv[1] = (a[2] * a[7] - a[1] * a[8]) / d;
+    inv[2] = (a[1] * a[5] - a[2] * a[4]) / d;
+    inv[3] = (a[5] * a[6] - a[3] * a[8]) / d;
+    inv[4] = (a[0] * a[8] - a[2] * a[6]) / d;
+    inv[5] = (a[2] * a[3] - a[0] * a[5]) / d;
+    inv[6] = (a[3] * a[7] - a[4] * a[6]) / d;
+    inv[7] = (a[1] * a[6] - a[0] * a[7]) / d;
+    inv[8] = (a[0] * a[4] - a[1] * a[3]) / d;
+}
+
+// Symmetric transfer error of one correspondence.  clamp: the batched
+// evaluation clamps the projective denominator at 1e-10
+// (pysift/core.py:2295, 2309); the LO reclassification divides plainly
+// (pysift/core.py:3079-3083).
+__device__ __forceinline__ double sym_err(const double* H, const double* Hi, double x1, double y1, double x2, double y2,
+                                          bool clamp) {
+    double fx = (H[0] * x1 + H[1] * y1) + H[2];
+    double fy = (H[3] * x1 + H[4] * y1) + H[5];
+    double fw = (H[6] * x1 + H[7] * y1) + H[8];
+    if (clamp) fw = fw < 1e-10 ? 1e-10 : fw;
+    const double ex = fx / fw - x2, ey = fy / fw - y2;
+    double bx = (Hi[0] * x2 + Hi[1] * y2) + Hi[2];
+    double by = (Hi[3] * x2 + Hi[4] * y2) + Hi[5];
+    double bw = (Hi[6] * x2 + Hi[7] * y2) + Hi[8];
+    if (clamp) bw = bw < 1e-10 ? 1e-10 : bw;
+    const double gx = bx / bw - x1, gy = by / bw - y1;
+    return (ex * ex + ey * ey) + (gx * gx + gy * gy);
+}
+
+// Null vector of the 8x9 DLT system of 4 normalised correspondences by
+// Gaussian elimination with partial pivoting; false if rank < 8.
+__device__ bool null_vector_8x9(const double* x1, const double* y1, const double* x2, const double* y2, double* h) {
+    double A[8][9];
+    for (int k = 0; k < 4; ++k) {
+        double* e = A[2 * k];
+        double* o = A[2 * k + 1];
+        e[0] = -x1[k]; e[1] = -y1[k]; e[2] = -1.0; e[3] = 0.0; e[4] = 0.0; e[5] = 0.0;
+        e[6] = x2[k] * x1[k]; e[7] = x2[k] * y1[k]; e[8] = x2[k];
+        o[0] = 0.0; o[1] = 0.0; o[2] = 0.0; o[3] = -x1[k]; o[4] = -y1[k]; o[5] = -1.0;
+        o[6] = y2[k] * x1[k]; o[7] = y2[k] * y1[k]; o[8] = y2[k];
+    }
+    for (int c = 0; c < 8; ++c) {
+        int piv = c;
+        double best = fabs(A[c][c]);
+        for (int r = c + 1; r < 8; ++r) {
+            const double v = fabs(A[r][c]);
+            if (v > best) {
+                best = v;
+                piv = r;
+            }
+        }
+        if (!(best > 1e-12)) return false;
+        if (piv != c)
+            for (int j = 0; j < 9; ++j) {
+                const double t = A[c][j];
+                A[c][j] = A[piv][j];
+                A[piv][j] = t;
+            }
+        for (int r = c + 1; r < 8; ++r) {
+            const double f = A[r][c] / A[c][c];
+            for (int j = c; j < 9; ++j) A[r][j] = A[r][j] - f * A[c][j];
+        }
+    }
+    h[8] = 1.0;
+    for (int c = 7; c >= 0; --c) {
+        double s = A[c][8];
+        for (int j = c + 1; j < 8; ++j) s = s + A[c][j] * h[j];
+        h[c] = -s / A[c][c];
+    }
+    return true;
+}
+
+struct RansacArgs {
+    const double* p1;  // n x 2
+    const double* p2;
+    int n, n_hyp;
+    const uint32_t* rnd;  // 4 * n_hyp raw MT19937 outputs
+    double tq, two_sig2;
+    int magsac, min_inliers;
+    double* prep;     // [T1(9), T2inv(9), n1(3), n2(3)]
+    double* p1n;      // n x 2 normalised
+    double* p2n;
+    double* hyp_H;    // n_hyp x 9
+    double* score;    // n_hyp
+    int* idx;         // n scratch indices
+    uint8_t* mask;    // n output
+    double* H_out;    // 9
+    int* info;        // [n_inliers, best_i, stage]
+};
+
+__global__ void __launch_bounds__(RT) k_ransac_prep(const RansacArgs a) {
+    __shared__ double sh[RT];
+    const Norm n1 = hartley(a.p1, nullptr, a.n, sh);
+    const Norm n2 = hartley(a.p2, nullptr, a.n, sh);
+    for (int i = threadIdx.x; i < a.n; i += RT) {
+        a.p1n[2 * i] = nrm(n1.s, n1.cx, a.p1[2 * i]);
+        a.p1n[2 * i + 1] = nrm(n1.s, n1.cy, a.p1[2 * i + 1]);
+        a.p2n[2 * i] = nrm(n2.s, n2.cx, a.p2[2 * i]);
+        a.p2n[2 * i + 1] = nrm(n2.s, n2.cy, a.p2[2 * i + 1]);
+    }
+    if (threadIdx.x == 0) {
+        norm_mats(n1, n2, a.prep, a.prep + 9);
+        a.prep[18] = n1.s; a.prep[19] = n1.cx; a.prep[20] = n1.cy;
+        a.prep[21] = n2.s; a.prep[22] = n2.cx; a.prep[23] = n2.cy;
+    }
+}
+
+// One warp per hypothesis: solve, denormalise, score all points
+// (lane-strided partial sums, then the warp tree 16, 8, 4, 2, 1).
+__global__ void __launch_bounds__(256) k_ransac_hyp(const RansacArgs a) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (warp >= a.n_hyp) return;
+    double x1[4], y1[4], x2[4], y2[4];
+    for (int k = 0; k < 4; ++k) {
+        const int i = (int)(a.rnd[4 * warp + k] % (uint32_t)a.n);
+        x1[k] = a.p1n[2 * i];
+        y1[k] = a.p1n[2 * i + 1];
+        x2[k] = a.p2n[2 * i];
+        y2[k] = a.p2n[2 * i + 1];
+    }
+    double hn[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, H[9], Hi[9];
+    const bool ok = null_vector_8x9(x1, y1, x2, y2, hn);
+    if (!ok)
+        for (int k = 0; k < 9; ++k) hn[k] = 0.0;
+    denormalise(hn, a.prep, a.prep + 9, H);
+    inv3_guarded(H, Hi, 1e-12);
+    double part = 0.0;
+    if (ok) {
+        for (int i = lane; i < a.n; i += 32) {
+            const double e = sym_err(H, Hi, a.p1[2 * i], a.p1[2 * i + 1], a.p2[2 * i], a.p2[2 * i + 1], true);
+            if (a.magsac)
+                part = part + ransac_exp(-e / a.two_sig2);
+            else
+                part = part + (e < a.tq ? 1.0 : 0.0);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) part = part + __shfl_down_sync(FULL_MASK, part, o);
+    if (lane == 0) {
+        a.score[warp] = ok ? part : -INFINITY;
+        for (int k = 0; k < 9; ++k) a.hyp_H[9 * warp + k] = H[k];
+    }
+}
+
+// Least-squares homography of the points idx[0..m): Hartley normalisation of
+// the subset, A^T A accumulated in a fixed order, cyclic Jacobi, the
+// eigenvector of the smallest eigenvalue, denormalised (pysift/core.py:2959-2981).
+__device__ void dlt_refit(const double* p1, const double* p2, const int* idx, int m, double* H, double* sh,
+                          double* s_M) {
+    const Norm n1 = hartley(p1, idx, m, sh);
+    const Norm n2 = hartley(p2, idx, m, sh);
+    double acc[45];
+    for (int k = 0; k < 45; ++k) acc[k] = 0.0;
+    const int chunk = (m + RT - 1) / RT;
+    const int b = threadIdx.x * chunk, e = min(m, b + chunk);
+    for (int i = b; i < e; ++i) {
+        const int k = idx[i];
+        const double x1 = nrm(n1.s, n1.cx, p1[2 * k]), y1 = nrm(n1.s, n1.cy, p1[2 * k + 1]);
+        const double x2 = nrm(n2.s, n2.cx, p2[2 * k]), y2 = nrm(n2.s, n2.cy, p2[2 * k + 1]);
+        const double re[9] = {-x1, -y1, -1.0, 0.0, 0.0, 0.0, x2 * x1, x2 * y1, x2};
+        const double ro[9] = {0.0, 0.0, 0.0, -x1, -y1, -1.0, y2 * x1, y2 * y1, y2};
+        int t = 0;
+        for (int r = 0; r < 9; ++r)
+            for (int c = r; c < 9; ++c, ++t) acc[t] = (acc[t] + re[r] * re[c]) + ro[r] * ro[c];
+    }
+    for (int t = 0; t < 45; ++t) {
+        const double v = block_tree_sum(acc[t], sh);
+        if (threadIdx.x == 0) s_M[t] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double M[9][9], V[9][9];
+        int t = 0;
+        for (int r = 0; r < 9; ++r)
+            for (int c = r; c < 9; ++c, ++t) M[r][c] = M[c][r] = s_M[t];
+        for (int r = 0; r < 9; ++r)
+            for (int c = 0; c < 9; ++c) V[r][c] = (r == c) ? 1.0 : 0.0;
+        for (int sweep = 0; sweep < 15; ++sweep)
+            for (int p = 0; p < 8; ++p)
+                for (int q = p + 1; q < 9; ++q) {
+                    const double apq = M[p][q];
+                    if (apq == 0.0) continue;
+                    const double theta = (M[q][q] - M[p][p]) / (2.0 * apq);
+                    const double tt = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                    const double c = 1.0 / sqrt(tt * tt + 1.0), s = tt * c;
+                    for (int k = 0; k < 9; ++k) {
+                        const double mkp = M[k][p], mkq = M[k][q];
+                        M[k][p] = c * mkp - s * mkq;
+                        M[k][q] = s * mkp + c * mkq;
+                    }
+                    for (int k = 0; k < 9; ++k) {
+                        const double mpk = M[p][k], mqk = M[q][k];
+                        M[p][k] = c * mpk - s * mqk;
+                        M[q][k] = s * mpk + c * mqk;
+                    }
+                    for (int k = 0; k < 9; ++k) {
+                        const double vkp = V[k][p], vkq = V[k][q];
+                        V[k][p] = c * vkp - s * vkq;
+                        V[k][q] = s * vkp + c * vkq;
+                    }
+                }
+        int best = 0;
+        for (int k = 1; k < 9; ++k)
+            if (M[k][k] < M[best][best]) best = k;
+        double hn[9], T1[9], T2inv[9];
+        for (int k = 0; k < 9; ++k) hn[k] = V[k][best];
+        norm_mats(n1, n2, T1, T2inv);
+        double t9[9];
+        mat3_mul(T2inv, hn, t9);
+        mat3_mul(t9, T1, H);
+        const double s = H[8];
+        for (int k = 0; k < 9; ++k) H[k] = H[k] / s;
+    }
+    __syncthreads();
+}
+
+// Compacts flags[0..n) into idx (in order); returns the count (all threads).
+__device__ int compact_mask(const uint8_t* flags, int n, int* idx, int* shi) {
+    int base = 0;
+    for (int c0 = 0; c0 < n; c0 += RT) {
+        const int i = c0 + threadIdx.x;
+        const int f = (i < n && flags[i]) ? 1 : 0;
+        int tot;
+        const int pos = base + block_excl_scan(f, &tot, shi);
+        if (f) idx[pos] = i;
+        base += tot;
+    }
+    return base;
+}
+
+// Best hypothesis (first maximum), its inlier set, LO refits (pysift/core.py:3060-3092).
+__global__ void __launch_bounds__(RT) k_ransac_select(const RansacArgs a) {
+    __shared__ double sh[RT];
+    __shared__ int shi[33];
+    __shared__ double s_M[45];
+    __shared__ double s_H[9], s_Hi[9], s_H1[9];
+    __shared__ int s_best;
+    __shared__ double s_bscore[RT];
+    __shared__ int s_bidx[RT];
+    // argmax, lowest index on ties
+    double bs = -INFINITY;
+    int bi = 0x7fffffff;
+    for (int h = threadIdx.x; h < a.n_hyp; h += RT) {
+        const double v = a.score[h];
+        if (v > bs || (v == bs && h < bi)) {
+            bs = v;
+            bi = h;
+        }
+    }
+    s_bscore[threadIdx.x] = bs;
+    s_bidx[threadIdx.x] = bi;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double B = s_bscore[0];
+        int I = s_bidx[0];
+        for (int t = 1; t < RT; ++t)
+            if (s_bscore[t] > B || (s_bscore[t] == B && s_bidx[t] < I)) {
+                B = s_bscore[t];
+                I = s_bidx[t];
+            }
+        s_best = (I == 0x7fffffff) ? 0 : I;
+        for (int k = 0; k < 9; ++k) s_H[k] = a.hyp_H[9 * s_best + k];
+        inv3_guarded(s_H, s_Hi, 1e-12);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < a.n; i += RT)
+        a.mask[i] = sym_err(s_H, s_Hi, a.p1[2 * i], a.p1[2 * i + 1], a.p2[2 * i], a.p2[2 * i + 1], true) < a.tq;
+    __syncthreads();
+    const int nb = compact_mask(a.mask, a.n, a.idx, shi);
+    int stage = 0, n_final = nb;
+    if (nb >= a.min_inliers) {
+        dlt_refit(a.p1, a.p2, a.idx, nb, s_H1, sh, s_M);
+        if (threadIdx.x == 0) inv3_guarded(s_H1, s_Hi, 0.0);
+        __syncthreads();
+        // reclassify with H1 into idx via a second flag pass (mask keeps the hypothesis set for now)
+        int base = 0;
+        for (int c0 = 0; c0 < a.n; c0 += RT) {
+            const int i = c0 + threadIdx.x;
+            int f = 0;
+            if (i < a.n) f = sym_err(s_H1, s_Hi, a.p1[2 * i], a.p1[2 * i + 1], a.p2[2 * i], a.p2[2 * i + 1], false) < a.tq;
+            int tot;
+            const int pos = base + block_excl_scan(f, &tot, shi);
+            if (f) a.idx[pos] = i;
+            base += tot;
+        }
+        const int n2 = base;
+        if (n2 >= a.min_inliers) {
+            dlt_refit(a.p1, a.p2, a.idx, n2, s_H, sh, s_M);
+            // mask = reclassified set
+            for (int i = threadIdx.x; i < a.n; i += RT) a.mask[i] = 0;
+            __syncthreads();
+            for (int k = threadIdx.x; k < n2; k += RT) a.mask[a.idx[k]] = 1;
+            stage = 2;
+            n_final = n2;
+        } else {
+            if (threadIdx.x < 9) s_H[threadIdx.x] = s_H1[threadIdx.x];
+            stage = 1;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < 9) a.H_out[threadIdx.x] = s_H[threadIdx.x];
+    if (threadIdx.x == 0) {
+        a.info[0] = n_final;
+        a.info[1] = s_best;
+        a.info[2] = stage;
+    }
+}
+
+// Plain DLT on all points (the reference's preliminary estimate, core.py:3753).
+__global__ void __launch_bounds__(RT) k_dlt_all(const double* p1, const double* p2, int n, int* idx, double* H_out) {
+    __shared__ double sh[RT];
+    __shared__ double s_M[45];
+    __shared__ double s_H[9];
+    for (int i = threadIdx.x; i < n; i += RT) idx[i] = i;
+    __syncthreads();
+    dlt_refit(p1, p2, idx, n, s_H, sh, s_M);
+    if (threadIdx.x < 9) H_out[threadIdx.x] = s_H[threadIdx.x];
+}
+
+// ---------------------------------------------------------------------------
+// Descriptor preparation for the stitch matcher (pysift/core.py:2877-2888,
+// 2703-2743): L2-normalise (+1e-7), optional PCA projection, L2-normalise,
+// round to fp16.  Norms sum squares in groups of 32 dimensions (warp tree
+// 16, 8, 4, 2, 1) and the groups in order; the projection is a fmaf chain
+// over k ascending of (d_k - mean_k) * proj[k][c].
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float warp_tree(float v) {
+    v += __shfl_down_sync(FULL_MASK, v, 16);
+    v += __shfl_down_sync(FULL_MASK, v, 8);
+    v += __shfl_down_sync(FULL_MASK, v, 4);
+    v += __shfl_down_sync(FULL_MASK, v, 2);
+    v += __shfl_down_sync(FULL_MASK, v, 1);
+    return __shfl_sync(FULL_MASK, v, 0);
+}
+
+// one warp per row; D <= 128 (D % 32 == 0)
+__global__ void k_l2_normalize(const float* __restrict__ in, int n, int D, float* __restrict__ out) {
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const float* r = in + (size_t)row * D;
+    float v[4];
+    float ss = 0.0f;
+    for (int g = 0; g < D / 32; ++g) {
+        v[g] = r[g * 32 + lane];
+        const float w = warp_tree(v[g] * v[g]);
+        ss = (g == 0) ? w : ss + w;
+    }
+    const float den = sqrtf(ss) + 1e-7f;
+    for (int g = 0; g < D / 32; ++g) out[(size_t)row * D + g * 32 + lane] = v[g] / den;
+}
+
+// one warp per row: project (D -> P), normalise, fp16
+__global__ void k_pca_project_f16(const float* __restrict__ in, int n, int D, const float* __restrict__ mean,
+                                  const float* __restrict__ proj, int P, uint16_t* __restrict__ out) {
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const float* r = in + (size_t)row * D;
+    float pv[4];
+    for (int g = 0; g < P / 32; ++g) {
+        const int c = g * 32 + lane;
+        float acc = 0.0f;
+        for (int k = 0; k < D; ++k) acc = fmaf(r[k] - mean[k], proj[(size_t)k * P + c], acc);
+        pv[g] = acc;
+    }
+    float ss = 0.0f;
+    for (int g = 0; g < P / 32; ++g) {
+        const float w = warp_tree(pv[g] * pv[g]);
+        ss = (g == 0) ? w : ss + w;
+    }
+    const float den = sqrtf(ss) + 1e-7f;
+    for (int g = 0; g < P / 32; ++g)
+        out[(size_t)row * P + g * 32 + lane] = __half_as_ushort(__float2half_rn(pv[g] / den));
+}
+
+__global__ void k_to_f16(const float* __restrict__ in, size_t n, uint16_t* __restrict__ out) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = __half_as_ushort(__float2half_rn(in[i]));
+}
+
+// PCA statistics of the stacked normalised sets: mean (float64 sequential sum
+// over rows / n, rounded to float32) and covariance (float64 sequential sum of
+// products of the float32 centred values / n).
+__global__ void k_pca_mean(const float* __restrict__ x, int n, int D, float* __restrict__ mean) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= D) return;
+    double s = 0.0;
+    for (int i = 0; i < n; ++i) s = s + (double)x[(size_t)i * D + k];
+    mean[k] = (float)(s / (double)n);
+}
+
+__global__ void k_pca_cov(const float* __restrict__ x, int n, int D, const float* __restrict__ mean,
+                          double* __restrict__ cov) {
+    const int k = blockIdx.y, l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= D || l < k) return;
+    double s = 0.0;
+    const float mk = mean[k], ml = mean[l];
+    for (int i = 0; i < n; ++i) {
+        const double a = (double)(x[(size_t)i * D + k] - mk), b = (double)(x[(size_t)i * D + l] - ml);
+        s = s + a * b;
+    }
+    const double v = s / (double)n;
+    cov[(size_t)k * D + l] = v;
+    cov[(size_t)l * D + k] = v;
+}
+
+struct RansacLayout {
+    size_t off_prep, off_p1n, off_p2n, off_hyp, off_score, off_idx, total;
+};
+
+static RansacLayout ransac_layout(int n, int n_hyp) {
+    RansacLayout l;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        size_t r = off;
+        off = align_up(off + bytes, 256);
+        return r;
+    };
+    l.off_prep = take(32 * sizeof(double));
+    l.off_p1n = take((size_t)n * 2 * sizeof(double));
+    l.off_p2n = take((size_t)n * 2 * sizeof(double));
+    l.off_hyp = take((size_t)n_hyp * 9 * sizeof(double));
+    l.off_score = take((size_t)n_hyp * sizeof(double));
+    l.off_idx = take((size_t)n * sizeof(int));
+    l.total = off;
+    return l;
+}
+
+}  // namespace pysift
+
+using namespace pysift;
+
+extern "C" {
+
+void pysift_mt19937_u32(uint32_t seed, uint32_t* out, int64_t n) {
+    uint32_t mt[624];
+    mt[0] = seed;
+    for (int i = 1; i < 624; ++i) mt[i] = 1812433253u * (mt[i - 1] ^ (mt[i - 1] >> 30)) + (uint32_t)i;
+    int idx = 624;
+    for (int64_t k = 0; k < n; ++k) {
+        if (idx >= 624) {
+            for (int i = 0; i < 624; ++i) {
+                const uint32_t y = (mt[i] & 0x80000000u) | (mt[(i + 1) % 624] & 0x7fffffffu);
+                mt[i] = mt[(i + 397) % 624] ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
+            }
+            idx = 0;
+        }
+        uint32_t y = mt[idx++];
+        y ^= y >> 11;
+        y ^= (y << 7) & 0x9d2c5680u;
+        y ^= (y << 15) & 0xefc60000u;
+        y ^= y >> 18;
+        out[k] = y;
+    }
+}
+
+int pysift_ransac_workspace_size(int32_t n, int32_t n_hyp, size_t* bytes) {
+    PYSIFT_CHECK_ARG(bytes && n >= 0 && n_hyp >= 1, "bad arguments");
+    *bytes = ransac_layout(n, n_hyp).total;
+    return PYSIFT_OK;
+}
+
+int pysift_ransac(const double* pts1, const double* pts2, int32_t n, const uint32_t* rand_u32, int32_t n_hyp,
+                  double inlier_thresh, double sigma_max, int32_t magsac, int32_t min_inliers, void* workspace,
+                  size_t workspace_bytes, double* H_out, uint8_t* mask_out, int32_t* info, pysift_stream_t stream) {
+    PYSIFT_CHECK_ARG(pts1 && pts2 && rand_u32 && workspace && H_out && mask_out && info, "NULL pointer argument");
+    PYSIFT_CHECK_ARG(n >= 4, "Need >= 4 correspondences, got %d", n);
+    PYSIFT_CHECK_ARG(n_hyp >= 1 && inlier_thresh > 0.0 && sigma_max > 0.0, "bad RANSAC parameters");
+    RansacLayout l = ransac_layout(n, n_hyp);
+    if (workspace_bytes < l.total) {
+        set_error("workspace %zu bytes < required %zu", workspace_bytes, l.total);
+        return PYSIFT_ERR_WORKSPACE;
+    }
+    RansacArgs a;
+    a.p1 = pts1;
+    a.p2 = pts2;
+    a.n = n;
+    a.n_hyp = n_hyp;
+    a.rnd = rand_u32;
+    a.tq = inlier_thresh * inlier_thresh;
+    a.two_sig2 = 2.0 * (sigma_max * sigma_max);
+    a.magsac = magsac;
+    a.min_inliers = min_inliers;
+    char* ws = static_cast<char*>(workspace);
+    a.prep = reinterpret_cast<double*>(ws + l.off_prep);
+    a.p1n = reinterpret_cast<double*>(ws + l.off_p1n);
+    a.p2n = reinterpret_cast<double*>(ws + l.off_p2n);
+    a.hyp_H = reinterpret_cast<double*>(ws + l.off_hyp);
+    a.score = reinterpret_cast<double*>(ws + l.off_score);
+    a.idx = reinterpret_cast<int*>(ws + l.off_idx);
+    a.mask = mask_out;
+    a.H_out = H_out;
+    a.info = info;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    k_ransac_prep<<<1, RT, 0, st>>>(a);
+    PYSIFT_LAUNCH_CHECK("k_ransac_prep");
+    k_ransac_hyp<<<ceil_div(n_hyp * 32, 256), 256, 0, st>>>(a);
+    PYSIFT_LAUNCH_CHECK("k_ransac_hyp");
+    k_ransac_select<<<1, RT, 0, st>>>(a);
+    PYSIFT_LAUNCH_CHECK("k_ransac_select");
+    return PYSIFT_OK;
+}
+
+int pysift_dlt_homography(const double* pts1, const double* pts2, int32_t n, int32_t* idx_scratch, double* H_out,
+                          pysift_stream_t stream) {
+    PYSIFT_CHECK_ARG(pts1 && pts2 && idx_scratch && H_out, "NULL pointer argument");
+    PYSIFT_CHECK_ARG(n >= 4, "Need >= 4 correspondences, got %d", n);
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    k_dlt_all<<<1, RT, 0, st>>>(pts1, pts2, n, idx_scratch, H_out);
+    PYSIFT_LAUNCH_CHECK("k_dlt_all");
+    return PYSIFT_OK;
+}
+
+int pysift_l2_normalize_rows(const float* in, int32_t n, int32_t D, float* out, pysift_stream_t stream) {
+    PYSIFT_CHECK_ARG(in && out && n >= 0 && D > 0 && D <= 128 && D % 32 == 0, "bad arguments");
+    if (n == 0) return PYSIFT_OK;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    k_l2_normalize<<<ceil_div(n * 32, 256), 256, 0, st>>>(in, n, D, out);
+    PYSIFT_LAUNCH_CHECK("k_l2_normalize");
+    return PYSIFT_OK;
+}
+
+int pysift_pca_stats(const float* x, int32_t n, int32_t D, float* mean, double* cov, pysift_stream_t stream) {
+    PYSIFT_CHECK_ARG(x && mean && cov && n >= 1 && D > 0 && D <= 1024, "bad arguments");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    k_pca_mean<<<ceil_div(D, 128), 128, 0, st>>>(x, n, D, mean);
+    PYSIFT_LAUNCH_CHECK("k_pca_mean");
+    k_pca_cov<<<dim3(ceil_div(D, 128), D), 128, 0, st>>>(x, n, D, mean, cov);
+    PYSIFT_LAUNCH_CHECK("k_pca_cov");
+    return PYSIFT_OK;
+}
+
+int pysift_pca_project_f16(const float* x, int32_t n, int32_t D, const float* mean, const float* proj, int32_t P,
+                           uint16_t* out, pysift_stream_t stream) {
+    PYSIFT_CHECK_ARG(x && mean && proj && out && n >= 0 && D > 0 && P > 0 && P <= 128 && P % 32 == 0,
+                     "bad arguments");
+    if (n == 0) return PYSIFT_OK;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    k_pca_project_f16<<<ceil_div(n * 32, 256), 256, 0, st>>>(x, n, D, mean, proj, P, out);
+    PYSIFT_LAUNCH_CHECK("k_pca_project_f16");
+    return PYSIFT_OK;
+}
+
+int pysift_to_f16(const float* in, int64_t n, uint16_t* out, pysift_stream_t stream) {
+    PYSIFT_CHECK_ARG(in && out && n >= 0, "bad arguments");
+    if (n == 0) return PYSIFT_OK;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    k_to_f16<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(in, (size_t)n, out);
+    PYSIFT_LAUNCH_CHECK("k_to_f16");
+    return PYSIFT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,362 @@
+"""GPUPyStitch drop-in (pysift/core.py:2401-4092) on the B200 kernels.
+
+The two-image path of the reference -- BGR->gray, CLAHE, SIFT, top-k by
+response, L2 + PCA-64 + fp16 mutual ratio-test matching, batched RANSAC with
+MAGSAC++ scoring and LO refits, canvas, bilinear warp -- runs as C-ABI calls
+on the current CUDA stream.  Composition: the reference's gain + DP seam +
+multiband blend is replaced by a linear feather blend (weights 1 + distance
+to each image's border) followed by the reference's inner-rectangle crop.
+The host reads back only the homography (72 bytes + 3 counters) to size the
+canvas, the coverage extents for the crop and the final panorama.
+"""
+import ctypes
+import os
+import time
+from datetime import datetime
+
+import numpy as np
+import torch
+
+from . import _lib
+from .core import PySIFT
+
+
+def _ptr_aligned(t, align=256):
+    off = (-t.data_ptr()) % align
+    return t.data_ptr() + off, t.numel() * t.element_size() - off
+
+
+class _Dev:
+    """Per-size device scratch reused across calls."""
+
+    def __init__(self):
+        self.bufs = {}
+
+    def get(self, key, shape, dtype, device):
+        t = self.bufs.get(key)
+        if t is None or tuple(t.shape) != tuple(shape) or t.dtype != dtype:
+            t = torch.empty(shape, dtype=dtype, device=device)
+            self.bufs[key] = t
+        return t
+
+
+class GPUPyStitch:
+    """Panorama stitcher with the reference's constructor (pysift/core.py:2429-2445).
+
+    Not thread-safe (per-instance buffers and the cached PCA basis, like the
+    reference).  Two images are supported; three-image stitching, depth-aware
+    warps, learned features and LightGlue raise NotImplementedError.
+    """
+
+    def __init__(self, n_depth_layers=4, n_blend_levels=6, ransac_iters=1500, inlier_thresh=5.0,
+                 ransac_method='magsac', sigma_max=None, match_ratio=0.75, match_batch=512, max_keypoints=8000,
+                 pca_dims=64, int8_matching=False, orientation='histogram', descriptor='sift', matcher='ratio',
+                 color_match='gain', dsp_sift=False, contrast_thresh=0.04, n_octaves=4, n_scales=3, sigma0=1.6,
+                 edge_thresh=10.0, double_image=True, max_dimension=0, denoise=False, sharpen=False,
+                 clahe_clip=2.0, clahe_tile=8, output_max_dim=0, post_sharpen=False, output_format='png',
+                 output_quality=90, *, device=None, save_output=True, verbose=True, high_vram=None):
+        if matcher != 'ratio':
+            raise NotImplementedError(f"matcher={matcher!r}: only the ratio-test matcher is implemented here")
+        if int8_matching:
+            raise NotImplementedError("int8_matching: not implemented on this backend (fp16 tensor-core matching)")
+        if pca_dims not in (0, 64, 128):
+            raise NotImplementedError("pca_dims must be 0, 64 or 128 on this backend")
+        if ransac_method not in ('magsac', 'classic'):
+            raise ValueError(f"ransac_method must be 'magsac' or 'classic' (got {ransac_method!r})")
+        self.n_depth_layers = n_depth_layers
+        self.n_blend_levels = n_blend_levels
+        self.ransac_iters = ransac_iters
+        self.inlier_thresh = inlier_thresh
+        self.ransac_method = ransac_method
+        self.sigma_max = sigma_max if sigma_max is not None else inlier_thresh
+        self.match_ratio = match_ratio
+        self.match_batch = match_batch
+        self.max_keypoints = max_keypoints
+        self.pca_dims = pca_dims
+        self.int8_matching = int8_matching
+        self.matcher = matcher
+        self.descriptor = descriptor
+        self.color_match = color_match
+        self.max_dimension = max_dimension
+        self.denoise = denoise
+        self.sharpen = sharpen
+        self.clahe_clip = clahe_clip
+        self.clahe_tile = clahe_tile
+        self.output_max_dim = output_max_dim
+        self.post_sharpen = post_sharpen
+        self.output_format = output_format.lower()
+        self.output_quality = output_quality
+        self.save_output = save_output
+        self.verbose = verbose
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self._detector = PySIFT(dsp=dsp_sift, orientation=orientation, descriptor=descriptor, n_octaves=n_octaves,
+                                n_scales=n_scales, sigma0=sigma0, contrast_thresh=contrast_thresh,
+                                edge_thresh=edge_thresh, double_image=double_image, device=self.device,
+                                high_vram=high_vram)
+        self._lib = _lib.load()
+        self._dev = _Dev()
+        self._pca_matrix = None   # float32 (128, pca_dims) on the device, fitted on the first pair
+        self._pca_mean = None
+        self._rand = {}
+        self.last_metrics = None
+        self.last_timings = None
+
+    # ------------------------------------------------------------------
+    def _stream(self):
+        return torch.cuda.current_stream(self.device).cuda_stream
+
+    def _upload_bgr(self, img, key):
+        if isinstance(img, torch.Tensor) and img.is_cuda:
+            return img.contiguous()
+        img = np.ascontiguousarray(img)
+        if img.dtype != np.uint8 or img.ndim != 3 or img.shape[2] != 3:
+            raise ValueError("images must be BGR uint8 arrays of shape (H, W, 3)")
+        host = self._dev.bufs.get(key + "_host")
+        if host is None or tuple(host.shape) != img.shape:
+            host = torch.empty(img.shape, dtype=torch.uint8).pin_memory()
+            self._dev.bufs[key + "_host"] = host
+        host.numpy()[...] = img
+        dev = self._dev.get(key, img.shape, torch.uint8, self.device)
+        dev.copy_(host, non_blocking=True)
+        return dev
+
+    def _gray_clahe(self, bgr, key):
+        """BGR -> gray -> CLAHE on the device (pysift/core.py:2545-2565)."""
+        H, W = bgr.shape[:2]
+        st = self._stream()
+        gray = self._dev.get(key + "_gray", (H, W), torch.uint8, self.device)
+        _lib.check(self._lib.pysift_bgr2gray(bgr.data_ptr(), H, W, bgr.stride(0), gray.data_ptr(), W, st),
+                   "pysift_bgr2gray")
+        if self.clahe_clip is None:
+            return gray
+        t = int(self.clahe_tile)
+        lut = self._dev.get(key + "_lut", (t * t * 256,), torch.uint8, self.device)
+        out = self._dev.get(key + "_clahe", (H, W), torch.uint8, self.device)
+        _lib.check(self._lib.pysift_clahe(gray.data_ptr(), H, W, W, float(self.clahe_clip), t, t, lut.data_ptr(),
+                                          out.data_ptr(), W, st), "pysift_clahe")
+        return out
+
+    def _features(self, bgr, key):
+        """Detect + describe, then keep the top max_keypoints by response
+        (stable, pysift/core.py:2566-2571).  Returns device (kpts (N,4), desc (N,128), N)."""
+        g = self._gray_clahe(bgr, key)
+        det = self._detector
+        b = det.run_device(g)
+        b.stats_host.copy_(b.stats, non_blocking=True)
+        torch.cuda.current_stream(self.device).synchronize()
+        n = int(b.stats_host[_lib.STAT_N_KEYPOINTS])
+        kp, desc, resp = b.kpts[:n], b.desc[:n], b.resp[:n]
+        if n > self.max_keypoints:
+            k = self.max_keypoints
+            rank = self._dev.get(key + "_rank", (n,), torch.int32, self.device)
+            idx = self._dev.get(key + "_topk", (k,), torch.int32, self.device)
+            _lib.check(self._lib.pysift_topk_by_response(resp.data_ptr(), n, k, rank.data_ptr(), idx.data_ptr(),
+                                                         self._stream()), "pysift_topk_by_response")
+            il = idx.long()
+            kp, desc = kp.index_select(0, il), desc.index_select(0, il)
+            n = k
+        else:
+            kp, desc = kp.clone(), desc.clone()
+        return kp, desc, n
+
+    def _prepare(self, d1, d2):
+        """L2-normalise, PCA (fitted once per instance), fp16 (pysift/core.py:2877-2888)."""
+        st = self._stream()
+        lib = self._lib
+        n1, n2 = d1.shape[0], d2.shape[0]
+        D = d1.shape[1]
+        both = torch.empty((n1 + n2, D), dtype=torch.float32, device=self.device)
+        _lib.check(lib.pysift_l2_normalize_rows(d1.data_ptr(), n1, D, both.data_ptr(), st), "l2")
+        _lib.check(lib.pysift_l2_normalize_rows(d2.data_ptr(), n2, D, both[n1:].data_ptr(), st), "l2")
+        P = self.pca_dims if (self.descriptor == 'sift' and 0 < self.pca_dims < D) else 0
+        if P == 0:
+            out = torch.empty((n1 + n2, D), dtype=torch.float16, device=self.device)
+            _lib.check(lib.pysift_to_f16(both.data_ptr(), both.numel(), out.data_ptr(), st), "to_f16")
+            return out[:n1], out[n1:], D
+        if self._pca_matrix is None:
+            mean = torch.empty(D, dtype=torch.float32, device=self.device)
+            cov = torch.empty((D, D), dtype=torch.float64, device=self.device)
+            _lib.check(lib.pysift_pca_stats(both.data_ptr(), n1 + n2, D, mean.data_ptr(), cov.data_ptr(), st),
+                       "pysift_pca_stats")
+            # one 128x128 symmetric eigendecomposition per instance (LAPACK),
+            # the basis cached like the reference's (pysift/core.py:2729-2736)
+            w, v = np.linalg.eigh(cov.cpu().numpy())
+            proj = np.ascontiguousarray(v[:, -P:].astype(np.float32))
+            self._pca_matrix = torch.from_numpy(proj).to(self.device)
+            self._pca_mean = mean
+        out = torch.empty((n1 + n2, P), dtype=torch.float16, device=self.device)
+        _lib.check(lib.pysift_pca_project_f16(both.data_ptr(), n1 + n2, D, self._pca_mean.data_ptr(),
+                                              self._pca_matrix.data_ptr(), P, out.data_ptr(), st),
+                   "pysift_pca_project_f16")
+        return out[:n1], out[n1:], P
+
+    def _match(self, d1, d2):
+        from . import match
+        a, b, D = self._prepare(d1, d2)
+        return match.match_fp16(a, b, self.match_ratio)
+
+    def _random_stream(self, n_hyp):
+        r = self._rand.get(n_hyp)
+        if r is None:
+            host = np.empty(4 * n_hyp, dtype=np.uint32)
+            self._lib.pysift_mt19937_u32(42, host.ctypes.data_as(ctypes.c_void_p), host.size)
+            r = torch.from_numpy(host).to(self.device)
+            self._rand[n_hyp] = r
+        return r
+
+    def _ransac(self, p1, p2, n):
+        st = self._stream()
+        n_hyp = int(self.ransac_iters)
+        sz = ctypes.c_size_t()
+        _lib.check(self._lib.pysift_ransac_workspace_size(n, n_hyp, ctypes.byref(sz)), "ransac ws")
+        ws = self._dev.get("ransac_ws", (int(sz.value) + 256,), torch.uint8, self.device)
+        wp, wn = _ptr_aligned(ws)
+        H = self._dev.get("ransac_H", (9,), torch.float64, self.device)
+        mask = self._dev.get("ransac_mask", (max(n, 1),), torch.uint8, self.device)
+        info = self._dev.get("ransac_info", (4,), torch.int32, self.device)
+        rnd = self._random_stream(n_hyp)
+        _lib.check(self._lib.pysift_ransac(p1.data_ptr(), p2.data_ptr(), n, rnd.data_ptr(), n_hyp,
+                                           float(self.inlier_thresh), float(self.sigma_max),
+                                           1 if self.ransac_method == 'magsac' else 0, 10, wp, wn, H.data_ptr(),
+                                           mask.data_ptr(), info.data_ptr(), st), "pysift_ransac")
+        return H, mask[:n], info
+
+    @staticmethod
+    def _compute_canvas_size(img1_shape, img2_shape, H):
+        """pysift/core.py:3171-3187 (float64, host)."""
+        h1, w1 = img1_shape[:2]
+        h2, w2 = img2_shape[:2]
+        c1 = np.array([[0, 0, 1], [w1, 0, 1], [w1, h1, 1], [0, h1, 1]], dtype=np.float64).T
+        wc = H @ c1
+        wc /= wc[2]
+        ax = np.concatenate([wc[0], [0, w2, w2, 0]])
+        ay = np.concatenate([wc[1], [0, 0, h2, h2]])
+        ox = max(0.0, -ax.min())
+        oy = max(0.0, -ay.min())
+        return int(np.ceil(ax.max() + ox)) + 1, int(np.ceil(ay.max() + oy)) + 1, ox, oy
+
+    def _compose(self, img1, img2, H, max_canvas_px=400_000_000):
+        hs, ws = img1.shape[:2]
+        h2, w2 = img2.shape[:2]
+        cw, ch, ox, oy = self._compute_canvas_size(img1.shape, img2.shape, H)
+        if cw * ch > max_canvas_px or cw <= 0 or ch <= 0:
+            raise RuntimeError(f"degenerate homography: canvas {cw}x{ch}")
+        hinv = np.linalg.inv(H).astype(np.float32).ravel()
+        iox, ioy = int(round(ox)), int(round(oy))
+        st = self._stream()
+        out = self._dev.get("pano", (ch, cw, 3), torch.uint8, self.device)
+        ext = self._dev.get("extents", (2 * ch + 2 * cw,), torch.int32, self.device)
+        hb = (ctypes.c_float * 9)(*[float(v) for v in hinv])
+        _lib.check(self._lib.pysift_warp_feather(img1.data_ptr(), hs, ws, img1.stride(0), img2.data_ptr(), h2, w2,
+                                                 img2.stride(0), cw, ch, ctypes.cast(hb, ctypes.c_void_p),
+                                                 float(np.float32(ox)), float(np.float32(oy)), iox, ioy, 1,
+                                                 out.data_ptr(), None, None, None, ext.data_ptr(),
+                                                 ext[ch:].data_ptr(), ext[2 * ch:].data_ptr(),
+                                                 ext[2 * ch + cw:].data_ptr(), st), "pysift_warp_feather")
+        e = ext.cpu().numpy()
+        row_lo, row_hi = e[:ch], e[ch:2 * ch]
+        col_lo, col_hi = e[2 * ch:2 * ch + cw], e[2 * ch + cw:]
+        r0, r1, c0, c1, ir0, ir1, ic0, ic1, degenerate = self._autocrop_box(row_lo, row_hi, col_lo, col_hi)
+        if r0 is None:
+            pano = out.cpu().numpy()
+        elif degenerate:
+            pano = out[r0:r1 + 1, c0:c1 + 1].cpu().numpy()
+        else:
+            pano = out[r0 + ir0:r0 + ir1 + 1, c0 + ic0:c0 + ic1 + 1].cpu().numpy()
+        covered = int(np.sum(np.maximum(row_hi - row_lo + 1, 0)))  # upper bound of coverage per row span
+        return pano, dict(canvas_w=cw, canvas_h=ch, ox=ox, oy=oy, coverage_rows_span=covered)
+
+    @staticmethod
+    def _autocrop_box(row_lo, row_hi, col_lo, col_hi):
+        """The reference's inner-rectangle crop (pysift/core.py:3627-3684)
+        from per-row/column coverage extents."""
+        rows = np.nonzero(row_hi >= 0)[0]
+        cols = np.nonzero(col_hi >= 0)[0]
+        if rows.size == 0:
+            return (None,) * 8 + (False,)
+        r0, r1 = int(rows[0]), int(rows[-1])
+        c0, c1 = int(cols[0]), int(cols[-1])
+        nr, nc = r1 - r0 + 1, c1 - c0 + 1
+        rl, rh = row_lo[r0:r1 + 1], row_hi[r0:r1 + 1]
+        cl, chh = col_lo[c0:c1 + 1], col_hi[c0:c1 + 1]
+        left = np.where(rh >= 0, rl - c0, 0)
+        right = np.where(rh >= 0, rh - c0, nc - 1)
+        top = np.where(chh >= 0, cl - r0, 0)
+        bot = np.where(chh >= 0, chh - r0, nr - 1)
+        ic0, ic1 = int(left.max()), int(right.min())
+        ir0, ir1 = int(top.max()), int(bot.min())
+        degenerate = ic0 >= ic1 or ir0 >= ir1
+        return r0, r1, c0, c1, ir0, ir1, ic0, ic1, degenerate
+
+    # ------------------------------------------------------------------
+    def _stitch_pair(self, img1, img2):
+        """pysift/core.py:3720-3818 (two images, img2 is the reference frame)."""
+        timings, metrics = {}, {}
+        with torch.cuda.device(self.device):
+            t0 = time.perf_counter()
+            g1 = self._upload_bgr(img1, "img1")
+            g2 = self._upload_bgr(img2, "img2")
+            kp1, d1, n1 = self._features(g1, "img1")
+            kp2, d2, n2 = self._features(g2, "img2")
+            metrics.update(kp1=n1, kp2=n2)
+            if n1 == 0 or n2 < 2:
+                raise RuntimeError(f"Insufficient matches (0), need >= 4")
+            m = self._match(d1, d2)
+            n_m = int(m["count"].item())
+            metrics.update(matches=n_m)
+            timings['st1'] = time.perf_counter() - t0
+            if n_m < 4:
+                raise RuntimeError(f"Insufficient matches ({n_m}), need >= 4")
+            st = self._stream()
+            p1 = torch.empty((n_m, 2), dtype=torch.float64, device=self.device)
+            p2 = torch.empty((n_m, 2), dtype=torch.float64, device=self.device)
+            _lib.check(self._lib.pysift_gather_points(kp1.data_ptr(), m["pairs"].data_ptr(), m["count"].data_ptr(),
+                                                      n_m, 0, p1.data_ptr(), st), "gather")
+            _lib.check(self._lib.pysift_gather_points(kp2.data_ptr(), m["pairs"].data_ptr(), m["count"].data_ptr(),
+                                                      n_m, 1, p2.data_ptr(), st), "gather")
+            timings['st2'] = 0.0
+            t0 = time.perf_counter()
+            H_d, mask_d, info_d = self._ransac(p1, p2, n_m)
+            H = H_d.cpu().numpy().reshape(3, 3).copy()
+            info = info_d.cpu().numpy()
+            n_in = int(info[0])
+            timings['st3'] = time.perf_counter() - t0
+            metrics.update(inliers=n_in, inlier_ratio=n_in / max(n_m, 1))
+            if n_in < 4:
+                raise RuntimeError(f"Only {n_in} inliers after RANSAC, need >= 4")
+            timings['st4'] = 0.0
+            metrics.update(depth_cv=None, bands=self.n_depth_layers)
+            t0 = time.perf_counter()
+            pano, cm = self._compose(g1, g2, H)
+            timings['st5'] = time.perf_counter() - t0
+            metrics.update(canvas_w=cm['canvas_w'], canvas_h=cm['canvas_h'], seam_rmse=float('nan'))
+        self._last = dict(H=H, mask=mask_d, pairs=m["pairs"][:n_m], kp1=kp1, kp2=kp2, p1=p1, p2=p2, info=info)
+        return pano, timings, metrics
+
+    def stitch(self, *args):
+        """Stitch two images (pysift/core.py:3972-4008); returns the BGR uint8
+        panorama and, as the reference does, writes panorama_<ts>.png to the
+        working directory unless the instance was built with save_output=False."""
+        if len(args) == 1 and isinstance(args[0], (list, tuple)):
+            images = list(args[0])
+        else:
+            images = list(args)
+        if len(images) == 3:
+            raise NotImplementedError("3-image stitching is not implemented on this backend")
+        if len(images) != 2:
+            raise ValueError(f"stitch() accepts 2 or 3 images, got {len(images)}")
+        pano, timings, metrics = self._stitch_pair(images[0], images[1])
+        self.last_timings, self.last_metrics = timings, metrics
+        if self.verbose:
+            print(f"[pysift_b200] kp {metrics['kp1']}/{metrics['kp2']}  matches {metrics['matches']}  "
+                  f"inliers {metrics['inliers']}  canvas {metrics['canvas_w']}x{metrics['canvas_h']}")
+        if self.save_output:
+            import cv2
+            ts = datetime.now().strftime("%Y%m%d_%H%M%S")
+            ext = 'jpg' if self.output_format in ('jpg', 'jpeg') else 'png'
+            fname = f"panorama_{ts}.{ext}"
+            if ext == 'jpg':
+                cv2.imwrite(fname, pano, [cv2.IMWRITE_JPEG_QUALITY, self.output_quality])
+            else:
+                cv2.imwrite(fname, pano)
+        return pano

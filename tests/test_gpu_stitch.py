@@ -1,0 +1,225 @@
+"""GPU parity of the stitch-path kernels (gray, CLAHE, top-k, matcher prep,
+RANSAC, DLT, warp + feather) and of the whole two-image stitch."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from pysift_b200 import synthetic
+
+pytestmark = pytest.mark.gpu
+
+
+def _lib():
+    from pysift_b200 import _lib
+    return _lib, _lib.load()
+
+
+def _st():
+    import torch
+    return torch.cuda.current_stream().cuda_stream
+
+
+@pytest.mark.parametrize("shape", [(960, 1280), (481, 643), (100, 77), (9, 13)])
+def test_gray_and_clahe_match_cv2(shape):
+    import cv2
+    import torch
+    L, lib = _lib()
+    H, W = shape
+    bgr = np.stack([synthetic.scene(H, W, seed=s) for s in range(3)], -1)
+    g = torch.from_numpy(bgr).cuda()
+    gray = torch.empty((H, W), dtype=torch.uint8, device="cuda")
+    assert lib.pysift_bgr2gray(g.data_ptr(), H, W, 3 * W, gray.data_ptr(), W, _st()) == 0
+    ref = cv2.cvtColor(bgr, cv2.COLOR_BGR2GRAY)
+    assert np.array_equal(gray.cpu().numpy(), ref)
+    lut = torch.empty(64 * 256, dtype=torch.uint8, device="cuda")
+    out = torch.empty((H, W), dtype=torch.uint8, device="cuda")
+    assert lib.pysift_clahe(gray.data_ptr(), H, W, W, 2.0, 8, 8, lut.data_ptr(), out.data_ptr(), W, _st()) == 0
+    ref_c = cv2.createCLAHE(clipLimit=2.0, tileGridSize=(8, 8)).apply(ref)
+    assert np.array_equal(out.cpu().numpy(), ref_c)
+
+
+def test_topk_by_response_is_stable_descending():
+    import torch
+    L, lib = _lib()
+    rng = np.random.default_rng(0)
+    resp = rng.integers(0, 50, size=20000).astype(np.float32)  # many ties
+    r = torch.from_numpy(resp).cuda()
+    rank = torch.empty(20000, dtype=torch.int32, device="cuda")
+    idx = torch.empty(8000, dtype=torch.int32, device="cuda")
+    assert lib.pysift_topk_by_response(r.data_ptr(), 20000, 8000, rank.data_ptr(), idx.data_ptr(), _st()) == 0
+    ref = np.array(sorted(range(20000), key=lambda i: -float(resp[i])))[:8000]
+    assert np.array_equal(idx.cpu().numpy(), ref)
+
+
+def test_matcher_preparation_bit_exact():
+    import torch
+    from oracle import stitch_oracle as so
+    L, lib = _lib()
+    rng = np.random.default_rng(1)
+    d = np.abs(rng.standard_normal((3000, 128))).astype(np.float32)
+    x = torch.from_numpy(d).cuda()
+    out = torch.empty_like(x)
+    assert lib.pysift_l2_normalize_rows(x.data_ptr(), 3000, 128, out.data_ptr(), _st()) == 0
+    ref = so.l2_normalize(d)
+    assert np.array_equal(out.cpu().numpy(), ref)
+    mean = torch.empty(128, dtype=torch.float32, device="cuda")
+    cov = torch.empty((128, 128), dtype=torch.float64, device="cuda")
+    assert lib.pysift_pca_stats(out.data_ptr(), 3000, 128, mean.data_ptr(), cov.data_ptr(), _st()) == 0
+    rmean, rcov = so.pca_stats(ref)
+    assert np.array_equal(mean.cpu().numpy(), rmean)
+    assert np.array_equal(cov.cpu().numpy(), rcov)
+    w, v = np.linalg.eigh(rcov)
+    proj = np.ascontiguousarray(v[:, -64:].astype(np.float32))
+    pj = torch.from_numpy(proj).cuda()
+    o16 = torch.empty((3000, 64), dtype=torch.float16, device="cuda")
+    assert lib.pysift_pca_project_f16(out.data_ptr(), 3000, 128, mean.data_ptr(), pj.data_ptr(), 64, o16.data_ptr(),
+                                      _st()) == 0
+    rp = so.pca_project(ref, rmean, proj).astype(np.float16)
+    assert np.array_equal(o16.cpu().numpy(), rp)
+
+
+def _correspondences(seed, n=1500, outliers=0.3):
+    rng = np.random.default_rng(seed)
+    Ht = synthetic.random_homography(rng, 1280, 960)
+    p1 = np.stack([rng.uniform(0, 1280, n), rng.uniform(0, 960, n)], 1)
+    ph = np.hstack([p1, np.ones((n, 1))]) @ Ht.T
+    p2 = ph[:, :2] / ph[:, 2:3] + rng.normal(0, 0.7, (n, 2))
+    k = int(outliers * n)
+    p2[:k] = np.stack([rng.uniform(-500, 1500, k), rng.uniform(-200, 1100, k)], 1)
+    p1 = p1.astype(np.float32).astype(np.float64)
+    p2 = p2.astype(np.float32).astype(np.float64)
+    return p1, p2, Ht
+
+
+@pytest.mark.parametrize("seed,magsac", [(0, True), (1, True), (2, False)])
+def test_ransac_bit_exact(seed, magsac):
+    import torch
+    from oracle import stitch_oracle as so
+    L, lib = _lib()
+    p1, p2, Ht = _correspondences(seed)
+    n, n_hyp = len(p1), 2048
+    rnd = so.mt19937_u32(42, 4 * n_hyp)
+    host = np.empty(4 * n_hyp, np.uint32)
+    lib.pysift_mt19937_u32(42, host.ctypes.data_as(ctypes.c_void_p), host.size)
+    assert np.array_equal(host, rnd)
+    gen = torch.Generator(device="cpu")
+    gen.manual_seed(42)
+    ti = torch.randint(0, n, (n_hyp, 4), generator=gen).numpy().ravel()
+    assert np.array_equal(ti, (rnd % n).astype(np.int64))
+    sz = ctypes.c_size_t()
+    lib.pysift_ransac_workspace_size(n, n_hyp, ctypes.byref(sz))
+    ws = torch.empty(sz.value + 256, dtype=torch.uint8, device="cuda")
+    off = (-ws.data_ptr()) % 256
+    d1, d2 = torch.from_numpy(p1).cuda(), torch.from_numpy(p2).cuda()
+    r = torch.from_numpy(rnd).cuda()
+    H = torch.empty(9, dtype=torch.float64, device="cuda")
+    mask = torch.empty(n, dtype=torch.uint8, device="cuda")
+    info = torch.empty(3, dtype=torch.int32, device="cuda")
+    rc = lib.pysift_ransac(d1.data_ptr(), d2.data_ptr(), n, r.data_ptr(), n_hyp, 4.0, 4.0, 1 if magsac else 0, 10,
+                           ws.data_ptr() + off, sz.value, H.data_ptr(), mask.data_ptr(), info.data_ptr(), _st())
+    assert rc == 0
+    rH, rmask, rinfo, _ = so.ransac(p1, p2, n_hyp, 4.0, 4.0, magsac)
+    assert np.array_equal(info.cpu().numpy(), rinfo)
+    assert np.array_equal(mask.cpu().numpy().astype(bool), rmask)
+    assert np.array_equal(H.cpu().numpy().reshape(3, 3), rH)
+    # and it found the true geometry
+    assert rinfo[0] > 0.6 * n
+    Hn = rH / rH[2, 2]
+    assert np.allclose(Hn, Ht / Ht[2, 2], rtol=5e-3, atol=5e-3 * np.abs(Ht).max())
+
+
+def test_dlt_matches_oracle_and_svd():
+    import torch
+    from oracle import stitch_oracle as so
+    L, lib = _lib()
+    p1, p2, Ht = _correspondences(5, n=400, outliers=0.0)
+    d1, d2 = torch.from_numpy(p1).cuda(), torch.from_numpy(p2).cuda()
+    idx = torch.empty(400, dtype=torch.int32, device="cuda")
+    H = torch.empty(9, dtype=torch.float64, device="cuda")
+    assert lib.pysift_dlt_homography(d1.data_ptr(), d2.data_ptr(), 400, idx.data_ptr(), H.data_ptr(), _st()) == 0
+    Hg = H.cpu().numpy().reshape(3, 3)
+    assert np.array_equal(Hg, so.dlt(p1, p2))
+    # the reference's SVD formulation (pysift/core.py:2959-2981) in float64
+    def norm(p):
+        c = p.mean(0); md = np.sqrt(((p - c) ** 2).sum(1)).mean(); s = np.sqrt(2) / (md + 1e-10)
+        T = np.array([[s, 0, -s * c[0]], [0, s, -s * c[1]], [0, 0, 1]])
+        return (T @ np.hstack([p, np.ones((len(p), 1))]).T).T[:, :2], T
+    a, T1 = norm(p1); b, T2 = norm(p2)
+    A = np.zeros((800, 9))
+    for i in range(400):
+        A[2 * i] = [-a[i, 0], -a[i, 1], -1, 0, 0, 0, b[i, 0] * a[i, 0], b[i, 0] * a[i, 1], b[i, 0]]
+        A[2 * i + 1] = [0, 0, 0, -a[i, 0], -a[i, 1], -1, b[i, 1] * a[i, 0], b[i, 1] * a[i, 1], b[i, 1]]
+    Hs = np.linalg.inv(T2) @ np.linalg.svd(A)[2][-1].reshape(3, 3) @ T1
+    Hs /= Hs[2, 2]
+    assert np.max(np.abs(Hg - Hs) / np.maximum(np.abs(Hs), 1e-9)) < 1e-6
+
+
+def test_warp_feather_bit_exact_and_grid_sample():
+    import torch
+    import torch.nn.functional as F
+    from oracle import stitch_oracle as so
+    L, lib = _lib()
+    img1, img2, Ht = synthetic.stitch_pair(240, 320, seed=3)
+    Hs = np.linalg.inv(Ht)  # maps view-1 to view-2: use the true homography image1 -> image2 frame
+    H = Ht
+    cw, ch, ox, oy = so.canvas_size(img1.shape, img2.shape, H)
+    hinv = np.linalg.inv(H).astype(np.float32)
+    iox, ioy = int(round(ox)), int(round(oy))
+    g1, g2 = torch.from_numpy(img1).cuda(), torch.from_numpy(img2).cuda()
+    out = torch.empty((ch, cw, 3), dtype=torch.uint8, device="cuda")
+    warped = torch.empty_like(out)
+    m1 = torch.empty((ch, cw), dtype=torch.uint8, device="cuda")
+    m2 = torch.empty_like(m1)
+    hb = (ctypes.c_float * 9)(*[float(v) for v in hinv.ravel()])
+    rc = lib.pysift_warp_feather(g1.data_ptr(), 240, 320, 960, g2.data_ptr(), 240, 320, 960, cw, ch,
+                                 ctypes.cast(hb, ctypes.c_void_p), float(np.float32(ox)), float(np.float32(oy)), iox,
+                                 ioy, 1, out.data_ptr(), warped.data_ptr(), m1.data_ptr(), m2.data_ptr(), None, None,
+                                 None, None, _st())
+    assert rc == 0
+    r_out, r_warp, r_m1, r_m2 = so.warp_feather(img1, img2, hinv, cw, ch, ox, oy, iox, ioy)
+    assert np.array_equal(out.cpu().numpy(), r_out)
+    assert np.array_equal(warped.cpu().numpy(), r_warp)
+    assert np.array_equal(m1.cpu().numpy().astype(bool), r_m1)
+    assert np.array_equal(m2.cpu().numpy().astype(bool), r_m2)
+    # the bilinear part equals torch's grid_sample on the same grid (the reference's call)
+    u = torch.arange(cw, dtype=torch.float32, device="cuda")
+    v = torch.arange(ch, dtype=torch.float32, device="cuda")
+    uu, vv = torch.meshgrid(u, v, indexing="xy")
+    X, Y = uu - float(np.float32(ox)), vv - float(np.float32(oy))
+    hi = torch.from_numpy(hinv).cuda()
+    s0 = hi[0, 0] * X + hi[0, 1] * Y + hi[0, 2]
+    s1 = hi[1, 0] * X + hi[1, 1] * Y + hi[1, 2]
+    s2 = hi[2, 0] * X + hi[2, 1] * Y + hi[2, 2]
+    den = s2.clamp(min=1e-10)
+    sxn = (2.0 * (s0 / den) / (320 - 1)) - 1.0
+    syn = (2.0 * (s1 / den) / (240 - 1)) - 1.0
+    grid = torch.stack([sxn, syn], -1).reshape(1, ch, cw, 2)
+    it = g1.float().permute(2, 0, 1).unsqueeze(0)
+    gs = F.grid_sample(it, grid, mode="bilinear", padding_mode="zeros", align_corners=True)
+    ref_w = gs.squeeze(0).permute(1, 2, 0).cpu().numpy().clip(0, 255).astype(np.uint8)
+    # (the cross-check with torch's kernel allows last-bit differences of its
+    # accumulation at uint8 truncation boundaries)
+    wv = warped.cpu().numpy()
+    assert np.mean(ref_w == wv) > 0.999
+    assert np.abs(ref_w.astype(int) - wv.astype(int)).max() <= 1
+
+
+def test_stitch_pair_end_to_end():
+    from oracle import stitch_oracle as so
+    from pysift_b200.stitch import GPUPyStitch
+    img1, img2, Ht = synthetic.stitch_pair(480, 640, seed=1)
+    st = GPUPyStitch(ransac_iters=2048, inlier_thresh=4.0, save_output=False, verbose=False)
+    pano = st.stitch(img1, img2)
+    orc = so.OracleStitch(ransac_iters=2048, inlier_thresh=4.0).stitch(img1, img2)
+    m = st.last_metrics
+    assert m["kp1"] == orc["n1"] and m["kp2"] == orc["n2"]
+    assert abs(m["matches"] - len(orc["pairs"])) <= max(2, 0.01 * len(orc["pairs"]))
+    Hg = st._last["H"]
+    rel = np.max(np.abs(Hg - orc["H"]) / np.maximum(np.abs(orc["H"]), 1e-6))
+    assert rel < 1e-3, rel
+    if pano.shape == orc["pano"].shape:
+        diff = np.abs(pano.astype(int) - orc["pano"].astype(int))
+        assert np.mean(diff <= 1) > 0.99
+    Ht_n = Ht / Ht[2, 2]
+    assert np.allclose(Hg / Hg[2, 2], Ht_n, rtol=2e-2, atol=2e-2 * np.abs(Ht_n).max())
