@@ -12,6 +12,8 @@ stand in for the reference's datasets; see pysift_b200/synthetic.py):
                     4 px, linear feather blend) -- the default
   detect_1280x960   detectAndCompute on one 1280x960 grayscale scene
   detect_640x480    detectAndCompute on one 640x480 scene
+  match_u8_8192     exact ratio-test matching of two 8192 x 128 uint8-valued
+                    descriptor sets (bf16 tcgen05 GEMM, exact against int64)
 
 A step is one pass of the hot path over one input.  `value` is measured
 with CUDA events on the launching stream, inputs resident in HBM, L2
@@ -37,6 +39,7 @@ WORKLOADS = {
     "stitch_pair_1280x960": dict(kind="stitch", H=960, W=1280, seed=0, ransac_iters=2048, inlier_thresh=4.0),
     "detect_1280x960": dict(kind="detect", H=960, W=1280, seed=0),
     "detect_640x480": dict(kind="detect", H=480, W=640, seed=0),
+    "match_u8_8192": dict(kind="match", N=8192, M=8192, D=128, seed=0),
 }
 DEFAULT_WORKLOAD = "stitch_pair_1280x960"
 METRIC = "SIFT Mpix/s + match-pairs/s on 1 B200: batched+BF16 vs plain, bit-exact"
@@ -175,6 +178,8 @@ def run_reference(args, wl, world, rank):
     from pysift_b200 import synthetic
     if wl["kind"] == "stitch":
         return run_reference_stitch(args, wl)
+    if wl["kind"] == "match":
+        return run_reference_match(args, wl)
     img = synthetic.scene(wl["H"], wl["W"], seed=wl["seed"])
     times = []
     from oracle import oracle
@@ -196,6 +201,135 @@ def run_reference(args, wl, world, rank):
         "cpu_baseline": {"value": value, "unit": "Mpix/s", "cores": os.cpu_count(), "kind": "port",
                          "sample": f"one {wl['W']}x{wl['H']} image per step, full detectAndCompute"},
         "e2e": {"value": value, "unit": "Mpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def measured_tensor_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        if "bf16_tflops" in d:
+            return float(d["bf16_tflops"]), "measured (cuBLAS bf16 burst)"
+    return 1590.0, "fallback"
+
+
+def run_match(args, wl, world, rank, local):
+    import torch
+    import torch.distributed as dist
+    from pysift_b200 import _lib, match, synthetic
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    N, M, D = wl["N"], wl["M"], wl["D"]
+    a, b = synthetic.descriptor_sets(N, M, seed=wl["seed"] + rank, D=D)
+    ga, gb = torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    lib = _lib.load()
+    for _ in range(args.warmup):
+        out = match.match_u8_exact(ga, gb)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    step_ms = []
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    launches0 = lib.pysift_launch_count()
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            e0.record(stream)
+            out = match.match_u8_exact(ga, gb)
+            e1.record(stream)
+            e1.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+    launches = lib.pysift_launch_count() - launches0
+    n_pairs = int(out["count"].item())
+    t = torch.tensor([float(np.sum(step_ms))], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    # end to end: pinned host sets -> device, match, pairs and count back to the host
+    ha = torch.from_numpy(a).pin_memory()
+    hb = torch.from_numpy(b).pin_memory()
+    e2e_ms = []
+    for i in range(args.warmup + args.steps):
+        flush.zero_()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        da, db = ha.to(dev, non_blocking=True), hb.to(dev, non_blocking=True)
+        o = match.match_u8_exact(da, db)
+        cnt = int(o["count"].item())
+        pairs_host = o["pairs"][:cnt].cpu()
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            e2e_ms.append(dt * 1e3)
+    e2e_t = torch.tensor([float(np.sum(e2e_ms))], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    if rank != 0:
+        return 0
+    step_s = total_ms / args.steps / 1e3
+    flops = 2.0 * N * M * D
+    peak, peak_kind = measured_tensor_peak()
+    achieved = flops / step_s / 1e12
+    if args.no_cpu_baseline:
+        cpu_s, cpu_n = float("nan"), 0
+    else:
+        from oracle import match_oracle as mo
+        times = []
+        t_start = time.perf_counter()
+        while time.perf_counter() - t_start < 15.0 and len(times) < 5:
+            t0 = time.perf_counter()
+            mo.match_u8_exact(a, b)
+            times.append(time.perf_counter() - t0)
+        cpu_s, cpu_n = float(np.median(times)), len(times)
+    line = {
+        "metric": METRIC, "value": world / step_s, "unit": "match-pairs/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "bf16", "data": "synthetic",
+        "config": {"workload": args.workload, "N": N, "M": M, "D": D, "seed": wl["seed"], "ratio": 0.75,
+                   "mutual_matches": n_pairs, "l2": "flushed (256 MiB write) before every step",
+                   "parallelism": f"replicas{world}"},
+        "roofline": {"bound": "tensor", "kernel": "whole match call (k_row_norms_u8 x2, k_match_rows x2, "
+                     "k_match_merge x2, k_match_mutual); flops 2*N*M*D counted once",
+                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                     "peak_source": peak_kind, "alg_flops_per_step": flops,
+                     "traffic": committed_traffic(args.workload)},
+        "cpu_baseline": {"value": 1.0 / cpu_s if cpu_s == cpu_s else None, "unit": "match-pairs/s",
+                         "cores": os.cpu_count(), "kind": "port",
+                         "sample": f"{cpu_n} full {N}x{M} exact matches by the oracle (numpy, BLAS float64)"},
+        "e2e": {"value": world * args.steps / (float(e2e_t.item()) / 1e3), "unit": "match-pairs/s",
+                "h2d_bytes_per_step": int(a.nbytes + b.nbytes), "d2h_bytes_per_step": 4 + 8 * n_pairs},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_reference_match(args, wl):
+    from oracle import match_oracle as mo
+    from pysift_b200 import synthetic
+    a, b = synthetic.descriptor_sets(wl["N"], wl["M"], seed=wl["seed"], D=wl["D"])
+    times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        mo.match_u8_exact(a, b)
+        if i >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    sec = float(np.mean(times))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": 1.0 / sec, "unit": "match-pairs/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+        "config": {"workload": args.workload, "N": wl["N"], "M": wl["M"], "D": wl["D"], "seed": wl["seed"]},
+        "cpu_baseline": {"value": 1.0 / sec, "unit": "match-pairs/s", "cores": os.cpu_count(), "kind": "port",
+                         "sample": "one full exact match per step (oracle, numpy + BLAS)"},
+        "e2e": {"value": 1.0 / sec, "unit": "match-pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -411,6 +545,13 @@ def run_stitch(args, wl, world, rank, local):
     e2e_tot = torch.tensor([float(np.sum(e2e_ms))], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(e2e_tot, op=dist.ReduceOp.MAX)
+    # stage breakdown of one more stitch (events on the stitch's stream)
+    st.stage_events = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+    st.stitch(g1, g2)
+    st.stage_events[5].synchronize()
+    stage_ms = {name: round(st.stage_events[i].elapsed_time(st.stage_events[i + 1]), 4)
+                for i, name in enumerate(st.STAGES)}
+    st.stage_events = None
     # roofline of the dominant kernel region: pyramid + DoG + extrema of one view
     sift = st._detector
     gray = st._gray_clahe(g1, "img1")
@@ -456,6 +597,7 @@ def run_stitch(args, wl, world, rank, local):
                 "d2h_bytes_per_step": int(pano.nbytes) + 72 + 16},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
+        "stage_ms": stage_ms,
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -482,6 +624,8 @@ def main():
     try:
         if wl["kind"] == "stitch":
             return run_stitch(args, wl, world, rank, local)
+        if wl["kind"] == "match":
+            return run_match(args, wl, world, rank, local)
         return run_detect(args, wl, world, rank, local)
     finally:
         if world > 1:

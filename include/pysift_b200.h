@@ -179,10 +179,14 @@ int pysift_gather_points(const float* kpts, const int32_t* pairs, const int32_t*
                          double* pts, pysift_stream_t stream);
 
 /* Matcher preparation (pysift/core.py:2877-2888, 2703-2743): row L2
- * normalisation (+1e-7), PCA statistics (float32 mean, float64 covariance)
- * of the stacked normalised sets, projection + normalisation to fp16. */
+ * normalisation (+1e-7), PCA statistics (float32 mean, float64 covariance,
+ * both summed over fixed 128-row chunks) of the stacked normalised sets in a
+ * caller workspace of pysift_pca_workspace_size bytes, projection (D in
+ * {64, 128}, P in {32, 64, 128}) + normalisation to fp16. */
 int pysift_l2_normalize_rows(const float* in, int32_t n, int32_t D, float* out, pysift_stream_t stream);
-int pysift_pca_stats(const float* x, int32_t n, int32_t D, float* mean, double* cov, pysift_stream_t stream);
+int pysift_pca_workspace_size(int32_t n, int32_t D, size_t* bytes);
+int pysift_pca_stats(const float* x, int32_t n, int32_t D, void* workspace, size_t workspace_bytes, float* mean,
+                     double* cov, pysift_stream_t stream);
 int pysift_pca_project_f16(const float* x, int32_t n, int32_t D, const float* mean, const float* proj, int32_t P,
                            uint16_t* out, pysift_stream_t stream);
 int pysift_to_f16(const float* in, int64_t n, uint16_t* out, pysift_stream_t stream);

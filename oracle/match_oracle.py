@@ -61,7 +61,9 @@ def match_fp16(d1h, d2h, ratio=0.75):
 def match_u8_exact(a, b, ratio=0.75):
     A = a.astype(np.int64)
     B = b.astype(np.int64)
-    D2 = (A * A).sum(1)[:, None] + (B * B).sum(1)[None, :] - 2 * (A @ B.T)
+    # float64 products and sums of uint8 values are exact integers (< 2^53)
+    G = (a.astype(np.float64) @ b.astype(np.float64).T).astype(np.int64)
+    D2 = (A * A).sum(1)[:, None] + (B * B).sum(1)[None, :] - 2 * G
     rs = ratio * ratio
     fb, f1, f2 = _top2(D2, False)
     fok = (f2 > 0) & (f1.astype(np.float64) < rs * f2.astype(np.float64))

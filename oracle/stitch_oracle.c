@@ -212,30 +212,65 @@ static void dlt_refit(const double* p1, const double* p2, const int* idx, int m,
         for (int c = r; c < 9; ++c, ++q) M[r][c] = M[c][r] = Mv[q];
     for (int r = 0; r < 9; ++r)
         for (int c = 0; c < 9; ++c) V[r][c] = (r == c) ? 1.0 : 0.0;
-    for (int sweep = 0; sweep < 15; ++sweep)
-        for (int p = 0; p < 8; ++p)
-            for (int qq = p + 1; qq < 9; ++qq) {
+    /* parallel (round-robin) Jacobi: round r rotates the disjoint pairs
+     * {(r+i) mod 9, (r-i) mod 9}, i = 1..4; angles from the start-of-round
+     * matrix, then all column rotations, then all row rotations; after sweep
+     * 3 negligible elements are zeroed instead of rotated; stop when every
+     * off-diagonal element is 0 (15 sweeps at most). */
+    for (int sweep = 0; sweep < 15; ++sweep) {
+        int nz = 0;
+        for (int r = 0; r < 9; ++r)
+            for (int c = r + 1; c < 9; ++c)
+                if (M[r][c] != 0.0) nz = 1;
+        if (!nz) break;
+        for (int rnd = 0; rnd < 9; ++rnd) {
+            int P[4], Q[4], act[4];
+            double C[4], S[4];
+            for (int j = 0; j < 4; ++j) {
+                int a = (rnd + j + 1) % 9, bb = (rnd + 9 - j - 1) % 9;
+                int p = a < bb ? a : bb, qq = a < bb ? bb : a;
+                P[j] = p;
+                Q[j] = qq;
+                act[j] = 0;
                 double apq = M[p][qq];
                 if (apq == 0.0) continue;
-                double theta = (M[qq][qq] - M[p][p]) / (2.0 * apq);
+                double app = M[p][p], aqq = M[qq][qq];
+                double g = 100.0 * fabs(apq);
+                if (sweep > 3 && fabs(app) + g == fabs(app) && fabs(aqq) + g == fabs(aqq)) {
+                    M[p][qq] = 0.0;
+                    M[qq][p] = 0.0;
+                    continue;
+                }
+                double theta = (aqq - app) / (2.0 * apq);
                 double tt = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
-                double c = 1.0 / sqrt(tt * tt + 1.0), s = tt * c;
+                double c = 1.0 / sqrt(tt * tt + 1.0);
+                C[j] = c;
+                S[j] = tt * c;
+                act[j] = 1;
+            }
+            for (int j = 0; j < 4; ++j) {
+                if (!act[j]) continue;
+                int p = P[j], qq = Q[j];
                 for (int k = 0; k < 9; ++k) {
                     double mkp = M[k][p], mkq = M[k][qq];
-                    M[k][p] = c * mkp - s * mkq;
-                    M[k][qq] = s * mkp + c * mkq;
-                }
-                for (int k = 0; k < 9; ++k) {
-                    double mpk = M[p][k], mqk = M[qq][k];
-                    M[p][k] = c * mpk - s * mqk;
-                    M[qq][k] = s * mpk + c * mqk;
-                }
-                for (int k = 0; k < 9; ++k) {
-                    double vkp = V[k][p], vkq = V[k][qq];
-                    V[k][p] = c * vkp - s * vkq;
-                    V[k][qq] = s * vkp + c * vkq;
+                    M[k][p] = C[j] * mkp - S[j] * mkq;
+                    M[k][qq] = S[j] * mkp + C[j] * mkq;
                 }
             }
+            for (int j = 0; j < 4; ++j) {
+                if (!act[j]) continue;
+                int p = P[j], qq = Q[j];
+                for (int k = 0; k < 9; ++k) {
+                    double mpk = M[p][k], mqk = M[qq][k];
+                    M[p][k] = C[j] * mpk - S[j] * mqk;
+                    M[qq][k] = S[j] * mpk + C[j] * mqk;
+                    double vkp = V[k][p], vkq = V[k][qq];
+                    V[k][p] = C[j] * vkp - S[j] * vkq;
+                    V[k][qq] = S[j] * vkp + C[j] * vkq;
+                }
+            }
+        }
+    }
     int best = 0;
     for (int k = 1; k < 9; ++k)
         if (M[k][k] < M[best][best]) best = k;
@@ -324,7 +359,7 @@ EXPORT void orc_ransac(const double* p1, const double* p2, int n, const uint32_t
             if (sym_err(H1, H1i, p1[2 * i], p1[2 * i + 1], p2[2 * i], p2[2 * i + 1], 0) < tq) idx[n2++] = i;
         if (n2 >= min_inliers) {
             dlt_refit(p1, p2, idx, n2, H);
-            memset(mask_out, 0, n);
+            memset(mask_out, 0, (size_t)(n > 0 ? n : 0));
             for (int k = 0; k < n2; ++k) mask_out[idx[k]] = 1;
             stage = 2;
             n_final = n2;
@@ -368,19 +403,32 @@ EXPORT void orc_l2_normalize(const float* in, long n, int D, float* out) {
     }
 }
 
+/* float64 sums over fixed 128-row chunks, sequential inside a chunk, then the
+ * chunk partials in order (pysift_b200/csrc/ransac.cu k_pca_*). */
 EXPORT void orc_pca_stats(const float* x, long n, int D, float* mean, double* cov) {
+    const long C = 128, nchunks = (n + C - 1) / C;
     for (int k = 0; k < D; ++k) {
         double s = 0.0;
-        for (long i = 0; i < n; ++i) s = s + (double)x[i * D + k];
+        for (long c = 0; c < nchunks; ++c) {
+            double p = 0.0;
+            long i1 = (c + 1) * C < n ? (c + 1) * C : n;
+            for (long i = c * C; i < i1; ++i) p = p + (double)x[i * D + k];
+            s = s + p;
+        }
         mean[k] = (float)(s / (double)n);
     }
     #pragma omp parallel for schedule(dynamic, 4)
     for (int k = 0; k < D; ++k)
         for (int l = k; l < D; ++l) {
             double s = 0.0;
-            for (long i = 0; i < n; ++i) {
-                double a = (double)(x[i * D + k] - mean[k]), b = (double)(x[i * D + l] - mean[l]);
-                s = s + a * b;
+            for (long c = 0; c < nchunks; ++c) {
+                double p = 0.0;
+                long i1 = (c + 1) * C < n ? (c + 1) * C : n;
+                for (long i = c * C; i < i1; ++i) {
+                    double a = (double)(x[i * D + k] - mean[k]), b = (double)(x[i * D + l] - mean[l]);
+                    p = p + a * b;
+                }
+                s = s + p;
             }
             cov[k * D + l] = cov[l * D + k] = s / (double)n;
         }

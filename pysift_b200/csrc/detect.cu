@@ -1038,11 +1038,20 @@ __global__ void __launch_bounds__(1024) k_cap(const CapArgs a, Ctrl* ctrl) {
         for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0u;
         __syncthreads();
         const unsigned int prefix = s_prefix, mask = s_mask;
-        for (int g = threadIdx.x; g < total; g += blockDim.x) {
-            int o, j;
-            long long src = load(g, &o, &j);
-            unsigned int key = __float_as_uint(a.rf_resp[src]);
-            if ((key & mask) == prefix) atomicAdd(&hist[(key >> (8 * pass)) & 255u], 1u);
+        // one shared atomic per distinct digit and warp: the keys crowd into a
+        // few exponent bytes, and per-key atomics on one bin serialise
+        for (int c0 = 0; c0 < total; c0 += blockDim.x) {
+            const int g = c0 + threadIdx.x;
+            unsigned int dig = 0xffffffffu;
+            if (g < total) {
+                int o, j;
+                const long long src = load(g, &o, &j);
+                const unsigned int key = __float_as_uint(a.rf_resp[src]);
+                if ((key & mask) == prefix) dig = (key >> (8 * pass)) & 255u;
+            }
+            const unsigned int peers = __match_any_sync(FULL_MASK, dig);
+            if (dig != 0xffffffffu && (int)(threadIdx.x & 31) == __ffs(peers) - 1)
+                atomicAdd(&hist[dig], (unsigned int)__popc(peers));
         }
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -1133,17 +1142,23 @@ struct WarpHist {
     unsigned int* hi;
     unsigned long long* tot;
     int nbins;
+    // Descriptor histograms (128 bins = 4 y-cells x 4 x-cells x 8 orientations)
+    // store bin b at b ^ (ycell << 3), so that the y-cell moves a bin to
+    // another shared-memory bank; other sizes are stored in order.
+    __device__ __forceinline__ int phys(int bin) const { return nbins == 128 ? bin ^ (((bin >> 5) & 3) << 3) : bin; }
     __device__ __forceinline__ void add(int bin, unsigned long long q) const {
-        atomicAdd(lo + bin, (unsigned int)(q & 0x1fffffull));
-        atomicAdd(hi + bin, (unsigned int)(q >> 21));
+        const int p = phys(bin);
+        atomicAdd(lo + p, (unsigned int)(q & 0x1fffffull));
+        atomicAdd(hi + p, (unsigned int)(q >> 21));
     }
     // all lanes of the warp call fold() together
     __device__ __forceinline__ void fold() const {
         __syncwarp();
         for (int b = (int)(threadIdx.x & 31); b < nbins; b += 32) {
-            tot[b] += ((unsigned long long)hi[b] << 21) + (unsigned long long)lo[b];
-            lo[b] = 0u;
-            hi[b] = 0u;
+            const int p = phys(b);
+            tot[b] += ((unsigned long long)hi[p] << 21) + (unsigned long long)lo[p];
+            lo[p] = 0u;
+            hi[p] = 0u;
         }
         __syncwarp();
     }
@@ -1380,6 +1395,21 @@ struct DescArgs {
 
 constexpr int DESC_T = 256;
 constexpr int DESC_W = DESC_T / 32;
+// Lane layout of a descriptor warp step: the 32 lanes form DESC_GR x DESC_GC
+// groups of DESC_L consecutive pixels of one row; the groups sit in
+// different row bands and column bands of the patch (a band is 1/DESC_GR of
+// the patch height, 1/DESC_GC of its width), so lanes of different groups
+// fall in different spatial bins and their histogram updates do not
+// serialise on one shared-memory word, while each group's loads stay
+// contiguous.
+#ifndef DESC_GR
+#define DESC_GR 4
+#endif
+#ifndef DESC_GC
+#define DESC_GC 2
+#endif
+constexpr int DESC_L = 32 / (DESC_GR * DESC_GC);
+static_assert(DESC_GR * DESC_GC * DESC_L == 32, "descriptor lane groups must tile a warp");
 
 __device__ __forceinline__ void desc_accumulate(const float* __restrict__ g, long long P, int H, int W, float ri,
                                                 float ci, float cos_a, float sin_a, float ang_rad, int ph,
@@ -1390,15 +1420,19 @@ __device__ __forceinline__ void desc_accumulate(const float* __restrict__ g, lon
     const int side = 2 * ph + 1;
     const int r0 = (int)ri, c0 = (int)ci;
     const int lane = tid & 31, warp = tid >> 5;
-    // the (2ph+1)^2 patch in 8x4 pixel blocks, one block per warp step
-    const int tcols = (side + 7) >> 3, trows = (side + 3) >> 2;
-    const int ntiles = tcols * trows;
+    const int k = lane % DESC_L, grp = lane / DESC_L;
+    const int gi = grp / DESC_GC, gj = grp - gi * DESC_GC;
+    const int band_r = (side + DESC_GR - 1) / DESC_GR;  // rows per row band
+    const int band_c = (side + DESC_GC - 1) / DESC_GC;  // columns per column band
+    const int runs = (band_c + DESC_L - 1) / DESC_L;    // DESC_L-pixel runs per band row
+    const int nsteps = band_r * runs;
     int steps = 0;
-    for (int t = warp; t < ntiles; t += DESC_W) {
-        const int ty = t / tcols, tx = t - ty * tcols;
-        const int r_off = ty * 4 + (lane >> 3) - ph, c_off = tx * 8 + (lane & 7) - ph;
+    for (int t = warp; t < nsteps; t += DESC_W) {
+        const int u = t / runs, v = t - u * runs;
+        const int pr = gi * band_r + u, pcb = v * DESC_L + k, pc = gj * band_c + pcb;
+        const int r_off = pr - ph, c_off = pc - ph;
         const int rr = r0 + r_off, cc = c0 + c_off;
-        bool act = r_off <= ph && c_off <= ph && !(rr < 1 || rr >= H - 1 || cc < 1 || cc >= W - 1);
+        bool act = pr < side && pcb < band_c && pc < side && !(rr < 1 || rr >= H - 1 || cc < 1 || cc >= W - 1);
         float fc = (float)c_off, fr = (float)r_off;
         float xr = cos_a * fc - sin_a * fr;
         float yr = sin_a * fc + cos_a * fr;

@@ -1,22 +1,30 @@
 // match.cu -- brute-force ratio-test matching on the 5th-generation tensor cores.
 //
-// One CTA computes a 128 x 128 tile of S = A * B^T with tcgen05.mma
-// (kind::f16, fp16 or bf16 operands staged in shared memory in the
-// no-swizzle K-major core-matrix layout, fp32 accumulators in tensor memory),
-// then reduces the tile in its epilogue to per-row and per-column top-2
-// candidates.  A second kernel merges the per-tile candidates, applies the
-// ratio test in both directions and keeps mutual matches
+// Matching runs as two row scans: queries against the train set (forward
+// top-2) and the train set against the queries (backward top-2).  Each CTA of
+// k_match_rows keeps a 128-row query block resident in shared memory and
+// streams 128-row train tiles through two cp.async buffers (no-swizzle
+// K-major core-matrix layout); one thread issues the tcgen05.mma of tile t+1
+// (kind::f16, fp32 accumulator in tensor memory, two accumulators of 128
+// columns) while all four warps reduce tile t, read back with tcgen05.ld, to
+// a running per-row top-2 in registers.  Train tiles are split into
+// segments so that the grid fills the SMs; k_match_merge combines the
+// segments and applies the ratio test; k_match_mutual keeps mutual matches
 // (pysift/core.py:2574-2701, 2840-2940).
 //
-// Two scoring modes share the kernel:
+// Two scoring modes share the kernels:
 //   SIM_F16   reference semantics: fp16 inputs, the fp32 tile rounded to fp16
 //             (torch.mm under fp16 autocast, core.py:2604-2605), larger is better,
 //             d^2 = max(0, 2 - 2 s), pass iff d2^2 > 1e-10 and d1^2 < r^2 d2^2 in float32.
 //   DIST_BF16 exact L2 on uint8-valued descriptors: bf16 holds 0..255 exactly and
 //             every partial sum of 128 products stays below 2^24, so the fp32
-//             accumulator is the exact integer dot product; d^2 = |a|^2 + |b|^2 - 2 a.b,
-//             smaller is better, pass iff d2^2 > 0 and d1^2 < r^2 d2^2 (exact).
-// Ties are broken towards the lower index in every direction.
+//             accumulator is the exact integer dot product.  Rows rank train
+//             entries by 2 a.b - |b|^2 (exact in fp32: |2 a.b| < 2^24), which orders
+//             them as -|a - b|^2; d^2 = |a|^2 - key, pass iff d2^2 > 0 and
+//             d1^2 < r^2 d2^2 (exact).
+// Ties are broken towards the lower index in every direction: a scan visits
+// train entries in increasing index order and replaces the best only on a
+// strictly larger key; segments merge in index order.
 #include <algorithm>
 #include <cstdint>
 
@@ -25,40 +33,17 @@
 
 namespace pysift {
 
-constexpr int MT = 128;           // tile rows (queries) = UMMA M
-constexpr int NT = 128;           // tile cols (train)   = UMMA N
+constexpr int MT = 128;           // query rows per CTA = UMMA M = TMEM lanes
+constexpr int NT = 128;           // train rows per tile = UMMA N
 constexpr int MATCH_THREADS = 128;
-constexpr unsigned SPIN_LIMIT = 1u << 26;  // bounded wait on the MMA barrier
+constexpr unsigned SPIN_LIMIT = 1u << 26;  // bounded waits on the MMA barriers
 
 enum MatchMode { SIM_F16 = 0, DIST_BF16 = 1 };
 
-struct Cand {  // top-2, "larger key is better", ties to the lower index
+struct Top2 {  // best key and index, second-best key
     float k1, k2;
-    int i1, i2;
+    int i1, pad;
 };
-
-__device__ __forceinline__ bool better(float ka, int ia, float kb, int ib) {
-    return ka > kb || (ka == kb && ia < ib);
-}
-
-__device__ __forceinline__ void cand_push(Cand& c, float k, int i) {
-    if (better(k, i, c.k1, c.i1)) {
-        c.k2 = c.k1;
-        c.i2 = c.i1;
-        c.k1 = k;
-        c.i1 = i;
-    } else if (better(k, i, c.k2, c.i2)) {
-        c.k2 = k;
-        c.i2 = i;
-    }
-}
-
-__device__ __forceinline__ Cand cand_empty() {
-    Cand c;
-    c.k1 = c.k2 = -INFINITY;
-    c.i1 = c.i2 = 0x7fffffff;
-    return c;
-}
 
 // byte offset of 16-byte chunk c (8 elements along K) of row r in the
 // no-swizzle K-major layout: core matrices of 8 rows x 16 bytes, adjacent
@@ -88,177 +73,232 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-struct MatchTileArgs {
-    const uint16_t* a;  // n_a x K (fp16 or bf16 bits), row stride K
-    const uint16_t* b;  // n_b x K
-    int n_a, n_b, K;
-    const int* norm_a;  // DIST_BF16: |a|^2 per row
-    const int* norm_b;
-    Cand* row_part;     // [n_a][n_tiles_b]
-    Cand* col_part;     // [n_b][n_tiles_a]
-    int* error;         // set when the MMA wait gives up
+// Stage rows [row0, row0 + 128) of a row-major (n x K) 16-bit matrix into the
+// core-matrix layout with cp.async; rows >= n are zero-filled.  A warp moves
+// 8 rows x 4 chunks per instruction: 64 contiguous bytes per row in global
+// memory, 512 contiguous bytes in shared memory.
+template <int K>
+__device__ __forceinline__ void stage_rows(uint8_t* dst, const uint16_t* src, int row0, int n) {
+    constexpr int KC = K / 8, G = KC / 4;
+    for (int q = threadIdx.x; q < MT * KC; q += MATCH_THREADS) {
+        const int lane = q & 31, blk = q >> 5;
+        const int r = (blk / G) * 8 + (lane & 7), c = (blk % G) * 4 + (lane >> 3);
+        const int gr = row0 + r;
+        const bool valid = gr < n;
+        const uint16_t* s = valid ? src + (size_t)gr * K + c * 8 : src;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst + core_off(r, c, KC))),
+                     "l"(s), "r"(valid ? 16 : 0)
+                     : "memory");
+    }
+}
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    uint32_t done = 0;
+    for (unsigned spins = 0; spins < SPIN_LIMIT; ++spins) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(smem_u32(bar)), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+struct RowScanArgs {
+    const uint16_t* q;   // n_q x K (fp16 or bf16 bits), row stride K
+    const uint16_t* t;   // n_t x K
+    int n_q, n_t;
+    const int* norm_t;   // DIST_BF16: |t|^2 per train row
+    int seg_tiles;       // train tiles per segment (blockIdx.y)
+    Top2* part;          // [n_q][gridDim.y]
+    int* error;          // set when an MMA wait gives up
 };
 
+template <int MODE>
+__device__ __forceinline__ void scan_chunk(const uint32_t (&v)[32], int col0, int lim, int nb_lane, float& k1,
+                                           float& k2, int& i1) {
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+        float key;
+        if (MODE == SIM_F16) {
+            key = __half2float(__float2half_rn(__uint_as_float(v[j])));
+        } else {
+            const float nb = __int_as_float(__shfl_sync(FULL_MASK, nb_lane, j));
+            key = __fsub_rn(2.0f * __uint_as_float(v[j]), nb);
+        }
+        if (j >= lim) key = -INFINITY;
+        k2 = fmaxf(k2, fminf(key, k1));
+        i1 = key > k1 ? col0 + j : i1;
+        k1 = fmaxf(k1, key);
+    }
+}
+
 template <int MODE, int K>
-__global__ void __launch_bounds__(MATCH_THREADS) k_match_tile(const MatchTileArgs args) {
-    constexpr int KC = K / 8;                  // 16-byte chunks per row
+__global__ void __launch_bounds__(MATCH_THREADS) k_match_rows(const RowScanArgs args) {
+    constexpr int KC = K / 8;
     constexpr uint32_t TILE_BYTES = MT * K * 2;
     extern __shared__ __align__(1024) uint8_t smem[];
-    uint8_t* sA = smem;
-    uint8_t* sB = smem + TILE_BYTES;
-    float* sT = reinterpret_cast<float*>(smem);  // reused after the MMA: 128 x 129 floats
-    __shared__ __align__(8) uint64_t mbar;
+    uint8_t* sQ = smem;
+    __shared__ __align__(8) uint64_t mbar[2];
     __shared__ uint32_t tmem_base;
-    __shared__ int s_fail;
 
-    const int tid = threadIdx.x, warp = tid >> 5;
-    const int ta = blockIdx.y, tb = blockIdx.x;
-    const int row0 = ta * MT, col0 = tb * NT;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int q0 = blockIdx.x * MT;
+    const int n_tt = (args.n_t + NT - 1) / NT;
+    const int t_begin = blockIdx.y * args.seg_tiles;
+    const int nt = min(n_tt, t_begin + args.seg_tiles) - t_begin;  // >= 1 by construction
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
-                     "r"(NT));
+                     "r"(2 * NT));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
-        s_fail = 0;
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mbar)), "r"(1));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mbar[0])), "r"(1));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mbar[1])), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    // stage the operand tiles (rows beyond n_a / n_b are zero)
-    for (int q = tid; q < MT * KC; q += MATCH_THREADS) {
-        const int r = q / KC, c = q - r * KC;
-        uint4 va = make_uint4(0, 0, 0, 0), vb = make_uint4(0, 0, 0, 0);
-        if (row0 + r < args.n_a) va = *reinterpret_cast<const uint4*>(args.a + (size_t)(row0 + r) * K + c * 8);
-        if (col0 + r < args.n_b) vb = *reinterpret_cast<const uint4*>(args.b + (size_t)(col0 + r) * K + c * 8);
-        *reinterpret_cast<uint4*>(sA + core_off(r, c, KC)) = va;
-        *reinterpret_cast<uint4*>(sB + core_off(r, c, KC)) = vb;
-    }
-    // make the generic-proxy shared-memory writes visible to the tensor cores
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    stage_rows<K>(sQ, args.q, q0, args.n_q);
+    stage_rows<K>(smem + TILE_BYTES, args.t, t_begin * NT, args.n_t);
+    asm volatile("cp.async.commit_group;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_base;
 
-    if (tid == 0) {
-        const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
-        constexpr uint32_t idesc = umma_idesc(MODE == SIM_F16 ? 0 : 1);
-#pragma unroll
-        for (int s = 0; s < K / 16; ++s) {
-            const uint64_t da = umma_desc(a0 + s * 256, 128, KC * 128);
-            const uint64_t db = umma_desc(b0 + s * 256, 128, KC * 128);
-            const uint32_t acc = s > 0 ? 1u : 0u;
-            asm volatile(
-                "{\n\t.reg .pred p;\n\t"
-                "setp.ne.b32 p, %4, 0;\n\t"
-                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
-                "l"(da), "l"(db), "r"(idesc), "r"(acc));
-        }
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-            smem_u32(&mbar)));
-    }
-    // bounded wait for the MMAs (phase 0)
-    {
-        unsigned done = 0, spins = 0;
-        while (!done) {
-            asm volatile(
-                "{\n\t.reg .pred p;\n\t"
-                "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-                "selp.u32 %0, 1, 0, p;\n\t}\n"
-                : "=r"(done)
-                : "r"(smem_u32(&mbar)), "r"(0));
-            if (!done && ++spins > SPIN_LIMIT) {
-                s_fail = 1;
+    float k1 = -INFINITY, k2 = -INFINITY;
+    int i1 = 0x7fffffff;
+    bool fail = false;
+    int issued = 0;  // MMA groups committed
+    for (int it = 0; it <= nt; ++it) {
+        // (1) the MMA of tile it-1 has finished: its train buffer and accumulator are free to read/reuse
+        if (it >= 1) {
+            const bool ok = mbar_wait_bounded(&mbar[(it - 1) & 1], (uint32_t)(((it - 1) >> 1) & 1));
+            if (__syncthreads_or(!ok)) {
+                fail = true;
                 break;
             }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         }
-    }
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    __syncthreads();
-    const bool ok = (s_fail == 0);
-    if (!ok && tid == 0) atomicExch(args.error, 1);
-
-    // epilogue: thread = tile row (TMEM lane 32*warp + lane)
-    const int row = row0 + tid;
-    Cand rc = cand_empty();
-    const int na_r = (MODE == DIST_BF16 && row < args.n_a) ? args.norm_a[row] : 0;
+        // (2) prefetch train tile it+1 into the buffer tile it-1 used
+        if (it + 1 < nt) stage_rows<K>(smem + (1 + ((it + 1) & 1)) * TILE_BYTES, args.t, (t_begin + it + 1) * NT, args.n_t);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        // (3) tile it is staged: issue its MMAs into accumulator it&1
+        if (it < nt) {
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncthreads();
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            if (tid == 0) {
+                const uint32_t a0 = smem_u32(sQ), b0 = smem_u32(smem + (1 + (it & 1)) * TILE_BYTES);
+                const uint32_t d = tmem + (uint32_t)((it & 1) * NT);
+                constexpr uint32_t idesc = umma_idesc(MODE == SIM_F16 ? 0 : 1);
 #pragma unroll
-    for (int chunk = 0; chunk < NT / 32; ++chunk) {
-        uint32_t v[32];
-        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(chunk * 32);
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-            "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
-              "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
-              "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
-              "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-            : "r"(taddr));
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-        for (int j = 0; j < 32; ++j) {
-            const int col = col0 + chunk * 32 + j;
-            float key;
-            if (MODE == SIM_F16) {
-                key = __half2float(__float2half_rn(__uint_as_float(v[j])));
-            } else {
-                const int dot = (int)__uint_as_float(v[j]);
-                const int nb = col < args.n_b ? args.norm_b[col] : 0;
-                key = -(float)(na_r + nb - 2 * dot);
+                for (int s = 0; s < K / 16; ++s) {
+                    const uint64_t da = umma_desc(a0 + s * 256, 128, KC * 128);
+                    const uint64_t db = umma_desc(b0 + s * 256, 128, KC * 128);
+                    const uint32_t acc = s > 0 ? 1u : 0u;
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\t"
+                        "setp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+                        "l"(da), "l"(db), "r"(idesc), "r"(acc));
+                }
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 smem_u32(&mbar[it & 1]))
+                             : "memory");
             }
-            if (!ok) key = -INFINITY;
-            sT[tid * (NT + 1) + chunk * 32 + j] = key;
-            if (col < args.n_b) cand_push(rc, key, col);
+            ++issued;
+        }
+        // (4) reduce tile it-1 (overlaps the MMA of tile it)
+        if (it >= 1) {
+            const int tcol0 = (t_begin + it - 1) * NT;
+            const int lim_tile = args.n_t - tcol0;
+#pragma unroll
+            for (int chunk = 0; chunk < NT / 32; ++chunk) {
+                int nb_lane = 0;
+                if (MODE == DIST_BF16) {
+                    const int c = tcol0 + chunk * 32 + lane;
+                    nb_lane = __float_as_int((float)(c < args.n_t ? args.norm_t[c] : 0));
+                }
+                uint32_t v[32];
+                const uint32_t taddr =
+                    tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(((it - 1) & 1) * NT + chunk * 32);
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                    "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                    "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                      "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                      "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]),
+                      "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]),
+                      "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                    : "r"(taddr));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                scan_chunk<MODE>(v, tcol0 + chunk * 32, lim_tile - chunk * 32, nb_lane, k1, k2, i1);
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         }
     }
-    const int n_tb = gridDim.x, n_ta = gridDim.y;
-    if (row < args.n_a) args.row_part[(size_t)row * n_tb + tb] = rc;
-    __syncthreads();
-    // column candidates: thread = tile column
-    {
-        const int col = col0 + tid;
-        Cand cc = cand_empty();
-        const int nrows = min(MT, args.n_a - row0);
-        for (int r = 0; r < nrows; ++r) cand_push(cc, sT[r * (NT + 1) + tid], row0 + r);
-        if (col < args.n_b) args.col_part[(size_t)col * n_ta + ta] = cc;
+    if (fail) {
+        // give the MMAs still in flight a bounded chance to finish before the
+        // shared memory and tensor memory they use are released
+        if (tid == 0) atomicExch(args.error, 1);
+        for (int g = 0; g < issued; ++g) mbar_wait_bounded(&mbar[g & 1], (uint32_t)((g >> 1) & 1));
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    const int row = q0 + tid;
+    if (!fail && row < args.n_q) {
+        Top2 r;
+        r.k1 = k1;
+        r.k2 = k2;
+        r.i1 = i1;
+        r.pad = 0;
+        args.part[(size_t)row * gridDim.y + blockIdx.y] = r;
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NT));
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * NT));
 }
 
-// Merge per-tile candidates of one side, ratio test.  best/pass per element.
+// Merge the segments of one scan (in index order), ratio test.
 template <int MODE>
-__global__ void k_match_merge(const Cand* __restrict__ part, int n, int ntiles, float ratio_sq, int* __restrict__ best,
-                              int* __restrict__ pass, float* __restrict__ dist) {
+__global__ void k_match_merge(const Top2* __restrict__ part, int n, int nseg, float ratio_sq,
+                              const int* __restrict__ norm_q, int* __restrict__ best, int* __restrict__ pass,
+                              float* __restrict__ dist) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    Cand c = cand_empty();
-    for (int t = 0; t < ntiles; ++t) {
-        const Cand p = part[(size_t)i * ntiles + t];
-        if (p.i1 != 0x7fffffff) cand_push(c, p.k1, p.i1);
-        if (p.i2 != 0x7fffffff) cand_push(c, p.k2, p.i2);
+    float k1 = -INFINITY, k2 = -INFINITY;
+    int i1 = 0x7fffffff;
+    for (int s = 0; s < nseg; ++s) {
+        const Top2 p = part[(size_t)i * nseg + s];
+        k2 = fmaxf(fmaxf(k2, p.k2), fminf(p.k1, k1));
+        i1 = p.k1 > k1 ? p.i1 : i1;
+        k1 = fmaxf(k1, p.k1);
     }
     int ok = 0;
     float d = 0.0f;
-    if (c.i2 != 0x7fffffff) {
+    if (k2 > -INFINITY) {
         if (MODE == SIM_F16) {
             // pysift/core.py:2676-2680 (float32)
-            float db = 2.0f - 2.0f * c.k1;
-            float ds = 2.0f - 2.0f * c.k2;
+            float db = 2.0f - 2.0f * k1;
+            float ds = 2.0f - 2.0f * k2;
             db = db < 0.0f ? 0.0f : db;
             ds = ds < 0.0f ? 0.0f : ds;
             ok = (ds > 1e-10f) && (db < ratio_sq * ds);
             d = sqrtf(db);
         } else {
-            const double d1 = -(double)c.k1, d2 = -(double)c.k2;  // exact integers
+            const double na = (double)norm_q[i];
+            const double d1 = na - (double)k1, d2 = na - (double)k2;  // exact integers
             ok = (d2 > 0.0) && (d1 < (double)ratio_sq * d2);
             d = sqrtf((float)d1);
         }
     }
-    best[i] = c.i1 == 0x7fffffff ? -1 : c.i1;
+    best[i] = (k1 > -INFINITY) ? i1 : -1;
     pass[i] = ok;
     if (dist) dist[i] = d;
 }
@@ -302,20 +342,42 @@ __global__ void k_row_norms_u8(const uint8_t* __restrict__ d, int n, int D, int*
     if (threadIdx.x == 0) norms[i] = s;
 }
 
+static int sm_count() {
+    int dev = 0, n = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return 148;
+    return n > 0 ? n : 148;
+}
+
+// Segments of the train side so that about two CTAs per SM are busy.
+static void scan_split(int n_q, int n_t, int& nseg, int& seg_tiles) {
+    const int n_qb = ceil_div(n_q, MT), n_tt = ceil_div(n_t, NT);
+    int want = ceil_div(2 * sm_count(), n_qb);
+    want = std::max(1, std::min(want, n_tt));
+    seg_tiles = ceil_div(n_tt, want);
+    nseg = ceil_div(n_tt, seg_tiles);
+}
+
 template <int MODE, int K>
-static int launch_tiles(const MatchTileArgs& a, cudaStream_t st) {
-    // operand tiles, later reused for the 128 x 129 float key tile
-    const size_t smem_launch = std::max(2 * (size_t)MT * K * 2, (size_t)MT * (NT + 1) * 4);
-    PYSIFT_CUDA_TRY(cudaFuncSetAttribute(k_match_tile<MODE, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+static int launch_scan(const RowScanArgs& a, int nseg, cudaStream_t st) {
+    // query block + two train buffers; at least 80 KB so that no more than two
+    // CTAs (2 x 256 tensor-memory columns) share an SM
+    const size_t smem_launch = std::max((size_t)3 * MT * K * 2, (size_t)80 * 1024);
+    PYSIFT_CUDA_TRY(cudaFuncSetAttribute(k_match_rows<MODE, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem_launch));
-    dim3 grid(ceil_div(a.n_b, NT), ceil_div(a.n_a, MT));
-    k_match_tile<MODE, K><<<grid, MATCH_THREADS, smem_launch, st>>>(a);
-    PYSIFT_LAUNCH_CHECK("k_match_tile");
+    dim3 grid(ceil_div(a.n_q, MT), nseg);
+    k_match_rows<MODE, K><<<grid, MATCH_THREADS, smem_launch, st>>>(a);
+    PYSIFT_LAUNCH_CHECK("k_match_rows");
     return PYSIFT_OK;
 }
 
+template <int MODE>
+static int launch_scan_k(const RowScanArgs& a, int K, int nseg, cudaStream_t st) {
+    return K == 64 ? launch_scan<MODE, 64>(a, nseg, st) : launch_scan<MODE, 128>(a, nseg, st);
+}
+
 struct MatchLayout {
-    size_t off_rowp, off_colp, off_fbest, off_fpass, off_fdist, off_bbest, off_bpass, off_bdist, off_err;
+    size_t off_fpart, off_bpart, off_fbest, off_fpass, off_fdist, off_bbest, off_bpass, off_bdist, off_err;
     size_t off_na, off_nb, off_bfa, off_bfb;
     size_t total;
 };
@@ -328,9 +390,9 @@ static MatchLayout match_layout(int n1, int n2, int D, bool exact) {
         off = align_up(off + bytes, 256);
         return r;
     };
-    const size_t ta = ceil_div(n1, MT), tb = ceil_div(n2, NT);
-    l.off_rowp = take((size_t)n1 * tb * sizeof(Cand));
-    l.off_colp = take((size_t)n2 * ta * sizeof(Cand));
+    // segments never exceed the tiles of the other side
+    l.off_fpart = take((size_t)n1 * ceil_div(n2, NT) * sizeof(Top2));
+    l.off_bpart = take((size_t)n2 * ceil_div(n1, MT) * sizeof(Top2));
     l.off_fbest = take((size_t)n1 * 4);
     l.off_fpass = take((size_t)n1 * 4);
     l.off_fdist = take((size_t)n1 * 4);
@@ -357,43 +419,41 @@ static T* wsp(void* ws, size_t off) {
 static int run_match(int mode, const uint16_t* a, int n1, const uint16_t* b, int n2, int D, float ratio_sq,
                      const MatchLayout& l, void* ws, int* fbest_out, int* fpass_out, int* bbest_out, int* bpass_out,
                      int32_t* pairs, float* pdist, int32_t* count, cudaStream_t st) {
-    MatchTileArgs ta;
-    ta.a = a;
-    ta.b = b;
-    ta.n_a = n1;
-    ta.n_b = n2;
-    ta.K = D;
-    ta.norm_a = mode == DIST_BF16 ? wsp<int>(ws, l.off_na) : nullptr;
-    ta.norm_b = mode == DIST_BF16 ? wsp<int>(ws, l.off_nb) : nullptr;
-    ta.row_part = wsp<Cand>(ws, l.off_rowp);
-    ta.col_part = wsp<Cand>(ws, l.off_colp);
-    ta.error = wsp<int>(ws, l.off_err);
-    PYSIFT_CUDA_TRY(cudaMemsetAsync(ta.error, 0, 4, st));
-    int rc;
-    if (mode == SIM_F16)
-        rc = (D == 64) ? launch_tiles<SIM_F16, 64>(ta, st) : launch_tiles<SIM_F16, 128>(ta, st);
-    else
-        rc = (D == 64) ? launch_tiles<DIST_BF16, 64>(ta, st) : launch_tiles<DIST_BF16, 128>(ta, st);
-    if (rc) return rc;
+    int* err = wsp<int>(ws, l.off_err);
+    PYSIFT_CUDA_TRY(cudaMemsetAsync(err, 0, 4, st));
+    const int* na = mode == DIST_BF16 ? wsp<int>(ws, l.off_na) : nullptr;
+    const int* nb = mode == DIST_BF16 ? wsp<int>(ws, l.off_nb) : nullptr;
     int* fbest = fbest_out ? fbest_out : wsp<int>(ws, l.off_fbest);
     int* fpass = fpass_out ? fpass_out : wsp<int>(ws, l.off_fpass);
     int* bbest = bbest_out ? bbest_out : wsp<int>(ws, l.off_bbest);
     int* bpass = bpass_out ? bpass_out : wsp<int>(ws, l.off_bpass);
     float* fdist = wsp<float>(ws, l.off_fdist);
     float* bdist = wsp<float>(ws, l.off_bdist);
-    const int ntb = ceil_div(n2, NT), nta = ceil_div(n1, MT);
-    if (mode == SIM_F16) {
-        k_match_merge<SIM_F16><<<ceil_div(n1, 256), 256, 0, st>>>(ta.row_part, n1, ntb, ratio_sq, fbest, fpass, fdist);
+    for (int dir = 0; dir < 2; ++dir) {
+        RowScanArgs s;
+        s.q = dir == 0 ? a : b;
+        s.t = dir == 0 ? b : a;
+        s.n_q = dir == 0 ? n1 : n2;
+        s.n_t = dir == 0 ? n2 : n1;
+        s.norm_t = dir == 0 ? nb : na;
+        s.part = wsp<Top2>(ws, dir == 0 ? l.off_fpart : l.off_bpart);
+        s.error = err;
+        int nseg;
+        scan_split(s.n_q, s.n_t, nseg, s.seg_tiles);
+        const int rc = mode == SIM_F16 ? launch_scan_k<SIM_F16>(s, D, nseg, st) : launch_scan_k<DIST_BF16>(s, D, nseg, st);
+        if (rc) return rc;
+        const int* nq = dir == 0 ? na : nb;
+        int* best = dir == 0 ? fbest : bbest;
+        int* pass = dir == 0 ? fpass : bpass;
+        float* dist = dir == 0 ? fdist : bdist;
+        if (mode == SIM_F16)
+            k_match_merge<SIM_F16><<<ceil_div(s.n_q, 256), 256, 0, st>>>(s.part, s.n_q, nseg, ratio_sq, nq, best, pass,
+                                                                       dist);
+        else
+            k_match_merge<DIST_BF16><<<ceil_div(s.n_q, 256), 256, 0, st>>>(s.part, s.n_q, nseg, ratio_sq, nq, best,
+                                                                         pass, dist);
         PYSIFT_LAUNCH_CHECK("k_match_merge");
-        k_match_merge<SIM_F16><<<ceil_div(n2, 256), 256, 0, st>>>(ta.col_part, n2, nta, ratio_sq, bbest, bpass, bdist);
-    } else {
-        k_match_merge<DIST_BF16><<<ceil_div(n1, 256), 256, 0, st>>>(ta.row_part, n1, ntb, ratio_sq, fbest, fpass,
-                                                                    fdist);
-        PYSIFT_LAUNCH_CHECK("k_match_merge");
-        k_match_merge<DIST_BF16><<<ceil_div(n2, 256), 256, 0, st>>>(ta.col_part, n2, nta, ratio_sq, bbest, bpass,
-                                                                    bdist);
     }
-    PYSIFT_LAUNCH_CHECK("k_match_merge");
     k_match_mutual<<<1, 1024, 0, st>>>(fbest, fpass, fdist, bbest, bpass, n1, reinterpret_cast<int2*>(pairs), pdist,
                                        count);
     PYSIFT_LAUNCH_CHECK("k_match_mutual");

@@ -276,11 +276,108 @@ __global__ void __launch_bounds__(256) k_ransac_hyp(const RansacArgs a) {
     }
 }
 
+// Smallest-eigenvalue eigenvector of the symmetric 9x9 M (row-major, shared
+// memory) by parallel Jacobi, run by warp 0 (V: shared 9x9 eigenvectors).
+// Round-robin ordering of the 36 index pairs: round r = 0..8 rotates the 4
+// disjoint pairs {(r+i) mod 9, (r-i) mod 9}, i = 1..4 (p < q); index r rests.
+// The 4 angles of a round come from the matrix at the start of the round,
+// then all column rotations are applied, then all row rotations (exact, as
+// the pairs are disjoint).  After sweep 3 a rotation whose off-diagonal
+// element is negligible (|a_pp| + 100|a_pq| == |a_pp| and the same for a_qq)
+// zeroes it instead; sweeps stop once every off-diagonal element is 0, at 15
+// at most.  Returns the index of the smallest diagonal element (lowest on ties).
+__device__ int jacobi9_smallest(double (*M)[9], double (*V)[9]) {
+    __shared__ double s_cs[4][2];
+    __shared__ int s_pq[4][2];
+    __shared__ int s_act[4];
+    __shared__ int s_best;
+    const int lane = threadIdx.x & 31;
+    if (threadIdx.x < 32) {
+        for (int it = lane; it < 81; it += 32) V[it / 9][it % 9] = (it / 9 == it % 9) ? 1.0 : 0.0;
+        __syncwarp();
+        for (int sweep = 0; sweep < 15; ++sweep) {
+            // every upper off-diagonal element exactly zero -> converged
+            bool nz = false;
+            for (int it = lane; it < 81; it += 32) {
+                const int r = it / 9, c = it % 9;
+                if (c > r && M[r][c] != 0.0) nz = true;
+            }
+            if (!__any_sync(FULL_MASK, nz)) break;
+            for (int rnd = 0; rnd < 9; ++rnd) {
+                if (lane < 4) {
+                    const int a = (rnd + lane + 1) % 9, bb = (rnd + 9 - lane - 1) % 9;
+                    const int p = a < bb ? a : bb, q = a < bb ? bb : a;
+                    s_pq[lane][0] = p;
+                    s_pq[lane][1] = q;
+                    const double apq = M[p][q];
+                    int act = 0;
+                    if (apq != 0.0) {
+                        const double app = M[p][p], aqq = M[q][q];
+                        const double g = 100.0 * fabs(apq);
+                        if (sweep > 3 && fabs(app) + g == fabs(app) && fabs(aqq) + g == fabs(aqq)) {
+                            M[p][q] = 0.0;
+                            M[q][p] = 0.0;
+                        } else {
+                            const double theta = (aqq - app) / (2.0 * apq);
+                            const double tt = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                            const double c = 1.0 / sqrt(tt * tt + 1.0);
+                            s_cs[lane][0] = c;
+                            s_cs[lane][1] = tt * c;
+                            act = 1;
+                        }
+                    }
+                    s_act[lane] = act;
+                }
+                __syncwarp();
+                // column rotations: item = (pair j, row k)
+                for (int it = lane; it < 36; it += 32) {
+                    const int j = it / 9, k = it % 9;
+                    if (s_act[j]) {
+                        const int p = s_pq[j][0], q = s_pq[j][1];
+                        const double c = s_cs[j][0], s = s_cs[j][1];
+                        const double mkp = M[k][p], mkq = M[k][q];
+                        M[k][p] = c * mkp - s * mkq;
+                        M[k][q] = s * mkp + c * mkq;
+                    }
+                }
+                __syncwarp();
+                // row rotations and the eigenvector columns
+                for (int it = lane; it < 36; it += 32) {
+                    const int j = it / 9, k = it % 9;
+                    if (s_act[j]) {
+                        const int p = s_pq[j][0], q = s_pq[j][1];
+                        const double c = s_cs[j][0], s = s_cs[j][1];
+                        const double mpk = M[p][k], mqk = M[q][k];
+                        M[p][k] = c * mpk - s * mqk;
+                        M[q][k] = s * mpk + c * mqk;
+                        const double vkp = V[k][p], vkq = V[k][q];
+                        V[k][p] = c * vkp - s * vkq;
+                        V[k][q] = s * vkp + c * vkq;
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        if (lane == 0) {
+            int best = 0;
+            for (int k = 1; k < 9; ++k)
+                if (M[k][k] < M[best][best]) best = k;
+            s_best = best;
+        }
+    }
+    __syncthreads();
+    return s_best;
+}
+
 // Least-squares homography of the points idx[0..m): Hartley normalisation of
-// the subset, A^T A accumulated in a fixed order, cyclic Jacobi, the
-// eigenvector of the smallest eigenvalue, denormalised (pysift/core.py:2959-2981).
+// the subset, A^T A accumulated in a fixed order (contiguous chunks per
+// thread, then a pairwise tree over the RT partials), its smallest-eigenvalue
+// eigenvector by jacobi9_smallest, denormalised (pysift/core.py:2959-2981).
 __device__ void dlt_refit(const double* p1, const double* p2, const int* idx, int m, double* H, double* sh,
                           double* s_M) {
+    constexpr int NB = 9;  // tree sums run 9 at a time
+    __shared__ double s_part[NB][RT];
+    __shared__ double s_Mj[9][9], s_Vj[9][9];
     const Norm n1 = hartley(p1, idx, m, sh);
     const Norm n2 = hartley(p2, idx, m, sh);
     double acc[45];
@@ -294,50 +391,41 @@ __device__ void dlt_refit(const double* p1, const double* p2, const int* idx, in
         const double re[9] = {-x1, -y1, -1.0, 0.0, 0.0, 0.0, x2 * x1, x2 * y1, x2};
         const double ro[9] = {0.0, 0.0, 0.0, -x1, -y1, -1.0, y2 * x1, y2 * y1, y2};
         int t = 0;
+#pragma unroll
         for (int r = 0; r < 9; ++r)
+#pragma unroll
             for (int c = r; c < 9; ++c, ++t) acc[t] = (acc[t] + re[r] * re[c]) + ro[r] * ro[c];
     }
-    for (int t = 0; t < 45; ++t) {
-        const double v = block_tree_sum(acc[t], sh);
-        if (threadIdx.x == 0) s_M[t] = v;
+#pragma unroll
+    for (int t0 = 0; t0 < 45; t0 += NB) {
+#pragma unroll
+        for (int u = 0; u < NB; ++u) s_part[u][threadIdx.x] = acc[t0 + u];
+        __syncthreads();
+        for (int s = RT / 2; s > 0; s >>= 1) {
+            if ((int)threadIdx.x < s)
+#pragma unroll
+                for (int u = 0; u < NB; ++u) s_part[u][threadIdx.x] = s_part[u][threadIdx.x] + s_part[u][threadIdx.x + s];
+            __syncthreads();
+        }
+        if (threadIdx.x < NB) s_M[t0 + threadIdx.x] = s_part[threadIdx.x][0];
+        __syncthreads();
+    }
+    for (int it = threadIdx.x; it < 45; it += RT) {
+        // upper-triangle index it -> (r, c)
+        int r = 0, rem = it;
+        while (rem >= 9 - r) {
+            rem -= 9 - r;
+            ++r;
+        }
+        const int c = r + rem;
+        s_Mj[r][c] = s_M[it];
+        s_Mj[c][r] = s_M[it];
     }
     __syncthreads();
+    const int best = jacobi9_smallest(s_Mj, s_Vj);
     if (threadIdx.x == 0) {
-        double M[9][9], V[9][9];
-        int t = 0;
-        for (int r = 0; r < 9; ++r)
-            for (int c = r; c < 9; ++c, ++t) M[r][c] = M[c][r] = s_M[t];
-        for (int r = 0; r < 9; ++r)
-            for (int c = 0; c < 9; ++c) V[r][c] = (r == c) ? 1.0 : 0.0;
-        for (int sweep = 0; sweep < 15; ++sweep)
-            for (int p = 0; p < 8; ++p)
-                for (int q = p + 1; q < 9; ++q) {
-                    const double apq = M[p][q];
-                    if (apq == 0.0) continue;
-                    const double theta = (M[q][q] - M[p][p]) / (2.0 * apq);
-                    const double tt = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
-                    const double c = 1.0 / sqrt(tt * tt + 1.0), s = tt * c;
-                    for (int k = 0; k < 9; ++k) {
-                        const double mkp = M[k][p], mkq = M[k][q];
-                        M[k][p] = c * mkp - s * mkq;
-                        M[k][q] = s * mkp + c * mkq;
-                    }
-                    for (int k = 0; k < 9; ++k) {
-                        const double mpk = M[p][k], mqk = M[q][k];
-                        M[p][k] = c * mpk - s * mqk;
-                        M[q][k] = s * mpk + c * mqk;
-                    }
-                    for (int k = 0; k < 9; ++k) {
-                        const double vkp = V[k][p], vkq = V[k][q];
-                        V[k][p] = c * vkp - s * vkq;
-                        V[k][q] = s * vkp + c * vkq;
-                    }
-                }
-        int best = 0;
-        for (int k = 1; k < 9; ++k)
-            if (M[k][k] < M[best][best]) best = k;
         double hn[9], T1[9], T2inv[9];
-        for (int k = 0; k < 9; ++k) hn[k] = V[k][best];
+        for (int k = 0; k < 9; ++k) hn[k] = s_Vj[k][best];
         norm_mats(n1, n2, T1, T2inv);
         double t9[9];
         mat3_mul(T2inv, hn, t9);
@@ -483,27 +571,72 @@ __global__ void k_l2_normalize(const float* __restrict__ in, int n, int D, float
     for (int g = 0; g < D / 32; ++g) out[(size_t)row * D + g * 32 + lane] = v[g] / den;
 }
 
-// one warp per row: project (D -> P), normalise, fp16
-__global__ void k_pca_project_f16(const float* __restrict__ in, int n, int D, const float* __restrict__ mean,
-                                  const float* __restrict__ proj, int P, uint16_t* __restrict__ out) {
-    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (row >= n) return;
-    const float* r = in + (size_t)row * D;
-    float pv[4];
-    for (int g = 0; g < P / 32; ++g) {
-        const int c = g * 32 + lane;
-        float acc = 0.0f;
-        for (int k = 0; k < D; ++k) acc = fmaf(r[k] - mean[k], proj[(size_t)k * P + c], acc);
-        pv[g] = acc;
+// Projection (D -> P), normalisation and fp16 rounding of 64-row blocks.
+// Each output is the fmaf chain over k ascending of (x_k - mean_k) * proj[k][c];
+// a thread computes a 4 x 4 register block of outputs from shared-memory
+// copies of the centred rows and of the projection.  Row norms sum squares
+// in groups of 32 outputs (warp tree 16, 8, 4, 2, 1) and the groups in order.
+constexpr int PJ_ROWS = 64;
+constexpr int PJ_T = 256;
+
+template <int D, int P>
+__global__ void __launch_bounds__(PJ_T) k_pca_project_f16(const float* __restrict__ in, int n,
+                                                         const float* __restrict__ mean, const float* __restrict__ proj,
+                                                         uint16_t* __restrict__ out) {
+    extern __shared__ float pj_smem[];
+    float* s_proj = pj_smem;                  // D x P
+    float* s_x = s_proj + D * P;              // PJ_ROWS x (D + 1), centred
+    float* s_y = s_x + PJ_ROWS * (D + 1);     // PJ_ROWS x (P + 1), projected
+    const int tid = threadIdx.x;
+    const int r0 = blockIdx.x * PJ_ROWS;
+    for (int q = tid; q < D * P; q += PJ_T) s_proj[q] = proj[q];
+    for (int q = tid; q < PJ_ROWS * D; q += PJ_T) {
+        const int r = q / D, k = q - r * D;
+        s_x[r * (D + 1) + k] = (r0 + r < n) ? in[(size_t)(r0 + r) * D + k] - mean[k] : 0.0f;
     }
-    float ss = 0.0f;
-    for (int g = 0; g < P / 32; ++g) {
-        const float w = warp_tree(pv[g] * pv[g]);
-        ss = (g == 0) ? w : ss + w;
+    __syncthreads();
+    constexpr int CT = P / 4;                // threads along the outputs
+    constexpr int RT_ = PJ_T / CT;           // threads along the rows
+    constexpr int RPT = PJ_ROWS / RT_;       // rows per thread
+    const int tc = tid % CT, tr = tid / CT;
+    float acc[RPT][4];
+#pragma unroll
+    for (int i = 0; i < RPT; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
+#pragma unroll 4
+    for (int k = 0; k < D; ++k) {
+        float pv[4], xv[RPT];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) pv[j] = s_proj[k * P + tc + CT * j];
+#pragma unroll
+        for (int i = 0; i < RPT; ++i) xv[i] = s_x[(tr + RT_ * i) * (D + 1) + k];
+#pragma unroll
+        for (int i = 0; i < RPT; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(xv[i], pv[j], acc[i][j]);
     }
-    const float den = sqrtf(ss) + 1e-7f;
-    for (int g = 0; g < P / 32; ++g)
-        out[(size_t)row * P + g * 32 + lane] = __half_as_ushort(__float2half_rn(pv[g] / den));
+#pragma unroll
+    for (int i = 0; i < RPT; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) s_y[(tr + RT_ * i) * (P + 1) + tc + CT * j] = acc[i][j];
+    __syncthreads();
+    const int lane = tid & 31, warp = tid >> 5;
+    for (int r = warp; r < PJ_ROWS; r += PJ_T / 32) {
+        if (r0 + r >= n) break;
+        float pvv[P / 32];
+        float ss = 0.0f;
+#pragma unroll
+        for (int g = 0; g < P / 32; ++g) {
+            pvv[g] = s_y[r * (P + 1) + g * 32 + lane];
+            const float w = warp_tree(pvv[g] * pvv[g]);
+            ss = (g == 0) ? w : ss + w;
+        }
+        const float den = sqrtf(ss) + 1e-7f;
+#pragma unroll
+        for (int g = 0; g < P / 32; ++g)
+            out[(size_t)(r0 + r) * P + g * 32 + lane] = __half_as_ushort(__float2half_rn(pvv[g] / den));
+    }
 }
 
 __global__ void k_to_f16(const float* __restrict__ in, size_t n, uint16_t* __restrict__ out) {
@@ -511,27 +644,66 @@ __global__ void k_to_f16(const float* __restrict__ in, size_t n, uint16_t* __res
     if (i < n) out[i] = __half_as_ushort(__float2half_rn(in[i]));
 }
 
-// PCA statistics of the stacked normalised sets: mean (float64 sequential sum
-// over rows / n, rounded to float32) and covariance (float64 sequential sum of
-// products of the float32 centred values / n).
-__global__ void k_pca_mean(const float* __restrict__ x, int n, int D, float* __restrict__ mean) {
+// PCA statistics of the stacked normalised sets, in float64 over fixed
+// 128-row chunks: each chunk is summed sequentially, then the chunk partials
+// in chunk order.  mean = (sum of rows) / n, rounded to float32; covariance =
+// (sum of products of the float32 centred values) / n.
+constexpr int PCA_CHUNK = 128;
+
+__global__ void k_pca_mean_part(const float* __restrict__ x, int n, int D, double* __restrict__ part) {
+    const int k = threadIdx.x, c = blockIdx.x;
+    if (k >= D) return;
+    const int i0 = c * PCA_CHUNK, i1 = min(n, i0 + PCA_CHUNK);
+    double s = 0.0;
+    for (int i = i0; i < i1; ++i) s = s + (double)x[(size_t)i * D + k];
+    part[(size_t)c * D + k] = s;
+}
+
+__global__ void k_pca_mean_final(const double* __restrict__ part, int nchunks, int n, int D, float* __restrict__ mean) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= D) return;
     double s = 0.0;
-    for (int i = 0; i < n; ++i) s = s + (double)x[(size_t)i * D + k];
+    for (int c = 0; c < nchunks; ++c) s = s + part[(size_t)c * D + k];
     mean[k] = (float)(s / (double)n);
 }
 
-__global__ void k_pca_cov(const float* __restrict__ x, int n, int D, const float* __restrict__ mean,
-                          double* __restrict__ cov) {
-    const int k = blockIdx.y, l = blockIdx.x * blockDim.x + threadIdx.x;
-    if (l >= D || l < k) return;
-    double s = 0.0;
-    const float mk = mean[k], ml = mean[l];
-    for (int i = 0; i < n; ++i) {
-        const double a = (double)(x[(size_t)i * D + k] - mk), b = (double)(x[(size_t)i * D + l] - ml);
-        s = s + a * b;
+// block = (chunk, 32 x 32 tile of the covariance); thread = 4 entries
+__global__ void __launch_bounds__(256) k_pca_cov_part(const float* __restrict__ x, int n, int D,
+                                                     const float* __restrict__ mean, double* __restrict__ part) {
+    __shared__ float s_a[PCA_CHUNK][33], s_b[PCA_CHUNK][33];
+    const int c = blockIdx.x, tk = blockIdx.y, tl = blockIdx.z;
+    if (tl < tk) return;
+    const int i0 = c * PCA_CHUNK, m = min(n - i0, PCA_CHUNK);
+    for (int q = threadIdx.x; q < PCA_CHUNK * 32; q += 256) {
+        const int i = q >> 5, j = q & 31;
+        const int k = tk * 32 + j, l = tl * 32 + j;
+        s_a[i][j] = (i < m && k < D) ? x[(size_t)(i0 + i) * D + k] - mean[k] : 0.0f;
+        s_b[i][j] = (i < m && l < D) ? x[(size_t)(i0 + i) * D + l] - mean[l] : 0.0f;
     }
+    __syncthreads();
+    const int jl = threadIdx.x & 31, jk0 = threadIdx.x >> 5;  // entries (jk0 + 8 u, jl)
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int i = 0; i < m; ++i) {
+        const double bv = (double)s_b[i][jl];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) s[u] = s[u] + (double)s_a[i][jk0 + 8 * u] * bv;
+    }
+    const size_t DD = (size_t)D * D;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int k = tk * 32 + jk0 + 8 * u, l = tl * 32 + jl;
+        if (k < D && l < D) part[(size_t)c * DD + (size_t)k * D + l] = s[u];
+    }
+}
+
+__global__ void k_pca_cov_final(const double* __restrict__ part, int nchunks, int n, int D, double* __restrict__ cov) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= D * D) return;
+    const int k = q / D, l = q - k * D;
+    if (l < k) return;
+    const size_t DD = (size_t)D * D;
+    double s = 0.0;
+    for (int c = 0; c < nchunks; ++c) s = s + part[(size_t)c * DD + q];
     const double v = s / (double)n;
     cov[(size_t)k * D + l] = v;
     cov[(size_t)l * D + k] = v;
@@ -557,6 +729,15 @@ static RansacLayout ransac_layout(int n, int n_hyp) {
     l.off_idx = take((size_t)n * sizeof(int));
     l.total = off;
     return l;
+}
+
+template <int D, int P>
+static int launch_project(const float* x, int n, const float* mean, const float* proj, uint16_t* out, cudaStream_t st) {
+    const size_t smem = ((size_t)D * P + (size_t)PJ_ROWS * (D + 1) + (size_t)PJ_ROWS * (P + 1)) * sizeof(float);
+    PYSIFT_CUDA_TRY(cudaFuncSetAttribute(k_pca_project_f16<D, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_pca_project_f16<D, P><<<ceil_div(n, PJ_ROWS), PJ_T, smem, st>>>(x, n, mean, proj, out);
+    PYSIFT_LAUNCH_CHECK("k_pca_project_f16");
+    return PYSIFT_OK;
 }
 
 }  // namespace pysift
@@ -653,25 +834,49 @@ int pysift_l2_normalize_rows(const float* in, int32_t n, int32_t D, float* out, 
     return PYSIFT_OK;
 }
 
-int pysift_pca_stats(const float* x, int32_t n, int32_t D, float* mean, double* cov, pysift_stream_t stream) {
-    PYSIFT_CHECK_ARG(x && mean && cov && n >= 1 && D > 0 && D <= 1024, "bad arguments");
+int pysift_pca_workspace_size(int32_t n, int32_t D, size_t* bytes) {
+    PYSIFT_CHECK_ARG(bytes && n >= 1 && D > 0 && D <= 1024, "bad arguments");
+    const size_t nchunks = (size_t)ceil_div(n, PCA_CHUNK);
+    *bytes = nchunks * (size_t)D * sizeof(double) + nchunks * (size_t)D * D * sizeof(double);
+    return PYSIFT_OK;
+}
+
+int pysift_pca_stats(const float* x, int32_t n, int32_t D, void* workspace, size_t workspace_bytes, float* mean,
+                     double* cov, pysift_stream_t stream) {
+    PYSIFT_CHECK_ARG(x && mean && cov && workspace && n >= 1 && D > 0 && D <= 1024, "bad arguments");
+    size_t need = 0;
+    pysift_pca_workspace_size(n, D, &need);
+    if (workspace_bytes < need) {
+        set_error("workspace %zu bytes < required %zu", workspace_bytes, need);
+        return PYSIFT_ERR_WORKSPACE;
+    }
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    k_pca_mean<<<ceil_div(D, 128), 128, 0, st>>>(x, n, D, mean);
-    PYSIFT_LAUNCH_CHECK("k_pca_mean");
-    k_pca_cov<<<dim3(ceil_div(D, 128), D), 128, 0, st>>>(x, n, D, mean, cov);
-    PYSIFT_LAUNCH_CHECK("k_pca_cov");
+    const int nchunks = ceil_div(n, PCA_CHUNK);
+    double* mpart = static_cast<double*>(workspace);
+    double* cpart = mpart + (size_t)nchunks * D;
+    k_pca_mean_part<<<nchunks, ceil_div(D, 32) * 32, 0, st>>>(x, n, D, mpart);
+    PYSIFT_LAUNCH_CHECK("k_pca_mean_part");
+    k_pca_mean_final<<<ceil_div(D, 128), 128, 0, st>>>(mpart, nchunks, n, D, mean);
+    PYSIFT_LAUNCH_CHECK("k_pca_mean_final");
+    k_pca_cov_part<<<dim3(nchunks, ceil_div(D, 32), ceil_div(D, 32)), 256, 0, st>>>(x, n, D, mean, cpart);
+    PYSIFT_LAUNCH_CHECK("k_pca_cov_part");
+    k_pca_cov_final<<<ceil_div(D * D, 256), 256, 0, st>>>(cpart, nchunks, n, D, cov);
+    PYSIFT_LAUNCH_CHECK("k_pca_cov_final");
     return PYSIFT_OK;
 }
 
 int pysift_pca_project_f16(const float* x, int32_t n, int32_t D, const float* mean, const float* proj, int32_t P,
                            uint16_t* out, pysift_stream_t stream) {
-    PYSIFT_CHECK_ARG(x && mean && proj && out && n >= 0 && D > 0 && P > 0 && P <= 128 && P % 32 == 0,
-                     "bad arguments");
+    PYSIFT_CHECK_ARG(x && mean && proj && out && n >= 0, "bad arguments");
+    PYSIFT_CHECK_ARG((D == 128 || D == 64) && (P == 32 || P == 64 || P == 128) && P <= D,
+                     "unsupported sizes (D in {64, 128}, P in {32, 64, 128}, P <= D)");
     if (n == 0) return PYSIFT_OK;
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    k_pca_project_f16<<<ceil_div(n * 32, 256), 256, 0, st>>>(x, n, D, mean, proj, P, out);
-    PYSIFT_LAUNCH_CHECK("k_pca_project_f16");
-    return PYSIFT_OK;
+    if (D == 128 && P == 64) return launch_project<128, 64>(x, n, mean, proj, out, st);
+    if (D == 128 && P == 32) return launch_project<128, 32>(x, n, mean, proj, out, st);
+    if (D == 128 && P == 128) return launch_project<128, 128>(x, n, mean, proj, out, st);
+    if (D == 64 && P == 64) return launch_project<64, 64>(x, n, mean, proj, out, st);
+    return launch_project<64, 32>(x, n, mean, proj, out, st);
 }
 
 int pysift_to_f16(const float* in, int64_t n, uint16_t* out, pysift_stream_t stream) {

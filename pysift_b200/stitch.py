@@ -100,8 +100,18 @@ class GPUPyStitch:
         self._rand = {}
         self.last_metrics = None
         self.last_timings = None
+        self.stage_events = None  # optional list of 6 torch.cuda.Event(enable_timing=True)
 
     # ------------------------------------------------------------------
+    #: stage names of the events recorded when ``stage_events`` holds six
+    #: CUDA events: upload+features(img1), features(img2), match, RANSAC, compose
+    STAGES = ("features1", "features2", "match", "ransac", "compose")
+
+    def _mark(self, i):
+        ev = getattr(self, "stage_events", None)
+        if ev is not None:
+            ev[i].record(torch.cuda.current_stream(self.device))
+
     def _stream(self):
         return torch.cuda.current_stream(self.device).cuda_stream
 
@@ -176,8 +186,11 @@ class GPUPyStitch:
         if self._pca_matrix is None:
             mean = torch.empty(D, dtype=torch.float32, device=self.device)
             cov = torch.empty((D, D), dtype=torch.float64, device=self.device)
-            _lib.check(lib.pysift_pca_stats(both.data_ptr(), n1 + n2, D, mean.data_ptr(), cov.data_ptr(), st),
-                       "pysift_pca_stats")
+            sz = ctypes.c_size_t()
+            _lib.check(lib.pysift_pca_workspace_size(n1 + n2, D, ctypes.byref(sz)), "pysift_pca_workspace_size")
+            ws = torch.empty(int(sz.value), dtype=torch.uint8, device=self.device)
+            _lib.check(lib.pysift_pca_stats(both.data_ptr(), n1 + n2, D, ws.data_ptr(), ws.numel(), mean.data_ptr(),
+                                            cov.data_ptr(), st), "pysift_pca_stats")
             # one 128x128 symmetric eigendecomposition per instance (LAPACK),
             # the basis cached like the reference's (pysift/core.py:2729-2736)
             w, v = np.linalg.eigh(cov.cpu().numpy())
@@ -294,14 +307,18 @@ class GPUPyStitch:
         timings, metrics = {}, {}
         with torch.cuda.device(self.device):
             t0 = time.perf_counter()
+            self._mark(0)
             g1 = self._upload_bgr(img1, "img1")
             g2 = self._upload_bgr(img2, "img2")
             kp1, d1, n1 = self._features(g1, "img1")
+            self._mark(1)
             kp2, d2, n2 = self._features(g2, "img2")
+            self._mark(2)
             metrics.update(kp1=n1, kp2=n2)
             if n1 == 0 or n2 < 2:
                 raise RuntimeError(f"Insufficient matches (0), need >= 4")
             m = self._match(d1, d2)
+            self._mark(3)
             n_m = int(m["count"].item())
             metrics.update(matches=n_m)
             timings['st1'] = time.perf_counter() - t0
@@ -317,6 +334,7 @@ class GPUPyStitch:
             timings['st2'] = 0.0
             t0 = time.perf_counter()
             H_d, mask_d, info_d = self._ransac(p1, p2, n_m)
+            self._mark(4)
             H = H_d.cpu().numpy().reshape(3, 3).copy()
             info = info_d.cpu().numpy()
             n_in = int(info[0])
@@ -328,6 +346,7 @@ class GPUPyStitch:
             metrics.update(depth_cv=None, bands=self.n_depth_layers)
             t0 = time.perf_counter()
             pano, cm = self._compose(g1, g2, H)
+            self._mark(5)
             timings['st5'] = time.perf_counter() - t0
             metrics.update(canvas_w=cm['canvas_w'], canvas_h=cm['canvas_h'], seam_rmse=float('nan'))
         self._last = dict(H=H, mask=mask_d, pairs=m["pairs"][:n_m], kp1=kp1, kp2=kp2, p1=p1, p2=p2, info=info)

@@ -7,7 +7,9 @@ from pysift_b200 import synthetic
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("n1,n2,D", [(1000, 1000, 128), (300, 517, 128), (129, 1, 128), (2000, 1500, 64)])
+@pytest.mark.parametrize("n1,n2,D", [(1000, 1000, 128), (300, 517, 128), (129, 1, 128), (1, 300, 128),
+                                     (2000, 1500, 64), (8192, 8192, 128), (500, 16000, 128), (16000, 700, 128),
+                                     (3001, 4099, 128)])
 def test_exact_u8_bit_exact(n1, n2, D):
     import torch
     from oracle import match_oracle as mo

@@ -65,7 +65,11 @@ def test_matcher_preparation_bit_exact():
     assert np.array_equal(out.cpu().numpy(), ref)
     mean = torch.empty(128, dtype=torch.float32, device="cuda")
     cov = torch.empty((128, 128), dtype=torch.float64, device="cuda")
-    assert lib.pysift_pca_stats(out.data_ptr(), 3000, 128, mean.data_ptr(), cov.data_ptr(), _st()) == 0
+    sz = ctypes.c_size_t()
+    assert lib.pysift_pca_workspace_size(3000, 128, ctypes.byref(sz)) == 0
+    ws = torch.empty(sz.value, dtype=torch.uint8, device="cuda")
+    assert lib.pysift_pca_stats(out.data_ptr(), 3000, 128, ws.data_ptr(), ws.numel(), mean.data_ptr(),
+                                cov.data_ptr(), _st()) == 0
     rmean, rcov = so.pca_stats(ref)
     assert np.array_equal(mean.cpu().numpy(), rmean)
     assert np.array_equal(cov.cpu().numpy(), rcov)
