@@ -176,8 +176,10 @@ class PySIFT:
         self._graphs = {}
 
     # -- plumbing ---------------------------------------------------------
-    def _buffers(self, H, W):
-        key = (H, W)
+    def _buffers(self, H, W, slot=0):
+        """Buffer set for one image size; distinct slots let detections of
+        two images of the same size be in flight at once."""
+        key = (H, W) if slot == 0 else (H, W, slot)
         b = self._bufs.get(key)
         if b is None:
             b = _Buffers(self._lib, self._cfg, H, W, self.device)
@@ -203,17 +205,18 @@ class PySIFT:
             b.stats.data_ptr(), ev, stream)
         _lib.check(rc, "pysift_detect_and_compute")
 
-    def run_device(self, gray_t, stream=None, stage_events=None):
+    def run_device(self, gray_t, stream=None, stage_events=None, slot=0):
         """Enqueue detection of a device uint8 (H, W) tensor on `stream`
         (default: the current stream).  Returns the buffer set holding the
         outputs; stats are read by the caller.  stage_events: optional list
-        of 7 torch.cuda.Event recorded at the stage boundaries."""
+        of 7 torch.cuda.Event recorded at the stage boundaries; slot selects
+        an independent buffer set (for concurrent detections)."""
         if gray_t.dtype != torch.uint8 or gray_t.dim() != 2:
             raise ValueError("expected a 2-D uint8 image")
         if gray_t.stride(1) != 1:
             gray_t = gray_t.contiguous()
         H, W = gray_t.shape
-        b = self._buffers(H, W)
+        b = self._buffers(H, W, slot)
         st = stream if stream is not None else torch.cuda.current_stream(self.device)
         self._launch(b, gray_t.data_ptr(), H, W, gray_t.stride(0), st.cuda_stream, stage_events)
         return b

@@ -101,11 +101,13 @@ class GPUPyStitch:
         self.last_metrics = None
         self.last_timings = None
         self.stage_events = None  # optional list of 6 torch.cuda.Event(enable_timing=True)
+        self._side = None         # two side streams, one per view
 
     # ------------------------------------------------------------------
     #: stage names of the events recorded when ``stage_events`` holds six
-    #: CUDA events: upload+features(img1), features(img2), match, RANSAC, compose
-    STAGES = ("features1", "features2", "match", "ransac", "compose")
+    #: CUDA events: upload + CLAHE + detection of both views (concurrent),
+    #: top-k + matcher preparation, matching, RANSAC, warp + blend + crop
+    STAGES = ("features", "prep", "match", "ransac", "compose")
 
     def _mark(self, i):
         ev = getattr(self, "stage_events", None)
@@ -146,14 +148,20 @@ class GPUPyStitch:
                                           out.data_ptr(), W, st), "pysift_clahe")
         return out
 
-    def _features(self, bgr, key):
-        """Detect + describe, then keep the top max_keypoints by response
-        (stable, pysift/core.py:2566-2571).  Returns device (kpts (N,4), desc (N,128), N)."""
-        g = self._gray_clahe(bgr, key)
-        det = self._detector
-        b = det.run_device(g)
-        b.stats_host.copy_(b.stats, non_blocking=True)
-        torch.cuda.current_stream(self.device).synchronize()
+    def _detect_view(self, img, key, slot, stream):
+        """Upload (host images), gray + CLAHE and detection of one view,
+        enqueued on `stream`; the keypoint count is copied to pinned host
+        memory on the same stream."""
+        with torch.cuda.stream(stream):
+            bgr = self._upload_bgr(img, key)
+            g = self._gray_clahe(bgr, key)
+            b = self._detector.run_device(g, slot=slot)
+            b.stats_host.copy_(b.stats, non_blocking=True)
+        return bgr, b
+
+    def _select(self, b, key):
+        """Keep the top max_keypoints by response (stable, pysift/core.py:2566-2571).
+        Returns device (kpts (N,4), desc (N,128), N); the stats must be on the host."""
         n = int(b.stats_host[_lib.STAT_N_KEYPOINTS])
         kp, desc, resp = b.kpts[:n], b.desc[:n], b.resp[:n]
         if n > self.max_keypoints:
@@ -168,6 +176,13 @@ class GPUPyStitch:
         else:
             kp, desc = kp.clone(), desc.clone()
         return kp, desc, n
+
+    def _features(self, bgr, key):
+        """Detect + describe one view on the current stream, then select."""
+        st = torch.cuda.current_stream(self.device)
+        _, b = self._detect_view(bgr, key, 0, st)
+        st.synchronize()
+        return self._select(b, key)
 
     def _prepare(self, d1, d2):
         """L2-normalise, PCA (fitted once per instance), fp16 (pysift/core.py:2877-2888)."""
@@ -308,16 +323,29 @@ class GPUPyStitch:
         with torch.cuda.device(self.device):
             t0 = time.perf_counter()
             self._mark(0)
-            g1 = self._upload_bgr(img1, "img1")
-            g2 = self._upload_bgr(img2, "img2")
-            kp1, d1, n1 = self._features(g1, "img1")
+            # the two views run concurrently, one side stream each
+            main = torch.cuda.current_stream(self.device)
+            if self._side is None:
+                self._side = (torch.cuda.Stream(self.device), torch.cuda.Stream(self.device))
+            s1, s2 = self._side
+            s1.wait_stream(main)
+            s2.wait_stream(main)
+            g1, b1 = self._detect_view(img1, "img1", 0, s1)
+            g2, b2 = self._detect_view(img2, "img2", 1, s2)
+            s1.synchronize()
+            s2.synchronize()
+            main.wait_stream(s1)
+            main.wait_stream(s2)
             self._mark(1)
-            kp2, d2, n2 = self._features(g2, "img2")
-            self._mark(2)
+            kp1, d1, n1 = self._select(b1, "img1")
+            kp2, d2, n2 = self._select(b2, "img2")
             metrics.update(kp1=n1, kp2=n2)
             if n1 == 0 or n2 < 2:
                 raise RuntimeError(f"Insufficient matches (0), need >= 4")
-            m = self._match(d1, d2)
+            from . import match as _match_mod
+            a, bq, _ = self._prepare(d1, d2)
+            self._mark(2)
+            m = _match_mod.match_fp16(a, bq, self.match_ratio)
             self._mark(3)
             n_m = int(m["count"].item())
             metrics.update(matches=n_m)
