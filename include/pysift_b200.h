@@ -67,6 +67,12 @@ typedef struct pysift_detect_config {
     float ori_sigma[PYSIFT_MAX_LEVELS];           /* orientation sigma per scale index   */
     float desc_ph[PYSIFT_MAX_LEVELS];             /* descriptor patch half-width per si  */
     float kp_size[2][PYSIFT_MAX_OCTAVES][PYSIFT_MAX_LEVELS]; /* [doubled][o][si]     */
+    /* 0: every oriented keypoint, rows in the reference's (x, y) order.
+     * N > 0: when there are more than N, only the N with the largest
+     * response are described and returned, ordered by response (descending,
+     * ties in (x, y) order) -- the selection GPUPyStitch's feature extraction
+     * makes after detection (pysift/core.py:2566-2571). */
+    int32_t output_limit;
 } pysift_detect_config;
 
 /* Device-side counters written by pysift_detect_and_compute (int32 each). */

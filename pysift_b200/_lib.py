@@ -61,6 +61,7 @@ class DetectConfig(ctypes.Structure):
         ("ori_sigma", c_float * MAX_LEVELS),
         ("desc_ph", c_float * MAX_LEVELS),
         ("kp_size", ((c_float * MAX_LEVELS) * MAX_OCTAVES) * 2),
+        ("output_limit", c_int32),
     ]
 
 

@@ -85,6 +85,65 @@ __device__ __forceinline__ int block_excl_scan(int v, int* total, int* sh) {
     return res;
 }
 
+// Exclusive scan of one value per warp (lane 0's v) across the block; returns
+// the warp's exclusive prefix, *total = block sum.  sh: 33 ints.
+__device__ __forceinline__ int block_warp_excl_scan(int v, int* total, int* sh) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nwarps = blockDim.x >> 5;
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        const int w = (lane < nwarps) ? sh[lane] : 0;
+        int s = w;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int y = __shfl_up_sync(FULL_MASK, s, d);
+            if (lane >= d) s += y;
+        }
+        sh[lane] = s - w;
+        if (lane == 31) sh[32] = s;
+    }
+    __syncthreads();
+    const int res = sh[warp];
+    *total = sh[32];
+    __syncthreads();
+    return res;
+}
+
+// Ordered compaction of [0, n) by the whole block (blockDim.x a multiple of
+// 32): flag(i) is evaluated once per element; emit(i, pos) is called for
+// every flagged i with pos = number of flagged elements before i.  A warp
+// covers 32*K consecutive elements per chunk (coalesced, K-major then
+// lane), positions come from ballot popcounts, and one scan of the warp
+// counts per chunk places the warps.  Returns the number of flagged elements.
+template <int K, typename FlagF, typename EmitF>
+__device__ __forceinline__ int block_compact(int n, FlagF flag, EmitF emit, int* sh) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned below = (1u << lane) - 1u;
+    const int chunk = (int)blockDim.x * K;
+    int base = 0;
+    for (int c0 = 0; c0 < n; c0 += chunk) {
+        const int wbase = c0 + warp * 32 * K;
+        unsigned bal[K];
+        int wcnt = 0;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int i = wbase + k * 32 + lane;
+            bal[k] = __ballot_sync(FULL_MASK, i < n && flag(i));
+            wcnt += __popc(bal[k]);
+        }
+        int tot;
+        int pos = base + block_warp_excl_scan(wcnt, &tot, sh);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            if ((bal[k] >> lane) & 1u) emit(wbase + k * 32 + lane, pos + __popc(bal[k] & below));
+            pos += __popc(bal[k]);
+        }
+        base += tot;
+    }
+    return base;
+}
+
 __device__ __forceinline__ int warp_excl_scan(int v, int* total) {
     const int lane = threadIdx.x & 31;
     int x = v;

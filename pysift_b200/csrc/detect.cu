@@ -85,7 +85,7 @@ struct Layout {
     size_t off_cand, off_rv_valid, off_rv_ri, off_rv_ci, off_rv_si, off_rv_resp;
     size_t off_rf_ri, off_rf_ci, off_rf_si, off_rf_resp;
     size_t off_kp_o, off_kp_si, off_kp_ri, off_kp_ci, off_kp_resp, off_kp_tb;
-    size_t off_ang, off_angcnt, off_ent_kp, off_ent_slot, off_keys, off_rank;
+    size_t off_ang, off_angcnt, off_ent_kp, off_ent_slot, off_keys, off_rank, off_row_resp, off_lrank;
     size_t rowcnt_bytes_total;
     size_t off_rowcnt_base;
     size_t total;
@@ -102,6 +102,7 @@ static int validate_cfg(const pysift_detect_config* c) {
     PYSIFT_CHECK_ARG(c->keypoint_cap >= 1 && c->keypoint_cap <= (1 << 20), "keypoint_cap %d out of range",
                      c->keypoint_cap);
     PYSIFT_CHECK_ARG(c->border >= 1 && c->border < 64, "border %d out of range", c->border);
+    PYSIFT_CHECK_ARG(c->output_limit >= 0, "output_limit %d is negative", c->output_limit);
     PYSIFT_CHECK_ARG(!c->dsp || (c->n_dsp >= 1 && c->n_dsp <= 8), "n_dsp %d out of range", c->n_dsp);
     for (int i = 0; i < 2 + c->n_scales + 2; ++i)
         PYSIFT_CHECK_ARG(c->blur_radius[i] >= 0 && c->blur_radius[i] <= PYSIFT_MAX_RADIUS,
@@ -176,6 +177,8 @@ static Layout make_layout(const pysift_detect_config* c, int H, int W) {
     l.off_ent_slot = take(kc * 4 * sizeof(int));
     l.off_keys = take(kc * 4 * sizeof(uint4));
     l.off_rank = take(kc * 4 * sizeof(int));
+    l.off_row_resp = take(kc * 4 * sizeof(float));
+    l.off_lrank = take(kc * 4 * sizeof(int));
     if (l.doubled) l.off_coef = take((size_t)H * W * sizeof(double));
     l.off_base = take((size_t)l.H0 * l.pitch0 * sizeof(float));
     for (int o = 0; o < l.n_oct; ++o) l.off_pyr[o] = take((size_t)l.L * l.H[o] * l.pitch[o] * sizeof(float));
@@ -750,43 +753,75 @@ __device__ __forceinline__ int find_octave(const int* blk_off, int n_oct, int b)
     return o;
 }
 
+// One block = 32 rows x 32 columns of one octave (a warp per 4 rows, a mask
+// word per row and scale).  The block stages the DoG levels of its tile and
+// a one-pixel halo in shared memory (D_s = G_{s+1} - G_s, computed once per
+// position), then tests its pixels: |D| > threshold inside the border and
+// D >= all 26 neighbours or D <= all 26 neighbours.
+constexpr int EX_ROWS = 32;
 __global__ void __launch_bounds__(256) k_extrema_mask(const ExtArgs a, Ctrl* ctrl) {
+    extern __shared__ float ex_smem[];
     if (a.retry_mode && !ctrl->retried) return;
+    constexpr int SR = EX_ROWS + 2, SC = 35;  // staged rows, padded columns
+    auto sD = [&](int s, int rr, int cc) -> float& { return ex_smem[(s * SR + rr) * SC + cc]; };
     const float thr = ctrl->thr[a.thr_idx];
     const int o = find_octave(a.blk_off, a.n_oct, blockIdx.x);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const OctView& v = a.oct[o];
     const int wpr = a.wpr[o];
-    const int unit = (blockIdx.x - a.blk_off[o]) * 8 + warp;
-    if (unit >= v.H * wpr) return;
-    const int r = unit / wpr, wc = unit - r * wpr;
-    const int c = wc * 32 + lane;
-    const int B = a.border;
-    const bool inb = (r >= B && r < v.H - B && c >= B && c < v.W - B);
-    for (int s = 1; s <= a.S; ++s) {
-        bool ext = false;
-        if (inb) {
-            float val = dog_at(v, s, r, c);
-            if (fabsf(val) > thr) {
-                bool is_max = true, is_min = true;
-                for (int ds = -1; ds <= 1 && (is_max || is_min); ++ds)
-                    for (int dr = -1; dr <= 1; ++dr)
-                        for (int dc = -1; dc <= 1; ++dc) {
-                            if (ds == 0 && dr == 0 && dc == 0) continue;
-                            float nb = dog_at(v, s + ds, r + dr, c + dc);
-                            is_max = is_max && (val >= nb);
-                            is_min = is_min && (val <= nb);
-                        }
-                ext = is_max || is_min;
-            }
+    const int bl = blockIdx.x - a.blk_off[o];
+    const int by = bl / wpr, wc = bl - by * wpr;
+    const int r0 = by * EX_ROWS, c0 = wc * 32;
+    const int ndog = a.S + 2;
+    for (int q = threadIdx.x; q < SR * 34; q += 256) {
+        const int rr = q / 34, cc = q - rr * 34;
+        const int r = r0 - 1 + rr, c = c0 - 1 + cc;
+        const bool in = r >= 0 && r < v.H && c >= 0 && c < v.W;
+        const long long off = in ? (long long)r * v.pitch + c : 0;
+        float lo = in ? v.lev[0][off] : 0.0f;
+        for (int s = 0; s < ndog; ++s) {
+            const float hi = in ? v.lev[s + 1][off] : 0.0f;
+            sD(s, rr, cc) = hi - lo;
+            lo = hi;
         }
-        unsigned m = __ballot_sync(FULL_MASK, ext);
-        if (lane == 0) {
-            a.mask[o][((long long)(s - 1) * v.H + r) * wpr + wc] = m;
-            if (m) atomicAdd(&a.rowcnt[o][(s - 1) * v.H + r], __popc(m));
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int c = c0 + lane;
+    const int B = a.border;
+    for (int i = 0; i < EX_ROWS / 8; ++i) {
+        const int lr = warp + 8 * i, r = r0 + lr;
+        if (r >= v.H) break;
+        const bool inb = (r >= B && r < v.H - B && c >= B && c < v.W - B);
+        for (int s = 1; s <= a.S; ++s) {
+            bool ext = false;
+            if (inb) {
+                const float val = sD(s, lr + 1, lane + 1);
+                if (fabsf(val) > thr) {
+                    bool is_max = true, is_min = true;
+#pragma unroll
+                    for (int ds = -1; ds <= 1; ++ds)
+#pragma unroll
+                        for (int dr = 0; dr < 3; ++dr)
+#pragma unroll
+                            for (int dc = 0; dc < 3; ++dc) {
+                                if (ds == 0 && dr == 1 && dc == 1) continue;
+                                const float nb = sD(s + ds, lr + dr, lane + dc);
+                                is_max = is_max && (val >= nb);
+                                is_min = is_min && (val <= nb);
+                            }
+                    ext = is_max || is_min;
+                }
+            }
+            const unsigned m = __ballot_sync(FULL_MASK, ext);
+            if (lane == 0) {
+                a.mask[o][((long long)(s - 1) * v.H + r) * wpr + wc] = m;
+                if (m) atomicAdd(&a.rowcnt[o][(s - 1) * v.H + r], __popc(m));
+            }
         }
     }
 }
+
+static size_t extrema_smem_bytes(int S) { return (size_t)(S + 2) * (EX_ROWS + 2) * 35 * sizeof(float); }
 
 __global__ void __launch_bounds__(1024) k_rowscan(const ExtArgs a, Ctrl* ctrl) {
     if (a.retry_mode && !ctrl->retried) return;
@@ -939,27 +974,23 @@ __global__ void __launch_bounds__(256) k_refine(const RefArgs a, Ctrl* ctrl) {
     }
 }
 
+// Ordered compaction of the valid refined candidates of one octave.
 __global__ void __launch_bounds__(1024) k_refine_compact(const RefArgs a, Ctrl* ctrl) {
     if (a.retry_mode && !ctrl->retried) return;
     __shared__ int sh[33];
     const int o = blockIdx.x;
     const int n = ctrl->ncand[o];
     const long long base = (long long)o * a.cap;
-    int out_base = 0;
-    for (int c0 = 0; c0 < n; c0 += blockDim.x) {
-        int j = c0 + threadIdx.x;
-        int f = (j < n) ? a.rv_valid[base + j] : 0;
-        int tot;
-        int pos = out_base + block_excl_scan(f, &tot, sh);
-        if (f) {
+    const int total = block_compact<8>(
+        n, [&](int j) { return a.rv_valid[base + j] != 0; },
+        [&](int j, int pos) {
             a.rf_ri[base + pos] = a.rv_ri[base + j];
             a.rf_ci[base + pos] = a.rv_ci[base + j];
             a.rf_si[base + pos] = a.rv_si[base + j];
             a.rf_resp[base + pos] = a.rv_resp[base + j];
-        }
-        out_base += tot;
-    }
-    if (threadIdx.x == 0) ctrl->nref[o] = out_base;
+        },
+        sh);
+    if (threadIdx.x == 0) ctrl->nref[o] = total;
 }
 
 __global__ void k_retry_decide(Ctrl* ctrl, int n_oct, int starvation_min) {
@@ -992,13 +1023,23 @@ __device__ __forceinline__ void global_to_local(const int* nref_pref, int n_oct,
     *j = g - nref_pref[oo];
 }
 
-__global__ void __launch_bounds__(1024) k_cap(const CapArgs a, Ctrl* ctrl) {
+// Keys of up to CAP_SMEM_KEYS refined keypoints are staged in shared memory
+// for the radix passes; larger sets are read from global memory each pass.
+constexpr int CAP_SMEM_KEYS = 40960;
+constexpr int CAP_T = 1024;
+constexpr size_t CAP_SMEM_BYTES = (size_t)(32 * 256 + CAP_SMEM_KEYS) * sizeof(unsigned int);
+
+__global__ void __launch_bounds__(CAP_T) k_cap(const CapArgs a, Ctrl* ctrl) {
+    extern __shared__ unsigned int cap_smem[];
+    unsigned int* whist = cap_smem;              // [32 warps][256] private digit histograms
+    unsigned int* s_keys = cap_smem + 32 * 256;  // staged keys
     __shared__ int sh[33];
     __shared__ int pref[PYSIFT_MAX_OCTAVES + 1];
     __shared__ unsigned int hist[256];
     __shared__ unsigned int s_prefix, s_mask;
     __shared__ int s_need;
-    if (threadIdx.x == 0) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) {
         pref[0] = 0;
         for (int o = 0; o < a.n_oct; ++o) pref[o + 1] = pref[o] + ctrl->nref[o];
     }
@@ -1010,7 +1051,7 @@ __global__ void __launch_bounds__(1024) k_cap(const CapArgs a, Ctrl* ctrl) {
         return (long long)(*o) * a.cap_cand + *j;
     };
     if (!capped) {
-        for (int g = threadIdx.x; g < total; g += blockDim.x) {
+        for (int g = tid; g < total; g += CAP_T) {
             int o, j;
             long long src = load(g, &o, &j);
             a.kp_o[g] = o;
@@ -1020,86 +1061,123 @@ __global__ void __launch_bounds__(1024) k_cap(const CapArgs a, Ctrl* ctrl) {
             a.kp_resp[g] = a.rf_resp[src];
             a.kp_tb[g] = 0u;
         }
-        if (threadIdx.x == 0) {
+        if (tid == 0) {
             ctrl->n_total_ref = total;
             ctrl->n_kept = total;
             ctrl->capped = 0;
         }
         return;
     }
+    const bool in_smem = total <= CAP_SMEM_KEYS;
+    if (in_smem) {
+        for (int g = tid; g < total; g += CAP_T) {
+            int o, j;
+            s_keys[g] = __float_as_uint(a.rf_resp[load(g, &o, &j)]);
+        }
+    }
+    auto key_at = [&](int g) {
+        if (in_smem) return s_keys[g];
+        int o, j;
+        return __float_as_uint(a.rf_resp[load(g, &o, &j)]);
+    };
     // radix select of the kp_cap-th largest response (non-negative float bits)
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
         s_prefix = 0u;
         s_mask = 0u;
         s_need = a.kp_cap;
     }
-    __syncthreads();
     for (int pass = 3; pass >= 0; --pass) {
-        for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0u;
+        for (int i = tid; i < 32 * 256; i += CAP_T) whist[i] = 0u;
         __syncthreads();
         const unsigned int prefix = s_prefix, mask = s_mask;
-        // one shared atomic per distinct digit and warp: the keys crowd into a
-        // few exponent bytes, and per-key atomics on one bin serialise
-        for (int c0 = 0; c0 < total; c0 += blockDim.x) {
-            const int g = c0 + threadIdx.x;
-            unsigned int dig = 0xffffffffu;
-            if (g < total) {
-                int o, j;
-                const long long src = load(g, &o, &j);
-                const unsigned int key = __float_as_uint(a.rf_resp[src]);
-                if ((key & mask) == prefix) dig = (key >> (8 * pass)) & 255u;
-            }
-            const unsigned int peers = __match_any_sync(FULL_MASK, dig);
-            if (dig != 0xffffffffu && (int)(threadIdx.x & 31) == __ffs(peers) - 1)
-                atomicAdd(&hist[dig], (unsigned int)__popc(peers));
+        for (int g = tid; g < total; g += CAP_T) {
+            const unsigned int key = key_at(g);
+            if ((key & mask) == prefix) atomicAdd(&whist[warp * 256 + ((key >> (8 * pass)) & 255u)], 1u);
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
-            int need = s_need;
-            int cum = 0;
-            int d = 255;
-            for (; d > 0; --d) {
-                if (cum + (int)hist[d] >= need) break;
-                cum += (int)hist[d];
+        for (int d = tid; d < 256; d += CAP_T) {
+            unsigned int s = 0u;
+#pragma unroll 8
+            for (int w = 0; w < 32; ++w) s += whist[w * 256 + d];
+            hist[d] = s;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            // digit d with cum(> d) < need <= cum(>= d): warp suffix sums over 8-digit groups
+            int grp = 0;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) grp += (int)hist[lane * 8 + q];
+            int suf = grp;  // inclusive suffix sum over lanes lane..31
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const int v = __shfl_down_sync(FULL_MASK, suf, off);
+                if (lane + off < 32) suf += v;
             }
-            s_need = need - cum;
-            s_prefix = prefix | ((unsigned int)d << (8 * pass));
-            s_mask = mask | (255u << (8 * pass));
+            const int need = s_need;
+            const int above = suf - grp;  // keys in higher groups
+            const unsigned int who = __ballot_sync(FULL_MASK, above < need && need <= suf);
+            if (lane == (who ? __ffs(who) - 1 : 0)) {
+                int cum = above, d = lane * 8 + 7;
+                for (; d > lane * 8; --d) {
+                    if (cum + (int)hist[d] >= need) break;
+                    cum += (int)hist[d];
+                }
+                s_need = need - cum;
+                s_prefix = prefix | ((unsigned int)d << (8 * pass));
+                s_mask = mask | (255u << (8 * pass));
+            }
         }
         __syncthreads();
     }
     const unsigned int T = s_prefix;
     const int need_eq = s_need;
-    int eq_base = 0, out_base = 0;
-    for (int c0 = 0; c0 < total; c0 += blockDim.x) {
-        int g = c0 + threadIdx.x;
-        unsigned int key = 0u;
-        long long src = 0;
-        int o = 0, j = 0;
-        if (g < total) {
-            src = load(g, &o, &j);
-            key = __float_as_uint(a.rf_resp[src]);
+    // kept = every key > T and the first need_eq keys == T (index order), at
+    // position #greater-before + min(#equal-before, need_eq); warp ballots of
+    // both conditions and one packed scan of the warp counts per chunk
+    constexpr int K = 8;
+    const unsigned below = (1u << lane) - 1u;
+    int gt_base = 0, eq_base = 0;
+    for (int c0 = 0; c0 < total; c0 += CAP_T * K) {
+        const int wbase = c0 + warp * 32 * K;
+        unsigned int key[K], bgt[K], beq[K];
+        int cg = 0, ce = 0;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int g = wbase + k * 32 + lane;
+            key[k] = g < total ? key_at(g) : 0u;
+            bgt[k] = __ballot_sync(FULL_MASK, g < total && key[k] > T);
+            beq[k] = __ballot_sync(FULL_MASK, g < total && key[k] == T);
+            cg += __popc(bgt[k]);
+            ce += __popc(beq[k]);
         }
-        int is_eq = (g < total && key == T) ? 1 : 0;
-        int tot_eq;
-        int eq_rank = eq_base + block_excl_scan(is_eq, &tot_eq, sh);
-        eq_base += tot_eq;
-        int keep = (g < total) && (key > T || (is_eq && eq_rank < need_eq));
-        int tot_keep;
-        int pos = out_base + block_excl_scan(keep, &tot_keep, sh);
-        out_base += tot_keep;
-        if (keep) {
-            a.kp_o[pos] = o;
-            a.kp_si[pos] = a.rf_si[src];
-            a.kp_ri[pos] = a.rf_ri[src];
-            a.kp_ci[pos] = a.rf_ci[src];
-            a.kp_resp[pos] = a.rf_resp[src];
-            a.kp_tb[pos] = ~key;
+        int tot;
+        const int pre = block_warp_excl_scan(cg | (ce << 16), &tot, sh);
+        int pg = gt_base + (pre & 0xffff), pe = eq_base + (pre >> 16);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int g = wbase + k * 32 + lane;
+            const bool is_gt = (bgt[k] >> lane) & 1u, is_eq = (beq[k] >> lane) & 1u;
+            const int gb = pg + __popc(bgt[k] & below), eb = pe + __popc(beq[k] & below);
+            if (is_gt || (is_eq && eb < need_eq)) {
+                const int pos = gb + min(eb, need_eq);
+                int o, j;
+                const long long src = load(g, &o, &j);
+                a.kp_o[pos] = o;
+                a.kp_si[pos] = a.rf_si[src];
+                a.kp_ri[pos] = a.rf_ri[src];
+                a.kp_ci[pos] = a.rf_ci[src];
+                a.kp_resp[pos] = a.rf_resp[src];
+                a.kp_tb[pos] = ~key[k];
+            }
+            pg += __popc(bgt[k]);
+            pe += __popc(beq[k]);
         }
+        gt_base += tot & 0xffff;
+        eq_base += tot >> 16;
     }
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
         ctrl->n_total_ref = total;
-        ctrl->n_kept = out_base;
+        ctrl->n_kept = gt_base + min(eq_base, need_eq);
         ctrl->capped = 1;
     }
 }
@@ -1387,6 +1465,8 @@ struct DescArgs {
     const int* ent_kp;
     const int* ent_slot;
     const int* rank;
+    const int* lrank;  // rank by response of each output row (output_limit > 0)
+    int limit;
     float* out_kpts;
     float* out_resp;
     int* out_oct;
@@ -1516,6 +1596,11 @@ __global__ void __launch_bounds__(DESC_T) k_descriptor(const DescArgs a, const C
             (&whi[0][0])[b] = 0u;
         }
         __syncthreads();
+        int row = a.rank[e];
+        if (a.limit > 0 && n > a.limit) {
+            row = a.lrank[row];
+            if (row >= a.limit) continue;  // the whole block skips this entry
+        }
         const int kp = a.ent_kp[e], slot = a.ent_slot[e];
         const int o = a.kp_o[kp], si = a.kp_si[kp];
         const float ri = a.kp_ri[kp], ci = a.kp_ci[kp];
@@ -1554,7 +1639,6 @@ __global__ void __launch_bounds__(DESC_T) k_descriptor(const DescArgs a, const C
                 if (q < 0.0f) q = 0.0f;
                 val = sqrtf(q);
             }
-            const int row = a.rank[e];
             a.out_desc[(long long)row * 128 + tid] = val;
             if (tid == 0) {
                 const float sc = a.coord_scale[o];
@@ -1570,14 +1654,50 @@ __global__ void __launch_bounds__(DESC_T) k_descriptor(const DescArgs a, const C
     }
 }
 
-__global__ void k_finalize(const Ctrl* ctrl, int32_t* stats, int n_oct, int doubled) {
+// Response of every output row (rows are the (x, y) ranks of the oriented entries).
+__global__ void k_row_resp(const int* __restrict__ ent_kp, const float* __restrict__ kp_resp,
+                           const int* __restrict__ rank, float* __restrict__ row_resp, const Ctrl* ctrl) {
+    const int n = ctrl->n_oriented;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x)
+        row_resp[rank[e]] = kp_resp[ent_kp[e]];
+}
+
+// lrank[row] = number of rows with a larger response, or an equal response
+// and a lower row (lrank must start at zero); nothing when n <= limit.
+__global__ void __launch_bounds__(256) k_limit_rank(const float* __restrict__ row_resp, int limit,
+                                                   int* __restrict__ lrank, const Ctrl* ctrl) {
+    __shared__ float tile[256];
+    const int n = ctrl->n_oriented;
+    if (n <= limit) return;
+    const int nt = (n + 255) / 256;
+    for (long long t = blockIdx.x; t < (long long)nt * nt; t += gridDim.x) {
+        const int ti = (int)(t / nt), tj = (int)(t - (long long)ti * nt);
+        __syncthreads();
+        const int j = tj * 256 + threadIdx.x;
+        if (j < n) tile[threadIdx.x] = row_resp[j];
+        __syncthreads();
+        const int i = ti * 256 + threadIdx.x;
+        if (i < n) {
+            const float me = row_resp[i];
+            const int m = min(256, n - tj * 256);
+            int cnt = 0;
+            for (int k = 0; k < m; ++k) {
+                const float o = tile[k];
+                cnt += (o > me || (o == me && tj * 256 + k < i)) ? 1 : 0;
+            }
+            if (cnt) atomicAdd(&lrank[i], cnt);
+        }
+    }
+}
+
+__global__ void k_finalize(const Ctrl* ctrl, int32_t* stats, int n_oct, int doubled, int limit) {
     int t = threadIdx.x;
     if (t < PYSIFT_STAT_COUNT) stats[t] = 0;
     __syncthreads();
     if (t == 0) {
         int nref = 0;
         for (int o = 0; o < n_oct; ++o) nref += ctrl->nref[o];
-        stats[PYSIFT_STAT_N_KEYPOINTS] = ctrl->n_oriented;
+        stats[PYSIFT_STAT_N_KEYPOINTS] = (limit > 0 && ctrl->n_oriented > limit) ? limit : ctrl->n_oriented;
         stats[PYSIFT_STAT_N_REFINED] = nref;
         stats[PYSIFT_STAT_N_KEPT] = ctrl->n_kept;
         stats[PYSIFT_STAT_RETRIED] = ctrl->retried;
@@ -1727,7 +1847,7 @@ static int run_detect(const pysift_detect_config* cfg, const uint8_t* gray, int 
     int row_off[PYSIFT_MAX_OCTAVES + 1];
     for (int o = 0; o < n_oct; ++o) {
         ea.blk_off[o] = mask_blocks;
-        mask_blocks += ceil_div(l.H[o] * l.wpr[o], 8);
+        mask_blocks += ceil_div(l.H[o], EX_ROWS) * l.wpr[o];
         row_off[o] = row_blocks;
         row_blocks += ceil_div(S * l.H[o], 8);
         ea.mask[o] = at<uint32_t>(ws, l.off_mask[o]);
@@ -1752,7 +1872,7 @@ static int run_detect(const pysift_detect_config* cfg, const uint8_t* gray, int 
         ea.thr_idx = ra.thr_idx = pass;
         ea.retry_mode = ra.retry_mode = pass;
         PYSIFT_CUDA_TRY(cudaMemsetAsync(at<char>(ws, l.off_rowcnt_base), 0, l.rowcnt_bytes_total, st));
-        k_extrema_mask<<<mask_blocks, 256, 0, st>>>(ea, ctrl);
+        k_extrema_mask<<<mask_blocks, 256, extrema_smem_bytes(S), st>>>(ea, ctrl);
         PYSIFT_LAUNCH_CHECK("k_extrema_mask");
         if (pass == 0) PYSIFT_STAGE(3);
         k_rowscan<<<n_oct, 1024, 0, st>>>(ea, ctrl);
@@ -1789,7 +1909,11 @@ static int run_detect(const pysift_detect_config* cfg, const uint8_t* gray, int 
     ca.kp_ci = at<float>(ws, l.off_kp_ci);
     ca.kp_resp = at<float>(ws, l.off_kp_resp);
     ca.kp_tb = at<uint32_t>(ws, l.off_kp_tb);
-    k_cap<<<1, 1024, 0, st>>>(ca, ctrl);
+    {
+        PYSIFT_CUDA_TRY(
+            cudaFuncSetAttribute(k_cap, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CAP_SMEM_BYTES));
+        k_cap<<<1, CAP_T, CAP_SMEM_BYTES, st>>>(ca, ctrl);
+    }
     PYSIFT_LAUNCH_CHECK("k_cap");
     PYSIFT_STAGE(4);
     // A10
@@ -1846,13 +1970,23 @@ static int run_detect(const pysift_detect_config* cfg, const uint8_t* gray, int 
     da.ent_kp = xa.ent_kp;
     da.ent_slot = xa.ent_slot;
     da.rank = rank;
+    da.limit = cfg->output_limit;
+    da.lrank = at<int>(ws, l.off_lrank);
+    if (cfg->output_limit > 0) {
+        float* row_resp = at<float>(ws, l.off_row_resp);
+        PYSIFT_CUDA_TRY(cudaMemsetAsync(at<int>(ws, l.off_lrank), 0, sizeof(int) * 4 * (size_t)kcap, st));
+        k_row_resp<<<ceil_div(4 * kcap, 256), 256, 0, st>>>(xa.ent_kp, ca.kp_resp, rank, row_resp, ctrl);
+        PYSIFT_LAUNCH_CHECK("k_row_resp");
+        k_limit_rank<<<num_sms() * 8, 256, 0, st>>>(row_resp, cfg->output_limit, at<int>(ws, l.off_lrank), ctrl);
+        PYSIFT_LAUNCH_CHECK("k_limit_rank");
+    }
     da.out_kpts = kpts;
     da.out_resp = resp;
     da.out_oct = octv;
     da.out_desc = desc;
     k_descriptor<<<std::min(4 * kcap, num_sms() * (2048 / DESC_T)), DESC_T, 0, st>>>(da, ctrl);
     PYSIFT_LAUNCH_CHECK("k_descriptor");
-    k_finalize<<<1, 32, 0, st>>>(ctrl, stats, n_oct, l.doubled ? 1 : 0);
+    k_finalize<<<1, 32, 0, st>>>(ctrl, stats, n_oct, l.doubled ? 1 : 0, cfg->output_limit);
     PYSIFT_LAUNCH_CHECK("k_finalize");
     PYSIFT_STAGE(6);
     return PYSIFT_OK;

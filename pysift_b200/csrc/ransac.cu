@@ -57,47 +57,75 @@ __device__ __forceinline__ double ransac_exp(double x) {
            __longlong_as_double((long long)(1023 - 600) << 52);
 }
 
-// Fixed-order block sum of per-thread partials (RT threads): pairwise tree.
-__device__ double block_tree_sum(double v, double* sh) {
-    sh[threadIdx.x] = v;
+// NV fixed-order pairwise trees at once, the same pairs as block_tree_sum
+// (t += t + s for s = 128, 64, ..., 1): the three top levels in shared
+// memory, the rest with warp shuffles.  out (shared) receives the NV sums.
+template <int NV>
+__device__ __forceinline__ void block_tree_sums(const double (&v)[NV], double (*sh)[RT], double* out) {
+    const int tid = threadIdx.x;
+#pragma unroll
+    for (int u = 0; u < NV; ++u) sh[u][tid] = v[u];
     __syncthreads();
-    for (int s = RT / 2; s > 0; s >>= 1) {
-        if ((int)threadIdx.x < s) sh[threadIdx.x] = sh[threadIdx.x] + sh[threadIdx.x + s];
-        __syncthreads();
+    if (tid < 128) {
+#pragma unroll
+        for (int u = 0; u < NV; ++u) sh[u][tid] = sh[u][tid] + sh[u][tid + 128];
     }
-    const double r = sh[0];
     __syncthreads();
-    return r;
+    if (tid < 64) {
+#pragma unroll
+        for (int u = 0; u < NV; ++u) sh[u][tid] = sh[u][tid] + sh[u][tid + 64];
+    }
+    __syncthreads();
+    if (tid < 32) {
+#pragma unroll
+        for (int u = 0; u < NV; ++u) {
+            double x = sh[u][tid] + sh[u][tid + 32];
+#pragma unroll
+            for (int s = 16; s > 0; s >>= 1) x = x + __shfl_down_sync(FULL_MASK, x, s);
+            if (tid == 0) out[u] = x;
+        }
+    }
+    __syncthreads();
 }
 
 struct Norm {
     double s, cx, cy;
 };
 
-// Hartley normalisation of the points listed in idx (or 0..n-1), pysift/core.py:2946-2957:
-// c = mean, md = mean |p - c|, s = sqrt(2) / (md + 1e-10).
-__device__ Norm hartley(const double* pts, const int* idx, int n, double* sh) {
+// Hartley normalisation (pysift/core.py:2946-2957) of both point sets over
+// the points listed in idx (or 0..n-1): c = mean, md = mean |p - c|,
+// s = sqrt(2) / (md + 1e-10); sums over contiguous per-thread chunks, then
+// the fixed-order trees of block_tree_sums.
+__device__ void hartley2(const double* p1, const double* p2, const int* idx, int n, double (*sh)[RT], double* red,
+                         Norm& n1, Norm& n2) {
     const int chunk = (n + RT - 1) / RT;
     const int b = threadIdx.x * chunk, e = min(n, b + chunk);
-    double sx = 0.0, sy = 0.0;
+    double s4[4] = {0.0, 0.0, 0.0, 0.0};
     for (int i = b; i < e; ++i) {
         const int k = idx ? idx[i] : i;
-        sx = sx + pts[2 * k];
-        sy = sy + pts[2 * k + 1];
+        s4[0] = s4[0] + p1[2 * k];
+        s4[1] = s4[1] + p1[2 * k + 1];
+        s4[2] = s4[2] + p2[2 * k];
+        s4[3] = s4[3] + p2[2 * k + 1];
     }
-    const double tx = block_tree_sum(sx, sh), ty = block_tree_sum(sy, sh);
-    Norm r;
-    r.cx = tx / (double)n;
-    r.cy = ty / (double)n;
-    double sd = 0.0;
+    block_tree_sums<4>(s4, sh, red);
+    n1.cx = red[0] / (double)n;
+    n1.cy = red[1] / (double)n;
+    n2.cx = red[2] / (double)n;
+    n2.cy = red[3] / (double)n;
+    __syncthreads();
+    double s2[2] = {0.0, 0.0};
     for (int i = b; i < e; ++i) {
         const int k = idx ? idx[i] : i;
-        const double dx = pts[2 * k] - r.cx, dy = pts[2 * k + 1] - r.cy;
-        sd = sd + sqrt(dx * dx + dy * dy);
+        const double dx1 = p1[2 * k] - n1.cx, dy1 = p1[2 * k + 1] - n1.cy;
+        const double dx2 = p2[2 * k] - n2.cx, dy2 = p2[2 * k + 1] - n2.cy;
+        s2[0] = s2[0] + sqrt(dx1 * dx1 + dy1 * dy1);
+        s2[1] = s2[1] + sqrt(dx2 * dx2 + dy2 * dy2);
     }
-    const double md = block_tree_sum(sd, sh) / (double)n;
-    r.s = sqrt(2.0) / (md + 1e-10);
-    return r;
+    block_tree_sums<2>(s2, sh, red);
+    n1.s = sqrt(2.0) / (red[0] / (double)n + 1e-10);
+    n2.s = sqrt(2.0) / (red[1] / (double)n + 1e-10);
+    __syncthreads();
 }
 
 __device__ __forceinline__ void mat3_mul(const double* A, const double* B, double* C) {
@@ -162,45 +190,75 @@ __device__ __forceinline__ double sym_err(const double* H, const double* Hi, dou
     return (ex * ex + ey * ey) + (gx * gx + gy * gy);
 }
 
-// Null vector of the 8x9 DLT system of 4 normalised correspondences by
-// Gaussian elimination with partial pivoting; false if rank < 8.
-__device__ bool null_vector_8x9(const double* x1, const double* y1, const double* x2, const double* y2, double* h) {
-    double A[8][9];
-    for (int k = 0; k < 4; ++k) {
-        double* e = A[2 * k];
-        double* o = A[2 * k + 1];
-        e[0] = -x1[k]; e[1] = -y1[k]; e[2] = -1.0; e[3] = 0.0; e[4] = 0.0; e[5] = 0.0;
-        e[6] = x2[k] * x1[k]; e[7] = x2[k] * y1[k]; e[8] = x2[k];
-        o[0] = 0.0; o[1] = 0.0; o[2] = 0.0; o[3] = -x1[k]; o[4] = -y1[k]; o[5] = -1.0;
-        o[6] = y2[k] * x1[k]; o[7] = y2[k] * y1[k]; o[8] = y2[k];
+// Null vector (h[8] = 1) of the 8x9 DLT system of 4 normalised
+// correspondences by Gaussian elimination with partial pivoting; false if a
+// pivot is <= 1e-12 (rank < 8).  Lanes 0..7 of a warp hold one row each
+// (every lane of the warp must call it; lane r < 8 passes correspondence
+// r >> 1).  The pivot of column c is the first maximum of |A[r][c]| over rows
+// r >= c; rows move by shuffles; row r -= (A[r][c] / A[c][c]) * row c for
+// columns c..8; back substitution sums j ascending.
+__device__ bool null_vector_warp(double x1, double y1, double x2, double y2, double* h) {
+    const int lane = threadIdx.x & 31;
+    double R[9];
+    if (lane >= 8) {
+#pragma unroll
+        for (int j = 0; j < 9; ++j) R[j] = 0.0;
+    } else if ((lane & 1) == 0) {
+        R[0] = -x1; R[1] = -y1; R[2] = -1.0; R[3] = 0.0; R[4] = 0.0; R[5] = 0.0;
+        R[6] = x2 * x1; R[7] = x2 * y1; R[8] = x2;
+    } else {
+        R[0] = 0.0; R[1] = 0.0; R[2] = 0.0; R[3] = -x1; R[4] = -y1; R[5] = -1.0;
+        R[6] = y2 * x1; R[7] = y2 * y1; R[8] = y2;
     }
+    bool ok = true;
+#pragma unroll
     for (int c = 0; c < 8; ++c) {
-        int piv = c;
-        double best = fabs(A[c][c]);
-        for (int r = c + 1; r < 8; ++r) {
-            const double v = fabs(A[r][c]);
-            if (v > best) {
-                best = v;
-                piv = r;
+        double bv = (lane >= c && lane < 8) ? fabs(R[c]) : -1.0;
+        int bi = lane;
+#pragma unroll
+        for (int off = 4; off > 0; off >>= 1) {
+            const double ov = __shfl_xor_sync(FULL_MASK, bv, off);
+            const int oi = __shfl_xor_sync(FULL_MASK, bi, off);
+            if (ov > bv || (ov == bv && oi < bi)) {
+                bv = ov;
+                bi = oi;
             }
         }
-        if (!(best > 1e-12)) return false;
-        if (piv != c)
+        const double best = __shfl_sync(FULL_MASK, bv, 0);
+        const int piv = __shfl_sync(FULL_MASK, bi, 0);
+        if (!(best > 1e-12)) {
+            ok = false;
+            break;
+        }
+        if (piv != c) {
+#pragma unroll
             for (int j = 0; j < 9; ++j) {
-                const double t = A[c][j];
-                A[c][j] = A[piv][j];
-                A[piv][j] = t;
+                const double rc = __shfl_sync(FULL_MASK, R[j], c), rp = __shfl_sync(FULL_MASK, R[j], piv);
+                if (lane == c) R[j] = rp;
+                else if (lane == piv) R[j] = rc;
             }
-        for (int r = c + 1; r < 8; ++r) {
-            const double f = A[r][c] / A[c][c];
-            for (int j = c; j < 9; ++j) A[r][j] = A[r][j] - f * A[c][j];
+        }
+        double P[9];
+#pragma unroll
+        for (int j = c; j < 9; ++j) P[j] = __shfl_sync(FULL_MASK, R[j], c);
+        if (lane > c && lane < 8) {
+            const double f = R[c] / P[c];
+#pragma unroll
+            for (int j = c; j < 9; ++j) R[j] = R[j] - f * P[j];
         }
     }
+    if (!ok) return false;
     h[8] = 1.0;
+#pragma unroll
     for (int c = 7; c >= 0; --c) {
-        double s = A[c][8];
-        for (int j = c + 1; j < 8; ++j) s = s + A[c][j] * h[j];
-        h[c] = -s / A[c][c];
+        double hc = 0.0;
+        if (lane == c) {
+            double s = R[8];
+#pragma unroll
+            for (int j = c + 1; j < 8; ++j) s = s + R[j] * h[j];
+            hc = -s / R[c];
+        }
+        h[c] = __shfl_sync(FULL_MASK, hc, c);
     }
     return true;
 }
@@ -224,9 +282,10 @@ struct RansacArgs {
 };
 
 __global__ void __launch_bounds__(RT) k_ransac_prep(const RansacArgs a) {
-    __shared__ double sh[RT];
-    const Norm n1 = hartley(a.p1, nullptr, a.n, sh);
-    const Norm n2 = hartley(a.p2, nullptr, a.n, sh);
+    __shared__ double sh[4][RT];
+    __shared__ double red[4];
+    Norm n1, n2;
+    hartley2(a.p1, a.p2, nullptr, a.n, sh, red, n1, n2);
     for (int i = threadIdx.x; i < a.n; i += RT) {
         a.p1n[2 * i] = nrm(n1.s, n1.cx, a.p1[2 * i]);
         a.p1n[2 * i + 1] = nrm(n1.s, n1.cy, a.p1[2 * i + 1]);
@@ -245,16 +304,16 @@ __global__ void __launch_bounds__(RT) k_ransac_prep(const RansacArgs a) {
 __global__ void __launch_bounds__(256) k_ransac_hyp(const RansacArgs a) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (warp >= a.n_hyp) return;
-    double x1[4], y1[4], x2[4], y2[4];
-    for (int k = 0; k < 4; ++k) {
-        const int i = (int)(a.rnd[4 * warp + k] % (uint32_t)a.n);
-        x1[k] = a.p1n[2 * i];
-        y1[k] = a.p1n[2 * i + 1];
-        x2[k] = a.p2n[2 * i];
-        y2[k] = a.p2n[2 * i + 1];
+    double x1 = 0.0, y1 = 0.0, x2 = 0.0, y2 = 0.0;
+    if (lane < 8) {
+        const int i = (int)(a.rnd[4 * warp + (lane >> 1)] % (uint32_t)a.n);
+        x1 = a.p1n[2 * i];
+        y1 = a.p1n[2 * i + 1];
+        x2 = a.p2n[2 * i];
+        y2 = a.p2n[2 * i + 1];
     }
     double hn[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, H[9], Hi[9];
-    const bool ok = null_vector_8x9(x1, y1, x2, y2, hn);
+    const bool ok = null_vector_warp(x1, y1, x2, y2, hn);
     if (!ok)
         for (int k = 0; k < 9; ++k) hn[k] = 0.0;
     denormalise(hn, a.prep, a.prep + 9, H);
@@ -378,8 +437,9 @@ __device__ void dlt_refit(const double* p1, const double* p2, const int* idx, in
     constexpr int NB = 9;  // tree sums run 9 at a time
     __shared__ double s_part[NB][RT];
     __shared__ double s_Mj[9][9], s_Vj[9][9];
-    const Norm n1 = hartley(p1, idx, m, sh);
-    const Norm n2 = hartley(p2, idx, m, sh);
+    __shared__ double s_red[NB];
+    Norm n1, n2;
+    hartley2(p1, p2, idx, m, s_part, s_red, n1, n2);
     double acc[45];
     for (int k = 0; k < 45; ++k) acc[k] = 0.0;
     const int chunk = (m + RT - 1) / RT;
@@ -398,17 +458,10 @@ __device__ void dlt_refit(const double* p1, const double* p2, const int* idx, in
     }
 #pragma unroll
     for (int t0 = 0; t0 < 45; t0 += NB) {
+        double vv[NB];
 #pragma unroll
-        for (int u = 0; u < NB; ++u) s_part[u][threadIdx.x] = acc[t0 + u];
-        __syncthreads();
-        for (int s = RT / 2; s > 0; s >>= 1) {
-            if ((int)threadIdx.x < s)
-#pragma unroll
-                for (int u = 0; u < NB; ++u) s_part[u][threadIdx.x] = s_part[u][threadIdx.x] + s_part[u][threadIdx.x + s];
-            __syncthreads();
-        }
-        if (threadIdx.x < NB) s_M[t0 + threadIdx.x] = s_part[threadIdx.x][0];
-        __syncthreads();
+        for (int u = 0; u < NB; ++u) vv[u] = acc[t0 + u];
+        block_tree_sums<NB>(vv, s_part, s_M + t0);
     }
     for (int it = threadIdx.x; it < 45; it += RT) {
         // upper-triangle index it -> (r, c)

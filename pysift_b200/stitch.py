@@ -93,6 +93,9 @@ class GPUPyStitch:
                                 n_scales=n_scales, sigma0=sigma0, contrast_thresh=contrast_thresh,
                                 edge_thresh=edge_thresh, double_image=double_image, device=self.device,
                                 high_vram=high_vram)
+        # the detector describes only the top max_keypoints by response, in
+        # the order of the reference's stable selection (pysift/core.py:2566-2571)
+        self._detector._cfg.output_limit = int(max_keypoints)
         self._lib = _lib.load()
         self._dev = _Dev()
         self._pca_matrix = None   # float32 (128, pca_dims) on the device, fitted on the first pair
@@ -160,22 +163,12 @@ class GPUPyStitch:
         return bgr, b
 
     def _select(self, b, key):
-        """Keep the top max_keypoints by response (stable, pysift/core.py:2566-2571).
-        Returns device (kpts (N,4), desc (N,128), N); the stats must be on the host."""
+        """Keypoints and descriptors of one view: the detector already kept the
+        top max_keypoints by response (stable, pysift/core.py:2566-2571).
+        Returns device views (kpts (N,4), desc (N,128), N); the stats must be
+        on the host."""
         n = int(b.stats_host[_lib.STAT_N_KEYPOINTS])
-        kp, desc, resp = b.kpts[:n], b.desc[:n], b.resp[:n]
-        if n > self.max_keypoints:
-            k = self.max_keypoints
-            rank = self._dev.get(key + "_rank", (n,), torch.int32, self.device)
-            idx = self._dev.get(key + "_topk", (k,), torch.int32, self.device)
-            _lib.check(self._lib.pysift_topk_by_response(resp.data_ptr(), n, k, rank.data_ptr(), idx.data_ptr(),
-                                                         self._stream()), "pysift_topk_by_response")
-            il = idx.long()
-            kp, desc = kp.index_select(0, il), desc.index_select(0, il)
-            n = k
-        else:
-            kp, desc = kp.clone(), desc.clone()
-        return kp, desc, n
+        return b.kpts[:n], b.desc[:n], n
 
     def _features(self, bgr, key):
         """Detect + describe one view on the current stream, then select."""
@@ -286,13 +279,24 @@ class GPUPyStitch:
         col_lo, col_hi = e[2 * ch:2 * ch + cw], e[2 * ch + cw:]
         r0, r1, c0, c1, ir0, ir1, ic0, ic1, degenerate = self._autocrop_box(row_lo, row_hi, col_lo, col_hi)
         if r0 is None:
-            pano = out.cpu().numpy()
+            crop = out
         elif degenerate:
-            pano = out[r0:r1 + 1, c0:c1 + 1].cpu().numpy()
+            crop = out[r0:r1 + 1, c0:c1 + 1]
         else:
-            pano = out[r0 + ir0:r0 + ir1 + 1, c0 + ic0:c0 + ic1 + 1].cpu().numpy()
+            crop = out[r0 + ir0:r0 + ir1 + 1, c0 + ic0:c0 + ic1 + 1]
+        pano = self._to_host(crop)
         covered = int(np.sum(np.maximum(row_hi - row_lo + 1, 0)))  # upper bound of coverage per row span
         return pano, dict(canvas_w=cw, canvas_h=ch, ox=ox, oy=oy, coverage_rows_span=covered)
+
+    def _to_host(self, t):
+        """Device tensor -> numpy array in page-locked memory from torch's
+        caching host allocator (the array keeps its block alive; a freed
+        block is reused by a later call)."""
+        t = t.contiguous()
+        host = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+        host.copy_(t, non_blocking=True)
+        torch.cuda.current_stream(self.device).synchronize()
+        return host.numpy()
 
     @staticmethod
     def _autocrop_box(row_lo, row_hi, col_lo, col_hi):

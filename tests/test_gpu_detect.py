@@ -140,3 +140,27 @@ def test_repeat_determinism():
     b = sift.detect_arrays(img)
     for k in a:
         assert np.array_equal(a[k], b[k])
+
+
+@pytest.mark.parametrize("limit", [500, 100000])
+def test_output_limit_is_stable_topk_by_response(limit):
+    """output_limit = N keeps the N largest responses, ordered by response
+    with ties in (x, y) order, exactly as a stable top-N of the full output."""
+    import torch
+    from pysift_b200 import PySIFT
+    img = synthetic.dense_texture(480, 640, seed=5, sigma=2.0)
+    full = PySIFT()
+    kp, desc = full.detectAndCompute(img, gpu_output=True)
+    n = kp.shape[0]
+    resp = full._buffers(480, 640).resp[:n].cpu().numpy()
+    lim = PySIFT()
+    lim._cfg.output_limit = limit
+    kp2, desc2 = lim.detectAndCompute(img, gpu_output=True)
+    if n > limit:
+        order = np.argsort(-resp, kind="stable")[:limit]
+    else:
+        order = np.arange(n)
+    assert kp2.shape[0] == len(order)
+    assert np.array_equal(kp2.cpu().numpy(), kp.cpu().numpy()[order])
+    assert np.array_equal(desc2.cpu().numpy(), desc.cpu().numpy()[order])
+    assert np.array_equal(lim._buffers(480, 640).resp[:len(order)].cpu().numpy(), resp[order])
