@@ -111,32 +111,40 @@ __device__ __forceinline__ int block_warp_excl_scan(int v, int* total, int* sh) 
 }
 
 // Ordered compaction of [0, n) by the whole block (blockDim.x a multiple of
-// 32): flag(i) is evaluated once per element; emit(i, pos) is called for
-// every flagged i with pos = number of flagged elements before i.  A warp
-// covers 32*K consecutive elements per chunk (coalesced, K-major then
-// lane), positions come from ballot popcounts, and one scan of the warp
-// counts per chunk places the warps.  Returns the number of flagged elements.
-template <int K, typename FlagF, typename EmitF>
-__device__ __forceinline__ int block_compact(int n, FlagF flag, EmitF emit, int* sh) {
+// 32).  load(i) returns element i's payload (called for every i < n, before
+// any store of the chunk, so the loads of a chunk are all in flight
+// together); keep(payload) says whether it is kept; store(pos, payload)
+// writes a kept element at pos = number of kept elements before it.  A warp
+// covers 32*K consecutive elements per chunk (coalesced, K-major then lane);
+// positions come from ballot popcounts and one scan of the warp counts per
+// chunk.  Returns the number of kept elements.
+template <int K, typename P, typename LoadF, typename KeepF, typename StoreF>
+__device__ __forceinline__ int block_compact(int n, LoadF load, KeepF keep, StoreF store, int* sh) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned below = (1u << lane) - 1u;
     const int chunk = (int)blockDim.x * K;
     int base = 0;
     for (int c0 = 0; c0 < n; c0 += chunk) {
         const int wbase = c0 + warp * 32 * K;
+        P pl[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int i = wbase + k * 32 + lane;
+            if (i < n) pl[k] = load(i);
+        }
         unsigned bal[K];
         int wcnt = 0;
 #pragma unroll
         for (int k = 0; k < K; ++k) {
             const int i = wbase + k * 32 + lane;
-            bal[k] = __ballot_sync(FULL_MASK, i < n && flag(i));
+            bal[k] = __ballot_sync(FULL_MASK, i < n && keep(pl[k]));
             wcnt += __popc(bal[k]);
         }
         int tot;
         int pos = base + block_warp_excl_scan(wcnt, &tot, sh);
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-            if ((bal[k] >> lane) & 1u) emit(wbase + k * 32 + lane, pos + __popc(bal[k] & below));
+            if ((bal[k] >> lane) & 1u) store(pos + __popc(bal[k] & below), pl[k]);
             pos += __popc(bal[k]);
         }
         base += tot;

@@ -975,19 +975,33 @@ __global__ void __launch_bounds__(256) k_refine(const RefArgs a, Ctrl* ctrl) {
 }
 
 // Ordered compaction of the valid refined candidates of one octave.
+struct RefinedRow {
+    float ri, ci, resp;
+    int si, valid;
+};
 __global__ void __launch_bounds__(1024) k_refine_compact(const RefArgs a, Ctrl* ctrl) {
     if (a.retry_mode && !ctrl->retried) return;
     __shared__ int sh[33];
     const int o = blockIdx.x;
     const int n = ctrl->ncand[o];
     const long long base = (long long)o * a.cap;
-    const int total = block_compact<8>(
-        n, [&](int j) { return a.rv_valid[base + j] != 0; },
-        [&](int j, int pos) {
-            a.rf_ri[base + pos] = a.rv_ri[base + j];
-            a.rf_ci[base + pos] = a.rv_ci[base + j];
-            a.rf_si[base + pos] = a.rv_si[base + j];
-            a.rf_resp[base + pos] = a.rv_resp[base + j];
+    const int total = block_compact<8, RefinedRow>(
+        n,
+        [&](int j) {
+            RefinedRow r;
+            r.valid = a.rv_valid[base + j];
+            r.ri = a.rv_ri[base + j];
+            r.ci = a.rv_ci[base + j];
+            r.si = a.rv_si[base + j];
+            r.resp = a.rv_resp[base + j];
+            return r;
+        },
+        [](const RefinedRow& r) { return r.valid != 0; },
+        [&](int pos, const RefinedRow& r) {
+            a.rf_ri[base + pos] = r.ri;
+            a.rf_ci[base + pos] = r.ci;
+            a.rf_si[base + pos] = r.si;
+            a.rf_resp[base + pos] = r.resp;
         },
         sh);
     if (threadIdx.x == 0) ctrl->nref[o] = total;
@@ -1140,11 +1154,30 @@ __global__ void __launch_bounds__(CAP_T) k_cap(const CapArgs a, Ctrl* ctrl) {
     for (int c0 = 0; c0 < total; c0 += CAP_T * K) {
         const int wbase = c0 + warp * 32 * K;
         unsigned int key[K], bgt[K], beq[K];
+        int so[K], ssi[K];
+        float sri[K], sci[K], sresp[K];
+        // every load of the chunk first (coalesced within an octave), then the stores
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int g = wbase + k * 32 + lane;
+            so[k] = 0;
+            ssi[k] = 0;
+            sri[k] = sci[k] = sresp[k] = 0.0f;
+            if (g < total) {
+                int o, j;
+                const long long src = load(g, &o, &j);
+                so[k] = o;
+                ssi[k] = a.rf_si[src];
+                sri[k] = a.rf_ri[src];
+                sci[k] = a.rf_ci[src];
+                sresp[k] = a.rf_resp[src];
+            }
+            key[k] = __float_as_uint(sresp[k]);
+        }
         int cg = 0, ce = 0;
 #pragma unroll
         for (int k = 0; k < K; ++k) {
             const int g = wbase + k * 32 + lane;
-            key[k] = g < total ? key_at(g) : 0u;
             bgt[k] = __ballot_sync(FULL_MASK, g < total && key[k] > T);
             beq[k] = __ballot_sync(FULL_MASK, g < total && key[k] == T);
             cg += __popc(bgt[k]);
@@ -1155,18 +1188,15 @@ __global__ void __launch_bounds__(CAP_T) k_cap(const CapArgs a, Ctrl* ctrl) {
         int pg = gt_base + (pre & 0xffff), pe = eq_base + (pre >> 16);
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-            const int g = wbase + k * 32 + lane;
             const bool is_gt = (bgt[k] >> lane) & 1u, is_eq = (beq[k] >> lane) & 1u;
             const int gb = pg + __popc(bgt[k] & below), eb = pe + __popc(beq[k] & below);
             if (is_gt || (is_eq && eb < need_eq)) {
                 const int pos = gb + min(eb, need_eq);
-                int o, j;
-                const long long src = load(g, &o, &j);
-                a.kp_o[pos] = o;
-                a.kp_si[pos] = a.rf_si[src];
-                a.kp_ri[pos] = a.rf_ri[src];
-                a.kp_ci[pos] = a.rf_ci[src];
-                a.kp_resp[pos] = a.rf_resp[src];
+                a.kp_o[pos] = so[k];
+                a.kp_si[pos] = ssi[k];
+                a.kp_ri[pos] = sri[k];
+                a.kp_ci[pos] = sci[k];
+                a.kp_resp[pos] = sresp[k];
                 a.kp_tb[pos] = ~key[k];
             }
             pg += __popc(bgt[k]);
@@ -1385,25 +1415,44 @@ struct ExpArgs {
     float coord_scale[PYSIFT_MAX_OCTAVES];  // 2^o * (0.5 if doubled else 1)
 };
 
+// Expansion of the kept keypoints into their oriented entries (1..4 each),
+// in keypoint order: each thread takes EXP_K consecutive keypoints, loads
+// them, and one block scan per chunk places their entries.
+constexpr int EXP_K = 8;
 __global__ void __launch_bounds__(1024) k_expand(const ExpArgs a, Ctrl* ctrl) {
     __shared__ int sh[33];
     const int n = ctrl->n_kept;
     int base = 0;
-    for (int c0 = 0; c0 < n; c0 += blockDim.x) {
-        int i = c0 + threadIdx.x;
-        int cnt = (i < n) ? a.angcnt[i] : 0;
-        int tot;
-        int pos = base + block_excl_scan(cnt, &tot, sh);
-        if (cnt) {
-            const int o = a.kp_o[i];
-            const float sc = a.coord_scale[o];
-            const float x = a.kp_ci[i] * sc, y = a.kp_ri[i] * sc;
-            for (int k = 0; k < cnt; ++k) {
-                a.ent_kp[pos + k] = i;
-                a.ent_slot[pos + k] = k;
-                a.keys[pos + k] = make_uint4(__float_as_uint(x), __float_as_uint(y), a.kp_tb[i],
-                                             (uint32_t)(i * 4 + k));
+    for (int c0 = 0; c0 < n; c0 += (int)blockDim.x * EXP_K) {
+        const int i0 = c0 + (int)threadIdx.x * EXP_K;
+        int cnt[EXP_K];
+        uint32_t kx[EXP_K], ky[EXP_K], tb[EXP_K];
+        int local = 0;
+#pragma unroll
+        for (int k = 0; k < EXP_K; ++k) {
+            const int i = i0 + k;
+            cnt[k] = 0;
+            kx[k] = ky[k] = tb[k] = 0u;
+            if (i < n) {
+                cnt[k] = a.angcnt[i];
+                const float sc = a.coord_scale[a.kp_o[i]];
+                kx[k] = __float_as_uint(a.kp_ci[i] * sc);
+                ky[k] = __float_as_uint(a.kp_ri[i] * sc);
+                tb[k] = a.kp_tb[i];
             }
+            local += cnt[k];
+        }
+        int tot;
+        int pos = base + block_excl_scan(local, &tot, sh);
+#pragma unroll
+        for (int k = 0; k < EXP_K; ++k) {
+            const int i = i0 + k;
+            for (int q = 0; q < cnt[k]; ++q) {
+                a.ent_kp[pos + q] = i;
+                a.ent_slot[pos + q] = q;
+                a.keys[pos + q] = make_uint4(kx[k], ky[k], tb[k], (uint32_t)(i * 4 + q));
+            }
+            pos += cnt[k];
         }
         base += tot;
     }
