@@ -14,6 +14,9 @@ stand in for the reference's datasets; see pysift_b200/synthetic.py):
   detect_640x480    detectAndCompute on one 640x480 scene
   match_u8_8192     exact ratio-test matching of two 8192 x 128 uint8-valued
                     descriptor sets (bf16 tcgen05 GEMM, exact against int64)
+  batch96_detect    PySIFT.detect_batch of 96 grayscale images of uneven sizes
+                    (480x360 .. 4000x3000, aspect 4:3, 3:2, 16:9) over 8 streams,
+                    next to the plain per-image detectAndCompute loop
 
 A step is one pass of the hot path over one input.  `value` is measured
 with CUDA events on the launching stream, inputs resident in HBM, L2
@@ -40,6 +43,7 @@ WORKLOADS = {
     "detect_1280x960": dict(kind="detect", H=960, W=1280, seed=0),
     "detect_640x480": dict(kind="detect", H=480, W=640, seed=0),
     "match_u8_8192": dict(kind="match", N=8192, M=8192, D=128, seed=0),
+    "batch96_detect": dict(kind="batch_detect", n=96, seed=0, streams=8),
 }
 DEFAULT_WORKLOAD = "stitch_pair_1280x960"
 METRIC = "SIFT Mpix/s + match-pairs/s on 1 B200: batched+BF16 vs plain, bit-exact"
@@ -180,6 +184,8 @@ def run_reference(args, wl, world, rank):
         return run_reference_stitch(args, wl)
     if wl["kind"] == "match":
         return run_reference_match(args, wl)
+    if wl["kind"] == "batch_detect":
+        return run_reference_batch(args, wl)
     img = synthetic.scene(wl["H"], wl["W"], seed=wl["seed"])
     times = []
     from oracle import oracle
@@ -311,6 +317,33 @@ def run_match(args, wl, world, rank, local):
     return 0
 
 
+def run_reference_batch(args, wl):
+    """The oracle on a bounded sample of the batch (its smallest images)."""
+    from oracle import oracle
+    from pysift_b200 import synthetic
+    imgs = sorted(synthetic.batch_images(wl["n"], seed=wl["seed"]), key=lambda im: im.size)[:4]
+    orc = oracle.OracleSIFT()
+    times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        for im in imgs:
+            orc.detect_and_compute(im)
+        if i >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    value = sum(im.size for im in imgs) / 1e6 / float(np.mean(times))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Mpix/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(times)) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "images": len(imgs), "seed": wl["seed"]},
+        "cpu_baseline": {"value": value, "unit": "Mpix/s", "cores": os.cpu_count(), "kind": "port",
+                         "sample": "the 4 smallest images of the batch per step (oracle, OpenMP)"},
+        "e2e": {"value": value, "unit": "Mpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_reference_match(args, wl):
     from oracle import match_oracle as mo
     from pysift_b200 import synthetic
@@ -330,6 +363,107 @@ def run_reference_match(args, wl):
         "cpu_baseline": {"value": 1.0 / sec, "unit": "match-pairs/s", "cores": os.cpu_count(), "kind": "port",
                          "sample": "one full exact match per step (oracle, numpy + BLAS)"},
         "e2e": {"value": 1.0 / sec, "unit": "match-pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_batch_detect(args, wl, world, rank, local):
+    import torch
+    import torch.distributed as dist
+    from pysift_b200 import PySIFT, _lib, synthetic
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    imgs = synthetic.batch_images(wl["n"], seed=wl["seed"] + rank)
+    mpix = sum(im.size for im in imgs) / 1e6
+    sift = PySIFT(device=dev)
+    g = [torch.from_numpy(im).to(dev) for im in imgs]
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    lib = _lib.load()
+    ns = wl["streams"]
+    for _ in range(args.warmup):
+        sift.detect_batch(g, n_streams=ns)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn, steps):
+        ms = []
+        for _ in range(steps):
+            flush.zero_()
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return ms
+
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    launches0 = lib.pysift_launch_count()
+    with ClockSampler(local) as clk:
+        step_ms = timed(lambda: sift.detect_batch(g, n_streams=ns), args.steps)
+    launches = lib.pysift_launch_count() - launches0
+    t = torch.tensor([float(np.sum(step_ms))], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    # the same images, the plain way: one detectAndCompute call per image
+    plain_steps = max(1, min(3, args.steps))
+    plain_ms = timed(lambda: [sift.detectAndCompute(x, gpu_output=True) for x in g], plain_steps)
+    one_ms = timed(lambda: sift.detect_batch(g, n_streams=1), plain_steps)
+    # end to end: host images in, host arrays out
+    e2e_ms = []
+    for i in range(args.warmup + args.steps):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        res = sift.detect_batch(imgs, n_streams=ns, gpu_output=False)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            e2e_ms.append(dt * 1e3)
+    e2e_t = torch.tensor([float(np.sum(e2e_ms))], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    if rank != 0:
+        return 0
+    n_kp = int(sum(r[0].shape[0] for r in res))
+    out_bytes = int(sum(r[0].nbytes + r[1].nbytes for r in res))
+    step_s = total_ms / args.steps / 1e3
+    peak, peak_kind = measured_peaks()
+    alg = sum(pyramid_alg_bytes(im.shape[0], im.shape[1], sift) for im in imgs)
+    achieved = alg / step_s / 1e9
+    if args.no_cpu_baseline:
+        cpu_v, cpu_n = None, 0
+    else:
+        from oracle import oracle
+        orc = oracle.OracleSIFT()
+        small = sorted(imgs, key=lambda im: im.size)[:4]
+        t0 = time.perf_counter()
+        for im in small:
+            orc.detect_and_compute(im)
+        cpu_v = sum(im.size for im in small) / 1e6 / (time.perf_counter() - t0)
+        cpu_n = len(small)
+    line = {
+        "metric": METRIC, "value": world * mpix / step_s, "unit": "Mpix/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "images": wl["n"], "seed": wl["seed"], "mpix_per_batch": mpix,
+                   "streams": ns, "keypoints": n_kp, "sizes": "480x360 .. 4000x3000, aspect 4:3 / 3:2 / 16:9",
+                   "l2": "flushed (256 MiB write) before every step", "parallelism": f"replicas{world}"},
+        "plain_mpix_per_s": mpix / (float(np.mean(plain_ms)) / 1e3),
+        "one_stream_mpix_per_s": mpix / (float(np.mean(one_ms)) / 1e3),
+        "roofline": {"bound": "hbm", "kernel": "whole batched detection: pyramid-region algorithmic bytes of all "
+                     "images over the whole batch time (a lower bound for the pyramid kernels)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_kind, "alg_bytes_per_launch": alg, "traffic": None},
+        "cpu_baseline": {"value": cpu_v, "unit": "Mpix/s", "cores": os.cpu_count(), "kind": "port",
+                         "sample": f"the {cpu_n} smallest images of the batch through the oracle (OpenMP)"},
+        "e2e": {"value": world * mpix / (float(e2e_t.item()) / args.steps / 1e3), "unit": "Mpix/s",
+                "h2d_bytes_per_step": int(sum(im.nbytes for im in imgs)), "d2h_bytes_per_step": out_bytes},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -626,6 +760,8 @@ def main():
             return run_stitch(args, wl, world, rank, local)
         if wl["kind"] == "match":
             return run_match(args, wl, world, rank, local)
+        if wl["kind"] == "batch_detect":
+            return run_batch_detect(args, wl, world, rank, local)
         return run_detect(args, wl, world, rank, local)
     finally:
         if world > 1:

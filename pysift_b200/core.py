@@ -128,6 +128,18 @@ class _Buffers:
         return self.ws.data_ptr() + self.ws_off
 
 
+class _BatchOutputs:
+    """Output buffers of one image of a batch."""
+
+    def __init__(self, max_out, device):
+        self.kpts = torch.empty((max_out, 4), dtype=torch.float32, device=device)
+        self.resp = torch.empty(max_out, dtype=torch.float32, device=device)
+        self.octv = torch.empty(max_out, dtype=torch.int32, device=device)
+        self.desc = torch.empty((max_out, 128), dtype=torch.float32, device=device)
+        self.stats = torch.zeros(_lib.STAT_COUNT, dtype=torch.int32, device=device)
+        self.stats_host = torch.zeros(_lib.STAT_COUNT, dtype=torch.int32).pin_memory()
+
+
 class PySIFT:
     """GPU SIFT detector/descriptor with the reference's interface
     (pysift/core.py:1150-2172).
@@ -271,6 +283,88 @@ class PySIFT:
         kps = [cv2.KeyPoint(float(kp[j, 0]), float(kp[j, 1]), float(kp[j, 2]), float(kp[j, 3]),
                             float(resp[j]), int(octv[j])) for j in range(n)]
         return kps, desc
+
+    # -- batched detection ----------------------------------------------------
+    def detect_batch(self, images, n_streams=8, gpu_output=True):
+        """Detect and describe a list of grayscale uint8 images of any sizes in
+        one call.  Images (numpy arrays or CUDA tensors) are dealt, largest
+        first, to `n_streams` slots; each slot runs its images in order on its
+        own CUDA stream with its own workspace (sized for its largest image),
+        so detections of different images overlap on the GPU; every image has
+        its own output buffers and the host waits once, after all of them.
+
+        Returns a list of (kpts (N,4) [x, y, size, angle], desc (N,128)) per
+        image, in input order: torch CUDA tensors with gpu_output, else numpy
+        arrays.  n_streams=1 runs the same work back to back on one stream."""
+        n = len(images)
+        if n == 0:
+            return []
+        lib = self._lib
+        with torch.cuda.device(self.device):
+            main = torch.cuda.current_stream(self.device)
+            gray = []
+            for img in images:
+                if isinstance(img, torch.Tensor) and img.is_cuda:
+                    t = img
+                else:
+                    a = np.ascontiguousarray(img)
+                    if a.dtype != np.uint8 or a.ndim != 2:
+                        raise ValueError("images must be 2-D uint8")
+                    t = torch.from_numpy(a).to(self.device)
+                if t.dtype != torch.uint8 or t.dim() != 2:
+                    raise ValueError("images must be 2-D uint8")
+                if t.stride(1) != 1:
+                    t = t.contiguous()
+                gray.append(t)
+            order = sorted(range(n), key=lambda i: -(gray[i].shape[0] * gray[i].shape[1]))
+            ns = max(1, min(int(n_streams), n))
+            slots = [order[s::ns] for s in range(ns)]
+            if not hasattr(self, "_batch"):
+                self._batch = {"streams": [], "ws": [], "outs": []}
+            bt = self._batch
+            while len(bt["streams"]) < ns:
+                bt["streams"].append(torch.cuda.Stream(self.device))
+                bt["ws"].append(None)
+            max_out = int(lib.pysift_detect_max_keypoints(ctypes.byref(self._cfg)))
+            while len(bt["outs"]) < n:
+                bt["outs"].append(_BatchOutputs(max_out, self.device))
+            for s, idxs in enumerate(slots):
+                need = 0
+                for i in idxs:
+                    H, W = gray[i].shape
+                    sz = ctypes.c_size_t(0)
+                    _lib.check(lib.pysift_detect_workspace_size(ctypes.byref(self._cfg), H, W, ctypes.byref(sz)),
+                               "pysift_detect_workspace_size")
+                    need = max(need, int(sz.value))
+                ws = bt["ws"][s]
+                if ws is None or ws.numel() < need + 256:
+                    ws = torch.empty(need + 256, dtype=torch.uint8, device=self.device)
+                    bt["ws"][s] = ws
+                st = bt["streams"][s]
+                st.wait_stream(main)
+                wptr = ws.data_ptr() + ((-ws.data_ptr()) % 256)
+                with torch.cuda.stream(st):
+                    for i in idxs:
+                        H, W = gray[i].shape
+                        o = bt["outs"][i]
+                        rc = lib.pysift_detect_and_compute(
+                            ctypes.byref(self._cfg), gray[i].data_ptr(), H, W, gray[i].stride(0), wptr, need,
+                            o.kpts.data_ptr(), o.resp.data_ptr(), o.octv.data_ptr(), o.desc.data_ptr(), max_out,
+                            o.stats.data_ptr(), None, st.cuda_stream)
+                        _lib.check(rc, "pysift_detect_and_compute")
+                        o.stats_host.copy_(o.stats, non_blocking=True)
+            for s in range(ns):
+                main.wait_stream(bt["streams"][s])
+            main.synchronize()
+            out = []
+            for i in range(n):
+                o = bt["outs"][i]
+                k = int(o.stats_host[_lib.STAT_N_KEYPOINTS])
+                if gpu_output:
+                    out.append((o.kpts[:k].clone(), o.desc[:k].clone()))
+                else:
+                    out.append((o.kpts[:k].cpu().numpy(), o.desc[:k].cpu().numpy()))
+        return out
 
     def detect_arrays(self, gray):
         """Host uint8 image in, host numpy arrays out: dict with x, y, size,

@@ -153,6 +153,41 @@ def batch_sizes(n=96, seed=0):
     return out
 
 
+def scene_fast(H, W, seed=0):
+    """A cheaper scene for large batches: the blob/rectangle scene drawn at a
+    quarter of the resolution (blob sigmas scaled with it), cubic-upsampled,
+    plus band-limited noise at full resolution (sigma 1 blur, std 6)."""
+    import cv2
+    rng = _rng(seed)
+    h, w = max(8, H // 4), max(8, W // 4)
+    base = np.zeros((h, w), np.float64) + 128.0
+    yy, xx = np.mgrid[0:h, 0:w].astype(np.float64)
+    for _ in range(50):
+        x0, x1 = sorted(rng.integers(0, w, size=2))
+        y0, y1 = sorted(rng.integers(0, h, size=2))
+        base[y0:y1 + 1, x0:x1 + 1] = rng.uniform(30, 220)
+    for _ in range(200):
+        cx, cy = rng.uniform(0, w), rng.uniform(0, h)
+        s = rng.uniform(2, 25) / 4.0
+        a = rng.uniform(-80, 80)
+        r = int(3 * s) + 1
+        ya, yb = max(0, int(cy) - r), min(h, int(cy) + r + 1)
+        xa, xb = max(0, int(cx) - r), min(w, int(cx) + r + 1)
+        if ya >= yb or xa >= xb:
+            continue
+        d2 = (yy[ya:yb, xa:xb] - cy) ** 2 + (xx[ya:yb, xa:xb] - cx) ** 2
+        base[ya:yb, xa:xb] += a * np.exp(-d2 / (2 * s * s))
+    img = cv2.resize(base.astype(np.float32), (W, H), interpolation=cv2.INTER_CUBIC)
+    noise = cv2.GaussianBlur(rng.standard_normal((H, W)).astype(np.float32), (0, 0), 1.0)
+    noise *= 6.0 / max(float(noise.std()), 1e-12)
+    return np.clip(np.rint(img + noise), 0, 255).astype(np.uint8)
+
+
+def batch_images(n=96, seed=0):
+    """n seeded uint8 scenes with the uneven sizes of batch_sizes(n, seed)."""
+    return [scene_fast(h, w, seed=seed * 1000 + i) for i, (h, w) in enumerate(batch_sizes(n, seed))]
+
+
 def dense_texture(H, W, seed=0, sigma=2.0):
     """Band-limited noise texture (white noise blurred with `sigma`, std 40
     around 128): thousands of extrema per megapixel, used to exercise the

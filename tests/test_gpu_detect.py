@@ -164,3 +164,46 @@ def test_output_limit_is_stable_topk_by_response(limit):
     assert np.array_equal(kp2.cpu().numpy(), kp.cpu().numpy()[order])
     assert np.array_equal(desc2.cpu().numpy(), desc.cpu().numpy()[order])
     assert np.array_equal(lim._buffers(480, 640).resp[:len(order)].cpu().numpy(), resp[order])
+
+
+@pytest.mark.parametrize("sigma", [0.0, 1.2, 3.0, 4.0, 5.0])
+@pytest.mark.parametrize("H,W,pitch", [(257, 301, 301), (200, 320, 331), (130, 128, 160)])
+def test_gauss_blur_entry_point(sigma, H, W, pitch, oracle_lib):
+    """pysift_gauss_blur with caller pitches (odd and even) against the
+    oracle's sequential FMA-chain blur, bit for bit; radii 0 (copy), 5, 12,
+    16 and 20 (the general kernel)."""
+    import torch
+    from oracle import oracle
+    from pysift_b200 import _lib
+    from pysift_b200.core import gaussian_weights
+    lib = _lib.load()
+    rng = np.random.default_rng(H * W + int(sigma * 10))
+    img = rng.random((H, W), dtype=np.float32)
+    src = torch.zeros((H, pitch), dtype=torch.float32, device="cuda")
+    src[:, :W] = torch.from_numpy(img).cuda()
+    dst = torch.full((H, pitch), float("nan"), dtype=torch.float32, device="cuda")
+    k, radius = gaussian_weights(sigma) if sigma > 0 else (np.ones(1, np.float32), 0)
+    k = np.ascontiguousarray(k, dtype=np.float32)
+    rc = lib.pysift_gauss_blur(src.data_ptr(), pitch, dst.data_ptr(), pitch, H, W,
+                               k.ctypes.data_as(ctypes.c_void_p), radius, torch.cuda.current_stream().cuda_stream)
+    assert rc == 0, lib.pysift_last_error()
+    ref = oracle.gauss_blur(img, sigma) if sigma > 0 else img
+    assert np.array_equal(dst[:, :W].cpu().numpy(), ref)
+
+
+def test_detect_batch_matches_single_image_calls():
+    """detect_batch on uneven sizes over several streams returns, per image,
+    exactly what detectAndCompute returns for that image alone."""
+    from pysift_b200 import PySIFT
+    sizes = [(240, 320), (361, 479), (480, 640), (200, 300), (333, 517), (480, 640), (97, 131)]
+    imgs = [synthetic.scene(h, w, seed=30 + i) for i, (h, w) in enumerate(sizes)]
+    sift = PySIFT()
+    ref = [sift.detectAndCompute(im, gpu_output=True) for im in imgs]
+    for n_streams in (3, 1):
+        got = sift.detect_batch(imgs, n_streams=n_streams)
+        assert len(got) == len(imgs)
+        for (k1, d1), (k2, d2) in zip(ref, got):
+            assert np.array_equal(k1.cpu().numpy(), k2.cpu().numpy())
+            assert np.array_equal(d1.cpu().numpy(), d2.cpu().numpy())
+    host = sift.detect_batch(imgs[:3], n_streams=2, gpu_output=False)
+    assert np.array_equal(host[1][1], ref[1][1].cpu().numpy())
