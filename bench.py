@@ -17,6 +17,8 @@ stand in for the reference's datasets; see pysift_b200/synthetic.py):
   batch96_detect    PySIFT.detect_batch of 96 grayscale images of uneven sizes
                     (480x360 .. 4000x3000, aspect 4:3, 3:2, 16:9) over 8 streams,
                     next to the plain per-image detectAndCompute loop
+  batch32_stitch    GPUPyStitch.stitch_batch of 32 uneven pairs (1280x960 ..
+                    3000x2000, 4096 hypotheses each) next to sequential stitch()
 
 A step is one pass of the hot path over one input.  `value` is measured
 with CUDA events on the launching stream, inputs resident in HBM, L2
@@ -44,6 +46,7 @@ WORKLOADS = {
     "detect_640x480": dict(kind="detect", H=480, W=640, seed=0),
     "match_u8_8192": dict(kind="match", N=8192, M=8192, D=128, seed=0),
     "batch96_detect": dict(kind="batch_detect", n=96, seed=0, streams=8),
+    "batch32_stitch": dict(kind="batch_stitch", n=32, seed=0, streams=8, ransac_iters=4096, inlier_thresh=4.0),
 }
 DEFAULT_WORKLOAD = "stitch_pair_1280x960"
 METRIC = "SIFT Mpix/s + match-pairs/s on 1 B200: batched+BF16 vs plain, bit-exact"
@@ -186,6 +189,8 @@ def run_reference(args, wl, world, rank):
         return run_reference_match(args, wl)
     if wl["kind"] == "batch_detect":
         return run_reference_batch(args, wl)
+    if wl["kind"] == "batch_stitch":
+        return run_reference_pairs(args, wl)
     img = synthetic.scene(wl["H"], wl["W"], seed=wl["seed"])
     times = []
     from oracle import oracle
@@ -312,6 +317,34 @@ def run_match(args, wl, world, rank, local):
                 "h2d_bytes_per_step": int(a.nbytes + b.nbytes), "d2h_bytes_per_step": 4 + 8 * n_pairs},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_reference_pairs(args, wl):
+    """The oracle stitch of the batch's smallest pair, per step."""
+    from oracle import stitch_oracle as so
+    from pysift_b200 import synthetic
+    sizes = synthetic.pair_sizes(wl["n"], wl["seed"])
+    i = int(np.argmin([h * w for h, w in sizes]))
+    a, b, _ = synthetic.stitch_pair_fast(sizes[i][0], sizes[i][1], wl["seed"] * 1000 + i)
+    times = []
+    for k in range(args.warmup + args.steps):
+        orc = so.OracleStitch(ransac_iters=wl["ransac_iters"], inlier_thresh=wl["inlier_thresh"])
+        t0 = time.perf_counter()
+        orc.stitch(a, b)
+        if k >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    value = 1.0 / float(np.mean(times))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(times)) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "pair": list(sizes[i]), "seed": wl["seed"]},
+        "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": os.cpu_count(), "kind": "port",
+                         "sample": "the batch's smallest pair per step (oracle port, OpenMP)"},
+        "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -462,6 +495,119 @@ def run_batch_detect(args, wl, world, rank, local):
                          "sample": f"the {cpu_n} smallest images of the batch through the oracle (OpenMP)"},
         "e2e": {"value": world * mpix / (float(e2e_t.item()) / args.steps / 1e3), "unit": "Mpix/s",
                 "h2d_bytes_per_step": int(sum(im.nbytes for im in imgs)), "d2h_bytes_per_step": out_bytes},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _gen_pairs(n, seed):
+    """Seeded synthetic pairs, generated in a spawned process pool (before any
+    CUDA work in this process)."""
+    from concurrent.futures import ProcessPoolExecutor
+    import multiprocessing as mp
+    from pysift_b200 import synthetic
+    sizes = synthetic.pair_sizes(n, seed)
+    with ProcessPoolExecutor(max_workers=min(16, os.cpu_count() or 1), mp_context=mp.get_context("spawn")) as ex:
+        futs = [ex.submit(synthetic.stitch_pair_fast, h, w, seed * 1000 + i) for i, (h, w) in enumerate(sizes)]
+        return [f.result()[:2] for f in futs]
+
+
+def run_batch_stitch(args, wl, world, rank, local, pairs):
+    import torch
+    import torch.distributed as dist
+    from pysift_b200 import _lib
+    from pysift_b200.stitch import GPUPyStitch
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    mpix = sum(a.shape[0] * a.shape[1] + b.shape[0] * b.shape[1] for a, b in pairs) / 1e6
+    st = GPUPyStitch(ransac_iters=wl["ransac_iters"], inlier_thresh=wl["inlier_thresh"], save_output=False,
+                     verbose=False, device=dev)
+    g = [(torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)) for a, b in pairs]
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    lib = _lib.load()
+    ns = wl["streams"]
+    for _ in range(args.warmup):
+        st.stitch_batch(g, n_streams=ns)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn, steps):
+        ms = []
+        for _ in range(steps):
+            flush.zero_()
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return ms
+
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    launches0 = lib.pysift_launch_count()
+    with ClockSampler(local) as clk:
+        step_ms = timed(lambda: st.stitch_batch(g, n_streams=ns), args.steps)
+    launches = lib.pysift_launch_count() - launches0
+    t = torch.tensor([float(np.sum(step_ms))], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    metrics = st.last_batch_metrics
+    plain_ms = timed(lambda: [st.stitch(a, b) for a, b in g], max(1, min(2, args.steps)))
+    e2e_ms = []
+    for i in range(args.warmup + args.steps):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        panos = st.stitch_batch(pairs, n_streams=ns)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            e2e_ms.append(dt * 1e3)
+    e2e_t = torch.tensor([float(np.sum(e2e_ms))], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    if rank != 0:
+        return 0
+    P = len(pairs)
+    step_s = total_ms / args.steps / 1e3
+    peak, peak_kind = measured_peaks()
+    sift = st._detector
+    alg = sum(pyramid_alg_bytes(a.shape[0], a.shape[1], sift) + pyramid_alg_bytes(b.shape[0], b.shape[1], sift)
+              for a, b in pairs)
+    achieved = alg / step_s / 1e9
+    if args.no_cpu_baseline:
+        cpu_v, cpu_n = None, 0
+    else:
+        from oracle import stitch_oracle as so
+        small = min(pairs, key=lambda pr: pr[0].size)
+        orc = so.OracleStitch(ransac_iters=wl["ransac_iters"], inlier_thresh=wl["inlier_thresh"])
+        t0 = time.perf_counter()
+        orc.stitch(small[0], small[1])
+        cpu_v, cpu_n = 1.0 / (time.perf_counter() - t0), 1
+    line = {
+        "metric": METRIC, "value": world * P / step_s, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "pairs": P, "seed": wl["seed"], "mpix_per_batch": mpix,
+                   "streams": ns, "ransac_iters": wl["ransac_iters"], "inlier_thresh": wl["inlier_thresh"],
+                   "sizes": "1280x960 .. 3000x2000", "matches": [m["matches"] for m in metrics],
+                   "inliers": [m["inliers"] for m in metrics],
+                   "l2": "flushed (256 MiB write) before every step", "parallelism": f"replicas{world}"},
+        "mpix_per_s": world * mpix / step_s,
+        "plain_pairs_per_s": P / (float(np.mean(plain_ms)) / 1e3),
+        "roofline": {"bound": "hbm", "kernel": "whole batched stitch: pyramid-region algorithmic bytes of all "
+                     "views over the whole batch time (a lower bound for the pyramid kernels)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_kind, "alg_bytes_per_launch": alg, "traffic": None},
+        "cpu_baseline": {"value": cpu_v, "unit": "pairs/s", "cores": os.cpu_count(), "kind": "port",
+                         "sample": f"{cpu_n} stitch of the smallest pair by the oracle port (OpenMP)"},
+        "e2e": {"value": world * P / (float(e2e_t.item()) / args.steps / 1e3), "unit": "pairs/s",
+                "h2d_bytes_per_step": int(sum(a.nbytes + b.nbytes for a, b in pairs)),
+                "d2h_bytes_per_step": int(sum(p.nbytes for p in panos))},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
@@ -751,6 +897,8 @@ def main():
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
         return run_reference(args, wl, world, rank)
+    # inputs that take a process pool are made before any CUDA work
+    pairs = _gen_pairs(wl["n"], wl["seed"] + rank) if wl["kind"] == "batch_stitch" else None
     if world > 1:
         import datetime
         import torch.distributed as dist
@@ -762,6 +910,8 @@ def main():
             return run_match(args, wl, world, rank, local)
         if wl["kind"] == "batch_detect":
             return run_batch_detect(args, wl, world, rank, local)
+        if wl["kind"] == "batch_stitch":
+            return run_batch_stitch(args, wl, world, rank, local, pairs)
         return run_detect(args, wl, world, rank, local)
     finally:
         if world > 1:

@@ -225,16 +225,16 @@ class GPUPyStitch:
             self._rand[n_hyp] = r
         return r
 
-    def _ransac(self, p1, p2, n):
+    def _ransac(self, p1, p2, n, key=""):
         st = self._stream()
         n_hyp = int(self.ransac_iters)
         sz = ctypes.c_size_t()
         _lib.check(self._lib.pysift_ransac_workspace_size(n, n_hyp, ctypes.byref(sz)), "ransac ws")
-        ws = self._dev.get("ransac_ws", (int(sz.value) + 256,), torch.uint8, self.device)
+        ws = self._dev.get(key + "ransac_ws", (int(sz.value) + 256,), torch.uint8, self.device)
         wp, wn = _ptr_aligned(ws)
-        H = self._dev.get("ransac_H", (9,), torch.float64, self.device)
-        mask = self._dev.get("ransac_mask", (max(n, 1),), torch.uint8, self.device)
-        info = self._dev.get("ransac_info", (4,), torch.int32, self.device)
+        H = self._dev.get(key + "ransac_H", (9,), torch.float64, self.device)
+        mask = self._dev.get(key + "ransac_mask", (max(n, 1),), torch.uint8, self.device)
+        info = self._dev.get(key + "ransac_info", (4,), torch.int32, self.device)
         rnd = self._random_stream(n_hyp)
         _lib.check(self._lib.pysift_ransac(p1.data_ptr(), p2.data_ptr(), n, rnd.data_ptr(), n_hyp,
                                            float(self.inlier_thresh), float(self.sigma_max),
@@ -256,7 +256,10 @@ class GPUPyStitch:
         oy = max(0.0, -ay.min())
         return int(np.ceil(ax.max() + ox)) + 1, int(np.ceil(ay.max() + oy)) + 1, ox, oy
 
-    def _compose(self, img1, img2, H, max_canvas_px=400_000_000):
+    def _compose_enqueue(self, img1, img2, H, key="", max_canvas_px=400_000_000):
+        """Canvas geometry on the host, then warp + feather blend and the
+        coverage extents on the current stream; the extents are copied to
+        pinned host memory (read them after the stream has finished)."""
         hs, ws = img1.shape[:2]
         h2, w2 = img2.shape[:2]
         cw, ch, ox, oy = self._compute_canvas_size(img1.shape, img2.shape, H)
@@ -265,8 +268,8 @@ class GPUPyStitch:
         hinv = np.linalg.inv(H).astype(np.float32).ravel()
         iox, ioy = int(round(ox)), int(round(oy))
         st = self._stream()
-        out = self._dev.get("pano", (ch, cw, 3), torch.uint8, self.device)
-        ext = self._dev.get("extents", (2 * ch + 2 * cw,), torch.int32, self.device)
+        out = self._dev.get(key + "pano", (ch, cw, 3), torch.uint8, self.device)
+        ext = self._dev.get(key + "extents", (2 * ch + 2 * cw,), torch.int32, self.device)
         hb = (ctypes.c_float * 9)(*[float(v) for v in hinv])
         _lib.check(self._lib.pysift_warp_feather(img1.data_ptr(), hs, ws, img1.stride(0), img2.data_ptr(), h2, w2,
                                                  img2.stride(0), cw, ch, ctypes.cast(hb, ctypes.c_void_p),
@@ -274,19 +277,28 @@ class GPUPyStitch:
                                                  out.data_ptr(), None, None, None, ext.data_ptr(),
                                                  ext[ch:].data_ptr(), ext[2 * ch:].data_ptr(),
                                                  ext[2 * ch + cw:].data_ptr(), st), "pysift_warp_feather")
-        e = ext.cpu().numpy()
+        ext_host = torch.empty(ext.shape, dtype=torch.int32, pin_memory=True)
+        ext_host.copy_(ext, non_blocking=True)
+        return dict(out=out, ext_host=ext_host, canvas_w=cw, canvas_h=ch, ox=ox, oy=oy)
+
+    def _compose_crop(self, c):
+        """The inner-rectangle crop of a composed canvas (its extents on the host)."""
+        cw, ch, out = c["canvas_w"], c["canvas_h"], c["out"]
+        e = c["ext_host"].numpy()
         row_lo, row_hi = e[:ch], e[ch:2 * ch]
         col_lo, col_hi = e[2 * ch:2 * ch + cw], e[2 * ch + cw:]
         r0, r1, c0, c1, ir0, ir1, ic0, ic1, degenerate = self._autocrop_box(row_lo, row_hi, col_lo, col_hi)
         if r0 is None:
-            crop = out
-        elif degenerate:
-            crop = out[r0:r1 + 1, c0:c1 + 1]
-        else:
-            crop = out[r0 + ir0:r0 + ir1 + 1, c0 + ic0:c0 + ic1 + 1]
-        pano = self._to_host(crop)
-        covered = int(np.sum(np.maximum(row_hi - row_lo + 1, 0)))  # upper bound of coverage per row span
-        return pano, dict(canvas_w=cw, canvas_h=ch, ox=ox, oy=oy, coverage_rows_span=covered)
+            return out
+        if degenerate:
+            return out[r0:r1 + 1, c0:c1 + 1]
+        return out[r0 + ir0:r0 + ir1 + 1, c0 + ic0:c0 + ic1 + 1]
+
+    def _compose(self, img1, img2, H, max_canvas_px=400_000_000):
+        c = self._compose_enqueue(img1, img2, H, max_canvas_px=max_canvas_px)
+        torch.cuda.current_stream(self.device).synchronize()
+        pano = self._to_host(self._compose_crop(c))
+        return pano, dict(canvas_w=c["canvas_w"], canvas_h=c["canvas_h"], ox=c["ox"], oy=c["oy"])
 
     def _to_host(self, t):
         """Device tensor -> numpy array in page-locked memory from torch's
@@ -383,6 +395,120 @@ class GPUPyStitch:
             metrics.update(canvas_w=cm['canvas_w'], canvas_h=cm['canvas_h'], seam_rmse=float('nan'))
         self._last = dict(H=H, mask=mask_d, pairs=m["pairs"][:n_m], kp1=kp1, kp2=kp2, p1=p1, p2=p2, info=info)
         return pano, timings, metrics
+
+    def _side_streams(self, n):
+        if not hasattr(self, "_batch_streams"):
+            self._batch_streams = []
+        while len(self._batch_streams) < n:
+            self._batch_streams.append(torch.cuda.Stream(self.device))
+        return self._batch_streams[:n]
+
+    def stitch_batch(self, pairs, n_streams=8):
+        """Stitch many two-image pairs in one call; returns the panoramas in
+        input order.  Each phase runs for all pairs at once, spread over
+        `n_streams` CUDA streams, with one host synchronisation per phase:
+        (1) CLAHE and detection of every view, (2) matcher preparation and
+        matching, (3) RANSAC, (4) warp + feather blend, crop and readback.
+        Every pair gets exactly the result stitch(img1, img2) gives on this
+        instance; the PCA basis is fitted on the first pair if it is not yet
+        fitted.  No file is written.  The per-pair metrics are kept in
+        last_batch_metrics."""
+        from . import match as _match_mod
+        P = len(pairs)
+        if P == 0:
+            return []
+        ns = max(1, min(int(n_streams), 2 * P))
+        with torch.cuda.device(self.device):
+            main = torch.cuda.current_stream(self.device)
+            streams = self._side_streams(ns)
+            for s in streams:
+                s.wait_stream(main)
+            # (1) features
+            bgrs, grays = [], []
+            for p, pr in enumerate(pairs):
+                if len(pr) != 2:
+                    raise ValueError("stitch_batch takes (img1, img2) pairs")
+                for v in range(2):
+                    st = streams[(2 * p + v) % ns]
+                    with torch.cuda.stream(st):
+                        key = f"b{p}_{v}"
+                        bgr = self._upload_bgr(pr[v], key)
+                        bgrs.append(bgr)
+                        grays.append(self._gray_clahe(bgr, key))
+            for s in streams:
+                main.wait_stream(s)
+            feats = self._detector.detect_batch(grays, n_streams=ns, gpu_output=True)
+            metrics = [dict(kp1=int(feats[2 * p][0].shape[0]), kp2=int(feats[2 * p + 1][0].shape[0]))
+                       for p in range(P)]
+            for p, m in enumerate(metrics):
+                if m["kp1"] == 0 or m["kp2"] < 2:
+                    raise RuntimeError(f"pair {p}: Insufficient matches (0), need >= 4")
+            # (2) preparation + matching (the PCA basis from the first pair, as stitch() does)
+            if self._pca_matrix is None:
+                self._prepare(feats[0][1], feats[1][1])
+            for s in streams:
+                s.wait_stream(main)
+            matches = []
+            for p in range(P):
+                st = streams[p % ns]
+                with torch.cuda.stream(st):
+                    a, bq, _ = self._prepare(feats[2 * p][1], feats[2 * p + 1][1])
+                    matches.append(_match_mod.match_fp16(a, bq, self.match_ratio, stream=st))
+            for s in streams:
+                main.wait_stream(s)
+            counts = torch.cat([m["count"] for m in matches]).cpu().numpy()
+            # (3) RANSAC
+            for s in streams:
+                s.wait_stream(main)
+            rs = []
+            for p in range(P):
+                n_m = int(counts[p])
+                metrics[p]["matches"] = n_m
+                if n_m < 4:
+                    raise RuntimeError(f"pair {p}: Insufficient matches ({n_m}), need >= 4")
+                st = streams[p % ns]
+                with torch.cuda.stream(st):
+                    sst = st.cuda_stream
+                    p1 = torch.empty((n_m, 2), dtype=torch.float64, device=self.device)
+                    p2 = torch.empty((n_m, 2), dtype=torch.float64, device=self.device)
+                    m = matches[p]
+                    _lib.check(self._lib.pysift_gather_points(feats[2 * p][0].data_ptr(), m["pairs"].data_ptr(),
+                                                              m["count"].data_ptr(), n_m, 0, p1.data_ptr(), sst),
+                               "gather")
+                    _lib.check(self._lib.pysift_gather_points(feats[2 * p + 1][0].data_ptr(), m["pairs"].data_ptr(),
+                                                              m["count"].data_ptr(), n_m, 1, p2.data_ptr(), sst),
+                               "gather")
+                    rs.append(self._ransac(p1, p2, n_m, key=f"b{p}_"))
+            for s in streams:
+                main.wait_stream(s)
+            Hs = torch.stack([r[0] for r in rs]).cpu().numpy().reshape(P, 3, 3)
+            infos = torch.stack([r[2] for r in rs]).cpu().numpy()
+            # (4) compose
+            for s in streams:
+                s.wait_stream(main)
+            comps = []
+            for p in range(P):
+                n_in = int(infos[p][0])
+                metrics[p].update(inliers=n_in)
+                if n_in < 4:
+                    raise RuntimeError(f"pair {p}: Only {n_in} inliers after RANSAC, need >= 4")
+                st = streams[p % ns]
+                with torch.cuda.stream(st):
+                    comps.append(self._compose_enqueue(bgrs[2 * p], bgrs[2 * p + 1], Hs[p].copy(), key=f"b{p}_"))
+                metrics[p].update(canvas_w=comps[p]["canvas_w"], canvas_h=comps[p]["canvas_h"])
+            for s in streams:
+                main.wait_stream(s)
+            main.synchronize()
+            hosts = []
+            for c in comps:
+                crop = self._compose_crop(c).contiguous()
+                host = torch.empty(crop.shape, dtype=crop.dtype, pin_memory=True)
+                host.copy_(crop, non_blocking=True)
+                hosts.append(host)
+            main.synchronize()
+        self.last_batch_metrics = metrics
+        self._last_batch_H = Hs
+        return [h.numpy() for h in hosts]
 
     def stitch(self, *args):
         """Stitch two images (pysift/core.py:3972-4008); returns the BGR uint8

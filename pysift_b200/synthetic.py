@@ -118,6 +118,42 @@ def stitch_pair(H=960, W=1280, seed=0):
     return img1, img2, Hm
 
 
+def stitch_pair_fast(H=960, W=1280, seed=0):
+    """stitch_pair with the cheaper scene_fast source scene (for large batches)."""
+    import cv2
+    rng = _rng(seed)
+    Hm = random_homography(rng, W, H)
+    big_w, big_h = int(W * 2.2), int(H * 1.4)
+    oy = (big_h - H) // 2
+    gains = rng.uniform(0.8, 1.2, size=3).astype(np.float32)
+    base = scene_fast(big_h, big_w, seed=int(rng.integers(0, 2**31 - 1))).astype(np.float32)
+    big = np.clip(base[:, :, None] * gains[None, None, :], 0, 255).astype(np.float32)
+    S = np.array([[1, 0, 0], [0, 1, -oy], [0, 0, 1]], np.float64)
+    M2 = Hm @ S
+    v1 = big[oy:oy + H, :W]
+    v2 = cv2.warpPerspective(big, M2, (W, H), flags=cv2.INTER_LINEAR, borderMode=cv2.BORDER_REFLECT)
+    img1 = np.clip(np.rint(v1 + 2.0 * rng.standard_normal(v1.shape, dtype=np.float32)), 0, 255).astype(np.uint8)
+    img2 = np.clip(np.rint(v2 + 2.0 * rng.standard_normal(v2.shape, dtype=np.float32)), 0, 255).astype(np.uint8)
+    return img1, img2, Hm
+
+
+def pair_sizes(n=32, seed=0):
+    """Uneven stitch-pair sizes between 1280x960 and 3000x2000 (aspect 4:3 or 3:2)."""
+    rng = _rng(seed + 7)
+    out = []
+    for _ in range(n):
+        ah, aw = ((3, 4), (2, 3))[int(rng.integers(0, 2))]
+        w = int(rng.uniform(1280, 3000))
+        h = max(960, min(2000, int(round(w * ah / aw))))
+        out.append((h, w))
+    return out
+
+
+def batch_pairs(n=32, seed=0):
+    """n seeded BGR view pairs with the sizes of pair_sizes(n, seed)."""
+    return [stitch_pair_fast(h, w, seed=seed * 1000 + i)[:2] for i, (h, w) in enumerate(pair_sizes(n, seed))]
+
+
 def descriptor_sets(N=8192, M=8192, seed=0, D=128):
     """uint8 descriptor sets (N,D), (M,D); half of set 2 are noisy copies."""
     rng = _rng(seed)

@@ -227,3 +227,19 @@ def test_stitch_pair_end_to_end():
         assert np.mean(diff <= 1) > 0.99
     Ht_n = Ht / Ht[2, 2]
     assert np.allclose(Hg / Hg[2, 2], Ht_n, rtol=2e-2, atol=2e-2 * np.abs(Ht_n).max())
+
+
+def test_stitch_batch_matches_sequential_stitch():
+    """stitch_batch returns, pair for pair, the panorama that sequential
+    stitch() calls on an instance in the same state return."""
+    from pysift_b200.stitch import GPUPyStitch
+    pairs = [synthetic.stitch_pair_fast(h, w, seed=50 + i)[:2] for i, (h, w) in
+             enumerate([(480, 640), (600, 800), (500, 700)])]
+    seq = GPUPyStitch(ransac_iters=512, inlier_thresh=4.0, save_output=False)
+    ref = [seq.stitch(a, b) for a, b in pairs]
+    bat = GPUPyStitch(ransac_iters=512, inlier_thresh=4.0, save_output=False)
+    for n_streams in (4, 1):
+        got = bat.stitch_batch(pairs, n_streams=n_streams)
+        assert len(got) == len(pairs)
+        for r, g in zip(ref, got):
+            assert r.shape == g.shape and np.array_equal(r, g)
