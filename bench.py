@@ -14,6 +14,7 @@ stand in for the reference's datasets; see pysift_b200/synthetic.py):
   detect_640x480    detectAndCompute on one 640x480 scene
   match_u8_8192     exact ratio-test matching of two 8192 x 128 uint8-valued
                     descriptor sets (bf16 tcgen05 GEMM, exact against int64)
+  match_u8_8192_fp8 the same through the split-nibble e4m3 tcgen05 GEMM
   batch96_detect    PySIFT.detect_batch of 96 grayscale images of uneven sizes
                     (480x360 .. 4000x3000, aspect 4:3, 3:2, 16:9) over 8 streams,
                     next to the plain per-image detectAndCompute loop
@@ -45,6 +46,7 @@ WORKLOADS = {
     "detect_1280x960": dict(kind="detect", H=960, W=1280, seed=0),
     "detect_640x480": dict(kind="detect", H=480, W=640, seed=0),
     "match_u8_8192": dict(kind="match", N=8192, M=8192, D=128, seed=0),
+    "match_u8_8192_fp8": dict(kind="match", N=8192, M=8192, D=128, seed=0, variant="split_fp8"),
     "batch96_detect": dict(kind="batch_detect", n=96, seed=0, streams=8),
     "batch32_stitch": dict(kind="batch_stitch", n=32, seed=0, streams=8, ransac_iters=4096, inlier_thresh=4.0),
 }
@@ -237,11 +239,13 @@ def run_match(args, wl, world, rank, local):
     N, M, D = wl["N"], wl["M"], wl["D"]
     a, b = synthetic.descriptor_sets(N, M, seed=wl["seed"] + rank, D=D)
     ga, gb = torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)
+    split = wl.get("variant") == "split_fp8"
+    mfn = match.match_u8_split_fp8 if split else match.match_u8_exact
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     lib = _lib.load()
     for _ in range(args.warmup):
-        out = match.match_u8_exact(ga, gb)
+        out = mfn(ga, gb)
     torch.cuda.synchronize(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     step_ms = []
@@ -253,7 +257,7 @@ def run_match(args, wl, world, rank, local):
         for _ in range(args.steps):
             flush.zero_()
             e0.record(stream)
-            out = match.match_u8_exact(ga, gb)
+            out = mfn(ga, gb)
             e1.record(stream)
             e1.synchronize()
             step_ms.append(e0.elapsed_time(e1))
@@ -272,7 +276,7 @@ def run_match(args, wl, world, rank, local):
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
         da, db = ha.to(dev, non_blocking=True), hb.to(dev, non_blocking=True)
-        o = match.match_u8_exact(da, db)
+        o = mfn(da, db)
         cnt = int(o["count"].item())
         pairs_host = o["pairs"][:cnt].cpu()
         dt = time.perf_counter() - t0
@@ -286,6 +290,8 @@ def run_match(args, wl, world, rank, local):
     step_s = total_ms / args.steps / 1e3
     flops = 2.0 * N * M * D
     peak, peak_kind = measured_tensor_peak()
+    if split:
+        peak, peak_kind = 2.0 * peak, "2 x " + peak_kind + " (dense fp8 rate)"
     achieved = flops / step_s / 1e12
     if args.no_cpu_baseline:
         cpu_s, cpu_n = float("nan"), 0
@@ -301,12 +307,13 @@ def run_match(args, wl, world, rank, local):
     line = {
         "metric": METRIC, "value": world / step_s, "unit": "match-pairs/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "bf16", "data": "synthetic",
+        "vs_baseline": None, "dtype": "fp8-e4m3" if split else "bf16", "data": "synthetic",
         "config": {"workload": args.workload, "N": N, "M": M, "D": D, "seed": wl["seed"], "ratio": 0.75,
                    "mutual_matches": n_pairs, "l2": "flushed (256 MiB write) before every step",
                    "parallelism": f"replicas{world}"},
-        "roofline": {"bound": "tensor", "kernel": "whole match call (k_row_norms_u8 x2, k_match_rows x2, "
-                     "k_match_merge x2, k_match_mutual); flops 2*N*M*D counted once",
+        "roofline": {"bound": "tensor", "kernel": "whole match call (k_row_norms_u8 x2, "
+                     + ("k_split_nibbles_u8 x2, " if split else "") + "k_match_rows x2, k_match_merge x2, "
+                     "k_match_mutual); flops 2*N*M*D counted once" + (" (the e4m3 GEMM does 4x that)" if split else ""),
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                      "peak_source": peak_kind, "alg_flops_per_step": flops,
                      "traffic": committed_traffic(args.workload)},

@@ -144,7 +144,9 @@ int pysift_zoom2x_u8(const uint8_t* gray, int32_t H, int32_t W, int64_t pitch_by
  * mutual intersection of _match_features (pysift/core.py:2574-2701,
  * 2930-2940).  Per direction: best index, ratio-test pass flag; the mutual
  * pairs (i, j) in query order with distance sqrt(d1^2).  Ties between equal
- * scores go to the lower index.  D must be 64 or 128. */
+ * scores go to the lower index.  D must be 64 or 128.  Workspace mode
+ * exact_u8: 0 = pysift_match_fp16, 1 = pysift_match_u8_exact,
+ * 2 = pysift_match_u8_split_fp8. */
 int pysift_match_workspace_size(int32_t n1, int32_t n2, int32_t D, int32_t exact_u8, size_t* bytes);
 
 /* Reference semantics: fp16 operands (16-byte aligned rows), the fp32
@@ -161,6 +163,16 @@ int pysift_match_u8_exact(const uint8_t* d1, int32_t n1, const uint8_t* d2, int3
                           void* workspace, size_t workspace_bytes, int32_t* fwd_best, int32_t* fwd_pass,
                           int32_t* bwd_best, int32_t* bwd_pass, int32_t* pairs, float* pair_dist,
                           int32_t* pair_count, pysift_stream_t stream);
+
+/* The same exact matching through FP8: each uint8 value v = 16 h + l is split
+ * into e4m3 planes (16h, h, 16l, l all exact in e4m3) and one kind::f8f6f4
+ * tcgen05 GEMM over the 4D concatenated planes forms 256 h.h' + 16 h.l' +
+ * 16 l.h' + l.l' = v.v' (the four nibble GEMMs in one accumulation).
+ * Workspace from pysift_match_workspace_size(..., exact_u8 = 2, ...). */
+int pysift_match_u8_split_fp8(const uint8_t* d1, int32_t n1, const uint8_t* d2, int32_t n2, int32_t D, float ratio,
+                              void* workspace, size_t workspace_bytes, int32_t* fwd_best, int32_t* fwd_pass,
+                              int32_t* bwd_best, int32_t* bwd_pass, int32_t* pairs, float* pair_dist,
+                              int32_t* pair_count, pysift_stream_t stream);
 
 /* ---- stitch path (GPUPyStitch) ---- */
 

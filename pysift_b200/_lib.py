@@ -102,6 +102,9 @@ EXPORTS.update({
     "pysift_match_u8_exact": (ctypes.c_int, [c_void_p, c_int32, c_void_p, c_int32, c_int32, c_float, c_void_p,
                                              c_size_t, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                              c_void_p, c_void_p]),
+    "pysift_match_u8_split_fp8": (ctypes.c_int, [c_void_p, c_int32, c_void_p, c_int32, c_int32, c_float, c_void_p,
+                                                 c_size_t, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                                 c_void_p, c_void_p, c_void_p]),
 })
 
 

@@ -30,6 +30,7 @@
 
 #include "common.cuh"
 #include <cuda_bf16.h>
+#include <cuda_fp8.h>
 
 namespace pysift {
 
@@ -38,7 +39,7 @@ constexpr int NT = 128;           // train rows per tile = UMMA N
 constexpr int MATCH_THREADS = 128;
 constexpr unsigned SPIN_LIMIT = 1u << 26;  // bounded waits on the MMA barriers
 
-enum MatchMode { SIM_F16 = 0, DIST_BF16 = 1 };
+enum MatchMode { SIM_F16 = 0, DIST_BF16 = 1, SPLIT_FP8 = 2 };
 
 struct Top2 {  // best key and index, second-best key
     float k1, k2;
@@ -73,19 +74,19 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-// Stage rows [row0, row0 + 128) of a row-major (n x K) 16-bit matrix into the
-// core-matrix layout with cp.async; rows >= n are zero-filled.  A warp moves
-// 8 rows x 4 chunks per instruction: 64 contiguous bytes per row in global
-// memory, 512 contiguous bytes in shared memory.
-template <int K>
-__device__ __forceinline__ void stage_rows(uint8_t* dst, const uint16_t* src, int row0, int n) {
-    constexpr int KC = K / 8, G = KC / 4;
+// Stage rows [row0, row0 + 128) of a row-major matrix of RB-byte rows into
+// the core-matrix layout with cp.async; rows >= n are zero-filled.  A warp
+// moves 8 rows x 4 chunks per instruction: 64 contiguous bytes per row in
+// global memory, 512 contiguous bytes in shared memory.
+template <int RB>
+__device__ __forceinline__ void stage_rows(uint8_t* dst, const uint8_t* src, int row0, int n) {
+    constexpr int KC = RB / 16, G = KC / 4;
     for (int q = threadIdx.x; q < MT * KC; q += MATCH_THREADS) {
         const int lane = q & 31, blk = q >> 5;
         const int r = (blk / G) * 8 + (lane & 7), c = (blk % G) * 4 + (lane >> 3);
         const int gr = row0 + r;
         const bool valid = gr < n;
-        const uint16_t* s = valid ? src + (size_t)gr * K + c * 8 : src;
+        const uint8_t* s = valid ? src + (size_t)gr * RB + c * 16 : src;
         asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst + core_off(r, c, KC))),
                      "l"(s), "r"(valid ? 16 : 0)
                      : "memory");
@@ -108,8 +109,8 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 }
 
 struct RowScanArgs {
-    const uint16_t* q;   // n_q x K (fp16 or bf16 bits), row stride K
-    const uint16_t* t;   // n_t x K
+    const uint8_t* q;    // n_q rows of RB bytes (fp16 / bf16 / e4m3 codes)
+    const uint8_t* t;    // n_t rows of RB bytes
     int n_q, n_t;
     const int* norm_t;   // DIST_BF16: |t|^2 per train row
     int seg_tiles;       // train tiles per segment (blockIdx.y)
@@ -136,10 +137,10 @@ __device__ __forceinline__ void scan_chunk(const uint32_t (&v)[32], int col0, in
     }
 }
 
-template <int MODE, int K>
+template <int MODE, int RB>
 __global__ void __launch_bounds__(MATCH_THREADS) k_match_rows(const RowScanArgs args) {
-    constexpr int KC = K / 8;
-    constexpr uint32_t TILE_BYTES = MT * K * 2;
+    constexpr int KC = RB / 16;
+    constexpr uint32_t TILE_BYTES = MT * RB;
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t* sQ = smem;
     __shared__ __align__(8) uint64_t mbar[2];
@@ -161,8 +162,8 @@ __global__ void __launch_bounds__(MATCH_THREADS) k_match_rows(const RowScanArgs 
         asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mbar[1])), "r"(1));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    stage_rows<K>(sQ, args.q, q0, args.n_q);
-    stage_rows<K>(smem + TILE_BYTES, args.t, t_begin * NT, args.n_t);
+    stage_rows<RB>(sQ, args.q, q0, args.n_q);
+    stage_rows<RB>(smem + TILE_BYTES, args.t, t_begin * NT, args.n_t);
     asm volatile("cp.async.commit_group;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -184,7 +185,7 @@ __global__ void __launch_bounds__(MATCH_THREADS) k_match_rows(const RowScanArgs 
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         }
         // (2) prefetch train tile it+1 into the buffer tile it-1 used
-        if (it + 1 < nt) stage_rows<K>(smem + (1 + ((it + 1) & 1)) * TILE_BYTES, args.t, (t_begin + it + 1) * NT, args.n_t);
+        if (it + 1 < nt) stage_rows<RB>(smem + (1 + ((it + 1) & 1)) * TILE_BYTES, args.t, (t_begin + it + 1) * NT, args.n_t);
         asm volatile("cp.async.commit_group;" ::: "memory");
         // (3) tile it is staged: issue its MMAs into accumulator it&1
         if (it < nt) {
@@ -196,17 +197,26 @@ __global__ void __launch_bounds__(MATCH_THREADS) k_match_rows(const RowScanArgs 
             if (tid == 0) {
                 const uint32_t a0 = smem_u32(sQ), b0 = smem_u32(smem + (1 + (it & 1)) * TILE_BYTES);
                 const uint32_t d = tmem + (uint32_t)((it & 1) * NT);
-                constexpr uint32_t idesc = umma_idesc(MODE == SIM_F16 ? 0 : 1);
+                // f16 / bf16 (kind::f16, format 0 / 1) or e4m3 (kind::f8f6f4, format 0);
+                // either way one MMA covers 32 bytes of K: two core matrices
+                constexpr uint32_t idesc = umma_idesc(MODE == DIST_BF16 ? 1 : 0);
 #pragma unroll
-                for (int s = 0; s < K / 16; ++s) {
+                for (int s = 0; s < RB / 32; ++s) {
                     const uint64_t da = umma_desc(a0 + s * 256, 128, KC * 128);
                     const uint64_t db = umma_desc(b0 + s * 256, 128, KC * 128);
                     const uint32_t acc = s > 0 ? 1u : 0u;
-                    asm volatile(
-                        "{\n\t.reg .pred p;\n\t"
-                        "setp.ne.b32 p, %4, 0;\n\t"
-                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
-                        "l"(da), "l"(db), "r"(idesc), "r"(acc));
+                    if (MODE == SPLIT_FP8)
+                        asm volatile(
+                            "{\n\t.reg .pred p;\n\t"
+                            "setp.ne.b32 p, %4, 0;\n\t"
+                            "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+                            "l"(da), "l"(db), "r"(idesc), "r"(acc));
+                    else
+                        asm volatile(
+                            "{\n\t.reg .pred p;\n\t"
+                            "setp.ne.b32 p, %4, 0;\n\t"
+                            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+                            "l"(da), "l"(db), "r"(idesc), "r"(acc));
                 }
                 asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                                  smem_u32(&mbar[it & 1]))
@@ -221,7 +231,7 @@ __global__ void __launch_bounds__(MATCH_THREADS) k_match_rows(const RowScanArgs 
 #pragma unroll
             for (int chunk = 0; chunk < NT / 32; ++chunk) {
                 int nb_lane = 0;
-                if (MODE == DIST_BF16) {
+                if (MODE != SIM_F16) {
                     const int c = tcol0 + chunk * 32 + lane;
                     nb_lane = __float_as_int((float)(c < args.n_t ? args.norm_t[c] : 0));
                 }
@@ -336,10 +346,38 @@ __global__ void k_row_norms_u8(const uint8_t* __restrict__ d, int n, int D, int*
     for (int k = threadIdx.x; k < D; k += 32) {
         const int v = d[(size_t)i * D + k];
         s += v * v;
-        bf[(size_t)i * D + k] = __bfloat16_as_ushort(__float2bfloat16_rn((float)v));
+        if (bf) bf[(size_t)i * D + k] = __bfloat16_as_ushort(__float2bfloat16_rn((float)v));
     }
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(FULL_MASK, s, o);
     if (threadIdx.x == 0) norms[i] = s;
+}
+
+// Split-nibble e4m3 planes of uint8-valued rows, v = 16 h + l with h, l in
+// 0..15 (e4m3 holds 0..15 and 16 * (0..15) exactly).  The query-side row is
+// [16h | h | 16l | l], the train-side row [16h | 16l | h | l], each plane D
+// bytes, so that the 4D-long dot product of the two is
+// 256 h.h' + 16 h.l' + 16 l.h' + l.l' = v.v', the four nibble GEMMs in one.
+__global__ void k_split_nibbles_u8(const uint8_t* __restrict__ d, int n, int D, uint8_t* __restrict__ qside,
+                                   uint8_t* __restrict__ tside) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)n * D) return;
+    const size_t r = i / D, k = i - r * D;
+    const int v = d[i];
+    const float h = (float)(v >> 4), l = (float)(v & 15);
+    const uint8_t e16h = __nv_cvt_float_to_fp8(16.0f * h, __NV_SATFINITE, __NV_E4M3);
+    const uint8_t eh = __nv_cvt_float_to_fp8(h, __NV_SATFINITE, __NV_E4M3);
+    const uint8_t e16l = __nv_cvt_float_to_fp8(16.0f * l, __NV_SATFINITE, __NV_E4M3);
+    const uint8_t el = __nv_cvt_float_to_fp8(l, __NV_SATFINITE, __NV_E4M3);
+    uint8_t* q = qside + r * 4 * D;
+    uint8_t* t = tside + r * 4 * D;
+    q[k] = e16h;
+    q[D + k] = eh;
+    q[2 * D + k] = e16l;
+    q[3 * D + k] = el;
+    t[k] = e16h;
+    t[D + k] = e16l;
+    t[2 * D + k] = eh;
+    t[3 * D + k] = el;
 }
 
 static int sm_count() {
@@ -358,31 +396,35 @@ static void scan_split(int n_q, int n_t, int& nseg, int& seg_tiles) {
     nseg = ceil_div(n_tt, seg_tiles);
 }
 
-template <int MODE, int K>
+template <int MODE, int RB>
 static int launch_scan(const RowScanArgs& a, int nseg, cudaStream_t st) {
     // query block + two train buffers; at least 80 KB so that no more than two
     // CTAs (2 x 256 tensor-memory columns) share an SM
-    const size_t smem_launch = std::max((size_t)3 * MT * K * 2, (size_t)80 * 1024);
-    PYSIFT_CUDA_TRY(cudaFuncSetAttribute(k_match_rows<MODE, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    const size_t smem_launch = std::max((size_t)3 * MT * RB, (size_t)80 * 1024);
+    PYSIFT_CUDA_TRY(cudaFuncSetAttribute(k_match_rows<MODE, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem_launch));
     dim3 grid(ceil_div(a.n_q, MT), nseg);
-    k_match_rows<MODE, K><<<grid, MATCH_THREADS, smem_launch, st>>>(a);
+    k_match_rows<MODE, RB><<<grid, MATCH_THREADS, smem_launch, st>>>(a);
     PYSIFT_LAUNCH_CHECK("k_match_rows");
     return PYSIFT_OK;
 }
 
-template <int MODE>
-static int launch_scan_k(const RowScanArgs& a, int K, int nseg, cudaStream_t st) {
-    return K == 64 ? launch_scan<MODE, 64>(a, nseg, st) : launch_scan<MODE, 128>(a, nseg, st);
+// row bytes: 2 D for fp16 / bf16 rows, 4 D for the split e4m3 planes
+static int launch_scan_mode(int mode, const RowScanArgs& a, int D, int nseg, cudaStream_t st) {
+    if (mode == SIM_F16) return D == 64 ? launch_scan<SIM_F16, 128>(a, nseg, st) : launch_scan<SIM_F16, 256>(a, nseg, st);
+    if (mode == DIST_BF16)
+        return D == 64 ? launch_scan<DIST_BF16, 128>(a, nseg, st) : launch_scan<DIST_BF16, 256>(a, nseg, st);
+    return D == 64 ? launch_scan<SPLIT_FP8, 256>(a, nseg, st) : launch_scan<SPLIT_FP8, 512>(a, nseg, st);
 }
 
 struct MatchLayout {
     size_t off_fpart, off_bpart, off_fbest, off_fpass, off_fdist, off_bbest, off_bpass, off_bdist, off_err;
-    size_t off_na, off_nb, off_bfa, off_bfb;
+    size_t off_na, off_nb, off_bfa, off_bfb, off_qa, off_ta, off_qb, off_tb;
     size_t total;
 };
 
-static MatchLayout match_layout(int n1, int n2, int D, bool exact) {
+// exact: 0 = fp16 similarity, 1 = exact via bf16, 2 = exact via split e4m3
+static MatchLayout match_layout(int n1, int n2, int D, int exact) {
     MatchLayout l;
     size_t off = 0;
     auto take = [&](size_t bytes) {
@@ -400,12 +442,20 @@ static MatchLayout match_layout(int n1, int n2, int D, bool exact) {
     l.off_bpass = take((size_t)n2 * 4);
     l.off_bdist = take((size_t)n2 * 4);
     l.off_err = take(4);
-    l.off_na = l.off_nb = l.off_bfa = l.off_bfb = 0;
+    l.off_na = l.off_nb = l.off_bfa = l.off_bfb = l.off_qa = l.off_ta = l.off_qb = l.off_tb = 0;
     if (exact) {
         l.off_na = take((size_t)n1 * 4);
         l.off_nb = take((size_t)n2 * 4);
+    }
+    if (exact == 1) {
         l.off_bfa = take((size_t)n1 * D * 2);
         l.off_bfb = take((size_t)n2 * D * 2);
+    }
+    if (exact == 2) {
+        l.off_qa = take((size_t)n1 * D * 4);
+        l.off_ta = take((size_t)n1 * D * 4);
+        l.off_qb = take((size_t)n2 * D * 4);
+        l.off_tb = take((size_t)n2 * D * 4);
     }
     l.total = off;
     return l;
@@ -416,13 +466,16 @@ static T* wsp(void* ws, size_t off) {
     return reinterpret_cast<T*>(static_cast<char*>(ws) + off);
 }
 
-static int run_match(int mode, const uint16_t* a, int n1, const uint16_t* b, int n2, int D, float ratio_sq,
+// a / b: the query-side and train-side rows of each set (the same rows
+// except for the split e4m3 planes, whose two sides differ)
+static int run_match(int mode, const uint8_t* a_q, const uint8_t* a_t, int n1, const uint8_t* b_q,
+                     const uint8_t* b_t, int n2, int D, float ratio_sq,
                      const MatchLayout& l, void* ws, int* fbest_out, int* fpass_out, int* bbest_out, int* bpass_out,
                      int32_t* pairs, float* pdist, int32_t* count, cudaStream_t st) {
     int* err = wsp<int>(ws, l.off_err);
     PYSIFT_CUDA_TRY(cudaMemsetAsync(err, 0, 4, st));
-    const int* na = mode == DIST_BF16 ? wsp<int>(ws, l.off_na) : nullptr;
-    const int* nb = mode == DIST_BF16 ? wsp<int>(ws, l.off_nb) : nullptr;
+    const int* na = mode != SIM_F16 ? wsp<int>(ws, l.off_na) : nullptr;
+    const int* nb = mode != SIM_F16 ? wsp<int>(ws, l.off_nb) : nullptr;
     int* fbest = fbest_out ? fbest_out : wsp<int>(ws, l.off_fbest);
     int* fpass = fpass_out ? fpass_out : wsp<int>(ws, l.off_fpass);
     int* bbest = bbest_out ? bbest_out : wsp<int>(ws, l.off_bbest);
@@ -431,8 +484,8 @@ static int run_match(int mode, const uint16_t* a, int n1, const uint16_t* b, int
     float* bdist = wsp<float>(ws, l.off_bdist);
     for (int dir = 0; dir < 2; ++dir) {
         RowScanArgs s;
-        s.q = dir == 0 ? a : b;
-        s.t = dir == 0 ? b : a;
+        s.q = dir == 0 ? a_q : b_q;
+        s.t = dir == 0 ? b_t : a_t;
         s.n_q = dir == 0 ? n1 : n2;
         s.n_t = dir == 0 ? n2 : n1;
         s.norm_t = dir == 0 ? nb : na;
@@ -440,7 +493,7 @@ static int run_match(int mode, const uint16_t* a, int n1, const uint16_t* b, int
         s.error = err;
         int nseg;
         scan_split(s.n_q, s.n_t, nseg, s.seg_tiles);
-        const int rc = mode == SIM_F16 ? launch_scan_k<SIM_F16>(s, D, nseg, st) : launch_scan_k<DIST_BF16>(s, D, nseg, st);
+        const int rc = launch_scan_mode(mode, s, D, nseg, st);
         if (rc) return rc;
         const int* nq = dir == 0 ? na : nb;
         int* best = dir == 0 ? fbest : bbest;
@@ -469,7 +522,8 @@ extern "C" {
 int pysift_match_workspace_size(int32_t n1, int32_t n2, int32_t D, int32_t exact_u8, size_t* bytes) {
     PYSIFT_CHECK_ARG(bytes != nullptr, "bytes is NULL");
     PYSIFT_CHECK_ARG(n1 >= 0 && n2 >= 0 && (D == 64 || D == 128), "bad sizes (D must be 64 or 128)");
-    *bytes = match_layout(n1, n2, D, exact_u8 != 0).total;
+    PYSIFT_CHECK_ARG(exact_u8 >= 0 && exact_u8 <= 2, "exact_u8 must be 0, 1 or 2");
+    *bytes = match_layout(n1, n2, D, exact_u8).total;
     return PYSIFT_OK;
 }
 
@@ -481,14 +535,16 @@ int pysift_match_fp16(const uint16_t* d1, int32_t n1, const uint16_t* d2, int32_
     PYSIFT_CHECK_ARG(n1 >= 1 && n2 >= 1 && (D == 64 || D == 128), "bad sizes (D must be 64 or 128)");
     PYSIFT_CHECK_ARG((reinterpret_cast<uintptr_t>(d1) & 15) == 0 && (reinterpret_cast<uintptr_t>(d2) & 15) == 0,
                      "descriptor arrays must be 16-byte aligned");
-    MatchLayout l = match_layout(n1, n2, D, false);
+    MatchLayout l = match_layout(n1, n2, D, 0);
     if (workspace_bytes < l.total) {
         set_error("workspace %zu bytes < required %zu", workspace_bytes, l.total);
         return PYSIFT_ERR_WORKSPACE;
     }
     const float ratio_sq = (float)((double)ratio * (double)ratio);
-    return run_match(SIM_F16, d1, n1, d2, n2, D, ratio_sq, l, workspace, fwd_best, fwd_pass, bwd_best, bwd_pass, pairs,
-                     pair_dist, pair_count, reinterpret_cast<cudaStream_t>(stream));
+    const uint8_t* a = reinterpret_cast<const uint8_t*>(d1);
+    const uint8_t* b = reinterpret_cast<const uint8_t*>(d2);
+    return run_match(SIM_F16, a, a, n1, b, b, n2, D, ratio_sq, l, workspace, fwd_best, fwd_pass, bwd_best, bwd_pass,
+                     pairs, pair_dist, pair_count, reinterpret_cast<cudaStream_t>(stream));
 }
 
 int pysift_match_u8_exact(const uint8_t* d1, int32_t n1, const uint8_t* d2, int32_t n2, int32_t D, float ratio,
@@ -497,7 +553,7 @@ int pysift_match_u8_exact(const uint8_t* d1, int32_t n1, const uint8_t* d2, int3
                           int32_t* pair_count, pysift_stream_t stream) {
     PYSIFT_CHECK_ARG(d1 && d2 && workspace && pairs && pair_dist && pair_count, "NULL pointer argument");
     PYSIFT_CHECK_ARG(n1 >= 1 && n2 >= 1 && (D == 64 || D == 128), "bad sizes (D must be 64 or 128)");
-    MatchLayout l = match_layout(n1, n2, D, true);
+    MatchLayout l = match_layout(n1, n2, D, 1);
     if (workspace_bytes < l.total) {
         set_error("workspace %zu bytes < required %zu", workspace_bytes, l.total);
         return PYSIFT_ERR_WORKSPACE;
@@ -510,8 +566,39 @@ int pysift_match_u8_exact(const uint8_t* d1, int32_t n1, const uint8_t* d2, int3
     k_row_norms_u8<<<ceil_div(n2, 8), dim3(32, 8), 0, st>>>(d2, n2, D, wsp<int>(workspace, l.off_nb), bfb);
     PYSIFT_LAUNCH_CHECK("k_row_norms_u8");
     const float ratio_sq = (float)((double)ratio * (double)ratio);
-    return run_match(DIST_BF16, bfa, n1, bfb, n2, D, ratio_sq, l, workspace, fwd_best, fwd_pass, bwd_best, bwd_pass,
+    const uint8_t* a = reinterpret_cast<const uint8_t*>(bfa);
+    const uint8_t* b = reinterpret_cast<const uint8_t*>(bfb);
+    return run_match(DIST_BF16, a, a, n1, b, b, n2, D, ratio_sq, l, workspace, fwd_best, fwd_pass, bwd_best, bwd_pass,
                      pairs, pair_dist, pair_count, st);
+}
+
+int pysift_match_u8_split_fp8(const uint8_t* d1, int32_t n1, const uint8_t* d2, int32_t n2, int32_t D, float ratio,
+                              void* workspace, size_t workspace_bytes, int32_t* fwd_best, int32_t* fwd_pass,
+                              int32_t* bwd_best, int32_t* bwd_pass, int32_t* pairs, float* pair_dist,
+                              int32_t* pair_count, pysift_stream_t stream) {
+    PYSIFT_CHECK_ARG(d1 && d2 && workspace && pairs && pair_dist && pair_count, "NULL pointer argument");
+    PYSIFT_CHECK_ARG(n1 >= 1 && n2 >= 1 && (D == 64 || D == 128), "bad sizes (D must be 64 or 128)");
+    MatchLayout l = match_layout(n1, n2, D, 2);
+    if (workspace_bytes < l.total) {
+        set_error("workspace %zu bytes < required %zu", workspace_bytes, l.total);
+        return PYSIFT_ERR_WORKSPACE;
+    }
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    k_row_norms_u8<<<ceil_div(n1, 8), dim3(32, 8), 0, st>>>(d1, n1, D, wsp<int>(workspace, l.off_na), nullptr);
+    PYSIFT_LAUNCH_CHECK("k_row_norms_u8");
+    k_row_norms_u8<<<ceil_div(n2, 8), dim3(32, 8), 0, st>>>(d2, n2, D, wsp<int>(workspace, l.off_nb), nullptr);
+    PYSIFT_LAUNCH_CHECK("k_row_norms_u8");
+    uint8_t* qa = wsp<uint8_t>(workspace, l.off_qa);
+    uint8_t* ta = wsp<uint8_t>(workspace, l.off_ta);
+    uint8_t* qb = wsp<uint8_t>(workspace, l.off_qb);
+    uint8_t* tb = wsp<uint8_t>(workspace, l.off_tb);
+    k_split_nibbles_u8<<<(unsigned)ceil_div_ll((long long)n1 * D, 256), 256, 0, st>>>(d1, n1, D, qa, ta);
+    PYSIFT_LAUNCH_CHECK("k_split_nibbles_u8");
+    k_split_nibbles_u8<<<(unsigned)ceil_div_ll((long long)n2 * D, 256), 256, 0, st>>>(d2, n2, D, qb, tb);
+    PYSIFT_LAUNCH_CHECK("k_split_nibbles_u8");
+    const float ratio_sq = (float)((double)ratio * (double)ratio);
+    return run_match(SPLIT_FP8, qa, ta, n1, qb, tb, n2, D, ratio_sq, l, workspace, fwd_best, fwd_pass, bwd_best,
+                     bwd_pass, pairs, pair_dist, pair_count, st);
 }
 
 }  // extern "C"

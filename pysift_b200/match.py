@@ -8,6 +8,8 @@ Two entry points:
   mutual consistency.
 * ``match_u8_exact(a, b, ratio)``: exact squared-L2 matching of uint8-valued
   descriptors through bf16 tensor-core products (exact for 128-d uint8).
+* ``match_u8_split_fp8(a, b, ratio)``: the same through one e4m3 GEMM over
+  split-nibble planes (v = 16 h + l).
 
 Both take CUDA tensors and return CUDA tensors; ties go to the lower index.
 """
@@ -20,7 +22,7 @@ from . import _lib
 
 def _ws(lib, n1, n2, D, exact, device):
     sz = ctypes.c_size_t()
-    _lib.check(lib.pysift_match_workspace_size(n1, n2, D, 1 if exact else 0, ctypes.byref(sz)),
+    _lib.check(lib.pysift_match_workspace_size(n1, n2, D, int(exact), ctypes.byref(sz)),
                "pysift_match_workspace_size")
     return torch.empty(int(sz.value) + 256, dtype=torch.uint8, device=device)
 
@@ -56,11 +58,19 @@ def match_fp16(d1, d2, ratio=0.75, stream=None):
     assert d1.dtype == torch.float16 and d2.dtype == torch.float16
     d1 = d1.contiguous()
     d2 = d2.contiguous()
-    return _run(_lib.load().pysift_match_fp16, "pysift_match_fp16", d1, d2, ratio, False, stream)
+    return _run(_lib.load().pysift_match_fp16, "pysift_match_fp16", d1, d2, ratio, 0, stream)
 
 
 def match_u8_exact(a, b, ratio=0.75, stream=None):
     """a (N,D), b (M,D) uint8 CUDA tensors, D in {64, 128}."""
     assert a.dtype == torch.uint8 and b.dtype == torch.uint8
     return _run(_lib.load().pysift_match_u8_exact, "pysift_match_u8_exact", a.contiguous(), b.contiguous(),
-                ratio, True, stream)
+                ratio, 1, stream)
+
+
+def match_u8_split_fp8(a, b, ratio=0.75, stream=None):
+    """The exact matching of match_u8_exact through one FP8 (e4m3) tensor-core
+    GEMM over split-nibble planes: a (N,D), b (M,D) uint8 CUDA tensors."""
+    assert a.dtype == torch.uint8 and b.dtype == torch.uint8
+    return _run(_lib.load().pysift_match_u8_split_fp8, "pysift_match_u8_split_fp8", a.contiguous(), b.contiguous(),
+                ratio, 2, stream)

@@ -60,3 +60,36 @@ def test_fp16_reference_mode(n1, n2, D):
     n = int(out["count"].item())
     assert abs(n - len(ref["pairs"])) <= max(2, 0.005 * len(ref["pairs"]))
     assert n > n2 // 4
+
+
+@pytest.mark.parametrize("n1,n2,D", [(1000, 1000, 128), (300, 517, 128), (129, 1, 128), (2000, 1500, 64),
+                                     (8192, 8192, 128), (500, 16000, 128)])
+def test_split_fp8_bit_exact(n1, n2, D):
+    """The split-nibble e4m3 GEMM gives the same exact matches as the int64 oracle."""
+    import torch
+    from oracle import match_oracle as mo
+    from pysift_b200 import match
+    a, b = synthetic.descriptor_sets(n1, n2, seed=n1 + n2 + 1, D=D)
+    out = match.match_u8_split_fp8(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda())
+    ref = mo.match_u8_exact(a, b)
+    for k in ("fwd_best", "fwd_pass", "bwd_best", "bwd_pass"):
+        assert np.array_equal(out[k].cpu().numpy(), ref[k]), k
+    n = int(out["count"].item())
+    assert np.array_equal(out["pairs"][:n].cpu().numpy(), ref["pairs"])
+    assert np.array_equal(out["dist"][:n].cpu().numpy(), ref["dist"])
+
+
+def test_split_fp8_extreme_values_and_ties():
+    """All-255 and all-0 rows, duplicates: exact distances up to 128 * 255^2."""
+    import torch
+    from oracle import match_oracle as mo
+    from pysift_b200 import match
+    rng = np.random.default_rng(9)
+    a = rng.integers(0, 256, size=(300, 128), dtype=np.uint8)
+    a[:10] = 255
+    a[10:20] = 0
+    b = np.concatenate([a[:150], a[:100], rng.integers(0, 256, size=(90, 128), dtype=np.uint8)])
+    out = match.match_u8_split_fp8(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda())
+    ref = mo.match_u8_exact(a, b)
+    for k in ("fwd_best", "fwd_pass", "bwd_best", "bwd_pass"):
+        assert np.array_equal(out[k].cpu().numpy(), ref[k]), k
