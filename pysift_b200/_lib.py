@@ -102,6 +102,18 @@ EXPORTS.update({
     "pysift_match_u8_exact": (ctypes.c_int, [c_void_p, c_int32, c_void_p, c_int32, c_int32, c_float, c_void_p,
                                              c_size_t, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                              c_void_p, c_void_p]),
+    "pysift_desc_f32_forward": (ctypes.c_int, [c_void_p, c_int32, c_int32, c_int32, c_void_p, c_int32, c_int32,
+                                               c_void_p, c_void_p, c_void_p]),
+    "pysift_desc_f32_backward": (ctypes.c_int, [c_void_p, c_int32, c_int32, c_int32, c_void_p, c_int32, c_int32,
+                                                c_void_p, c_void_p, c_void_p, c_void_p]),
+    "pysift_blur_adjoint": (ctypes.c_int, [c_void_p, c_int32, c_void_p, c_int32, c_void_p, c_int32, c_int32, c_int32,
+                                           c_void_p, c_int32, c_int32, c_void_p]),
+    "pysift_warp_f32_forward": (ctypes.c_int, [c_void_p, c_int32, c_int32, c_int32, c_void_p, c_int32, c_int32,
+                                               c_int32, c_int32, c_void_p, c_double, c_double, c_int32, c_int32,
+                                               c_void_p, c_void_p]),
+    "pysift_warp_f32_backward": (ctypes.c_int, [c_void_p, c_int32, c_int32, c_int32, c_void_p, c_int32, c_int32,
+                                                c_int32, c_int32, c_void_p, c_double, c_double, c_int32, c_int32,
+                                                c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "pysift_match_u8_split_fp8": (ctypes.c_int, [c_void_p, c_int32, c_void_p, c_int32, c_int32, c_float, c_void_p,
                                                  c_size_t, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                                  c_void_p, c_void_p, c_void_p]),
