@@ -239,6 +239,37 @@ int pysift_warp_feather(const uint8_t* img1, int32_t hs, int32_t ws, int32_t pit
                         uint8_t* mask2, int32_t* row_lo, int32_t* row_hi, int32_t* col_lo, int32_t* col_hi,
                         pysift_stream_t stream);
 
+/* Differentiation (no counterpart in the reference, which has no autograd):
+ * float forms of the descriptor and of the warp + feather blend with
+ * hand-written adjoints, used by pysift_b200/grad.py.
+ *
+ * pysift_desc_f32_forward: float descriptors (L2 -> clip 0.2 -> L2, no
+ * RootSIFT) of n keypoints on one Gaussian level (kp: n rows [centre row,
+ * centre column, angle in degrees]; patch half-width ph, pysift/core.py:
+ * 693-835), the raw 128-bin histograms in hist.  pysift_desc_f32_backward
+ * adds dL/dlevel (glevel, same pitch as level) given dL/ddesc, recomputing
+ * the samples from the level and hist.  pysift_blur_adjoint: gin (+)= B^T gout
+ * for the separable blur B of pysift_gauss_blur with half-sample symmetric
+ * reflection (radius below both sides; weights on the device; tmp: H x W
+ * scratch).  pysift_warp_f32_forward/backward: the float warp of image 1 by
+ * hinv onto a cw x ch canvas, image 2 at (iox, ioy), linear feather blend;
+ * the backward adds dL/dimg1, dL/dimg2 and dL/dhinv (float64). */
+int pysift_desc_f32_forward(const float* level, int32_t H, int32_t W, int32_t pitch, const float* kp, int32_t n,
+                            int32_t ph, float* hist, float* desc, pysift_stream_t stream);
+int pysift_desc_f32_backward(const float* level, int32_t H, int32_t W, int32_t pitch, const float* kp, int32_t n,
+                             int32_t ph, const float* hist, const float* gdesc, float* glevel,
+                             pysift_stream_t stream);
+int pysift_blur_adjoint(const float* gout, int32_t gout_pitch, float* gin, int32_t gin_pitch, float* tmp,
+                        int32_t tmp_pitch, int32_t H, int32_t W, const float* weights_dev, int32_t radius,
+                        int32_t accumulate, pysift_stream_t stream);
+int pysift_warp_f32_forward(const float* img1, int32_t hs, int32_t ws, int32_t C, const float* img2, int32_t h2,
+                            int32_t w2, int32_t cw, int32_t ch, const double* hinv_host, double ox, double oy,
+                            int32_t iox, int32_t ioy, float* out, pysift_stream_t stream);
+int pysift_warp_f32_backward(const float* img1, int32_t hs, int32_t ws, int32_t C, const float* img2, int32_t h2,
+                             int32_t w2, int32_t cw, int32_t ch, const double* hinv_host, double ox, double oy,
+                             int32_t iox, int32_t ioy, const float* gout, float* gimg1, float* gimg2, double* ghinv,
+                             pysift_stream_t stream);
+
 /* Allocation-free 2x zoom (no counterpart in the reference; it exists for
  * callers that cannot allocate device memory at the call site, such as a
  * plugin inside a host application that owns the device heap).  Same result
