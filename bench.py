@@ -20,6 +20,9 @@ stand in for the reference's datasets; see pysift_b200/synthetic.py):
                     next to the plain per-image detectAndCompute loop
   batch32_stitch    GPUPyStitch.stitch_batch of 32 uneven pairs (1280x960 ..
                     3000x2000, 4096 hypotheses each) next to sequential stitch()
+  grad_16x1024x768  forward + backward of the differentiable descriptors (2000
+                    fixed keypoints per image) and of warp + feather blend on
+                    16 float32 1024x768 images
 
 A step is one pass of the hot path over one input.  `value` is measured
 with CUDA events on the launching stream, inputs resident in HBM, L2
@@ -49,6 +52,7 @@ WORKLOADS = {
     "match_u8_8192_fp8": dict(kind="match", N=8192, M=8192, D=128, seed=0, variant="split_fp8"),
     "batch96_detect": dict(kind="batch_detect", n=96, seed=0, streams=8),
     "batch32_stitch": dict(kind="batch_stitch", n=32, seed=0, streams=8, ransac_iters=4096, inlier_thresh=4.0),
+    "grad_16x1024x768": dict(kind="grad", n=16, H=768, W=1024, kps=2000, seed=0),
 }
 DEFAULT_WORKLOAD = "stitch_pair_1280x960"
 METRIC = "SIFT Mpix/s + match-pairs/s on 1 B200: batched+BF16 vs plain, bit-exact"
@@ -193,6 +197,9 @@ def run_reference(args, wl, world, rank):
         return run_reference_batch(args, wl)
     if wl["kind"] == "batch_stitch":
         return run_reference_pairs(args, wl)
+    if wl["kind"] == "grad":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no differentiable path"}))
+        return 0
     img = synthetic.scene(wl["H"], wl["W"], seed=wl["seed"])
     times = []
     from oracle import oracle
@@ -622,6 +629,96 @@ def run_batch_stitch(args, wl, world, rank, local, pairs):
     return 0
 
 
+def run_grad(args, wl, world, rank, local):
+    import cv2
+    import torch
+    from pysift_b200 import PySIFT, _lib, grad, synthetic
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    H, W, n = wl["H"], wl["W"], wl["n"]
+    rng = np.random.default_rng(wl["seed"] + rank)
+    sift = PySIFT(double_image=False, device=dev)
+    sift._cfg.output_limit = wl["kps"]
+    items = []
+    for i in range(n):
+        u8 = synthetic.scene(H, W, seed=wl["seed"] * 100 + i)
+        Hm = synthetic.random_homography(rng, W, H)
+        Hm[0, 2] *= 0.3  # a mild view change, as in the stitch pair
+        warped = cv2.warpPerspective(u8, Hm, (W, H), flags=cv2.INTER_LINEAR, borderMode=cv2.BORDER_REFLECT)
+        kp, _ = sift.detectAndCompute(u8, gpu_output=True)
+        octv = sift._buffers(H, W).octv[:kp.shape[0]]
+        table = grad.keypoints_for_grad(sift, kp, octv)
+        x = torch.from_numpy(u8.astype(np.float32) / 255.0).to(dev)
+        x2 = torch.from_numpy(warped.astype(np.float32) / 255.0).to(dev)
+        with torch.no_grad():
+            target = grad.descriptors(x2, table, sift)
+        geo = grad.canvas_geometry((H, W), (H, W), Hm)
+        h8 = torch.from_numpy(Hm.ravel()[:8].copy()).to(dev)
+        ptarget = torch.zeros((geo[1], geo[0], 1), dtype=torch.float32, device=dev)
+        items.append((x, x2, table, target, geo, h8, ptarget))
+    stream = torch.cuda.current_stream(dev)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+
+    def step():
+        df, db, wf, wb = 0.0, 0.0, 0.0, 0.0
+        for x, x2, table, target, geo, h8, ptarget in items:
+            xi = x.clone().requires_grad_(True)
+            ev[0].record(stream)
+            d = grad.descriptors(xi, table, sift)
+            loss = ((d - target) ** 2).sum()
+            ev[1].record(stream)
+            loss.backward()
+            ev[2].record(stream)
+            a = x.unsqueeze(-1).clone().requires_grad_(True)
+            bimg = x2.unsqueeze(-1).clone().requires_grad_(True)
+            hh = h8.clone().requires_grad_(True)
+            out = grad.warp_blend(a, bimg, hh, geo)
+            pl = ((out - ptarget) ** 2).sum()
+            ev[3].record(stream)
+            pl.backward()
+            ev[4].record(stream)
+            ev[4].synchronize()
+            df += ev[0].elapsed_time(ev[1])
+            db += ev[1].elapsed_time(ev[2])
+            wf += ev[2].elapsed_time(ev[3])
+            wb += ev[3].elapsed_time(ev[4])
+        return df, db, wf, wb
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    lib = _lib.load()
+    launches0 = lib.pysift_launch_count()
+    tot = np.zeros(4)
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            tot += np.array(step())
+    launches = lib.pysift_launch_count() - launches0
+    if rank != 0:
+        return 0
+    df, db, wf, wb = (tot / args.steps).tolist()
+    step_ms = df + db + wf + wb
+    line = {
+        "metric": METRIC, "value": world * n / ((df + db) / 1e3), "unit": "images/s (descriptor forward+backward)",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "images": n, "H": H, "W": W, "keypoints_per_image": wl["kps"],
+                   "loss1": "sum of squared descriptor differences to a homography-warped copy (constant target)",
+                   "loss2": "photometric L2 of warp + feather blend (gradients: both images, 8 homography params)",
+                   "pyramid": "recomputed in backward", "parallelism": f"replicas{world}"},
+        "desc_forward_ms": df, "desc_backward_ms": db, "desc_backward_over_forward": db / df,
+        "warp_forward_ms": wf, "warp_backward_ms": wb, "warp_backward_over_forward": wb / wf,
+        "roofline": None,
+        "cpu_baseline": None,
+        "e2e": None,
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_reference_stitch(args, wl):
     from oracle import stitch_oracle as so
     from pysift_b200 import synthetic
@@ -919,6 +1016,8 @@ def main():
             return run_batch_detect(args, wl, world, rank, local)
         if wl["kind"] == "batch_stitch":
             return run_batch_stitch(args, wl, world, rank, local, pairs)
+        if wl["kind"] == "grad":
+            return run_grad(args, wl, world, rank, local)
         return run_detect(args, wl, world, rank, local)
     finally:
         if world > 1:
