@@ -232,7 +232,8 @@ int pysift_dlt_homography(const double* pts1, const double* pts2, int32_t n, int
  * (pysift/core.py:3210-3239), placement of image 2 at (iox, ioy)
  * (pysift/core.py:3794-3800) and, where both cover the canvas, a linear
  * feather blend (weights 1 + distance to the image border).  Optional
- * outputs: warped image 1, both masks, per-row/column coverage extents. */
+ * outputs: warped image 1, both masks, per-row/column coverage extents;
+ * out may be NULL when warped image 1 and both masks are requested. */
 int pysift_warp_feather(const uint8_t* img1, int32_t hs, int32_t ws, int32_t pitch1, const uint8_t* img2, int32_t h2,
                         int32_t w2, int32_t pitch2, int32_t cw, int32_t ch, const float* hinv9, float ox, float oy,
                         int32_t iox, int32_t ioy, int32_t feather, uint8_t* out, uint8_t* warped, uint8_t* mask1,
@@ -269,6 +270,25 @@ int pysift_warp_f32_backward(const float* img1, int32_t hs, int32_t ws, int32_t 
                              int32_t w2, int32_t cw, int32_t ch, const double* hinv_host, double ox, double oy,
                              int32_t iox, int32_t ioy, const float* gout, float* gimg1, float* gimg2, double* ghinv,
                              pysift_stream_t stream);
+
+/* Reference composition (pysift/core.py:3386-3553, 3686-3714, 3794-3814):
+ * gain compensation, seam cost (colour difference + 0.05 |Sobel| of the
+ * average gray), dynamic-programming seam along the longer overlap axis,
+ * seam mask blurred with sigma 3 inside the overlap, Laplacian pyramid blend
+ * of n_levels levels and the paste with uint8 truncation.  warped1 / canvas2:
+ * cw x ch x 3 uint8 (BGR), masks: cw x ch bytes (0 / 1), all on the device.
+ * seam_k25: the 25 float32 taps of the sigma-3 seam-mask blur (host);
+ * gauss_w9: the 9 float64 taps of gaussian_filter(sigma = 1) (host).
+ * Outputs: pano (cw x ch x 3, zero where neither image covers), optionally
+ * both (union mask) and seam_rmse (one double on the device: the RMS colour
+ * difference over the overlap after gain, NaN when there is no overlap). */
+int pysift_place_image(const uint8_t* img, int32_t h, int32_t w, int32_t pitch, int32_t cw, int32_t ch, int32_t iox,
+                       int32_t ioy, uint8_t* canvas, uint8_t* mask, pysift_stream_t stream);
+int pysift_blend_workspace_size(int32_t cw, int32_t ch, int32_t n_levels, size_t* bytes);
+int pysift_blend_multiband(const uint8_t* warped1, const uint8_t* mask1, const uint8_t* canvas2,
+                           const uint8_t* mask2, int32_t cw, int32_t ch, int32_t n_levels, const float* seam_k25,
+                           const double* gauss_w9, void* workspace, size_t workspace_bytes, uint8_t* pano,
+                           uint8_t* both, double* seam_rmse, pysift_stream_t stream);
 
 /* Allocation-free 2x zoom (no counterpart in the reference; it exists for
  * callers that cannot allocate device memory at the call site, such as a

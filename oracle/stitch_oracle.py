@@ -4,7 +4,8 @@ Follows pysift/core.py:3720-3818: cv2 BGR->gray and CLAHE (the calls the
 reference itself makes on this machine: kornia is absent), SIFT (the
 OracleSIFT restatement with GPUPyStitch's n_octaves=4), stable top-k by
 response, L2 + PCA-64 + fp16 mutual ratio test (oracle/match_oracle.py),
-RANSAC/MAGSAC++ with LO refits (stitch_oracle.c), canvas, warp + feather
+RANSAC/MAGSAC++ with LO refits (stitch_oracle.c), canvas, warp, the
+reference's gain + seam + multiband composition (blend_oracle.py) or a feather
 (stitch_oracle.c) and the reference's inner-rectangle crop.
 """
 import ctypes
@@ -142,7 +143,9 @@ def autocrop(pano, both):
 
 class OracleStitch:
     def __init__(self, ransac_iters=1500, inlier_thresh=5.0, match_ratio=0.75, max_keypoints=8000, pca_dims=64,
-                 n_octaves=4, clahe_clip=2.0, clahe_tile=8, high_vram=True):
+                 n_octaves=4, clahe_clip=2.0, clahe_tile=8, high_vram=True, blend="multiband", n_blend_levels=6):
+        self.blend = blend
+        self.n_blend_levels = n_blend_levels
         self.ransac_iters = ransac_iters
         self.inlier_thresh = inlier_thresh
         self.match_ratio = match_ratio
@@ -185,6 +188,13 @@ class OracleStitch:
         H, mask, info, _ = ransac(p1, p2, self.ransac_iters, self.inlier_thresh, self.inlier_thresh)
         cw, ch, ox, oy = canvas_size(img1.shape, img2.shape, H)
         hinv = np.linalg.inv(H).astype(np.float32)
-        out, warped, m1, m2 = warp_feather(img1, img2, hinv, cw, ch, ox, oy, int(round(ox)), int(round(oy)))
+        iox, ioy = int(round(ox)), int(round(oy))
+        out, warped, m1, m2 = warp_feather(img1, img2, hinv, cw, ch, ox, oy, iox, ioy)
+        if self.blend == "multiband":
+            from . import blend_oracle
+            canvas2 = np.zeros((ch, cw, 3), np.uint8)
+            ye, xe = min(ioy + img2.shape[0], ch), min(iox + img2.shape[1], cw)
+            canvas2[ioy:ye, iox:xe] = img2[:ye - ioy, :xe - iox]
+            out, _ = blend_oracle.blend_pair(warped, m1, canvas2, m2, self.n_blend_levels)
         pano = autocrop(out, m1 | m2)
         return dict(pano=pano, H=H, mask=mask, info=info, pairs=pairs, p1=p1, p2=p2, n1=len(pts1), n2=len(pts2))

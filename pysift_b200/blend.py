@@ -1,0 +1,99 @@
+"""The reference's two-image composition on the device: gain compensation,
+dynamic-programming seam and Laplacian (multi-band) blend
+(GPUPyStitch._blend_pair, pysift/core.py:3686-3714; _find_seam 3386-3472;
+_multiband_blend 3495-3553; the paste of _stitch_pair 3806-3809) as one
+C-ABI call, pysift_blend_multiband, with no host synchronisation.
+
+Arithmetic: float32 images; gaussian_filter(sigma=1), sobel and
+zoom(order=1) with scipy.ndimage's float64 line sums (the algorithms
+cupyx.scipy.ndimage implements); the seam DP in float64 with numpy's
+first-minimum tie order.  Two steps take a canonical form: the overlap means
+of the gain are exact (the reference takes float32 pairwise means), and the
+sigma-3 seam-mask blur is the separable 25-tap filter of :func:`seam_kernel`
+with reflect-101 borders and float64 sums (the reference calls
+cv2.GaussianBlur).
+"""
+import numpy as np
+import torch
+
+from . import _lib
+
+
+def seam_kernel(sigma=3.0, taps=25):
+    """float32 taps of the seam-mask blur: exp(-x^2 / (2 sigma^2)) normalised
+    (the kernel cv2.GaussianBlur(sigmaX=3) builds: 25 taps for sigma 3)."""
+    x = np.arange(taps, dtype=np.float64) - (taps - 1) / 2.0
+    t = np.exp((-0.5 / (sigma * sigma)) * (x * x))
+    return (t / t.sum()).astype(np.float32)
+
+
+def gauss_weights(sigma=1.0, truncate=4.0):
+    """float64 taps of scipy.ndimage.gaussian_filter1d(sigma) (radius
+    int(truncate * sigma + 0.5))."""
+    r = int(truncate * sigma + 0.5)
+    x = np.arange(-r, r + 1)
+    p = np.exp(-0.5 / (sigma * sigma) * x ** 2)
+    return p / p.sum()
+
+
+_SEAM_K = seam_kernel()
+_GAUSS_W = np.ascontiguousarray(gauss_weights(), dtype=np.float64)
+
+
+def workspace_bytes(cw, ch, n_levels=6):
+    lib = _lib.load()
+    import ctypes
+    n = ctypes.c_size_t()
+    _lib.check(lib.pysift_blend_workspace_size(int(cw), int(ch), int(n_levels), ctypes.byref(n)),
+               "pysift_blend_workspace_size")
+    return n.value
+
+
+def place_image(img, cw, ch, iox, ioy, canvas=None, mask=None, stream=None):
+    """Image 2 (h, w, 3 uint8 on the device) pasted on a zero canvas at
+    (iox, ioy) (pysift/core.py:3794-3800); returns (canvas, mask)."""
+    lib = _lib.load()
+    dev = img.device
+    if canvas is None:
+        canvas = torch.empty((ch, cw, 3), dtype=torch.uint8, device=dev)
+    if mask is None:
+        mask = torch.empty((ch, cw), dtype=torch.uint8, device=dev)
+    st = stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
+    h, w = img.shape[:2]
+    _lib.check(lib.pysift_place_image(img.data_ptr(), h, w, img.stride(0), cw, ch, int(iox), int(ioy),
+                                      canvas.data_ptr(), mask.data_ptr(), st), "pysift_place_image")
+    return canvas, mask
+
+
+def blend_multiband(warped1, mask1, canvas2, mask2, n_levels=6, workspace=None, pano=None, both=None,
+                    seam_rmse=None, stream=None):
+    """_blend_pair + paste: warped1 / canvas2 (ch, cw, 3) uint8 and the masks
+    (ch, cw) uint8 / bool on the device.  Returns (pano uint8 (ch, cw, 3),
+    both uint8 (ch, cw), seam_rmse float64 (1,)), all on the device and
+    enqueued on the current stream."""
+    lib = _lib.load()
+    ch, cw = mask1.shape
+    dev = mask1.device
+    for t in (warped1, canvas2):
+        if t.shape != (ch, cw, 3) or t.dtype != torch.uint8 or not t.is_contiguous() or t.device != dev:
+            raise ValueError("warped1 / canvas2 must be contiguous (ch, cw, 3) uint8 on the masks' device")
+    m1 = mask1.view(torch.uint8) if mask1.dtype == torch.bool else mask1
+    m2 = mask2.view(torch.uint8) if mask2.dtype == torch.bool else mask2
+    if m1.dtype != torch.uint8 or m2.shape != (ch, cw) or not (m1.is_contiguous() and m2.is_contiguous()):
+        raise ValueError("masks must be contiguous (ch, cw) uint8 or bool")
+    need = workspace_bytes(cw, ch, n_levels)
+    if workspace is None or workspace.numel() < need + 256:
+        workspace = torch.empty(need + 256, dtype=torch.uint8, device=dev)
+    wp = workspace.data_ptr() + ((-workspace.data_ptr()) % 256)
+    if pano is None:
+        pano = torch.empty((ch, cw, 3), dtype=torch.uint8, device=dev)
+    if both is None:
+        both = torch.empty((ch, cw), dtype=torch.uint8, device=dev)
+    if seam_rmse is None:
+        seam_rmse = torch.empty(1, dtype=torch.float64, device=dev)
+    st = stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
+    _lib.check(lib.pysift_blend_multiband(warped1.data_ptr(), m1.data_ptr(), canvas2.data_ptr(), m2.data_ptr(), cw,
+                                          ch, int(n_levels), _SEAM_K.ctypes.data, _GAUSS_W.ctypes.data, wp, need,
+                                          pano.data_ptr(), both.data_ptr(), seam_rmse.data_ptr(), st),
+               "pysift_blend_multiband")
+    return pano, both, seam_rmse

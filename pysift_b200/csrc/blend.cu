@@ -1,0 +1,720 @@
+// blend.cu -- the reference's two-image composition on the GPU: gain
+// compensation, seam cost, dynamic-programming seam, seam mask and the
+// 6-level Laplacian (multi-band) blend (pysift/core.py:3286-3553, 3686-3714,
+// 3794-3814), with no host synchronisation.
+//
+// Arithmetic follows the numpy / scipy.ndimage restatement (the algorithms
+// cupyx implements): float32 images and elementwise ops without contraction;
+// gaussian_filter(sigma = 1) and sobel as scipy's correlate1d does them
+// (float64 sums, symmetric filters as w0 * x[i] + sum_k w_k (x[i-k] + x[i+k])
+// from the outermost tap in, half-sample symmetric reflection, axis 0 then
+// axis 1, float32 between the passes); zoom(order = 1) with the coordinate
+// k * (in - 1) / (out - 1) and products ((v * w_row) * w_col) summed over the
+// 2 x 2 corners in row-major order, in float64; the DP in float64 with
+// numpy's first-minimum tie order.  Canonical choices: the gain means are
+// exact (int64 sums / count); the seam-mask blur (cv2.GaussianBlur, sigma 3)
+// is separable with the float32 kernel getGaussianKernel(25, 3), reflect-101,
+// rows then columns, float64 sums.
+#include <cstdint>
+
+#include "common.cuh"
+
+namespace pysift {
+
+constexpr double BL_INF = 1e18;
+
+__device__ __forceinline__ int refl_half(int i, int n) {
+    while (i < 0 || i >= n) {
+        if (i < 0) i = -i - 1;
+        if (i >= n) i = 2 * n - 1 - i;
+    }
+    return i;
+}
+
+__device__ __forceinline__ int refl_101(int i, int n) {
+    if (n == 1) return 0;
+    while (i < 0 || i >= n) {
+        if (i < 0) i = -i;
+        if (i >= n) i = 2 * n - 2 - i;
+    }
+    return i;
+}
+
+struct BlendCtl {
+    unsigned long long sum1[3], sum2[3], n_ov, sq;
+    float gain[3];
+    int have_ov, vertical, first_side;  // first_side: image 1 left of (vertical) / above the seam
+    int line0, line1;                   // first and last DP line holding overlap
+};
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ int warp_or(int v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v |= __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Per pixel: overlap sums (exact) and line flags per row and column
+// (bit 0 overlap, bit 1 image 1 only, bit 2 image 2 only).  One row per block.
+__global__ void __launch_bounds__(256) k_blend_stats(const uint8_t* __restrict__ w1, const uint8_t* __restrict__ m1,
+                                                     const uint8_t* __restrict__ c2, const uint8_t* __restrict__ m2,
+                                                     int cw, BlendCtl* ctl, int* __restrict__ rowf,
+                                                     int* __restrict__ colf) {
+    __shared__ unsigned int s[7];
+    __shared__ int s_or;
+    if (threadIdx.x < 7) s[threadIdx.x] = 0u;
+    if (threadIdx.x == 0) s_or = 0;
+    __syncthreads();
+    const int v = blockIdx.y;
+    int f_row = 0;
+    unsigned int acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < cw; u += gridDim.x * blockDim.x) {
+        const long long p = (long long)v * cw + u;
+        const bool a = m1[p] != 0, b = m2[p] != 0;
+        const int f = (a && b ? 1 : 0) | (a && !b ? 2 : 0) | (!a && b ? 4 : 0);
+        if (f) atomicOr(&colf[u], f);
+        f_row |= f;
+        if (a && b) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                acc[c] += w1[p * 3 + c];
+                acc[3 + c] += c2[p * 3 + c];
+            }
+            acc[6] += 1u;
+        }
+    }
+    f_row = warp_or(f_row);
+#pragma unroll
+    for (int k = 0; k < 7; ++k) acc[k] = warp_sum(acc[k]);
+    if ((threadIdx.x & 31) == 0) {
+        if (f_row) atomicOr(&s_or, f_row);
+        if (acc[6]) {
+#pragma unroll
+            for (int k = 0; k < 7; ++k) atomicAdd(&s[k], acc[k]);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (s_or) atomicOr(&rowf[v], s_or);
+        if (s[6]) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                atomicAdd(&ctl->sum1[c], (unsigned long long)s[c]);
+                atomicAdd(&ctl->sum2[c], (unsigned long long)s[3 + c]);
+            }
+            atomicAdd(&ctl->n_ov, (unsigned long long)s[6]);
+        }
+    }
+}
+
+// block-wide sums of 6 integers (1024 threads)
+__device__ void block_sum6(long long v[6], long long* sh /* [32][6] */) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) v[k] = warp_sum(v[k]);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) sh[w * 6 + k] = v[k];
+    }
+    __syncthreads();
+    if (w == 0) {
+        const int nw = blockDim.x >> 5;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            long long t = l < nw ? sh[l * 6 + k] : 0;
+            v[k] = warp_sum(t);
+        }
+    }
+}
+
+// gain (pysift/core.py:3692-3699) and the seam orientation (pysift/core.py:3424-3438)
+__global__ void __launch_bounds__(1024) k_blend_decide(BlendCtl* ctl, const int* __restrict__ rowf,
+                                                       const int* __restrict__ colf, int cw, int ch) {
+    __shared__ long long sh[32 * 6];
+    __shared__ long long s_rows[6];
+    __shared__ int s_lo, s_hi;
+    // rows: {n overlap rows, n rows with image 1 only, sum of their indices, same for image 2, -}
+    long long v[6] = {0, 0, 0, 0, 0, 0};
+    for (int r = threadIdx.x; r < ch; r += blockDim.x) {
+        const int f = rowf[r];
+        if (f & 1) v[0] += 1;
+        if (f & 2) { v[1] += 1; v[2] += r; }
+        if (f & 4) { v[3] += 1; v[4] += r; }
+    }
+    block_sum6(v, sh);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) s_rows[k] = v[k];
+    }
+    __syncthreads();
+    long long c[6] = {0, 0, 0, 0, 0, 0};
+    for (int u = threadIdx.x; u < cw; u += blockDim.x) {
+        const int f = colf[u];
+        if (f & 1) c[0] += 1;
+        if (f & 2) { c[1] += 1; c[2] += u; }
+        if (f & 4) { c[3] += 1; c[4] += u; }
+    }
+    block_sum6(c, sh);
+    if (threadIdx.x == 0) {
+        const unsigned long long n = ctl->n_ov;
+        ctl->have_ov = n > 0;
+        for (int k = 0; k < 3; ++k) {
+            float g = 1.0f;
+            if (n > 0) {
+                const float mean1 = (float)((double)ctl->sum1[k] / (double)n);
+                const float mean2 = (float)((double)ctl->sum2[k] / (double)n);
+                g = (mean2 + 1e-3f) / (mean1 + 1e-3f);
+                g = g < 0.5f ? 0.5f : (g > 2.0f ? 2.0f : g);
+            }
+            ctl->gain[k] = g;
+        }
+        const bool vert = s_rows[0] >= c[0];
+        ctl->vertical = vert;
+        if (vert)
+            ctl->first_side = c[1] == 0 || c[3] == 0 || (double)c[2] / (double)c[1] <= (double)c[4] / (double)c[3];
+        else
+            ctl->first_side = s_rows[1] == 0 || s_rows[3] == 0 ||
+                              (double)s_rows[2] / (double)s_rows[1] <= (double)s_rows[4] / (double)s_rows[3];
+        s_lo = 0x7fffffff;
+        s_hi = -1;
+    }
+    __syncthreads();
+    const bool vert = ctl->vertical != 0;
+    const int L = vert ? ch : cw;
+    const int* lf = vert ? rowf : colf;
+    for (int i = threadIdx.x; i < L; i += blockDim.x)
+        if (lf[i] & 1) {
+            atomicMin(&s_lo, i);
+            atomicMax(&s_hi, i);
+        }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ctl->line0 = s_lo;
+        ctl->line1 = s_hi;
+    }
+}
+
+// gained image 1, the pyramid inputs I1 / I2 (pysift/core.py:3703-3708),
+// colour cost, average gray and the seam-RMSE sum (pysift/core.py:3555-3562)
+__global__ void k_blend_prepare(const uint8_t* __restrict__ w1, const uint8_t* __restrict__ m1,
+                                const uint8_t* __restrict__ c2, const uint8_t* __restrict__ m2, int cw,
+                                BlendCtl* ctl, float* __restrict__ I1, float* __restrict__ I2,
+                                float* __restrict__ color, float* __restrict__ avg) {
+    const int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
+    unsigned int sq = 0;
+    if (u < cw) {
+        const long long p = (long long)v * cw + u;
+        const bool a = m1[p] != 0, b = m2[p] != 0;
+        const bool gained = ctl->have_ov != 0;
+        float g1[3], g2[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            float x = (float)w1[p * 3 + c];
+            if (gained) {
+                x = x * ctl->gain[c];
+                x = x < 0.0f ? 0.0f : (x > 255.0f ? 255.0f : x);
+            }
+            g1[c] = x;
+            g2[c] = (float)c2[p * 3 + c];
+            if (a && b) {
+                const int d = (int)x - (int)c2[p * 3 + c];
+                sq += (unsigned int)(d * d);
+            }
+        }
+        const float d0 = g1[0] - g2[0], d1 = g1[1] - g2[1], d2 = g1[2] - g2[2];
+        color[p] = sqrtf((d0 * d0 + d1 * d1) + d2 * d2);
+        const float s0 = (g1[0] + g2[0]) * 0.5f, s1 = (g1[1] + g2[1]) * 0.5f, s2 = (g1[2] + g2[2]) * 0.5f;
+        avg[p] = ((s0 + s1) + s2) / 3.0f;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            I1[p * 3 + c] = a ? g1[c] : (b ? g2[c] : 0.0f);
+            I2[p * 3 + c] = b ? g2[c] : (a ? g1[c] : 0.0f);
+        }
+    }
+    sq = warp_sum(sq);
+    if ((threadIdx.x & 31) == 0 && sq) atomicAdd(&ctl->sq, (unsigned long long)sq);
+}
+
+// scipy sobel, first pass: derivative [-1, 0, 1] along `axis` (antisymmetric: (x[i+1] - x[i-1]))
+__global__ void k_sobel_deriv(const float* __restrict__ in, float* __restrict__ dx, float* __restrict__ dy, int W,
+                              int H) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= W) return;
+    const long long row = (long long)y * W;
+    dx[row + x] = (float)((double)in[row + refl_half(x + 1, W)] - (double)in[row + refl_half(x - 1, W)]);
+    dy[row + x] = (float)((double)in[(long long)refl_half(y + 1, H) * W + x] -
+                          (double)in[(long long)refl_half(y - 1, H) * W + x]);
+}
+
+// second pass: [1, 2, 1] along the other axis; then the cost (pysift/core.py:3411-3420).
+// The DP reads `dpc`: the cost where both images cover the canvas, else -1,
+// laid out line by line (transposed for a horizontal seam).
+__global__ void k_sobel_cost(const float* __restrict__ dxp, const float* __restrict__ dyp,
+                             const float* __restrict__ color, const uint8_t* __restrict__ m1,
+                             const uint8_t* __restrict__ m2, const BlendCtl* ctl, float* __restrict__ dpc, int W,
+                             int H) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= W) return;
+    const long long p = (long long)y * W + x;
+    const double gxd = 2.0 * (double)dxp[p] + ((double)dxp[(long long)refl_half(y - 1, H) * W + x] +
+                                               (double)dxp[(long long)refl_half(y + 1, H) * W + x]);
+    const double gyd = 2.0 * (double)dyp[p] + ((double)dyp[(long long)y * W + refl_half(x - 1, W)] +
+                                               (double)dyp[(long long)y * W + refl_half(x + 1, W)]);
+    const float gx = (float)gxd, gy = (float)gyd;
+    const float c = color[p] + 0.05f * sqrtf(gx * gx + gy * gy);
+    const float out = (m1[p] && m2[p]) ? c : -1.0f;
+    if (ctl->vertical) dpc[p] = out;
+    else dpc[(long long)x * H + y] = out;
+}
+
+// Dynamic-programming seam (pysift/core.py:3286-3383) in one CTA: lines in
+// order (rows for a vertical seam, columns for a horizontal one), positions
+// in parallel; the two DP lines live in shared memory when they fit.
+// dir[i][j] is the argmin (0 left, 1 centre, 2 right) of line i.
+__global__ void __launch_bounds__(1024) k_blend_dp(const float* __restrict__ dpc, const int* __restrict__ rowf,
+                                                   const int* __restrict__ colf, int cw, int ch,
+                                                   const BlendCtl* ctl, double* __restrict__ rowA,
+                                                   double* __restrict__ rowB, int use_smem,
+                                                   uint8_t* __restrict__ dir, int* __restrict__ seam) {
+    extern __shared__ double dp_sm[];
+    if (!ctl->have_ov) return;
+    const bool vert = ctl->vertical != 0;
+    const int L = vert ? ch : cw, M = vert ? cw : ch;
+    const int* lf = vert ? rowf : colf;
+    const int i0 = ctl->line0, i1 = ctl->line1;
+    double* prev = use_smem ? dp_sm : rowA;
+    double* cur = use_smem ? dp_sm + M : rowB;
+    for (int j = threadIdx.x; j < M; j += blockDim.x) {
+        const float c = dpc[(long long)i0 * M + j];
+        prev[j] = c >= 0.0f ? (double)c : BL_INF;
+    }
+    __syncthreads();
+    for (int i = i0 + 1; i <= i1; ++i) {
+        if (!(lf[i] & 1)) continue;  // the same flag for every thread
+        const float* crow = dpc + (long long)i * M;
+        uint8_t* drow = dir + (long long)i * M;
+        for (int j = threadIdx.x; j < M; j += blockDim.x) {
+            const float c = crow[j];
+            const double pl = j > 0 ? prev[j - 1] : BL_INF;
+            const double pm = prev[j];
+            const double pr = j < M - 1 ? prev[j + 1] : BL_INF;
+            int a = 0;
+            double best = pl;
+            if (pm < best) { best = pm; a = 1; }
+            if (pr < best) { best = pr; a = 2; }
+            cur[j] = c >= 0.0f ? (double)c + best : BL_INF;
+            drow[j] = (uint8_t)a;
+        }
+        __syncthreads();
+        double* t = prev;
+        prev = cur;
+        cur = t;
+    }
+    // first minimum of the last overlap line: per-thread, then across the block
+    __shared__ double s_best[32];
+    __shared__ int s_idx[32];
+    double bv = BL_INF * 4.0;
+    int bj = 0x7fffffff;
+    for (int j = threadIdx.x; j < M; j += blockDim.x) {
+        const double vv = dpc[(long long)i1 * M + j] >= 0.0f ? prev[j] : BL_INF;
+        if (vv < bv) { bv = vv; bj = j; }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+        const int oj = __shfl_xor_sync(0xffffffffu, bj, o);
+        if (ov < bv || (ov == bv && oj < bj)) { bv = ov; bj = oj; }
+    }
+    if ((threadIdx.x & 31) == 0) {
+        s_best[threadIdx.x >> 5] = bv;
+        s_idx[threadIdx.x >> 5] = bj;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
+            if (s_best[w] < bv || (s_best[w] == bv && s_idx[w] < bj)) { bv = s_best[w]; bj = s_idx[w]; }
+        int sc = bj;
+        for (int i = 0; i < L; ++i) seam[i] = sc;
+        int r = i1;
+        for (int i = i1 - 1; i >= i0; --i) {
+            if (!(lf[i] & 1)) continue;
+            int k = seam[r] + (int)dir[(long long)r * M + seam[r]] - 1;
+            k = k < 0 ? 0 : (k > M - 1 ? M - 1 : k);
+            seam[i] = k;
+            r = i;
+        }
+    }
+}
+
+// seam mask before the blur (pysift/core.py:3406-3467): 1 = image 1
+__global__ void k_blend_seam_mask(const uint8_t* __restrict__ m1, const uint8_t* __restrict__ m2,
+                                  const int* __restrict__ seam, const BlendCtl* ctl, float* __restrict__ mask, int cw) {
+    const int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
+    if (u >= cw) return;
+    const long long p = (long long)v * cw + u;
+    const bool a = m1[p] != 0, b = m2[p] != 0;
+    float val = (a && !b) ? 1.0f : 0.0f;
+    if (a && b) {
+        const bool first = ctl->vertical ? (u <= seam[v]) : (v <= seam[u]);
+        val = (ctl->first_side ? first : !first) ? 1.0f : 0.0f;
+    }
+    mask[p] = val;
+}
+
+// seam-mask blur (sigma 3, 25 taps, reflect-101): one axis, float64 sums in tap order
+__global__ void k_blend_seam_blur(const float* __restrict__ in, float* __restrict__ out, int W, int H, int axis,
+                                  const float* __restrict__ k25) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= W) return;
+    double s = 0.0;
+#pragma unroll 5
+    for (int t = 0; t < 25; ++t) {
+        const float v = axis == 1 ? in[(long long)y * W + refl_101(x + t - 12, W)]
+                                  : in[(long long)refl_101(y + t - 12, H) * W + x];
+        s = s + (double)k25[t] * (double)v;
+    }
+    out[(long long)y * W + x] = (float)s;
+}
+
+// the blurred values replace the mask where both images cover the canvas
+__global__ void k_blend_seam_select(const float* __restrict__ blurred, const uint8_t* __restrict__ m1,
+                                    const uint8_t* __restrict__ m2, float* __restrict__ mask, long long n) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    if (m1[p] && m2[p]) mask[p] = blurred[p];
+}
+
+// gaussian_filter(sigma = 1) of a C-channel level followed by [::2, ::2]
+// (pysift/core.py:3475-3483): the axis-0 pass at even rows ...
+__global__ void k_gauss_rows_even(const float* __restrict__ in, float* __restrict__ out, int W, int H, int C,
+                                  const double* __restrict__ w9) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, yo = blockIdx.y;
+    if (x >= W * C) return;
+    const int y = 2 * yo;
+    const long long rs = (long long)W * C;
+    double s = w9[4] * (double)in[y * rs + x];
+#pragma unroll
+    for (int k = 4; k >= 1; --k) {
+        const double a = (double)in[refl_half(y - k, H) * rs + x];
+        const double b = (double)in[refl_half(y + k, H) * rs + x];
+        s = s + (a + b) * w9[4 - k];
+    }
+    out[yo * rs + x] = (float)s;
+}
+
+// ... then the axis-1 pass at even columns
+__global__ void k_gauss_cols_even(const float* __restrict__ in, float* __restrict__ out, int W, int Wo, int C,
+                                  const double* __restrict__ w9) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= Wo * C) return;
+    const int colo = x / C, c = x - colo * C;
+    const int col = 2 * colo;
+    const float* row = in + (long long)y * W * C + c;
+    double s = w9[4] * (double)row[(long long)col * C];
+#pragma unroll
+    for (int k = 4; k >= 1; --k) {
+        const double a = (double)row[(long long)refl_half(col - k, W) * C];
+        const double b = (double)row[(long long)refl_half(col + k, W) * C];
+        s = s + (a + b) * w9[4 - k];
+    }
+    out[(long long)y * Wo * C + x] = (float)s;
+}
+
+// zoom(order = 1) of an (h, w) level to (H, W) (pysift/core.py:3485-3493):
+// coordinate k * (in - 1) / (out - 1), corners reflected (mirror) at the edge
+struct Zoom1 {
+    long long o[4];
+    double wy[2], wx[2];
+    __device__ Zoom1(int h, int w, int H, int W, int y, int x) {
+        const double zy = H > 1 ? (double)(h - 1) / (double)(H - 1) : 1.0;
+        const double zx = W > 1 ? (double)(w - 1) / (double)(W - 1) : 1.0;
+        const double cy = (double)y * zy, cx = (double)x * zx;
+        const int y0 = (int)floor(cy), x0 = (int)floor(cx);
+        const double ty = cy - (double)y0, tx = cx - (double)x0;
+        wy[0] = 1.0 - ty;
+        wy[1] = ty;
+        wx[0] = 1.0 - tx;
+        wx[1] = tx;
+        const int ya = refl_101(y0, h), yb = refl_101(y0 + 1, h);
+        const int xa = refl_101(x0, w), xb = refl_101(x0 + 1, w);
+        o[0] = (long long)ya * w + xa;
+        o[1] = (long long)ya * w + xb;
+        o[2] = (long long)yb * w + xa;
+        o[3] = (long long)yb * w + xb;
+    }
+    // sum over the corners in row-major order of ((v * wy) * wx)
+    __device__ float at(const float* __restrict__ in, int C, int c) const {
+        double t = 0.0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            double coeff = (double)in[o[k] * C + c];
+            coeff = coeff * wy[k >> 1];
+            coeff = coeff * wx[k & 1];
+            t = t + coeff;
+        }
+        return (float)t;
+    }
+};
+
+// one blended Laplacian level: m * (G1 - up(G1')) + (1 - m) * (G2 - up(G2'))
+// (pysift/core.py:3535-3541); the coarsest level blends the Gaussians
+__global__ void k_blend_level(const float* __restrict__ g1, const float* __restrict__ g2,
+                              const float* __restrict__ gm, const float* __restrict__ g1n,
+                              const float* __restrict__ g2n, int H, int W, int hn, int wn,
+                              float* __restrict__ out) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= W) return;
+    const long long p = (long long)y * W + x;
+    const float m = gm[p];
+    const float mc = 1.0f - m;
+    if (g1n) {
+        const Zoom1 z(hn, wn, H, W, y, x);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const float l1 = g1[p * 3 + c] - z.at(g1n, 3, c);
+            const float l2 = g2[p * 3 + c] - z.at(g2n, 3, c);
+            out[p * 3 + c] = m * l1 + mc * l2;
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) out[p * 3 + c] = m * g1[p * 3 + c] + mc * g2[p * 3 + c];
+    }
+}
+
+// reconstruction step (pysift/core.py:3544-3547): out = up(res) + lb
+__global__ void k_blend_reconstruct(const float* __restrict__ res, int hn, int wn, const float* __restrict__ lb,
+                                    int H, int W, float* __restrict__ out) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= W) return;
+    const long long p = (long long)y * W + x;
+    const Zoom1 z(hn, wn, H, W, y, x);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) out[p * 3 + c] = z.at(res, 3, c) + lb[p * 3 + c];
+}
+
+// the finest reconstruction step fused with the paste (pysift/core.py:3808-3809):
+// uint8 truncation of the clipped value where either image covers the canvas
+__global__ void k_blend_final(const float* __restrict__ res, int hn, int wn, const float* __restrict__ lb,
+                              const uint8_t* __restrict__ m1, const uint8_t* __restrict__ m2, int H, int W,
+                              uint8_t* __restrict__ pano, uint8_t* __restrict__ both, const BlendCtl* ctl,
+                              double* __restrict__ seam_rmse) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x == 0 && y == 0 && seam_rmse)
+        *seam_rmse = ctl->n_ov ? sqrt((double)ctl->sq / (3.0 * (double)ctl->n_ov)) : __longlong_as_double(0x7ff8000000000000ll);
+    if (x >= W) return;
+    const long long p = (long long)y * W + x;
+    const bool any = m1[p] || m2[p];
+    if (both) both[p] = any;
+    const Zoom1* zp = nullptr;
+    Zoom1 z(hn > 0 ? hn : 1, wn > 0 ? wn : 1, H, W, y, x);
+    if (res) zp = &z;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        float v = zp ? zp->at(res, 3, c) + lb[p * 3 + c] : lb[p * 3 + c];
+        v = v < 0.0f ? 0.0f : (v > 255.0f ? 255.0f : v);
+        pano[p * 3 + c] = any ? (uint8_t)(int)v : (uint8_t)0;
+    }
+}
+
+// image 2 pasted on the canvas at (iox, ioy) (pysift/core.py:3794-3800)
+__global__ void k_place_image(const uint8_t* __restrict__ img, int h, int w, int pitch, int cw, int iox, int ioy,
+                              uint8_t* __restrict__ canvas, uint8_t* __restrict__ mask) {
+    const int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
+    if (u >= cw) return;
+    const int x = u - iox, y = v - ioy;
+    const bool in = x >= 0 && x < w && y >= 0 && y < h;
+    const long long p = (long long)v * cw + u;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) canvas[p * 3 + c] = in ? img[(long long)y * pitch + 3 * x + c] : (uint8_t)0;
+    if (mask) mask[p] = in;
+}
+
+constexpr int DP_SMEM_MAX = 200 * 1024;
+
+struct BlendLayout {
+    size_t off_ctl, off_rowf, off_colf, off_color, off_avg, off_d1, off_d2, off_dpc, off_rowA, off_rowB, off_dir,
+        off_seam, off_blur, off_w9, off_k25, off_tmp;
+    size_t off_g1[8], off_g2[8], off_gm[8], off_lb[8], off_res[2];
+    int h[8], w[8];
+    size_t total;
+};
+
+static BlendLayout blend_layout(int cw, int ch, int levels) {
+    BlendLayout l;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t r = off;
+        off = align_up(off + bytes, 256);
+        return r;
+    };
+    const size_t N = (size_t)cw * ch;
+    const int M = cw > ch ? cw : ch;
+    l.off_ctl = take(sizeof(BlendCtl));
+    l.off_rowf = take((size_t)ch * 4);
+    l.off_colf = take((size_t)cw * 4);
+    l.off_color = take(N * 4);
+    l.off_avg = take(N * 4);
+    l.off_d1 = take(N * 4);
+    l.off_d2 = take(N * 4);
+    l.off_dpc = take(N * 4);
+    l.off_rowA = take((size_t)M * 8);
+    l.off_rowB = take((size_t)M * 8);
+    l.off_dir = take(N);
+    l.off_seam = take((size_t)M * 4);
+    l.off_blur = take(N * 4);
+    l.off_w9 = take(9 * 8);
+    l.off_k25 = take(25 * 4);
+    int h = ch, w = cw;
+    size_t tmp = 0;
+    for (int k = 0; k < levels; ++k) {
+        l.h[k] = h;
+        l.w[k] = w;
+        l.off_g1[k] = take((size_t)h * w * 12);
+        l.off_g2[k] = take((size_t)h * w * 12);
+        l.off_gm[k] = take((size_t)h * w * 4);
+        l.off_lb[k] = take((size_t)h * w * 12);
+        tmp = std::max(tmp, (size_t)((h + 1) / 2) * w * 12);
+        h = (h + 1) / 2;
+        w = (w + 1) / 2;
+    }
+    l.off_tmp = take(tmp);
+    l.off_res[0] = take(N * 12);
+    l.off_res[1] = take(N * 12);
+    l.total = off;
+    return l;
+}
+
+template <typename T>
+static T* bwp(void* ws, size_t off) {
+    return reinterpret_cast<T*>(static_cast<char*>(ws) + off);
+}
+
+static void blend_down(const float* in, int h, int w, int C, float* tmp, float* out, const double* w9,
+                       cudaStream_t st) {
+    const int ho = (h + 1) / 2, wo = (w + 1) / 2;
+    k_gauss_rows_even<<<dim3(ceil_div(w * C, 256), ho), 256, 0, st>>>(in, tmp, w, h, C, w9);
+    k_gauss_cols_even<<<dim3(ceil_div(wo * C, 256), ho), 256, 0, st>>>(tmp, out, w, wo, C, w9);
+}
+
+}  // namespace pysift
+
+using namespace pysift;
+
+extern "C" {
+
+int pysift_place_image(const uint8_t* img, int32_t h, int32_t w, int32_t pitch, int32_t cw, int32_t ch, int32_t iox,
+                       int32_t ioy, uint8_t* canvas, uint8_t* mask, pysift_stream_t stream) {
+    PYSIFT_CHECK_ARG(img && canvas, "NULL pointer argument");
+    PYSIFT_CHECK_ARG(h > 0 && w > 0 && pitch >= 3 * w && cw > 0 && ch > 0, "bad sizes");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    k_place_image<<<dim3(ceil_div(cw, 256), ch), 256, 0, st>>>(img, h, w, pitch, cw, iox, ioy, canvas, mask);
+    PYSIFT_LAUNCH_CHECK("k_place_image");
+    return PYSIFT_OK;
+}
+
+int pysift_blend_workspace_size(int32_t cw, int32_t ch, int32_t n_levels, size_t* bytes) {
+    PYSIFT_CHECK_ARG(bytes && cw > 1 && ch > 1 && n_levels >= 1 && n_levels <= 8, "bad arguments");
+    *bytes = blend_layout(cw, ch, n_levels).total;
+    return PYSIFT_OK;
+}
+
+int pysift_blend_multiband(const uint8_t* warped1, const uint8_t* mask1, const uint8_t* canvas2,
+                           const uint8_t* mask2, int32_t cw, int32_t ch, int32_t n_levels, const float* seam_k25,
+                           const double* gauss_w9, void* workspace, size_t workspace_bytes, uint8_t* pano,
+                           uint8_t* both, double* seam_rmse, pysift_stream_t stream) {
+    PYSIFT_CHECK_ARG(warped1 && mask1 && canvas2 && mask2 && seam_k25 && gauss_w9 && workspace && pano,
+                     "NULL pointer argument");
+    PYSIFT_CHECK_ARG(cw > 1 && ch > 1 && n_levels >= 1 && n_levels <= 8, "bad sizes");
+    const BlendLayout l = blend_layout(cw, ch, n_levels);
+    if (workspace_bytes < l.total) {
+        set_error("workspace %zu bytes < required %zu", workspace_bytes, l.total);
+        return PYSIFT_ERR_WORKSPACE;
+    }
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    void* ws = workspace;
+    BlendCtl* ctl = bwp<BlendCtl>(ws, l.off_ctl);
+    int* rowf = bwp<int>(ws, l.off_rowf);
+    int* colf = bwp<int>(ws, l.off_colf);
+    PYSIFT_CUDA_TRY(cudaMemsetAsync(ctl, 0, sizeof(BlendCtl), st));
+    PYSIFT_CUDA_TRY(cudaMemsetAsync(rowf, 0, (size_t)ch * 4, st));
+    PYSIFT_CUDA_TRY(cudaMemsetAsync(colf, 0, (size_t)cw * 4, st));
+    double* w9 = bwp<double>(ws, l.off_w9);
+    float* k25 = bwp<float>(ws, l.off_k25);
+    PYSIFT_CUDA_TRY(cudaMemcpyAsync(w9, gauss_w9, 9 * sizeof(double), cudaMemcpyHostToDevice, st));
+    PYSIFT_CUDA_TRY(cudaMemcpyAsync(k25, seam_k25, 25 * sizeof(float), cudaMemcpyHostToDevice, st));
+    const dim3 g2d(ceil_div(cw, 256), ch);
+    const long long N = (long long)cw * ch;
+    k_blend_stats<<<dim3(1, ch), 256, 0, st>>>(warped1, mask1, canvas2, mask2, cw, ctl, rowf, colf);
+    PYSIFT_LAUNCH_CHECK("k_blend_stats");
+    k_blend_decide<<<1, 1024, 0, st>>>(ctl, rowf, colf, cw, ch);
+    PYSIFT_LAUNCH_CHECK("k_blend_decide");
+    float* I1 = bwp<float>(ws, l.off_g1[0]);
+    float* I2 = bwp<float>(ws, l.off_g2[0]);
+    float* color = bwp<float>(ws, l.off_color);
+    float* avg = bwp<float>(ws, l.off_avg);
+    k_blend_prepare<<<g2d, 256, 0, st>>>(warped1, mask1, canvas2, mask2, cw, ctl, I1, I2, color, avg);
+    PYSIFT_LAUNCH_CHECK("k_blend_prepare");
+    float* d1 = bwp<float>(ws, l.off_d1);
+    float* d2 = bwp<float>(ws, l.off_d2);
+    float* dpc = bwp<float>(ws, l.off_dpc);
+    k_sobel_deriv<<<g2d, 256, 0, st>>>(avg, d1, d2, cw, ch);
+    PYSIFT_LAUNCH_CHECK("k_sobel_deriv");
+    k_sobel_cost<<<g2d, 256, 0, st>>>(d1, d2, color, mask1, mask2, ctl, dpc, cw, ch);
+    PYSIFT_LAUNCH_CHECK("k_sobel_cost");
+    int* seam = bwp<int>(ws, l.off_seam);
+    const int M = cw > ch ? cw : ch;
+    const size_t dp_smem = (size_t)M * 16;
+    const int use_smem = dp_smem <= (size_t)DP_SMEM_MAX;
+    if (use_smem) PYSIFT_CUDA_TRY(cudaFuncSetAttribute(k_blend_dp, cudaFuncAttributeMaxDynamicSharedMemorySize, DP_SMEM_MAX));
+    k_blend_dp<<<1, 1024, use_smem ? dp_smem : 0, st>>>(dpc, rowf, colf, cw, ch, ctl, bwp<double>(ws, l.off_rowA),
+                                                        bwp<double>(ws, l.off_rowB), use_smem,
+                                                        bwp<uint8_t>(ws, l.off_dir), seam);
+    PYSIFT_LAUNCH_CHECK("k_blend_dp");
+    float* gm0 = bwp<float>(ws, l.off_gm[0]);
+    float* blur = bwp<float>(ws, l.off_blur);
+    k_blend_seam_mask<<<g2d, 256, 0, st>>>(mask1, mask2, seam, ctl, gm0, cw);
+    PYSIFT_LAUNCH_CHECK("k_blend_seam_mask");
+    k_blend_seam_blur<<<g2d, 256, 0, st>>>(gm0, d1, cw, ch, 1, k25);
+    k_blend_seam_blur<<<g2d, 256, 0, st>>>(d1, blur, cw, ch, 0, k25);
+    PYSIFT_LAUNCH_CHECK("k_blend_seam_blur");
+    k_blend_seam_select<<<(unsigned)ceil_div_ll(N, 256), 256, 0, st>>>(blur, mask1, mask2, gm0, N);
+    PYSIFT_LAUNCH_CHECK("k_blend_seam_select");
+    float* tmp = bwp<float>(ws, l.off_tmp);
+    for (int k = 0; k + 1 < n_levels; ++k) {
+        blend_down(bwp<float>(ws, l.off_g1[k]), l.h[k], l.w[k], 3, tmp, bwp<float>(ws, l.off_g1[k + 1]), w9, st);
+        blend_down(bwp<float>(ws, l.off_g2[k]), l.h[k], l.w[k], 3, tmp, bwp<float>(ws, l.off_g2[k + 1]), w9, st);
+        blend_down(bwp<float>(ws, l.off_gm[k]), l.h[k], l.w[k], 1, tmp, bwp<float>(ws, l.off_gm[k + 1]), w9, st);
+    }
+    PYSIFT_LAUNCH_CHECK("k_gauss_down");
+    for (int k = 0; k < n_levels; ++k) {
+        const bool top = k + 1 == n_levels;
+        k_blend_level<<<dim3(ceil_div(l.w[k], 256), l.h[k]), 256, 0, st>>>(
+            bwp<float>(ws, l.off_g1[k]), bwp<float>(ws, l.off_g2[k]), bwp<float>(ws, l.off_gm[k]),
+            top ? nullptr : bwp<float>(ws, l.off_g1[k + 1]), top ? nullptr : bwp<float>(ws, l.off_g2[k + 1]), l.h[k],
+            l.w[k], top ? 0 : l.h[k + 1], top ? 0 : l.w[k + 1], bwp<float>(ws, l.off_lb[k]));
+    }
+    PYSIFT_LAUNCH_CHECK("k_blend_level");
+    const float* res = n_levels > 1 ? bwp<float>(ws, l.off_lb[n_levels - 1]) : nullptr;
+    int rh = l.h[n_levels - 1], rw = l.w[n_levels - 1];
+    for (int k = n_levels - 2; k >= 1; --k) {
+        float* out = bwp<float>(ws, l.off_res[k & 1]);
+        k_blend_reconstruct<<<dim3(ceil_div(l.w[k], 256), l.h[k]), 256, 0, st>>>(res, rh, rw, bwp<float>(ws, l.off_lb[k]),
+                                                                                l.h[k], l.w[k], out);
+        res = out;
+        rh = l.h[k];
+        rw = l.w[k];
+    }
+    PYSIFT_LAUNCH_CHECK("k_blend_reconstruct");
+    k_blend_final<<<g2d, 256, 0, st>>>(res, n_levels > 1 ? rh : 0, n_levels > 1 ? rw : 0, bwp<float>(ws, l.off_lb[0]),
+                                       mask1, mask2, ch, cw, pano, both, ctl, seam_rmse);
+    PYSIFT_LAUNCH_CHECK("k_blend_final");
+    return PYSIFT_OK;
+}
+
+}  // extern "C"

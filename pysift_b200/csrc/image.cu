@@ -189,6 +189,15 @@ __global__ void __launch_bounds__(256) k_warp_feather(const WarpArgs a) {
     }
     if (a.mask1) a.mask1[(long long)v * a.cw + u] = valid1;
     if (a.mask2) a.mask2[(long long)v * a.cw + u] = valid2;
+    if (valid1 || valid2) {
+        if (a.row_lo) {
+            atomicMin(&a.row_lo[v], u);
+            atomicMax(&a.row_hi[v], u);
+            atomicMin(&a.col_lo[u], v);
+            atomicMax(&a.col_hi[u], v);
+        }
+    }
+    if (!a.out) return;
     uint8_t res[3] = {0, 0, 0};
     if (valid1 && valid2 && a.feather) {
         // linear feather: weights = 1 + distance to the nearest border of each image
@@ -214,14 +223,6 @@ __global__ void __launch_bounds__(256) k_warp_feather(const WarpArgs a) {
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) a.out[o + c] = res[c];
-    if (valid1 || valid2) {
-        if (a.row_lo) {
-            atomicMin(&a.row_lo[v], u);
-            atomicMax(&a.row_hi[v], u);
-            atomicMin(&a.col_lo[u], v);
-            atomicMax(&a.col_hi[u], v);
-        }
-    }
 }
 
 __global__ void k_fill_int(int* p, int n, int value) {
@@ -329,7 +330,8 @@ int pysift_warp_feather(const uint8_t* img1, int32_t hs, int32_t ws, int32_t pit
                         int32_t iox, int32_t ioy, int32_t feather, uint8_t* out, uint8_t* warped, uint8_t* mask1,
                         uint8_t* mask2, int32_t* row_lo, int32_t* row_hi, int32_t* col_lo, int32_t* col_hi,
                         pysift_stream_t stream) {
-    PYSIFT_CHECK_ARG(img1 && img2 && hinv9 && out, "NULL pointer argument");
+    PYSIFT_CHECK_ARG(img1 && img2 && hinv9, "NULL pointer argument");
+    PYSIFT_CHECK_ARG(out || (warped && mask1 && mask2), "no output requested");
     PYSIFT_CHECK_ARG(hs > 1 && ws > 1 && h2 > 0 && w2 > 0 && cw > 0 && ch > 0, "bad sizes");
     PYSIFT_CHECK_ARG((row_lo && row_hi && col_lo && col_hi) || !(row_lo || row_hi || col_lo || col_hi),
                      "extents must be all or none");

@@ -3,9 +3,11 @@
 The two-image path of the reference -- BGR->gray, CLAHE, SIFT, top-k by
 response, L2 + PCA-64 + fp16 mutual ratio-test matching, batched RANSAC with
 MAGSAC++ scoring and LO refits, canvas, bilinear warp -- runs as C-ABI calls
-on the current CUDA stream.  Composition: the reference's gain + DP seam +
-multiband blend is replaced by a linear feather blend (weights 1 + distance
-to each image's border) followed by the reference's inner-rectangle crop.
+on the current CUDA stream.  Composition (blend='multiband', the default) is
+the reference's: gain compensation, dynamic-programming seam and a 6-level
+Laplacian blend (pysift/core.py:3386-3553, 3686-3714) on the device;
+blend='feather' swaps in a linear feather blend (weights 1 + distance to
+each image's border).  Both end with the reference's inner-rectangle crop.
 The host reads back only the homography (72 bytes + 3 counters) to size the
 canvas, the coverage extents for the crop and the final panorama.
 """
@@ -54,17 +56,25 @@ class GPUPyStitch:
                  color_match='gain', dsp_sift=False, contrast_thresh=0.04, n_octaves=4, n_scales=3, sigma0=1.6,
                  edge_thresh=10.0, double_image=True, max_dimension=0, denoise=False, sharpen=False,
                  clahe_clip=2.0, clahe_tile=8, output_max_dim=0, post_sharpen=False, output_format='png',
-                 output_quality=90, *, device=None, save_output=True, verbose=True, high_vram=None):
+                 output_quality=90, *, device=None, save_output=True, verbose=True, high_vram=None,
+                 blend='multiband'):
         if matcher != 'ratio':
             raise NotImplementedError(f"matcher={matcher!r}: only the ratio-test matcher is implemented here")
         if int8_matching:
             raise NotImplementedError("int8_matching: not implemented on this backend (fp16 tensor-core matching)")
         if pca_dims not in (0, 64, 128):
             raise NotImplementedError("pca_dims must be 0, 64 or 128 on this backend")
+        if blend not in ('multiband', 'feather'):
+            raise ValueError(f"blend must be 'multiband' or 'feather' (got {blend!r})")
+        if blend == 'multiband' and color_match != 'gain':
+            raise NotImplementedError(f"color_match={color_match!r}: only gain compensation is implemented")
+        if blend == 'multiband' and not 1 <= int(n_blend_levels) <= 8:
+            raise ValueError("n_blend_levels must be within 1..8")
         if ransac_method not in ('magsac', 'classic'):
             raise ValueError(f"ransac_method must be 'magsac' or 'classic' (got {ransac_method!r})")
         self.n_depth_layers = n_depth_layers
         self.n_blend_levels = n_blend_levels
+        self.blend = blend
         self.ransac_iters = ransac_iters
         self.inlier_thresh = inlier_thresh
         self.ransac_method = ransac_method
@@ -257,9 +267,10 @@ class GPUPyStitch:
         return int(np.ceil(ax.max() + ox)) + 1, int(np.ceil(ay.max() + oy)) + 1, ox, oy
 
     def _compose_enqueue(self, img1, img2, H, key="", max_canvas_px=400_000_000):
-        """Canvas geometry on the host, then warp + feather blend and the
-        coverage extents on the current stream; the extents are copied to
-        pinned host memory (read them after the stream has finished)."""
+        """Canvas geometry on the host, then warp, composition and the
+        coverage extents on the current stream; the extents (and the seam
+        RMSE) are copied to pinned host memory (read them after the stream
+        has finished)."""
         hs, ws = img1.shape[:2]
         h2, w2 = img2.shape[:2]
         cw, ch, ox, oy = self._compute_canvas_size(img1.shape, img2.shape, H)
@@ -268,18 +279,42 @@ class GPUPyStitch:
         hinv = np.linalg.inv(H).astype(np.float32).ravel()
         iox, ioy = int(round(ox)), int(round(oy))
         st = self._stream()
-        out = self._dev.get(key + "pano", (ch, cw, 3), torch.uint8, self.device)
-        ext = self._dev.get(key + "extents", (2 * ch + 2 * cw,), torch.int32, self.device)
+        dev = self.device
+        out = self._dev.get(key + "pano", (ch, cw, 3), torch.uint8, dev)
+        ext = self._dev.get(key + "extents", (2 * ch + 2 * cw,), torch.int32, dev)
         hb = (ctypes.c_float * 9)(*[float(v) for v in hinv])
+        multiband = self.blend == 'multiband' and cw > 1 and ch > 1
+        if multiband:
+            warped = self._dev.get(key + "warped1", (ch, cw, 3), torch.uint8, dev)
+            m1 = self._dev.get(key + "mask1", (ch, cw), torch.uint8, dev)
+            m2 = self._dev.get(key + "mask2", (ch, cw), torch.uint8, dev)
+            outs = (None, warped.data_ptr(), m1.data_ptr(), m2.data_ptr())
+        else:
+            outs = (out.data_ptr(), None, None, None)
         _lib.check(self._lib.pysift_warp_feather(img1.data_ptr(), hs, ws, img1.stride(0), img2.data_ptr(), h2, w2,
                                                  img2.stride(0), cw, ch, ctypes.cast(hb, ctypes.c_void_p),
-                                                 float(np.float32(ox)), float(np.float32(oy)), iox, ioy, 1,
-                                                 out.data_ptr(), None, None, None, ext.data_ptr(),
-                                                 ext[ch:].data_ptr(), ext[2 * ch:].data_ptr(),
+                                                 float(np.float32(ox)), float(np.float32(oy)), iox, ioy, 1, *outs,
+                                                 ext.data_ptr(), ext[ch:].data_ptr(), ext[2 * ch:].data_ptr(),
                                                  ext[2 * ch + cw:].data_ptr(), st), "pysift_warp_feather")
+        res = dict(out=out, canvas_w=cw, canvas_h=ch, ox=ox, oy=oy, seam_rmse_host=None)
+        if multiband:
+            from . import blend as _blend
+            canvas2 = self._dev.get(key + "canvas2", (ch, cw, 3), torch.uint8, dev)
+            _lib.check(self._lib.pysift_place_image(img2.data_ptr(), h2, w2, img2.stride(0), cw, ch, iox, ioy,
+                                                    canvas2.data_ptr(), None, st), "pysift_place_image")
+            need = _blend.workspace_bytes(cw, ch, self.n_blend_levels) + 256
+            wsb = self._dev.get(key + "blend_ws", (need,), torch.uint8, dev)
+            both = self._dev.get(key + "both", (ch, cw), torch.uint8, dev)
+            rmse = self._dev.get(key + "seam_rmse", (1,), torch.float64, dev)
+            _blend.blend_multiband(warped, m1, canvas2, m2, self.n_blend_levels, workspace=wsb, pano=out,
+                                   both=both, seam_rmse=rmse, stream=st)
+            rmse_host = torch.empty(1, dtype=torch.float64, pin_memory=True)
+            rmse_host.copy_(rmse, non_blocking=True)
+            res.update(seam_rmse_host=rmse_host, warped1=warped, mask1=m1, mask2=m2, canvas2=canvas2)
         ext_host = torch.empty(ext.shape, dtype=torch.int32, pin_memory=True)
         ext_host.copy_(ext, non_blocking=True)
-        return dict(out=out, ext_host=ext_host, canvas_w=cw, canvas_h=ch, ox=ox, oy=oy)
+        res["ext_host"] = ext_host
+        return res
 
     def _compose_crop(self, c):
         """The inner-rectangle crop of a composed canvas (its extents on the host)."""
@@ -298,7 +333,14 @@ class GPUPyStitch:
         c = self._compose_enqueue(img1, img2, H, max_canvas_px=max_canvas_px)
         torch.cuda.current_stream(self.device).synchronize()
         pano = self._to_host(self._compose_crop(c))
-        return pano, dict(canvas_w=c["canvas_w"], canvas_h=c["canvas_h"], ox=c["ox"], oy=c["oy"])
+        self._last_compose = c
+        return pano, dict(canvas_w=c["canvas_w"], canvas_h=c["canvas_h"], ox=c["ox"], oy=c["oy"],
+                          seam_rmse=self._seam_rmse_of(c))
+
+    @staticmethod
+    def _seam_rmse_of(c):
+        r = c.get("seam_rmse_host")
+        return float(r[0]) if r is not None else float('nan')
 
     def _to_host(self, t):
         """Device tensor -> numpy array in page-locked memory from torch's
@@ -392,7 +434,7 @@ class GPUPyStitch:
             pano, cm = self._compose(g1, g2, H)
             self._mark(5)
             timings['st5'] = time.perf_counter() - t0
-            metrics.update(canvas_w=cm['canvas_w'], canvas_h=cm['canvas_h'], seam_rmse=float('nan'))
+            metrics.update(canvas_w=cm['canvas_w'], canvas_h=cm['canvas_h'], seam_rmse=cm['seam_rmse'])
         self._last = dict(H=H, mask=mask_d, pairs=m["pairs"][:n_m], kp1=kp1, kp2=kp2, p1=p1, p2=p2, info=info)
         return pano, timings, metrics
 
@@ -408,7 +450,7 @@ class GPUPyStitch:
         input order.  Each phase runs for all pairs at once, spread over
         `n_streams` CUDA streams, with one host synchronisation per phase:
         (1) CLAHE and detection of every view, (2) matcher preparation and
-        matching, (3) RANSAC, (4) warp + feather blend, crop and readback.
+        matching, (3) RANSAC, (4) warp + composition, crop and readback.
         Every pair gets exactly the result stitch(img1, img2) gives on this
         instance; the PCA basis is fitted on the first pair if it is not yet
         fitted.  No file is written.  The per-pair metrics are kept in
@@ -499,6 +541,8 @@ class GPUPyStitch:
             for s in streams:
                 main.wait_stream(s)
             main.synchronize()
+            for p, c in enumerate(comps):
+                metrics[p]["seam_rmse"] = self._seam_rmse_of(c)
             hosts = []
             for c in comps:
                 crop = self._compose_crop(c).contiguous()

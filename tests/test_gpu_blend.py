@@ -1,0 +1,159 @@
+"""GPU parity of the reference composition (gain, DP seam, multiband blend,
+paste): bit-exact against the reference's own output on the golden canvases
+and against the oracle (oracle/blend_oracle.py) on larger seeded canvases,
+and inside GPUPyStitch."""
+import os
+
+import numpy as np
+import pytest
+
+from pysift_b200 import synthetic
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "blend_cases.npz")
+
+
+def _run(w1, m1, c2, m2, n_levels=6):
+    import torch
+    from pysift_b200 import blend
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    pano, both, rmse = blend.blend_multiband(t(w1), t(m1.astype(np.uint8)), t(c2), t(m2.astype(np.uint8)), n_levels)
+    torch.cuda.synchronize()
+    return pano.cpu().numpy(), both.cpu().numpy().astype(bool), float(rmse.cpu()[0])
+
+
+def _rmse(w1, m1, c2, m2):
+    """_seam_rmse of the gained image 1 (pysift/core.py:3555-3562), exact."""
+    from oracle import blend_oracle as bo
+    ov = m1 & m2
+    if not ov.any():
+        return float("nan")
+    g = bo.gain_compensate(w1.astype(np.float32), c2.astype(np.float32), ov)
+    d = g.astype(np.uint8)[ov].astype(np.int64) - c2[ov].astype(np.int64)
+    return float(np.sqrt((d * d).sum() / d.size))
+
+
+def _case(seed, ch, cw, stacked=False, flip=False):
+    """Seeded canvas: a projective quad for image 1, a rectangle for image 2,
+    textured images with a colour gain between them and stray values of the
+    warp outside image 1's mask."""
+    rng = np.random.default_rng(seed)
+    # masks are drawn side by side; a stacked canvas draws them transposed
+    yy, xx = np.mgrid[0:cw, 0:ch] if stacked else np.mgrid[0:ch, 0:cw]
+    yy, xx = yy.astype(np.float64), xx.astype(np.float64)
+    L = xx.shape[1]
+    k = rng.uniform(-0.15, 0.15)
+    m1 = (xx < 0.62 * L + k * (yy - yy.mean())) & (yy > 0.03 * yy.max() + 0.02 * xx)
+    m2 = (xx >= 0.38 * L) & (yy >= 2) & (yy < yy.max() - 1)
+    if stacked:
+        m1, m2 = m1.T.copy(), m2.T.copy()
+    if flip:
+        m1, m2 = m1[:, ::-1].copy(), m2[:, ::-1].copy()
+    base = synthetic.dense_texture(ch, cw, seed=seed).astype(np.float64)
+    g1 = rng.uniform(0.6, 1.3, 3)
+    w1 = np.clip(base[:, :, None] * g1 + rng.normal(0, 3, (ch, cw, 3)), 0, 255).astype(np.uint8)
+    c2 = np.clip(base[:, :, None] * rng.uniform(0.8, 1.2, 3) + rng.normal(0, 3, (ch, cw, 3)), 0, 255).astype(np.uint8)
+    stray = (~m1) & (rng.random((ch, cw)) < 0.03)
+    w1[~m1] = 0
+    w1[stray] = 41
+    c2[~m2] = 0
+    return w1, m1, c2, m2
+
+
+def test_blend_reference_golden_bit_exact():
+    g = np.load(GOLDEN)
+    for name in g["names"]:
+        w1, m1, c2, m2 = (g[f"{name}_{k}"] for k in ("warped1", "mask1", "canvas2", "mask2"))
+        pano, both, rmse = _run(w1, m1, c2, m2)
+        assert np.array_equal(both, g[f"{name}_both"]), name
+        assert np.array_equal(pano, g[f"{name}_pano"]), name
+        ref = float(g[f"{name}_seam_rmse"])
+        if np.isnan(ref):
+            assert np.isnan(rmse)
+        else:
+            assert abs(rmse - ref) <= 1e-5 * ref, (name, rmse, ref)
+
+
+@pytest.mark.parametrize("seed,ch,cw,stacked,flip", [
+    (1, 300, 520, False, False),
+    (2, 300, 520, False, True),
+    (3, 520, 300, True, False),
+    (4, 257, 611, False, False),
+    (5, 611, 257, True, True),
+    (6, 720, 1300, False, False),
+])
+def test_blend_matches_oracle(seed, ch, cw, stacked, flip):
+    from oracle import blend_oracle as bo
+    w1, m1, c2, m2 = _case(seed, ch, cw, stacked, flip)
+    pano, both, rmse = _run(w1, m1, c2, m2)
+    ref, ref_both = bo.blend_pair(w1, m1, c2, m2)
+    assert np.array_equal(both, ref_both)
+    assert np.array_equal(pano, ref), np.argwhere(pano != ref)[:5]
+    assert abs(rmse - _rmse(w1, m1, c2, m2)) <= 1e-12 * max(1.0, rmse)
+
+
+@pytest.mark.parametrize("n_levels", [1, 2, 3, 5])
+def test_blend_levels(n_levels):
+    from oracle import blend_oracle as bo
+    w1, m1, c2, m2 = _case(11, 190, 333)
+    pano, _, _ = _run(w1, m1, c2, m2, n_levels)
+    ref, _ = bo.blend_pair(w1, m1, c2, m2, n_levels=n_levels)
+    assert np.array_equal(pano, ref)
+
+
+def test_blend_no_overlap_and_edges():
+    """No overlap (no gain, no seam), an overlap of one column and one of one row."""
+    from oracle import blend_oracle as bo
+    ch, cw = 64, 97
+    rng = np.random.default_rng(3)
+    w1 = rng.integers(0, 256, (ch, cw, 3), dtype=np.uint8)
+    c2 = rng.integers(0, 256, (ch, cw, 3), dtype=np.uint8)
+    yy, xx = np.mgrid[0:ch, 0:cw]
+    for m1, m2 in [(xx < 40, xx >= 50), (xx <= 48, xx >= 48), (yy <= 30, yy >= 30), (xx >= 0, xx >= 0)]:
+        a, b = w1.copy(), c2.copy()
+        a[~m1] = 0
+        b[~m2] = 0
+        pano, both, _ = _run(a, m1, b, m2)
+        ref, ref_both = bo.blend_pair(a, m1, b, m2)
+        assert np.array_equal(pano, ref) and np.array_equal(both, ref_both)
+
+
+def test_stitch_multiband_compose_bit_exact():
+    """GPUPyStitch's default composition equals the oracle on the warp the
+    stitcher made, and image 2's canvas is the reference's paste."""
+    from oracle import blend_oracle as bo
+    from pysift_b200.stitch import GPUPyStitch
+    img1, img2, _ = synthetic.stitch_pair(480, 640, seed=1)
+    st = GPUPyStitch(ransac_iters=2048, inlier_thresh=4.0, save_output=False, verbose=False)
+    pano = st.stitch(img1, img2)
+    c = st._last_compose
+    ch, cw = c["canvas_h"], c["canvas_w"]
+    w1 = c["warped1"].cpu().numpy()
+    m1 = c["mask1"].cpu().numpy().astype(bool)
+    m2 = c["mask2"].cpu().numpy().astype(bool)
+    c2 = c["canvas2"].cpu().numpy()
+    iox, ioy = int(round(c["ox"])), int(round(c["oy"]))
+    ref_c2 = np.zeros((ch, cw, 3), np.uint8)
+    ye, xe = min(ioy + img2.shape[0], ch), min(iox + img2.shape[1], cw)
+    ref_c2[ioy:ye, iox:xe] = img2[:ye - ioy, :xe - iox]
+    assert np.array_equal(c2, ref_c2)
+    ref, _ = bo.blend_pair(w1, m1, c2, m2)
+    assert np.array_equal(c["out"].cpu().numpy(), ref)
+    assert pano.ndim == 3 and pano.shape[2] == 3
+    assert np.isfinite(st.last_metrics["seam_rmse"])
+    assert abs(st.last_metrics["seam_rmse"] - _rmse(w1, m1, c2, m2)) < 1e-9
+
+
+def test_stitch_multiband_end_to_end():
+    from oracle import stitch_oracle as so
+    from pysift_b200.stitch import GPUPyStitch
+    img1, img2, _ = synthetic.stitch_pair(480, 640, seed=2)
+    st = GPUPyStitch(ransac_iters=2048, inlier_thresh=4.0, save_output=False, verbose=False)
+    pano = st.stitch(img1, img2)
+    orc = so.OracleStitch(ransac_iters=2048, inlier_thresh=4.0).stitch(img1, img2)
+    Hg = st._last["H"]
+    assert np.max(np.abs(Hg - orc["H"]) / np.maximum(np.abs(orc["H"]), 1e-6)) < 1e-3
+    if pano.shape == orc["pano"].shape:
+        diff = np.abs(pano.astype(int) - orc["pano"].astype(int))
+        assert np.mean(diff <= 1) > 0.98

@@ -213,9 +213,9 @@ def test_stitch_pair_end_to_end():
     from oracle import stitch_oracle as so
     from pysift_b200.stitch import GPUPyStitch
     img1, img2, Ht = synthetic.stitch_pair(480, 640, seed=1)
-    st = GPUPyStitch(ransac_iters=2048, inlier_thresh=4.0, save_output=False, verbose=False)
+    st = GPUPyStitch(ransac_iters=2048, inlier_thresh=4.0, save_output=False, verbose=False, blend="feather")
     pano = st.stitch(img1, img2)
-    orc = so.OracleStitch(ransac_iters=2048, inlier_thresh=4.0).stitch(img1, img2)
+    orc = so.OracleStitch(ransac_iters=2048, inlier_thresh=4.0, blend="feather").stitch(img1, img2)
     m = st.last_metrics
     assert m["kp1"] == orc["n1"] and m["kp2"] == orc["n2"]
     assert abs(m["matches"] - len(orc["pairs"])) <= max(2, 0.01 * len(orc["pairs"]))

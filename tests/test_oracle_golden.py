@@ -101,3 +101,33 @@ def test_pin_reference_dumps(name, oracle_lib):
     fx = np.load(os.path.join(REF, "determinism_reference", name + ".npz"))
     r = _oracle_for_fixture(oracle_lib).detect_and_compute(gray)
     check_pin(r, fx["points"], fx["angles"], fx["descriptors"])
+
+
+@pytest.mark.parametrize("faithful", [False, True])
+def test_blend_oracle_matches_reference_composition(faithful):
+    """oracle/blend_oracle.py against the reference's own _blend_pair + paste
+    (tests/golden/make_blend_golden.py): bit-exact in both forms."""
+    from oracle import blend_oracle as bo
+    g = np.load(os.path.join(HERE, "golden", "blend_cases.npz"))
+    assert len(g["names"]) >= 4
+    for name in g["names"]:
+        w1, m1, c2, m2 = (g[f"{name}_{k}"] for k in ("warped1", "mask1", "canvas2", "mask2"))
+        pano, both = bo.blend_pair(w1, m1, c2, m2, faithful=faithful)
+        assert np.array_equal(both, g[f"{name}_both"]), name
+        assert np.array_equal(pano, g[f"{name}_pano"]), name
+
+
+@pytest.mark.skipif(not os.path.isfile(os.path.join(REF, "pysift", "core.py")), reason="reference tree absent")
+def test_blend_fixture_regenerates():
+    """The committed composition fixtures are what the reference produces now."""
+    import subprocess
+    import sys
+    import tempfile
+    src = os.path.join(HERE, "golden", "make_blend_golden.py")
+    with tempfile.TemporaryDirectory() as d:
+        r = subprocess.run([sys.executable, src, REF, d], capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        new = np.load(os.path.join(d, "blend_cases.npz"))
+        old = np.load(os.path.join(HERE, "golden", "blend_cases.npz"))
+        for k in old.files:
+            assert np.array_equal(new[k], old[k], equal_nan=k.endswith("seam_rmse")), k
