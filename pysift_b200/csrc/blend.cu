@@ -45,6 +45,7 @@ struct BlendCtl {
     float gain[3];
     int have_ov, vertical, first_side;  // first_side: image 1 left of (vertical) / above the seam
     int line0, line1;                   // first and last DP line holding overlap
+    int n_lines, seam_end;              // overlap lines; seam position on the last one
 };
 
 template <typename T>
@@ -65,14 +66,20 @@ __device__ __forceinline__ int warp_or(int v) {
 __global__ void __launch_bounds__(256) k_blend_stats(const uint8_t* __restrict__ w1, const uint8_t* __restrict__ m1,
                                                      const uint8_t* __restrict__ c2, const uint8_t* __restrict__ m2,
                                                      int cw, BlendCtl* ctl, int* __restrict__ rowf,
-                                                     int* __restrict__ colf) {
+                                                     int* __restrict__ colf, int* __restrict__ rlo,
+                                                     int* __restrict__ rhi, int* __restrict__ clo,
+                                                     int* __restrict__ chi) {
     __shared__ unsigned int s[7];
-    __shared__ int s_or;
+    __shared__ int s_or, s_lo, s_hi;
     if (threadIdx.x < 7) s[threadIdx.x] = 0u;
-    if (threadIdx.x == 0) s_or = 0;
+    if (threadIdx.x == 0) {
+        s_or = 0;
+        s_lo = 0x7fffffff;
+        s_hi = -1;
+    }
     __syncthreads();
     const int v = blockIdx.y;
-    int f_row = 0;
+    int f_row = 0, lo = 0x7fffffff, hi = -1;
     unsigned int acc[7] = {0, 0, 0, 0, 0, 0, 0};
     for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < cw; u += gridDim.x * blockDim.x) {
         const long long p = (long long)v * cw + u;
@@ -87,9 +94,22 @@ __global__ void __launch_bounds__(256) k_blend_stats(const uint8_t* __restrict__
                 acc[3 + c] += c2[p * 3 + c];
             }
             acc[6] += 1u;
+            lo = min(lo, u);
+            hi = max(hi, u);
+            atomicMin(&clo[u], v);
+            atomicMax(&chi[u], v);
         }
     }
     f_row = warp_or(f_row);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if ((threadIdx.x & 31) == 0 && hi >= 0) {
+        atomicMin(&s_lo, lo);
+        atomicMax(&s_hi, hi);
+    }
 #pragma unroll
     for (int k = 0; k < 7; ++k) acc[k] = warp_sum(acc[k]);
     if ((threadIdx.x & 31) == 0) {
@@ -101,6 +121,8 @@ __global__ void __launch_bounds__(256) k_blend_stats(const uint8_t* __restrict__
     }
     __syncthreads();
     if (threadIdx.x == 0) {
+        rlo[v] = s_lo;
+        rhi[v] = s_hi;
         if (s_or) atomicOr(&rowf[v], s_or);
         if (s[6]) {
 #pragma unroll
@@ -273,56 +295,168 @@ __global__ void k_sobel_cost(const float* __restrict__ dxp, const float* __restr
     else dpc[(long long)x * H + y] = out;
 }
 
-// Dynamic-programming seam (pysift/core.py:3286-3383) in one CTA: lines in
-// order (rows for a vertical seam, columns for a horizontal one), positions
-// in parallel; the two DP lines live in shared memory when they fit.
-// dir[i][j] is the argmin (0 left, 1 centre, 2 right) of line i.
+__device__ __forceinline__ void bl_cp_async4(void* dst, const void* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void bl_cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void bl_cp_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Dynamic-programming seam, forward pass (pysift/core.py:3286-3383), in one
+// CTA: overlap lines in order (rows for a vertical seam, columns for a
+// horizontal one), positions in parallel.  Line q only computes its window:
+// its own overlap range widened to one past the previous overlap line's range.
+// Outside it all three predecessors are INF, so the DP value is INF and the
+// argmin is 0 (dir is cleared beforehand).  The DP lines hold INF outside the
+// window (positions of the line before last that fall outside are reset) and
+// carry one INF sentinel at each end.  With K > 0 the cost lines stream
+// through a K-deep cp.async ring, each thread copying the positions it reads.
+// Outputs: dir[line][pos] = argmin (0 left, 1 centre, 2 right), the compacted
+// overlap lines, and in ctl their count and the seam position on the last one
+// (numpy's first minimum over the whole line).
+template <int K>
 __global__ void __launch_bounds__(1024) k_blend_dp(const float* __restrict__ dpc, const int* __restrict__ rowf,
-                                                   const int* __restrict__ colf, int cw, int ch,
-                                                   const BlendCtl* ctl, double* __restrict__ rowA,
-                                                   double* __restrict__ rowB, int use_smem,
-                                                   uint8_t* __restrict__ dir, int* __restrict__ seam) {
-    extern __shared__ double dp_sm[];
+                                                   const int* __restrict__ colf, const int* __restrict__ rlo,
+                                                   const int* __restrict__ rhi, const int* __restrict__ clo,
+                                                   const int* __restrict__ chi, int cw, int ch, BlendCtl* ctl,
+                                                   double* __restrict__ gA, double* __restrict__ gB,
+                                                   int2* __restrict__ gwin, int in_global,
+                                                   uint8_t* __restrict__ dir, int* __restrict__ ovl) {
+    extern __shared__ __align__(16) unsigned char dsm[];
+    __shared__ int s_sh[33];
+    __shared__ double s_best[32];
+    __shared__ int s_idx[32];
     if (!ctl->have_ov) return;
     const bool vert = ctl->vertical != 0;
     const int L = vert ? ch : cw, M = vert ? cw : ch;
     const int* lf = vert ? rowf : colf;
-    const int i0 = ctl->line0, i1 = ctl->line1;
-    double* prev = use_smem ? dp_sm : rowA;
-    double* cur = use_smem ? dp_sm + M : rowB;
-    for (int j = threadIdx.x; j < M; j += blockDim.x) {
-        const float c = dpc[(long long)i0 * M + j];
-        prev[j] = c >= 0.0f ? (double)c : BL_INF;
+    const int* lo_of = vert ? rlo : clo;
+    const int* hi_of = vert ? rhi : chi;
+    const int nfw = (L + 31) >> 5;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    // shared layout: line bitmask | windows | the two DP lines (M + 2 each) | ring
+    unsigned* fl = reinterpret_cast<unsigned*>(dsm);
+    size_t off = ((size_t)nfw * 4 + 15) & ~(size_t)15;
+    int2* win = in_global ? gwin : reinterpret_cast<int2*>(dsm + off);
+    if (!in_global) off += ((size_t)L * 8 + 15) & ~(size_t)15;
+    double* lineA = in_global ? gA : reinterpret_cast<double*>(dsm + off);
+    double* lineB = in_global ? gB : lineA + (M + 2);
+    if (!in_global) off += (size_t)(M + 2) * 16;
+    float* ring = reinterpret_cast<float*>(dsm + off);
+    // overlap-line bitmask and the compacted list of overlap lines
+    const int per = (nfw + nt - 1) / nt;
+    const int w0 = min(nfw, tid * per), w1 = min(nfw, (tid + 1) * per);
+    int cnt = 0;
+    for (int w = w0; w < w1; ++w) {
+        unsigned b = 0u;
+        for (int k = 0; k < 32; ++k) {
+            const int i = (w << 5) + k;
+            if (i < L && (lf[i] & 1)) b |= 1u << k;
+        }
+        fl[w] = b;
+        cnt += __popc(b);
+    }
+    int nL;
+    int base = block_excl_scan(cnt, &nL, s_sh);
+    for (int w = w0; w < w1; ++w) {
+        unsigned b = fl[w];
+        while (b) {
+            const int k = __ffs(b) - 1;
+            b &= b - 1u;
+            const int line = (w << 5) + k;
+            const int lo = lo_of[line], hi = hi_of[line];
+            int2 wn = make_int2(lo, hi);
+            if (base > 0) {
+                // the previous overlap line: the highest set bit below `line`
+                int pw = line >> 5;
+                unsigned pb = fl[pw] & ((1u << (line & 31)) - 1u);
+                while (!pb) pb = fl[--pw];  // base > 0: an earlier overlap line exists
+                const int pline = (pw << 5) + 31 - __clz(pb);
+                wn.x = max(0, min(lo_of[pline] - 1, lo));
+                wn.y = min(M - 1, max(hi_of[pline] + 1, hi));
+            }
+            win[base] = wn;
+            ovl[base++] = line;
+        }
+    }
+    for (int j = tid; j < M + 2; j += nt) {
+        lineA[j] = BL_INF;
+        lineB[j] = BL_INF;
     }
     __syncthreads();
-    for (int i = i0 + 1; i <= i1; ++i) {
-        if (!(lf[i] & 1)) continue;  // the same flag for every thread
-        const float* crow = dpc + (long long)i * M;
-        uint8_t* drow = dir + (long long)i * M;
-        for (int j = threadIdx.x; j < M; j += blockDim.x) {
+    double* prev = lineA + 1;  // prev[-1] and prev[M] stay INF
+    double* cur = lineB + 1;
+    {
+        const int2 w = win[0];
+        const float* crow = dpc + (long long)ovl[0] * M;
+        for (int j = w.x + tid; j <= w.y; j += nt) {
             const float c = crow[j];
-            const double pl = j > 0 ? prev[j - 1] : BL_INF;
-            const double pm = prev[j];
-            const double pr = j < M - 1 ? prev[j + 1] : BL_INF;
+            prev[j] = c >= 0.0f ? (double)c : BL_INF;
+        }
+    }
+    constexpr int KR = K > 0 ? K : 1;
+    if (K > 0) {
+        for (int s = 0; s < K - 1; ++s) {
+            const int q = 1 + s;
+            if (q < nL) {
+                const int2 w = win[q];
+                const float* src = dpc + (long long)ovl[q] * M;
+                float* slot = ring + (size_t)s * M;
+                for (int j = w.x + tid; j <= w.y; j += nt) bl_cp_async4(slot + j, src + j);
+            }
+            bl_cp_commit();
+        }
+    }
+    __syncthreads();
+    for (int q = 1; q < nL; ++q) {
+        const int2 w = win[q];
+        const float* crow;
+        if (K > 0) {
+            const int qn = q + K - 1;
+            if (qn < nL) {
+                const int2 wn = win[qn];
+                const float* src = dpc + (long long)ovl[qn] * M;
+                float* slot = ring + (size_t)((q + K - 2) % KR) * M;
+                for (int j = wn.x + tid; j <= wn.y; j += nt) bl_cp_async4(slot + j, src + j);
+            }
+            bl_cp_commit();
+            bl_cp_wait<KR - 1>();
+            crow = ring + (size_t)((q - 1) % KR) * M;
+        } else {
+            crow = dpc + (long long)ovl[q] * M;
+        }
+        // positions of the line before last outside this window go back to INF
+        if (q >= 2) {
+            const int2 o = win[q - 2];
+            for (int j = o.x + tid; j < min(o.y + 1, w.x); j += nt) cur[j] = BL_INF;
+            for (int j = max(o.x, w.y + 1) + tid; j <= o.y; j += nt) cur[j] = BL_INF;
+        }
+        uint8_t* drow = dir + (long long)ovl[q] * M;
+        for (int j = w.x + tid; j <= w.y; j += nt) {
+            const float c = crow[j];
+            const double pl = prev[j - 1], pm = prev[j], pr = prev[j + 1];
             int a = 0;
             double best = pl;
             if (pm < best) { best = pm; a = 1; }
             if (pr < best) { best = pr; a = 2; }
             cur[j] = c >= 0.0f ? (double)c + best : BL_INF;
-            drow[j] = (uint8_t)a;
+            if (a) drow[j] = (uint8_t)a;
         }
         __syncthreads();
         double* t = prev;
         prev = cur;
         cur = t;
     }
-    // first minimum of the last overlap line: per-thread, then across the block
-    __shared__ double s_best[32];
-    __shared__ int s_idx[32];
+    if (K > 0) bl_cp_wait<0>();
+    // first minimum of the last overlap line (non-overlap positions count as INF)
+    const int last = ovl[nL - 1];
     double bv = BL_INF * 4.0;
     int bj = 0x7fffffff;
-    for (int j = threadIdx.x; j < M; j += blockDim.x) {
-        const double vv = dpc[(long long)i1 * M + j] >= 0.0f ? prev[j] : BL_INF;
+    for (int j = tid; j < M; j += nt) {
+        const double vv = dpc[(long long)last * M + j] >= 0.0f ? prev[j] : BL_INF;
         if (vv < bv) { bv = vv; bj = j; }
     }
 #pragma unroll
@@ -331,23 +465,71 @@ __global__ void __launch_bounds__(1024) k_blend_dp(const float* __restrict__ dpc
         const int oj = __shfl_xor_sync(0xffffffffu, bj, o);
         if (ov < bv || (ov == bv && oj < bj)) { bv = ov; bj = oj; }
     }
-    if ((threadIdx.x & 31) == 0) {
-        s_best[threadIdx.x >> 5] = bv;
-        s_idx[threadIdx.x >> 5] = bj;
+    if ((tid & 31) == 0) {
+        s_best[tid >> 5] = bv;
+        s_idx[tid >> 5] = bj;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
+    if (tid == 0) {
+        for (int w = 1; w < (nt >> 5); ++w)
             if (s_best[w] < bv || (s_best[w] == bv && s_idx[w] < bj)) { bv = s_best[w]; bj = s_idx[w]; }
-        int sc = bj;
-        for (int i = 0; i < L; ++i) seam[i] = sc;
-        int r = i1;
-        for (int i = i1 - 1; i >= i0; --i) {
-            if (!(lf[i] & 1)) continue;
-            int k = seam[r] + (int)dir[(long long)r * M + seam[r]] - 1;
-            k = k < 0 ? 0 : (k > M - 1 ? M - 1 : k);
-            seam[i] = k;
-            r = i;
+        ctl->seam_end = bj;
+        ctl->n_lines = nL;
+    }
+}
+
+// one backtrack step from overlap line q (position p) to overlap line q - 1
+__device__ __forceinline__ int bt_step(const uint8_t* __restrict__ dir, const int* __restrict__ ovl, int M, int q,
+                                       int p) {
+    const int k = p + (int)dir[(long long)ovl[q] * M + p] - 1;
+    return k < 0 ? 0 : (k > M - 1 ? M - 1 : k);
+}
+
+// Backtrack, stage 1: the overlap lines are cut into chunks of R; for chunk
+// c below the last and every position j on overlap line (c + 1) R, the
+// position the seam reaches on overlap line c R.
+__global__ void k_seam_jump(const uint8_t* __restrict__ dir, const int* __restrict__ ovl, const BlendCtl* ctl,
+                            int cw, int ch, int R, int* __restrict__ jump) {
+    if (!ctl->have_ov) return;
+    const int M = ctl->vertical ? cw : ch;
+    const int C = (ctl->n_lines + R - 1) / R;
+    const int c = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= C - 1 || j >= M) return;
+    int p = j;
+    for (int q = (c + 1) * R; q > c * R; --q) p = bt_step(dir, ovl, M, q, p);
+    jump[(long long)c * M + j] = p;
+}
+
+// Backtrack, stage 2 (one CTA): the chunk entry positions in sequence, then
+// the lines of every chunk in parallel; lines without overlap keep the end
+// position (pysift/core.py:3326-3334).
+__global__ void __launch_bounds__(1024) k_seam_walk(const uint8_t* __restrict__ dir, const int* __restrict__ ovl,
+                                                    const BlendCtl* ctl, int cw, int ch, int R,
+                                                    const int* __restrict__ jump, int* __restrict__ entry,
+                                                    int* __restrict__ seam) {
+    if (!ctl->have_ov) return;
+    const bool vert = ctl->vertical != 0;
+    const int L = vert ? ch : cw, M = vert ? cw : ch;
+    const int nL = ctl->n_lines, sc = ctl->seam_end;
+    const int C = (nL + R - 1) / R;
+    for (int i = threadIdx.x; i < L; i += blockDim.x) seam[i] = sc;
+    if (threadIdx.x == 0) {
+        int p = sc;
+        for (int q = nL - 1; q > (C - 1) * R; --q) p = bt_step(dir, ovl, M, q, p);
+        entry[C - 1] = p;  // the position on overlap line (C - 1) R
+        for (int c = C - 2; c >= 0; --c) {
+            p = jump[(long long)c * M + p];
+            entry[c] = p;
+        }
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < C; c += blockDim.x) {
+        const int qtop = c == C - 1 ? nL - 1 : (c + 1) * R;
+        int p = c == C - 1 ? sc : entry[c + 1];
+        seam[ovl[qtop]] = p;
+        for (int q = qtop; q > c * R; --q) {
+            p = bt_step(dir, ovl, M, q, p);
+            seam[ovl[q - 1]] = p;
         }
     }
 }
@@ -537,9 +719,17 @@ __global__ void k_place_image(const uint8_t* __restrict__ img, int h, int w, int
 
 constexpr int DP_SMEM_MAX = 200 * 1024;
 
+// backtrack chunk length: about the square root of the line count, at least 16
+static int seam_chunk(int L) {
+    int R = 16;
+    while ((long long)R * R < L) R *= 2;
+    return R;
+}
+
 struct BlendLayout {
-    size_t off_ctl, off_rowf, off_colf, off_color, off_avg, off_d1, off_d2, off_dpc, off_rowA, off_rowB, off_dir,
-        off_seam, off_blur, off_w9, off_k25, off_tmp;
+    size_t off_ctl, off_rowf, off_colf, off_rlo, off_rhi, off_clo, off_chi, off_win, off_color, off_avg, off_d1, off_d2, off_dpc, off_rowA, off_rowB, off_dir,
+        off_seam, off_ovl, off_jump, off_entry, off_blur, off_w9, off_k25, off_tmp;
+    int R;
     size_t off_g1[8], off_g2[8], off_gm[8], off_lb[8], off_res[2];
     int h[8], w[8];
     size_t total;
@@ -558,15 +748,24 @@ static BlendLayout blend_layout(int cw, int ch, int levels) {
     l.off_ctl = take(sizeof(BlendCtl));
     l.off_rowf = take((size_t)ch * 4);
     l.off_colf = take((size_t)cw * 4);
+    l.off_rlo = take((size_t)ch * 4);
+    l.off_rhi = take((size_t)ch * 4);
+    l.off_clo = take((size_t)cw * 4);
+    l.off_chi = take((size_t)cw * 4);
+    l.off_win = take((size_t)(cw > ch ? cw : ch) * 8);
     l.off_color = take(N * 4);
     l.off_avg = take(N * 4);
     l.off_d1 = take(N * 4);
     l.off_d2 = take(N * 4);
     l.off_dpc = take(N * 4);
-    l.off_rowA = take((size_t)M * 8);
-    l.off_rowB = take((size_t)M * 8);
+    l.off_rowA = take((size_t)(M + 2) * 8);
+    l.off_rowB = take((size_t)(M + 2) * 8);
     l.off_dir = take(N);
     l.off_seam = take((size_t)M * 4);
+    l.off_ovl = take((size_t)M * 4);
+    l.R = seam_chunk(M);
+    l.off_jump = take((size_t)((M + l.R - 1) / l.R) * M * 4);
+    l.off_entry = take((size_t)((M + l.R - 1) / l.R + 1) * 4);
     l.off_blur = take(N * 4);
     l.off_w9 = take(9 * 8);
     l.off_k25 = take(25 * 4);
@@ -650,7 +849,14 @@ int pysift_blend_multiband(const uint8_t* warped1, const uint8_t* mask1, const u
     PYSIFT_CUDA_TRY(cudaMemcpyAsync(k25, seam_k25, 25 * sizeof(float), cudaMemcpyHostToDevice, st));
     const dim3 g2d(ceil_div(cw, 256), ch);
     const long long N = (long long)cw * ch;
-    k_blend_stats<<<dim3(1, ch), 256, 0, st>>>(warped1, mask1, canvas2, mask2, cw, ctl, rowf, colf);
+    int* rlo = bwp<int>(ws, l.off_rlo);
+    int* rhi = bwp<int>(ws, l.off_rhi);
+    int* clo = bwp<int>(ws, l.off_clo);
+    int* chi = bwp<int>(ws, l.off_chi);
+    PYSIFT_CUDA_TRY(cudaMemsetAsync(clo, 0x7f, (size_t)cw * 4, st));
+    PYSIFT_CUDA_TRY(cudaMemsetAsync(chi, 0xff, (size_t)cw * 4, st));
+    k_blend_stats<<<dim3(1, ch), 256, 0, st>>>(warped1, mask1, canvas2, mask2, cw, ctl, rowf, colf, rlo, rhi, clo,
+                                                chi);
     PYSIFT_LAUNCH_CHECK("k_blend_stats");
     k_blend_decide<<<1, 1024, 0, st>>>(ctl, rowf, colf, cw, ch);
     PYSIFT_LAUNCH_CHECK("k_blend_decide");
@@ -668,14 +874,46 @@ int pysift_blend_multiband(const uint8_t* warped1, const uint8_t* mask1, const u
     k_sobel_cost<<<g2d, 256, 0, st>>>(d1, d2, color, mask1, mask2, ctl, dpc, cw, ch);
     PYSIFT_LAUNCH_CHECK("k_sobel_cost");
     int* seam = bwp<int>(ws, l.off_seam);
-    const int M = cw > ch ? cw : ch;
-    const size_t dp_smem = (size_t)M * 16;
-    const int use_smem = dp_smem <= (size_t)DP_SMEM_MAX;
-    if (use_smem) PYSIFT_CUDA_TRY(cudaFuncSetAttribute(k_blend_dp, cudaFuncAttributeMaxDynamicSharedMemorySize, DP_SMEM_MAX));
-    k_blend_dp<<<1, 1024, use_smem ? dp_smem : 0, st>>>(dpc, rowf, colf, cw, ch, ctl, bwp<double>(ws, l.off_rowA),
-                                                        bwp<double>(ws, l.off_rowB), use_smem,
-                                                        bwp<uint8_t>(ws, l.off_dir), seam);
-    PYSIFT_LAUNCH_CHECK("k_blend_dp");
+    {
+        int* ovl = bwp<int>(ws, l.off_ovl);
+        uint8_t* dir = bwp<uint8_t>(ws, l.off_dir);
+        // the orientation is decided on the device: size shared memory for the longer side
+        const int M = cw > ch ? cw : ch;
+        const size_t flags = (((size_t)(M + 31) / 32) * 4 + 15) & ~(size_t)15;
+        const size_t wins = ((size_t)M * 8 + 15) & ~(size_t)15;
+        const size_t lines = (size_t)(M + 2) * 16;
+        double* gA = bwp<double>(ws, l.off_rowA);
+        double* gB = bwp<double>(ws, l.off_rowB);
+        int2* gwin = bwp<int2>(ws, l.off_win);
+        PYSIFT_CUDA_TRY(cudaMemsetAsync(dir, 0, (size_t)cw * ch, st));
+        const size_t base = flags + wins + lines;
+        if (base + (size_t)M * 32 <= (size_t)DP_SMEM_MAX) {
+            const size_t sm = base + (size_t)M * 32;
+            PYSIFT_CUDA_TRY(cudaFuncSetAttribute(k_blend_dp<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            k_blend_dp<8><<<1, 1024, sm, st>>>(dpc, rowf, colf, rlo, rhi, clo, chi, cw, ch, ctl, gA, gB, gwin, 0, dir,
+                                               ovl);
+        } else if (base + (size_t)M * 16 <= (size_t)DP_SMEM_MAX) {
+            const size_t sm = base + (size_t)M * 16;
+            PYSIFT_CUDA_TRY(cudaFuncSetAttribute(k_blend_dp<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            k_blend_dp<4><<<1, 1024, sm, st>>>(dpc, rowf, colf, rlo, rhi, clo, chi, cw, ch, ctl, gA, gB, gwin, 0, dir,
+                                               ovl);
+        } else if (base <= (size_t)DP_SMEM_MAX) {
+            PYSIFT_CUDA_TRY(cudaFuncSetAttribute(k_blend_dp<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)base));
+            k_blend_dp<0><<<1, 1024, base, st>>>(dpc, rowf, colf, rlo, rhi, clo, chi, cw, ch, ctl, gA, gB, gwin, 0, dir,
+                                                 ovl);
+        } else {
+            PYSIFT_CUDA_TRY(cudaFuncSetAttribute(k_blend_dp<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)flags));
+            k_blend_dp<0><<<1, 1024, flags, st>>>(dpc, rowf, colf, rlo, rhi, clo, chi, cw, ch, ctl, gA, gB, gwin, 1,
+                                                  dir, ovl);
+        }
+        PYSIFT_LAUNCH_CHECK("k_blend_dp");
+        const int R = l.R;
+        int* jump = bwp<int>(ws, l.off_jump);
+        k_seam_jump<<<dim3(ceil_div(M, 256), (M + R - 1) / R), 256, 0, st>>>(dir, ovl, ctl, cw, ch, R, jump);
+        PYSIFT_LAUNCH_CHECK("k_seam_jump");
+        k_seam_walk<<<1, 1024, 0, st>>>(dir, ovl, ctl, cw, ch, R, jump, bwp<int>(ws, l.off_entry), seam);
+        PYSIFT_LAUNCH_CHECK("k_seam_walk");
+    }
     float* gm0 = bwp<float>(ws, l.off_gm[0]);
     float* blur = bwp<float>(ws, l.off_blur);
     k_blend_seam_mask<<<g2d, 256, 0, st>>>(mask1, mask2, seam, ctl, gm0, cw);

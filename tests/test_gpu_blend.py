@@ -102,6 +102,50 @@ def test_blend_levels(n_levels):
     assert np.array_equal(pano, ref)
 
 
+@pytest.mark.parametrize("cw", [5000, 9000, 13000])
+def test_blend_long_canvas(cw):
+    """A vertical seam across wide canvases: the DP lines in shared memory with
+    an 8- or 4-deep cost ring, without the ring, and in global memory."""
+    from oracle import blend_oracle as bo
+    ch = 90
+    rng = np.random.default_rng(cw)
+    yy, xx = np.mgrid[0:ch, 0:cw]
+    a = cw // 2
+    m1 = xx < a + 20 + yy // 8
+    m2 = (xx >= a - 25) & (yy >= 3)
+    base = synthetic.dense_texture(ch, cw, seed=cw).astype(np.float64)
+    w1 = np.clip(base[:, :, None] * 0.8 + rng.normal(0, 3, (ch, cw, 3)), 0, 255).astype(np.uint8)
+    c2 = np.clip(base[:, :, None] * 1.1 + rng.normal(0, 3, (ch, cw, 3)), 0, 255).astype(np.uint8)
+    w1[~m1] = 0
+    c2[~m2] = 0
+    pano, both, _ = _run(w1, m1, c2, m2)
+    ref, ref_both = bo.blend_pair(w1, m1, c2, m2)
+    assert np.array_equal(both, ref_both)
+    assert np.array_equal(pano, ref)
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2, 3])
+def test_blend_degenerate_masks(seed):
+    """Overlaps with holes, disconnected parts and lines far apart: the DP
+    window logic and the backtrack through INF positions."""
+    from oracle import blend_oracle as bo
+    rng = np.random.default_rng(100 + seed)
+    ch, cw = 120, 170
+    m1 = rng.random((ch, cw)) < (0.3 + 0.1 * seed)
+    m2 = rng.random((ch, cw)) < 0.5
+    if seed % 2:
+        m1[:, : cw // 3] = True
+        m2[: ch // 2, cw // 2:] = True
+    w1 = rng.integers(0, 256, (ch, cw, 3), dtype=np.uint8)
+    c2 = rng.integers(0, 256, (ch, cw, 3), dtype=np.uint8)
+    w1[~m1] = 0
+    c2[~m2] = 0
+    pano, both, _ = _run(w1, m1, c2, m2)
+    ref, ref_both = bo.blend_pair(w1, m1, c2, m2)
+    assert np.array_equal(both, ref_both)
+    assert np.array_equal(pano, ref)
+
+
 def test_blend_no_overlap_and_edges():
     """No overlap (no gain, no seam), an overlap of one column and one of one row."""
     from oracle import blend_oracle as bo
