@@ -13,8 +13,8 @@
 // 2 x 2 corners in row-major order, in float64; the DP in float64 with
 // numpy's first-minimum tie order.  Canonical choices: the gain means are
 // exact (int64 sums / count); the seam-mask blur (cv2.GaussianBlur, sigma 3)
-// is separable with the float32 kernel getGaussianKernel(25, 3), reflect-101,
-// rows then columns, float64 sums.
+// is separable with the 25 float32 taps the caller passes (exp(-x^2 / 18)
+// normalised), reflect-101, rows then columns, float64 sums.
 #include <cstdint>
 
 #include "common.cuh"
@@ -222,17 +222,42 @@ __global__ void __launch_bounds__(1024) k_blend_decide(BlendCtl* ctl, const int*
     }
 }
 
-// gained image 1, the pyramid inputs I1 / I2 (pysift/core.py:3703-3708),
-// colour cost, average gray and the seam-RMSE sum (pysift/core.py:3555-3562)
+// image 1 after gain, the pyramid inputs I1 / I2 (pysift/core.py:3703-3708)
+// at one pixel, from the uint8 canvases; the level-0 passes recompute them
+// instead of storing two float images
+struct Level0 {
+    const uint8_t* w1;
+    const uint8_t* m1;
+    const uint8_t* c2;
+    const uint8_t* m2;
+    const BlendCtl* ctl;
+    __device__ __forceinline__ void px(long long p, float i1[3], float i2[3]) const {
+        const bool a = m1[p] != 0, b = m2[p] != 0;
+        const bool gained = ctl->have_ov != 0;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            float x = (float)w1[p * 3 + c];
+            if (gained) {
+                x = x * ctl->gain[c];
+                x = x < 0.0f ? 0.0f : (x > 255.0f ? 255.0f : x);
+            }
+            const float y = (float)c2[p * 3 + c];
+            i1[c] = a ? x : (b ? y : 0.0f);
+            i2[c] = b ? y : (a ? x : 0.0f);
+        }
+    }
+};
+
+// colour cost, average gray (pysift/core.py:3411-3415) and the seam-RMSE sum
+// (pysift/core.py:3555-3562) of the gained image 1
 __global__ void k_blend_prepare(const uint8_t* __restrict__ w1, const uint8_t* __restrict__ m1,
                                 const uint8_t* __restrict__ c2, const uint8_t* __restrict__ m2, int cw,
-                                BlendCtl* ctl, float* __restrict__ I1, float* __restrict__ I2,
-                                float* __restrict__ color, float* __restrict__ avg) {
+                                BlendCtl* ctl, float* __restrict__ color, float* __restrict__ avg) {
     const int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
     unsigned int sq = 0;
     if (u < cw) {
         const long long p = (long long)v * cw + u;
-        const bool a = m1[p] != 0, b = m2[p] != 0;
+        const bool ov = m1[p] != 0 && m2[p] != 0;
         const bool gained = ctl->have_ov != 0;
         float g1[3], g2[3];
 #pragma unroll
@@ -244,7 +269,7 @@ __global__ void k_blend_prepare(const uint8_t* __restrict__ w1, const uint8_t* _
             }
             g1[c] = x;
             g2[c] = (float)c2[p * 3 + c];
-            if (a && b) {
+            if (ov) {
                 const int d = (int)x - (int)c2[p * 3 + c];
                 sq += (unsigned int)(d * d);
             }
@@ -253,42 +278,33 @@ __global__ void k_blend_prepare(const uint8_t* __restrict__ w1, const uint8_t* _
         color[p] = sqrtf((d0 * d0 + d1 * d1) + d2 * d2);
         const float s0 = (g1[0] + g2[0]) * 0.5f, s1 = (g1[1] + g2[1]) * 0.5f, s2 = (g1[2] + g2[2]) * 0.5f;
         avg[p] = ((s0 + s1) + s2) / 3.0f;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            I1[p * 3 + c] = a ? g1[c] : (b ? g2[c] : 0.0f);
-            I2[p * 3 + c] = b ? g2[c] : (a ? g1[c] : 0.0f);
-        }
     }
     sq = warp_sum(sq);
     if ((threadIdx.x & 31) == 0 && sq) atomicAdd(&ctl->sq, (unsigned long long)sq);
 }
 
-// scipy sobel, first pass: derivative [-1, 0, 1] along `axis` (antisymmetric: (x[i+1] - x[i-1]))
-__global__ void k_sobel_deriv(const float* __restrict__ in, float* __restrict__ dx, float* __restrict__ dy, int W,
-                              int H) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    if (x >= W) return;
-    const long long row = (long long)y * W;
-    dx[row + x] = (float)((double)in[row + refl_half(x + 1, W)] - (double)in[row + refl_half(x - 1, W)]);
-    dy[row + x] = (float)((double)in[(long long)refl_half(y + 1, H) * W + x] -
-                          (double)in[(long long)refl_half(y - 1, H) * W + x]);
-}
-
-// second pass: [1, 2, 1] along the other axis; then the cost (pysift/core.py:3411-3420).
-// The DP reads `dpc`: the cost where both images cover the canvas, else -1,
-// laid out line by line (transposed for a horizontal seam).
-__global__ void k_sobel_cost(const float* __restrict__ dxp, const float* __restrict__ dyp,
-                             const float* __restrict__ color, const uint8_t* __restrict__ m1,
-                             const uint8_t* __restrict__ m2, const BlendCtl* ctl, float* __restrict__ dpc, int W,
-                             int H) {
+// scipy sobel of the average gray along both axes and the seam cost
+// (pysift/core.py:3416-3420).  Each sobel is correlate1d([-1, 0, 1]) along its
+// axis (antisymmetric: x[i+1] - x[i-1]) rounded to float32, then [1, 2, 1]
+// along the other (2 x[i] + (x[i-1] + x[i+1])), both in float64 with
+// half-sample reflection.  The DP reads `dpc`: the cost where both images
+// cover the canvas, else -1, line by line (transposed for a horizontal seam).
+__global__ void k_sobel_cost(const float* __restrict__ avg, const float* __restrict__ color,
+                             const uint8_t* __restrict__ m1, const uint8_t* __restrict__ m2, const BlendCtl* ctl,
+                             float* __restrict__ dpc, int W, int H) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x >= W) return;
     const long long p = (long long)y * W + x;
-    const double gxd = 2.0 * (double)dxp[p] + ((double)dxp[(long long)refl_half(y - 1, H) * W + x] +
-                                               (double)dxp[(long long)refl_half(y + 1, H) * W + x]);
-    const double gyd = 2.0 * (double)dyp[p] + ((double)dyp[(long long)y * W + refl_half(x - 1, W)] +
-                                               (double)dyp[(long long)y * W + refl_half(x + 1, W)]);
-    const float gx = (float)gxd, gy = (float)gyd;
+    const int xl = refl_half(x - 1, W), xr = refl_half(x + 1, W);
+    const int yu = refl_half(y - 1, H), yd = refl_half(y + 1, H);
+    auto dxr = [&](int r) {  // the axis-1 derivative on row r, as float32
+        return (double)(float)((double)avg[(long long)r * W + xr] - (double)avg[(long long)r * W + xl]);
+    };
+    auto dyc = [&](int c) {  // the axis-0 derivative on column c, as float32
+        return (double)(float)((double)avg[(long long)yd * W + c] - (double)avg[(long long)yu * W + c]);
+    };
+    const float gx = (float)(2.0 * dxr(y) + (dxr(yu) + dxr(yd)));
+    const float gy = (float)(2.0 * dyc(x) + (dyc(xl) + dyc(xr)));
     const float c = color[p] + 0.05f * sqrtf(gx * gx + gy * gy);
     const float out = (m1[p] && m2[p]) ? c : -1.0f;
     if (ctl->vertical) dpc[p] = out;
@@ -323,7 +339,7 @@ __global__ void __launch_bounds__(1024) k_blend_dp(const float* __restrict__ dpc
                                                    const int* __restrict__ rhi, const int* __restrict__ clo,
                                                    const int* __restrict__ chi, int cw, int ch, BlendCtl* ctl,
                                                    double* __restrict__ gA, double* __restrict__ gB,
-                                                   int2* __restrict__ gwin, int in_global,
+                                                   int4* __restrict__ gwin, int in_global,
                                                    uint8_t* __restrict__ dir, int* __restrict__ ovl) {
     extern __shared__ __align__(16) unsigned char dsm[];
     __shared__ int s_sh[33];
@@ -337,11 +353,11 @@ __global__ void __launch_bounds__(1024) k_blend_dp(const float* __restrict__ dpc
     const int* hi_of = vert ? rhi : chi;
     const int nfw = (L + 31) >> 5;
     const int tid = threadIdx.x, nt = blockDim.x;
-    // shared layout: line bitmask | windows | the two DP lines (M + 2 each) | ring
+    // shared layout: line bitmask | windows {lo, hi, line} | the two DP lines (M + 2 each) | ring
     unsigned* fl = reinterpret_cast<unsigned*>(dsm);
     size_t off = ((size_t)nfw * 4 + 15) & ~(size_t)15;
-    int2* win = in_global ? gwin : reinterpret_cast<int2*>(dsm + off);
-    if (!in_global) off += ((size_t)L * 8 + 15) & ~(size_t)15;
+    int4* win = in_global ? gwin : reinterpret_cast<int4*>(dsm + off);
+    if (!in_global) off += (size_t)L * 16;
     double* lineA = in_global ? gA : reinterpret_cast<double*>(dsm + off);
     double* lineB = in_global ? gB : lineA + (M + 2);
     if (!in_global) off += (size_t)(M + 2) * 16;
@@ -368,7 +384,7 @@ __global__ void __launch_bounds__(1024) k_blend_dp(const float* __restrict__ dpc
             b &= b - 1u;
             const int line = (w << 5) + k;
             const int lo = lo_of[line], hi = hi_of[line];
-            int2 wn = make_int2(lo, hi);
+            int4 wn = make_int4(lo, hi, line, 0);
             if (base > 0) {
                 // the previous overlap line: the highest set bit below `line`
                 int pw = line >> 5;
@@ -390,8 +406,8 @@ __global__ void __launch_bounds__(1024) k_blend_dp(const float* __restrict__ dpc
     double* prev = lineA + 1;  // prev[-1] and prev[M] stay INF
     double* cur = lineB + 1;
     {
-        const int2 w = win[0];
-        const float* crow = dpc + (long long)ovl[0] * M;
+        const int4 w = win[0];
+        const float* crow = dpc + (long long)w.z * M;
         for (int j = w.x + tid; j <= w.y; j += nt) {
             const float c = crow[j];
             prev[j] = c >= 0.0f ? (double)c : BL_INF;
@@ -402,8 +418,8 @@ __global__ void __launch_bounds__(1024) k_blend_dp(const float* __restrict__ dpc
         for (int s = 0; s < K - 1; ++s) {
             const int q = 1 + s;
             if (q < nL) {
-                const int2 w = win[q];
-                const float* src = dpc + (long long)ovl[q] * M;
+                const int4 w = win[q];
+                const float* src = dpc + (long long)w.z * M;
                 float* slot = ring + (size_t)s * M;
                 for (int j = w.x + tid; j <= w.y; j += nt) bl_cp_async4(slot + j, src + j);
             }
@@ -412,13 +428,13 @@ __global__ void __launch_bounds__(1024) k_blend_dp(const float* __restrict__ dpc
     }
     __syncthreads();
     for (int q = 1; q < nL; ++q) {
-        const int2 w = win[q];
+        const int4 w = win[q];
         const float* crow;
         if (K > 0) {
             const int qn = q + K - 1;
             if (qn < nL) {
-                const int2 wn = win[qn];
-                const float* src = dpc + (long long)ovl[qn] * M;
+                const int4 wn = win[qn];
+                const float* src = dpc + (long long)wn.z * M;
                 float* slot = ring + (size_t)((q + K - 2) % KR) * M;
                 for (int j = wn.x + tid; j <= wn.y; j += nt) bl_cp_async4(slot + j, src + j);
             }
@@ -426,15 +442,15 @@ __global__ void __launch_bounds__(1024) k_blend_dp(const float* __restrict__ dpc
             bl_cp_wait<KR - 1>();
             crow = ring + (size_t)((q - 1) % KR) * M;
         } else {
-            crow = dpc + (long long)ovl[q] * M;
+            crow = dpc + (long long)w.z * M;
         }
         // positions of the line before last outside this window go back to INF
         if (q >= 2) {
-            const int2 o = win[q - 2];
+            const int4 o = win[q - 2];
             for (int j = o.x + tid; j < min(o.y + 1, w.x); j += nt) cur[j] = BL_INF;
             for (int j = max(o.x, w.y + 1) + tid; j <= o.y; j += nt) cur[j] = BL_INF;
         }
-        uint8_t* drow = dir + (long long)ovl[q] * M;
+        uint8_t* drow = dir + (long long)w.z * M;
         for (int j = w.x + tid; j <= w.y; j += nt) {
             const float c = crow[j];
             const double pl = prev[j - 1], pm = prev[j], pr = prev[j + 1];
@@ -452,7 +468,7 @@ __global__ void __launch_bounds__(1024) k_blend_dp(const float* __restrict__ dpc
     }
     if (K > 0) bl_cp_wait<0>();
     // first minimum of the last overlap line (non-overlap positions count as INF)
-    const int last = ovl[nL - 1];
+    const int last = win[nL - 1].z;
     double bv = BL_INF * 4.0;
     int bj = 0x7fffffff;
     for (int j = tid; j < M; j += nt) {
@@ -534,78 +550,141 @@ __global__ void __launch_bounds__(1024) k_seam_walk(const uint8_t* __restrict__ 
     }
 }
 
-// seam mask before the blur (pysift/core.py:3406-3467): 1 = image 1
-__global__ void k_blend_seam_mask(const uint8_t* __restrict__ m1, const uint8_t* __restrict__ m2,
-                                  const int* __restrict__ seam, const BlendCtl* ctl, float* __restrict__ mask, int cw) {
-    const int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
-    if (u >= cw) return;
+// the seam mask before its blur (pysift/core.py:3406-3467): 1 = image 1
+__device__ __forceinline__ float seam_value(const uint8_t* __restrict__ m1, const uint8_t* __restrict__ m2,
+                                            const int* __restrict__ seam, const BlendCtl* ctl, int u, int v, int cw) {
     const long long p = (long long)v * cw + u;
     const bool a = m1[p] != 0, b = m2[p] != 0;
-    float val = (a && !b) ? 1.0f : 0.0f;
-    if (a && b) {
-        const bool first = ctl->vertical ? (u <= seam[v]) : (v <= seam[u]);
-        val = (ctl->first_side ? first : !first) ? 1.0f : 0.0f;
-    }
-    mask[p] = val;
+    if (!a) return 0.0f;
+    if (!b) return 1.0f;
+    const bool first = ctl->vertical ? (u <= seam[v]) : (v <= seam[u]);
+    return (ctl->first_side ? first : !first) ? 1.0f : 0.0f;
 }
 
-// seam-mask blur (sigma 3, 25 taps, reflect-101): one axis, float64 sums in tap order
-__global__ void k_blend_seam_blur(const float* __restrict__ in, float* __restrict__ out, int W, int H, int axis,
-                                  const float* __restrict__ k25) {
+// seam-mask blur (sigma 3, 25 taps, reflect-101, float64 sums in tap order):
+// the row pass over the mask values ...
+__global__ void k_seam_rows(const uint8_t* __restrict__ m1, const uint8_t* __restrict__ m2,
+                            const int* __restrict__ seam, const BlendCtl* ctl, const float* __restrict__ k25,
+                            float* __restrict__ out, int W) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x >= W) return;
     double s = 0.0;
 #pragma unroll 5
-    for (int t = 0; t < 25; ++t) {
-        const float v = axis == 1 ? in[(long long)y * W + refl_101(x + t - 12, W)]
-                                  : in[(long long)refl_101(y + t - 12, H) * W + x];
-        s = s + (double)k25[t] * (double)v;
-    }
+    for (int t = 0; t < 25; ++t)
+        s = s + (double)k25[t] * (double)seam_value(m1, m2, seam, ctl, refl_101(x + t - 12, W), y, W);
     out[(long long)y * W + x] = (float)s;
 }
 
-// the blurred values replace the mask where both images cover the canvas
-__global__ void k_blend_seam_select(const float* __restrict__ blurred, const uint8_t* __restrict__ m1,
-                                    const uint8_t* __restrict__ m2, float* __restrict__ mask, long long n) {
-    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
-    if (m1[p] && m2[p]) mask[p] = blurred[p];
-}
-
-// gaussian_filter(sigma = 1) of a C-channel level followed by [::2, ::2]
-// (pysift/core.py:3475-3483): the axis-0 pass at even rows ...
-__global__ void k_gauss_rows_even(const float* __restrict__ in, float* __restrict__ out, int W, int H, int C,
-                                  const double* __restrict__ w9) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, yo = blockIdx.y;
-    if (x >= W * C) return;
-    const int y = 2 * yo;
-    const long long rs = (long long)W * C;
-    double s = w9[4] * (double)in[y * rs + x];
-#pragma unroll
-    for (int k = 4; k >= 1; --k) {
-        const double a = (double)in[refl_half(y - k, H) * rs + x];
-        const double b = (double)in[refl_half(y + k, H) * rs + x];
-        s = s + (a + b) * w9[4 - k];
-    }
-    out[yo * rs + x] = (float)s;
-}
-
-// ... then the axis-1 pass at even columns
-__global__ void k_gauss_cols_even(const float* __restrict__ in, float* __restrict__ out, int W, int Wo, int C,
-                                  const double* __restrict__ w9) {
+// ... then the column pass; the blurred value replaces the mask where both
+// images cover the canvas (pysift/core.py:3469-3471)
+__global__ void k_seam_cols(const float* __restrict__ rows, const uint8_t* __restrict__ m1,
+                            const uint8_t* __restrict__ m2, const int* __restrict__ seam, const BlendCtl* ctl,
+                            const float* __restrict__ k25, float* __restrict__ gm0, int W, int H) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    if (x >= Wo * C) return;
-    const int colo = x / C, c = x - colo * C;
-    const int col = 2 * colo;
-    const float* row = in + (long long)y * W * C + c;
-    double s = w9[4] * (double)row[(long long)col * C];
+    if (x >= W) return;
+    const long long p = (long long)y * W + x;
+    if (m1[p] && m2[p]) {
+        double s = 0.0;
+#pragma unroll 5
+        for (int t = 0; t < 25; ++t) s = s + (double)k25[t] * (double)rows[(long long)refl_101(y + t - 12, H) * W + x];
+        gm0[p] = (float)s;
+    } else {
+        gm0[p] = seam_value(m1, m2, seam, ctl, x, y, W);
+    }
+}
+
+// The Gaussian pyramids of I1, I2 and the seam mask (pysift/core.py:3520-3526):
+// gaussian_filter(sigma = 1) per channel followed by [::2, ::2]
+// (pysift/core.py:3475-3483), the three images in one pass.  Row pass at
+// even rows; level 0 reads I1 / I2 from the uint8 canvases.
+struct PyrLevel {
+    const float* g1;  // (h, w, 3)
+    const float* g2;
+    const float* gm;  // (h, w)
+};
+
+template <bool L0>
+__global__ void k_pyr_rows(const Level0 src, const PyrLevel in, int W, int H, float* __restrict__ t1,
+                           float* __restrict__ t2, float* __restrict__ tm, const double* __restrict__ w9) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, yo = blockIdx.y;
+    if (x >= W) return;
+    auto load = [&](int r, double v[7]) {
+        const long long p = (long long)r * W + x;
+        if (L0) {
+            float i1[3], i2[3];
+            src.px(p, i1, i2);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                v[c] = (double)i1[c];
+                v[3 + c] = (double)i2[c];
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                v[c] = (double)in.g1[p * 3 + c];
+                v[3 + c] = (double)in.g2[p * 3 + c];
+            }
+        }
+        v[6] = (double)in.gm[p];
+    };
+    const int y = 2 * yo;
+    double s[7], a[7], b[7];
+    load(y, a);
+#pragma unroll
+    for (int c = 0; c < 7; ++c) s[c] = w9[4] * a[c];
 #pragma unroll
     for (int k = 4; k >= 1; --k) {
-        const double a = (double)row[(long long)refl_half(col - k, W) * C];
-        const double b = (double)row[(long long)refl_half(col + k, W) * C];
-        s = s + (a + b) * w9[4 - k];
+        load(refl_half(y - k, H), a);
+        load(refl_half(y + k, H), b);
+        const double w = w9[4 - k];
+#pragma unroll
+        for (int c = 0; c < 7; ++c) s[c] = s[c] + (a[c] + b[c]) * w;
     }
-    out[(long long)y * Wo * C + x] = (float)s;
+    const long long o = (long long)yo * W + x;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        t1[o * 3 + c] = (float)s[c];
+        t2[o * 3 + c] = (float)s[3 + c];
+    }
+    tm[o] = (float)s[6];
+}
+
+// column pass at even columns: level k + 1 of the three pyramids
+__global__ void k_pyr_cols(const float* __restrict__ t1, const float* __restrict__ t2, const float* __restrict__ tm,
+                           int W, int Wo, const double* __restrict__ w9, float* __restrict__ g1,
+                           float* __restrict__ g2, float* __restrict__ gm) {
+    const int xo = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (xo >= Wo) return;
+    const int col = 2 * xo;
+    const long long row = (long long)y * W;
+    auto load = [&](int cc, double v[7]) {
+        const long long p = row + cc;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            v[c] = (double)t1[p * 3 + c];
+            v[3 + c] = (double)t2[p * 3 + c];
+        }
+        v[6] = (double)tm[p];
+    };
+    double s[7], a[7], b[7];
+    load(col, a);
+#pragma unroll
+    for (int c = 0; c < 7; ++c) s[c] = w9[4] * a[c];
+#pragma unroll
+    for (int k = 4; k >= 1; --k) {
+        load(refl_half(col - k, W), a);
+        load(refl_half(col + k, W), b);
+        const double w = w9[4 - k];
+#pragma unroll
+        for (int c = 0; c < 7; ++c) s[c] = s[c] + (a[c] + b[c]) * w;
+    }
+    const long long o = (long long)y * Wo + xo;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        g1[o * 3 + c] = (float)s[c];
+        g2[o * 3 + c] = (float)s[3 + c];
+    }
+    gm[o] = (float)s[6];
 }
 
 // zoom(order = 1) of an (h, w) level to (H, W) (pysift/core.py:3485-3493):
@@ -644,8 +723,8 @@ struct Zoom1 {
     }
 };
 
-// one blended Laplacian level: m * (G1 - up(G1')) + (1 - m) * (G2 - up(G2'))
-// (pysift/core.py:3535-3541); the coarsest level blends the Gaussians
+// one blended Laplacian level k >= 1: m * (G1 - up(G1')) + (1 - m) * (G2 - up(G2'))
+// (pysift/core.py:3529-3541); the coarsest level blends the Gaussians
 __global__ void k_blend_level(const float* __restrict__ g1, const float* __restrict__ g2,
                               const float* __restrict__ gm, const float* __restrict__ g1n,
                               const float* __restrict__ g2n, int H, int W, int hn, int wn,
@@ -680,27 +759,46 @@ __global__ void k_blend_reconstruct(const float* __restrict__ res, int hn, int w
     for (int c = 0; c < 3; ++c) out[p * 3 + c] = z.at(res, 3, c) + lb[p * 3 + c];
 }
 
-// the finest reconstruction step fused with the paste (pysift/core.py:3808-3809):
-// uint8 truncation of the clipped value where either image covers the canvas
-__global__ void k_blend_final(const float* __restrict__ res, int hn, int wn, const float* __restrict__ lb,
-                              const uint8_t* __restrict__ m1, const uint8_t* __restrict__ m2, int H, int W,
-                              uint8_t* __restrict__ pano, uint8_t* __restrict__ both, const BlendCtl* ctl,
+// Level 0 in one pass: its Laplacian blend, the last reconstruction step
+// (result = up(res) + lb0) and the paste (pysift/core.py:3806-3809): uint8
+// truncation of the clipped value where either image covers the canvas.
+// With one level there is no pyramid: result = m * I1 + (1 - m) * I2.
+__global__ void k_blend_final(const Level0 src, const float* __restrict__ gm0, const float* __restrict__ g1n,
+                              const float* __restrict__ g2n, const float* __restrict__ res, int hn, int wn, int H,
+                              int W, uint8_t* __restrict__ pano, uint8_t* __restrict__ both,
                               double* __restrict__ seam_rmse) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    if (x == 0 && y == 0 && seam_rmse)
-        *seam_rmse = ctl->n_ov ? sqrt((double)ctl->sq / (3.0 * (double)ctl->n_ov)) : __longlong_as_double(0x7ff8000000000000ll);
+    if (x == 0 && y == 0 && seam_rmse) {
+        const BlendCtl* ctl = src.ctl;
+        *seam_rmse = ctl->n_ov ? sqrt((double)ctl->sq / (3.0 * (double)ctl->n_ov))
+                               : __longlong_as_double(0x7ff8000000000000ll);
+    }
     if (x >= W) return;
     const long long p = (long long)y * W + x;
-    const bool any = m1[p] || m2[p];
+    const bool any = src.m1[p] || src.m2[p];
     if (both) both[p] = any;
-    const Zoom1* zp = nullptr;
-    Zoom1 z(hn > 0 ? hn : 1, wn > 0 ? wn : 1, H, W, y, x);
-    if (res) zp = &z;
+    float i1[3], i2[3];
+    src.px(p, i1, i2);
+    const float m = gm0[p];
+    const float mc = 1.0f - m;
+    float v[3];
+    if (res) {
+        const Zoom1 z(hn, wn, H, W, y, x);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const float l1 = i1[c] - z.at(g1n, 3, c);
+            const float l2 = i2[c] - z.at(g2n, 3, c);
+            const float lb = m * l1 + mc * l2;
+            v[c] = z.at(res, 3, c) + lb;
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) v[c] = m * i1[c] + mc * i2[c];
+    }
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        float v = zp ? zp->at(res, 3, c) + lb[p * 3 + c] : lb[p * 3 + c];
-        v = v < 0.0f ? 0.0f : (v > 255.0f ? 255.0f : v);
-        pano[p * 3 + c] = any ? (uint8_t)(int)v : (uint8_t)0;
+        const float t = v[c] < 0.0f ? 0.0f : (v[c] > 255.0f ? 255.0f : v[c]);
+        pano[p * 3 + c] = any ? (uint8_t)(int)t : (uint8_t)0;
     }
 }
 
@@ -727,14 +825,17 @@ static int seam_chunk(int L) {
 }
 
 struct BlendLayout {
-    size_t off_ctl, off_rowf, off_colf, off_rlo, off_rhi, off_clo, off_chi, off_win, off_color, off_avg, off_d1, off_d2, off_dpc, off_rowA, off_rowB, off_dir,
-        off_seam, off_ovl, off_jump, off_entry, off_blur, off_w9, off_k25, off_tmp;
+    size_t off_ctl, off_rowf, off_colf, off_rlo, off_rhi, off_clo, off_chi, off_win, off_color, off_avg, off_dpc,
+        off_rowA, off_rowB, off_dir, off_seam, off_ovl, off_jump, off_entry, off_srow, off_w9, off_k25, off_t1,
+        off_t2, off_tm;
     int R;
     size_t off_g1[8], off_g2[8], off_gm[8], off_lb[8], off_res[2];
     int h[8], w[8];
     size_t total;
 };
 
+// level k >= 1 holds G1, G2 (3 floats a pixel), the mask and the blended
+// Laplacian; level 0 keeps only the seam mask (I1 / I2 come from the canvases)
 static BlendLayout blend_layout(int cw, int ch, int levels) {
     BlendLayout l;
     size_t off = 0;
@@ -752,11 +853,9 @@ static BlendLayout blend_layout(int cw, int ch, int levels) {
     l.off_rhi = take((size_t)ch * 4);
     l.off_clo = take((size_t)cw * 4);
     l.off_chi = take((size_t)cw * 4);
-    l.off_win = take((size_t)(cw > ch ? cw : ch) * 8);
+    l.off_win = take((size_t)M * 16);
     l.off_color = take(N * 4);
     l.off_avg = take(N * 4);
-    l.off_d1 = take(N * 4);
-    l.off_d2 = take(N * 4);
     l.off_dpc = take(N * 4);
     l.off_rowA = take((size_t)(M + 2) * 8);
     l.off_rowB = take((size_t)(M + 2) * 8);
@@ -766,25 +865,30 @@ static BlendLayout blend_layout(int cw, int ch, int levels) {
     l.R = seam_chunk(M);
     l.off_jump = take((size_t)((M + l.R - 1) / l.R) * M * 4);
     l.off_entry = take((size_t)((M + l.R - 1) / l.R + 1) * 4);
-    l.off_blur = take(N * 4);
+    l.off_srow = take(N * 4);
     l.off_w9 = take(9 * 8);
     l.off_k25 = take(25 * 4);
+    const size_t half = (size_t)((ch + 1) / 2) * cw;
+    l.off_t1 = take(half * 12);
+    l.off_t2 = take(half * 12);
+    l.off_tm = take(half * 4);
     int h = ch, w = cw;
-    size_t tmp = 0;
     for (int k = 0; k < levels; ++k) {
         l.h[k] = h;
         l.w[k] = w;
-        l.off_g1[k] = take((size_t)h * w * 12);
-        l.off_g2[k] = take((size_t)h * w * 12);
-        l.off_gm[k] = take((size_t)h * w * 4);
-        l.off_lb[k] = take((size_t)h * w * 12);
-        tmp = std::max(tmp, (size_t)((h + 1) / 2) * w * 12);
+        const size_t n = (size_t)h * w;
+        l.off_gm[k] = take(n * 4);
+        if (k > 0) {
+            l.off_g1[k] = take(n * 12);
+            l.off_g2[k] = take(n * 12);
+            l.off_lb[k] = take(n * 12);
+        }
         h = (h + 1) / 2;
         w = (w + 1) / 2;
     }
-    l.off_tmp = take(tmp);
-    l.off_res[0] = take(N * 12);
-    l.off_res[1] = take(N * 12);
+    const size_t n1 = levels > 1 ? (size_t)l.h[1] * l.w[1] : 1;
+    l.off_res[0] = take(n1 * 12);
+    l.off_res[1] = take(n1 * 12);
     l.total = off;
     return l;
 }
@@ -792,13 +896,6 @@ static BlendLayout blend_layout(int cw, int ch, int levels) {
 template <typename T>
 static T* bwp(void* ws, size_t off) {
     return reinterpret_cast<T*>(static_cast<char*>(ws) + off);
-}
-
-static void blend_down(const float* in, int h, int w, int C, float* tmp, float* out, const double* w9,
-                       cudaStream_t st) {
-    const int ho = (h + 1) / 2, wo = (w + 1) / 2;
-    k_gauss_rows_even<<<dim3(ceil_div(w * C, 256), ho), 256, 0, st>>>(in, tmp, w, h, C, w9);
-    k_gauss_cols_even<<<dim3(ceil_div(wo * C, 256), ho), 256, 0, st>>>(tmp, out, w, wo, C, w9);
 }
 
 }  // namespace pysift
@@ -840,39 +937,35 @@ int pysift_blend_multiband(const uint8_t* warped1, const uint8_t* mask1, const u
     BlendCtl* ctl = bwp<BlendCtl>(ws, l.off_ctl);
     int* rowf = bwp<int>(ws, l.off_rowf);
     int* colf = bwp<int>(ws, l.off_colf);
+    int* rlo = bwp<int>(ws, l.off_rlo);
+    int* rhi = bwp<int>(ws, l.off_rhi);
+    int* clo = bwp<int>(ws, l.off_clo);
+    int* chi = bwp<int>(ws, l.off_chi);
     PYSIFT_CUDA_TRY(cudaMemsetAsync(ctl, 0, sizeof(BlendCtl), st));
     PYSIFT_CUDA_TRY(cudaMemsetAsync(rowf, 0, (size_t)ch * 4, st));
     PYSIFT_CUDA_TRY(cudaMemsetAsync(colf, 0, (size_t)cw * 4, st));
+    PYSIFT_CUDA_TRY(cudaMemsetAsync(clo, 0x7f, (size_t)cw * 4, st));
+    PYSIFT_CUDA_TRY(cudaMemsetAsync(chi, 0xff, (size_t)cw * 4, st));
     double* w9 = bwp<double>(ws, l.off_w9);
     float* k25 = bwp<float>(ws, l.off_k25);
     PYSIFT_CUDA_TRY(cudaMemcpyAsync(w9, gauss_w9, 9 * sizeof(double), cudaMemcpyHostToDevice, st));
     PYSIFT_CUDA_TRY(cudaMemcpyAsync(k25, seam_k25, 25 * sizeof(float), cudaMemcpyHostToDevice, st));
     const dim3 g2d(ceil_div(cw, 256), ch);
-    const long long N = (long long)cw * ch;
-    int* rlo = bwp<int>(ws, l.off_rlo);
-    int* rhi = bwp<int>(ws, l.off_rhi);
-    int* clo = bwp<int>(ws, l.off_clo);
-    int* chi = bwp<int>(ws, l.off_chi);
-    PYSIFT_CUDA_TRY(cudaMemsetAsync(clo, 0x7f, (size_t)cw * 4, st));
-    PYSIFT_CUDA_TRY(cudaMemsetAsync(chi, 0xff, (size_t)cw * 4, st));
+    // gain, overlap flags and ranges, seam orientation
     k_blend_stats<<<dim3(1, ch), 256, 0, st>>>(warped1, mask1, canvas2, mask2, cw, ctl, rowf, colf, rlo, rhi, clo,
                                                 chi);
     PYSIFT_LAUNCH_CHECK("k_blend_stats");
     k_blend_decide<<<1, 1024, 0, st>>>(ctl, rowf, colf, cw, ch);
     PYSIFT_LAUNCH_CHECK("k_blend_decide");
-    float* I1 = bwp<float>(ws, l.off_g1[0]);
-    float* I2 = bwp<float>(ws, l.off_g2[0]);
+    // seam cost
     float* color = bwp<float>(ws, l.off_color);
     float* avg = bwp<float>(ws, l.off_avg);
-    k_blend_prepare<<<g2d, 256, 0, st>>>(warped1, mask1, canvas2, mask2, cw, ctl, I1, I2, color, avg);
-    PYSIFT_LAUNCH_CHECK("k_blend_prepare");
-    float* d1 = bwp<float>(ws, l.off_d1);
-    float* d2 = bwp<float>(ws, l.off_d2);
     float* dpc = bwp<float>(ws, l.off_dpc);
-    k_sobel_deriv<<<g2d, 256, 0, st>>>(avg, d1, d2, cw, ch);
-    PYSIFT_LAUNCH_CHECK("k_sobel_deriv");
-    k_sobel_cost<<<g2d, 256, 0, st>>>(d1, d2, color, mask1, mask2, ctl, dpc, cw, ch);
+    k_blend_prepare<<<g2d, 256, 0, st>>>(warped1, mask1, canvas2, mask2, cw, ctl, color, avg);
+    PYSIFT_LAUNCH_CHECK("k_blend_prepare");
+    k_sobel_cost<<<g2d, 256, 0, st>>>(avg, color, mask1, mask2, ctl, dpc, cw, ch);
     PYSIFT_LAUNCH_CHECK("k_sobel_cost");
+    // DP seam and backtrack
     int* seam = bwp<int>(ws, l.off_seam);
     {
         int* ovl = bwp<int>(ws, l.off_ovl);
@@ -880,11 +973,11 @@ int pysift_blend_multiband(const uint8_t* warped1, const uint8_t* mask1, const u
         // the orientation is decided on the device: size shared memory for the longer side
         const int M = cw > ch ? cw : ch;
         const size_t flags = (((size_t)(M + 31) / 32) * 4 + 15) & ~(size_t)15;
-        const size_t wins = ((size_t)M * 8 + 15) & ~(size_t)15;
+        const size_t wins = (size_t)M * 16;
         const size_t lines = (size_t)(M + 2) * 16;
         double* gA = bwp<double>(ws, l.off_rowA);
         double* gB = bwp<double>(ws, l.off_rowB);
-        int2* gwin = bwp<int2>(ws, l.off_win);
+        int4* gwin = bwp<int4>(ws, l.off_win);
         PYSIFT_CUDA_TRY(cudaMemsetAsync(dir, 0, (size_t)cw * ch, st));
         const size_t base = flags + wins + lines;
         if (base + (size_t)M * 32 <= (size_t)DP_SMEM_MAX) {
@@ -914,23 +1007,38 @@ int pysift_blend_multiband(const uint8_t* warped1, const uint8_t* mask1, const u
         k_seam_walk<<<1, 1024, 0, st>>>(dir, ovl, ctl, cw, ch, R, jump, bwp<int>(ws, l.off_entry), seam);
         PYSIFT_LAUNCH_CHECK("k_seam_walk");
     }
+    // seam mask and its blur
     float* gm0 = bwp<float>(ws, l.off_gm[0]);
-    float* blur = bwp<float>(ws, l.off_blur);
-    k_blend_seam_mask<<<g2d, 256, 0, st>>>(mask1, mask2, seam, ctl, gm0, cw);
-    PYSIFT_LAUNCH_CHECK("k_blend_seam_mask");
-    k_blend_seam_blur<<<g2d, 256, 0, st>>>(gm0, d1, cw, ch, 1, k25);
-    k_blend_seam_blur<<<g2d, 256, 0, st>>>(d1, blur, cw, ch, 0, k25);
-    PYSIFT_LAUNCH_CHECK("k_blend_seam_blur");
-    k_blend_seam_select<<<(unsigned)ceil_div_ll(N, 256), 256, 0, st>>>(blur, mask1, mask2, gm0, N);
-    PYSIFT_LAUNCH_CHECK("k_blend_seam_select");
-    float* tmp = bwp<float>(ws, l.off_tmp);
+    float* srow = bwp<float>(ws, l.off_srow);
+    k_seam_rows<<<g2d, 256, 0, st>>>(mask1, mask2, seam, ctl, k25, srow, cw);
+    PYSIFT_LAUNCH_CHECK("k_seam_rows");
+    k_seam_cols<<<g2d, 256, 0, st>>>(srow, mask1, mask2, seam, ctl, k25, gm0, cw, ch);
+    PYSIFT_LAUNCH_CHECK("k_seam_cols");
+    // Gaussian pyramids of I1, I2 and the mask
+    Level0 src;
+    src.w1 = warped1;
+    src.m1 = mask1;
+    src.c2 = canvas2;
+    src.m2 = mask2;
+    src.ctl = ctl;
+    float* t1 = bwp<float>(ws, l.off_t1);
+    float* t2 = bwp<float>(ws, l.off_t2);
+    float* tm = bwp<float>(ws, l.off_tm);
     for (int k = 0; k + 1 < n_levels; ++k) {
-        blend_down(bwp<float>(ws, l.off_g1[k]), l.h[k], l.w[k], 3, tmp, bwp<float>(ws, l.off_g1[k + 1]), w9, st);
-        blend_down(bwp<float>(ws, l.off_g2[k]), l.h[k], l.w[k], 3, tmp, bwp<float>(ws, l.off_g2[k + 1]), w9, st);
-        blend_down(bwp<float>(ws, l.off_gm[k]), l.h[k], l.w[k], 1, tmp, bwp<float>(ws, l.off_gm[k + 1]), w9, st);
+        PyrLevel in;
+        in.g1 = k ? bwp<float>(ws, l.off_g1[k]) : nullptr;
+        in.g2 = k ? bwp<float>(ws, l.off_g2[k]) : nullptr;
+        in.gm = bwp<float>(ws, l.off_gm[k]);
+        const int ho = l.h[k + 1], wo = l.w[k + 1];
+        if (k == 0) k_pyr_rows<true><<<dim3(ceil_div(l.w[k], 128), ho), 128, 0, st>>>(src, in, l.w[k], l.h[k], t1, t2, tm, w9);
+        else k_pyr_rows<false><<<dim3(ceil_div(l.w[k], 128), ho), 128, 0, st>>>(src, in, l.w[k], l.h[k], t1, t2, tm, w9);
+        k_pyr_cols<<<dim3(ceil_div(wo, 128), ho), 128, 0, st>>>(t1, t2, tm, l.w[k], wo, w9, bwp<float>(ws, l.off_g1[k + 1]),
+                                                                bwp<float>(ws, l.off_g2[k + 1]),
+                                                                bwp<float>(ws, l.off_gm[k + 1]));
     }
-    PYSIFT_LAUNCH_CHECK("k_gauss_down");
-    for (int k = 0; k < n_levels; ++k) {
+    PYSIFT_LAUNCH_CHECK("k_pyr");
+    // blended Laplacian levels 1 .. n - 1 and the reconstruction down to level 1
+    for (int k = 1; k < n_levels; ++k) {
         const bool top = k + 1 == n_levels;
         k_blend_level<<<dim3(ceil_div(l.w[k], 256), l.h[k]), 256, 0, st>>>(
             bwp<float>(ws, l.off_g1[k]), bwp<float>(ws, l.off_g2[k]), bwp<float>(ws, l.off_gm[k]),
@@ -949,8 +1057,10 @@ int pysift_blend_multiband(const uint8_t* warped1, const uint8_t* mask1, const u
         rw = l.w[k];
     }
     PYSIFT_LAUNCH_CHECK("k_blend_reconstruct");
-    k_blend_final<<<g2d, 256, 0, st>>>(res, n_levels > 1 ? rh : 0, n_levels > 1 ? rw : 0, bwp<float>(ws, l.off_lb[0]),
-                                       mask1, mask2, ch, cw, pano, both, ctl, seam_rmse);
+    // level 0: Laplacian blend, last reconstruction step and paste
+    k_blend_final<<<g2d, 256, 0, st>>>(src, gm0, n_levels > 1 ? bwp<float>(ws, l.off_g1[1]) : nullptr,
+                                       n_levels > 1 ? bwp<float>(ws, l.off_g2[1]) : nullptr, res, rh, rw, ch, cw,
+                                       pano, both, seam_rmse);
     PYSIFT_LAUNCH_CHECK("k_blend_final");
     return PYSIFT_OK;
 }

@@ -102,10 +102,10 @@ def test_blend_levels(n_levels):
     assert np.array_equal(pano, ref)
 
 
-@pytest.mark.parametrize("cw", [5000, 9000, 13000])
+@pytest.mark.parametrize("cw", [4000, 5000, 9000, 13000])
 def test_blend_long_canvas(cw):
     """A vertical seam across wide canvases: the DP lines in shared memory with
-    an 8- or 4-deep cost ring, without the ring, and in global memory."""
+    a 4-deep cost ring or without one, and in global memory."""
     from oracle import blend_oracle as bo
     ch = 90
     rng = np.random.default_rng(cw)
