@@ -46,6 +46,7 @@ struct BlendCtl {
     int have_ov, vertical, first_side;  // first_side: image 1 left of (vertical) / above the seam
     int line0, line1;                   // first and last DP line holding overlap
     int n_lines, seam_end;              // overlap lines; seam position on the last one
+    int chunk;                          // backtrack chunk length
 };
 
 template <typename T>
@@ -451,15 +452,33 @@ __global__ void __launch_bounds__(1024) k_blend_dp(const float* __restrict__ dpc
             for (int j = max(o.x, w.y + 1) + tid; j <= o.y; j += nt) cur[j] = BL_INF;
         }
         uint8_t* drow = dir + (long long)w.z * M;
-        for (int j = w.x + tid; j <= w.y; j += nt) {
-            const float c = crow[j];
-            const double pl = prev[j - 1], pm = prev[j], pr = prev[j + 1];
-            int a = 0;
-            double best = pl;
-            if (pm < best) { best = pm; a = 1; }
-            if (pr < best) { best = pr; a = 2; }
-            cur[j] = c >= 0.0f ? (double)c + best : BL_INF;
-            if (a) drow[j] = (uint8_t)a;
+        // DP values are non-negative doubles (or INF), which order like their
+        // bit patterns as int64: the first minimum is taken on those
+        const long long* prevb = reinterpret_cast<const long long*>(prev);
+        constexpr int U = 4;
+        for (int j0 = w.x + tid; j0 <= w.y; j0 += U * nt) {
+            float c[U];
+            long long pl[U], pm[U], pr[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int j = j0 + u * nt;
+                const bool in = j <= w.y;
+                c[u] = in ? crow[j] : -1.0f;
+                pl[u] = in ? prevb[j - 1] : 0;
+                pm[u] = in ? prevb[j] : 0;
+                pr[u] = in ? prevb[j + 1] : 0;
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int j = j0 + u * nt;
+                if (j > w.y) break;
+                int a = 0;
+                long long best = pl[u];
+                if (pm[u] < best) { best = pm[u]; a = 1; }
+                if (pr[u] < best) { best = pr[u]; a = 2; }
+                cur[j] = c[u] >= 0.0f ? (double)c[u] + __longlong_as_double(best) : BL_INF;
+                if (a) drow[j] = (uint8_t)a;
+            }
         }
         __syncthreads();
         double* t = prev;
@@ -491,6 +510,9 @@ __global__ void __launch_bounds__(1024) k_blend_dp(const float* __restrict__ dpc
             if (s_best[w] < bv || (s_best[w] == bv && s_idx[w] < bj)) { bv = s_best[w]; bj = s_idx[w]; }
         ctl->seam_end = bj;
         ctl->n_lines = nL;
+        int R = 16;
+        while (2 * R * R < nL) R *= 2;
+        ctl->chunk = R;
     }
 }
 
@@ -505,8 +527,9 @@ __device__ __forceinline__ int bt_step(const uint8_t* __restrict__ dir, const in
 // c below the last and every position j on overlap line (c + 1) R, the
 // position the seam reaches on overlap line c R.
 __global__ void k_seam_jump(const uint8_t* __restrict__ dir, const int* __restrict__ ovl, const BlendCtl* ctl,
-                            int cw, int ch, int R, int* __restrict__ jump) {
+                            int cw, int ch, int* __restrict__ jump) {
     if (!ctl->have_ov) return;
+    const int R = ctl->chunk;
     const int M = ctl->vertical ? cw : ch;
     const int C = (ctl->n_lines + R - 1) / R;
     const int c = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -520,10 +543,11 @@ __global__ void k_seam_jump(const uint8_t* __restrict__ dir, const int* __restri
 // the lines of every chunk in parallel; lines without overlap keep the end
 // position (pysift/core.py:3326-3334).
 __global__ void __launch_bounds__(1024) k_seam_walk(const uint8_t* __restrict__ dir, const int* __restrict__ ovl,
-                                                    const BlendCtl* ctl, int cw, int ch, int R,
+                                                    const BlendCtl* ctl, int cw, int ch,
                                                     const int* __restrict__ jump, int* __restrict__ entry,
                                                     int* __restrict__ seam) {
     if (!ctl->have_ov) return;
+    const int R = ctl->chunk;
     const bool vert = ctl->vertical != 0;
     const int L = vert ? ch : cw, M = vert ? cw : ch;
     const int nL = ctl->n_lines, sc = ctl->seam_end;
@@ -563,15 +587,19 @@ __device__ __forceinline__ float seam_value(const uint8_t* __restrict__ m1, cons
 
 // seam-mask blur (sigma 3, 25 taps, reflect-101, float64 sums in tap order):
 // the row pass over the mask values ...
-__global__ void k_seam_rows(const uint8_t* __restrict__ m1, const uint8_t* __restrict__ m2,
-                            const int* __restrict__ seam, const BlendCtl* ctl, const float* __restrict__ k25,
-                            float* __restrict__ out, int W) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+__global__ void __launch_bounds__(256) k_seam_rows(const uint8_t* __restrict__ m1, const uint8_t* __restrict__ m2,
+                                                   const int* __restrict__ seam, const BlendCtl* ctl,
+                                                   const float* __restrict__ k25, float* __restrict__ out, int W) {
+    __shared__ float sv[256 + 24];
+    const int y = blockIdx.y, x0 = blockIdx.x * 256;
+    for (int i = threadIdx.x; i < 256 + 24; i += 256)
+        sv[i] = seam_value(m1, m2, seam, ctl, refl_101(x0 + i - 12, W), y, W);
+    __syncthreads();
+    const int x = x0 + threadIdx.x;
     if (x >= W) return;
     double s = 0.0;
-#pragma unroll 5
-    for (int t = 0; t < 25; ++t)
-        s = s + (double)k25[t] * (double)seam_value(m1, m2, seam, ctl, refl_101(x + t - 12, W), y, W);
+#pragma unroll
+    for (int t = 0; t < 25; ++t) s = s + (double)k25[t] * (double)sv[threadIdx.x + t];
     out[(long long)y * W + x] = (float)s;
 }
 
@@ -595,107 +623,129 @@ __global__ void k_seam_cols(const float* __restrict__ rows, const uint8_t* __res
 
 // The Gaussian pyramids of I1, I2 and the seam mask (pysift/core.py:3520-3526):
 // gaussian_filter(sigma = 1) per channel followed by [::2, ::2]
-// (pysift/core.py:3475-3483), the three images in one pass.  Row pass at
-// even rows; level 0 reads I1 / I2 from the uint8 canvases.
+// (pysift/core.py:3475-3483).  Two channel groups: the images (I1 and I2,
+// six channels; level 0 recomputed from the uint8 canvases) and the mask,
+// so the image pyramids can run while the seam is being found.  Row pass at
+// even rows, then the column pass at even columns.
 struct PyrLevel {
     const float* g1;  // (h, w, 3)
     const float* g2;
     const float* gm;  // (h, w)
 };
 
-template <bool L0>
-__global__ void k_pyr_rows(const Level0 src, const PyrLevel in, int W, int H, float* __restrict__ t1,
-                           float* __restrict__ t2, float* __restrict__ tm, const double* __restrict__ w9) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, yo = blockIdx.y;
-    if (x >= W) return;
-    auto load = [&](int r, double v[7]) {
-        const long long p = (long long)r * W + x;
-        if (L0) {
-            float i1[3], i2[3];
-            src.px(p, i1, i2);
+template <int NC, bool L0>
+__device__ __forceinline__ void pyr_load(const Level0& src, const PyrLevel& in, long long p, double v[NC]) {
+    if (NC == 1) {
+        v[0] = (double)in.gm[p];
+    } else if (L0) {
+        float i1[3], i2[3];
+        src.px(p, i1, i2);
 #pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                v[c] = (double)i1[c];
-                v[3 + c] = (double)i2[c];
-            }
-        } else {
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                v[c] = (double)in.g1[p * 3 + c];
-                v[3 + c] = (double)in.g2[p * 3 + c];
-            }
+        for (int c = 0; c < 3; ++c) {
+            v[c] = (double)i1[c];
+            v[3 + c] = (double)i2[c];
         }
-        v[6] = (double)in.gm[p];
-    };
-    const int y = 2 * yo;
-    double s[7], a[7], b[7];
-    load(y, a);
+    } else {
 #pragma unroll
-    for (int c = 0; c < 7; ++c) s[c] = w9[4] * a[c];
-#pragma unroll
-    for (int k = 4; k >= 1; --k) {
-        load(refl_half(y - k, H), a);
-        load(refl_half(y + k, H), b);
-        const double w = w9[4 - k];
-#pragma unroll
-        for (int c = 0; c < 7; ++c) s[c] = s[c] + (a[c] + b[c]) * w;
+        for (int c = 0; c < 3; ++c) {
+            v[c] = (double)in.g1[p * 3 + c];
+            v[3 + c] = (double)in.g2[p * 3 + c];
+        }
     }
-    const long long o = (long long)yo * W + x;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        t1[o * 3 + c] = (float)s[c];
-        t2[o * 3 + c] = (float)s[3 + c];
-    }
-    tm[o] = (float)s[6];
 }
 
-// column pass at even columns: level k + 1 of the three pyramids
-__global__ void k_pyr_cols(const float* __restrict__ t1, const float* __restrict__ t2, const float* __restrict__ tm,
-                           int W, int Wo, const double* __restrict__ w9, float* __restrict__ g1,
-                           float* __restrict__ g2, float* __restrict__ gm) {
+// NC = 6: t1 / t2 get I1 / I2 (3 floats a pixel); NC = 1: t1 gets the mask
+template <int NC, bool L0>
+__global__ void k_pyr_rows(const Level0 src, const PyrLevel in, int W, int H, float* __restrict__ t1,
+                           float* __restrict__ t2, const double* __restrict__ w9) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, yo = blockIdx.y;
+    if (x >= W) return;
+    const int y = 2 * yo;
+    double s[NC], a[NC], b[NC];
+    pyr_load<NC, L0>(src, in, (long long)y * W + x, a);
+#pragma unroll
+    for (int c = 0; c < NC; ++c) s[c] = w9[4] * a[c];
+#pragma unroll
+    for (int k = 4; k >= 1; --k) {
+        pyr_load<NC, L0>(src, in, (long long)refl_half(y - k, H) * W + x, a);
+        pyr_load<NC, L0>(src, in, (long long)refl_half(y + k, H) * W + x, b);
+        const double w = w9[4 - k];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) s[c] = s[c] + (a[c] + b[c]) * w;
+    }
+    const long long o = (long long)yo * W + x;
+    if (NC == 1) {
+        t1[o] = (float)s[0];
+    } else {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            t1[o * 3 + c] = (float)s[c];
+            t2[o * 3 + c] = (float)s[(3 + c) % NC];
+        }
+    }
+}
+
+template <int NC>
+__global__ void k_pyr_cols(const float* __restrict__ t1, const float* __restrict__ t2, int W, int Wo,
+                           const double* __restrict__ w9, float* __restrict__ g1, float* __restrict__ g2) {
     const int xo = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (xo >= Wo) return;
     const int col = 2 * xo;
     const long long row = (long long)y * W;
-    auto load = [&](int cc, double v[7]) {
+    auto load = [&](int cc, double v[NC]) {
         const long long p = row + cc;
+        if (NC == 1) {
+            v[0] = (double)t1[p];
+        } else {
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            v[c] = (double)t1[p * 3 + c];
-            v[3 + c] = (double)t2[p * 3 + c];
+            for (int c = 0; c < 3; ++c) {
+                v[c] = (double)t1[p * 3 + c];
+                v[(3 + c) % NC] = (double)t2[p * 3 + c];
+            }
         }
-        v[6] = (double)tm[p];
     };
-    double s[7], a[7], b[7];
+    double s[NC], a[NC], b[NC];
     load(col, a);
 #pragma unroll
-    for (int c = 0; c < 7; ++c) s[c] = w9[4] * a[c];
+    for (int c = 0; c < NC; ++c) s[c] = w9[4] * a[c];
 #pragma unroll
     for (int k = 4; k >= 1; --k) {
         load(refl_half(col - k, W), a);
         load(refl_half(col + k, W), b);
         const double w = w9[4 - k];
 #pragma unroll
-        for (int c = 0; c < 7; ++c) s[c] = s[c] + (a[c] + b[c]) * w;
+        for (int c = 0; c < NC; ++c) s[c] = s[c] + (a[c] + b[c]) * w;
     }
     const long long o = (long long)y * Wo + xo;
+    if (NC == 1) {
+        g1[o] = (float)s[0];
+    } else {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        g1[o * 3 + c] = (float)s[c];
-        g2[o * 3 + c] = (float)s[3 + c];
+        for (int c = 0; c < 3; ++c) {
+            g1[o * 3 + c] = (float)s[c];
+            g2[o * 3 + c] = (float)s[(3 + c) % NC];
+        }
     }
-    gm[o] = (float)s[6];
 }
 
 // zoom(order = 1) of an (h, w) level to (H, W) (pysift/core.py:3485-3493):
 // coordinate k * (in - 1) / (out - 1), corners reflected (mirror) at the edge
+struct ZoomF {
+    double zy, zx;  // (in - 1) / (out - 1) per axis, 1 when out == 1
+};
+
+static ZoomF zoom_factors(int h, int w, int H, int W) {
+    ZoomF z;
+    z.zy = H > 1 ? (double)(h - 1) / (double)(H - 1) : 1.0;
+    z.zx = W > 1 ? (double)(w - 1) / (double)(W - 1) : 1.0;
+    return z;
+}
+
 struct Zoom1 {
     long long o[4];
     double wy[2], wx[2];
-    __device__ Zoom1(int h, int w, int H, int W, int y, int x) {
-        const double zy = H > 1 ? (double)(h - 1) / (double)(H - 1) : 1.0;
-        const double zx = W > 1 ? (double)(w - 1) / (double)(W - 1) : 1.0;
-        const double cy = (double)y * zy, cx = (double)x * zx;
+    __device__ Zoom1(int h, int w, ZoomF f, int y, int x) {
+        const double cy = (double)y * f.zy, cx = (double)x * f.zx;
         const int y0 = (int)floor(cy), x0 = (int)floor(cx);
         const double ty = cy - (double)y0, tx = cx - (double)x0;
         wy[0] = 1.0 - ty;
@@ -727,7 +777,7 @@ struct Zoom1 {
 // (pysift/core.py:3529-3541); the coarsest level blends the Gaussians
 __global__ void k_blend_level(const float* __restrict__ g1, const float* __restrict__ g2,
                               const float* __restrict__ gm, const float* __restrict__ g1n,
-                              const float* __restrict__ g2n, int H, int W, int hn, int wn,
+                              const float* __restrict__ g2n, int H, int W, int hn, int wn, ZoomF zf,
                               float* __restrict__ out) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x >= W) return;
@@ -735,7 +785,7 @@ __global__ void k_blend_level(const float* __restrict__ g1, const float* __restr
     const float m = gm[p];
     const float mc = 1.0f - m;
     if (g1n) {
-        const Zoom1 z(hn, wn, H, W, y, x);
+        const Zoom1 z(hn, wn, zf, y, x);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             const float l1 = g1[p * 3 + c] - z.at(g1n, 3, c);
@@ -750,11 +800,11 @@ __global__ void k_blend_level(const float* __restrict__ g1, const float* __restr
 
 // reconstruction step (pysift/core.py:3544-3547): out = up(res) + lb
 __global__ void k_blend_reconstruct(const float* __restrict__ res, int hn, int wn, const float* __restrict__ lb,
-                                    int H, int W, float* __restrict__ out) {
+                                    int H, int W, ZoomF zf, float* __restrict__ out) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x >= W) return;
     const long long p = (long long)y * W + x;
-    const Zoom1 z(hn, wn, H, W, y, x);
+    const Zoom1 z(hn, wn, zf, y, x);
 #pragma unroll
     for (int c = 0; c < 3; ++c) out[p * 3 + c] = z.at(res, 3, c) + lb[p * 3 + c];
 }
@@ -765,7 +815,7 @@ __global__ void k_blend_reconstruct(const float* __restrict__ res, int hn, int w
 // With one level there is no pyramid: result = m * I1 + (1 - m) * I2.
 __global__ void k_blend_final(const Level0 src, const float* __restrict__ gm0, const float* __restrict__ g1n,
                               const float* __restrict__ g2n, const float* __restrict__ res, int hn, int wn, int H,
-                              int W, uint8_t* __restrict__ pano, uint8_t* __restrict__ both,
+                              int W, ZoomF zf, uint8_t* __restrict__ pano, uint8_t* __restrict__ both,
                               double* __restrict__ seam_rmse) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x == 0 && y == 0 && seam_rmse) {
@@ -783,7 +833,7 @@ __global__ void k_blend_final(const Level0 src, const float* __restrict__ gm0, c
     const float mc = 1.0f - m;
     float v[3];
     if (res) {
-        const Zoom1 z(hn, wn, H, W, y, x);
+        const Zoom1 z(hn, wn, zf, y, x);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             const float l1 = i1[c] - z.at(g1n, 3, c);
@@ -816,19 +866,40 @@ __global__ void k_place_image(const uint8_t* __restrict__ img, int h, int w, int
 }
 
 constexpr int DP_SMEM_MAX = 200 * 1024;
+constexpr int DP_THREADS = 256;
 
-// backtrack chunk length: about the square root of the line count, at least 16
-static int seam_chunk(int L) {
-    int R = 16;
-    while ((long long)R * R < L) R *= 2;
-    return R;
+// backtrack chunks: the chunk length R (a power of two, at least 16, with
+// 2 R^2 >= the number of overlap lines, which balances the sequential walk of
+// about 2 R + lines / R steps) is chosen on the device, so there are at most
+// ceil(sqrt(2 M)) + 1 chunks for lines of M positions
+static int max_seam_chunks(int M) {
+    int c = 1;
+    while ((long long)c * c < 2LL * M) ++c;
+    return c + 1;
+}
+
+// another stream on the current device for work that can overlap the seam
+// search; one per host thread and device, created on first use
+static cudaStream_t side_stream() {
+    constexpr int MAXDEV = 64;
+    thread_local cudaStream_t streams[MAXDEV] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAXDEV) {
+        set_error("side_stream: no current device");
+        return nullptr;
+    }
+    if (!streams[dev] && cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking) != cudaSuccess) {
+        set_error("side_stream: cudaStreamCreateWithFlags failed");
+        streams[dev] = nullptr;
+    }
+    return streams[dev];
 }
 
 struct BlendLayout {
     size_t off_ctl, off_rowf, off_colf, off_rlo, off_rhi, off_clo, off_chi, off_win, off_color, off_avg, off_dpc,
         off_rowA, off_rowB, off_dir, off_seam, off_ovl, off_jump, off_entry, off_srow, off_w9, off_k25, off_t1,
         off_t2, off_tm;
-    int R;
+    int nchunk;
     size_t off_g1[8], off_g2[8], off_gm[8], off_lb[8], off_res[2];
     int h[8], w[8];
     size_t total;
@@ -862,9 +933,9 @@ static BlendLayout blend_layout(int cw, int ch, int levels) {
     l.off_dir = take(N);
     l.off_seam = take((size_t)M * 4);
     l.off_ovl = take((size_t)M * 4);
-    l.R = seam_chunk(M);
-    l.off_jump = take((size_t)((M + l.R - 1) / l.R) * M * 4);
-    l.off_entry = take((size_t)((M + l.R - 1) / l.R + 1) * 4);
+    l.nchunk = max_seam_chunks(M);
+    l.off_jump = take((size_t)l.nchunk * M * 4);
+    l.off_entry = take((size_t)(l.nchunk + 1) * 4);
     l.off_srow = take(N * 4);
     l.off_w9 = take(9 * 8);
     l.off_k25 = take(25 * 4);
@@ -957,6 +1028,38 @@ int pysift_blend_multiband(const uint8_t* warped1, const uint8_t* mask1, const u
     PYSIFT_LAUNCH_CHECK("k_blend_stats");
     k_blend_decide<<<1, 1024, 0, st>>>(ctl, rowf, colf, cw, ch);
     PYSIFT_LAUNCH_CHECK("k_blend_decide");
+    // Gaussian pyramids of I1 and I2 on a side stream: they need only the gain
+    Level0 src;
+    src.w1 = warped1;
+    src.m1 = mask1;
+    src.c2 = canvas2;
+    src.m2 = mask2;
+    src.ctl = ctl;
+    cudaStream_t side = side_stream();
+    if (!side) return PYSIFT_ERR_CUDA;
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+    PYSIFT_CUDA_TRY(cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming));
+    PYSIFT_CUDA_TRY(cudaEventCreateWithFlags(&join_ev, cudaEventDisableTiming));
+    PYSIFT_CUDA_TRY(cudaEventRecord(fork_ev, st));
+    PYSIFT_CUDA_TRY(cudaStreamWaitEvent(side, fork_ev, 0));
+    {
+        float* t1 = bwp<float>(ws, l.off_t1);
+        float* t2 = bwp<float>(ws, l.off_t2);
+        for (int k = 0; k + 1 < n_levels; ++k) {
+            PyrLevel in;
+            in.g1 = k ? bwp<float>(ws, l.off_g1[k]) : nullptr;
+            in.g2 = k ? bwp<float>(ws, l.off_g2[k]) : nullptr;
+            in.gm = nullptr;
+            const int ho = l.h[k + 1], wo = l.w[k + 1];
+            const dim3 gr(ceil_div(l.w[k], 128), ho), gc(ceil_div(wo, 128), ho);
+            if (k == 0) k_pyr_rows<6, true><<<gr, 128, 0, side>>>(src, in, l.w[k], l.h[k], t1, t2, w9);
+            else k_pyr_rows<6, false><<<gr, 128, 0, side>>>(src, in, l.w[k], l.h[k], t1, t2, w9);
+            k_pyr_cols<6><<<gc, 128, 0, side>>>(t1, t2, l.w[k], wo, w9, bwp<float>(ws, l.off_g1[k + 1]),
+                                                bwp<float>(ws, l.off_g2[k + 1]));
+        }
+        PYSIFT_LAUNCH_CHECK("k_pyr images");
+    }
+    PYSIFT_CUDA_TRY(cudaEventRecord(join_ev, side));
     // seam cost
     float* color = bwp<float>(ws, l.off_color);
     float* avg = bwp<float>(ws, l.off_avg);
@@ -983,28 +1086,27 @@ int pysift_blend_multiband(const uint8_t* warped1, const uint8_t* mask1, const u
         if (base + (size_t)M * 32 <= (size_t)DP_SMEM_MAX) {
             const size_t sm = base + (size_t)M * 32;
             PYSIFT_CUDA_TRY(cudaFuncSetAttribute(k_blend_dp<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-            k_blend_dp<8><<<1, 1024, sm, st>>>(dpc, rowf, colf, rlo, rhi, clo, chi, cw, ch, ctl, gA, gB, gwin, 0, dir,
+            k_blend_dp<8><<<1, DP_THREADS, sm, st>>>(dpc, rowf, colf, rlo, rhi, clo, chi, cw, ch, ctl, gA, gB, gwin, 0, dir,
                                                ovl);
         } else if (base + (size_t)M * 16 <= (size_t)DP_SMEM_MAX) {
             const size_t sm = base + (size_t)M * 16;
             PYSIFT_CUDA_TRY(cudaFuncSetAttribute(k_blend_dp<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-            k_blend_dp<4><<<1, 1024, sm, st>>>(dpc, rowf, colf, rlo, rhi, clo, chi, cw, ch, ctl, gA, gB, gwin, 0, dir,
+            k_blend_dp<4><<<1, DP_THREADS, sm, st>>>(dpc, rowf, colf, rlo, rhi, clo, chi, cw, ch, ctl, gA, gB, gwin, 0, dir,
                                                ovl);
         } else if (base <= (size_t)DP_SMEM_MAX) {
             PYSIFT_CUDA_TRY(cudaFuncSetAttribute(k_blend_dp<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)base));
-            k_blend_dp<0><<<1, 1024, base, st>>>(dpc, rowf, colf, rlo, rhi, clo, chi, cw, ch, ctl, gA, gB, gwin, 0, dir,
+            k_blend_dp<0><<<1, DP_THREADS, base, st>>>(dpc, rowf, colf, rlo, rhi, clo, chi, cw, ch, ctl, gA, gB, gwin, 0, dir,
                                                  ovl);
         } else {
             PYSIFT_CUDA_TRY(cudaFuncSetAttribute(k_blend_dp<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)flags));
-            k_blend_dp<0><<<1, 1024, flags, st>>>(dpc, rowf, colf, rlo, rhi, clo, chi, cw, ch, ctl, gA, gB, gwin, 1,
+            k_blend_dp<0><<<1, DP_THREADS, flags, st>>>(dpc, rowf, colf, rlo, rhi, clo, chi, cw, ch, ctl, gA, gB, gwin, 1,
                                                   dir, ovl);
         }
         PYSIFT_LAUNCH_CHECK("k_blend_dp");
-        const int R = l.R;
         int* jump = bwp<int>(ws, l.off_jump);
-        k_seam_jump<<<dim3(ceil_div(M, 256), (M + R - 1) / R), 256, 0, st>>>(dir, ovl, ctl, cw, ch, R, jump);
+        k_seam_jump<<<dim3(ceil_div(M, 256), l.nchunk), 256, 0, st>>>(dir, ovl, ctl, cw, ch, jump);
         PYSIFT_LAUNCH_CHECK("k_seam_jump");
-        k_seam_walk<<<1, 1024, 0, st>>>(dir, ovl, ctl, cw, ch, R, jump, bwp<int>(ws, l.off_entry), seam);
+        k_seam_walk<<<1, 1024, 0, st>>>(dir, ovl, ctl, cw, ch, jump, bwp<int>(ws, l.off_entry), seam);
         PYSIFT_LAUNCH_CHECK("k_seam_walk");
     }
     // seam mask and its blur
@@ -1014,44 +1116,41 @@ int pysift_blend_multiband(const uint8_t* warped1, const uint8_t* mask1, const u
     PYSIFT_LAUNCH_CHECK("k_seam_rows");
     k_seam_cols<<<g2d, 256, 0, st>>>(srow, mask1, mask2, seam, ctl, k25, gm0, cw, ch);
     PYSIFT_LAUNCH_CHECK("k_seam_cols");
-    // Gaussian pyramids of I1, I2 and the mask
-    Level0 src;
-    src.w1 = warped1;
-    src.m1 = mask1;
-    src.c2 = canvas2;
-    src.m2 = mask2;
-    src.ctl = ctl;
-    float* t1 = bwp<float>(ws, l.off_t1);
-    float* t2 = bwp<float>(ws, l.off_t2);
-    float* tm = bwp<float>(ws, l.off_tm);
-    for (int k = 0; k + 1 < n_levels; ++k) {
-        PyrLevel in;
-        in.g1 = k ? bwp<float>(ws, l.off_g1[k]) : nullptr;
-        in.g2 = k ? bwp<float>(ws, l.off_g2[k]) : nullptr;
-        in.gm = bwp<float>(ws, l.off_gm[k]);
-        const int ho = l.h[k + 1], wo = l.w[k + 1];
-        if (k == 0) k_pyr_rows<true><<<dim3(ceil_div(l.w[k], 128), ho), 128, 0, st>>>(src, in, l.w[k], l.h[k], t1, t2, tm, w9);
-        else k_pyr_rows<false><<<dim3(ceil_div(l.w[k], 128), ho), 128, 0, st>>>(src, in, l.w[k], l.h[k], t1, t2, tm, w9);
-        k_pyr_cols<<<dim3(ceil_div(wo, 128), ho), 128, 0, st>>>(t1, t2, tm, l.w[k], wo, w9, bwp<float>(ws, l.off_g1[k + 1]),
-                                                                bwp<float>(ws, l.off_g2[k + 1]),
-                                                                bwp<float>(ws, l.off_gm[k + 1]));
+    // Gaussian pyramid of the seam mask, then join the image pyramids
+    {
+        float* tm = bwp<float>(ws, l.off_tm);
+        for (int k = 0; k + 1 < n_levels; ++k) {
+            PyrLevel in;
+            in.g1 = nullptr;
+            in.g2 = nullptr;
+            in.gm = bwp<float>(ws, l.off_gm[k]);
+            const int ho = l.h[k + 1], wo = l.w[k + 1];
+            k_pyr_rows<1, false><<<dim3(ceil_div(l.w[k], 128), ho), 128, 0, st>>>(src, in, l.w[k], l.h[k], tm, nullptr,
+                                                                                  w9);
+            k_pyr_cols<1><<<dim3(ceil_div(wo, 128), ho), 128, 0, st>>>(tm, nullptr, l.w[k], wo, w9,
+                                                                       bwp<float>(ws, l.off_gm[k + 1]), nullptr);
+        }
+        PYSIFT_LAUNCH_CHECK("k_pyr mask");
     }
-    PYSIFT_LAUNCH_CHECK("k_pyr");
+    PYSIFT_CUDA_TRY(cudaStreamWaitEvent(st, join_ev, 0));
+    cudaEventDestroy(fork_ev);
+    cudaEventDestroy(join_ev);
     // blended Laplacian levels 1 .. n - 1 and the reconstruction down to level 1
     for (int k = 1; k < n_levels; ++k) {
         const bool top = k + 1 == n_levels;
         k_blend_level<<<dim3(ceil_div(l.w[k], 256), l.h[k]), 256, 0, st>>>(
             bwp<float>(ws, l.off_g1[k]), bwp<float>(ws, l.off_g2[k]), bwp<float>(ws, l.off_gm[k]),
             top ? nullptr : bwp<float>(ws, l.off_g1[k + 1]), top ? nullptr : bwp<float>(ws, l.off_g2[k + 1]), l.h[k],
-            l.w[k], top ? 0 : l.h[k + 1], top ? 0 : l.w[k + 1], bwp<float>(ws, l.off_lb[k]));
+            l.w[k], top ? 0 : l.h[k + 1], top ? 0 : l.w[k + 1],
+            top ? ZoomF{1.0, 1.0} : zoom_factors(l.h[k + 1], l.w[k + 1], l.h[k], l.w[k]), bwp<float>(ws, l.off_lb[k]));
     }
     PYSIFT_LAUNCH_CHECK("k_blend_level");
     const float* res = n_levels > 1 ? bwp<float>(ws, l.off_lb[n_levels - 1]) : nullptr;
     int rh = l.h[n_levels - 1], rw = l.w[n_levels - 1];
     for (int k = n_levels - 2; k >= 1; --k) {
         float* out = bwp<float>(ws, l.off_res[k & 1]);
-        k_blend_reconstruct<<<dim3(ceil_div(l.w[k], 256), l.h[k]), 256, 0, st>>>(res, rh, rw, bwp<float>(ws, l.off_lb[k]),
-                                                                                l.h[k], l.w[k], out);
+        k_blend_reconstruct<<<dim3(ceil_div(l.w[k], 256), l.h[k]), 256, 0, st>>>(
+            res, rh, rw, bwp<float>(ws, l.off_lb[k]), l.h[k], l.w[k], zoom_factors(rh, rw, l.h[k], l.w[k]), out);
         res = out;
         rh = l.h[k];
         rw = l.w[k];
@@ -1060,7 +1159,7 @@ int pysift_blend_multiband(const uint8_t* warped1, const uint8_t* mask1, const u
     // level 0: Laplacian blend, last reconstruction step and paste
     k_blend_final<<<g2d, 256, 0, st>>>(src, gm0, n_levels > 1 ? bwp<float>(ws, l.off_g1[1]) : nullptr,
                                        n_levels > 1 ? bwp<float>(ws, l.off_g2[1]) : nullptr, res, rh, rw, ch, cw,
-                                       pano, both, seam_rmse);
+                                       zoom_factors(rh, rw, ch, cw), pano, both, seam_rmse);
     PYSIFT_LAUNCH_CHECK("k_blend_final");
     return PYSIFT_OK;
 }
