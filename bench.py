@@ -9,7 +9,8 @@ stand in for the reference's datasets; see pysift_b200/synthetic.py):
 
   stitch_pair_1280x960  GPUPyStitch().stitch(img1, img2) on a seeded synthetic
                     pair of 1280x960 BGR views (ratio 0.75, 2048 hypotheses,
-                    4 px, linear feather blend) -- the default
+                    4 px, the reference's gain + DP seam + 6-level multiband
+                    composition) -- the default
   detect_1280x960   detectAndCompute on one 1280x960 grayscale scene
   detect_640x480    detectAndCompute on one 640x480 scene
   match_u8_8192     exact ratio-test matching of two 8192 x 128 uint8-valued
@@ -737,9 +738,11 @@ def run_reference_stitch(args, wl):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": args.workload, "H": wl["H"], "W": wl["W"], "seed": wl["seed"],
-                   "ransac_iters": wl["ransac_iters"], "inlier_thresh": wl["inlier_thresh"]},
+                   "ransac_iters": wl["ransac_iters"], "inlier_thresh": wl["inlier_thresh"], "match_ratio": 0.75,
+                   "blend": "multiband (gain, DP seam, 6 levels)"},
         "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": os.cpu_count(), "kind": "port",
-                         "sample": "one full two-image stitch per step (oracle port, OpenMP over the host cores)"},
+                         "sample": "one full two-image stitch per step (oracle port: C/OpenMP detection and "
+                                   "RANSAC, numpy/scipy composition)"},
         "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -965,7 +968,9 @@ def run_stitch(args, wl, world, rank, local):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": args.workload, "H": H, "W": W, "seed": wl["seed"],
                    "ransac_iters": wl["ransac_iters"], "inlier_thresh": wl["inlier_thresh"], "match_ratio": 0.75,
-                   "blend": "linear feather", "keypoints": [m["kp1"], m["kp2"]], "matches": m["matches"],
+                   "blend": "multiband (gain, DP seam, %d levels)" % st.n_blend_levels
+                   if st.blend == "multiband" else "linear feather",
+                   "keypoints": [m["kp1"], m["kp2"]], "matches": m["matches"],
                    "inliers": m["inliers"], "canvas": [m["canvas_w"], m["canvas_h"]],
                    "l2": "flushed (256 MiB write) before every step", "parallelism": f"replicas{world}"},
         "mpix_per_s": pairs_s * mpix,
@@ -978,7 +983,7 @@ def run_stitch(args, wl, world, rank, local):
                          "cores": os.cpu_count(), "kind": "port",
                          "sample": f"{cpu_n} full stitches of the same pair by the oracle port (OpenMP)"},
         "e2e": {"value": e2e_pairs_s, "unit": "pairs/s", "h2d_bytes_per_step": int(img1.nbytes + img2.nbytes),
-                "d2h_bytes_per_step": int(pano.nbytes) + 72 + 16},
+                "d2h_bytes_per_step": int(pano.nbytes) + 72 + 16 + (8 if st.blend == "multiband" else 0)},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
         "stage_ms": stage_ms,

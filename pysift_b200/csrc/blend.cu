@@ -452,33 +452,15 @@ __global__ void __launch_bounds__(1024) k_blend_dp(const float* __restrict__ dpc
             for (int j = max(o.x, w.y + 1) + tid; j <= o.y; j += nt) cur[j] = BL_INF;
         }
         uint8_t* drow = dir + (long long)w.z * M;
-        // DP values are non-negative doubles (or INF), which order like their
-        // bit patterns as int64: the first minimum is taken on those
-        const long long* prevb = reinterpret_cast<const long long*>(prev);
-        constexpr int U = 4;
-        for (int j0 = w.x + tid; j0 <= w.y; j0 += U * nt) {
-            float c[U];
-            long long pl[U], pm[U], pr[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int j = j0 + u * nt;
-                const bool in = j <= w.y;
-                c[u] = in ? crow[j] : -1.0f;
-                pl[u] = in ? prevb[j - 1] : 0;
-                pm[u] = in ? prevb[j] : 0;
-                pr[u] = in ? prevb[j + 1] : 0;
-            }
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int j = j0 + u * nt;
-                if (j > w.y) break;
-                int a = 0;
-                long long best = pl[u];
-                if (pm[u] < best) { best = pm[u]; a = 1; }
-                if (pr[u] < best) { best = pr[u]; a = 2; }
-                cur[j] = c[u] >= 0.0f ? (double)c[u] + __longlong_as_double(best) : BL_INF;
-                if (a) drow[j] = (uint8_t)a;
-            }
+        for (int j = w.x + tid; j <= w.y; j += nt) {
+            const float c = crow[j];
+            const double pl = prev[j - 1], pm = prev[j], pr = prev[j + 1];
+            int a = 0;
+            double best = pl;
+            if (pm < best) { best = pm; a = 1; }
+            if (pr < best) { best = pr; a = 2; }
+            cur[j] = c >= 0.0f ? (double)c + best : BL_INF;
+            if (a) drow[j] = (uint8_t)a;
         }
         __syncthreads();
         double* t = prev;

@@ -82,6 +82,7 @@ def test_blend_reference_golden_bit_exact():
     (4, 257, 611, False, False),
     (5, 611, 257, True, True),
     (6, 720, 1300, False, False),
+    (8, 900, 2100, False, True),
 ])
 def test_blend_matches_oracle(seed, ch, cw, stacked, flip):
     from oracle import blend_oracle as bo
