@@ -174,6 +174,11 @@ int pysift_match_u8_split_fp8(const uint8_t* d1, int32_t n1, const uint8_t* d2, 
                               int32_t* bwd_best, int32_t* bwd_pass, int32_t* pairs, float* pair_dist,
                               int32_t* pair_count, pysift_stream_t stream);
 
+/* uint8 descriptors as OpenCV writes them: saturate(rint(512 v)) of each
+ * float of n_rows x 128 descriptors (the L2 / clip / L2 vector, i.e. a
+ * detection with rootsift = 0); device pointers. */
+int pysift_desc_to_u8(const float* desc, int64_t n_rows, uint8_t* out, pysift_stream_t stream);
+
 /* ---- stitch path (GPUPyStitch) ---- */
 
 /* cv2.cvtColor(BGR2GRAY) for uint8 (pysift/core.py:2546). */
@@ -208,6 +213,22 @@ int pysift_pca_stats(const float* x, int32_t n, int32_t D, void* workspace, size
 int pysift_pca_project_f16(const float* x, int32_t n, int32_t D, const float* mean, const float* proj, int32_t P,
                            uint16_t* out, pysift_stream_t stream);
 int pysift_to_f16(const float* in, int64_t n, uint16_t* out, pysift_stream_t stream);
+
+/* int8 matching (GPUPyStitch(int8_matching=True), pysift/core.py:2894-2923):
+ * pysift_pca_project_f32 is pysift_pca_project_f16 with the normalised rows
+ * kept in float32; pysift_quantize_i8_rows quantises float32 rows per row,
+ * scale = 127 / (max |x| + 1e-7) (as reciprocal * 127), q = trunc(clamp(x *
+ * scale, -127, 127)); pysift_match_i8 matches int8 rows (16-byte aligned)
+ * with a tcgen05 kind::i8 GEMM, similarity = int32 / (s1 * s2) in float32,
+ * then the ratio test, mutual check and outputs of pysift_match_fp16
+ * (workspace from pysift_match_workspace_size(..., exact_u8 = 0, ...)). */
+int pysift_pca_project_f32(const float* x, int32_t n, int32_t D, const float* mean, const float* proj, int32_t P,
+                           float* out, pysift_stream_t stream);
+int pysift_quantize_i8_rows(const float* x, int32_t n, int32_t D, int8_t* q, float* scale, pysift_stream_t stream);
+int pysift_match_i8(const int8_t* d1, const float* s1, int32_t n1, const int8_t* d2, const float* s2, int32_t n2,
+                    int32_t D, float ratio, void* workspace, size_t workspace_bytes, int32_t* fwd_best,
+                    int32_t* fwd_pass, int32_t* bwd_best, int32_t* bwd_pass, int32_t* pairs, float* pair_dist,
+                    int32_t* pair_count, pysift_stream_t stream);
 
 /* The raw 32-bit MT19937 stream of torch.Generator(device='cpu').manual_seed(seed):
  * torch.randint(0, N, (B, 4), generator=g) equals out[0:4B] % N (host function). */

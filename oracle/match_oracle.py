@@ -11,6 +11,10 @@ torch.topk.
   differ from it only when the exact value lies within ~1e-7 of an fp16
   rounding boundary.
 * exact mode: int64 squared L2 distances of uint8 descriptors.
+* int8 mode (int8_matching=True, pysift/core.py:2894-2923): per-row
+  symmetric quantisation of the float32 (PCA-projected, L2-normalised)
+  descriptors, an exact int32 GEMM, the similarity int / (s1 s2) in float32,
+  then the fp16 mode's ratio test on it.
 """
 import numpy as np
 
@@ -84,3 +88,36 @@ def _mutual(fb, fok, fdist, bb, bok, S):
     return dict(fwd_best=fb.astype(np.int32), fwd_pass=fok.astype(np.int32), bwd_best=bb.astype(np.int32),
                 bwd_pass=bok.astype(np.int32), pairs=np.array(pairs, np.int32).reshape(-1, 2),
                 dist=np.array(dist, np.float32), scores=S)
+
+
+def quantize_i8(d):
+    """_to_int8_torch (pysift/core.py:2902-2905) in float32: scale =
+    127.0 / (max |d| + 1e-7) per row, which torch evaluates (scalar / tensor)
+    as reciprocal(max |d| + 1e-7) * 127; q = trunc(clip(d * scale, -127, 127))."""
+    d = np.asarray(d, np.float32)
+    scale = (np.float32(1.0) / (np.abs(d).max(axis=1) + np.float32(1e-7))) * np.float32(127.0)
+    q = np.trunc(np.clip(d * scale[:, None], np.float32(-127.0), np.float32(127.0))).astype(np.int8)
+    return q, scale.astype(np.float32)
+
+
+def sim_i8(q1, s1, q2, s2):
+    """torch._int_mm(q1, q2.T).float() / (s1 * s2.T) (pysift/core.py:2908-2910)."""
+    acc = q1.astype(np.int64) @ q2.astype(np.int64).T
+    den = s1[:, None].astype(np.float32) * s2[None, :].astype(np.float32)
+    return acc.astype(np.float32) / den
+
+
+def match_i8(d1, d2, ratio=0.75):
+    """int8 matching of float32 descriptors (quantised here)."""
+    q1, s1 = quantize_i8(d1)
+    q2, s2 = quantize_i8(d2)
+    S = sim_i8(q1, s1, q2, s2)
+    rs = np.float32(ratio * ratio)
+    fb, f1, f2 = _top2(S, True)
+    fok, fdist = ratio_pass_fp16(f1, f2, rs)
+    bb, b1, b2 = _top2(S.T.copy(), True)
+    bok, _ = ratio_pass_fp16(b1, b2, rs)
+    out = _mutual(fb, fok, fdist, bb, bok, S)
+    out.update(q1=q1, s1=s1, q2=q2, s2=s2)
+    return out
+

@@ -143,7 +143,9 @@ def autocrop(pano, both):
 
 class OracleStitch:
     def __init__(self, ransac_iters=1500, inlier_thresh=5.0, match_ratio=0.75, max_keypoints=8000, pca_dims=64,
-                 n_octaves=4, clahe_clip=2.0, clahe_tile=8, high_vram=True, blend="multiband", n_blend_levels=6):
+                 n_octaves=4, clahe_clip=2.0, clahe_tile=8, high_vram=True, blend="multiband", n_blend_levels=6,
+                 int8_matching=False):
+        self.int8_matching = int8_matching
         self.blend = blend
         self.n_blend_levels = n_blend_levels
         self.ransac_iters = ransac_iters
@@ -174,14 +176,19 @@ class OracleStitch:
             mean, cov = pca_stats(both)
             w, v = np.linalg.eigh(cov)
             self.pca = (mean, np.ascontiguousarray(v[:, -self.pca_dims:].astype(np.float32)))
-        p = pca_project(both, *self.pca).astype(np.float16)
+        p = pca_project(both, *self.pca)
+        if not self.int8_matching:
+            p = p.astype(np.float16)
         return p[:len(d1)], p[len(d1):]
 
     def stitch(self, img1, img2):
         pts1, d1, _ = self.features(img1)
         pts2, d2, _ = self.features(img2)
         a, b = self.prepare(d1, d2)
-        m = match_oracle.match_fp16(a, b, self.match_ratio)
+        if self.int8_matching:
+            m = match_oracle.match_i8(a, b, self.match_ratio)   # pysift/core.py:2894-2923
+        else:
+            m = match_oracle.match_fp16(a, b, self.match_ratio)
         pairs = m["pairs"]
         p1 = pts1[pairs[:, 0]].astype(np.float64)
         p2 = pts2[pairs[:, 1]].astype(np.float64)

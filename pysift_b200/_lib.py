@@ -153,6 +153,7 @@ def check(rc, what):
 
 EXPORTS.update({
     "pysift_bgr2gray": (ctypes.c_int, [c_void_p, c_int32, c_int32, c_int64, c_void_p, c_int32, c_void_p]),
+    "pysift_desc_to_u8": (ctypes.c_int, [c_void_p, c_int64, c_void_p, c_void_p]),
     "pysift_clahe_lut_bytes": (ctypes.c_int, [c_int32, c_int32, ctypes.POINTER(c_size_t)]),
     "pysift_clahe": (ctypes.c_int, [c_void_p, c_int32, c_int32, c_int32, c_double, c_int32, c_int32, c_void_p,
                                     c_void_p, c_int32, c_void_p]),
@@ -174,6 +175,12 @@ EXPORTS.update({
                                            c_int32, c_int32, c_void_p, c_float, c_float, c_int32, c_int32, c_int32,
                                            c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                            c_void_p, c_void_p]),
+    "pysift_pca_project_f32": (ctypes.c_int, [c_void_p, c_int32, c_int32, c_void_p, c_void_p, c_int32, c_void_p,
+                                              c_void_p]),
+    "pysift_quantize_i8_rows": (ctypes.c_int, [c_void_p, c_int32, c_int32, c_void_p, c_void_p, c_void_p]),
+    "pysift_match_i8": (ctypes.c_int, [c_void_p, c_void_p, c_int32, c_void_p, c_void_p, c_int32, c_int32, c_float,
+                                       c_void_p, c_size_t, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                       c_void_p, c_void_p]),
     "pysift_place_image": (ctypes.c_int, [c_void_p, c_int32, c_int32, c_int32, c_int32, c_int32, c_int32, c_int32,
                                           c_void_p, c_void_p, c_void_p]),
     "pysift_blend_workspace_size": (ctypes.c_int, [c_int32, c_int32, c_int32, c_void_p]),

@@ -140,6 +140,16 @@ class _BatchOutputs:
         self.stats_host = torch.zeros(_lib.STAT_COUNT, dtype=torch.int32).pin_memory()
 
 
+def keypoints_from_rows(kp, resp, octv):
+    """cv2.KeyPoint list from output rows [x, y, size, angle], response and
+    octave (pysift/core.py:2139-2142), built by mapping the constructor over
+    Python lists (about 3.5x faster than a per-row loop)."""
+    import cv2
+    c = np.asarray(kp, np.float64).T.tolist()
+    return list(map(cv2.KeyPoint, c[0], c[1], c[2], c[3], np.asarray(resp, np.float64).tolist(),
+                    np.asarray(octv).astype(np.int64).tolist()))
+
+
 class PySIFT:
     """GPU SIFT detector/descriptor with the reference's interface
     (pysift/core.py:1150-2172).
@@ -150,7 +160,7 @@ class PySIFT:
 
     def __init__(self, n_octaves=None, n_scales=3, sigma0=1.6, contrast_thresh=0.04, edge_thresh=10.0,
                  dsp=False, dsp_n_scales=3, fp16_pyramid=None, orientation='histogram', descriptor='sift',
-                 double_image=True, rootsift=True, *, device=None, high_vram=None):
+                 double_image=True, rootsift=True, *, device=None, high_vram=None, as_uint8=False):
         if dsp_n_scales not in DSP_PRESETS:
             raise ValueError(f"dsp_n_scales must be 3, 4, or 5 (got {dsp_n_scales})")
         if orientation != 'histogram':
@@ -161,6 +171,9 @@ class PySIFT:
             raise NotImplementedError(
                 f"descriptor={descriptor!r}: only the SIFT descriptor is implemented on this backend "
                 "(the learned HardNet/HyNet paths are not part of it)")
+        if as_uint8 and rootsift:
+            raise ValueError("as_uint8 converts the L2 / clip / L2 descriptor as OpenCV does: "
+                             "construct with rootsift=False")
         if not torch.cuda.is_available():
             raise RuntimeError("PySIFT (pysift_b200) needs a CUDA device")
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
@@ -172,6 +185,7 @@ class PySIFT:
         self.contrast_thresh = contrast_thresh
         self.edge_thresh = edge_thresh
         self.rootsift = rootsift
+        self.as_uint8 = bool(as_uint8)
         self.dsp = dsp
         self.dsp_n_scales = dsp_n_scales
         self._dsp_scales_np = DSP_PRESETS[dsp_n_scales]
@@ -271,18 +285,24 @@ class PySIFT:
         if profile:
             t1 = time.perf_counter()
             self._phase_timings = {'total_ms': (t1 - t0) * 1000.0}
+        desc_dev = self._desc_u8(b.desc[:n]) if self.as_uint8 else b.desc[:n]
         if gpu_output:
-            return b.kpts[:n].clone(), b.desc[:n].clone()
+            return b.kpts[:n].clone(), desc_dev.clone()
         kp = b.kpts[:n].cpu().numpy()
         resp = b.resp[:n].cpu().numpy()
         octv = b.octv[:n].cpu().numpy()
-        desc = b.desc[:n].cpu().numpy()
+        desc = desc_dev.cpu().numpy()
         if n == 0:
-            return [], np.zeros((0, 128), np.float32)
-        import cv2
-        kps = [cv2.KeyPoint(float(kp[j, 0]), float(kp[j, 1]), float(kp[j, 2]), float(kp[j, 3]),
-                            float(resp[j]), int(octv[j])) for j in range(n)]
-        return kps, desc
+            return [], np.zeros((0, 128), np.uint8 if self.as_uint8 else np.float32)
+        return keypoints_from_rows(kp, resp, octv), desc
+
+    def _desc_u8(self, desc):
+        """OpenCV's uint8 form saturate(rint(512 v)) of float descriptors (device)."""
+        out = torch.empty(desc.shape, dtype=torch.uint8, device=desc.device)
+        _lib.check(self._lib.pysift_desc_to_u8(desc.data_ptr(), desc.shape[0], out.data_ptr(),
+                                               torch.cuda.current_stream(desc.device).cuda_stream),
+                   "pysift_desc_to_u8")
+        return out
 
     # -- batched detection ----------------------------------------------------
     def detect_batch(self, images, n_streams=8, gpu_output=True):
@@ -360,10 +380,11 @@ class PySIFT:
             for i in range(n):
                 o = bt["outs"][i]
                 k = int(o.stats_host[_lib.STAT_N_KEYPOINTS])
+                d = self._desc_u8(o.desc[:k]) if self.as_uint8 else o.desc[:k]
                 if gpu_output:
-                    out.append((o.kpts[:k].clone(), o.desc[:k].clone()))
+                    out.append((o.kpts[:k].clone(), d.clone()))
                 else:
-                    out.append((o.kpts[:k].cpu().numpy(), o.desc[:k].cpu().numpy()))
+                    out.append((o.kpts[:k].cpu().numpy(), d.cpu().numpy()))
         return out
 
     def detect_arrays(self, gray):

@@ -274,6 +274,16 @@ __global__ void k_gather_points(const float* __restrict__ kpts, const int* __res
 
 using namespace pysift;
 
+// OpenCV's uint8 SIFT descriptor: saturate(rint(512 v)) of the L2 / clip 0.2 /
+// L2 vector (512 v is exact in float32; rint rounds half to even)
+__global__ void k_desc_to_u8(const float* __restrict__ desc, long long n, uint8_t* __restrict__ out) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float v = rintf(desc[i] * 512.0f);
+    v = v < 0.0f ? 0.0f : (v > 255.0f ? 255.0f : v);
+    out[i] = (uint8_t)(int)v;
+}
+
 extern "C" {
 
 int pysift_bgr2gray(const uint8_t* bgr, int32_t H, int32_t W, int64_t pitch_bytes, uint8_t* gray, int32_t gray_pitch,
@@ -396,6 +406,16 @@ int pysift_gather_points(const float* kpts, const int32_t* pairs, const int32_t*
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     k_gather_points<<<ceil_div(max_pairs, 256), 256, 0, st>>>(kpts, pairs, count, max_pairs, col, pts);
     PYSIFT_LAUNCH_CHECK("k_gather_points");
+    return PYSIFT_OK;
+}
+
+int pysift_desc_to_u8(const float* desc, int64_t n_rows, uint8_t* out, pysift_stream_t stream) {
+    PYSIFT_CHECK_ARG(n_rows >= 0, "bad sizes");
+    if (n_rows == 0) return PYSIFT_OK;
+    PYSIFT_CHECK_ARG(desc && out, "NULL pointer argument");
+    const long long n = (long long)n_rows * 128;
+    k_desc_to_u8<<<(unsigned)ceil_div_ll(n, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(desc, n, out);
+    PYSIFT_LAUNCH_CHECK("k_desc_to_u8");
     return PYSIFT_OK;
 }
 

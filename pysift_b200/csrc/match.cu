@@ -39,7 +39,7 @@ constexpr int NT = 128;           // train rows per tile = UMMA N
 constexpr int MATCH_THREADS = 128;
 constexpr unsigned SPIN_LIMIT = 1u << 26;  // bounded waits on the MMA barriers
 
-enum MatchMode { SIM_F16 = 0, DIST_BF16 = 1, SPLIT_FP8 = 2 };
+enum MatchMode { SIM_F16 = 0, DIST_BF16 = 1, SPLIT_FP8 = 2, SIM_I8 = 3 };
 
 struct Top2 {  // best key and index, second-best key
     float k1, k2;
@@ -68,6 +68,12 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint
 __host__ __device__ constexpr uint32_t umma_idesc(int ab_format) {
     return (1u << 4) | ((uint32_t)ab_format << 7) | ((uint32_t)ab_format << 10) | ((uint32_t)(NT >> 3) << 17) |
            ((uint32_t)(MT >> 4) << 24);
+}
+
+// kind::i8 instruction descriptor: D = s32 (2), A/B = signed 8-bit (1),
+// both K-major, N = 128, M = 128.
+__host__ __device__ constexpr uint32_t umma_idesc_s8() {
+    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NT >> 3) << 17) | ((uint32_t)(MT >> 4) << 24);
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -113,19 +119,26 @@ struct RowScanArgs {
     const uint8_t* t;    // n_t rows of RB bytes
     int n_q, n_t;
     const int* norm_t;   // DIST_BF16: |t|^2 per train row
+    const float* scale_q;  // SIM_I8: quantisation scale per query row
+    const float* scale_t;  //         and per train row
     int seg_tiles;       // train tiles per segment (blockIdx.y)
     Top2* part;          // [n_q][gridDim.y]
     int* error;          // set when an MMA wait gives up
 };
 
 template <int MODE>
-__device__ __forceinline__ void scan_chunk(const uint32_t (&v)[32], int col0, int lim, int nb_lane, float& k1,
-                                           float& k2, int& i1) {
+__device__ __forceinline__ void scan_chunk(const uint32_t (&v)[32], int col0, int lim, int nb_lane, float sq,
+                                           float& k1, float& k2, int& i1) {
 #pragma unroll
     for (int j = 0; j < 32; ++j) {
         float key;
         if (MODE == SIM_F16) {
             key = __half2float(__float2half_rn(__uint_as_float(v[j])));
+        } else if (MODE == SIM_I8) {
+            // torch._int_mm(...).float() / (s1 * s2.T) (pysift/core.py:2908-2910):
+            // the int32 dot product is exact (|.| < 2^24, so exact in float32)
+            const float st = __int_as_float(__shfl_sync(FULL_MASK, nb_lane, j));
+            key = __fdiv_rn((float)(int)v[j], __fmul_rn(sq, st));
         } else {
             const float nb = __int_as_float(__shfl_sync(FULL_MASK, nb_lane, j));
             key = __fsub_rn(2.0f * __uint_as_float(v[j]), nb);
@@ -172,6 +185,7 @@ __global__ void __launch_bounds__(MATCH_THREADS) k_match_rows(const RowScanArgs 
 
     float k1 = -INFINITY, k2 = -INFINITY;
     int i1 = 0x7fffffff;
+    const float sq = (MODE == SIM_I8 && q0 + tid < args.n_q) ? args.scale_q[q0 + tid] : 1.0f;
     bool fail = false;
     int issued = 0;  // MMA groups committed
     for (int it = 0; it <= nt; ++it) {
@@ -199,13 +213,19 @@ __global__ void __launch_bounds__(MATCH_THREADS) k_match_rows(const RowScanArgs 
                 const uint32_t d = tmem + (uint32_t)((it & 1) * NT);
                 // f16 / bf16 (kind::f16, format 0 / 1) or e4m3 (kind::f8f6f4, format 0);
                 // either way one MMA covers 32 bytes of K: two core matrices
-                constexpr uint32_t idesc = umma_idesc(MODE == DIST_BF16 ? 1 : 0);
+                constexpr uint32_t idesc = MODE == SIM_I8 ? umma_idesc_s8() : umma_idesc(MODE == DIST_BF16 ? 1 : 0);
 #pragma unroll
                 for (int s = 0; s < RB / 32; ++s) {
                     const uint64_t da = umma_desc(a0 + s * 256, 128, KC * 128);
                     const uint64_t db = umma_desc(b0 + s * 256, 128, KC * 128);
                     const uint32_t acc = s > 0 ? 1u : 0u;
-                    if (MODE == SPLIT_FP8)
+                    if (MODE == SIM_I8)
+                        asm volatile(
+                            "{\n\t.reg .pred p;\n\t"
+                            "setp.ne.b32 p, %4, 0;\n\t"
+                            "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+                            "l"(da), "l"(db), "r"(idesc), "r"(acc));
+                    else if (MODE == SPLIT_FP8)
                         asm volatile(
                             "{\n\t.reg .pred p;\n\t"
                             "setp.ne.b32 p, %4, 0;\n\t"
@@ -231,7 +251,10 @@ __global__ void __launch_bounds__(MATCH_THREADS) k_match_rows(const RowScanArgs 
 #pragma unroll
             for (int chunk = 0; chunk < NT / 32; ++chunk) {
                 int nb_lane = 0;
-                if (MODE != SIM_F16) {
+                if (MODE == SIM_I8) {
+                    const int c = tcol0 + chunk * 32 + lane;
+                    nb_lane = __float_as_int(c < args.n_t ? args.scale_t[c] : 1.0f);
+                } else if (MODE != SIM_F16) {
                     const int c = tcol0 + chunk * 32 + lane;
                     nb_lane = __float_as_int((float)(c < args.n_t ? args.norm_t[c] : 0));
                 }
@@ -249,7 +272,7 @@ __global__ void __launch_bounds__(MATCH_THREADS) k_match_rows(const RowScanArgs 
                       "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
                     : "r"(taddr));
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                scan_chunk<MODE>(v, tcol0 + chunk * 32, lim_tile - chunk * 32, nb_lane, k1, k2, i1);
+                scan_chunk<MODE>(v, tcol0 + chunk * 32, lim_tile - chunk * 32, nb_lane, sq, k1, k2, i1);
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         }
@@ -409,8 +432,9 @@ static int launch_scan(const RowScanArgs& a, int nseg, cudaStream_t st) {
     return PYSIFT_OK;
 }
 
-// row bytes: 2 D for fp16 / bf16 rows, 4 D for the split e4m3 planes
+// row bytes: 2 D for fp16 / bf16 rows, 4 D for the split e4m3 planes, D for int8
 static int launch_scan_mode(int mode, const RowScanArgs& a, int D, int nseg, cudaStream_t st) {
+    if (mode == SIM_I8) return D == 64 ? launch_scan<SIM_I8, 64>(a, nseg, st) : launch_scan<SIM_I8, 128>(a, nseg, st);
     if (mode == SIM_F16) return D == 64 ? launch_scan<SIM_F16, 128>(a, nseg, st) : launch_scan<SIM_F16, 256>(a, nseg, st);
     if (mode == DIST_BF16)
         return D == 64 ? launch_scan<DIST_BF16, 128>(a, nseg, st) : launch_scan<DIST_BF16, 256>(a, nseg, st);
@@ -471,11 +495,13 @@ static T* wsp(void* ws, size_t off) {
 static int run_match(int mode, const uint8_t* a_q, const uint8_t* a_t, int n1, const uint8_t* b_q,
                      const uint8_t* b_t, int n2, int D, float ratio_sq,
                      const MatchLayout& l, void* ws, int* fbest_out, int* fpass_out, int* bbest_out, int* bpass_out,
-                     int32_t* pairs, float* pdist, int32_t* count, cudaStream_t st) {
+                     int32_t* pairs, float* pdist, int32_t* count, cudaStream_t st, const float* sa = nullptr,
+                     const float* sb = nullptr) {
     int* err = wsp<int>(ws, l.off_err);
     PYSIFT_CUDA_TRY(cudaMemsetAsync(err, 0, 4, st));
-    const int* na = mode != SIM_F16 ? wsp<int>(ws, l.off_na) : nullptr;
-    const int* nb = mode != SIM_F16 ? wsp<int>(ws, l.off_nb) : nullptr;
+    const bool sim = mode == SIM_F16 || mode == SIM_I8;
+    const int* na = !sim ? wsp<int>(ws, l.off_na) : nullptr;
+    const int* nb = !sim ? wsp<int>(ws, l.off_nb) : nullptr;
     int* fbest = fbest_out ? fbest_out : wsp<int>(ws, l.off_fbest);
     int* fpass = fpass_out ? fpass_out : wsp<int>(ws, l.off_fpass);
     int* bbest = bbest_out ? bbest_out : wsp<int>(ws, l.off_bbest);
@@ -489,6 +515,8 @@ static int run_match(int mode, const uint8_t* a_q, const uint8_t* a_t, int n1, c
         s.n_q = dir == 0 ? n1 : n2;
         s.n_t = dir == 0 ? n2 : n1;
         s.norm_t = dir == 0 ? nb : na;
+        s.scale_q = dir == 0 ? sa : sb;
+        s.scale_t = dir == 0 ? sb : sa;
         s.part = wsp<Top2>(ws, dir == 0 ? l.off_fpart : l.off_bpart);
         s.error = err;
         int nseg;
@@ -499,7 +527,7 @@ static int run_match(int mode, const uint8_t* a_q, const uint8_t* a_t, int n1, c
         int* best = dir == 0 ? fbest : bbest;
         int* pass = dir == 0 ? fpass : bpass;
         float* dist = dir == 0 ? fdist : bdist;
-        if (mode == SIM_F16)
+        if (sim)
             k_match_merge<SIM_F16><<<ceil_div(s.n_q, 256), 256, 0, st>>>(s.part, s.n_q, nseg, ratio_sq, nq, best, pass,
                                                                        dist);
         else
@@ -599,6 +627,26 @@ int pysift_match_u8_split_fp8(const uint8_t* d1, int32_t n1, const uint8_t* d2, 
     const float ratio_sq = (float)((double)ratio * (double)ratio);
     return run_match(SPLIT_FP8, qa, ta, n1, qb, tb, n2, D, ratio_sq, l, workspace, fwd_best, fwd_pass, bwd_best,
                      bwd_pass, pairs, pair_dist, pair_count, st);
+}
+
+int pysift_match_i8(const int8_t* d1, const float* s1, int32_t n1, const int8_t* d2, const float* s2, int32_t n2,
+                    int32_t D, float ratio, void* workspace, size_t workspace_bytes, int32_t* fwd_best,
+                    int32_t* fwd_pass, int32_t* bwd_best, int32_t* bwd_pass, int32_t* pairs, float* pair_dist,
+                    int32_t* pair_count, pysift_stream_t stream) {
+    PYSIFT_CHECK_ARG(d1 && d2 && s1 && s2 && workspace && pairs && pair_dist && pair_count, "NULL pointer argument");
+    PYSIFT_CHECK_ARG(n1 >= 1 && n2 >= 1 && (D == 64 || D == 128), "bad sizes (D must be 64 or 128)");
+    PYSIFT_CHECK_ARG((reinterpret_cast<uintptr_t>(d1) & 15) == 0 && (reinterpret_cast<uintptr_t>(d2) & 15) == 0,
+                     "descriptor arrays must be 16-byte aligned");
+    MatchLayout l = match_layout(n1, n2, D, 0);
+    if (workspace_bytes < l.total) {
+        set_error("workspace %zu bytes < required %zu", workspace_bytes, l.total);
+        return PYSIFT_ERR_WORKSPACE;
+    }
+    const float ratio_sq = (float)((double)ratio * (double)ratio);
+    const uint8_t* a = reinterpret_cast<const uint8_t*>(d1);
+    const uint8_t* b = reinterpret_cast<const uint8_t*>(d2);
+    return run_match(SIM_I8, a, a, n1, b, b, n2, D, ratio_sq, l, workspace, fwd_best, fwd_pass, bwd_best, bwd_pass,
+                     pairs, pair_dist, pair_count, reinterpret_cast<cudaStream_t>(stream), s1, s2);
 }
 
 }  // extern "C"

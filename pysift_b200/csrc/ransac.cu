@@ -632,10 +632,11 @@ __global__ void k_l2_normalize(const float* __restrict__ in, int n, int D, float
 constexpr int PJ_ROWS = 64;
 constexpr int PJ_T = 256;
 
-template <int D, int P>
+// OUT_F32: the normalised float32 rows (for the int8 matcher) instead of fp16
+template <int D, int P, bool OUT_F32 = false>
 __global__ void __launch_bounds__(PJ_T) k_pca_project_f16(const float* __restrict__ in, int n,
                                                          const float* __restrict__ mean, const float* __restrict__ proj,
-                                                         uint16_t* __restrict__ out) {
+                                                         void* __restrict__ out_v) {
     extern __shared__ float pj_smem[];
     float* s_proj = pj_smem;                  // D x P
     float* s_x = s_proj + D * P;              // PJ_ROWS x (D + 1), centred
@@ -687,8 +688,13 @@ __global__ void __launch_bounds__(PJ_T) k_pca_project_f16(const float* __restric
         }
         const float den = sqrtf(ss) + 1e-7f;
 #pragma unroll
-        for (int g = 0; g < P / 32; ++g)
-            out[(size_t)(r0 + r) * P + g * 32 + lane] = __half_as_ushort(__float2half_rn(pvv[g] / den));
+        for (int g = 0; g < P / 32; ++g) {
+            const float y = pvv[g] / den;
+            if (OUT_F32)
+                static_cast<float*>(out_v)[(size_t)(r0 + r) * P + g * 32 + lane] = y;
+            else
+                static_cast<uint16_t*>(out_v)[(size_t)(r0 + r) * P + g * 32 + lane] = __half_as_ushort(__float2half_rn(y));
+        }
     }
 }
 
@@ -784,13 +790,50 @@ static RansacLayout ransac_layout(int n, int n_hyp) {
     return l;
 }
 
-template <int D, int P>
-static int launch_project(const float* x, int n, const float* mean, const float* proj, uint16_t* out, cudaStream_t st) {
+template <int D, int P, bool OUT_F32>
+static int launch_project(const float* x, int n, const float* mean, const float* proj, void* out, cudaStream_t st) {
     const size_t smem = ((size_t)D * P + (size_t)PJ_ROWS * (D + 1) + (size_t)PJ_ROWS * (P + 1)) * sizeof(float);
-    PYSIFT_CUDA_TRY(cudaFuncSetAttribute(k_pca_project_f16<D, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_pca_project_f16<D, P><<<ceil_div(n, PJ_ROWS), PJ_T, smem, st>>>(x, n, mean, proj, out);
+    PYSIFT_CUDA_TRY(cudaFuncSetAttribute(k_pca_project_f16<D, P, OUT_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem));
+    k_pca_project_f16<D, P, OUT_F32><<<ceil_div(n, PJ_ROWS), PJ_T, smem, st>>>(x, n, mean, proj, out);
     PYSIFT_LAUNCH_CHECK("k_pca_project_f16");
     return PYSIFT_OK;
+}
+
+template <bool OUT_F32>
+static int project_any(const float* x, int n, int D, const float* mean, const float* proj, int P, void* out,
+                       cudaStream_t st) {
+    if (D == 128 && P == 64) return launch_project<128, 64, OUT_F32>(x, n, mean, proj, out, st);
+    if (D == 128 && P == 32) return launch_project<128, 32, OUT_F32>(x, n, mean, proj, out, st);
+    if (D == 128 && P == 128) return launch_project<128, 128, OUT_F32>(x, n, mean, proj, out, st);
+    if (D == 64 && P == 64) return launch_project<64, 64, OUT_F32>(x, n, mean, proj, out, st);
+    return launch_project<64, 32, OUT_F32>(x, n, mean, proj, out, st);
+}
+
+// Symmetric int8 quantisation per row (pysift/core.py:2902-2905), one warp a
+// row: scale = 127 / (max |x| + 1e-7) evaluated as torch evaluates a scalar
+// divided by a tensor, reciprocal(max |x| + 1e-7) * 127, all in float32;
+// q = trunc(clamp(x * scale, -127, 127)).
+__global__ void k_quantize_i8_rows(const float* __restrict__ in, int n, int D, int8_t* __restrict__ q,
+                                   float* __restrict__ scale) {
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const float* r = in + (size_t)row * D;
+    float v[4];
+    float amax = 0.0f;
+    for (int g = 0; g < D / 32; ++g) {
+        v[g] = r[g * 32 + lane];
+        amax = fmaxf(amax, fabsf(v[g]));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(FULL_MASK, amax, o));
+    const float s = __fmul_rn(__frcp_rn(__fadd_rn(amax, 1e-7f)), 127.0f);
+    for (int g = 0; g < D / 32; ++g) {
+        float y = __fmul_rn(v[g], s);
+        y = fminf(fmaxf(y, -127.0f), 127.0f);
+        q[(size_t)row * D + g * 32 + lane] = (int8_t)(int)y;
+    }
+    if (lane == 0) scale[row] = s;
 }
 
 }  // namespace pysift
@@ -924,12 +967,25 @@ int pysift_pca_project_f16(const float* x, int32_t n, int32_t D, const float* me
     PYSIFT_CHECK_ARG((D == 128 || D == 64) && (P == 32 || P == 64 || P == 128) && P <= D,
                      "unsupported sizes (D in {64, 128}, P in {32, 64, 128}, P <= D)");
     if (n == 0) return PYSIFT_OK;
-    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    if (D == 128 && P == 64) return launch_project<128, 64>(x, n, mean, proj, out, st);
-    if (D == 128 && P == 32) return launch_project<128, 32>(x, n, mean, proj, out, st);
-    if (D == 128 && P == 128) return launch_project<128, 128>(x, n, mean, proj, out, st);
-    if (D == 64 && P == 64) return launch_project<64, 64>(x, n, mean, proj, out, st);
-    return launch_project<64, 32>(x, n, mean, proj, out, st);
+    return project_any<false>(x, n, D, mean, proj, P, out, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int pysift_pca_project_f32(const float* x, int32_t n, int32_t D, const float* mean, const float* proj, int32_t P,
+                           float* out, pysift_stream_t stream) {
+    PYSIFT_CHECK_ARG(x && mean && proj && out && n >= 0, "bad arguments");
+    PYSIFT_CHECK_ARG((D == 128 || D == 64) && (P == 32 || P == 64 || P == 128) && P <= D,
+                     "unsupported sizes (D in {64, 128}, P in {32, 64, 128}, P <= D)");
+    if (n == 0) return PYSIFT_OK;
+    return project_any<true>(x, n, D, mean, proj, P, out, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int pysift_quantize_i8_rows(const float* x, int32_t n, int32_t D, int8_t* q, float* scale, pysift_stream_t stream) {
+    PYSIFT_CHECK_ARG(x && q && scale && n >= 0, "bad arguments");
+    PYSIFT_CHECK_ARG(D == 32 || D == 64 || D == 96 || D == 128, "D must be a multiple of 32, at most 128");
+    if (n == 0) return PYSIFT_OK;
+    k_quantize_i8_rows<<<ceil_div(n, 8), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(x, n, D, q, scale);
+    PYSIFT_LAUNCH_CHECK("k_quantize_i8_rows");
+    return PYSIFT_OK;
 }
 
 int pysift_to_f16(const float* in, int64_t n, uint16_t* out, pysift_stream_t stream) {

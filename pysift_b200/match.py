@@ -15,6 +15,7 @@ Both take CUDA tensors and return CUDA tensors; ties go to the lower index.
 """
 import ctypes
 
+import numpy as np
 import torch
 
 from . import _lib
@@ -74,3 +75,61 @@ def match_u8_split_fp8(a, b, ratio=0.75, stream=None):
     assert a.dtype == torch.uint8 and b.dtype == torch.uint8
     return _run(_lib.load().pysift_match_u8_split_fp8, "pysift_match_u8_split_fp8", a.contiguous(), b.contiguous(),
                 ratio, 2, stream)
+
+
+def quantize_i8(x, stream=None):
+    """Per-row symmetric int8 quantisation of float32 CUDA rows (N, D)
+    (pysift/core.py:2902-2905): returns (int8 (N, D), float32 scales (N,))."""
+    assert x.dtype == torch.float32 and x.is_cuda
+    x = x.contiguous()
+    n, D = x.shape
+    q = torch.empty((n, D), dtype=torch.int8, device=x.device)
+    s = torch.empty(n, dtype=torch.float32, device=x.device)
+    st = (stream or torch.cuda.current_stream(x.device)).cuda_stream
+    _lib.check(_lib.load().pysift_quantize_i8_rows(x.data_ptr(), n, D, q.data_ptr(), s.data_ptr(), st),
+               "pysift_quantize_i8_rows")
+    return q, s
+
+
+def match_i8(q1, s1, q2, s2, ratio=0.75, stream=None):
+    """int8 matching (int8_matching=True, pysift/core.py:2894-2923) of
+    quantised rows q (N, D) int8 with their scales s (N,) float32, D in
+    {64, 128}: similarity int32 / (s1 s2) in float32 from a tcgen05 kind::i8
+    GEMM, then the fp16 mode's ratio test and mutual check."""
+    assert q1.dtype == torch.int8 and q2.dtype == torch.int8
+    lib = _lib.load()
+    q1, q2 = q1.contiguous(), q2.contiguous()
+    s1, s2 = s1.contiguous(), s2.contiguous()
+    n1, D = q1.shape
+    n2 = q2.shape[0]
+    dev = q1.device
+    ws = _ws(lib, n1, n2, D, 0, dev)
+    wp, wn = _aligned(ws)
+    out = {k: torch.empty(n, dtype=torch.int32, device=dev) for k, n in
+           (("fwd_best", n1), ("fwd_pass", n1), ("bwd_best", n2), ("bwd_pass", n2))}
+    pairs = torch.empty((n1, 2), dtype=torch.int32, device=dev)
+    dist = torch.empty(n1, dtype=torch.float32, device=dev)
+    count = torch.zeros(1, dtype=torch.int32, device=dev)
+    st = (stream or torch.cuda.current_stream(dev)).cuda_stream
+    rc = lib.pysift_match_i8(q1.data_ptr(), s1.data_ptr(), n1, q2.data_ptr(), s2.data_ptr(), n2, D, float(ratio),
+                             wp, wn, out["fwd_best"].data_ptr(), out["fwd_pass"].data_ptr(),
+                             out["bwd_best"].data_ptr(), out["bwd_pass"].data_ptr(), pairs.data_ptr(),
+                             dist.data_ptr(), count.data_ptr(), st)
+    _lib.check(rc, "pysift_match_i8")
+    out.update(pairs=pairs, dist=dist, count=count, workspace=ws)
+    return out
+
+
+def to_dmatches(m):
+    """The mutual matches of a match_* result as the reference's list of
+    cv2.DMatch(queryIdx, trainIdx, distance) in query order
+    (pysift/core.py:2929-2934), built by mapping the constructor over Python
+    lists.  Reads the count, pairs and distances back to the host."""
+    import cv2
+    n = int(m["count"].item())
+    if n == 0:
+        return []
+    pairs = m["pairs"][:n].cpu().numpy()
+    dist = m["dist"][:n].cpu().numpy().astype(np.float64)
+    return list(map(cv2.DMatch, pairs[:, 0].tolist(), pairs[:, 1].tolist(), dist.tolist()))
+

@@ -60,8 +60,6 @@ class GPUPyStitch:
                  blend='multiband'):
         if matcher != 'ratio':
             raise NotImplementedError(f"matcher={matcher!r}: only the ratio-test matcher is implemented here")
-        if int8_matching:
-            raise NotImplementedError("int8_matching: not implemented on this backend (fp16 tensor-core matching)")
         if pca_dims not in (0, 64, 128):
             raise NotImplementedError("pca_dims must be 0, 64 or 128 on this backend")
         if blend not in ('multiband', 'feather'):
@@ -188,7 +186,9 @@ class GPUPyStitch:
         return self._select(b, key)
 
     def _prepare(self, d1, d2):
-        """L2-normalise, PCA (fitted once per instance), fp16 (pysift/core.py:2877-2888)."""
+        """L2-normalise, PCA (fitted once per instance), then fp16 or, with
+        int8_matching, per-row int8 quantisation (pysift/core.py:2877-2905).
+        Returns ("f16", a, b) or ("i8", q1, s1, q2, s2) for _match_prepared."""
         st = self._stream()
         lib = self._lib
         n1, n2 = d1.shape[0], d2.shape[0]
@@ -198,9 +198,11 @@ class GPUPyStitch:
         _lib.check(lib.pysift_l2_normalize_rows(d2.data_ptr(), n2, D, both[n1:].data_ptr(), st), "l2")
         P = self.pca_dims if (self.descriptor == 'sift' and 0 < self.pca_dims < D) else 0
         if P == 0:
+            if self.int8_matching:
+                return self._quantize(both[:n1], both[n1:])
             out = torch.empty((n1 + n2, D), dtype=torch.float16, device=self.device)
             _lib.check(lib.pysift_to_f16(both.data_ptr(), both.numel(), out.data_ptr(), st), "to_f16")
-            return out[:n1], out[n1:], D
+            return ("f16", out[:n1], out[n1:])
         if self._pca_matrix is None:
             mean = torch.empty(D, dtype=torch.float32, device=self.device)
             cov = torch.empty((D, D), dtype=torch.float64, device=self.device)
@@ -215,16 +217,35 @@ class GPUPyStitch:
             proj = np.ascontiguousarray(v[:, -P:].astype(np.float32))
             self._pca_matrix = torch.from_numpy(proj).to(self.device)
             self._pca_mean = mean
+        if self.int8_matching:
+            outf = torch.empty((n1 + n2, P), dtype=torch.float32, device=self.device)
+            _lib.check(lib.pysift_pca_project_f32(both.data_ptr(), n1 + n2, D, self._pca_mean.data_ptr(),
+                                                  self._pca_matrix.data_ptr(), P, outf.data_ptr(), st),
+                       "pysift_pca_project_f32")
+            return self._quantize(outf[:n1], outf[n1:])
         out = torch.empty((n1 + n2, P), dtype=torch.float16, device=self.device)
         _lib.check(lib.pysift_pca_project_f16(both.data_ptr(), n1 + n2, D, self._pca_mean.data_ptr(),
                                               self._pca_matrix.data_ptr(), P, out.data_ptr(), st),
                    "pysift_pca_project_f16")
-        return out[:n1], out[n1:], P
+        return ("f16", out[:n1], out[n1:])
+
+    def _quantize(self, f1, f2):
+        """int8 rows and scales of both sets (each quantised on its own, as
+        pysift/core.py:2906-2907 does)."""
+        from . import match
+        st = torch.cuda.current_stream(self.device)
+        q1, s1 = match.quantize_i8(f1, stream=st)
+        q2, s2 = match.quantize_i8(f2, stream=st)
+        return ("i8", q1, s1, q2, s2)
+
+    def _match_prepared(self, prep, stream=None):
+        from . import match
+        if prep[0] == "i8":
+            return match.match_i8(*prep[1:], self.match_ratio, stream=stream)
+        return match.match_fp16(prep[1], prep[2], self.match_ratio, stream=stream)
 
     def _match(self, d1, d2):
-        from . import match
-        a, b, D = self._prepare(d1, d2)
-        return match.match_fp16(a, b, self.match_ratio)
+        return self._match_prepared(self._prepare(d1, d2))
 
     def _random_stream(self, n_hyp):
         r = self._rand.get(n_hyp)
@@ -401,9 +422,9 @@ class GPUPyStitch:
             if n1 == 0 or n2 < 2:
                 raise RuntimeError(f"Insufficient matches (0), need >= 4")
             from . import match as _match_mod
-            a, bq, _ = self._prepare(d1, d2)
+            prep = self._prepare(d1, d2)
             self._mark(2)
-            m = _match_mod.match_fp16(a, bq, self.match_ratio)
+            m = self._match_prepared(prep)
             self._mark(3)
             n_m = int(m["count"].item())
             metrics.update(matches=n_m)
@@ -494,8 +515,8 @@ class GPUPyStitch:
             for p in range(P):
                 st = streams[p % ns]
                 with torch.cuda.stream(st):
-                    a, bq, _ = self._prepare(feats[2 * p][1], feats[2 * p + 1][1])
-                    matches.append(_match_mod.match_fp16(a, bq, self.match_ratio, stream=st))
+                    prep = self._prepare(feats[2 * p][1], feats[2 * p + 1][1])
+                    matches.append(self._match_prepared(prep, stream=st))
             for s in streams:
                 main.wait_stream(s)
             counts = torch.cat([m["count"] for m in matches]).cpu().numpy()

@@ -136,3 +136,34 @@ def test_oracle_detect_runs_and_is_sorted(oracle_lib):
     order = np.lexsort((r["y"], r["x"]))
     assert np.array_equal(order, np.arange(n))
     assert np.allclose(np.linalg.norm(r["desc"], axis=1), 1.0, atol=1e-5)
+
+
+def test_fast_keypoint_and_dmatch_construction():
+    """keypoints_from_rows / to_dmatches build the same cv2 objects as the
+    reference's per-row constructors (pysift/core.py:2139-2142, 2929-2934)."""
+    import cv2
+    import torch
+    from pysift_b200.core import keypoints_from_rows
+    from pysift_b200.match import to_dmatches
+    rng = np.random.default_rng(5)
+    kp = (rng.random((300, 4)) * 500).astype(np.float32)
+    resp = rng.random(300).astype(np.float32)
+    octv = rng.integers(0, 5, 300).astype(np.int32)
+    fast = keypoints_from_rows(kp, resp, octv)
+    for j in (0, 17, 299):
+        ref = cv2.KeyPoint(float(kp[j, 0]), float(kp[j, 1]), float(kp[j, 2]), float(kp[j, 3]), float(resp[j]),
+                           int(octv[j]))
+        k = fast[j]
+        assert (k.pt, k.size, k.angle, k.response, k.octave) == (ref.pt, ref.size, ref.angle, ref.response,
+                                                                   ref.octave)
+    pairs = torch.tensor([[0, 5], [3, 1], [7, 2]], dtype=torch.int32)
+    dist = torch.tensor([0.5, 0.25, 0.125], dtype=torch.float32)
+    dm = to_dmatches(dict(pairs=pairs, dist=dist, count=torch.tensor([2], dtype=torch.int32)))
+    assert [(d.queryIdx, d.trainIdx, d.distance, d.imgIdx) for d in dm] == [(0, 5, 0.5, -1), (3, 1, 0.25, -1)]
+    assert to_dmatches(dict(pairs=pairs, dist=dist, count=torch.tensor([0], dtype=torch.int32))) == []
+
+
+def test_as_uint8_requires_plain_sift():
+    from pysift_b200 import PySIFT
+    with pytest.raises(ValueError):
+        PySIFT(as_uint8=True)

@@ -207,3 +207,39 @@ def test_detect_batch_matches_single_image_calls():
             assert np.array_equal(d1.cpu().numpy(), d2.cpu().numpy())
     host = sift.detect_batch(imgs[:3], n_streams=2, gpu_output=False)
     assert np.array_equal(host[1][1], ref[1][1].cpu().numpy())
+
+
+def test_as_uint8_descriptors_and_exact_matching(oracle_lib):
+    """PySIFT(rootsift=False, as_uint8=True): OpenCV's uint8 form
+    saturate(rint(512 v)) of the oracle's L2 / clip / L2 descriptors, bit for
+    bit, through detectAndCompute and detect_batch; the uint8 sets of two
+    views then match exactly (BF16 tcgen05 path) like the int64 oracle."""
+    import torch
+    from oracle import match_oracle as mo
+    from pysift_b200 import PySIFT, match
+    img1, img2, _ = synthetic.stitch_pair(480, 640, seed=4)
+    import cv2
+    g1 = cv2.cvtColor(img1, cv2.COLOR_BGR2GRAY)
+    g2 = cv2.cvtColor(img2, cv2.COLOR_BGR2GRAY)
+    sift = PySIFT(rootsift=False, as_uint8=True)
+    orc = oracle_lib.OracleSIFT(rootsift=False)
+    outs = []
+    for g in (g1, g2):
+        kps, desc = sift.detectAndCompute(g)
+        ref = orc.detect_and_compute(g)
+        ref_u8 = np.clip(np.rint(ref["desc"] * np.float32(512.0)), 0, 255).astype(np.uint8)
+        assert desc.dtype == np.uint8 and np.array_equal(desc, ref_u8)
+        assert len(kps) == len(ref["x"])
+        outs.append(desc)
+    batch = sift.detect_batch([g1, g2], gpu_output=False)
+    for (k, d), ref in zip(batch, outs):
+        assert np.array_equal(d, ref)
+    a = torch.from_numpy(outs[0]).cuda()
+    b = torch.from_numpy(outs[1]).cuda()
+    m = match.match_u8_exact(a, b, 0.75)
+    n = int(m["count"].item())
+    ref = mo.match_u8_exact(outs[0], outs[1], 0.75)
+    assert n == len(ref["pairs"]) and n > 20
+    assert np.array_equal(m["pairs"][:n].cpu().numpy(), ref["pairs"])
+    dm = match.to_dmatches(m)
+    assert len(dm) == n and dm[0].queryIdx == int(ref["pairs"][0, 0]) and dm[0].trainIdx == int(ref["pairs"][0, 1])

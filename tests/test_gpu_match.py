@@ -93,3 +93,104 @@ def test_split_fp8_extreme_values_and_ties():
     ref = mo.match_u8_exact(a, b)
     for k in ("fwd_best", "fwd_pass", "bwd_best", "bwd_pass"):
         assert np.array_equal(out[k].cpu().numpy(), ref[k]), k
+
+
+def _unit_rows(rng, n, D, dup_from=None, frac=0.5, noise=0.02):
+    x = np.abs(rng.standard_normal((n, D))).astype(np.float32) if dup_from is None else None
+    if dup_from is not None:
+        x = rng.standard_normal((n, D)).astype(np.float32)
+        k = int(frac * n)
+        x[:k] = dup_from[:k] + noise * rng.standard_normal((k, D)).astype(np.float32)
+    return (x / np.linalg.norm(x, axis=1, keepdims=True)).astype(np.float32)
+
+
+@pytest.mark.parametrize("D", [64, 128])
+def test_int8_quantisation_bit_exact(D):
+    """pysift_quantize_i8_rows against the oracle and against torch's own
+    expression of the reference (pysift/core.py:2902-2905)."""
+    import torch
+    from oracle import match_oracle as mo
+    from pysift_b200 import match
+    rng = np.random.default_rng(D)
+    x = rng.standard_normal((3001, D)).astype(np.float32)
+    x /= np.linalg.norm(x, axis=1, keepdims=True)
+    x[7] = 0.0  # an all-zero row: scale 127 / 1e-7
+    q, s = match.quantize_i8(torch.from_numpy(x).cuda())
+    rq, rs = mo.quantize_i8(x)
+    assert np.array_equal(q.cpu().numpy(), rq) and np.array_equal(s.cpu().numpy(), rs)
+    t = torch.from_numpy(x).cuda()
+    sc = 127.0 / (t.abs().amax(dim=1, keepdim=True) + 1e-7)
+    tq = (t * sc).clamp(-127, 127).to(torch.int8)
+    assert torch.equal(tq, q) and torch.equal(sc[:, 0], s)
+
+
+@pytest.mark.parametrize("n1,n2,D", [(1000, 1200, 64), (3000, 2500, 128), (129, 5000, 64), (8000, 8000, 64)])
+def test_int8_matching_bit_exact(n1, n2, D):
+    """int8 matching (tcgen05 kind::i8): every forward / backward best index,
+    pass flag and mutual pair equal to the oracle's."""
+    import torch
+    from oracle import match_oracle as mo
+    from pysift_b200 import match
+    rng = np.random.default_rng(n1 + n2 + D)
+    a = _unit_rows(rng, n1, D)
+    b = _unit_rows(rng, n2, D, dup_from=a, frac=min(0.5, n1 / n2 * 0.5))
+    q1, s1 = match.quantize_i8(torch.from_numpy(a).cuda())
+    q2, s2 = match.quantize_i8(torch.from_numpy(b).cuda())
+    m = match.match_i8(q1, s1, q2, s2, 0.75)
+    ref = mo.match_i8(a, b, 0.75)
+    for k in ("fwd_best", "fwd_pass", "bwd_best", "bwd_pass"):
+        assert np.array_equal(m[k].cpu().numpy(), ref[k]), k
+    n = int(m["count"].item())
+    assert n == len(ref["pairs"]) and n > 0
+    assert np.array_equal(m["pairs"][:n].cpu().numpy(), ref["pairs"])
+    assert np.array_equal(m["dist"][:n].cpu().numpy(), ref["dist"])
+
+
+def test_int8_matching_ties_go_to_lower_index():
+    import torch
+    from oracle import match_oracle as mo
+    from pysift_b200 import match
+    rng = np.random.default_rng(3)
+    a = _unit_rows(rng, 300, 64)
+    b = np.concatenate([a[:100], a[:100], _unit_rows(rng, 100, 64)])  # exact duplicates: equal similarities
+    q1, s1 = match.quantize_i8(torch.from_numpy(a).cuda())
+    q2, s2 = match.quantize_i8(torch.from_numpy(b).cuda())
+    m = match.match_i8(q1, s1, q2, s2, 0.99)
+    ref = mo.match_i8(a, b, 0.99)
+    assert np.array_equal(m["fwd_best"].cpu().numpy(), ref["fwd_best"])
+    assert np.array_equal(m["bwd_best"].cpu().numpy(), ref["bwd_best"])
+
+
+def test_pca_project_f32_matches_oracle_and_fp16_path():
+    import torch
+    from oracle import stitch_oracle as so
+    from pysift_b200 import _lib
+    lib = _lib.load()
+    rng = np.random.default_rng(11)
+    x = np.abs(rng.standard_normal((2000, 128))).astype(np.float32)
+    x /= np.linalg.norm(x, axis=1, keepdims=True)
+    mean = x.mean(0).astype(np.float32)
+    w, v = np.linalg.eigh(np.cov(x.T))
+    proj = np.ascontiguousarray(v[:, -64:].astype(np.float32))
+    xt, mt, pt = (torch.from_numpy(t).cuda() for t in (x, mean, proj))
+    f32 = torch.empty((2000, 64), dtype=torch.float32, device="cuda")
+    f16 = torch.empty((2000, 64), dtype=torch.float16, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    assert lib.pysift_pca_project_f32(xt.data_ptr(), 2000, 128, mt.data_ptr(), pt.data_ptr(), 64, f32.data_ptr(), st) == 0
+    assert lib.pysift_pca_project_f16(xt.data_ptr(), 2000, 128, mt.data_ptr(), pt.data_ptr(), 64, f16.data_ptr(), st) == 0
+    ref = so.pca_project(x, mean, proj)
+    assert np.array_equal(f32.cpu().numpy(), ref)
+    assert np.array_equal(f32.half().cpu().numpy(), f16.cpu().numpy())
+
+
+def test_stitch_int8_matching_end_to_end():
+    from oracle import stitch_oracle as so
+    from pysift_b200.stitch import GPUPyStitch
+    img1, img2, _ = synthetic.stitch_pair(480, 640, seed=6)
+    st = GPUPyStitch(ransac_iters=1024, inlier_thresh=4.0, save_output=False, verbose=False, int8_matching=True)
+    st.stitch(img1, img2)
+    orc = so.OracleStitch(ransac_iters=1024, inlier_thresh=4.0, int8_matching=True, blend="feather").stitch(img1, img2)
+    assert st.last_metrics["matches"] == len(orc["pairs"])
+    assert np.array_equal(st._last["pairs"].cpu().numpy(), orc["pairs"])
+    rel = np.max(np.abs(st._last["H"] - orc["H"]) / np.maximum(np.abs(orc["H"]), 1e-6))
+    assert rel < 1e-6, rel
