@@ -8,8 +8,10 @@ numpy + scipy.ndimage (the algorithms cupyx.scipy.ndimage implements).
 
 Canonical choices where the reference's arithmetic is not reproducible
 (the CUDA path implements the same definition):
-  * gain: the overlap means are exact (float64 sums / count) rounded to
-    float32; the reference takes numpy's float32 pairwise means;
+  * gain: the overlap means come from order-free integer sums -- each value
+    rounded to a multiple of 2^-24 (exact for uint8 images), summed in int64,
+    scaled back in float64, divided by the count and rounded to float32; the
+    reference takes numpy's float32 means (a sequential sum over the rows);
   * seam-mask blur: separable, the float32 kernel of _seam_kernel,
     BORDER_REFLECT_101, rows then columns, float64 sums rounded to float32
     after each pass; the reference calls cv2.GaussianBlur (SIMD float sums).
@@ -53,6 +55,14 @@ def seam_blur(x, faithful=False):
     return out.astype(np.float32)
 
 
+def canonical_mean(v):
+    """Per-channel mean of the rows of v (n, 3) float32: values rounded to
+    multiples of 2^-24, summed in int64, scaled back in float64, divided by n
+    in float64, rounded to float32."""
+    q = np.rint(v.astype(np.float64) * 16777216.0).astype(np.int64).sum(0)
+    return ((q.astype(np.float64) / 16777216.0) / float(len(v))).astype(np.float32)
+
+
 def gain_compensate(w1, c2, ov, faithful=False):
     """core.py:3692-3699 (color_match='gain')."""
     if not ov.any():
@@ -61,9 +71,8 @@ def gain_compensate(w1, c2, ov, faithful=False):
         m2 = c2[ov].mean(0)
         m1 = w1[ov].mean(0)
     else:
-        n = float(ov.sum())
-        m2 = (c2[ov].astype(np.float64).sum(0) / n).astype(np.float32)
-        m1 = (w1[ov].astype(np.float64).sum(0) / n).astype(np.float32)
+        m2 = canonical_mean(c2[ov])
+        m1 = canonical_mean(w1[ov])
     gain = (m2 + np.float32(1e-3)) / (m1 + np.float32(1e-3))
     return np.clip(w1 * np.clip(gain, np.float32(0.5), np.float32(2.0)), 0, 255).astype(np.float32)
 
@@ -193,11 +202,23 @@ def multiband(I1, I2, seam, n_levels=6):
     return res.astype(np.float32)
 
 
-def blend_pair(warped1, m1, canvas2, m2, n_levels=6, faithful=False):
-    """_blend_pair + the paste of _stitch_pair: uint8 (H, W, 3) canvas (before
-    the inner-rectangle crop) and the union mask."""
-    w1 = warped1.astype(np.float32)
-    c2 = canvas2.astype(np.float32)
+def seam_rmse(w1_gained, m1, c2, m2):
+    """_seam_rmse (core.py:3555-3562) of the gained image 1, exact: the
+    uint8-truncated differences squared, summed as integers."""
+    ov = m1 & m2
+    if not ov.any():
+        return float("nan")
+    a = np.clip(w1_gained, 0, 255).astype(np.uint8)[ov].astype(np.int64)
+    b = np.clip(c2, 0, 255).astype(np.uint8)[ov].astype(np.int64)
+    d = a - b
+    return float(np.sqrt((d * d).sum() / d.size))
+
+
+def blend_core(w1, m1, c2, m2, n_levels=6, faithful=False):
+    """_blend_pair (core.py:3686-3714) on float32 canvases: the blended float32
+    image (before any clipping), the union mask and the seam RMSE."""
+    w1 = np.asarray(w1, np.float32)
+    c2 = np.asarray(c2, np.float32)
     ov = m1 & m2
     w1 = gain_compensate(w1, c2, ov, faithful)
     seam = find_seam(w1, c2, m1, m2, faithful)
@@ -208,7 +229,28 @@ def blend_pair(warped1, m1, canvas2, m2, n_levels=6, faithful=False):
     I1[~m1 & m2] = c2[~m1 & m2]
     I2[~m2 & m1] = w1[~m2 & m1]
     out = multiband(I1, I2, seam, n_levels)
-    both = m1 | m2
+    return out, m1 | m2, seam_rmse(w1, m1, c2, m2)
+
+
+def paste(out, both):
+    """The paste of _stitch_pair (core.py:3806-3809)."""
     pano = np.zeros(out.shape, np.uint8)
     pano[both] = np.clip(out[both], 0, 255).astype(np.uint8)
-    return pano, both
+    return pano
+
+
+def blend_pair(warped1, m1, canvas2, m2, n_levels=6, faithful=False):
+    """_blend_pair + the paste of _stitch_pair: uint8 (H, W, 3) canvas (before
+    the inner-rectangle crop) and the union mask."""
+    out, both, _ = blend_core(warped1.astype(np.float32), m1, canvas2.astype(np.float32), m2, n_levels, faithful)
+    return paste(out, both), both
+
+
+def compose3(warped1, m1, canvas2, m2, warped3, m3, n_levels=6, faithful=False):
+    """The composition of _stitch_triple (core.py:3913-3953): image 1 blended
+    with image 2, the float result blended with image 3 (gain on the float
+    image, seam, multiband), paste.  Returns (pano uint8 before the crop,
+    union mask, seam RMSE 1-2, seam RMSE 12-3)."""
+    b12, m12, r12 = blend_core(warped1.astype(np.float32), m1, canvas2.astype(np.float32), m2, n_levels, faithful)
+    out, both, r23 = blend_core(b12, m12, warped3.astype(np.float32), m3, n_levels, faithful)
+    return paste(out, both), both, r12, r23

@@ -1,7 +1,11 @@
 """Regenerates tests/golden/blend_cases.npz: the reference's own composition
 (GPUPyStitch._blend_pair -- gain, _find_seam with the DP seams and the
 sigma-3 mask blur, _multiband_blend -- and the paste of _stitch_pair) run on
-small synthetic canvases.
+small synthetic canvases, and tests/golden/triple_cases.npz: the
+reference's _stitch_triple on three small synthetic views, its stages before
+the composition (preprocessing, features, matching, RANSAC, depth) replaced
+by stubs that hand it fixed homographies, so that its own warps, two-pass
+composition, paste and inner-rectangle crop run unchanged.
 
 pysift/core.py imports cupy, cupyx.scipy.ndimage and numba at module level
 and this machine has no GPU, so the script puts numpy in place of cupy and
@@ -119,6 +123,72 @@ def make_cases():
     return cases
 
 
+def make_triples():
+    """(name, img1, img2, img3, H12, H32): views of one texture, image 1 left
+    of image 2 and image 3 right of it, with a little rotation / perspective."""
+    rng = np.random.default_rng(77)
+    out = []
+    for k, (h, w, sh1, sh3) in enumerate([(90, 120, 70, 74), (72, 100, 58, 61)]):
+        big = _texture(rng, h + 20, 3 * w, (1.0, 0.92, 0.85))
+        c2 = w  # image 2 starts here; image 1 sh1 columns left of it, image 3 sh3 right
+        img1 = big[10:10 + h, c2 - sh1:c2 - sh1 + w].copy()
+        img2 = big[10:10 + h, c2:c2 + w].copy()
+        img3 = big[10:10 + h, c2 + sh3:c2 + sh3 + w].copy()
+        img3 = np.clip(img3.astype(np.float32) * np.float32(0.9) + 6, 0, 255).astype(np.uint8)
+        a = 0.01 * (k + 1)
+        H12 = np.array([[np.cos(a), -np.sin(a), -float(sh1)], [np.sin(a), np.cos(a), 1.5], [2e-5, 0, 1.0]])
+        H32 = np.array([[1.0, 0.0, float(sh3)], [0.0, 1.0, -1.0], [0.0, -1e-5, 1.0]])
+        out.append((f"triple{k}", img1, img2, img3, H12, H32))
+    return out
+
+
+def run_triples(st_cls, out_dir):
+    import cv2
+    res = {}
+    names = []
+    for name, img1, img2, img3, H12, H32 in make_triples():
+        st = object.__new__(st_cls)
+        st.color_match = "gain"
+        st.n_blend_levels = 6
+        st.n_depth_layers = 4
+        kps = [cv2.KeyPoint(float(i), float(i), 1.0) for i in range(12)]
+        dms = [cv2.DMatch(i, i, 0.0) for i in range(12)]
+        hs = iter([H12, H32])
+        st._preprocess_image = lambda img: img
+        st._extract_features = lambda img: (kps, None, None)
+        st._match_features = lambda *a: dms
+        st._compute_homography = lambda *a: None
+        st._ransac = lambda p, q: (next(hs), np.ones(len(p), bool))
+        st._get_depth_estimator = lambda: None
+        warps = []
+        orig = st_cls._warp_image
+
+        def rec(img, H, cw, ch, ox, oy, _orig=orig):
+            w, m = _orig(img, H, cw, ch, ox, oy)
+            warps.append((w, m))
+            return w, m
+
+        st._warp_image = rec
+        pano, _, metrics = st._stitch_triple(img1, img2, img3)
+        cw, ch, ox, oy = st_cls._compute_canvas_size_3(img1, img2, img3, H12, H32)
+        iox, ioy = int(round(ox)), int(round(oy))
+        canvas2 = np.zeros((ch, cw, 3), np.uint8)
+        mask2 = np.zeros((ch, cw), bool)
+        ye, xe = min(ioy + img2.shape[0], ch), min(iox + img2.shape[1], cw)
+        canvas2[ioy:ye, iox:xe] = img2[:ye - ioy, :xe - iox]
+        mask2[ioy:ye, iox:xe] = True
+        names.append(name)
+        res.update({f"{name}_img1": img1, f"{name}_img2": img2, f"{name}_img3": img3, f"{name}_H12": H12,
+                    f"{name}_H32": H32, f"{name}_warped1": warps[0][0], f"{name}_mask1": warps[0][1],
+                    f"{name}_warped3": warps[1][0], f"{name}_mask3": warps[1][1], f"{name}_canvas2": canvas2,
+                    f"{name}_mask2": mask2, f"{name}_pano": pano,
+                    f"{name}_seam_rmse": np.float64(metrics["seam_rmse"]),
+                    f"{name}_seam_rmse_23": np.float64(metrics["seam_rmse_23"])})
+        print(name, "canvas", (cw, ch), "pano", pano.shape, "rmse", metrics["seam_rmse"], metrics["seam_rmse_23"])
+    res["names"] = np.array(names)
+    np.savez_compressed(os.path.join(out_dir, "triple_cases.npz"), **res)
+
+
 def main(ref_root, out_dir=HERE):
     sys.dont_write_bytecode = True
     _install_shims()
@@ -140,6 +210,7 @@ def main(ref_root, out_dir=HERE):
         print(name, pano.shape, "rmse", rmse)
     out["names"] = np.array(names)
     np.savez_compressed(os.path.join(out_dir, "blend_cases.npz"), **out)
+    run_triples(GPUPyStitch, out_dir)
 
 
 if __name__ == "__main__":

@@ -119,7 +119,8 @@ def test_blend_oracle_matches_reference_composition(faithful):
 
 @pytest.mark.skipif(not os.path.isfile(os.path.join(REF, "pysift", "core.py")), reason="reference tree absent")
 def test_blend_fixture_regenerates():
-    """The committed composition fixtures are what the reference produces now."""
+    """The committed composition fixtures (two- and three-image) are what the
+    reference produces now."""
     import subprocess
     import sys
     import tempfile
@@ -127,7 +128,32 @@ def test_blend_fixture_regenerates():
     with tempfile.TemporaryDirectory() as d:
         r = subprocess.run([sys.executable, src, REF, d], capture_output=True, text=True, timeout=600)
         assert r.returncode == 0, r.stderr[-2000:]
-        new = np.load(os.path.join(d, "blend_cases.npz"))
-        old = np.load(os.path.join(HERE, "golden", "blend_cases.npz"))
-        for k in old.files:
-            assert np.array_equal(new[k], old[k], equal_nan=k.endswith("seam_rmse")), k
+        for fname in ("blend_cases.npz", "triple_cases.npz"):
+            new = np.load(os.path.join(d, fname))
+            old = np.load(os.path.join(HERE, "golden", fname))
+            for k in old.files:
+                assert np.array_equal(new[k], old[k], equal_nan="seam_rmse" in k), (fname, k)
+
+
+def test_triple_composition_oracle_matches_reference():
+    """oracle/blend_oracle.py compose3 + the crop against the reference's own
+    _stitch_triple composition (tests/golden/make_blend_golden.py): bit-exact
+    with the reference's numpy means and cv2 blur; in the canonical form the
+    second pass's gain (a mean over float values, which numpy sums
+    sequentially in float32) moves at most a few values by one level."""
+    from oracle import blend_oracle as bo
+    from oracle import stitch_oracle as so
+    g = np.load(os.path.join(HERE, "golden", "triple_cases.npz"))
+    assert len(g["names"]) >= 2
+    for name in g["names"]:
+        args = [g[f"{name}_{k}"] for k in ("warped1", "mask1", "canvas2", "mask2", "warped3", "mask3")]
+        ref = g[f"{name}_pano"]
+        pano, both, r12, r23 = bo.compose3(*args, faithful=True)
+        assert np.array_equal(so.autocrop(pano, both), ref), name
+        pano, both, r12, r23 = bo.compose3(*args)
+        crop = so.autocrop(pano, both)
+        assert crop.shape == ref.shape
+        d = np.abs(crop.astype(int) - ref.astype(int))
+        assert d.max() <= 1 and (d > 0).mean() < 5e-4, (name, int((d > 0).sum()))
+        assert abs(r12 - float(g[f"{name}_seam_rmse"])) < 1e-5 * r12
+
