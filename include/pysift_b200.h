@@ -296,20 +296,29 @@ int pysift_warp_f32_backward(const float* img1, int32_t hs, int32_t ws, int32_t 
  * gain compensation, seam cost (colour difference + 0.05 |Sobel| of the
  * average gray), dynamic-programming seam along the longer overlap axis,
  * seam mask blurred with sigma 3 inside the overlap, Laplacian pyramid blend
- * of n_levels levels and the paste with uint8 truncation.  warped1 / canvas2:
- * cw x ch x 3 uint8 (BGR), masks: cw x ch bytes (0 / 1), all on the device.
- * seam_k25: the 25 float32 taps of the sigma-3 seam-mask blur (host);
- * gauss_w9: the 9 float64 taps of gaussian_filter(sigma = 1) (host).
- * Outputs: pano (cw x ch x 3, zero where neither image covers), optionally
- * both (union mask) and seam_rmse (one double on the device: the RMS colour
- * difference over the overlap after gain, NaN when there is no overlap). */
+ * of n_levels levels and the paste with uint8 truncation.  image1: cw x ch
+ * x 3, uint8 (image1_f32 = 0: the warped image) or float32 (image1_f32 = 1:
+ * the unclipped result of an earlier blend, as the second pass of a
+ * three-image stitch takes it, pysift/core.py:3931-3947); canvas2: cw x ch x
+ * 3 uint8; masks: cw x ch bytes (0 / 1); all on the device.  seam_k25: the 25
+ * float32 taps of the sigma-3 seam-mask blur (host); gauss_w9: the 9 float64
+ * taps of gaussian_filter(sigma = 1) (host).  Outputs (at least one of pano
+ * and blended): pano (cw x ch x 3 uint8, zero where neither image covers),
+ * blended (cw x ch x 3 float32, the blend before any clipping), both (union
+ * mask) and seam_rmse (one double on the device: the RMS colour difference
+ * over the overlap after gain, NaN when there is no overlap). */
 int pysift_place_image(const uint8_t* img, int32_t h, int32_t w, int32_t pitch, int32_t cw, int32_t ch, int32_t iox,
                        int32_t ioy, uint8_t* canvas, uint8_t* mask, pysift_stream_t stream);
 int pysift_blend_workspace_size(int32_t cw, int32_t ch, int32_t n_levels, size_t* bytes);
-int pysift_blend_multiband(const uint8_t* warped1, const uint8_t* mask1, const uint8_t* canvas2,
+int pysift_blend_multiband(const void* image1, int32_t image1_f32, const uint8_t* mask1, const uint8_t* canvas2,
                            const uint8_t* mask2, int32_t cw, int32_t ch, int32_t n_levels, const float* seam_k25,
                            const double* gauss_w9, void* workspace, size_t workspace_bytes, uint8_t* pano,
-                           uint8_t* both, double* seam_rmse, pysift_stream_t stream);
+                           uint8_t* both, float* blended, double* seam_rmse, pysift_stream_t stream);
+/* Per-row and per-column first / last set pixel of a cw x ch coverage mask
+ * (INT32_MAX / -1 where a line is empty): the inputs of the inner-rectangle
+ * crop (pysift/core.py:3627-3684). */
+int pysift_mask_extents(const uint8_t* mask, int32_t cw, int32_t ch, int32_t* row_lo, int32_t* row_hi,
+                        int32_t* col_lo, int32_t* col_hi, pysift_stream_t stream);
 
 /* Allocation-free 2x zoom (no counterpart in the reference; it exists for
  * callers that cannot allocate device memory at the call site, such as a

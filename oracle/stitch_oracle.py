@@ -205,3 +205,50 @@ class OracleStitch:
             out, _ = blend_oracle.blend_pair(warped, m1, canvas2, m2, self.n_blend_levels)
         pano = autocrop(out, m1 | m2)
         return dict(pano=pano, H=H, mask=mask, info=info, pairs=pairs, p1=p1, p2=p2, n1=len(pts1), n2=len(pts2))
+
+    def stitch3(self, img1, img2, img3):
+        """_stitch_triple (pysift/core.py:3820-3966) without depth: matches 1-2
+        and 2-3 (PCA fitted on the first pair), RANSAC 1->2 and 3->2, the
+        shared canvas, the two-pass composition (blend_oracle.compose3) and
+        the crop."""
+        from . import blend_oracle
+        pts1, d1, _ = self.features(img1)
+        pts2, d2, _ = self.features(img2)
+        pts3, d3, _ = self.features(img3)
+        ms = []
+        for da, db in ((d1, d2), (d2, d3)):
+            a, b = self.prepare(da, db)
+            ms.append(match_oracle.match_i8(a, b, self.match_ratio) if self.int8_matching
+                      else match_oracle.match_fp16(a, b, self.match_ratio))
+        p12, p23 = ms[0]["pairs"], ms[1]["pairs"]
+        pA, pB1 = pts1[p12[:, 0]].astype(np.float64), pts2[p12[:, 1]].astype(np.float64)
+        pB2, pC = pts2[p23[:, 0]].astype(np.float64), pts3[p23[:, 1]].astype(np.float64)
+        H12, _, info12, _ = ransac(pA, pB1, self.ransac_iters, self.inlier_thresh, self.inlier_thresh)
+        H32, _, info32, _ = ransac(pC, pB2, self.ransac_iters, self.inlier_thresh, self.inlier_thresh)
+        cw, ch, ox, oy = canvas_size3(img1.shape, img2.shape, img3.shape, H12, H32)
+        iox, ioy = int(round(ox)), int(round(oy))
+        _, w1, m1, m2 = warp_feather(img1, img2, np.linalg.inv(H12).astype(np.float32), cw, ch, ox, oy, iox, ioy)
+        _, w3, m3, _ = warp_feather(img3, img2, np.linalg.inv(H32).astype(np.float32), cw, ch, ox, oy, iox, ioy)
+        canvas2 = np.zeros((ch, cw, 3), np.uint8)
+        ye, xe = min(ioy + img2.shape[0], ch), min(iox + img2.shape[1], cw)
+        canvas2[ioy:ye, iox:xe] = img2[:ye - ioy, :xe - iox]
+        pano, both, r12, r23 = blend_oracle.compose3(w1, m1, canvas2, m2, w3, m3, self.n_blend_levels)
+        return dict(pano=autocrop(pano, both), H12=H12, H32=H32, pairs12=p12, pairs23=p23, info12=info12,
+                    info32=info32, rmse12=r12, rmse23=r23, canvas=(cw, ch))
+
+
+def canvas_size3(shape1, shape2, shape3, H12, H32):
+    """_compute_canvas_size_3 (pysift/core.py:3190-3208)."""
+    h2, w2 = shape2[:2]
+    xs, ys = [0.0, float(w2), float(w2), 0.0], [0.0, 0.0, float(h2), float(h2)]
+    for shp, H in ((shape1, H12), (shape3, H32)):
+        h, w = shp[:2]
+        c = np.array([[0, 0, 1], [w, 0, 1], [w, h, 1], [0, h, 1]], dtype=np.float64).T
+        wc = H @ c
+        wc /= wc[2]
+        xs.extend(wc[0].tolist())
+        ys.extend(wc[1].tolist())
+    ax, ay = np.array(xs), np.array(ys)
+    ox, oy = max(0.0, -ax.min()), max(0.0, -ay.min())
+    return int(np.ceil(ax.max() + ox)) + 1, int(np.ceil(ay.max() + oy)) + 1, ox, oy
+

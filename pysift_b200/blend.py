@@ -65,18 +65,24 @@ def place_image(img, cw, ch, iox, ioy, canvas=None, mask=None, stream=None):
     return canvas, mask
 
 
-def blend_multiband(warped1, mask1, canvas2, mask2, n_levels=6, workspace=None, pano=None, both=None,
-                    seam_rmse=None, stream=None):
-    """_blend_pair + paste: warped1 / canvas2 (ch, cw, 3) uint8 and the masks
-    (ch, cw) uint8 / bool on the device.  Returns (pano uint8 (ch, cw, 3),
-    both uint8 (ch, cw), seam_rmse float64 (1,)), all on the device and
-    enqueued on the current stream."""
+def blend_multiband(image1, mask1, canvas2, mask2, n_levels=6, workspace=None, pano=None, both=None,
+                    seam_rmse=None, blended=None, want_pano=True, stream=None):
+    """_blend_pair + paste.  image1: (ch, cw, 3) uint8 (a warped image) or
+    float32 (an earlier blend's unclipped result); canvas2: (ch, cw, 3)
+    uint8; masks (ch, cw) uint8 / bool; all on the device.  Returns (pano
+    uint8 (ch, cw, 3) or None, both uint8 (ch, cw), seam_rmse float64 (1,),
+    blended float32 (ch, cw, 3) or None), enqueued on the current stream;
+    pass a `blended` tensor to get the unclipped blend."""
     lib = _lib.load()
     ch, cw = mask1.shape
     dev = mask1.device
-    for t in (warped1, canvas2):
-        if t.shape != (ch, cw, 3) or t.dtype != torch.uint8 or not t.is_contiguous() or t.device != dev:
-            raise ValueError("warped1 / canvas2 must be contiguous (ch, cw, 3) uint8 on the masks' device")
+    f32 = image1.dtype == torch.float32
+    if image1.shape != (ch, cw, 3) or image1.dtype not in (torch.uint8, torch.float32) or \
+            not image1.is_contiguous() or image1.device != dev:
+        raise ValueError("image1 must be a contiguous (ch, cw, 3) uint8 or float32 tensor on the masks' device")
+    if canvas2.shape != (ch, cw, 3) or canvas2.dtype != torch.uint8 or not canvas2.is_contiguous() or \
+            canvas2.device != dev:
+        raise ValueError("canvas2 must be a contiguous (ch, cw, 3) uint8 tensor on the masks' device")
     m1 = mask1.view(torch.uint8) if mask1.dtype == torch.bool else mask1
     m2 = mask2.view(torch.uint8) if mask2.dtype == torch.bool else mask2
     if m1.dtype != torch.uint8 or m2.shape != (ch, cw) or not (m1.is_contiguous() and m2.is_contiguous()):
@@ -85,15 +91,33 @@ def blend_multiband(warped1, mask1, canvas2, mask2, n_levels=6, workspace=None, 
     if workspace is None or workspace.numel() < need + 256:
         workspace = torch.empty(need + 256, dtype=torch.uint8, device=dev)
     wp = workspace.data_ptr() + ((-workspace.data_ptr()) % 256)
-    if pano is None:
+    if pano is None and want_pano:
         pano = torch.empty((ch, cw, 3), dtype=torch.uint8, device=dev)
     if both is None:
         both = torch.empty((ch, cw), dtype=torch.uint8, device=dev)
     if seam_rmse is None:
         seam_rmse = torch.empty(1, dtype=torch.float64, device=dev)
+    if pano is None and blended is None:
+        raise ValueError("nothing to compute: want_pano=False and no blended tensor")
     st = stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
-    _lib.check(lib.pysift_blend_multiband(warped1.data_ptr(), m1.data_ptr(), canvas2.data_ptr(), m2.data_ptr(), cw,
-                                          ch, int(n_levels), _SEAM_K.ctypes.data, _GAUSS_W.ctypes.data, wp, need,
-                                          pano.data_ptr(), both.data_ptr(), seam_rmse.data_ptr(), st),
+    _lib.check(lib.pysift_blend_multiband(image1.data_ptr(), 1 if f32 else 0, m1.data_ptr(), canvas2.data_ptr(),
+                                          m2.data_ptr(), cw, ch, int(n_levels), _SEAM_K.ctypes.data,
+                                          _GAUSS_W.ctypes.data, wp, need, pano.data_ptr() if pano is not None else None,
+                                          both.data_ptr(), blended.data_ptr() if blended is not None else None,
+                                          seam_rmse.data_ptr(), st),
                "pysift_blend_multiband")
-    return pano, both, seam_rmse
+    return pano, both, seam_rmse, blended
+
+
+def mask_extents(mask, out=None, stream=None):
+    """Per-row / per-column first and last set pixel of a (ch, cw) uint8 mask
+    on the device: int32 (2 ch + 2 cw,) = row_lo, row_hi, col_lo, col_hi."""
+    lib = _lib.load()
+    ch, cw = mask.shape
+    if out is None:
+        out = torch.empty(2 * ch + 2 * cw, dtype=torch.int32, device=mask.device)
+    st = stream if stream is not None else torch.cuda.current_stream(mask.device).cuda_stream
+    _lib.check(lib.pysift_mask_extents(mask.data_ptr(), cw, ch, out.data_ptr(), out[ch:].data_ptr(),
+                                       out[2 * ch:].data_ptr(), out[2 * ch + cw:].data_ptr(), st),
+               "pysift_mask_extents")
+    return out

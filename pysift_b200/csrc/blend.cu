@@ -62,17 +62,34 @@ __device__ __forceinline__ int warp_or(int v) {
     return v;
 }
 
-// Per pixel: overlap sums (exact) and line flags per row and column
+// Image 1 of a blend: a uint8 canvas (the warped image) or a float32 one (the
+// unclipped result of an earlier blend, as the second pass of a three-image
+// stitch takes it, pysift/core.py:3931-3947).
+struct Img1 {
+    const uint8_t* u8;
+    const float* f32;
+    __device__ __forceinline__ float at(long long p, int c) const {
+        return f32 ? f32[p * 3 + c] : (float)u8[p * 3 + c];
+    }
+};
+
+// image-1 values for the gain means: rounded to multiples of 2^-24 (exact for
+// uint8) and summed as 64-bit integers, an order-free sum
+__device__ __forceinline__ long long fixed24(float v) { return __double2ll_rn((double)v * 16777216.0); }
+
+// Per pixel: overlap sums (order-free) and line flags per row and column
 // (bit 0 overlap, bit 1 image 1 only, bit 2 image 2 only).  One row per block.
-__global__ void __launch_bounds__(256) k_blend_stats(const uint8_t* __restrict__ w1, const uint8_t* __restrict__ m1,
+__global__ void __launch_bounds__(256) k_blend_stats(const Img1 w1, const uint8_t* __restrict__ m1,
                                                      const uint8_t* __restrict__ c2, const uint8_t* __restrict__ m2,
                                                      int cw, BlendCtl* ctl, int* __restrict__ rowf,
                                                      int* __restrict__ colf, int* __restrict__ rlo,
                                                      int* __restrict__ rhi, int* __restrict__ clo,
                                                      int* __restrict__ chi) {
     __shared__ unsigned int s[7];
+    __shared__ unsigned long long s1[3];
     __shared__ int s_or, s_lo, s_hi;
     if (threadIdx.x < 7) s[threadIdx.x] = 0u;
+    if (threadIdx.x < 3) s1[threadIdx.x] = 0ull;
     if (threadIdx.x == 0) {
         s_or = 0;
         s_lo = 0x7fffffff;
@@ -81,7 +98,8 @@ __global__ void __launch_bounds__(256) k_blend_stats(const uint8_t* __restrict__
     __syncthreads();
     const int v = blockIdx.y;
     int f_row = 0, lo = 0x7fffffff, hi = -1;
-    unsigned int acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    unsigned int acc[7] = {0, 0, 0, 0, 0, 0, 0};  // [3..5]: image 2, [6]: count
+    long long acc1[3] = {0, 0, 0};               // image 1, fixed point 2^-24
     for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < cw; u += gridDim.x * blockDim.x) {
         const long long p = (long long)v * cw + u;
         const bool a = m1[p] != 0, b = m2[p] != 0;
@@ -91,7 +109,7 @@ __global__ void __launch_bounds__(256) k_blend_stats(const uint8_t* __restrict__
         if (a && b) {
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                acc[c] += w1[p * 3 + c];
+                acc1[c] += fixed24(w1.at(p, c));
                 acc[3 + c] += c2[p * 3 + c];
             }
             acc[6] += 1u;
@@ -112,12 +130,16 @@ __global__ void __launch_bounds__(256) k_blend_stats(const uint8_t* __restrict__
         atomicMax(&s_hi, hi);
     }
 #pragma unroll
-    for (int k = 0; k < 7; ++k) acc[k] = warp_sum(acc[k]);
+    for (int k = 3; k < 7; ++k) acc[k] = warp_sum(acc[k]);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) acc1[k] = warp_sum(acc1[k]);
     if ((threadIdx.x & 31) == 0) {
         if (f_row) atomicOr(&s_or, f_row);
         if (acc[6]) {
 #pragma unroll
-            for (int k = 0; k < 7; ++k) atomicAdd(&s[k], acc[k]);
+            for (int k = 3; k < 7; ++k) atomicAdd(&s[k], acc[k]);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) atomicAdd(&s1[k], (unsigned long long)acc1[k]);
         }
     }
     __syncthreads();
@@ -128,7 +150,7 @@ __global__ void __launch_bounds__(256) k_blend_stats(const uint8_t* __restrict__
         if (s[6]) {
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                atomicAdd(&ctl->sum1[c], (unsigned long long)s[c]);
+                atomicAdd(&ctl->sum1[c], s1[c]);
                 atomicAdd(&ctl->sum2[c], (unsigned long long)s[3 + c]);
             }
             atomicAdd(&ctl->n_ov, (unsigned long long)s[6]);
@@ -190,7 +212,7 @@ __global__ void __launch_bounds__(1024) k_blend_decide(BlendCtl* ctl, const int*
         for (int k = 0; k < 3; ++k) {
             float g = 1.0f;
             if (n > 0) {
-                const float mean1 = (float)((double)ctl->sum1[k] / (double)n);
+                const float mean1 = (float)(((double)(long long)ctl->sum1[k] / 16777216.0) / (double)n);
                 const float mean2 = (float)((double)ctl->sum2[k] / (double)n);
                 g = (mean2 + 1e-3f) / (mean1 + 1e-3f);
                 g = g < 0.5f ? 0.5f : (g > 2.0f ? 2.0f : g);
@@ -227,7 +249,7 @@ __global__ void __launch_bounds__(1024) k_blend_decide(BlendCtl* ctl, const int*
 // at one pixel, from the uint8 canvases; the level-0 passes recompute them
 // instead of storing two float images
 struct Level0 {
-    const uint8_t* w1;
+    Img1 w1;
     const uint8_t* m1;
     const uint8_t* c2;
     const uint8_t* m2;
@@ -237,7 +259,7 @@ struct Level0 {
         const bool gained = ctl->have_ov != 0;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            float x = (float)w1[p * 3 + c];
+            float x = w1.at(p, c);
             if (gained) {
                 x = x * ctl->gain[c];
                 x = x < 0.0f ? 0.0f : (x > 255.0f ? 255.0f : x);
@@ -251,7 +273,7 @@ struct Level0 {
 
 // colour cost, average gray (pysift/core.py:3411-3415) and the seam-RMSE sum
 // (pysift/core.py:3555-3562) of the gained image 1
-__global__ void k_blend_prepare(const uint8_t* __restrict__ w1, const uint8_t* __restrict__ m1,
+__global__ void k_blend_prepare(const Img1 w1, const uint8_t* __restrict__ m1,
                                 const uint8_t* __restrict__ c2, const uint8_t* __restrict__ m2, int cw,
                                 BlendCtl* ctl, float* __restrict__ color, float* __restrict__ avg) {
     const int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
@@ -263,7 +285,7 @@ __global__ void k_blend_prepare(const uint8_t* __restrict__ w1, const uint8_t* _
         float g1[3], g2[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            float x = (float)w1[p * 3 + c];
+            float x = w1.at(p, c);
             if (gained) {
                 x = x * ctl->gain[c];
                 x = x < 0.0f ? 0.0f : (x > 255.0f ? 255.0f : x);
@@ -798,7 +820,7 @@ __global__ void k_blend_reconstruct(const float* __restrict__ res, int hn, int w
 __global__ void k_blend_final(const Level0 src, const float* __restrict__ gm0, const float* __restrict__ g1n,
                               const float* __restrict__ g2n, const float* __restrict__ res, int hn, int wn, int H,
                               int W, ZoomF zf, uint8_t* __restrict__ pano, uint8_t* __restrict__ both,
-                              double* __restrict__ seam_rmse) {
+                              float* __restrict__ blended, double* __restrict__ seam_rmse) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x == 0 && y == 0 && seam_rmse) {
         const BlendCtl* ctl = src.ctl;
@@ -827,10 +849,58 @@ __global__ void k_blend_final(const Level0 src, const float* __restrict__ gm0, c
 #pragma unroll
         for (int c = 0; c < 3; ++c) v[c] = m * i1[c] + mc * i2[c];
     }
+    if (blended) {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        const float t = v[c] < 0.0f ? 0.0f : (v[c] > 255.0f ? 255.0f : v[c]);
-        pano[p * 3 + c] = any ? (uint8_t)(int)t : (uint8_t)0;
+        for (int c = 0; c < 3; ++c) blended[p * 3 + c] = v[c];
+    }
+    if (pano) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const float t = v[c] < 0.0f ? 0.0f : (v[c] > 255.0f ? 255.0f : v[c]);
+            pano[p * 3 + c] = any ? (uint8_t)(int)t : (uint8_t)0;
+        }
+    }
+}
+
+__global__ void k_fill_i32(int* __restrict__ p, int n, int v) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
+// per-row and per-column extents of a coverage mask (the inner-rectangle
+// crop's inputs, pysift/core.py:3655-3675); one row per block
+__global__ void __launch_bounds__(256) k_mask_extents(const uint8_t* __restrict__ mask, int cw, int* __restrict__ row_lo,
+                                                      int* __restrict__ row_hi, int* __restrict__ col_lo,
+                                                      int* __restrict__ col_hi) {
+    __shared__ int s_lo, s_hi;
+    if (threadIdx.x == 0) {
+        s_lo = 0x7fffffff;
+        s_hi = -1;
+    }
+    __syncthreads();
+    const int v = blockIdx.y;
+    int lo = 0x7fffffff, hi = -1;
+    for (int u = threadIdx.x; u < cw; u += blockDim.x) {
+        if (mask[(long long)v * cw + u]) {
+            lo = min(lo, u);
+            hi = max(hi, u);
+            atomicMin(&col_lo[u], v);
+            atomicMax(&col_hi[u], v);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if ((threadIdx.x & 31) == 0 && hi >= 0) {
+        atomicMin(&s_lo, lo);
+        atomicMax(&s_hi, hi);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        row_lo[v] = s_lo;
+        row_hi[v] = s_hi;
     }
 }
 
@@ -973,12 +1043,27 @@ int pysift_blend_workspace_size(int32_t cw, int32_t ch, int32_t n_levels, size_t
     return PYSIFT_OK;
 }
 
-int pysift_blend_multiband(const uint8_t* warped1, const uint8_t* mask1, const uint8_t* canvas2,
+int pysift_mask_extents(const uint8_t* mask, int32_t cw, int32_t ch, int32_t* row_lo, int32_t* row_hi,
+                        int32_t* col_lo, int32_t* col_hi, pysift_stream_t stream) {
+    PYSIFT_CHECK_ARG(mask && row_lo && row_hi && col_lo && col_hi, "NULL pointer argument");
+    PYSIFT_CHECK_ARG(cw > 0 && ch > 0, "bad sizes");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    k_fill_i32<<<ceil_div(cw, 256), 256, 0, st>>>(col_lo, cw, 0x7fffffff);
+    PYSIFT_CUDA_TRY(cudaMemsetAsync(col_hi, 0xff, (size_t)cw * 4, st));
+    k_mask_extents<<<dim3(1, ch), 256, 0, st>>>(mask, cw, row_lo, row_hi, col_lo, col_hi);
+    PYSIFT_LAUNCH_CHECK("k_mask_extents");
+    return PYSIFT_OK;
+}
+
+int pysift_blend_multiband(const void* image1, int32_t image1_f32, const uint8_t* mask1, const uint8_t* canvas2,
                            const uint8_t* mask2, int32_t cw, int32_t ch, int32_t n_levels, const float* seam_k25,
                            const double* gauss_w9, void* workspace, size_t workspace_bytes, uint8_t* pano,
-                           uint8_t* both, double* seam_rmse, pysift_stream_t stream) {
-    PYSIFT_CHECK_ARG(warped1 && mask1 && canvas2 && mask2 && seam_k25 && gauss_w9 && workspace && pano,
+                           uint8_t* both, float* blended, double* seam_rmse, pysift_stream_t stream) {
+    PYSIFT_CHECK_ARG(image1 && mask1 && canvas2 && mask2 && seam_k25 && gauss_w9 && workspace && (pano || blended),
                      "NULL pointer argument");
+    Img1 w1;
+    w1.u8 = image1_f32 ? nullptr : static_cast<const uint8_t*>(image1);
+    w1.f32 = image1_f32 ? static_cast<const float*>(image1) : nullptr;
     PYSIFT_CHECK_ARG(cw > 1 && ch > 1 && n_levels >= 1 && n_levels <= 8, "bad sizes");
     const BlendLayout l = blend_layout(cw, ch, n_levels);
     if (workspace_bytes < l.total) {
@@ -1005,14 +1090,13 @@ int pysift_blend_multiband(const uint8_t* warped1, const uint8_t* mask1, const u
     PYSIFT_CUDA_TRY(cudaMemcpyAsync(k25, seam_k25, 25 * sizeof(float), cudaMemcpyHostToDevice, st));
     const dim3 g2d(ceil_div(cw, 256), ch);
     // gain, overlap flags and ranges, seam orientation
-    k_blend_stats<<<dim3(1, ch), 256, 0, st>>>(warped1, mask1, canvas2, mask2, cw, ctl, rowf, colf, rlo, rhi, clo,
-                                                chi);
+    k_blend_stats<<<dim3(1, ch), 256, 0, st>>>(w1, mask1, canvas2, mask2, cw, ctl, rowf, colf, rlo, rhi, clo, chi);
     PYSIFT_LAUNCH_CHECK("k_blend_stats");
     k_blend_decide<<<1, 1024, 0, st>>>(ctl, rowf, colf, cw, ch);
     PYSIFT_LAUNCH_CHECK("k_blend_decide");
     // Gaussian pyramids of I1 and I2 on a side stream: they need only the gain
     Level0 src;
-    src.w1 = warped1;
+    src.w1 = w1;
     src.m1 = mask1;
     src.c2 = canvas2;
     src.m2 = mask2;
@@ -1046,7 +1130,7 @@ int pysift_blend_multiband(const uint8_t* warped1, const uint8_t* mask1, const u
     float* color = bwp<float>(ws, l.off_color);
     float* avg = bwp<float>(ws, l.off_avg);
     float* dpc = bwp<float>(ws, l.off_dpc);
-    k_blend_prepare<<<g2d, 256, 0, st>>>(warped1, mask1, canvas2, mask2, cw, ctl, color, avg);
+    k_blend_prepare<<<g2d, 256, 0, st>>>(w1, mask1, canvas2, mask2, cw, ctl, color, avg);
     PYSIFT_LAUNCH_CHECK("k_blend_prepare");
     k_sobel_cost<<<g2d, 256, 0, st>>>(avg, color, mask1, mask2, ctl, dpc, cw, ch);
     PYSIFT_LAUNCH_CHECK("k_sobel_cost");
@@ -1141,7 +1225,7 @@ int pysift_blend_multiband(const uint8_t* warped1, const uint8_t* mask1, const u
     // level 0: Laplacian blend, last reconstruction step and paste
     k_blend_final<<<g2d, 256, 0, st>>>(src, gm0, n_levels > 1 ? bwp<float>(ws, l.off_g1[1]) : nullptr,
                                        n_levels > 1 ? bwp<float>(ws, l.off_g2[1]) : nullptr, res, rh, rw, ch, cw,
-                                       zoom_factors(rh, rw, ch, cw), pano, both, seam_rmse);
+                                       zoom_factors(rh, rw, ch, cw), pano, both, blended, seam_rmse);
     PYSIFT_LAUNCH_CHECK("k_blend_final");
     return PYSIFT_OK;
 }

@@ -46,8 +46,8 @@ class GPUPyStitch:
     """Panorama stitcher with the reference's constructor (pysift/core.py:2429-2445).
 
     Not thread-safe (per-instance buffers and the cached PCA basis, like the
-    reference).  Two images are supported; three-image stitching, depth-aware
-    warps, learned features and LightGlue raise NotImplementedError.
+    reference).  Two and three images are supported; depth-aware warps,
+    learned features and LightGlue raise NotImplementedError.
     """
 
     def __init__(self, n_depth_layers=4, n_blend_levels=6, ransac_iters=1500, inlier_thresh=5.0,
@@ -459,6 +459,138 @@ class GPUPyStitch:
         self._last = dict(H=H, mask=mask_d, pairs=m["pairs"][:n_m], kp1=kp1, kp2=kp2, p1=p1, p2=p2, info=info)
         return pano, timings, metrics
 
+    @staticmethod
+    def _compute_canvas_size_3(img1_shape, img2_shape, img3_shape, H12, H32):
+        """pysift/core.py:3190-3208 (float64, host)."""
+        h2, w2 = img2_shape[:2]
+        all_x = [0.0, float(w2), float(w2), 0.0]
+        all_y = [0.0, 0.0, float(h2), float(h2)]
+        for shp, H in ((img1_shape, H12), (img3_shape, H32)):
+            h, w = shp[:2]
+            c = np.array([[0, 0, 1], [w, 0, 1], [w, h, 1], [0, h, 1]], dtype=np.float64).T
+            wc = H @ c
+            wc /= wc[2]
+            all_x.extend(wc[0].tolist())
+            all_y.extend(wc[1].tolist())
+        ax, ay = np.array(all_x), np.array(all_y)
+        ox = max(0.0, -ax.min())
+        oy = max(0.0, -ay.min())
+        return int(np.ceil(ax.max() + ox)) + 1, int(np.ceil(ay.max() + oy)) + 1, ox, oy
+
+    def _warp_to_canvas(self, img, H, ref, cw, ch, ox, oy, key):
+        """Warped uint8 image and mask of `img` on the canvas (the warp of
+        pysift/core.py:3210-3239); `ref` is the reference view the kernel
+        places (its outputs are not used here)."""
+        hs, ws = img.shape[:2]
+        hinv = np.linalg.inv(H).astype(np.float32).ravel()
+        hb = (ctypes.c_float * 9)(*[float(v) for v in hinv])
+        warped = self._dev.get(key + "warped", (ch, cw, 3), torch.uint8, self.device)
+        mask = self._dev.get(key + "mask", (ch, cw), torch.uint8, self.device)
+        _lib.check(self._lib.pysift_warp_feather(img.data_ptr(), hs, ws, img.stride(0), ref.data_ptr(), ref.shape[0],
+                                                 ref.shape[1], ref.stride(0), cw, ch, ctypes.cast(hb, ctypes.c_void_p),
+                                                 float(np.float32(ox)), float(np.float32(oy)), int(round(ox)),
+                                                 int(round(oy)), 0, None, warped.data_ptr(), mask.data_ptr(), None,
+                                                 None, None, None, None, self._stream()), "pysift_warp_feather")
+        return warped, mask
+
+    def _stitch_triple(self, img1, img2, img3):
+        """pysift/core.py:3820-3966 (three images, img2 is the reference
+        frame): features of all three views, matches 1-2 and 2-3 (the PCA
+        basis fitted on the first pair), RANSAC 1->2 and 3->2, one canvas,
+        then the two-pass composition: image 1 blended with image 2, the
+        unclipped float result blended with image 3, paste and crop."""
+        if self.blend != 'multiband':
+            raise NotImplementedError("three-image stitching composes with the reference's multiband blend only")
+        from . import blend as _blend
+        timings, metrics = {}, {}
+        with torch.cuda.device(self.device):
+            t0 = time.perf_counter()
+            main = torch.cuda.current_stream(self.device)
+            if self._side is None:
+                self._side = (torch.cuda.Stream(self.device), torch.cuda.Stream(self.device))
+            if not hasattr(self, "_side3"):
+                self._side3 = torch.cuda.Stream(self.device)
+            streams = (self._side[0], self._side[1], self._side3)
+            for s_ in streams:
+                s_.wait_stream(main)
+            views = [self._detect_view(img, f"img{i + 1}", i, s_) for i, (img, s_) in
+                     enumerate(zip((img1, img2, img3), streams))]
+            for s_ in streams:
+                s_.synchronize()
+                main.wait_stream(s_)
+            (g1, b1), (g2, b2), (g3, b3) = views
+            kp1, d1, n1 = self._select(b1, "img1")
+            kp2, d2, n2 = self._select(b2, "img2")
+            kp3, d3, n3 = self._select(b3, "img3")
+            metrics.update(kp1=n1, kp2=n2, kp3=n3)
+            if min(n1, n2, n3) < 2:
+                raise RuntimeError("Insufficient matches for 3-image stitching")
+            m12 = self._match_prepared(self._prepare(d1, d2))
+            m23 = self._match_prepared(self._prepare(d2, d3))
+            c12, c23 = (int(v) for v in torch.cat([m12["count"], m23["count"]]).cpu().numpy())
+            metrics.update(matches_12=c12, matches_23=c23)
+            timings['st1'] = time.perf_counter() - t0
+            if c12 < 4 or c23 < 4:
+                raise RuntimeError("Insufficient matches for 3-image stitching")
+            st = self._stream()
+
+            def gather(kp, m, n, side):
+                p = torch.empty((n, 2), dtype=torch.float64, device=self.device)
+                _lib.check(self._lib.pysift_gather_points(kp.data_ptr(), m["pairs"].data_ptr(), m["count"].data_ptr(),
+                                                          n, side, p.data_ptr(), st), "gather")
+                return p
+
+            pA, pB1 = gather(kp1, m12, c12, 0), gather(kp2, m12, c12, 1)
+            pB2, pC = gather(kp2, m23, c23, 0), gather(kp3, m23, c23, 1)
+            timings['st2'] = 0.0
+            t0 = time.perf_counter()
+            H12_d, _, info12 = self._ransac(pA, pB1, c12, key="t12_")
+            H32_d, _, info32 = self._ransac(pC, pB2, c23, key="t32_")
+            Hs = torch.stack([H12_d, H32_d]).cpu().numpy().reshape(2, 3, 3)
+            infos = torch.stack([info12, info32]).cpu().numpy()
+            H12, H32 = Hs[0].copy(), Hs[1].copy()
+            timings['st3'] = time.perf_counter() - t0
+            metrics.update(inliers_12=int(infos[0][0]), inliers_32=int(infos[1][0]))
+            if min(int(infos[0][0]), int(infos[1][0])) < 4:
+                raise RuntimeError("Too few inliers for 3-image stitching")
+            timings['st4'] = 0.0
+            metrics.update(depth_cv=None, bands=self.n_depth_layers)
+            t0 = time.perf_counter()
+            cw, ch, ox, oy = self._compute_canvas_size_3(g1.shape, g2.shape, g3.shape, H12, H32)
+            if cw * ch > 400_000_000 or cw <= 1 or ch <= 1:
+                raise RuntimeError(f"degenerate homography: canvas {cw}x{ch}")
+            w1, mk1 = self._warp_to_canvas(g1, H12, g2, cw, ch, ox, oy, "t1_")
+            w3, mk3 = self._warp_to_canvas(g3, H32, g2, cw, ch, ox, oy, "t3_")
+            canvas2 = self._dev.get("t2_canvas", (ch, cw, 3), torch.uint8, self.device)
+            mk2 = self._dev.get("t2_mask", (ch, cw), torch.uint8, self.device)
+            _lib.check(self._lib.pysift_place_image(g2.data_ptr(), g2.shape[0], g2.shape[1], g2.stride(0), cw, ch,
+                                                    int(round(ox)), int(round(oy)), canvas2.data_ptr(),
+                                                    mk2.data_ptr(), st), "pysift_place_image")
+            need = _blend.workspace_bytes(cw, ch, self.n_blend_levels) + 256
+            wsb = self._dev.get("t_blend_ws", (need,), torch.uint8, self.device)
+            b12 = self._dev.get("t_b12", (ch, cw, 3), torch.float32, self.device)
+            m12u = self._dev.get("t_m12", (ch, cw), torch.uint8, self.device)
+            r12 = self._dev.get("t_r12", (1,), torch.float64, self.device)
+            _blend.blend_multiband(w1, mk1, canvas2, mk2, self.n_blend_levels, workspace=wsb, both=m12u,
+                                   seam_rmse=r12, blended=b12, want_pano=False, stream=st)
+            pano = self._dev.get("t_pano", (ch, cw, 3), torch.uint8, self.device)
+            both = self._dev.get("t_both", (ch, cw), torch.uint8, self.device)
+            r23 = self._dev.get("t_r23", (1,), torch.float64, self.device)
+            _blend.blend_multiband(b12, m12u, w3, mk3, self.n_blend_levels, workspace=wsb, pano=pano, both=both,
+                                   seam_rmse=r23, stream=st)
+            ext = _blend.mask_extents(both, out=self._dev.get("t_ext", (2 * ch + 2 * cw,), torch.int32, self.device),
+                                      stream=st)
+            e = ext.cpu().numpy()
+            rmse = torch.cat([r12, r23]).cpu().numpy()
+            crop = self._compose_crop(dict(out=pano, canvas_w=cw, canvas_h=ch, ext_host=torch.from_numpy(e)))
+            pano_h = self._to_host(crop)
+            timings['st5'] = time.perf_counter() - t0
+            metrics.update(seam_rmse=float(rmse[0]), seam_rmse_23=float(rmse[1]), canvas_w=cw, canvas_h=ch)
+        self._last = dict(H12=H12, H32=H32, info12=infos[0], info32=infos[1], pairs12=m12["pairs"][:c12],
+                          pairs23=m23["pairs"][:c23], warped1=w1, mask1=mk1, warped3=w3, mask3=mk3, canvas2=canvas2,
+                          mask2=mk2, ox=ox, oy=oy)
+        return pano_h, timings, metrics
+
     def _side_streams(self, n):
         if not hasattr(self, "_batch_streams"):
             self._batch_streams = []
@@ -576,22 +708,29 @@ class GPUPyStitch:
         return [h.numpy() for h in hosts]
 
     def stitch(self, *args):
-        """Stitch two images (pysift/core.py:3972-4008); returns the BGR uint8
+        """Stitch two or three images (pysift/core.py:3972-4008; with three, the
+        middle one is the reference frame); returns the BGR uint8
         panorama and, as the reference does, writes panorama_<ts>.png to the
         working directory unless the instance was built with save_output=False."""
         if len(args) == 1 and isinstance(args[0], (list, tuple)):
             images = list(args[0])
         else:
             images = list(args)
-        if len(images) == 3:
-            raise NotImplementedError("3-image stitching is not implemented on this backend")
-        if len(images) != 2:
+        if len(images) == 2:
+            pano, timings, metrics = self._stitch_pair(images[0], images[1])
+        elif len(images) == 3:
+            pano, timings, metrics = self._stitch_triple(images[0], images[1], images[2])
+        else:
             raise ValueError(f"stitch() accepts 2 or 3 images, got {len(images)}")
-        pano, timings, metrics = self._stitch_pair(images[0], images[1])
         self.last_timings, self.last_metrics = timings, metrics
         if self.verbose:
-            print(f"[pysift_b200] kp {metrics['kp1']}/{metrics['kp2']}  matches {metrics['matches']}  "
-                  f"inliers {metrics['inliers']}  canvas {metrics['canvas_w']}x{metrics['canvas_h']}")
+            if len(images) == 2:
+                print(f"[pysift_b200] kp {metrics['kp1']}/{metrics['kp2']}  matches {metrics['matches']}  "
+                      f"inliers {metrics['inliers']}  canvas {metrics['canvas_w']}x{metrics['canvas_h']}")
+            else:
+                print(f"[pysift_b200] kp {metrics['kp1']}/{metrics['kp2']}/{metrics['kp3']}  matches "
+                      f"{metrics['matches_12']}/{metrics['matches_23']}  inliers {metrics['inliers_12']}/"
+                      f"{metrics['inliers_32']}  canvas {metrics['canvas_w']}x{metrics['canvas_h']}")
         if self.save_output:
             import cv2
             ts = datetime.now().strftime("%Y%m%d_%H%M%S")

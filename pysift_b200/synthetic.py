@@ -137,6 +137,29 @@ def stitch_pair_fast(H=960, W=1280, seed=0):
     return img1, img2, Hm
 
 
+def stitch_triple(H=480, W=640, seed=0):
+    """Three overlapping BGR uint8 views (left, centre, right) of one scene and
+    the true homographies view1 -> view2 and view3 -> view2 (view 2, the
+    centre, is the reference frame of a three-image stitch)."""
+    import cv2
+    rng = _rng(seed)
+    Ha = random_homography(rng, W, H)          # view1 -> view2
+    Hb = random_homography(rng, W, H)          # view2 -> view3
+    big_w, big_h = int(W * 2.9), int(H * 1.5)
+    oy = (big_h - H) // 2
+    gains = rng.uniform(0.8, 1.2, size=3).astype(np.float32)
+    base = scene_fast(big_h, big_w, seed=int(rng.integers(0, 2**31 - 1))).astype(np.float32)
+    big = np.clip(base[:, :, None] * gains[None, None, :], 0, 255).astype(np.float32)
+    S = np.array([[1, 0, 0], [0, 1, -oy], [0, 0, 1]], np.float64)   # scene -> view1
+    v1 = big[oy:oy + H, :W]
+    v2 = cv2.warpPerspective(big, Ha @ S, (W, H), flags=cv2.INTER_LINEAR, borderMode=cv2.BORDER_REFLECT)
+    v3 = cv2.warpPerspective(big, Hb @ Ha @ S, (W, H), flags=cv2.INTER_LINEAR, borderMode=cv2.BORDER_REFLECT)
+    imgs = [np.clip(np.rint(v + 2.0 * rng.standard_normal(v.shape, dtype=np.float32)), 0, 255).astype(np.uint8)
+            for v in (v1, v2, v3)]
+    H32 = np.linalg.inv(Hb)
+    return imgs[0], imgs[1], imgs[2], Ha, H32 / H32[2, 2]
+
+
 def pair_sizes(n=32, seed=0):
     """Uneven stitch-pair sizes between 1280x960 and 3000x2000 (aspect 4:3 or 3:2)."""
     rng = _rng(seed + 7)

@@ -18,7 +18,7 @@ def _run(w1, m1, c2, m2, n_levels=6):
     import torch
     from pysift_b200 import blend
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
-    pano, both, rmse = blend.blend_multiband(t(w1), t(m1.astype(np.uint8)), t(c2), t(m2.astype(np.uint8)), n_levels)
+    pano, both, rmse, _ = blend.blend_multiband(t(w1), t(m1.astype(np.uint8)), t(c2), t(m2.astype(np.uint8)), n_levels)
     torch.cuda.synchronize()
     return pano.cpu().numpy(), both.cpu().numpy().astype(bool), float(rmse.cpu()[0])
 
@@ -202,3 +202,68 @@ def test_stitch_multiband_end_to_end():
     if pano.shape == orc["pano"].shape:
         diff = np.abs(pano.astype(int) - orc["pano"].astype(int))
         assert np.mean(diff <= 1) > 0.98
+
+
+TRIPLES = os.path.join(os.path.dirname(__file__), "golden", "triple_cases.npz")
+
+
+def test_float_image_blend_and_triple_composition():
+    """The two-pass composition of _stitch_triple on the reference's own
+    canvases: pass 1's unclipped float blend equals the oracle's float32
+    output bit for bit, pass 2 (float image 1) gives the oracle's panorama,
+    and after the crop the reference's own panorama within one level on a
+    few values (the second pass's float gain mean)."""
+    import torch
+    from oracle import blend_oracle as bo
+    from oracle import stitch_oracle as so
+    from pysift_b200 import blend
+    g = np.load(TRIPLES)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    for name in g["names"]:
+        w1, m1, c2, m2, w3, m3 = (g[f"{name}_{k}"] for k in ("warped1", "mask1", "canvas2", "mask2", "warped3",
+                                                             "mask3"))
+        ch, cw = m1.shape
+        b12 = torch.empty((ch, cw, 3), dtype=torch.float32, device="cuda")
+        _, m12, r12, _ = blend.blend_multiband(t(w1), t(m1.astype(np.uint8)), t(c2), t(m2.astype(np.uint8)),
+                                               blended=b12, want_pano=False)
+        ref_b12, ref_m12, ref_r12 = bo.blend_core(w1.astype(np.float32), m1, c2.astype(np.float32), m2)
+        assert np.array_equal(b12.cpu().numpy(), ref_b12)
+        assert np.array_equal(m12.cpu().numpy().astype(bool), ref_m12)
+        pano, both, r23, _ = blend.blend_multiband(b12, m12, t(w3), t(m3.astype(np.uint8)))
+        torch.cuda.synchronize()
+        ref_pano, ref_both, _, ref_r23 = bo.compose3(w1, m1, c2, m2, w3, m3)
+        assert np.array_equal(pano.cpu().numpy(), ref_pano)
+        assert np.array_equal(both.cpu().numpy().astype(bool), ref_both)
+        assert abs(float(r12.cpu()[0]) - ref_r12) < 1e-12 and abs(float(r23.cpu()[0]) - ref_r23) < 1e-12
+        ext = blend.mask_extents(both).cpu().numpy()
+        bb = ref_both
+        rows_lo = np.where(bb.any(1), bb.argmax(1), 0x7fffffff)
+        rows_hi = np.where(bb.any(1), cw - 1 - bb[:, ::-1].argmax(1), -1)
+        cols_lo = np.where(bb.any(0), bb.argmax(0), 0x7fffffff)
+        cols_hi = np.where(bb.any(0), ch - 1 - bb[::-1, :].argmax(0), -1)
+        assert np.array_equal(ext, np.concatenate([rows_lo, rows_hi, cols_lo, cols_hi]).astype(np.int32))
+        crop = so.autocrop(pano.cpu().numpy(), ref_both)
+        d = np.abs(crop.astype(int) - g[f"{name}_pano"].astype(int))
+        assert d.max() <= 1 and (d > 0).mean() < 5e-4
+
+
+@pytest.mark.parametrize("int8", [False, True])
+def test_stitch_three_images_end_to_end(int8):
+    """GPUPyStitch.stitch(img1, img2, img3) against the oracle's
+    _stitch_triple restatement: the same matches, homographies and panorama."""
+    from oracle import stitch_oracle as so
+    from pysift_b200.stitch import GPUPyStitch
+    a, b, c, H12, H32 = synthetic.stitch_triple(360, 480, seed=1)
+    st = GPUPyStitch(ransac_iters=1024, inlier_thresh=4.0, save_output=False, verbose=False, int8_matching=int8)
+    pano = st.stitch(a, b, c)
+    orc = so.OracleStitch(ransac_iters=1024, inlier_thresh=4.0, int8_matching=int8).stitch3(a, b, c)
+    m = st.last_metrics
+    assert m["matches_12"] == len(orc["pairs12"]) and m["matches_23"] == len(orc["pairs23"])
+    assert np.array_equal(st._last["pairs12"].cpu().numpy(), orc["pairs12"])
+    assert np.array_equal(st._last["pairs23"].cpu().numpy(), orc["pairs23"])
+    assert np.array_equal(st._last["H12"], orc["H12"]) and np.array_equal(st._last["H32"], orc["H32"])
+    assert (m["canvas_w"], m["canvas_h"]) == orc["canvas"]
+    assert pano.shape == orc["pano"].shape and np.array_equal(pano, orc["pano"])
+    assert abs(m["seam_rmse"] - orc["rmse12"]) < 1e-9 and abs(m["seam_rmse_23"] - orc["rmse23"]) < 1e-9
+    H12n = H12 / H12[2, 2]
+    assert np.allclose(st._last["H12"] / st._last["H12"][2, 2], H12n, rtol=2e-2, atol=2e-2 * np.abs(H12n).max())
