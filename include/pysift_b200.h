@@ -254,7 +254,7 @@ int pysift_dlt_homography(const double* pts1, const double* pts2, int32_t n, int
  * (pysift/core.py:3794-3800) and, where both cover the canvas, a linear
  * feather blend (weights 1 + distance to the image border).  Optional
  * outputs: warped image 1, both masks, per-row/column coverage extents;
- * out may be NULL when warped image 1 and both masks are requested. */
+ * out may be NULL when warped image 1 and its mask are requested. */
 int pysift_warp_feather(const uint8_t* img1, int32_t hs, int32_t ws, int32_t pitch1, const uint8_t* img2, int32_t h2,
                         int32_t w2, int32_t pitch2, int32_t cw, int32_t ch, const float* hinv9, float ox, float oy,
                         int32_t iox, int32_t ioy, int32_t feather, uint8_t* out, uint8_t* warped, uint8_t* mask1,

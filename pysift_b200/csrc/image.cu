@@ -341,7 +341,7 @@ int pysift_warp_feather(const uint8_t* img1, int32_t hs, int32_t ws, int32_t pit
                         uint8_t* mask2, int32_t* row_lo, int32_t* row_hi, int32_t* col_lo, int32_t* col_hi,
                         pysift_stream_t stream) {
     PYSIFT_CHECK_ARG(img1 && img2 && hinv9, "NULL pointer argument");
-    PYSIFT_CHECK_ARG(out || (warped && mask1 && mask2), "no output requested");
+    PYSIFT_CHECK_ARG(out || (warped && mask1), "no output requested");
     PYSIFT_CHECK_ARG(hs > 1 && ws > 1 && h2 > 0 && w2 > 0 && cw > 0 && ch > 0, "bad sizes");
     PYSIFT_CHECK_ARG((row_lo && row_hi && col_lo && col_hi) || !(row_lo || row_hi || col_lo || col_hi),
                      "extents must be all or none");
