@@ -202,6 +202,24 @@ def multiband(I1, I2, seam, n_levels=6):
     return res.astype(np.float32)
 
 
+def hist_match(src, ref, ov):
+    """_hist_match (core.py:3591-3625): per channel, the CDFs of the overlap
+    values of src and ref (integer bins, np.histogram), the LUT
+    np.interp(cdf_src, cdf_ref, 0..255) and src mapped through it."""
+    out = src.copy()
+    bins = np.arange(257, dtype=np.float32)
+    for c in range(3):
+        s_cnt, _ = np.histogram(src[ov, c].clip(0, 255), bins=bins)
+        r_cnt, _ = np.histogram(ref[ov, c].clip(0, 255), bins=bins)
+        s_cdf = np.cumsum(s_cnt).astype(np.float64)
+        r_cdf = np.cumsum(r_cnt).astype(np.float64)
+        s_cdf /= s_cdf[-1] + 1e-8
+        r_cdf /= r_cdf[-1] + 1e-8
+        lut = np.interp(s_cdf, r_cdf, np.arange(256))
+        out[:, :, c] = np.interp(src[:, :, c].ravel().clip(0, 255), np.arange(256), lut).reshape(src.shape[:2])
+    return out.astype(np.float32)
+
+
 def seam_rmse(w1_gained, m1, c2, m2):
     """_seam_rmse (core.py:3555-3562) of the gained image 1, exact: the
     uint8-truncated differences squared, summed as integers."""
@@ -214,13 +232,18 @@ def seam_rmse(w1_gained, m1, c2, m2):
     return float(np.sqrt((d * d).sum() / d.size))
 
 
-def blend_core(w1, m1, c2, m2, n_levels=6, faithful=False):
+def blend_core(w1, m1, c2, m2, n_levels=6, faithful=False, color_match="gain"):
     """_blend_pair (core.py:3686-3714) on float32 canvases: the blended float32
-    image (before any clipping), the union mask and the seam RMSE."""
+    image (before any clipping), the union mask and the seam RMSE.
+    color_match 'hist' matches histograms, anything else applies the gain."""
     w1 = np.asarray(w1, np.float32)
     c2 = np.asarray(c2, np.float32)
     ov = m1 & m2
-    w1 = gain_compensate(w1, c2, ov, faithful)
+    if color_match == "hist":
+        if ov.any():
+            w1 = hist_match(w1, c2, ov)
+    else:
+        w1 = gain_compensate(w1, c2, ov, faithful)
     seam = find_seam(w1, c2, m1, m2, faithful)
     I1 = np.zeros_like(w1)
     I2 = np.zeros_like(w1)
@@ -239,18 +262,20 @@ def paste(out, both):
     return pano
 
 
-def blend_pair(warped1, m1, canvas2, m2, n_levels=6, faithful=False):
+def blend_pair(warped1, m1, canvas2, m2, n_levels=6, faithful=False, color_match="gain"):
     """_blend_pair + the paste of _stitch_pair: uint8 (H, W, 3) canvas (before
     the inner-rectangle crop) and the union mask."""
-    out, both, _ = blend_core(warped1.astype(np.float32), m1, canvas2.astype(np.float32), m2, n_levels, faithful)
+    out, both, _ = blend_core(warped1.astype(np.float32), m1, canvas2.astype(np.float32), m2, n_levels, faithful,
+                              color_match)
     return paste(out, both), both
 
 
-def compose3(warped1, m1, canvas2, m2, warped3, m3, n_levels=6, faithful=False):
+def compose3(warped1, m1, canvas2, m2, warped3, m3, n_levels=6, faithful=False, color_match="gain"):
     """The composition of _stitch_triple (core.py:3913-3953): image 1 blended
     with image 2, the float result blended with image 3 (gain on the float
     image, seam, multiband), paste.  Returns (pano uint8 before the crop,
     union mask, seam RMSE 1-2, seam RMSE 12-3)."""
-    b12, m12, r12 = blend_core(warped1.astype(np.float32), m1, canvas2.astype(np.float32), m2, n_levels, faithful)
-    out, both, r23 = blend_core(b12, m12, warped3.astype(np.float32), m3, n_levels, faithful)
+    b12, m12, r12 = blend_core(warped1.astype(np.float32), m1, canvas2.astype(np.float32), m2, n_levels, faithful,
+                               color_match)
+    out, both, r23 = blend_core(b12, m12, warped3.astype(np.float32), m3, n_levels, faithful, color_match)
     return paste(out, both), both, r12, r23

@@ -208,6 +208,13 @@ def main(ref_root, out_dir=HERE):
         out.update({f"{name}_warped1": w1, f"{name}_mask1": m1, f"{name}_canvas2": c2, f"{name}_mask2": m2,
                     f"{name}_pano": pano, f"{name}_both": both, f"{name}_seam_rmse": np.float64(rmse)})
         print(name, pano.shape, "rmse", rmse)
+        # the same canvases with histogram matching in place of the gain (core.py:3694-3695)
+        st.color_match = "hist"
+        blended, both, rmse = st._blend_pair(w1.astype(np.float32), m1, c2.astype(np.float32), m2, cw, ch)
+        st.color_match = "gain"
+        pano = np.zeros((ch, cw, 3), np.uint8)
+        pano[both] = np.clip(blended[both], 0, 255).astype(np.uint8)
+        out.update({f"{name}_hist_pano": pano, f"{name}_hist_seam_rmse": np.float64(rmse)})
     out["names"] = np.array(names)
     np.savez_compressed(os.path.join(out_dir, "blend_cases.npz"), **out)
     run_triples(GPUPyStitch, out_dir)
