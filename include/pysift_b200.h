@@ -302,7 +302,9 @@ int pysift_warp_f32_backward(const float* img1, int32_t hs, int32_t ws, int32_t 
  * three-image stitch takes it, pysift/core.py:3931-3947); canvas2: cw x ch x
  * 3 uint8; masks: cw x ch bytes (0 / 1); all on the device.  seam_k25: the 25
  * float32 taps of the sigma-3 seam-mask blur (host); gauss_w9: the 9 float64
- * taps of gaussian_filter(sigma = 1) (host).  Outputs (at least one of pano
+ * taps of gaussian_filter(sigma = 1) (host).  color_match: 0 = the gain
+ * (pysift/core.py:3697-3698), 1 = histogram matching (_hist_match,
+ * pysift/core.py:3591-3625, color_match='hist').  Outputs (at least one of pano
  * and blended): pano (cw x ch x 3 uint8, zero where neither image covers),
  * blended (cw x ch x 3 float32, the blend before any clipping), both (union
  * mask) and seam_rmse (one double on the device: the RMS colour difference
@@ -311,7 +313,8 @@ int pysift_place_image(const uint8_t* img, int32_t h, int32_t w, int32_t pitch, 
                        int32_t ioy, uint8_t* canvas, uint8_t* mask, pysift_stream_t stream);
 int pysift_blend_workspace_size(int32_t cw, int32_t ch, int32_t n_levels, size_t* bytes);
 int pysift_blend_multiband(const void* image1, int32_t image1_f32, const uint8_t* mask1, const uint8_t* canvas2,
-                           const uint8_t* mask2, int32_t cw, int32_t ch, int32_t n_levels, const float* seam_k25,
+                           const uint8_t* mask2, int32_t cw, int32_t ch, int32_t n_levels, int32_t color_match,
+                           const float* seam_k25,
                            const double* gauss_w9, void* workspace, size_t workspace_bytes, uint8_t* pano,
                            uint8_t* both, float* blended, double* seam_rmse, pysift_stream_t stream);
 /* Per-row and per-column first / last set pixel of a cw x ch coverage mask

@@ -144,7 +144,8 @@ def autocrop(pano, both):
 class OracleStitch:
     def __init__(self, ransac_iters=1500, inlier_thresh=5.0, match_ratio=0.75, max_keypoints=8000, pca_dims=64,
                  n_octaves=4, clahe_clip=2.0, clahe_tile=8, high_vram=True, blend="multiband", n_blend_levels=6,
-                 int8_matching=False):
+                 int8_matching=False, color_match="gain"):
+        self.color_match = color_match
         self.int8_matching = int8_matching
         self.blend = blend
         self.n_blend_levels = n_blend_levels
@@ -202,7 +203,8 @@ class OracleStitch:
             canvas2 = np.zeros((ch, cw, 3), np.uint8)
             ye, xe = min(ioy + img2.shape[0], ch), min(iox + img2.shape[1], cw)
             canvas2[ioy:ye, iox:xe] = img2[:ye - ioy, :xe - iox]
-            out, _ = blend_oracle.blend_pair(warped, m1, canvas2, m2, self.n_blend_levels)
+            out, _ = blend_oracle.blend_pair(warped, m1, canvas2, m2, self.n_blend_levels,
+                                             color_match=self.color_match)
         pano = autocrop(out, m1 | m2)
         return dict(pano=pano, H=H, mask=mask, info=info, pairs=pairs, p1=p1, p2=p2, n1=len(pts1), n2=len(pts2))
 
@@ -232,7 +234,8 @@ class OracleStitch:
         canvas2 = np.zeros((ch, cw, 3), np.uint8)
         ye, xe = min(ioy + img2.shape[0], ch), min(iox + img2.shape[1], cw)
         canvas2[ioy:ye, iox:xe] = img2[:ye - ioy, :xe - iox]
-        pano, both, r12, r23 = blend_oracle.compose3(w1, m1, canvas2, m2, w3, m3, self.n_blend_levels)
+        pano, both, r12, r23 = blend_oracle.compose3(w1, m1, canvas2, m2, w3, m3, self.n_blend_levels,
+                                                     color_match=self.color_match)
         return dict(pano=autocrop(pano, both), H12=H12, H32=H32, pairs12=p12, pairs23=p23, info12=info12,
                     info32=info32, rmse12=r12, rmse23=r23, canvas=(cw, ch))
 

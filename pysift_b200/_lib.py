@@ -185,8 +185,8 @@ EXPORTS.update({
                                           c_void_p, c_void_p, c_void_p]),
     "pysift_blend_workspace_size": (ctypes.c_int, [c_int32, c_int32, c_int32, c_void_p]),
     "pysift_blend_multiband": (ctypes.c_int, [c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_int32, c_int32,
-                                              c_int32, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p, c_void_p,
-                                              c_void_p, c_void_p, c_void_p]),
+                                              c_int32, c_int32, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p,
+                                              c_void_p, c_void_p, c_void_p, c_void_p]),
     "pysift_mask_extents": (ctypes.c_int, [c_void_p, c_int32, c_int32, c_void_p, c_void_p, c_void_p, c_void_p,
                                            c_void_p]),
 })

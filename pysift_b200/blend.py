@@ -66,13 +66,15 @@ def place_image(img, cw, ch, iox, ioy, canvas=None, mask=None, stream=None):
 
 
 def blend_multiband(image1, mask1, canvas2, mask2, n_levels=6, workspace=None, pano=None, both=None,
-                    seam_rmse=None, blended=None, want_pano=True, stream=None):
+                    seam_rmse=None, blended=None, want_pano=True, stream=None, color_match="gain"):
     """_blend_pair + paste.  image1: (ch, cw, 3) uint8 (a warped image) or
     float32 (an earlier blend's unclipped result); canvas2: (ch, cw, 3)
     uint8; masks (ch, cw) uint8 / bool; all on the device.  Returns (pano
     uint8 (ch, cw, 3) or None, both uint8 (ch, cw), seam_rmse float64 (1,),
     blended float32 (ch, cw, 3) or None), enqueued on the current stream;
-    pass a `blended` tensor to get the unclipped blend."""
+    pass a `blended` tensor to get the unclipped blend.  color_match 'hist'
+    matches histograms (_hist_match), anything else applies the gain, as
+    pysift/core.py:3694-3698 does."""
     lib = _lib.load()
     ch, cw = mask1.shape
     dev = mask1.device
@@ -101,7 +103,8 @@ def blend_multiband(image1, mask1, canvas2, mask2, n_levels=6, workspace=None, p
         raise ValueError("nothing to compute: want_pano=False and no blended tensor")
     st = stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
     _lib.check(lib.pysift_blend_multiband(image1.data_ptr(), 1 if f32 else 0, m1.data_ptr(), canvas2.data_ptr(),
-                                          m2.data_ptr(), cw, ch, int(n_levels), _SEAM_K.ctypes.data,
+                                          m2.data_ptr(), cw, ch, int(n_levels), 1 if color_match == "hist" else 0,
+                                          _SEAM_K.ctypes.data,
                                           _GAUSS_W.ctypes.data, wp, need, pano.data_ptr() if pano is not None else None,
                                           both.data_ptr(), blended.data_ptr() if blended is not None else None,
                                           seam_rmse.data_ptr(), st),

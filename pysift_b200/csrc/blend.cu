@@ -47,7 +47,31 @@ struct BlendCtl {
     int line0, line1;                   // first and last DP line holding overlap
     int n_lines, seam_end;              // overlap lines; seam position on the last one
     int chunk;                          // backtrack chunk length
+    int hist;                           // colour matching: 0 gain, 1 histograms (pysift/core.py:3694-3699)
+    unsigned int hist1[3][256], hist2[3][256];  // overlap histograms of images 1 and 2
+    double lut[3][256];                 // histogram-matching LUT per channel
 };
+
+// image 1 after the colour matching of pysift/core.py:3692-3699 where both
+// images overlap (unchanged without overlap): the clipped gain, or the
+// histogram-matching LUT applied as np.interp(clip(v, 0, 255), 0..255, lut)
+// does (pysift/core.py:3621-3623): the LUT entry at integers, else
+// (lut[j + 1] - lut[j]) * (v - j) + lut[j] in float64
+__device__ __forceinline__ float color_matched(const BlendCtl* ctl, float v, int c) {
+    if (!ctl->have_ov) return v;
+    if (ctl->hist) {
+        const float vc = v < 0.0f ? 0.0f : (v > 255.0f ? 255.0f : v);
+        const int j = (int)floorf(vc);
+        const double* lut = ctl->lut[c];
+        double r;
+        if (j >= 255) r = lut[255];
+        else if (vc == (float)j) r = lut[j];
+        else r = ((lut[j + 1] - lut[j]) / 1.0) * ((double)vc - (double)j) + lut[j];
+        return (float)r;
+    }
+    const float x = v * ctl->gain[c];
+    return x < 0.0f ? 0.0f : (x > 255.0f ? 255.0f : x);
+}
 
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
@@ -84,7 +108,13 @@ __global__ void __launch_bounds__(256) k_blend_stats(const Img1 w1, const uint8_
                                                      int cw, BlendCtl* ctl, int* __restrict__ rowf,
                                                      int* __restrict__ colf, int* __restrict__ rlo,
                                                      int* __restrict__ rhi, int* __restrict__ clo,
-                                                     int* __restrict__ chi) {
+                                                     int* __restrict__ chi, int hist) {
+    __shared__ unsigned int sh1[3][256], sh2[3][256];
+    if (hist)
+        for (int k = threadIdx.x; k < 3 * 256; k += blockDim.x) {
+            (&sh1[0][0])[k] = 0u;
+            (&sh2[0][0])[k] = 0u;
+        }
     __shared__ unsigned int s[7];
     __shared__ unsigned long long s1[3];
     __shared__ int s_or, s_lo, s_hi;
@@ -109,8 +139,15 @@ __global__ void __launch_bounds__(256) k_blend_stats(const Img1 w1, const uint8_
         if (a && b) {
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                acc1[c] += fixed24(w1.at(p, c));
+                const float v1 = w1.at(p, c);
+                acc1[c] += fixed24(v1);
                 acc[3 + c] += c2[p * 3 + c];
+                if (hist) {
+                    // np.histogram with edges 0..256: bin floor(v), 255 inclusive
+                    const float vc = v1 < 0.0f ? 0.0f : (v1 > 255.0f ? 255.0f : v1);
+                    atomicAdd(&sh1[c][min((int)floorf(vc), 255)], 1u);
+                    atomicAdd(&sh2[c][c2[p * 3 + c]], 1u);
+                }
             }
             acc[6] += 1u;
             lo = min(lo, u);
@@ -143,6 +180,12 @@ __global__ void __launch_bounds__(256) k_blend_stats(const Img1 w1, const uint8_
         }
     }
     __syncthreads();
+    if (hist && s[6])
+        for (int k = threadIdx.x; k < 3 * 256; k += blockDim.x) {
+            const unsigned a = (&sh1[0][0])[k], b = (&sh2[0][0])[k];
+            if (a) atomicAdd(&(&ctl->hist1[0][0])[k], a);
+            if (b) atomicAdd(&(&ctl->hist2[0][0])[k], b);
+        }
     if (threadIdx.x == 0) {
         rlo[v] = s_lo;
         rhi[v] = s_hi;
@@ -180,7 +223,7 @@ __device__ void block_sum6(long long v[6], long long* sh /* [32][6] */) {
 
 // gain (pysift/core.py:3692-3699) and the seam orientation (pysift/core.py:3424-3438)
 __global__ void __launch_bounds__(1024) k_blend_decide(BlendCtl* ctl, const int* __restrict__ rowf,
-                                                       const int* __restrict__ colf, int cw, int ch) {
+                                                       const int* __restrict__ colf, int cw, int ch, int hist) {
     __shared__ long long sh[32 * 6];
     __shared__ long long s_rows[6];
     __shared__ int s_lo, s_hi;
@@ -209,6 +252,7 @@ __global__ void __launch_bounds__(1024) k_blend_decide(BlendCtl* ctl, const int*
     if (threadIdx.x == 0) {
         const unsigned long long n = ctl->n_ov;
         ctl->have_ov = n > 0;
+        ctl->hist = hist;
         for (int k = 0; k < 3; ++k) {
             float g = 1.0f;
             if (n > 0) {
@@ -256,20 +300,52 @@ struct Level0 {
     const BlendCtl* ctl;
     __device__ __forceinline__ void px(long long p, float i1[3], float i2[3]) const {
         const bool a = m1[p] != 0, b = m2[p] != 0;
-        const bool gained = ctl->have_ov != 0;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            float x = w1.at(p, c);
-            if (gained) {
-                x = x * ctl->gain[c];
-                x = x < 0.0f ? 0.0f : (x > 255.0f ? 255.0f : x);
-            }
+            const float x = color_matched(ctl, w1.at(p, c), c);
             const float y = (float)c2[p * 3 + c];
             i1[c] = a ? x : (b ? y : 0.0f);
             i2[c] = b ? y : (a ? x : 0.0f);
         }
     }
 };
+
+// The histogram-matching LUT of one channel (pysift/core.py:3611-3620), one
+// block of 256 threads a channel: CDFs of the overlap histograms in float64,
+// each divided by (total + 1e-8); lut[k] = np.interp(cdf1[k], cdf2, 0..255):
+// 0 below cdf2[0], 255 above cdf2[255], else with j the last index where
+// cdf2[j] <= x: j if j == 255 or cdf2[j] == x, else
+// (1 / (cdf2[j + 1] - cdf2[j])) * (x - cdf2[j]) + j.
+__global__ void __launch_bounds__(256) k_blend_hist_lut(BlendCtl* ctl) {
+    __shared__ int sh[33];
+    __shared__ double cdf2[256];
+    if (!ctl->hist || !ctl->have_ov) return;
+    const int c = blockIdx.x, k = threadIdx.x;
+    int tot1, tot2;
+    const int a = (int)ctl->hist1[c][k], b = (int)ctl->hist2[c][k];
+    const int cum1 = block_excl_scan(a, &tot1, sh) + a;
+    const int cum2 = block_excl_scan(b, &tot2, sh) + b;
+    const double x = (double)cum1 / ((double)tot1 + 1e-8);
+    cdf2[k] = (double)cum2 / ((double)tot2 + 1e-8);
+    __syncthreads();
+    double r;
+    if (x > cdf2[255]) {
+        r = 255.0;
+    } else if (x < cdf2[0]) {
+        r = 0.0;
+    } else {
+        int lo = 0, hi = 256;  // first index with cdf2 > x
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (x >= cdf2[mid]) lo = mid + 1;
+            else hi = mid;
+        }
+        const int j = lo - 1;
+        if (j == 255 || cdf2[j] == x) r = (double)j;
+        else r = (1.0 / (cdf2[j + 1] - cdf2[j])) * (x - cdf2[j]) + (double)j;
+    }
+    ctl->lut[c][k] = r;
+}
 
 // colour cost, average gray (pysift/core.py:3411-3415) and the seam-RMSE sum
 // (pysift/core.py:3555-3562) of the gained image 1
@@ -281,15 +357,10 @@ __global__ void k_blend_prepare(const Img1 w1, const uint8_t* __restrict__ m1,
     if (u < cw) {
         const long long p = (long long)v * cw + u;
         const bool ov = m1[p] != 0 && m2[p] != 0;
-        const bool gained = ctl->have_ov != 0;
         float g1[3], g2[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            float x = w1.at(p, c);
-            if (gained) {
-                x = x * ctl->gain[c];
-                x = x < 0.0f ? 0.0f : (x > 255.0f ? 255.0f : x);
-            }
+            const float x = color_matched(ctl, w1.at(p, c), c);
             g1[c] = x;
             g2[c] = (float)c2[p * 3 + c];
             if (ov) {
@@ -1056,7 +1127,8 @@ int pysift_mask_extents(const uint8_t* mask, int32_t cw, int32_t ch, int32_t* ro
 }
 
 int pysift_blend_multiband(const void* image1, int32_t image1_f32, const uint8_t* mask1, const uint8_t* canvas2,
-                           const uint8_t* mask2, int32_t cw, int32_t ch, int32_t n_levels, const float* seam_k25,
+                           const uint8_t* mask2, int32_t cw, int32_t ch, int32_t n_levels, int32_t color_match,
+                           const float* seam_k25,
                            const double* gauss_w9, void* workspace, size_t workspace_bytes, uint8_t* pano,
                            uint8_t* both, float* blended, double* seam_rmse, pysift_stream_t stream) {
     PYSIFT_CHECK_ARG(image1 && mask1 && canvas2 && mask2 && seam_k25 && gauss_w9 && workspace && (pano || blended),
@@ -1065,6 +1137,7 @@ int pysift_blend_multiband(const void* image1, int32_t image1_f32, const uint8_t
     w1.u8 = image1_f32 ? nullptr : static_cast<const uint8_t*>(image1);
     w1.f32 = image1_f32 ? static_cast<const float*>(image1) : nullptr;
     PYSIFT_CHECK_ARG(cw > 1 && ch > 1 && n_levels >= 1 && n_levels <= 8, "bad sizes");
+    PYSIFT_CHECK_ARG(color_match == 0 || color_match == 1, "color_match must be 0 (gain) or 1 (histograms)");
     const BlendLayout l = blend_layout(cw, ch, n_levels);
     if (workspace_bytes < l.total) {
         set_error("workspace %zu bytes < required %zu", workspace_bytes, l.total);
@@ -1090,10 +1163,16 @@ int pysift_blend_multiband(const void* image1, int32_t image1_f32, const uint8_t
     PYSIFT_CUDA_TRY(cudaMemcpyAsync(k25, seam_k25, 25 * sizeof(float), cudaMemcpyHostToDevice, st));
     const dim3 g2d(ceil_div(cw, 256), ch);
     // gain, overlap flags and ranges, seam orientation
-    k_blend_stats<<<dim3(1, ch), 256, 0, st>>>(w1, mask1, canvas2, mask2, cw, ctl, rowf, colf, rlo, rhi, clo, chi);
+    const int hist = color_match == 1;
+    k_blend_stats<<<dim3(1, ch), 256, 0, st>>>(w1, mask1, canvas2, mask2, cw, ctl, rowf, colf, rlo, rhi, clo, chi,
+                                                hist);
     PYSIFT_LAUNCH_CHECK("k_blend_stats");
-    k_blend_decide<<<1, 1024, 0, st>>>(ctl, rowf, colf, cw, ch);
+    k_blend_decide<<<1, 1024, 0, st>>>(ctl, rowf, colf, cw, ch, hist);
     PYSIFT_LAUNCH_CHECK("k_blend_decide");
+    if (hist) {
+        k_blend_hist_lut<<<3, 256, 0, st>>>(ctl);
+        PYSIFT_LAUNCH_CHECK("k_blend_hist_lut");
+    }
     // Gaussian pyramids of I1 and I2 on a side stream: they need only the gain
     Level0 src;
     src.w1 = w1;

@@ -64,8 +64,6 @@ class GPUPyStitch:
             raise NotImplementedError("pca_dims must be 0, 64 or 128 on this backend")
         if blend not in ('multiband', 'feather'):
             raise ValueError(f"blend must be 'multiband' or 'feather' (got {blend!r})")
-        if blend == 'multiband' and color_match != 'gain':
-            raise NotImplementedError(f"color_match={color_match!r}: only gain compensation is implemented")
         if blend == 'multiband' and not 1 <= int(n_blend_levels) <= 8:
             raise ValueError("n_blend_levels must be within 1..8")
         if ransac_method not in ('magsac', 'classic'):
@@ -327,7 +325,8 @@ class GPUPyStitch:
             wsb = self._dev.get(key + "blend_ws", (need,), torch.uint8, dev)
             both = self._dev.get(key + "both", (ch, cw), torch.uint8, dev)
             rmse = self._dev.get(key + "seam_rmse", (1,), torch.float64, dev)
-            _blend.blend_multiband(warped, m1, canvas2, m2, self.n_blend_levels, workspace=wsb, pano=out,
+            _blend.blend_multiband(warped, m1, canvas2, m2, self.n_blend_levels, color_match=self.color_match,
+                                   workspace=wsb, pano=out,
                                    both=both, seam_rmse=rmse, stream=st)
             rmse_host = torch.empty(1, dtype=torch.float64, pin_memory=True)
             rmse_host.copy_(rmse, non_blocking=True)
@@ -571,12 +570,14 @@ class GPUPyStitch:
             b12 = self._dev.get("t_b12", (ch, cw, 3), torch.float32, self.device)
             m12u = self._dev.get("t_m12", (ch, cw), torch.uint8, self.device)
             r12 = self._dev.get("t_r12", (1,), torch.float64, self.device)
-            _blend.blend_multiband(w1, mk1, canvas2, mk2, self.n_blend_levels, workspace=wsb, both=m12u,
+            _blend.blend_multiband(w1, mk1, canvas2, mk2, self.n_blend_levels, color_match=self.color_match,
+                                   workspace=wsb, both=m12u,
                                    seam_rmse=r12, blended=b12, want_pano=False, stream=st)
             pano = self._dev.get("t_pano", (ch, cw, 3), torch.uint8, self.device)
             both = self._dev.get("t_both", (ch, cw), torch.uint8, self.device)
             r23 = self._dev.get("t_r23", (1,), torch.float64, self.device)
-            _blend.blend_multiband(b12, m12u, w3, mk3, self.n_blend_levels, workspace=wsb, pano=pano, both=both,
+            _blend.blend_multiband(b12, m12u, w3, mk3, self.n_blend_levels, color_match=self.color_match,
+                                   workspace=wsb, pano=pano, both=both,
                                    seam_rmse=r23, stream=st)
             ext = _blend.mask_extents(both, out=self._dev.get("t_ext", (2 * ch + 2 * cw,), torch.int32, self.device),
                                       stream=st)

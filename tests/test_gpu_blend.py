@@ -14,11 +14,12 @@ pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "blend_cases.npz")
 
 
-def _run(w1, m1, c2, m2, n_levels=6):
+def _run(w1, m1, c2, m2, n_levels=6, color_match="gain"):
     import torch
     from pysift_b200 import blend
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
-    pano, both, rmse, _ = blend.blend_multiband(t(w1), t(m1.astype(np.uint8)), t(c2), t(m2.astype(np.uint8)), n_levels)
+    pano, both, rmse, _ = blend.blend_multiband(t(w1), t(m1.astype(np.uint8)), t(c2), t(m2.astype(np.uint8)), n_levels,
+                                                color_match=color_match)
     torch.cuda.synchronize()
     return pano.cpu().numpy(), both.cpu().numpy().astype(bool), float(rmse.cpu()[0])
 
@@ -267,3 +268,52 @@ def test_stitch_three_images_end_to_end(int8):
     assert abs(m["seam_rmse"] - orc["rmse12"]) < 1e-9 and abs(m["seam_rmse_23"] - orc["rmse23"]) < 1e-9
     H12n = H12 / H12[2, 2]
     assert np.allclose(st._last["H12"] / st._last["H12"][2, 2], H12n, rtol=2e-2, atol=2e-2 * np.abs(H12n).max())
+
+
+def test_histogram_matching():
+    """color_match='hist' (_hist_match, pysift/core.py:3591-3625): bit-exact
+    against the oracle on the golden canvases and seeded canvases, with a
+    float image 1 too (the second pass of a three-image stitch); against the
+    reference's own output within one level (the canonical seam blur)."""
+    import torch
+    from oracle import blend_oracle as bo
+    from pysift_b200 import blend
+    g = np.load(GOLDEN)
+    for name in g["names"]:
+        w1, m1, c2, m2 = (g[f"{name}_{k}"] for k in ("warped1", "mask1", "canvas2", "mask2"))
+        pano, both, rmse = _run(w1, m1, c2, m2, color_match="hist")
+        ref, _ = bo.blend_pair(w1, m1, c2, m2, color_match="hist")
+        assert np.array_equal(pano, ref), name
+        d = np.abs(pano.astype(int) - g[f"{name}_hist_pano"].astype(int))
+        assert d.max() <= 1 and (d > 0).mean() < 1e-3
+    for args in [(21, 300, 520, False, False), (22, 520, 300, True, True)]:
+        w1, m1, c2, m2 = _case(*args)
+        pano, _, rmse = _run(w1, m1, c2, m2, color_match="hist")
+        ref, _ = bo.blend_pair(w1, m1, c2, m2, color_match="hist")
+        assert np.array_equal(pano, ref)
+    g = np.load(TRIPLES)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    for name in g["names"]:
+        w1, m1, c2, m2, w3, m3 = (g[f"{name}_{k}"] for k in ("warped1", "mask1", "canvas2", "mask2", "warped3",
+                                                             "mask3"))
+        ch, cw = m1.shape
+        b12 = torch.empty((ch, cw, 3), dtype=torch.float32, device="cuda")
+        _, m12, _, _ = blend.blend_multiband(t(w1), t(m1.astype(np.uint8)), t(c2), t(m2.astype(np.uint8)),
+                                             blended=b12, want_pano=False, color_match="hist")
+        pano, _, _, _ = blend.blend_multiband(b12, m12, t(w3), t(m3.astype(np.uint8)), color_match="hist")
+        ref, _, _, _ = bo.compose3(w1, m1, c2, m2, w3, m3, color_match="hist")
+        assert np.array_equal(pano.cpu().numpy(), ref), name
+
+
+def test_stitch_color_match_hist_end_to_end():
+    """GPUPyStitch(color_match='hist'): the composed canvas equals the
+    oracle's composition of the stitcher's own warp."""
+    from oracle import blend_oracle as bo
+    from pysift_b200.stitch import GPUPyStitch
+    img1, img2, _ = synthetic.stitch_pair(480, 640, seed=3)
+    st = GPUPyStitch(ransac_iters=1024, inlier_thresh=4.0, save_output=False, verbose=False, color_match="hist")
+    st.stitch(img1, img2)
+    c = st._last_compose
+    ref, _ = bo.blend_pair(c["warped1"].cpu().numpy(), c["mask1"].cpu().numpy().astype(bool),
+                           c["canvas2"].cpu().numpy(), c["mask2"].cpu().numpy().astype(bool), color_match="hist")
+    assert np.array_equal(c["out"].cpu().numpy(), ref)
