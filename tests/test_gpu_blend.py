@@ -317,3 +317,25 @@ def test_stitch_color_match_hist_end_to_end():
     ref, _ = bo.blend_pair(c["warped1"].cpu().numpy(), c["mask1"].cpu().numpy().astype(bool),
                            c["canvas2"].cpu().numpy(), c["mask2"].cpu().numpy().astype(bool), color_match="hist")
     assert np.array_equal(c["out"].cpu().numpy(), ref)
+
+
+@pytest.mark.parametrize("ch,cw,ov_lo,ov_hi", [(1100, 1500, 500, 1400), (1500, 1900, 300, 1750),
+                                                (2150, 2500, 200, 2330)])
+def test_blend_wide_overlap_bands(ch, cw, ov_lo, ov_hi):
+    """Wide overlap bands (~900 and ~1470 columns for a vertical seam, ~2150
+    rows for a horizontal one): windows of a thousand and more positions per
+    DP line."""
+    from oracle import blend_oracle as bo
+    rng = np.random.default_rng(cw)
+    yy, xx = np.mgrid[0:ch, 0:cw]
+    m1 = xx < ov_hi + (yy * 0.04).astype(int) - 40
+    m2 = (xx >= ov_lo + (yy * 0.03).astype(int)) & (yy >= 2)
+    base = synthetic.dense_texture(ch, cw, seed=ch).astype(np.float64)
+    w1 = np.clip(base[:, :, None] * 0.9 + rng.normal(0, 3, (ch, cw, 3)), 0, 255).astype(np.uint8)
+    c2 = np.clip(base[:, :, None] * 1.05 + rng.normal(0, 3, (ch, cw, 3)), 0, 255).astype(np.uint8)
+    w1[~m1] = 0
+    c2[~m2] = 0
+    pano, both, _ = _run(w1, m1, c2, m2)
+    ref, ref_both = bo.blend_pair(w1, m1, c2, m2)
+    assert np.array_equal(both, ref_both)
+    assert np.array_equal(pano, ref)
