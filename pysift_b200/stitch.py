@@ -621,6 +621,7 @@ class GPUPyStitch:
                 s.wait_stream(main)
             # (1) features
             bgrs, grays = [], []
+            pairs = [tuple(self._preprocess_image(im) for im in pr) for pr in pairs]
             for p, pr in enumerate(pairs):
                 if len(pr) != 2:
                     raise ValueError("stitch_batch takes (img1, img2) pairs")
@@ -717,6 +718,8 @@ class GPUPyStitch:
             images = list(args[0])
         else:
             images = list(args)
+        if len(images) in (2, 3):
+            images = [self._preprocess_image(im) for im in images]
         if len(images) == 2:
             pano, timings, metrics = self._stitch_pair(images[0], images[1])
         elif len(images) == 3:
@@ -734,11 +737,56 @@ class GPUPyStitch:
                       f"{metrics['inliers_32']}  canvas {metrics['canvas_w']}x{metrics['canvas_h']}")
         if self.save_output:
             import cv2
+            out = self._postprocess(pano)
             ts = datetime.now().strftime("%Y%m%d_%H%M%S")
             ext = 'jpg' if self.output_format in ('jpg', 'jpeg') else 'png'
             fname = f"panorama_{ts}.{ext}"
             if ext == 'jpg':
-                cv2.imwrite(fname, pano, [cv2.IMWRITE_JPEG_QUALITY, self.output_quality])
+                cv2.imwrite(fname, out, [cv2.IMWRITE_JPEG_QUALITY, self.output_quality])
             else:
-                cv2.imwrite(fname, pano)
+                cv2.imwrite(fname, out)
+        return pano
+
+    def _preprocess_image(self, img):
+        """The reference's optional preprocessing of each input
+        (pysift/core.py:2486-2514), with its own OpenCV calls on host images:
+        resize the longest side to max_dimension (INTER_AREA), bilateral
+        filter (denoise), unsharp mask (sharpen).  CUDA tensor inputs take no
+        preprocessing options."""
+        if not (self.max_dimension > 0 or self.denoise or self.sharpen):
+            return img
+        if isinstance(img, torch.Tensor):
+            raise NotImplementedError("max_dimension / denoise / sharpen apply to host (numpy) images only")
+        import cv2
+        if self.max_dimension > 0:
+            h, w = img.shape[:2]
+            scale = self.max_dimension / max(h, w)
+            if scale < 1.0:
+                nw, nh = int(w * scale), int(h * scale)
+                img = cv2.resize(img, (nw, nh), interpolation=cv2.INTER_AREA)
+                if self.verbose:
+                    print(f"    Resized {w}x{h} -> {nw}x{nh}  (scale {scale:.2f})")
+        if self.denoise:
+            img = cv2.bilateralFilter(img, d=9, sigmaColor=75, sigmaSpace=75)
+        if self.sharpen:
+            blur = cv2.GaussianBlur(img, (0, 0), sigmaX=2.0)
+            img = cv2.addWeighted(img, 1.5, blur, -0.5, 0)
+        return np.ascontiguousarray(img)
+
+    def _postprocess(self, pano):
+        """The reference's post-processing of the saved panorama
+        (pysift/core.py:4054-4075): resize the longest side to output_max_dim
+        (INTER_AREA), unsharp mask (post_sharpen).  The returned panorama is
+        not post-processed, as in the reference."""
+        if not (self.output_max_dim > 0 or self.post_sharpen):
+            return pano
+        import cv2
+        if self.output_max_dim > 0:
+            h, w = pano.shape[:2]
+            scale = self.output_max_dim / max(h, w)
+            if scale < 1.0:
+                pano = cv2.resize(pano, (int(w * scale), int(h * scale)), interpolation=cv2.INTER_AREA)
+        if self.post_sharpen:
+            blur = cv2.GaussianBlur(pano, (0, 0), sigmaX=2.0)
+            pano = cv2.addWeighted(pano, 1.5, blur, -0.5, 0)
         return pano

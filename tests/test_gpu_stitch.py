@@ -243,3 +243,37 @@ def test_stitch_batch_matches_sequential_stitch():
         assert len(got) == len(pairs)
         for r, g in zip(ref, got):
             assert r.shape == g.shape and np.array_equal(r, g)
+
+
+def test_pre_and_post_processing_options(tmp_path, monkeypatch):
+    """max_dimension / denoise / sharpen preprocess the inputs with the
+    reference's OpenCV calls (pysift/core.py:2486-2514): the stitch equals one
+    of the preprocessed images; output_max_dim / post_sharpen change only the
+    saved file (pysift/core.py:4054-4092)."""
+    import cv2
+    from pysift_b200.stitch import GPUPyStitch
+    img1, img2, _ = synthetic.stitch_pair(600, 800, seed=8)
+    kw = dict(ransac_iters=512, inlier_thresh=4.0, verbose=False)
+    st = GPUPyStitch(max_dimension=640, denoise=True, sharpen=True, save_output=False, **kw)
+    pano = st.stitch(img1, img2)
+
+    def prep(im):
+        im = cv2.resize(im, (640, 480), interpolation=cv2.INTER_AREA)
+        im = cv2.bilateralFilter(im, d=9, sigmaColor=75, sigmaSpace=75)
+        blur = cv2.GaussianBlur(im, (0, 0), sigmaX=2.0)
+        return cv2.addWeighted(im, 1.5, blur, -0.5, 0)
+
+    ref = GPUPyStitch(save_output=False, **kw).stitch(prep(img1), prep(img2))
+    assert np.array_equal(pano, ref)
+    monkeypatch.chdir(tmp_path)
+    st2 = GPUPyStitch(output_max_dim=300, post_sharpen=True, save_output=True, **kw)
+    out = st2.stitch(img1, img2)
+    files = list(tmp_path.glob("panorama_*.png"))
+    assert len(files) == 1
+    saved = cv2.imread(str(files[0]))
+    exp = out
+    h, w = exp.shape[:2]
+    if 300 / max(h, w) < 1.0:
+        exp = cv2.resize(exp, (int(w * 300 / max(h, w)), int(h * 300 / max(h, w))), interpolation=cv2.INTER_AREA)
+    exp = cv2.addWeighted(exp, 1.5, cv2.GaussianBlur(exp, (0, 0), sigmaX=2.0), -0.5, 0)
+    assert np.array_equal(saved, exp)
