@@ -18,7 +18,8 @@ stand in for the reference's datasets; see pysift_b200/synthetic.py):
   match_u8_8192_fp8 the same through the split-nibble e4m3 tcgen05 GEMM
   batch96_detect    PySIFT.detect_batch of 96 grayscale images of uneven sizes
                     (480x360 .. 4000x3000, aspect 4:3, 3:2, 16:9) over 8 streams,
-                    next to the plain per-image detectAndCompute loop
+                    next to the plain per-image detectAndCompute loop and the
+                    same batch replayed as one CUDA graph
   batch32_stitch    GPUPyStitch.stitch_batch of 32 uneven pairs (1280x960 ..
                     3000x2000, 4096 hypotheses each) next to sequential stitch()
   grad_16x1024x768  forward + backward of the differentiable descriptors (2000
@@ -462,6 +463,11 @@ def run_batch_detect(args, wl, world, rank, local):
     plain_steps = max(1, min(3, args.steps))
     plain_ms = timed(lambda: [sift.detectAndCompute(x, gpu_output=True) for x in g], plain_steps)
     one_ms = timed(lambda: sift.detect_batch(g, n_streams=1), plain_steps)
+    # the same batch replayed as one CUDA graph (captured on the first call)
+    for _ in range(2):
+        sift.detect_batch(g, n_streams=ns, graph=True)
+    torch.cuda.synchronize(dev)
+    graph_ms = timed(lambda: sift.detect_batch(g, n_streams=ns, graph=True), args.steps)
     # end to end: host images in, host arrays out
     e2e_ms = []
     for i in range(args.warmup + args.steps):
@@ -502,6 +508,7 @@ def run_batch_detect(args, wl, world, rank, local):
                    "l2": "flushed (256 MiB write) before every step", "parallelism": f"replicas{world}"},
         "plain_mpix_per_s": mpix / (float(np.mean(plain_ms)) / 1e3),
         "one_stream_mpix_per_s": mpix / (float(np.mean(one_ms)) / 1e3),
+        "graph_mpix_per_s": mpix / (float(np.mean(graph_ms)) / 1e3),
         "roofline": {"bound": "hbm", "kernel": "whole batched detection: pyramid-region algorithmic bytes of all "
                      "images over the whole batch time (a lower bound for the pyramid kernels)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

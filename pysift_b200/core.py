@@ -305,7 +305,7 @@ class PySIFT:
         return out
 
     # -- batched detection ----------------------------------------------------
-    def detect_batch(self, images, n_streams=8, gpu_output=True):
+    def detect_batch(self, images, n_streams=8, gpu_output=True, graph=False):
         """Detect and describe a list of grayscale uint8 images of any sizes in
         one call.  Images (numpy arrays or CUDA tensors) are dealt, largest
         first, to `n_streams` slots; each slot runs its images in order on its
@@ -315,13 +315,17 @@ class PySIFT:
 
         Returns a list of (kpts (N,4) [x, y, size, angle], desc (N,128)) per
         image, in input order: torch CUDA tensors with gpu_output, else numpy
-        arrays.  n_streams=1 runs the same work back to back on one stream."""
+        arrays.  n_streams=1 runs the same work back to back on one stream.
+
+        graph=True replays the whole batch as one CUDA graph: the first call
+        for a list of image shapes runs the batch once, then captures it
+        (every stream's launches, forked from and joined back to one capture
+        stream); later calls with the same shapes copy the images into the
+        graph's input buffers and replay it.  Results are identical."""
         n = len(images)
         if n == 0:
             return []
-        lib = self._lib
         with torch.cuda.device(self.device):
-            main = torch.cuda.current_stream(self.device)
             gray = []
             for img in images:
                 if isinstance(img, torch.Tensor) and img.is_cuda:
@@ -336,56 +340,97 @@ class PySIFT:
                 if t.stride(1) != 1:
                     t = t.contiguous()
                 gray.append(t)
-            order = sorted(range(n), key=lambda i: -(gray[i].shape[0] * gray[i].shape[1]))
-            ns = max(1, min(int(n_streams), n))
-            slots = [order[s::ns] for s in range(ns)]
-            if not hasattr(self, "_batch"):
-                self._batch = {"streams": [], "ws": [], "outs": []}
-            bt = self._batch
-            while len(bt["streams"]) < ns:
-                bt["streams"].append(torch.cuda.Stream(self.device))
-                bt["ws"].append(None)
-            max_out = int(lib.pysift_detect_max_keypoints(ctypes.byref(self._cfg)))
-            while len(bt["outs"]) < n:
-                bt["outs"].append(_BatchOutputs(max_out, self.device))
-            for s, idxs in enumerate(slots):
-                need = 0
+            if graph:
+                return self._detect_batch_graph(gray, n_streams, gpu_output)
+            self._enqueue_batch(gray, n_streams)
+            torch.cuda.current_stream(self.device).synchronize()
+            return self._collect_batch(n, gpu_output)
+
+    def _enqueue_batch(self, gray, n_streams):
+        """Enqueue the detection of every image of `gray` (device uint8
+        tensors): images dealt largest first to the slot streams, forked from
+        and joined back to the current stream; stats copied to pinned memory."""
+        lib = self._lib
+        n = len(gray)
+        main = torch.cuda.current_stream(self.device)
+        order = sorted(range(n), key=lambda i: -(gray[i].shape[0] * gray[i].shape[1]))
+        ns = max(1, min(int(n_streams), n))
+        slots = [order[s::ns] for s in range(ns)]
+        if not hasattr(self, "_batch"):
+            self._batch = {"streams": [], "ws": [], "outs": []}
+        bt = self._batch
+        while len(bt["streams"]) < ns:
+            bt["streams"].append(torch.cuda.Stream(self.device))
+            bt["ws"].append(None)
+        max_out = int(lib.pysift_detect_max_keypoints(ctypes.byref(self._cfg)))
+        while len(bt["outs"]) < n:
+            bt["outs"].append(_BatchOutputs(max_out, self.device))
+        for s, idxs in enumerate(slots):
+            need = 0
+            for i in idxs:
+                H, W = gray[i].shape
+                sz = ctypes.c_size_t(0)
+                _lib.check(lib.pysift_detect_workspace_size(ctypes.byref(self._cfg), H, W, ctypes.byref(sz)),
+                           "pysift_detect_workspace_size")
+                need = max(need, int(sz.value))
+            ws = bt["ws"][s]
+            if ws is None or ws.numel() < need + 256:
+                ws = torch.empty(need + 256, dtype=torch.uint8, device=self.device)
+                bt["ws"][s] = ws
+            st = bt["streams"][s]
+            st.wait_stream(main)
+            wptr = ws.data_ptr() + ((-ws.data_ptr()) % 256)
+            with torch.cuda.stream(st):
                 for i in idxs:
                     H, W = gray[i].shape
-                    sz = ctypes.c_size_t(0)
-                    _lib.check(lib.pysift_detect_workspace_size(ctypes.byref(self._cfg), H, W, ctypes.byref(sz)),
-                               "pysift_detect_workspace_size")
-                    need = max(need, int(sz.value))
-                ws = bt["ws"][s]
-                if ws is None or ws.numel() < need + 256:
-                    ws = torch.empty(need + 256, dtype=torch.uint8, device=self.device)
-                    bt["ws"][s] = ws
-                st = bt["streams"][s]
-                st.wait_stream(main)
-                wptr = ws.data_ptr() + ((-ws.data_ptr()) % 256)
-                with torch.cuda.stream(st):
-                    for i in idxs:
-                        H, W = gray[i].shape
-                        o = bt["outs"][i]
-                        rc = lib.pysift_detect_and_compute(
-                            ctypes.byref(self._cfg), gray[i].data_ptr(), H, W, gray[i].stride(0), wptr, need,
-                            o.kpts.data_ptr(), o.resp.data_ptr(), o.octv.data_ptr(), o.desc.data_ptr(), max_out,
-                            o.stats.data_ptr(), None, st.cuda_stream)
-                        _lib.check(rc, "pysift_detect_and_compute")
-                        o.stats_host.copy_(o.stats, non_blocking=True)
-            for s in range(ns):
-                main.wait_stream(bt["streams"][s])
-            main.synchronize()
-            out = []
-            for i in range(n):
-                o = bt["outs"][i]
-                k = int(o.stats_host[_lib.STAT_N_KEYPOINTS])
-                d = self._desc_u8(o.desc[:k]) if self.as_uint8 else o.desc[:k]
-                if gpu_output:
-                    out.append((o.kpts[:k].clone(), d.clone()))
-                else:
-                    out.append((o.kpts[:k].cpu().numpy(), d.cpu().numpy()))
+                    o = bt["outs"][i]
+                    rc = lib.pysift_detect_and_compute(
+                        ctypes.byref(self._cfg), gray[i].data_ptr(), H, W, gray[i].stride(0), wptr, need,
+                        o.kpts.data_ptr(), o.resp.data_ptr(), o.octv.data_ptr(), o.desc.data_ptr(), max_out,
+                        o.stats.data_ptr(), None, st.cuda_stream)
+                    _lib.check(rc, "pysift_detect_and_compute")
+                    o.stats_host.copy_(o.stats, non_blocking=True)
+        for s in range(ns):
+            main.wait_stream(bt["streams"][s])
+
+    def _collect_batch(self, n, gpu_output):
+        """The results of the last enqueued batch (the stream has finished)."""
+        bt = self._batch
+        out = []
+        for i in range(n):
+            o = bt["outs"][i]
+            k = int(o.stats_host[_lib.STAT_N_KEYPOINTS])
+            d = self._desc_u8(o.desc[:k]) if self.as_uint8 else o.desc[:k]
+            if gpu_output:
+                out.append((o.kpts[:k].clone(), d.clone()))
+            else:
+                out.append((o.kpts[:k].cpu().numpy(), d.cpu().numpy()))
         return out
+
+    def _detect_batch_graph(self, gray, n_streams, gpu_output):
+        key = (tuple(tuple(g.shape) for g in gray), int(n_streams))
+        ent = self._graphs.get(key)
+        main = torch.cuda.current_stream(self.device)
+        if ent is None:
+            # inputs live in buffers the graph reads; the first run (eager)
+            # sizes the workspaces and outputs, the capture records the same
+            # launches on those buffers
+            inp = [torch.empty_like(g) for g in gray]
+            for b, g in zip(inp, gray):
+                b.copy_(g)
+            self.detect_batch(inp, n_streams=n_streams, gpu_output=True)
+            torch.cuda.synchronize(self.device)
+            g_ = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g_):
+                self._enqueue_batch(inp, n_streams)
+            ent = (g_, inp)
+            self._graphs[key] = ent
+        g_, inp = ent
+        for b, g in zip(inp, gray):
+            b.copy_(g, non_blocking=True)
+        g_.replay()
+        main.synchronize()
+        return self._collect_batch(len(gray), gpu_output)
 
     def detect_arrays(self, gray):
         """Host uint8 image in, host numpy arrays out: dict with x, y, size,

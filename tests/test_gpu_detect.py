@@ -243,3 +243,19 @@ def test_as_uint8_descriptors_and_exact_matching(oracle_lib):
     assert np.array_equal(m["pairs"][:n].cpu().numpy(), ref["pairs"])
     dm = match.to_dmatches(m)
     assert len(dm) == n and dm[0].queryIdx == int(ref["pairs"][0, 0]) and dm[0].trainIdx == int(ref["pairs"][0, 1])
+
+
+def test_detect_batch_graph_replay_matches_eager():
+    """detect_batch(graph=True): the batch captured once as a CUDA graph and
+    replayed on new images of the same sizes gives exactly the eager results."""
+    from pysift_b200 import PySIFT
+    sizes = [(480, 640), (360, 480), (600, 800), (480, 640), (300, 400)]
+    sift = PySIFT()
+    first = [synthetic.scene(h, w, seed=30 + i) for i, (h, w) in enumerate(sizes)]
+    second = [synthetic.scene(h, w, seed=60 + i) for i, (h, w) in enumerate(sizes)]
+    for imgs in (first, second, first):
+        eager = sift.detect_batch(imgs, n_streams=4, gpu_output=False)
+        graph = sift.detect_batch(imgs, n_streams=4, gpu_output=False, graph=True)
+        assert len(eager) == len(graph)
+        for (k1, d1), (k2, d2) in zip(eager, graph):
+            assert k1.shape[0] > 0 and np.array_equal(k1, k2) and np.array_equal(d1, d2)
