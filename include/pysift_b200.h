@@ -340,8 +340,12 @@ int pysift_zoom2x_u8_noalloc(const uint8_t* gray, int32_t H, int32_t W, int64_t 
                              float* out, int32_t out_pitch, pysift_stream_t stream);
 
 /* Number of kernel launches the library has issued in this process
- * (monotonic, all threads and devices). */
+ * (all threads and devices).  A caller that captures library calls into a
+ * CUDA graph and replays it adds the graph's kernel count per replay with
+ * pysift_count_launches (and subtracts the captured launches, which did not
+ * run), so that the count stays the number of kernels that ran. */
 int64_t pysift_launch_count(void);
+void pysift_count_launches(int64_t n);
 
 const char* pysift_last_error(void);
 const char* pysift_b200_version(void);

@@ -160,7 +160,8 @@ class PySIFT:
 
     def __init__(self, n_octaves=None, n_scales=3, sigma0=1.6, contrast_thresh=0.04, edge_thresh=10.0,
                  dsp=False, dsp_n_scales=3, fp16_pyramid=None, orientation='histogram', descriptor='sift',
-                 double_image=True, rootsift=True, *, device=None, high_vram=None, as_uint8=False):
+                 double_image=True, rootsift=True, *, device=None, high_vram=None, as_uint8=False,
+                 graphs=True):
         if dsp_n_scales not in DSP_PRESETS:
             raise ValueError(f"dsp_n_scales must be 3, 4, or 5 (got {dsp_n_scales})")
         if orientation != 'histogram':
@@ -197,6 +198,7 @@ class PySIFT:
         self._cfg = build_detect_config(self.n_octaves, n_scales, sigma0, contrast_thresh, edge_thresh, dsp,
                                         dsp_n_scales, self.fp16_pyramid, double_image, rootsift, hv)
         self._bufs = {}
+        self._use_graphs = bool(graphs)
         self._phase_timings = None
         self._last_stats = None
         self._graphs = {}
@@ -236,7 +238,10 @@ class PySIFT:
         (default: the current stream).  Returns the buffer set holding the
         outputs; stats are read by the caller.  stage_events: optional list
         of 7 torch.cuda.Event recorded at the stage boundaries; slot selects
-        an independent buffer set (for concurrent detections)."""
+        an independent buffer set (for concurrent detections).  Unless the
+        instance was built with graphs=False (or stage_events are asked for),
+        the detection is a CUDA graph replay, captured on the first call for
+        each image size, slot and configuration."""
         if gray_t.dtype != torch.uint8 or gray_t.dim() != 2:
             raise ValueError("expected a 2-D uint8 image")
         if gray_t.stride(1) != 1:
@@ -244,8 +249,36 @@ class PySIFT:
         H, W = gray_t.shape
         b = self._buffers(H, W, slot)
         st = stream if stream is not None else torch.cuda.current_stream(self.device)
-        self._launch(b, gray_t.data_ptr(), H, W, gray_t.stride(0), st.cuda_stream, stage_events)
+        if self._use_graphs and stage_events is None:
+            self._run_graph(b, gray_t, H, W, slot, st)
+        else:
+            self._launch(b, gray_t.data_ptr(), H, W, gray_t.stride(0), st.cuda_stream, stage_events)
         return b
+
+    def _run_graph(self, b, gray_t, H, W, slot, st):
+        """Detection of one image as a CUDA graph replay.  The graph reads the
+        buffer set's input image, so the image is copied there first (host
+        uploads already land there); the first call for a size, slot and
+        configuration runs eagerly and then captures the same launches."""
+        if gray_t.data_ptr() != b.gray.data_ptr():
+            with torch.cuda.stream(st):
+                b.gray.copy_(gray_t, non_blocking=True)
+        key = ("one", H, W, slot, bytes(self._cfg))
+        ent = self._graphs.get(key)
+        if ent is None:
+            self._launch(b, b.gray.data_ptr(), H, W, W, st.cuda_stream)
+            n0 = self._lib.pysift_launch_count()
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=torch.cuda.Stream(self.device)):
+                self._launch(b, b.gray.data_ptr(), H, W, W, torch.cuda.current_stream(self.device).cuda_stream)
+            n = self._lib.pysift_launch_count() - n0
+            self._lib.pysift_count_launches(-n)  # captured, not run
+            self._graphs[key] = (g, n)
+            return
+        g, n = ent
+        with torch.cuda.stream(st):
+            g.replay()
+        self._lib.pysift_count_launches(n)
 
     def _upload(self, gray, b):
         """Host numpy image -> pinned staging -> device (async on the current stream)."""

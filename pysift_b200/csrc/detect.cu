@@ -2055,6 +2055,8 @@ size_t pysift_detect_config_size(void) { return sizeof(pysift_detect_config); }
 
 int64_t pysift_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
+void pysift_count_launches(int64_t n) { g_launches.fetch_add((long long)n, std::memory_order_relaxed); }
+
 int pysift_detect_workspace_size(const pysift_detect_config* cfg, int32_t H, int32_t W, size_t* bytes) {
     int rc = validate_cfg(cfg);
     if (rc) return rc;

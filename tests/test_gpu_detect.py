@@ -259,3 +259,31 @@ def test_detect_batch_graph_replay_matches_eager():
         assert len(eager) == len(graph)
         for (k1, d1), (k2, d2) in zip(eager, graph):
             assert k1.shape[0] > 0 and np.array_equal(k1, k2) and np.array_equal(d1, d2)
+
+
+def test_single_image_graph_replay(oracle_lib):
+    """detectAndCompute replays a captured CUDA graph from the second call on
+    (per size): results equal the eager instance's and the oracle's, and each
+    replay adds the same number of launches to the library's count as an
+    eager call."""
+    from pysift_b200 import PySIFT, _lib
+    lib = _lib.load()
+    a = synthetic.scene(480, 640, seed=41)
+    b = synthetic.scene(480, 640, seed=42)
+    eager = PySIFT(graphs=False)
+    graph = PySIFT()
+    for img in (a, b, a, b):
+        n0 = lib.pysift_launch_count()
+        k1, d1 = eager.detectAndCompute(img, gpu_output=True)
+        n1 = lib.pysift_launch_count()
+        k2, d2 = graph.detectAndCompute(img, gpu_output=True)
+        n2 = lib.pysift_launch_count()
+        assert torch_equal(k1, k2) and torch_equal(d1, d2)
+        assert n2 - n1 == n1 - n0
+    ref = oracle_lib.OracleSIFT().detect_and_compute(b)
+    assert np.array_equal(d2.cpu().numpy(), ref["desc"])
+
+
+def torch_equal(x, y):
+    import torch
+    return x.shape == y.shape and bool(torch.equal(x, y))
