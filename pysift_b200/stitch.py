@@ -476,6 +476,29 @@ class GPUPyStitch:
         oy = max(0.0, -ay.min())
         return int(np.ceil(ax.max() + ox)) + 1, int(np.ceil(ay.max() + oy)) + 1, ox, oy
 
+    def _verify_chain(self, H_AB, H_CB):
+        """pysift/core.py:3564-3586: rotation and scale of inv(H_CB) H_AB,
+        printed with a warning past 5 degrees or 15 % (when verbose); returned
+        as metrics chain_rotation_deg / chain_scale."""
+        try:
+            Hc = np.linalg.inv(H_CB) @ H_AB
+            Hc /= Hc[2, 2]
+        except np.linalg.LinAlgError:
+            if self.verbose:
+                print("  [Chain] WARNING: H_CB is singular")
+            return {}
+        theta = float(np.degrees(np.arctan2(Hc[1, 0], Hc[0, 0])))
+        scale = float(np.sqrt(abs(np.linalg.det(Hc[:2, :2]))))
+        if self.verbose:
+            warns = []
+            if abs(theta) > 5.0:
+                warns.append(f"rotation drift {theta:+.1f} deg")
+            if abs(scale - 1.0) > 0.15:
+                warns.append(f"scale drift {scale:.3f}x")
+            status = "OK" if not warns else "WARN: " + ", ".join(warns)
+            print(f"  [Chain] rotation={theta:+.1f} deg scale={scale:.3f}  [{status}]")
+        return dict(chain_rotation_deg=theta, chain_scale=scale)
+
     def _warp_to_canvas(self, img, H, ref, cw, ch, ox, oy, key):
         """Warped uint8 image and mask of `img` on the canvas (the warp of
         pysift/core.py:3210-3239); `ref` is the reference view the kernel
@@ -552,6 +575,7 @@ class GPUPyStitch:
             metrics.update(inliers_12=int(infos[0][0]), inliers_32=int(infos[1][0]))
             if min(int(infos[0][0]), int(infos[1][0])) < 4:
                 raise RuntimeError("Too few inliers for 3-image stitching")
+            metrics.update(self._verify_chain(H12, H32))
             timings['st4'] = 0.0
             metrics.update(depth_cv=None, bands=self.n_depth_layers)
             t0 = time.perf_counter()

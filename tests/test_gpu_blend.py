@@ -268,6 +268,10 @@ def test_stitch_three_images_end_to_end(int8):
     assert abs(m["seam_rmse"] - orc["rmse12"]) < 1e-9 and abs(m["seam_rmse_23"] - orc["rmse23"]) < 1e-9
     H12n = H12 / H12[2, 2]
     assert np.allclose(st._last["H12"] / st._last["H12"][2, 2], H12n, rtol=2e-2, atol=2e-2 * np.abs(H12n).max())
+    Hc = np.linalg.inv(st._last["H32"]) @ st._last["H12"]
+    Hc /= Hc[2, 2]
+    assert abs(m["chain_scale"] - np.sqrt(abs(np.linalg.det(Hc[:2, :2])))) < 1e-12
+    assert abs(m["chain_rotation_deg"] - np.degrees(np.arctan2(Hc[1, 0], Hc[0, 0]))) < 1e-9
 
 
 def test_histogram_matching():
