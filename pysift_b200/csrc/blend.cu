@@ -649,6 +649,15 @@ __global__ void __launch_bounds__(1024) k_seam_walk(const uint8_t* __restrict__ 
     }
 }
 
+// filter taps passed by value (kernel parameters: no host copies, so the
+// composition can be captured in a CUDA graph)
+struct SeamTaps {
+    float k[25];
+};
+struct GaussTaps {
+    double w[9];
+};
+
 // the seam mask before its blur (pysift/core.py:3406-3467): 1 = image 1
 __device__ __forceinline__ float seam_value(const uint8_t* __restrict__ m1, const uint8_t* __restrict__ m2,
                                             const int* __restrict__ seam, const BlendCtl* ctl, int u, int v, int cw) {
@@ -664,7 +673,7 @@ __device__ __forceinline__ float seam_value(const uint8_t* __restrict__ m1, cons
 // the row pass over the mask values ...
 __global__ void __launch_bounds__(256) k_seam_rows(const uint8_t* __restrict__ m1, const uint8_t* __restrict__ m2,
                                                    const int* __restrict__ seam, const BlendCtl* ctl,
-                                                   const float* __restrict__ k25, float* __restrict__ out, int W) {
+                                                   const SeamTaps k25, float* __restrict__ out, int W) {
     __shared__ float sv[256 + 24];
     const int y = blockIdx.y, x0 = blockIdx.x * 256;
     for (int i = threadIdx.x; i < 256 + 24; i += 256)
@@ -674,7 +683,7 @@ __global__ void __launch_bounds__(256) k_seam_rows(const uint8_t* __restrict__ m
     if (x >= W) return;
     double s = 0.0;
 #pragma unroll
-    for (int t = 0; t < 25; ++t) s = s + (double)k25[t] * (double)sv[threadIdx.x + t];
+    for (int t = 0; t < 25; ++t) s = s + (double)k25.k[t] * (double)sv[threadIdx.x + t];
     out[(long long)y * W + x] = (float)s;
 }
 
@@ -682,14 +691,14 @@ __global__ void __launch_bounds__(256) k_seam_rows(const uint8_t* __restrict__ m
 // images cover the canvas (pysift/core.py:3469-3471)
 __global__ void k_seam_cols(const float* __restrict__ rows, const uint8_t* __restrict__ m1,
                             const uint8_t* __restrict__ m2, const int* __restrict__ seam, const BlendCtl* ctl,
-                            const float* __restrict__ k25, float* __restrict__ gm0, int W, int H) {
+                            const SeamTaps k25, float* __restrict__ gm0, int W, int H) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x >= W) return;
     const long long p = (long long)y * W + x;
     if (m1[p] && m2[p]) {
         double s = 0.0;
 #pragma unroll 5
-        for (int t = 0; t < 25; ++t) s = s + (double)k25[t] * (double)rows[(long long)refl_101(y + t - 12, H) * W + x];
+        for (int t = 0; t < 25; ++t) s = s + (double)k25.k[t] * (double)rows[(long long)refl_101(y + t - 12, H) * W + x];
         gm0[p] = (float)s;
     } else {
         gm0[p] = seam_value(m1, m2, seam, ctl, x, y, W);
@@ -732,19 +741,19 @@ __device__ __forceinline__ void pyr_load(const Level0& src, const PyrLevel& in, 
 // NC = 6: t1 / t2 get I1 / I2 (3 floats a pixel); NC = 1: t1 gets the mask
 template <int NC, bool L0>
 __global__ void k_pyr_rows(const Level0 src, const PyrLevel in, int W, int H, float* __restrict__ t1,
-                           float* __restrict__ t2, const double* __restrict__ w9) {
+                           float* __restrict__ t2, const GaussTaps w9) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, yo = blockIdx.y;
     if (x >= W) return;
     const int y = 2 * yo;
     double s[NC], a[NC], b[NC];
     pyr_load<NC, L0>(src, in, (long long)y * W + x, a);
 #pragma unroll
-    for (int c = 0; c < NC; ++c) s[c] = w9[4] * a[c];
+    for (int c = 0; c < NC; ++c) s[c] = w9.w[4] * a[c];
 #pragma unroll
     for (int k = 4; k >= 1; --k) {
         pyr_load<NC, L0>(src, in, (long long)refl_half(y - k, H) * W + x, a);
         pyr_load<NC, L0>(src, in, (long long)refl_half(y + k, H) * W + x, b);
-        const double w = w9[4 - k];
+        const double w = w9.w[4 - k];
 #pragma unroll
         for (int c = 0; c < NC; ++c) s[c] = s[c] + (a[c] + b[c]) * w;
     }
@@ -762,7 +771,7 @@ __global__ void k_pyr_rows(const Level0 src, const PyrLevel in, int W, int H, fl
 
 template <int NC>
 __global__ void k_pyr_cols(const float* __restrict__ t1, const float* __restrict__ t2, int W, int Wo,
-                           const double* __restrict__ w9, float* __restrict__ g1, float* __restrict__ g2) {
+                           const GaussTaps w9, float* __restrict__ g1, float* __restrict__ g2) {
     const int xo = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (xo >= Wo) return;
     const int col = 2 * xo;
@@ -782,12 +791,12 @@ __global__ void k_pyr_cols(const float* __restrict__ t1, const float* __restrict
     double s[NC], a[NC], b[NC];
     load(col, a);
 #pragma unroll
-    for (int c = 0; c < NC; ++c) s[c] = w9[4] * a[c];
+    for (int c = 0; c < NC; ++c) s[c] = w9.w[4] * a[c];
 #pragma unroll
     for (int k = 4; k >= 1; --k) {
         load(refl_half(col - k, W), a);
         load(refl_half(col + k, W), b);
-        const double w = w9[4 - k];
+        const double w = w9.w[4 - k];
 #pragma unroll
         for (int c = 0; c < NC; ++c) s[c] = s[c] + (a[c] + b[c]) * w;
     }
@@ -1020,7 +1029,7 @@ static cudaStream_t side_stream() {
 
 struct BlendLayout {
     size_t off_ctl, off_rowf, off_colf, off_rlo, off_rhi, off_clo, off_chi, off_win, off_color, off_avg, off_dpc,
-        off_rowA, off_rowB, off_dir, off_seam, off_ovl, off_jump, off_entry, off_srow, off_w9, off_k25, off_t1,
+        off_rowA, off_rowB, off_dir, off_seam, off_ovl, off_jump, off_entry, off_srow, off_t1,
         off_t2, off_tm;
     int nchunk;
     size_t off_g1[8], off_g2[8], off_gm[8], off_lb[8], off_res[2];
@@ -1060,8 +1069,6 @@ static BlendLayout blend_layout(int cw, int ch, int levels) {
     l.off_jump = take((size_t)l.nchunk * M * 4);
     l.off_entry = take((size_t)(l.nchunk + 1) * 4);
     l.off_srow = take(N * 4);
-    l.off_w9 = take(9 * 8);
-    l.off_k25 = take(25 * 4);
     const size_t half = (size_t)((ch + 1) / 2) * cw;
     l.off_t1 = take(half * 12);
     l.off_t2 = take(half * 12);
@@ -1157,10 +1164,10 @@ int pysift_blend_multiband(const void* image1, int32_t image1_f32, const uint8_t
     PYSIFT_CUDA_TRY(cudaMemsetAsync(colf, 0, (size_t)cw * 4, st));
     PYSIFT_CUDA_TRY(cudaMemsetAsync(clo, 0x7f, (size_t)cw * 4, st));
     PYSIFT_CUDA_TRY(cudaMemsetAsync(chi, 0xff, (size_t)cw * 4, st));
-    double* w9 = bwp<double>(ws, l.off_w9);
-    float* k25 = bwp<float>(ws, l.off_k25);
-    PYSIFT_CUDA_TRY(cudaMemcpyAsync(w9, gauss_w9, 9 * sizeof(double), cudaMemcpyHostToDevice, st));
-    PYSIFT_CUDA_TRY(cudaMemcpyAsync(k25, seam_k25, 25 * sizeof(float), cudaMemcpyHostToDevice, st));
+    GaussTaps w9;
+    SeamTaps k25;
+    for (int i = 0; i < 9; ++i) w9.w[i] = gauss_w9[i];
+    for (int i = 0; i < 25; ++i) k25.k[i] = seam_k25[i];
     const dim3 g2d(ceil_div(cw, 256), ch);
     // gain, overlap flags and ranges, seam orientation
     const int hist = color_match == 1;

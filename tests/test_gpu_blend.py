@@ -343,3 +343,36 @@ def test_blend_wide_overlap_bands(ch, cw, ov_lo, ov_hi):
     ref, ref_both = bo.blend_pair(w1, m1, c2, m2)
     assert np.array_equal(both, ref_both)
     assert np.array_equal(pano, ref)
+
+
+def test_blend_in_a_cuda_graph():
+    """The composition captures into a CUDA graph (no host copies or syncs
+    inside, the side stream forked and joined): replays on new canvases of the
+    same size give the eager results."""
+    import torch
+    from pysift_b200 import blend
+    w1, m1, c2, m2 = _case(31, 240, 400)
+    w1b, _, c2b, _ = _case(32, 240, 400)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    W1, M1, C2, M2 = t(w1), t(m1.astype(np.uint8)), t(c2), t(m2.astype(np.uint8))
+    ch, cw = m1.shape
+    ws = torch.empty(blend.workspace_bytes(cw, ch) + 256, dtype=torch.uint8, device="cuda")
+    pano = torch.empty((ch, cw, 3), dtype=torch.uint8, device="cuda")
+    both = torch.empty((ch, cw), dtype=torch.uint8, device="cuda")
+    rmse = torch.empty(1, dtype=torch.float64, device="cuda")
+    eager = []
+    for a, b in ((w1, c2), (w1b, c2b)):
+        p, _, _, _ = blend.blend_multiband(t(a), M1, t(b), M2)
+        eager.append(p.cpu().numpy())
+    blend.blend_multiband(W1, M1, C2, M2, workspace=ws, pano=pano, both=both, seam_rmse=rmse)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        blend.blend_multiband(W1, M1, C2, M2, workspace=ws, pano=pano, both=both, seam_rmse=rmse,
+                              stream=torch.cuda.current_stream().cuda_stream)
+    for k, (a, b) in enumerate(((w1b, c2b), (w1, c2))):
+        W1.copy_(t(a))
+        C2.copy_(t(b))
+        g.replay()
+        torch.cuda.synchronize()
+        assert np.array_equal(pano.cpu().numpy(), eager[1 - k])
