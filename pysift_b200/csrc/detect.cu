@@ -3,7 +3,7 @@
 // Pipeline (all launches on the caller's stream, no host synchronisation,
 // capturable into a CUDA graph):
 //   k_histogram          256-bin histogram + entropy threshold (pysift/core.py:1129-1148)
-//   k_prefilter_cols, k_zoom_rows_interp
+//   k_prefilter_cols, k_prefilter_rows, k_zoom_interp
 //                        2x cubic B-spline upsample (pysift/core.py:1270-1275)
 //   k_u8_to_f32          base image when not upsampled (pysift/core.py:1248-1261)
 //   k_blur<R>            fused H+V separable blur per level (pysift/core.py:475-608,
@@ -200,12 +200,48 @@ __global__ void __launch_bounds__(256) k_histogram(const uint8_t* __restrict__ i
     __shared__ unsigned int sh[8][256];
     __shared__ double terms[256];
     __shared__ int is_last;
-    const int tid = threadIdx.x, warp = tid >> 5;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     for (int i = tid; i < 8 * 256; i += 256) (&sh[0][0])[i] = 0u;
     __syncthreads();
-    for (int r = blockIdx.y; r < H; r += gridDim.y) {
+    // a warp per row; 16-byte loads when every row starts on a 16-byte
+    // boundary, else byte loads in batches of 8, all in flight before the
+    // shared-memory counts
+    const bool vec = ((reinterpret_cast<uintptr_t>(img) | (uintptr_t)pitch) & 15) == 0;
+    const int nw = W >> 4;
+    for (int r = blockIdx.x * 8 + warp; r < H; r += gridDim.x * 8) {
         const uint8_t* row = img + (long long)r * pitch;
-        for (int c = blockIdx.x * 256 + tid; c < W; c += gridDim.x * 256) atomicAdd(&sh[warp][row[c]], 1u);
+        int c0 = 0;
+        if (vec) {
+            for (int q0 = 0; q0 < nw; q0 += 64) {
+                uint4 u[2];
+#pragma unroll
+                for (int k = 0; k < 2; ++k) {
+                    const int q = q0 + lane + 32 * k;
+                    u[k] = q < nw ? reinterpret_cast<const uint4*>(row)[q] : make_uint4(0u, 0u, 0u, 0u);
+                }
+#pragma unroll
+                for (int k = 0; k < 2; ++k) {
+                    if (q0 + lane + 32 * k >= nw) continue;
+                    const uint32_t w4[4] = {u[k].x, u[k].y, u[k].z, u[k].w};
+#pragma unroll
+                    for (int e = 0; e < 4; ++e)
+#pragma unroll
+                        for (int sh8 = 0; sh8 < 32; sh8 += 8) atomicAdd(&sh[warp][(w4[e] >> sh8) & 255u], 1u);
+                }
+            }
+            c0 = nw << 4;
+        }
+        for (int cb = c0; cb < W; cb += 32 * 8) {
+            uint8_t u[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int c = cb + lane + 32 * k;
+                u[k] = c < W ? row[c] : 0;
+            }
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                if (cb + lane + 32 * k < W) atomicAdd(&sh[warp][u[k]], 1u);
+        }
     }
     __syncthreads();
     unsigned int mine = 0;
@@ -213,7 +249,7 @@ __global__ void __launch_bounds__(256) k_histogram(const uint8_t* __restrict__ i
     if (mine) atomicAdd(&ctrl->hist[tid], mine);
     __threadfence();
     __syncthreads();
-    if (tid == 0) is_last = (atomicAdd(&ctrl->blocks_done, 1u) == gridDim.x * gridDim.y - 1);
+    if (tid == 0) is_last = (atomicAdd(&ctrl->blocks_done, 1u) == gridDim.x - 1);
     __syncthreads();
     if (!is_last) return;
     __threadfence();
@@ -228,9 +264,12 @@ __global__ void __launch_bounds__(256) k_histogram(const uint8_t* __restrict__ i
     sh[0][tid] = h;
     __syncthreads();
     if (tid == 0) {
+        // ascending bins, one double sum; an empty bin holds +0.0, which
+        // leaves a sum that started at +0.0 unchanged, so every term is added
+        // and the loads run ahead of the chain
         double ent = 0.0;
-        for (int b = 0; b < 256; ++b)
-            if (sh[0][b]) ent = ent + terms[b];
+#pragma unroll 32
+        for (int b = 0; b < 256; ++b) ent = ent + terms[b];
         ent = -ent;
         double scale = 0.8 + ent / 40.0;
         if (scale > 1.0) scale = 1.0;
@@ -313,13 +352,20 @@ __global__ void __launch_bounds__(256) k_prefilter_cols(const uint8_t* __restric
     const int x0 = blockIdx.x * PC_TW, r0 = blockIdx.y * PC_TH;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const int x = x0 + tx;
-    for (int rr = ty; rr < PC_TH + 2 * SPL_K; rr += 8) {
-        double v = 0.0;
-        if (x < W) {
-            long long gr = mirror_index(r0 - SPL_K + rr, H);
-            v = (double)u8_to_unit(img[gr * pitch + x], fp16);
+    {
+        // every load of the window issued before the first conversion
+        constexpr int NL = (PC_TH + 2 * SPL_K + 7) / 8;
+        uint8_t u[NL];
+#pragma unroll
+        for (int q = 0; q < NL; ++q) {
+            const int rr = ty + 8 * q;
+            u[q] = (x < W && rr < PC_TH + 2 * SPL_K) ? img[mirror_index(r0 - SPL_K + rr, H) * pitch + x] : 0;
         }
-        tile[rr * PC_TW + tx] = v;
+#pragma unroll
+        for (int q = 0; q < NL; ++q) {
+            const int rr = ty + 8 * q;
+            if (rr < PC_TH + 2 * SPL_K) tile[rr * PC_TW + tx] = x < W ? (double)u8_to_unit(u[q], fp16) : 0.0;
+        }
     }
     __syncthreads();
     if (x >= W) return;
@@ -364,22 +410,99 @@ __device__ __forceinline__ bool zoom_axis(long long k, long long in_len, long lo
     return true;
 }
 
-constexpr int ZI_TW = 64, ZI_TH = 32;   // output tile
-constexpr int ZI_CR = 24, ZI_CC = 40;   // input rows / cols a tile can touch (span <= 20 x 36)
-constexpr int ZI_XB = 4;                // row-FIR outputs per thread
+// Row FIR in place: coef[r][x] <- sum_k h[k] coef[r][mirror(x-SPL_K+k)], one
+// block per row, the row processed in chunks of PR_CW outputs left to right.
+// A chunk's window is read before any of its outputs is written; its left
+// halo, which the previous chunk has overwritten, comes from a carry of the
+// previous chunk's last SPL_K inputs.  Mirrored positions past the right
+// end fall at or after the chunk start minus SPL_K once the row spans more
+// than one chunk, so the carry and the unwritten part of the row hold every
+// input.  The window sits in shared memory with one padding double per 8 so
+// that lanes reading 8-output strips hit distinct banks.
+constexpr int PR_NT = 256, PR_CW = 2048;
+constexpr int PR_EXT = PR_CW + 2 * SPL_K;
+__device__ __forceinline__ int pr_phys(int e) { return e + (e >> 3); }
 
-// Row FIR of the column-filtered coefficients for the input window a tile
-// needs, then the 4x4 cubic interpolation t = sum_i sum_j (c*wy_i)*wx_j in
-// scipy's order, rounded to float32.
-__global__ void __launch_bounds__(256) k_zoom_rows_interp(const double* __restrict__ coef, int H, int W, int fp16,
-                                                          float* __restrict__ out, int out_pitch, const SplTaps taps) {
-    __shared__ int rvalid[ZI_TH], ridx[ZI_TH][4];
-    __shared__ double rw[ZI_TH][4];
-    __shared__ int cvalid[ZI_TW], cidx[ZI_TW][4];
-    __shared__ double cw[ZI_TW][4];
+__global__ void __launch_bounds__(PR_NT) k_prefilter_rows(double* __restrict__ coef, int W, const SplTaps taps) {
+    // a strip that ends past the chunk reads up to 7 positions beyond the
+    // window (values that feed no stored output), so the array covers them
+    __shared__ double ext[PR_EXT + 7 + (PR_EXT + 7) / 8 + 1];
+    __shared__ double carry[SPL_K];
+    double* row = coef + (long long)blockIdx.x * W;
+    for (int x0 = 0; x0 < W; x0 += PR_CW) {
+        const int len = min(PR_CW, W - x0);
+        for (int e = threadIdx.x; e < len + 2 * SPL_K; e += PR_NT) {
+            const int m = (int)mirror_index((long long)x0 - SPL_K + e, W);
+            if (m >= x0) {
+                const unsigned d = (unsigned)__cvta_generic_to_shared(&ext[pr_phys(e)]);
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(row + m) : "memory");
+            } else {
+                ext[pr_phys(e)] = carry[m - (x0 - SPL_K)];
+            }
+        }
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        __syncthreads();
+        if (x0 + PR_CW < W)
+            for (int i = threadIdx.x; i < SPL_K; i += PR_NT) carry[i] = ext[pr_phys(PR_CW + i)];
+        for (int b = threadIdx.x * 8; b < len; b += PR_NT * 8) {
+            double acc[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) acc[j] = 0.0;
+#pragma unroll
+            for (int m = 0; m < 8 + 2 * SPL_K; ++m) {
+                const double t = ext[pr_phys(b + m)];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int k = m - j;
+                    if (k >= 0 && k < SPL_TAPS) acc[j] = fma(taps.h[k], t, acc[j]);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+                if (b + j < len) row[x0 + b + j] = acc[j];
+        }
+        __syncthreads();
+    }
+}
+
+// 4x4 cubic interpolation of the prefiltered coefficients on the 2x output
+// grid, t = sum_a sum_b (c[a][b] * wy_a) * wx_b in scipy's order, rounded to
+// float32.  On the 2x grid the output columns 2k-1 and 2k interpolate the
+// same 4 input columns (their input coordinates share the floor k-1), and
+// likewise the output rows 2k-1 and 2k.  A tile covers output rows
+// oy0-1 .. oy0+30 and columns ox0-1 .. ox0+62, so it splits into 16 x 32
+// such 2x2 quads; each thread takes 2 quads, loads the quad's 16
+// coefficients once and forms each c * wy_a once per row for both columns.
+// A quad whose rows or columns do not share their support (mirrored image
+// edges) reads each output's coefficients separately; either way each
+// output is the same sequence of products and sums.  The tile touches at
+// most 20 input rows and 36 input columns (zoom factor below 1/2).
+constexpr int ZI_TW = 64, ZI_TH = 32;
+constexpr int ZI_CR = 20, ZI_CC = 36;
+
+__device__ __forceinline__ double zoom_term_sum(const double (*win)[ZI_CC], const int* ry, const double* wy,
+                                                const int* cx, const double* wx) {
+    double t = 0.0;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            double coeff = win[ry[a]][cx[b]];
+            coeff *= wy[a];
+            coeff *= wx[b];
+            t += coeff;
+        }
+    return t;
+}
+
+__global__ void __launch_bounds__(256) k_zoom_interp(const double* __restrict__ coef, int H, int W, int fp16,
+                                                     float* __restrict__ out, int out_pitch) {
+    __shared__ int rvalid[ZI_TH], ridx[4][ZI_TH];
+    __shared__ double rw[4][ZI_TH];
+    __shared__ int cvalid[ZI_TW], cidx[4][ZI_TW];
+    __shared__ double cw[4][ZI_TW];
     __shared__ int s_lo[2], s_hi[2];
-    __shared__ double c1[ZI_CR][ZI_CC + 2 * SPL_K + ZI_XB];
-    __shared__ double c2[ZI_CR][ZI_CC];
+    __shared__ double win[ZI_CR][ZI_CC];
     const int OH = 2 * H, OW = 2 * W;
     const int ox0 = blockIdx.x * ZI_TW, oy0 = blockIdx.y * ZI_TH;
     const int tid = threadIdx.x;
@@ -389,16 +512,16 @@ __global__ void __launch_bounds__(256) k_zoom_rows_interp(const double* __restri
     }
     __syncthreads();
     if (tid < ZI_TH) {
-        const int r = oy0 + tid;
+        const int r = oy0 - 1 + tid;
         long long idx[4];
         double w[4];
-        bool v = (r < OH) && zoom_axis(r, H, OH, idx, w);
+        bool v = (r >= 0 && r < OH) && zoom_axis(r, H, OH, idx, w);
         rvalid[tid] = v;
         if (v) {
             int lo = 0x7fffffff, hi = -1;
             for (int q = 0; q < 4; ++q) {
-                ridx[tid][q] = (int)idx[q];
-                rw[tid][q] = w[q];
+                ridx[q][tid] = (int)idx[q];
+                rw[q][tid] = w[q];
                 lo = min(lo, (int)idx[q]);
                 hi = max(hi, (int)idx[q]);
             }
@@ -407,16 +530,16 @@ __global__ void __launch_bounds__(256) k_zoom_rows_interp(const double* __restri
         }
     } else if (tid >= 32 && tid < 32 + ZI_TW) {
         const int t = tid - 32;
-        const int x = ox0 + t;
+        const int x = ox0 - 1 + t;
         long long idx[4];
         double w[4];
-        bool v = (x < OW) && zoom_axis(x, W, OW, idx, w);
+        bool v = (x >= 0 && x < OW) && zoom_axis(x, W, OW, idx, w);
         cvalid[t] = v;
         if (v) {
             int lo = 0x7fffffff, hi = -1;
             for (int q = 0; q < 4; ++q) {
-                cidx[t][q] = (int)idx[q];
-                cw[t][q] = w[q];
+                cidx[q][t] = (int)idx[q];
+                cw[q][t] = w[q];
                 lo = min(lo, (int)idx[q]);
                 hi = max(hi, (int)idx[q]);
             }
@@ -429,73 +552,92 @@ __global__ void __launch_bounds__(256) k_zoom_rows_interp(const double* __restri
     const bool any = (yhi >= 0 && xhi >= 0);
     const int ny = any ? yhi - ylo + 1 : 0, nx = any ? xhi - xlo + 1 : 0;
     const bool fits = ny <= ZI_CR && nx <= ZI_CC;
+    const int warp = tid >> 5, lane = tid & 31;
     if (any && fits) {
-        const int nxw = nx + 2 * SPL_K;
-        for (int i = tid; i < ny * nxw; i += blockDim.x) {
-            const int yy = i / nxw, xx = i - yy * nxw;
-            const long long gx = mirror_index((long long)xlo - SPL_K + xx, W);
-            c1[yy][xx] = coef[(long long)(ylo + yy) * W + gx];
-        }
-        __syncthreads();
-        const int nxg = (nx + ZI_XB - 1) / ZI_XB;
-        for (int i = tid; i < ny * nxg; i += blockDim.x) {
-            const int yy = i / nxg, x0 = (i - yy * nxg) * ZI_XB;
-            double acc[ZI_XB];
-#pragma unroll
-            for (int j = 0; j < ZI_XB; ++j) acc[j] = 0.0;
-#pragma unroll
-            for (int m = 0; m < ZI_XB + 2 * SPL_K; ++m) {
-                const double t = c1[yy][x0 + m];
-#pragma unroll
-                for (int j = 0; j < ZI_XB; ++j) {
-                    const int k = m - j;
-                    if (k >= 0 && k < SPL_TAPS) acc[j] = fma(taps.h[k], t, acc[j]);
-                }
+        for (int yy = warp; yy < ny; yy += 8) {
+            const double* src = coef + (long long)(ylo + yy) * W + xlo;
+            for (int xx = lane; xx < nx; xx += 32) {
+                const unsigned d = (unsigned)__cvta_generic_to_shared(&win[yy][xx]);
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src + xx) : "memory");
             }
-#pragma unroll
-            for (int j = 0; j < ZI_XB; ++j)
-                if (x0 + j < nx) c2[yy][x0 + j] = acc[j];
         }
-        __syncthreads();
+        asm volatile("cp.async.wait_all;" ::: "memory");
     }
-    // each thread: one output column, every 4th output row of the tile
-    const int tx = tid % ZI_TW;
-    const int x = ox0 + tx;
-    if (x >= OW) return;
-    const bool cv = cvalid[tx];
-    int cx[4];
-    double wx[4];
+    __syncthreads();
+    // this lane's column pair
+    const int ta = 2 * lane, tb = ta + 1;
+    const int xa = ox0 - 1 + ta, xb = xa + 1;
+    const bool cva = cvalid[ta], cvb = cvalid[tb];
+    int cxa[4], cxb[4];
+    double wxa[4], wxb[4];
+    bool csame = cva && cvb;
 #pragma unroll
-    for (int b = 0; b < 4; ++b) {
-        cx[b] = cv ? cidx[tx][b] - xlo : 0;
-        wx[b] = cv ? cw[tx][b] : 0.0;
+    for (int q = 0; q < 4; ++q) {
+        cxa[q] = cva ? cidx[q][ta] - xlo : 0;
+        cxb[q] = cvb ? cidx[q][tb] - xlo : 0;
+        wxa[q] = cva ? cw[q][ta] : 0.0;
+        wxb[q] = cvb ? cw[q][tb] : 0.0;
+        csame = csame && cxa[q] == cxb[q];
     }
-    for (int ty = tid / ZI_TW; ty < ZI_TH; ty += 256 / ZI_TW) {
-        const int r = oy0 + ty;
-        if (r >= OH) break;
-        float res = 0.0f;
-        if (rvalid[ty] && cv) {
-            if (fits) {
-                double t = 0.0;
+    const float nan = __int_as_float(0x7fc00000);  // unreachable by construction; visible in parity tests
+    for (int pr = warp; pr < ZI_TH / 2; pr += 8) {
+        const int ua = 2 * pr, ub = ua + 1;
+        const int ra = oy0 - 1 + ua, rb = ra + 1;
+        const bool rva = rvalid[ua], rvb = rvalid[ub];
+        int rya[4], ryb[4];
+        double wya[4], wyb[4];
+        bool rsame = rva && rvb;
 #pragma unroll
-                for (int a = 0; a < 4; ++a) {
-                    const double* row = c2[ridx[ty][a] - ylo];
-                    const double wy = rw[ty][a];
+        for (int q = 0; q < 4; ++q) {
+            rya[q] = rva ? ridx[q][ua] - ylo : 0;
+            ryb[q] = rvb ? ridx[q][ub] - ylo : 0;
+            wya[q] = rva ? rw[q][ua] : 0.0;
+            wyb[q] = rvb ? rw[q][ub] : 0.0;
+            rsame = rsame && rya[q] == ryb[q];
+        }
+        double t00 = 0.0, t01 = 0.0, t10 = 0.0, t11 = 0.0;
+        if (fits) {
+            if (rsame && csame) {
+                double c[4][4];
+#pragma unroll
+                for (int a = 0; a < 4; ++a)
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) c[a][b] = win[rya[a]][cxa[b]];
+#pragma unroll
+                for (int a = 0; a < 4; ++a)
 #pragma unroll
                     for (int b = 0; b < 4; ++b) {
-                        double coeff = row[cx[b]];
-                        coeff *= wy;
-                        coeff *= wx[b];
-                        t += coeff;
+                        const double pa = c[a][b] * wya[a];
+                        const double pb = c[a][b] * wyb[a];
+                        t00 += pa * wxa[b];
+                        t01 += pa * wxb[b];
+                        t10 += pb * wxa[b];
+                        t11 += pb * wxb[b];
                     }
-                }
-                res = (float)t;
-                if (fp16) res = round_half(res);
             } else {
-                res = __int_as_float(0x7fc00000);  // unreachable by construction; visible in parity tests
+                if (rva && cva) t00 = zoom_term_sum(win, rya, wya, cxa, wxa);
+                if (rva && cvb) t01 = zoom_term_sum(win, rya, wya, cxb, wxb);
+                if (rvb && cva) t10 = zoom_term_sum(win, ryb, wyb, cxa, wxa);
+                if (rvb && cvb) t11 = zoom_term_sum(win, ryb, wyb, cxb, wxb);
             }
         }
-        out[(long long)r * out_pitch + x] = res;
+        const double tq[2][2] = {{t00, t01}, {t10, t11}};
+        const bool rv[2] = {rva, rvb}, cv[2] = {cva, cvb};
+        const int rr[2] = {ra, rb}, xx[2] = {xa, xb};
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            if (rr[i] < 0 || rr[i] >= OH) continue;
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                if (xx[j] < 0 || xx[j] >= OW) continue;
+                float res = 0.0f;
+                if (rv[i] && cv[j]) {
+                    res = fits ? (float)tq[i][j] : nan;
+                    if (fits && fp16) res = round_half(res);
+                }
+                out[(long long)rr[i] * out_pitch + xx[j]] = res;
+            }
+        }
     }
 }
 
@@ -505,9 +647,11 @@ static int launch_zoom2x(const uint8_t* gray, int H, int W, long long pitch, int
     k_prefilter_cols<<<dim3(ceil_div(W, PC_TW), ceil_div(H, PC_TH)), 256, 0, st>>>(gray, H, W, pitch, fp16, coef,
                                                                                   taps);
     PYSIFT_LAUNCH_CHECK("k_prefilter_cols");
-    k_zoom_rows_interp<<<dim3(ceil_div(2 * W, ZI_TW), ceil_div(2 * H, ZI_TH)), 256, 0, st>>>(coef, H, W, fp16, out,
-                                                                                            out_pitch, taps);
-    PYSIFT_LAUNCH_CHECK("k_zoom_rows_interp");
+    k_prefilter_rows<<<H, PR_NT, 0, st>>>(coef, W, taps);
+    PYSIFT_LAUNCH_CHECK("k_prefilter_rows");
+    k_zoom_interp<<<dim3(ceil_div(2 * W + 1, ZI_TW), ceil_div(2 * H + 1, ZI_TH)), 256, 0, st>>>(coef, H, W, fp16,
+                                                                                               out, out_pitch);
+    PYSIFT_LAUNCH_CHECK("k_zoom_interp");
     return PYSIFT_OK;
 }
 
@@ -573,42 +717,98 @@ __device__ __forceinline__ void blur_load_tile(const BlurArgs& a, float* tile, i
     }
 }
 
+__device__ __forceinline__ void cp_async4(float* dst, const float* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+}
+
+// Tile geometry of k_blur<R>: input rows [r0-R, r0+TH+R) and columns
+// [c0-R, c0+TW+R) at an odd row stride (lanes that own different rows hit
+// different banks), then the row-filtered rows at an odd stride of TW+1.
+template <int R>
+struct BlurTile {
+    static constexpr int ROWS = BLUR_TH + 2 * R;
+    static constexpr int TWR = BLUR_TW + 2 * R;
+    static constexpr int TS = TWR | 1;
+    static constexpr int HS = BLUR_TW + 1;
+    static constexpr size_t bytes = (size_t)(ROWS * TS + ROWS * HS) * sizeof(float);
+};
+
+// Fused H+V separable blur of one 64x32 output tile.  The tile and its
+// reflected halo are filled with cp.async (every load in flight at once;
+// reflection computed once per row and once per column), then each lane
+// row-filters 8 outputs of its own row (taps in ascending order, one fmaf
+// chain per output) and each thread column-filters 8 outputs of a column.
 template <int R>
 __global__ void __launch_bounds__(BLUR_NT) k_blur(const BlurArgs a) {
-    constexpr int TW = BLUR_TW, TH = BLUR_TH;
-    constexpr int RA = (R + 3) / 4 * 4;
-    constexpr int TWP = TW + 2 * RA, ROWS = TH + 2 * R;
+    using T = BlurTile<R>;
+    constexpr int TW = BLUR_TW, TH = BLUR_TH, ROWS = T::ROWS, TWR = T::TWR, TS = T::TS, HS = T::HS;
+    constexpr int CQ = (TWR + 31) / 32;
+    static_assert(BLUR_NT / 32 == TW / 8, "one warp per 8-column strip in the row pass");
     extern __shared__ float smem[];
     float* tile = smem;
-    float* hb = smem + ROWS * TWP;
+    float* hb = smem + ROWS * TS;
     const int c0 = blockIdx.x * TW, r0 = blockIdx.y * TH;
-    blur_load_tile(a, tile, R, RA, TWP, ROWS, r0, c0);
-    __syncthreads();
-    constexpr int SPR = TW / 8;
-    for (int sidx = threadIdx.x; sidx < ROWS * SPR; sidx += BLUR_NT) {
-        int rr = sidx / SPR, x0 = (sidx - rr * SPR) * 8;
-        const float* src = tile + rr * TWP + x0 + (RA - R);
-        float v[8 + 2 * R];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    {
+        long long gcs[CQ];
 #pragma unroll
-        for (int j = 0; j < 8 + 2 * R; ++j) v[j] = src[j];
-        float acc[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) acc[j] = 0.0f;
-#pragma unroll
-        for (int k = 0; k <= 2 * R; ++k) {
-            const float wk = a.w[k];
-#pragma unroll
-            for (int j = 0; j < 8; ++j) acc[j] = fmaf(v[j + k], wk, acc[j]);
+        for (int q = 0; q < CQ; ++q) {
+            const int cc = lane + 32 * q;
+            gcs[q] = (long long)reflect_idx(c0 - R + (cc < TWR ? cc : 0), a.W) * a.step;
         }
+        for (int rr = warp; rr < ROWS; rr += BLUR_NT / 32) {
+            const float* rowp = a.in + (long long)reflect_idx(r0 - R + rr, a.H) * a.step * a.in_pitch;
 #pragma unroll
-        for (int j = 0; j < 8; ++j) hb[rr * TW + x0 + j] = acc[j];
+            for (int q = 0; q < CQ; ++q) {
+                const int cc = lane + 32 * q;
+                if (cc < TWR) cp_async4(tile + rr * TS + cc, rowp + gcs[q]);
+            }
+        }
+        asm volatile("cp.async.wait_all;" ::: "memory");
+    }
+    __syncthreads();
+    if (a.copy0) {
+        for (int i = threadIdx.x; i < TH * TW; i += BLUR_NT) {
+            const int y = i / TW, x = i - y * TW;
+            const int orow = r0 + y, ocol = c0 + x;
+            if (orow < a.H && ocol < a.W) {
+                const float v = tile[(y + R) * TS + x + R];
+                a.copy0[(long long)orow * a.out_pitch + ocol] = v;
+                if (a.copy0_r) a.copy0_r[(long long)orow * a.out_pitch + ocol] = round_half(v);
+            }
+        }
+    }
+    {
+        const int x0 = warp * 8;
+#pragma unroll
+        for (int round = 0; round < (ROWS + 31) / 32; ++round) {
+            const int rr = round * 32 + lane;
+            if (rr < ROWS) {
+                const float* src = tile + rr * TS + x0;
+                float v[8 + 2 * R];
+#pragma unroll
+                for (int j = 0; j < 8 + 2 * R; ++j) v[j] = src[j];
+                float acc[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[j] = 0.0f;
+#pragma unroll
+                for (int k = 0; k <= 2 * R; ++k) {
+                    const float wk = a.w[k];
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) acc[j] = fmaf(v[j + k], wk, acc[j]);
+                }
+#pragma unroll
+                for (int j = 0; j < 8; ++j) hb[rr * HS + x0 + j] = acc[j];
+            }
+        }
     }
     __syncthreads();
     {
         const int col = threadIdx.x % TW, y0 = (threadIdx.x / TW) * 8;
         float v[8 + 2 * R];
 #pragma unroll
-        for (int j = 0; j < 8 + 2 * R; ++j) v[j] = hb[(y0 + j) * TW + col];
+        for (int j = 0; j < 8 + 2 * R; ++j) v[j] = hb[(y0 + j) * HS + col];
         float acc[8];
 #pragma unroll
         for (int j = 0; j < 8; ++j) acc[j] = 0.0f;
@@ -672,8 +872,19 @@ static size_t blur_smem_bytes(int R) {
 
 typedef void (*BlurKernel)(const BlurArgs);
 
-template <int R>
-static BlurKernel blur_kernel_for() { return k_blur<R>; }
+static size_t blur_fast_smem_bytes(int R) {
+    switch (R) {
+#define PYSIFT_BLUR_BYTES(r) \
+    case r: return BlurTile<r>::bytes;
+        PYSIFT_BLUR_BYTES(1) PYSIFT_BLUR_BYTES(2) PYSIFT_BLUR_BYTES(3) PYSIFT_BLUR_BYTES(4)
+        PYSIFT_BLUR_BYTES(5) PYSIFT_BLUR_BYTES(6) PYSIFT_BLUR_BYTES(7) PYSIFT_BLUR_BYTES(8)
+        PYSIFT_BLUR_BYTES(9) PYSIFT_BLUR_BYTES(10) PYSIFT_BLUR_BYTES(11) PYSIFT_BLUR_BYTES(12)
+        PYSIFT_BLUR_BYTES(13) PYSIFT_BLUR_BYTES(14) PYSIFT_BLUR_BYTES(15) PYSIFT_BLUR_BYTES(16)
+#undef PYSIFT_BLUR_BYTES
+        default: return 0;
+    }
+}
+static_assert(BlurTile<16>::bytes <= 48 * 1024, "k_blur<R> stays within the default dynamic shared memory");
 
 static BlurKernel blur_table(int R) {
     switch (R) {
@@ -717,7 +928,7 @@ static int launch_blur(BlurArgs& a, int R, const float* w, cudaStream_t st) {
     dim3 grid(ceil_div(a.W, BLUR_TW), ceil_div(a.H, BLUR_TH));
     BlurKernel kfn = (R >= 1) ? blur_table(R) : nullptr;
     if (kfn) {
-        kfn<<<grid, BLUR_NT, blur_smem_bytes(R), st>>>(a);
+        kfn<<<grid, BLUR_NT, blur_fast_smem_bytes(R), st>>>(a);
         PYSIFT_LAUNCH_CHECK("k_blur");
     } else {
         int rc = ensure_blur_attrs();
@@ -756,14 +967,21 @@ __device__ __forceinline__ int find_octave(const int* blk_off, int n_oct, int b)
 // One block = 32 rows x 32 columns of one octave (a warp per 4 rows, a mask
 // word per row and scale).  The block stages the DoG levels of its tile and
 // a one-pixel halo in shared memory (D_s = G_{s+1} - G_s, computed once per
-// position), then tests its pixels: |D| > threshold inside the border and
-// D >= all 26 neighbours or D <= all 26 neighbours.
+// position from the NL Gaussian levels, every load of the tile issued before
+// the first subtraction), then tests its pixels: |D| > threshold inside the
+// border and D >= all 26 neighbours or D <= all 26 neighbours.  Each lane k
+// < 4*S of a warp finally writes the mask word (row k / S, scale k % S + 1)
+// and adds its population to the row's count.
 constexpr int EX_ROWS = 32;
+constexpr int EX_SR = EX_ROWS + 2, EX_SW = 34, EX_SC = 35;  // staged rows, columns, padded stride
+
+template <int NL>
 __global__ void __launch_bounds__(256) k_extrema_mask(const ExtArgs a, Ctrl* ctrl) {
-    extern __shared__ float ex_smem[];
+    constexpr int S = NL - 3, ND = NL - 1;
+    constexpr int NQ = (EX_SR * EX_SW + 255) / 256;
+    __shared__ float sDm[ND * EX_SR * EX_SC];
     if (a.retry_mode && !ctrl->retried) return;
-    constexpr int SR = EX_ROWS + 2, SC = 35;  // staged rows, padded columns
-    auto sD = [&](int s, int rr, int cc) -> float& { return ex_smem[(s * SR + rr) * SC + cc]; };
+    auto sD = [&](int s, int rr, int cc) -> float& { return sDm[(s * EX_SR + rr) * EX_SC + cc]; };
     const float thr = ctrl->thr[a.thr_idx];
     const int o = find_octave(a.blk_off, a.n_oct, blockIdx.x);
     const OctView& v = a.oct[o];
@@ -771,28 +989,38 @@ __global__ void __launch_bounds__(256) k_extrema_mask(const ExtArgs a, Ctrl* ctr
     const int bl = blockIdx.x - a.blk_off[o];
     const int by = bl / wpr, wc = bl - by * wpr;
     const int r0 = by * EX_ROWS, c0 = wc * 32;
-    const int ndog = a.S + 2;
-    for (int q = threadIdx.x; q < SR * 34; q += 256) {
-        const int rr = q / 34, cc = q - rr * 34;
-        const int r = r0 - 1 + rr, c = c0 - 1 + cc;
-        const bool in = r >= 0 && r < v.H && c >= 0 && c < v.W;
-        const long long off = in ? (long long)r * v.pitch + c : 0;
-        float lo = in ? v.lev[0][off] : 0.0f;
-        for (int s = 0; s < ndog; ++s) {
-            const float hi = in ? v.lev[s + 1][off] : 0.0f;
-            sD(s, rr, cc) = hi - lo;
-            lo = hi;
+    {
+        float g[NQ][NL];
+#pragma unroll
+        for (int k = 0; k < NQ; ++k) {
+            const int q = threadIdx.x + 256 * k;
+            const int rr = q / EX_SW, cc = q - rr * EX_SW;
+            const int r = r0 - 1 + rr, c = c0 - 1 + cc;
+            const bool in = q < EX_SR * EX_SW && r >= 0 && r < v.H && c >= 0 && c < v.W;
+            const long long off = in ? (long long)r * v.pitch + c : 0;
+#pragma unroll
+            for (int l = 0; l < NL; ++l) g[k][l] = in ? v.lev[l][off] : 0.0f;
+        }
+#pragma unroll
+        for (int k = 0; k < NQ; ++k) {
+            const int q = threadIdx.x + 256 * k;
+            if (q >= EX_SR * EX_SW) break;
+            const int rr = q / EX_SW, cc = q - rr * EX_SW;
+#pragma unroll
+            for (int s = 0; s < ND; ++s) sD(s, rr, cc) = g[k][s + 1] - g[k][s];
         }
     }
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int c = c0 + lane;
     const int B = a.border;
+    unsigned mine = 0;  // the mask word this lane writes
+#pragma unroll
     for (int i = 0; i < EX_ROWS / 8; ++i) {
         const int lr = warp + 8 * i, r = r0 + lr;
-        if (r >= v.H) break;
         const bool inb = (r >= B && r < v.H - B && c >= B && c < v.W - B);
-        for (int s = 1; s <= a.S; ++s) {
+#pragma unroll
+        for (int s = 1; s <= S; ++s) {
             bool ext = false;
             if (inb) {
                 const float val = sD(s, lr + 1, lane + 1);
@@ -813,15 +1041,32 @@ __global__ void __launch_bounds__(256) k_extrema_mask(const ExtArgs a, Ctrl* ctr
                 }
             }
             const unsigned m = __ballot_sync(FULL_MASK, ext);
-            if (lane == 0) {
-                a.mask[o][((long long)(s - 1) * v.H + r) * wpr + wc] = m;
-                if (m) atomicAdd(&a.rowcnt[o][(s - 1) * v.H + r], __popc(m));
-            }
+            if (lane == i * S + (s - 1)) mine = m;
+        }
+    }
+    if (lane < (EX_ROWS / 8) * S) {
+        const int i = lane / S, s = lane - i * S + 1;
+        const int r = r0 + warp + 8 * i;
+        if (r < v.H) {
+            a.mask[o][((long long)(s - 1) * v.H + r) * wpr + wc] = mine;
+            if (mine) atomicAdd(&a.rowcnt[o][(s - 1) * v.H + r], __popc(mine));
         }
     }
 }
 
-static size_t extrema_smem_bytes(int S) { return (size_t)(S + 2) * (EX_ROWS + 2) * 35 * sizeof(float); }
+typedef void (*ExtremaKernel)(const ExtArgs, Ctrl*);
+
+static ExtremaKernel extrema_kernel(int S) {
+    switch (S + 3) {
+        case 4: return k_extrema_mask<4>;
+        case 5: return k_extrema_mask<5>;
+        case 6: return k_extrema_mask<6>;
+        case 7: return k_extrema_mask<7>;
+        case 8: return k_extrema_mask<8>;
+        default: return nullptr;
+    }
+}
+static_assert(PYSIFT_MAX_LEVELS == 8, "extrema_kernel covers n_scales 1..5");
 
 __global__ void __launch_bounds__(1024) k_rowscan(const ExtArgs a, Ctrl* ctrl) {
     if (a.retry_mode && !ctrl->retried) return;
@@ -1815,9 +2060,8 @@ static int run_detect(const pysift_detect_config* cfg, const uint8_t* gray, int 
     PYSIFT_CUDA_TRY(cudaMemsetAsync(ctrl, 0, sizeof(Ctrl), st));
     // A1
     {
-        const int gx = ceil_div(W, 256);
-        int gy = std::max(1, std::min(H, (num_sms() * 4) / gx));
-        k_histogram<<<dim3(gx, gy), 256, 0, st>>>(gray, H, W, pitch, ctrl, cfg->contrast_thresh, S);
+        const int blocks = std::max(1, std::min(ceil_div(H, 8), num_sms() * 2));
+        k_histogram<<<blocks, 256, 0, st>>>(gray, H, W, pitch, ctrl, cfg->contrast_thresh, S);
         PYSIFT_LAUNCH_CHECK("k_histogram");
     }
     // A2/A3: base image
@@ -1921,7 +2165,7 @@ static int run_detect(const pysift_detect_config* cfg, const uint8_t* gray, int 
         ea.thr_idx = ra.thr_idx = pass;
         ea.retry_mode = ra.retry_mode = pass;
         PYSIFT_CUDA_TRY(cudaMemsetAsync(at<char>(ws, l.off_rowcnt_base), 0, l.rowcnt_bytes_total, st));
-        k_extrema_mask<<<mask_blocks, 256, extrema_smem_bytes(S), st>>>(ea, ctrl);
+        extrema_kernel(S)<<<mask_blocks, 256, 0, st>>>(ea, ctrl);
         PYSIFT_LAUNCH_CHECK("k_extrema_mask");
         if (pass == 0) PYSIFT_STAGE(3);
         k_rowscan<<<n_oct, 1024, 0, st>>>(ea, ctrl);
