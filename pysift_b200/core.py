@@ -266,11 +266,18 @@ class PySIFT:
         key = ("one", H, W, slot, bytes(self._cfg))
         ent = self._graphs.get(key)
         if ent is None:
-            self._launch(b, b.gray.data_ptr(), H, W, W, st.cuda_stream)
+            # the eager run goes on the capture stream, so the library's
+            # per-stream side stream exists before the capture opens
+            cap = self._capture_stream()
+            cap.wait_stream(st)
+            with torch.cuda.stream(cap):
+                self._launch(b, b.gray.data_ptr(), H, W, W, cap.cuda_stream)
+            st.wait_stream(cap)
+            cap.synchronize()
             n0 = self._lib.pysift_launch_count()
             g = torch.cuda.CUDAGraph()
-            with torch.cuda.graph(g, stream=torch.cuda.Stream(self.device)):
-                self._launch(b, b.gray.data_ptr(), H, W, W, torch.cuda.current_stream(self.device).cuda_stream)
+            with torch.cuda.graph(g, stream=cap):
+                self._launch(b, b.gray.data_ptr(), H, W, W, cap.cuda_stream)
             n = self._lib.pysift_launch_count() - n0
             self._lib.pysift_count_launches(-n)  # captured, not run
             self._graphs[key] = (g, n)
@@ -279,6 +286,11 @@ class PySIFT:
         with torch.cuda.stream(st):
             g.replay()
         self._lib.pysift_count_launches(n)
+
+    def _capture_stream(self):
+        if getattr(self, "_cap_stream", None) is None:
+            self._cap_stream = torch.cuda.Stream(self.device)
+        return self._cap_stream
 
     def _upload(self, gray, b):
         """Host numpy image -> pinned staging -> device (async on the current stream)."""

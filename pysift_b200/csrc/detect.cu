@@ -2039,6 +2039,52 @@ static int num_sms() {
     return g_num_sms;
 }
 
+// A second stream paired with each caller stream (per host thread and
+// device), with events reused from call to call: work that only depends on
+// part of the pyramid (the entropy histogram; levels S+1 and S+2 of each
+// octave, which no later octave reads) runs there, forked from and joined
+// back into the caller's stream, inside a CUDA graph capture too.  The pair
+// is created on the first call made with that caller stream outside a
+// capture; a call that captures on a stream without a pair returns null
+// here and runs everything on the caller's stream (no objects are created
+// while a capture is open).
+struct SidePair {
+    int dev;
+    cudaStream_t main, side;
+    cudaEvent_t ev[PYSIFT_MAX_OCTAVES + 2];
+};
+
+static SidePair* side_pair(cudaStream_t st) {
+    constexpr int MAXP = 64;
+    thread_local SidePair pairs[MAXP];
+    thread_local int n = 0;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        set_error("side_pair: no current device");
+        return nullptr;
+    }
+    for (int i = 0; i < n; ++i)
+        if (pairs[i].dev == dev && pairs[i].main == st) return &pairs[i];
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return nullptr;
+    if (n == MAXP) return nullptr;
+    SidePair p{};
+    p.dev = dev;
+    p.main = st;
+    if (cudaStreamCreateWithFlags(&p.side, cudaStreamNonBlocking) != cudaSuccess) {
+        set_error("side_pair: cudaStreamCreateWithFlags failed");
+        return nullptr;
+    }
+    for (auto& e : p.ev) {
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+            set_error("side_pair: cudaEventCreateWithFlags failed");
+            return nullptr;
+        }
+    }
+    pairs[n] = p;
+    return &pairs[n++];
+}
+
 static int record_stage(void* const* ev, int i, cudaStream_t st) {
     if (ev && ev[i]) PYSIFT_CUDA_TRY(cudaEventRecord(reinterpret_cast<cudaEvent_t>(ev[i]), st));
     return PYSIFT_OK;
@@ -2058,10 +2104,16 @@ static int run_detect(const pysift_detect_config* cfg, const uint8_t* gray, int 
     const int cap = cfg->max_cands_per_octave, kcap = cfg->keypoint_cap;
     Ctrl* ctrl = at<Ctrl>(ws, l.off_ctrl);
     PYSIFT_CUDA_TRY(cudaMemsetAsync(ctrl, 0, sizeof(Ctrl), st));
-    // A1
+    SidePair* sp = side_pair(st);  // null: everything on st
+    const cudaStream_t side = sp ? sp->side : st;
+    if (sp) {
+        PYSIFT_CUDA_TRY(cudaEventRecord(sp->ev[0], st));
+        PYSIFT_CUDA_TRY(cudaStreamWaitEvent(side, sp->ev[0], 0));
+    }
+    // A1 (side stream; read by the extrema test after the join)
     {
         const int blocks = std::max(1, std::min(ceil_div(H, 8), num_sms() * 2));
-        k_histogram<<<blocks, 256, 0, st>>>(gray, H, W, pitch, ctrl, cfg->contrast_thresh, S);
+        k_histogram<<<blocks, 256, 0, side>>>(gray, H, W, pitch, ctrl, cfg->contrast_thresh, S);
         PYSIFT_LAUNCH_CHECK("k_histogram");
     }
     // A2/A3: base image
@@ -2099,6 +2151,15 @@ static int run_detect(const pysift_detect_config* cfg, const uint8_t* gray, int 
                 if (rc) return rc;
             }
             for (int s = 0; s < S + 2; ++s) {
+                // levels S+1 and S+2 on the side stream, once level S exists
+                cudaStream_t ls = st;
+                if (s >= S) {
+                    ls = side;
+                    if (s == S && sp) {
+                        PYSIFT_CUDA_TRY(cudaEventRecord(sp->ev[1 + o], st));
+                        PYSIFT_CUDA_TRY(cudaStreamWaitEvent(side, sp->ev[1 + o], 0));
+                    }
+                }
                 memset(&a, 0, sizeof(a));
                 a.H = l.H[o];
                 a.W = l.W[o];
@@ -2117,10 +2178,14 @@ static int run_detect(const pysift_detect_config* cfg, const uint8_t* gray, int 
                 }
                 a.out = pyr + (size_t)(s + 1) * lev;
                 a.out_r = pyr_r ? pyr_r + (size_t)(s + 1) * lev : nullptr;
-                int rc = launch_blur(a, cfg->blur_radius[2 + s], cfg->blur_weights[2 + s], st);
+                int rc = launch_blur(a, cfg->blur_radius[2 + s], cfg->blur_weights[2 + s], ls);
                 if (rc) return rc;
             }
         }
+    }
+    if (sp) {
+        PYSIFT_CUDA_TRY(cudaEventRecord(sp->ev[PYSIFT_MAX_OCTAVES + 1], side));
+        PYSIFT_CUDA_TRY(cudaStreamWaitEvent(st, sp->ev[PYSIFT_MAX_OCTAVES + 1], 0));
     }
     PYSIFT_STAGE(2);
     // A7/A8 (+ retry)
