@@ -658,6 +658,8 @@ static int launch_zoom2x(const uint8_t* gray, int H, int W, long long pitch, int
 // ---------------------------------------------------------------------------
 // A4/A5: fused separable blur.
 // ---------------------------------------------------------------------------
+constexpr int BLUR_PAIR_MAX_R = 16;  // radii with a register-blocked kernel
+
 struct BlurArgs {
     const float* in;
     long long in_pitch;
@@ -669,6 +671,7 @@ struct BlurArgs {
     int out_pitch;
     int H, W;
     float w[PYSIFT_MAX_TAPS];
+    unsigned long long w2[2 * BLUR_PAIR_MAX_R + 1];  // (w[k], w[k]) packed, radii up to BLUR_PAIR_MAX_R
 };
 
 // Half-sample-symmetric reflection into [0, n) (period 2n), as the
@@ -722,30 +725,73 @@ __device__ __forceinline__ void cp_async4(float* dst, const float* src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
 }
 
+// Packed single-precision pairs: fma.rn.f32x2 is an IEEE fused multiply-add
+// with round-to-nearest on each half, the same result as fmaf per element.
+__device__ __forceinline__ unsigned long long ffma2(unsigned long long a, unsigned long long b,
+                                                    unsigned long long c) {
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ unsigned long long pack2(float lo, float hi) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ float lo2(unsigned long long v) { return __uint_as_float((unsigned)(v & 0xffffffffull)); }
+__device__ __forceinline__ float hi2(unsigned long long v) { return __uint_as_float((unsigned)(v >> 32)); }
+
 // Tile geometry of k_blur<R>: input rows [r0-R, r0+TH+R) and columns
-// [c0-R, c0+TW+R) at an odd row stride (lanes that own different rows hit
-// different banks), then the row-filtered rows at an odd stride of TW+1.
+// [c0-R, c0+TW+R) at a row stride TS = 2 (mod 4) (8-byte aligned rows; lanes
+// that own consecutive rows read 8-byte pairs from distinct banks), then the
+// row-filtered rows at the stride HS = 66, also 2 (mod 4).
 template <int R>
 struct BlurTile {
     static constexpr int ROWS = BLUR_TH + 2 * R;
     static constexpr int TWR = BLUR_TW + 2 * R;
-    static constexpr int TS = TWR | 1;
-    static constexpr int HS = BLUR_TW + 1;
+    static constexpr int TS = (TWR % 4 == 2) ? TWR : TWR + 2;
+    static constexpr int HS = BLUR_TW + 2;
     static constexpr size_t bytes = (size_t)(ROWS * TS + ROWS * HS) * sizeof(float);
 };
 
+// Row filter of 8 outputs src[0..7] (+R halo each side) of one tile row into
+// dst[0..7]: 4 output pairs, one packed fma per pair and tap, taps in
+// ascending order.  Pairs at even offsets are loaded as 8-byte words; the
+// pairs at odd offsets are formed from their neighbours.
+template <int R>
+__device__ __forceinline__ void blur_row_strip(const float* src, float* dst, const unsigned long long* w2) {
+    constexpr int NP = 4 + R;
+    unsigned long long E[NP], O[NP - 1];
+#pragma unroll
+    for (int m = 0; m < NP; ++m) E[m] = reinterpret_cast<const unsigned long long*>(src)[m];
+#pragma unroll
+    for (int m = 0; m < NP - 1; ++m) O[m] = pack2(hi2(E[m]), lo2(E[m + 1]));
+    unsigned long long A[4] = {0ull, 0ull, 0ull, 0ull};
+#pragma unroll
+    for (int k = 0; k <= 2 * R; ++k) {
+        const unsigned long long wk = w2[k];
+#pragma unroll
+        for (int p = 0; p < 4; ++p) A[p] = ffma2((k & 1) ? O[p + (k >> 1)] : E[p + (k >> 1)], wk, A[p]);
+    }
+#pragma unroll
+    for (int p = 0; p < 4; ++p) reinterpret_cast<unsigned long long*>(dst)[p] = A[p];
+}
+
 // Fused H+V separable blur of one 64x32 output tile.  The tile and its
 // reflected halo are filled with cp.async (every load in flight at once;
-// reflection computed once per row and once per column), then each lane
-// row-filters 8 outputs of its own row (taps in ascending order, one fmaf
-// chain per output) and each thread column-filters 8 outputs of a column.
+// reflection computed once per row and once per column).  Row pass: a lane
+// per tile row (the rows past the first 32 packed densely onto the first
+// warps), 8 outputs per lane.  Column pass: each thread filters a pair of
+// adjacent columns over 4 rows.  Both passes use packed fma pairs; each
+// output is the same fmaf chain over the taps in ascending order.
 template <int R>
 __global__ void __launch_bounds__(BLUR_NT) k_blur(const BlurArgs a) {
     using T = BlurTile<R>;
     constexpr int TW = BLUR_TW, TH = BLUR_TH, ROWS = T::ROWS, TWR = T::TWR, TS = T::TS, HS = T::HS;
     constexpr int CQ = (TWR + 31) / 32;
     static_assert(BLUR_NT / 32 == TW / 8, "one warp per 8-column strip in the row pass");
-    extern __shared__ float smem[];
+    static_assert(BLUR_NT == (TW / 2) * (TH / 4), "one thread per column pair and 4 rows in the column pass");
+    extern __shared__ __align__(16) float smem[];
     float* tile = smem;
     float* hb = smem + ROWS * TS;
     const int c0 = blockIdx.x * TW, r0 = blockIdx.y * TH;
@@ -780,52 +826,48 @@ __global__ void __launch_bounds__(BLUR_NT) k_blur(const BlurArgs a) {
         }
     }
     {
-        const int x0 = warp * 8;
+        constexpr int NF = ROWS / 32, N2 = ROWS % 32;
 #pragma unroll
-        for (int round = 0; round < (ROWS + 31) / 32; ++round) {
+        for (int round = 0; round < NF; ++round) {
             const int rr = round * 32 + lane;
-            if (rr < ROWS) {
-                const float* src = tile + rr * TS + x0;
-                float v[8 + 2 * R];
-#pragma unroll
-                for (int j = 0; j < 8 + 2 * R; ++j) v[j] = src[j];
-                float acc[8];
-#pragma unroll
-                for (int j = 0; j < 8; ++j) acc[j] = 0.0f;
-#pragma unroll
-                for (int k = 0; k <= 2 * R; ++k) {
-                    const float wk = a.w[k];
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) acc[j] = fmaf(v[j + k], wk, acc[j]);
-                }
-#pragma unroll
-                for (int j = 0; j < 8; ++j) hb[rr * HS + x0 + j] = acc[j];
-            }
+            blur_row_strip<R>(tile + rr * TS + warp * 8, hb + rr * HS + warp * 8, a.w2);
+        }
+        if (N2 > 0 && threadIdx.x < N2 * 8) {
+            const int rr = NF * 32 + threadIdx.x % N2, x0 = (threadIdx.x / N2) * 8;
+            blur_row_strip<R>(tile + rr * TS + x0, hb + rr * HS + x0, a.w2);
         }
     }
     __syncthreads();
     {
-        const int col = threadIdx.x % TW, y0 = (threadIdx.x / TW) * 8;
-        float v[8 + 2 * R];
+        const int cp = lane, y0 = warp * 4;
+        constexpr int NV = 4 + 2 * R;
+        unsigned long long V[NV];
 #pragma unroll
-        for (int j = 0; j < 8 + 2 * R; ++j) v[j] = hb[(y0 + j) * HS + col];
-        float acc[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) acc[j] = 0.0f;
+        for (int m = 0; m < NV; ++m) V[m] = reinterpret_cast<const unsigned long long*>(hb + (y0 + m) * HS)[cp];
+        unsigned long long A[4] = {0ull, 0ull, 0ull, 0ull};
 #pragma unroll
         for (int k = 0; k <= 2 * R; ++k) {
-            const float wk = a.w[k];
+            const unsigned long long wk = a.w2[k];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) acc[j] = fmaf(v[j + k], wk, acc[j]);
+            for (int j = 0; j < 4; ++j) A[j] = ffma2(V[j + k], wk, A[j]);
         }
-        const int gc = c0 + col;
-        if (gc < a.W) {
+        const int gc = c0 + 2 * cp;
+        const bool vec = gc + 1 < a.W && (a.out_pitch & 1) == 0;
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                int gr = r0 + y0 + j;
-                if (gr < a.H) {
-                    a.out[(long long)gr * a.out_pitch + gc] = acc[j];
-                    if (a.out_r) a.out_r[(long long)gr * a.out_pitch + gc] = round_half(acc[j]);
+        for (int j = 0; j < 4; ++j) {
+            const int gr = r0 + y0 + j;
+            if (gr >= a.H || gc >= a.W) continue;
+            const float v0 = lo2(A[j]), v1 = hi2(A[j]);
+            const long long off = (long long)gr * a.out_pitch + gc;
+            if (vec) {
+                *reinterpret_cast<float2*>(a.out + off) = make_float2(v0, v1);
+                if (a.out_r) *reinterpret_cast<float2*>(a.out_r + off) = make_float2(round_half(v0), round_half(v1));
+            } else {
+                a.out[off] = v0;
+                if (a.out_r) a.out_r[off] = round_half(v0);
+                if (gc + 1 < a.W) {
+                    a.out[off + 1] = v1;
+                    if (a.out_r) a.out_r[off + 1] = round_half(v1);
                 }
             }
         }
@@ -925,6 +967,11 @@ static int ensure_blur_attrs() {
 
 static int launch_blur(BlurArgs& a, int R, const float* w, cudaStream_t st) {
     for (int k = 0; k <= 2 * R; ++k) a.w[k] = w[k];
+    for (int k = 0; k <= 2 * R && k <= 2 * BLUR_PAIR_MAX_R; ++k) {
+        unsigned u = 0;
+        memcpy(&u, &w[k], sizeof(u));
+        a.w2[k] = ((unsigned long long)u << 32) | u;
+    }
     dim3 grid(ceil_div(a.W, BLUR_TW), ceil_div(a.H, BLUR_TH));
     BlurKernel kfn = (R >= 1) ? blur_table(R) : nullptr;
     if (kfn) {
