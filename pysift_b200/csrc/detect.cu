@@ -63,7 +63,8 @@ struct Ctrl {
     int capped;
     int n_oriented;
     int overflow_octs;
-    int pad[2];
+    int desc_next;  // next oriented entry a descriptor block takes
+    int pad[1];
 };
 
 struct OctView {
@@ -1847,10 +1848,22 @@ __device__ __forceinline__ void desc_accumulate(const float* __restrict__ g, lon
     const int band_c = (side + DESC_GC - 1) / DESC_GC;  // columns per column band
     const int runs = (band_c + DESC_L - 1) / DESC_L;    // DESC_L-pixel runs per band row
     const int nsteps = band_r * runs;
+    // step t -> (u, v) = (t / runs, t % runs), advanced by DESC_W steps at a
+    // time with one carry instead of a division per step
+    const int du = DESC_W / runs, dv = DESC_W - du * runs;
+    int u = warp / runs, v = warp - u * runs;
+    const int pr0 = gi * band_r, pc0 = gj * band_c + k;
+    unsigned* const lo = hw.lo;
+    unsigned* const hi = hw.hi;
     int steps = 0;
     for (int t = warp; t < nsteps; t += DESC_W) {
-        const int u = t / runs, v = t - u * runs;
-        const int pr = gi * band_r + u, pcb = v * DESC_L + k, pc = gj * band_c + pcb;
+        const int pr = pr0 + u, pcb = v * DESC_L + k, pc = pc0 + v * DESC_L;
+        v += dv;
+        u += du;
+        if (v >= runs) {
+            v -= runs;
+            ++u;
+        }
         const int r_off = pr - ph, c_off = pc - ph;
         const int rr = r0 + r_off, cc = c0 + c_off;
         bool act = pr < side && pcb < band_c && pc < side && !(rr < 1 || rr >= H - 1 || cc < 1 || cc >= W - 1);
@@ -1873,23 +1886,32 @@ __device__ __forceinline__ void desc_accumulate(const float* __restrict__ g, lon
             float df = ob - (float)oi0;
             int xi0 = (int)floorf(xb), yi0 = (int)floorf(yb);
             float dx_b = xb - (float)xi0, dy_b = yb - (float)yi0;
-            int xi0c = max(0, min(xi0, 3));
-            int yi0c = max(0, min(yi0, 3));
-            int xi1c = max(0, min(xi0 + 1, 3));
-            int yi1c = max(0, min(yi0 + 1, 3));
-            int oi0w = ((oi0 % 8) + 8) % 8;
-            int oi1w = ((oi0 + 1) % 8 + 8) % 8;
+            const int xi0c = max(0, min(xi0, 3));
+            const int yi0c = max(0, min(yi0, 3));
+            const int xi1c = max(0, min(xi0 + 1, 3));
+            const int yi1c = max(0, min(yi0 + 1, 3));
+            // orientation bins mod 8 (two's complement & 7 is the
+            // non-negative remainder for every int)
+            const int oi0w = oi0 & 7, oi1w = (oi0 + 1) & 7;
             float w_y0 = 1.0f - dy_b, w_y1 = dy_b;
             float w_x0 = 1.0f - dx_b, w_x1 = dx_b;
             float w_o0 = 1.0f - df, w_o1 = df;
-            hw.add(yi0c * 32 + xi0c * 8 + oi0w, fix40(w_y0 * w_x0 * w_o0 * wmag));
-            hw.add(yi0c * 32 + xi0c * 8 + oi1w, fix40(w_y0 * w_x0 * w_o1 * wmag));
-            hw.add(yi0c * 32 + xi1c * 8 + oi0w, fix40(w_y0 * w_x1 * w_o0 * wmag));
-            hw.add(yi0c * 32 + xi1c * 8 + oi1w, fix40(w_y0 * w_x1 * w_o1 * wmag));
-            hw.add(yi1c * 32 + xi0c * 8 + oi0w, fix40(w_y1 * w_x0 * w_o0 * wmag));
-            hw.add(yi1c * 32 + xi0c * 8 + oi1w, fix40(w_y1 * w_x0 * w_o1 * wmag));
-            hw.add(yi1c * 32 + xi1c * 8 + oi0w, fix40(w_y1 * w_x1 * w_o0 * wmag));
-            hw.add(yi1c * 32 + xi1c * 8 + oi1w, fix40(w_y1 * w_x1 * w_o1 * wmag));
+            // shared-memory word of bin y*32 + x*8 + o: the descriptor
+            // histograms store it at y*32 + ((x ^ y) << 3) + o
+            const int b00 = yi0c * 32 + ((xi0c ^ yi0c) << 3), b01 = yi0c * 32 + ((xi1c ^ yi0c) << 3);
+            const int b10 = yi1c * 32 + ((xi0c ^ yi1c) << 3), b11 = yi1c * 32 + ((xi1c ^ yi1c) << 3);
+            const unsigned long long q[8] = {
+                fix40(w_y0 * w_x0 * w_o0 * wmag), fix40(w_y0 * w_x0 * w_o1 * wmag),
+                fix40(w_y0 * w_x1 * w_o0 * wmag), fix40(w_y0 * w_x1 * w_o1 * wmag),
+                fix40(w_y1 * w_x0 * w_o0 * wmag), fix40(w_y1 * w_x0 * w_o1 * wmag),
+                fix40(w_y1 * w_x1 * w_o0 * wmag), fix40(w_y1 * w_x1 * w_o1 * wmag)};
+            const int pb[8] = {b00 + oi0w, b00 + oi1w, b01 + oi0w, b01 + oi1w,
+                               b10 + oi0w, b10 + oi1w, b11 + oi0w, b11 + oi1w};
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                atomicAdd(lo + pb[c], (unsigned)q[c] & 0x1fffffu);
+                atomicAdd(hi + pb[c], (unsigned)(q[c] >> 21));
+            }
         }
         if (++steps == FOLD_STEPS) {
             hw.fold();
@@ -1921,16 +1943,24 @@ __device__ __forceinline__ float bins_sum(float x, float* part) {
     return s;
 }
 
-// One DESC_T-thread block per oriented keypoint (grid-stride).  Warps
-// accumulate into private fixed-point histograms; threads 0..127 then own one
-// bin each for the merge, normalisation and RootSIFT.
-__global__ void __launch_bounds__(DESC_T) k_descriptor(const DescArgs a, const Ctrl* ctrl) {
+// One DESC_T-thread block per oriented keypoint at a time; a block takes its
+// next entry from a counter (entries differ in patch size, so blocks stay
+// busy until the list is done; every entry writes its own output row).
+// Warps accumulate into private fixed-point histograms; threads 0..127 then
+// own one bin each for the merge, normalisation and RootSIFT.
+__global__ void __launch_bounds__(DESC_T, 5) k_descriptor(const DescArgs a, Ctrl* ctrl) {
     __shared__ unsigned int wlo[DESC_W][128], whi[DESC_W][128];
     __shared__ unsigned long long whist[DESC_W][128];
     __shared__ float part[4];
+    __shared__ int s_entry[2];  // alternates, so a late reader never sees the next entry
     const int tid = threadIdx.x, warp = tid >> 5;
     const int n = ctrl->n_oriented;
-    for (int e = blockIdx.x; e < n; e += gridDim.x) {
+    // the first entry is the block index, later ones come from the counter;
+    // the next index is requested when an entry starts and read when it ends
+    int e = blockIdx.x;
+    for (int it = 0; e < n; ++it) {
+        int next = 0;
+        if (tid == 0) next = (int)gridDim.x + atomicAdd(&ctrl->desc_next, 1);
         for (int b = tid; b < DESC_W * 128; b += DESC_T) {
             (&whist[0][0])[b] = 0ull;
             (&wlo[0][0])[b] = 0u;
@@ -1938,60 +1968,61 @@ __global__ void __launch_bounds__(DESC_T) k_descriptor(const DescArgs a, const C
         }
         __syncthreads();
         int row = a.rank[e];
-        if (a.limit > 0 && n > a.limit) {
-            row = a.lrank[row];
-            if (row >= a.limit) continue;  // the whole block skips this entry
-        }
-        const int kp = a.ent_kp[e], slot = a.ent_slot[e];
-        const int o = a.kp_o[kp], si = a.kp_si[kp];
-        const float ri = a.kp_ri[kp], ci = a.kp_ci[kp];
-        const float angle = a.ang[kp * 4 + slot];
-        const float ang_rad = angle * (float)(3.14159265358979323846 / 180.0);
-        const float phf = a.desc_ph[si];
-        const OctView& v = a.oct[o];
-        float sin_a, cos_a;
-        sm::sincosf_(ang_rad, &sin_a, &cos_a);
-        const float* g = v.lev[si];
-        const WarpHist hw{wlo[warp], whi[warp], whist[warp], 128};
-        if (a.n_dsp > 0) {
-            for (int dd = 0; dd < a.n_dsp; ++dd) {
-                int ph = (int)(phf * a.dsp_scales[dd] + 0.5f);
-                if (ph < 4) ph = 4;
-                desc_accumulate(g, v.pitch, v.H, v.W, ri, ci, cos_a, sin_a, ang_rad, ph, hw, tid);
+        if (a.limit > 0 && n > a.limit) row = a.lrank[row];
+        if (!(a.limit > 0 && n > a.limit) || row < a.limit) {  // else the whole block skips this entry
+            const int kp = a.ent_kp[e], slot = a.ent_slot[e];
+            const int o = a.kp_o[kp], si = a.kp_si[kp];
+            const float ri = a.kp_ri[kp], ci = a.kp_ci[kp];
+            const float angle = a.ang[kp * 4 + slot];
+            const float ang_rad = angle * (float)(3.14159265358979323846 / 180.0);
+            const float phf = a.desc_ph[si];
+            const OctView& v = a.oct[o];
+            float sin_a, cos_a;
+            sm::sincosf_(ang_rad, &sin_a, &cos_a);
+            const float* g = v.lev[si];
+            const WarpHist hw{wlo[warp], whi[warp], whist[warp], 128};
+            if (a.n_dsp > 0) {
+                for (int dd = 0; dd < a.n_dsp; ++dd) {
+                    int ph = (int)(phf * a.dsp_scales[dd] + 0.5f);
+                    if (ph < 4) ph = 4;
+                    desc_accumulate(g, v.pitch, v.H, v.W, ri, ci, cos_a, sin_a, ang_rad, ph, hw, tid);
+                }
+            } else {
+                desc_accumulate(g, v.pitch, v.H, v.W, ri, ci, cos_a, sin_a, ang_rad, (int)phf, hw, tid);
             }
-        } else {
-            desc_accumulate(g, v.pitch, v.H, v.W, ri, ci, cos_a, sin_a, ang_rad, (int)phf, hw, tid);
+            __syncthreads();
+            if (tid < 128) {
+                unsigned long long s = 0ull;
+    #pragma unroll
+                for (int w = 0; w < DESC_W; ++w) s += whist[w][tid];
+                float val = unfix40(s);
+                if (a.n_dsp > 0) val = val * (1.0f / (float)a.n_dsp);
+                float inv = 1.0f / sqrtf(bins_sum(val * val, part) + 1e-14f);
+                float t = val * inv;
+                val = t > 0.2f ? 0.2f : t;
+                inv = 1.0f / sqrtf(bins_sum(val * val, part) + 1e-14f);
+                val = val * inv;
+                if (a.rootsift) {
+                    const float den = bins_sum(fabsf(val), part) + 1e-7f;
+                    float q = val / den;
+                    if (q < 0.0f) q = 0.0f;
+                    val = sqrtf(q);
+                }
+                a.out_desc[(long long)row * 128 + tid] = val;
+                if (tid == 0) {
+                    const float sc = a.coord_scale[o];
+                    a.out_kpts[row * 4 + 0] = ci * sc;
+                    a.out_kpts[row * 4 + 1] = ri * sc;
+                    a.out_kpts[row * 4 + 2] = a.kp_size[o][si];
+                    a.out_kpts[row * 4 + 3] = angle;
+                    a.out_resp[row] = a.kp_resp[kp];
+                    a.out_oct[row] = o;
+                }
+            }
         }
+        if (tid == 0) s_entry[it & 1] = next;
         __syncthreads();
-        if (tid < 128) {
-            unsigned long long s = 0ull;
-#pragma unroll
-            for (int w = 0; w < DESC_W; ++w) s += whist[w][tid];
-            float val = unfix40(s);
-            if (a.n_dsp > 0) val = val * (1.0f / (float)a.n_dsp);
-            float inv = 1.0f / sqrtf(bins_sum(val * val, part) + 1e-14f);
-            float t = val * inv;
-            val = t > 0.2f ? 0.2f : t;
-            inv = 1.0f / sqrtf(bins_sum(val * val, part) + 1e-14f);
-            val = val * inv;
-            if (a.rootsift) {
-                const float den = bins_sum(fabsf(val), part) + 1e-7f;
-                float q = val / den;
-                if (q < 0.0f) q = 0.0f;
-                val = sqrtf(q);
-            }
-            a.out_desc[(long long)row * 128 + tid] = val;
-            if (tid == 0) {
-                const float sc = a.coord_scale[o];
-                a.out_kpts[row * 4 + 0] = ci * sc;
-                a.out_kpts[row * 4 + 1] = ri * sc;
-                a.out_kpts[row * 4 + 2] = a.kp_size[o][si];
-                a.out_kpts[row * 4 + 3] = angle;
-                a.out_resp[row] = a.kp_resp[kp];
-                a.out_oct[row] = o;
-            }
-        }
-        __syncthreads();
+        e = s_entry[it & 1];
     }
 }
 
@@ -2389,7 +2420,7 @@ static int run_detect(const pysift_detect_config* cfg, const uint8_t* gray, int 
     da.out_resp = resp;
     da.out_oct = octv;
     da.out_desc = desc;
-    k_descriptor<<<std::min(4 * kcap, num_sms() * (2048 / DESC_T)), DESC_T, 0, st>>>(da, ctrl);
+    k_descriptor<<<std::min(4 * kcap, num_sms() * 5), DESC_T, 0, st>>>(da, ctrl);
     PYSIFT_LAUNCH_CHECK("k_descriptor");
     k_finalize<<<1, 32, 0, st>>>(ctrl, stats, n_oct, l.doubled ? 1 : 0, cfg->output_limit);
     PYSIFT_LAUNCH_CHECK("k_finalize");
