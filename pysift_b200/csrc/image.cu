@@ -58,10 +58,36 @@ __global__ void __launch_bounds__(256) k_clahe_lut(const ClaheArgs a) {
     if (t == 0) s_clipped = 0;
     __syncthreads();
     const int x0 = tx * a.tile_w, y0 = ty * a.tile_h;
-    for (int i = t; i < a.tile_w * a.tile_h; i += 256) {
-        const int yy = y0 + i / a.tile_w, xx = x0 + i % a.tile_w;
-        const uint8_t v = a.src[(long long)reflect101(yy, a.H) * a.pitch + reflect101(xx, a.W)];
-        atomicAdd(&hist[v], 1u);
+    {
+        // element i = t + 256 k of the tile, walked without a division per
+        // element; loads go out CL_B at a time before their counts
+        constexpr int CL_B = 16;
+        const int area = a.tile_w * a.tile_h;
+        const int sy = 256 / a.tile_w, sx = 256 - sy * a.tile_w;
+        int yy = t / a.tile_w, xx = t - yy * a.tile_w;
+        const bool inside = y0 + a.tile_h <= a.H && x0 + a.tile_w <= a.W;
+        for (int i0 = t; i0 < area; i0 += 256 * CL_B) {
+            uint8_t v[CL_B];
+#pragma unroll
+            for (int k = 0; k < CL_B; ++k) {
+                v[k] = 0;
+                if (i0 + 256 * k < area) {
+                    const int gy = y0 + yy, gx = x0 + xx;
+                    const long long off = inside ? (long long)gy * a.pitch + gx
+                                                 : (long long)reflect101(gy, a.H) * a.pitch + reflect101(gx, a.W);
+                    v[k] = a.src[off];
+                }
+                xx += sx;
+                yy += sy;
+                if (xx >= a.tile_w) {
+                    xx -= a.tile_w;
+                    ++yy;
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < CL_B; ++k)
+                if (i0 + 256 * k < area) atomicAdd(&hist[v[k]], 1u);
+        }
     }
     __syncthreads();
     int h = (int)hist[t];
@@ -313,8 +339,12 @@ int pysift_clahe(const uint8_t* src, int32_t H, int32_t W, int32_t pitch, double
     a.pitch = pitch;
     a.tiles_x = tiles_x;
     a.tiles_y = tiles_y;
-    const int ew = (W % tiles_x == 0) ? W : W + (tiles_x - W % tiles_x);
-    const int eh = (H % tiles_y == 0) ? H : H + (tiles_y - H % tiles_y);
+    // cv2's CLAHE extends the image (reflect-101) only when a side does not
+    // divide by its tile count, and then extends BOTH sides by
+    // tiles - size % tiles: a side that divides gains a whole tile count
+    const bool exact = (W % tiles_x == 0) && (H % tiles_y == 0);
+    const int ew = exact ? W : W + (tiles_x - W % tiles_x);
+    const int eh = exact ? H : H + (tiles_y - H % tiles_y);
     a.tile_w = ew / tiles_x;
     a.tile_h = eh / tiles_y;
     const int area = a.tile_w * a.tile_h;

@@ -20,7 +20,7 @@ def _st():
     return torch.cuda.current_stream().cuda_stream
 
 
-@pytest.mark.parametrize("shape", [(960, 1280), (481, 643), (100, 77), (9, 13)])
+@pytest.mark.parametrize("shape", [(960, 1280), (481, 643), (100, 77), (9, 13), (240, 2100), (243, 2096)])
 def test_gray_and_clahe_match_cv2(shape):
     import cv2
     import torch
