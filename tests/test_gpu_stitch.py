@@ -209,10 +209,13 @@ def test_warp_feather_bit_exact_and_grid_sample():
     assert np.abs(ref_w.astype(int) - wv.astype(int)).max() <= 1
 
 
-def test_stitch_pair_end_to_end():
+@pytest.mark.parametrize("H,W", [(480, 640), (482, 640)])
+def test_stitch_pair_end_to_end(H, W):
+    """The whole pair against the oracle; 482 x 640 has one side that does
+    not divide by the CLAHE tile count (cv2 then extends both sides)."""
     from oracle import stitch_oracle as so
     from pysift_b200.stitch import GPUPyStitch
-    img1, img2, Ht = synthetic.stitch_pair(480, 640, seed=1)
+    img1, img2, Ht = synthetic.stitch_pair(H, W, seed=1)
     st = GPUPyStitch(ransac_iters=2048, inlier_thresh=4.0, save_output=False, verbose=False, blend="feather")
     pano = st.stitch(img1, img2)
     orc = so.OracleStitch(ransac_iters=2048, inlier_thresh=4.0, blend="feather").stitch(img1, img2)
@@ -227,6 +230,28 @@ def test_stitch_pair_end_to_end():
         assert np.mean(diff <= 1) > 0.99
     Ht_n = Ht / Ht[2, 2]
     assert np.allclose(Hg / Hg[2, 2], Ht_n, rtol=2e-2, atol=2e-2 * np.abs(Ht_n).max())
+
+
+def test_stitch_pair_of_different_sizes():
+    """Views of different sizes (the second cropped at its bottom and right
+    edges, which keeps the true homography): keypoint counts, homography and
+    panorama against the oracle."""
+    from oracle import stitch_oracle as so
+    from pysift_b200.stitch import GPUPyStitch
+    img1, img2, Ht = synthetic.stitch_pair(480, 640, seed=2)
+    img2 = np.ascontiguousarray(img2[:473, :629])
+    st = GPUPyStitch(ransac_iters=2048, inlier_thresh=4.0, save_output=False, verbose=False, blend="feather")
+    pano = st.stitch(img1, img2)
+    orc = so.OracleStitch(ransac_iters=2048, inlier_thresh=4.0, blend="feather").stitch(img1, img2)
+    m = st.last_metrics
+    assert m["kp1"] == orc["n1"] and m["kp2"] == orc["n2"]
+    assert abs(m["matches"] - len(orc["pairs"])) <= max(2, 0.01 * len(orc["pairs"]))
+    Hg = st._last["H"]
+    rel = np.max(np.abs(Hg - orc["H"]) / np.maximum(np.abs(orc["H"]), 1e-6))
+    assert rel < 1e-3, rel
+    assert pano.shape == orc["pano"].shape
+    diff = np.abs(pano.astype(int) - orc["pano"].astype(int))
+    assert np.mean(diff <= 1) > 0.99
 
 
 def test_stitch_batch_matches_sequential_stitch():
