@@ -19,7 +19,8 @@
 //   k_cap                top-cap by response, stable (pysift/core.py:2078-2080)
 //   k_orientation        36-bin histogram, peaks (pysift/core.py:228-333)
 //   k_expand             orientation expansion + (x, y) sort keys (pysift/core.py:1592-1598)
-//   k_rank               rank of each key = output row (pysift/core.py:2128-2134)
+//   k_br_scan/scatter/rank  rank of each key = output row (pysift/core.py:2128-2134),
+//                        and the output-limit order, exactly, through buckets
 //   k_descriptor         4x4x8 descriptor (+DSP) + L2/clip/L2 + RootSIFT, written at its
 //                        output row (pysift/core.py:693-997, 1870-1873)
 #include <cstdarg>
@@ -67,6 +68,9 @@ struct Ctrl {
     int pad[1];
 };
 
+// buckets of the exact rank kernels (k_br_*)
+constexpr int BR_NB = 4096;
+
 struct OctView {
     const float* lev[PYSIFT_MAX_LEVELS];
     int H, W, pitch;
@@ -87,6 +91,8 @@ struct Layout {
     size_t off_rf_ri, off_rf_ci, off_rf_si, off_rf_resp;
     size_t off_kp_o, off_kp_si, off_kp_ri, off_kp_ci, off_kp_resp, off_kp_tb;
     size_t off_ang, off_angcnt, off_ent_kp, off_ent_slot, off_keys, off_rank, off_row_resp, off_lrank;
+    size_t off_bkt, off_members;  // bucket ranks: [2 orders][cnt | off | cursor][BR_NB], [2][4 kc] members
+    size_t off_xblk;              // k_expand block counts
     size_t rowcnt_bytes_total;
     size_t off_rowcnt_base;
     size_t total;
@@ -180,6 +186,9 @@ static Layout make_layout(const pysift_detect_config* c, int H, int W) {
     l.off_rank = take(kc * 4 * sizeof(int));
     l.off_row_resp = take(kc * 4 * sizeof(float));
     l.off_lrank = take(kc * 4 * sizeof(int));
+    l.off_bkt = take(2 * 3 * BR_NB * sizeof(int));
+    l.off_members = take(2 * kc * 4 * sizeof(int));
+    l.off_xblk = take(((size_t)kc / 2048 + 2) * sizeof(int));
     if (l.doubled) l.off_coef = take((size_t)H * W * sizeof(double));
     l.off_base = take((size_t)l.H0 * l.pitch0 * sizeof(float));
     for (int o = 0; o < l.n_oct; ++o) l.off_pyr[o] = take((size_t)l.L * l.H[o] * l.pitch[o] * sizeof(float));
@@ -833,9 +842,11 @@ __global__ void __launch_bounds__(BLUR_NT) k_blur(const BlurArgs a) {
             const int rr = round * 32 + lane;
             blur_row_strip<R>(tile + rr * TS + warp * 8, hb + rr * HS + warp * 8, a.w2);
         }
-        if (N2 > 0 && threadIdx.x < N2 * 8) {
-            const int rr = NF * 32 + threadIdx.x % N2, x0 = (threadIdx.x / N2) * 8;
-            blur_row_strip<R>(tile + rr * TS + x0, hb + rr * HS + x0, a.w2);
+        if constexpr (N2 > 0) {
+            if (threadIdx.x < N2 * 8) {
+                const int rr = NF * 32 + threadIdx.x % N2, x0 = (threadIdx.x / N2) * 8;
+                blur_row_strip<R>(tile + rr * TS + x0, hb + rr * HS + x0, a.w2);
+            }
         }
     }
     __syncthreads();
@@ -1706,50 +1717,95 @@ struct ExpArgs {
     int* ent_slot;
     uint4* keys;
     float coord_scale[PYSIFT_MAX_OCTAVES];  // 2^o * (0.5 if doubled else 1)
+    int* xy_cnt;                             // per-bucket counts of the (x, y) order (zeroed)
+    int* blk_cnt;                            // entries per k_expand block
+    float xy_bscale;                         // BR_NB / image width
 };
 
+// Bucket of an (x, y) sort key: its x (a non-negative float) scaled to
+// BR_NB bins over the image width.  Non-decreasing in x, hence in the key
+// order (x first).
+__device__ __forceinline__ int br_bucket_xy(const uint4& k, float bscale) {
+    const float t = __uint_as_float(k.x) * bscale;
+    return t < (float)(BR_NB - 1) ? (int)t : BR_NB - 1;
+}
+// Bucket of a response in the output-limit order (larger first): BR_NB - 1
+// minus the float's exponent and top 8 mantissa bits, offset so that the
+// BR_NB buckets span [2^-12, 2^4) (256 per octave) and clamped at both ends.
+// Non-decreasing in that order for non-negative responses.
+__device__ __forceinline__ int br_bucket_resp(float r) {
+    constexpr int OFF = (127 - 12) << 8;  // the bucket of 2^-12
+    const int f = (int)(__float_as_uint(r) >> 15) - OFF;
+    return BR_NB - 1 - (f < 0 ? 0 : (f > BR_NB - 1 ? BR_NB - 1 : f));
+}
+
 // Expansion of the kept keypoints into their oriented entries (1..4 each),
-// in keypoint order: each thread takes EXP_K consecutive keypoints, loads
-// them, and one block scan per chunk places their entries.
+// in keypoint order, over EXP_T x EXP_K keypoints per block: k_expand_count
+// writes each block's entry count; in k_expand each block adds up the counts
+// of the blocks before it (there are few) for its first entry, and a block
+// scan places its own entries.  The last block stores the total.
 constexpr int EXP_K = 8;
-__global__ void __launch_bounds__(1024) k_expand(const ExpArgs a, Ctrl* ctrl) {
+constexpr int EXP_T = 256;
+constexpr int EXP_PER_BLOCK = EXP_T * EXP_K;
+
+__global__ void __launch_bounds__(EXP_T) k_expand_count(const ExpArgs a, const Ctrl* ctrl) {
     __shared__ int sh[33];
     const int n = ctrl->n_kept;
-    int base = 0;
-    for (int c0 = 0; c0 < n; c0 += (int)blockDim.x * EXP_K) {
-        const int i0 = c0 + (int)threadIdx.x * EXP_K;
-        int cnt[EXP_K];
-        uint32_t kx[EXP_K], ky[EXP_K], tb[EXP_K];
-        int local = 0;
+    const int i0 = blockIdx.x * EXP_PER_BLOCK + (int)threadIdx.x * EXP_K;
+    int local = 0;
 #pragma unroll
-        for (int k = 0; k < EXP_K; ++k) {
-            const int i = i0 + k;
-            cnt[k] = 0;
-            kx[k] = ky[k] = tb[k] = 0u;
-            if (i < n) {
-                cnt[k] = a.angcnt[i];
-                const float sc = a.coord_scale[a.kp_o[i]];
-                kx[k] = __float_as_uint(a.kp_ci[i] * sc);
-                ky[k] = __float_as_uint(a.kp_ri[i] * sc);
-                tb[k] = a.kp_tb[i];
-            }
-            local += cnt[k];
-        }
-        int tot;
-        int pos = base + block_excl_scan(local, &tot, sh);
+    for (int k = 0; k < EXP_K; ++k)
+        if (i0 + k < n) local += a.angcnt[i0 + k];
+    int tot;
+    block_excl_scan(local, &tot, sh);
+    if (threadIdx.x == 0) a.blk_cnt[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(EXP_T) k_expand(const ExpArgs a, Ctrl* ctrl) {
+    __shared__ int sh[33];
+    __shared__ int s_base;
+    const int n = ctrl->n_kept;
+    if (threadIdx.x < 32) {
+        int sum = 0;
+        for (int b = (int)threadIdx.x; b < (int)blockIdx.x; b += 32) sum += a.blk_cnt[b];
 #pragma unroll
-        for (int k = 0; k < EXP_K; ++k) {
-            const int i = i0 + k;
-            for (int q = 0; q < cnt[k]; ++q) {
-                a.ent_kp[pos + q] = i;
-                a.ent_slot[pos + q] = q;
-                a.keys[pos + q] = make_uint4(kx[k], ky[k], tb[k], (uint32_t)(i * 4 + q));
-            }
-            pos += cnt[k];
-        }
-        base += tot;
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(FULL_MASK, sum, o);
+        if (threadIdx.x == 0) s_base = sum;
     }
-    if (threadIdx.x == 0) ctrl->n_oriented = base;
+    const int i0 = blockIdx.x * EXP_PER_BLOCK + (int)threadIdx.x * EXP_K;
+    int cnt[EXP_K];
+    uint32_t kx[EXP_K], ky[EXP_K], tb[EXP_K];
+    int local = 0;
+#pragma unroll
+    for (int k = 0; k < EXP_K; ++k) {
+        const int i = i0 + k;
+        cnt[k] = 0;
+        kx[k] = ky[k] = tb[k] = 0u;
+        if (i < n) {
+            cnt[k] = a.angcnt[i];
+            const float sc = a.coord_scale[a.kp_o[i]];
+            kx[k] = __float_as_uint(a.kp_ci[i] * sc);
+            ky[k] = __float_as_uint(a.kp_ri[i] * sc);
+            tb[k] = a.kp_tb[i];
+        }
+        local += cnt[k];
+    }
+    int tot;
+    const int excl = block_excl_scan(local, &tot, sh);  // its barriers also publish s_base
+    int pos = s_base + excl;
+#pragma unroll
+    for (int k = 0; k < EXP_K; ++k) {
+        const int i = i0 + k;
+        for (int q = 0; q < cnt[k]; ++q) {
+            a.ent_kp[pos + q] = i;
+            a.ent_slot[pos + q] = q;
+            const uint4 key = make_uint4(kx[k], ky[k], tb[k], (uint32_t)(i * 4 + q));
+            a.keys[pos + q] = key;
+            atomicAdd(&a.xy_cnt[br_bucket_xy(key, a.xy_bscale)], 1);
+        }
+        pos += cnt[k];
+    }
+    if (threadIdx.x == 0 && blockIdx.x == gridDim.x - 1) ctrl->n_oriented = s_base + tot;
 }
 
 __device__ __forceinline__ bool key_less(const uint4& p, const uint4& q) {
@@ -1759,31 +1815,87 @@ __device__ __forceinline__ bool key_less(const uint4& p, const uint4& q) {
     return p.w < q.w;
 }
 
-constexpr int RANK_T = 256;
+// Exact ranks through buckets.  Keys follow a strict total order; a bucket
+// function that never decreases along the order gives
+//   rank[i] = #{keys in lower buckets} + #{keys of i's bucket ordered before i},
+// the same count as comparing every pair.  Counts come from the kernel that
+// writes the keys; k_br_scan turns them into bucket starts, k_br_scatter
+// lists each bucket's members (in any order: the in-bucket count does not
+// depend on it) and k_br_rank counts.  ORD 0: the (x, y) sort keys, rank =
+// output row.  ORD 1: the rows' responses, larger first, ties by lower row
+// (the output-limit order); nothing to do unless there are more rows than
+// the limit.
+struct BRArgs {
+    const uint4* keys;      // ORD 0
+    const float* row_resp;  // ORD 1
+    float xy_bscale;
+    int limit;              // ORD 1
+    int* cnt;               // [BR_NB] counts
+    int* off;               // [BR_NB] bucket starts
+    int* cursor;            // [BR_NB] fill positions
+    int* members;
+    int* rank;
+};
 
-// rank[i] = #{j : key[j] < key[i]} over all (i-tile, j-tile) pairs; partial
-// counts are added with integer atomics (exact, order-independent).  rank
-// must be zeroed before the launch.
-__global__ void __launch_bounds__(RANK_T) k_rank(const uint4* __restrict__ keys, int* __restrict__ rank,
-                                                 const Ctrl* ctrl) {
-    __shared__ uint4 tile[RANK_T];
+template <int ORD>
+__device__ __forceinline__ bool br_skip(const BRArgs& a, int n) {
+    return ORD == 1 && n <= a.limit;
+}
+template <int ORD>
+__device__ __forceinline__ int br_bucket(const BRArgs& a, int i) {
+    if (ORD == 0) return br_bucket_xy(a.keys[i], a.xy_bscale);
+    return br_bucket_resp(a.row_resp[i]);
+}
+
+template <int ORD>
+__global__ void __launch_bounds__(1024) k_br_scan(const BRArgs a, const Ctrl* ctrl) {
+    __shared__ int sh[33];
+    if (br_skip<ORD>(a, ctrl->n_oriented)) return;
+    constexpr int PER = BR_NB / 1024;
+    int c[PER], local = 0;
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+        c[k] = a.cnt[threadIdx.x * PER + k];
+        local += c[k];
+    }
+    int tot;
+    int pos = block_excl_scan(local, &tot, sh);
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+        a.off[threadIdx.x * PER + k] = pos;
+        a.cursor[threadIdx.x * PER + k] = pos;
+        pos += c[k];
+    }
+}
+
+template <int ORD>
+__global__ void k_br_scatter(const BRArgs a, const Ctrl* ctrl) {
     const int n = ctrl->n_oriented;
-    const int nt = (n + RANK_T - 1) / RANK_T;
-    const long long pairs = (long long)nt * nt;
-    for (long long t = blockIdx.x; t < pairs; t += gridDim.x) {
-        const int ti = (int)(t / nt), tj = (int)(t - (long long)ti * nt);
-        __syncthreads();
-        const int j = tj * RANK_T + threadIdx.x;
-        if (j < n) tile[threadIdx.x] = keys[j];
-        __syncthreads();
-        const int i = ti * RANK_T + threadIdx.x;
-        if (i < n) {
-            const uint4 me = keys[i];
-            const int m = min(RANK_T, n - tj * RANK_T);
-            int cnt = 0;
-            for (int k = 0; k < m; ++k) cnt += key_less(tile[k], me) ? 1 : 0;
-            if (cnt) atomicAdd(&rank[i], cnt);
+    if (br_skip<ORD>(a, n)) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        a.members[atomicAdd(&a.cursor[br_bucket<ORD>(a, i)], 1)] = i;
+}
+
+template <int ORD>
+__global__ void k_br_rank(const BRArgs a, const Ctrl* ctrl) {
+    const int n = ctrl->n_oriented;
+    if (br_skip<ORD>(a, n)) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int b = br_bucket<ORD>(a, i);
+        const int s0 = a.off[b], s1 = s0 + a.cnt[b];
+        int r = s0;
+        if (ORD == 0) {
+            const uint4 me = a.keys[i];
+            for (int s = s0; s < s1; ++s) r += key_less(a.keys[a.members[s]], me) ? 1 : 0;
+        } else {
+            const float me = a.row_resp[i];
+            for (int s = s0; s < s1; ++s) {
+                const int j = a.members[s];
+                const float o = a.row_resp[j];
+                r += (o > me || (o == me && j < i)) ? 1 : 0;
+            }
         }
+        a.rank[i] = r;
     }
 }
 
@@ -2026,39 +2138,16 @@ __global__ void __launch_bounds__(DESC_T, 5) k_descriptor(const DescArgs a, Ctrl
     }
 }
 
-// Response of every output row (rows are the (x, y) ranks of the oriented entries).
+// Response of every output row (rows are the (x, y) ranks of the oriented
+// entries), counted into the output-limit order's buckets.
 __global__ void k_row_resp(const int* __restrict__ ent_kp, const float* __restrict__ kp_resp,
-                           const int* __restrict__ rank, float* __restrict__ row_resp, const Ctrl* ctrl) {
+                           const int* __restrict__ rank, float* __restrict__ row_resp, int* __restrict__ resp_cnt,
+                           const Ctrl* ctrl) {
     const int n = ctrl->n_oriented;
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x)
-        row_resp[rank[e]] = kp_resp[ent_kp[e]];
-}
-
-// lrank[row] = number of rows with a larger response, or an equal response
-// and a lower row (lrank must start at zero); nothing when n <= limit.
-__global__ void __launch_bounds__(256) k_limit_rank(const float* __restrict__ row_resp, int limit,
-                                                   int* __restrict__ lrank, const Ctrl* ctrl) {
-    __shared__ float tile[256];
-    const int n = ctrl->n_oriented;
-    if (n <= limit) return;
-    const int nt = (n + 255) / 256;
-    for (long long t = blockIdx.x; t < (long long)nt * nt; t += gridDim.x) {
-        const int ti = (int)(t / nt), tj = (int)(t - (long long)ti * nt);
-        __syncthreads();
-        const int j = tj * 256 + threadIdx.x;
-        if (j < n) tile[threadIdx.x] = row_resp[j];
-        __syncthreads();
-        const int i = ti * 256 + threadIdx.x;
-        if (i < n) {
-            const float me = row_resp[i];
-            const int m = min(256, n - tj * 256);
-            int cnt = 0;
-            for (int k = 0; k < m; ++k) {
-                const float o = tile[k];
-                cnt += (o > me || (o == me && tj * 256 + k < i)) ? 1 : 0;
-            }
-            if (cnt) atomicAdd(&lrank[i], cnt);
-        }
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const float r = kp_resp[ent_kp[e]];
+        row_resp[rank[e]] = r;
+        atomicAdd(&resp_cnt[br_bucket_resp(r)], 1);
     }
 }
 
@@ -2378,12 +2467,29 @@ static int run_detect(const pysift_detect_config* cfg, const uint8_t* gray, int 
     xa.ent_slot = at<int>(ws, l.off_ent_slot);
     xa.keys = at<uint4>(ws, l.off_keys);
     for (int o = 0; o < n_oct; ++o) xa.coord_scale[o] = (float)((double)(1 << o) * (l.doubled ? 0.5 : 1.0));
-    k_expand<<<1, 1024, 0, st>>>(xa, ctrl);
+    int* bkt = at<int>(ws, l.off_bkt);  // [order][cnt | off | cursor][BR_NB]
+    PYSIFT_CUDA_TRY(cudaMemsetAsync(bkt, 0, sizeof(int) * 2 * 3 * BR_NB, st));
+    xa.xy_cnt = bkt;
+    xa.xy_bscale = (float)BR_NB / (float)W;
+    xa.blk_cnt = at<int>(ws, l.off_xblk);
+    const int exp_blocks = ceil_div(kcap, EXP_PER_BLOCK);
+    k_expand_count<<<exp_blocks, EXP_T, 0, st>>>(xa, ctrl);
+    k_expand<<<exp_blocks, EXP_T, 0, st>>>(xa, ctrl);
     PYSIFT_LAUNCH_CHECK("k_expand");
     int* rank = at<int>(ws, l.off_rank);
-    PYSIFT_CUDA_TRY(cudaMemsetAsync(rank, 0, sizeof(int) * 4 * (size_t)kcap, st));
-    k_rank<<<num_sms() * 8, RANK_T, 0, st>>>(xa.keys, rank, ctrl);
-    PYSIFT_LAUNCH_CHECK("k_rank");
+    const int br_blocks = std::max(1, std::min(ceil_div(4 * kcap, 256), num_sms() * 4));
+    BRArgs bx{};
+    bx.keys = xa.keys;
+    bx.xy_bscale = xa.xy_bscale;
+    bx.cnt = bkt;
+    bx.off = bkt + BR_NB;
+    bx.cursor = bkt + 2 * BR_NB;
+    bx.members = at<int>(ws, l.off_members);
+    bx.rank = rank;
+    k_br_scan<0><<<1, 1024, 0, st>>>(bx, ctrl);
+    k_br_scatter<0><<<br_blocks, 256, 0, st>>>(bx, ctrl);
+    k_br_rank<0><<<br_blocks, 256, 0, st>>>(bx, ctrl);
+    PYSIFT_LAUNCH_CHECK("k_br (x, y)");
     PYSIFT_STAGE(5);
     // A11
     static thread_local DescArgs da;
@@ -2410,11 +2516,20 @@ static int run_detect(const pysift_detect_config* cfg, const uint8_t* gray, int 
     da.lrank = at<int>(ws, l.off_lrank);
     if (cfg->output_limit > 0) {
         float* row_resp = at<float>(ws, l.off_row_resp);
-        PYSIFT_CUDA_TRY(cudaMemsetAsync(at<int>(ws, l.off_lrank), 0, sizeof(int) * 4 * (size_t)kcap, st));
-        k_row_resp<<<ceil_div(4 * kcap, 256), 256, 0, st>>>(xa.ent_kp, ca.kp_resp, rank, row_resp, ctrl);
+        BRArgs br{};
+        br.row_resp = row_resp;
+        br.limit = cfg->output_limit;
+        br.cnt = bkt + 3 * BR_NB;
+        br.off = bkt + 4 * BR_NB;
+        br.cursor = bkt + 5 * BR_NB;
+        br.members = at<int>(ws, l.off_members) + 4 * (size_t)kcap;
+        br.rank = at<int>(ws, l.off_lrank);
+        k_row_resp<<<br_blocks, 256, 0, st>>>(xa.ent_kp, ca.kp_resp, rank, row_resp, br.cnt, ctrl);
         PYSIFT_LAUNCH_CHECK("k_row_resp");
-        k_limit_rank<<<num_sms() * 8, 256, 0, st>>>(row_resp, cfg->output_limit, at<int>(ws, l.off_lrank), ctrl);
-        PYSIFT_LAUNCH_CHECK("k_limit_rank");
+        k_br_scan<1><<<1, 1024, 0, st>>>(br, ctrl);
+        k_br_scatter<1><<<br_blocks, 256, 0, st>>>(br, ctrl);
+        k_br_rank<1><<<br_blocks, 256, 0, st>>>(br, ctrl);
+        PYSIFT_LAUNCH_CHECK("k_br (response)");
     }
     da.out_kpts = kpts;
     da.out_resp = resp;
