@@ -1588,8 +1588,6 @@ __global__ void __launch_bounds__(ORI_T) k_orientation(const OriArgs a, const Ct
     __shared__ unsigned int wlo[ORI_W][36], whi[ORI_W][36];
     __shared__ unsigned long long whist[ORI_W][36];
     __shared__ float h0[36], h1[36];
-    __shared__ float s_peak;
-    __shared__ unsigned s_mask[2];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int n = ctrl->n_kept;
     for (int i = blockIdx.x; i < n; i += gridDim.x) {
@@ -1627,9 +1625,17 @@ __global__ void __launch_bounds__(ORI_T) k_orientation(const OriArgs a, const Ct
         const int tcols = (n_cols + 7) >> 3, trows = (nr + 3) >> 2;
         const int ntiles = tcols * trows;
         int steps = 0;
+        // tile t -> (t / tcols, t % tcols), advanced ORI_W tiles at a time
+        const int dty = ORI_W / tcols, dtx = ORI_W - dty * tcols;
+        int ty = warp / tcols, tx = warp - ty * tcols;
         for (int t = warp; t < ntiles; t += ORI_W) {
-            const int ty = t / tcols, tx = t - ty * tcols;
             const int pr = ty * 4 + (lane >> 3), pc = tx * 8 + (lane & 7);
+            tx += dtx;
+            ty += dty;
+            if (tx >= tcols) {
+                tx -= tcols;
+                ++ty;
+            }
             const bool act = pr < nr && pc < n_cols;
             if (act) {
                 const int r = r_min + pr, c = c_min + pc;
@@ -1655,49 +1661,53 @@ __global__ void __launch_bounds__(ORI_T) k_orientation(const OriArgs a, const Ct
         }
         hw.fold();
         __syncthreads();
-        // smoothing and peaks, one bin per thread, same arithmetic per bin
-        if (tid < 36) {
-            unsigned long long s = 0ull;
-            for (int w = 0; w < ORI_W; ++w) s += whist[w][tid];
-            h0[tid] = unfix40(s);
-        }
-        __syncthreads();
-        if (tid < 36) h1[tid] = 0.25f * h0[(tid + 35) % 36] + 0.5f * h0[tid] + 0.25f * h0[(tid + 1) % 36];
-        __syncthreads();
-        if (tid < 36) h0[tid] = 0.25f * h1[(tid + 35) % 36] + 0.5f * h1[tid] + 0.25f * h1[(tid + 1) % 36];
-        __syncthreads();
-        if (tid == 0) {
+        // smoothing and peaks in warp 0: lane l owns bins l and l + 32 (l < 4),
+        // same arithmetic per bin; the peak height is a maximum (order-free)
+        if (warp == 0) {
+            for (int b = lane; b < 36; b += 32) {
+                unsigned long long s = 0ull;
+                for (int w = 0; w < ORI_W; ++w) s += whist[w][b];
+                h0[b] = unfix40(s);
+            }
+            __syncwarp();
+            for (int b = lane; b < 36; b += 32)
+                h1[b] = 0.25f * h0[(b + 35) % 36] + 0.5f * h0[b] + 0.25f * h0[(b + 1) % 36];
+            __syncwarp();
+            for (int b = lane; b < 36; b += 32)
+                h0[b] = 0.25f * h1[(b + 35) % 36] + 0.5f * h1[b] + 0.25f * h1[(b + 1) % 36];
+            __syncwarp();
             float peak = 0.0f;
-            for (int b = 0; b < 36; ++b)
-                if (h0[b] > peak) peak = h0[b];
-            s_peak = peak;
-        }
-        __syncthreads();
-        bool is_peak = false;
-        float angle = 0.0f;
-        if (tid < 36) {
-            const float thr = 0.8f * s_peak;
-            const float hb = h0[tid];
-            if (hb >= thr) {
-                const float l = h0[(tid + 35) % 36], rv = h0[(tid + 1) % 36];
-                if (hb >= l && hb >= rv) {
-                    is_peak = true;
-                    const float denom = l - 2.0f * hb + rv;
-                    const float fine = (float)tid + (fabsf(denom) > 1e-12f ? 0.5f * (l - rv) / denom : 0.0f);
-                    angle = fmodf(fine / 36.0f * 360.0f + 360.0f, 360.0f);
+            for (int b = lane; b < 36; b += 32) peak = fmaxf(peak, h0[b]);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) peak = fmaxf(peak, __shfl_xor_sync(FULL_MASK, peak, o));
+            const float thr = 0.8f * peak;
+            bool pk[2] = {false, false};
+            float ang2[2] = {0.0f, 0.0f};
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int b = lane + 32 * h;
+                if (b >= 36) continue;
+                const float hb = h0[b];
+                if (hb >= thr) {
+                    const float l = h0[(b + 35) % 36], rv = h0[(b + 1) % 36];
+                    if (hb >= l && hb >= rv) {
+                        pk[h] = true;
+                        const float denom = l - 2.0f * hb + rv;
+                        const float fine = (float)b + (fabsf(denom) > 1e-12f ? 0.5f * (l - rv) / denom : 0.0f);
+                        ang2[h] = fmodf(fine / 36.0f * 360.0f + 360.0f, 360.0f);
+                    }
                 }
             }
-        }
-        const unsigned m = __ballot_sync(FULL_MASK, is_peak);
-        if (lane == 0) s_mask[warp] = m;
-        __syncthreads();
-        const unsigned m0 = s_mask[0], m1 = s_mask[1] & 0xfu;
-        const int before = warp == 0 ? __popc(m0 & ((1u << lane) - 1u)) : __popc(m0) + __popc(m1 & ((1u << lane) - 1u));
-        if (is_peak && before < 4) a.ang[i * 4 + before] = angle;
-        if (tid == 0) {
-            const int cnt = min(4, __popc(m0) + __popc(m1));
-            a.angcnt[i] = cnt;
-            for (int k = cnt; k < 4; ++k) a.ang[i * 4 + k] = -1.0f;
+            const unsigned m0 = __ballot_sync(FULL_MASK, pk[0]), m1 = __ballot_sync(FULL_MASK, pk[1]) & 0xfu;
+            const unsigned below = (1u << lane) - 1u;
+            const int before0 = __popc(m0 & below), before1 = __popc(m0) + __popc(m1 & below);
+            if (pk[0] && before0 < 4) a.ang[i * 4 + before0] = ang2[0];
+            if (pk[1] && before1 < 4) a.ang[i * 4 + before1] = ang2[1];
+            if (lane == 0) {
+                const int cnt = min(4, __popc(m0) + __popc(m1));
+                a.angcnt[i] = cnt;
+                for (int k = cnt; k < 4; ++k) a.ang[i * 4 + k] = -1.0f;
+            }
         }
         __syncthreads();
     }
