@@ -273,7 +273,6 @@ class PySIFT:
             with torch.cuda.stream(cap):
                 self._launch(b, b.gray.data_ptr(), H, W, W, cap.cuda_stream)
             st.wait_stream(cap)
-            cap.synchronize()
             n0 = self._lib.pysift_launch_count()
             g = torch.cuda.CUDAGraph()
             with torch.cuda.graph(g, stream=cap):
