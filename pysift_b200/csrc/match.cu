@@ -3,11 +3,14 @@
 // Matching runs as two row scans: queries against the train set (forward
 // top-2) and the train set against the queries (backward top-2).  Each CTA of
 // k_match_rows keeps a 128-row query block resident in shared memory and
-// streams 128-row train tiles through two cp.async buffers (no-swizzle
+// streams 128-row train tiles through a ring of cp.async buffers (three for
+// 128-byte rows, two for 256-byte rows; no-swizzle
 // K-major core-matrix layout); one thread issues the tcgen05.mma of tile t+1
 // (kind::f16, fp32 accumulator in tensor memory, two accumulators of 128
-// columns) while all four warps reduce tile t, read back with tcgen05.ld, to
-// a running per-row top-2 in registers.  Train tiles are split into
+// columns) while eight warps reduce tile t, read back with tcgen05.ld, to
+// running per-row top-2s in registers (two warps per TMEM lane quadrant, each
+// half of the tile's columns, even and odd columns in separate chains; the
+// partials merge exactly at the end).  Train tiles are split into
 // segments so that the grid fills the SMs; k_match_merge combines the
 // segments and applies the ratio test; k_match_mutual keeps mutual matches
 // (pysift/core.py:2574-2701, 2840-2940).
@@ -36,7 +39,7 @@ namespace pysift {
 
 constexpr int MT = 128;           // query rows per CTA = UMMA M = TMEM lanes
 constexpr int NT = 128;           // train rows per tile = UMMA N
-constexpr int MATCH_THREADS = 128;
+constexpr int MATCH_THREADS = 256;  // 2 warps per TMEM lane quadrant, each half the tile's columns
 constexpr unsigned SPIN_LIMIT = 1u << 26;  // bounded waits on the MMA barriers
 
 enum MatchMode { SIM_F16 = 0, DIST_BF16 = 1, SPLIT_FP8 = 2, SIM_I8 = 3 };
@@ -126,9 +129,13 @@ struct RowScanArgs {
     int* error;          // set when an MMA wait gives up
 };
 
+// Running top-2 of one 32-column chunk: even columns into (k1, k2, i1), odd
+// columns into (m1, m2, j1) (two independent chains); each partial visits
+// its columns in increasing index order and replaces its best only on a
+// strictly larger key.
 template <int MODE>
 __device__ __forceinline__ void scan_chunk(const uint32_t (&v)[32], int col0, int lim, int nb_lane, float sq,
-                                           float& k1, float& k2, int& i1) {
+                                           float& k1, float& k2, int& i1, float& m1, float& m2, int& j1) {
 #pragma unroll
     for (int j = 0; j < 32; ++j) {
         float key;
@@ -144,22 +151,44 @@ __device__ __forceinline__ void scan_chunk(const uint32_t (&v)[32], int col0, in
             key = __fsub_rn(2.0f * __uint_as_float(v[j]), nb);
         }
         if (j >= lim) key = -INFINITY;
-        k2 = fmaxf(k2, fminf(key, k1));
-        i1 = key > k1 ? col0 + j : i1;
-        k1 = fmaxf(k1, key);
+        if (j & 1) {
+            m2 = fmaxf(m2, fminf(key, m1));
+            j1 = key > m1 ? col0 + j : j1;
+            m1 = fmaxf(m1, key);
+        } else {
+            k2 = fmaxf(k2, fminf(key, k1));
+            i1 = key > k1 ? col0 + j : i1;
+            k1 = fmaxf(k1, key);
+        }
     }
+}
+
+// Top-2 of the union of two disjoint column sets: the best is the larger
+// best (the lower index on equal keys, i.e. its first occurrence in index
+// order), the second the largest of the smaller best and the two seconds --
+// the result a single scan in index order would give.
+__device__ __forceinline__ void top2_merge(float& k1, float& k2, int& i1, float bk1, float bk2, int bi1) {
+    k2 = fmaxf(fmaxf(k2, bk2), fminf(k1, bk1));
+    i1 = bk1 > k1 ? bi1 : (bk1 == k1 ? min(i1, bi1) : i1);
+    k1 = fmaxf(k1, bk1);
 }
 
 template <int MODE, int RB>
 __global__ void __launch_bounds__(MATCH_THREADS) k_match_rows(const RowScanArgs args) {
     constexpr int KC = RB / 16;
     constexpr uint32_t TILE_BYTES = MT * RB;
+    // train tiles in flight: a 3-deep ring for 128-byte rows (4 tiles in the
+    // 80 KB a CTA is given), 2 for 256-byte rows
+    constexpr int NB = RB <= 128 ? 3 : 2;
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t* sQ = smem;
     __shared__ __align__(8) uint64_t mbar[2];
     __shared__ uint32_t tmem_base;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int quad = warp & 3, half = warp >> 2;  // TMEM lane quadrant, column half of each tile
+    const int rloc = quad * 32 + lane;            // this thread's query row in the block
+    __shared__ Top2 s_half[MT];
     const int q0 = blockIdx.x * MT;
     const int n_tt = (args.n_t + NT - 1) / NT;
     const int t_begin = blockIdx.y * args.seg_tiles;
@@ -178,16 +207,37 @@ __global__ void __launch_bounds__(MATCH_THREADS) k_match_rows(const RowScanArgs 
     stage_rows<RB>(sQ, args.q, q0, args.n_q);
     stage_rows<RB>(smem + TILE_BYTES, args.t, t_begin * NT, args.n_t);
     asm volatile("cp.async.commit_group;" ::: "memory");
+#pragma unroll
+    for (int p = 1; p < NB - 1; ++p) {  // tiles 1 .. NB-2, one commit group each
+        if (p < nt) stage_rows<RB>(smem + (1 + p) * TILE_BYTES, args.t, (t_begin + p) * NT, args.n_t);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_base;
 
-    float k1 = -INFINITY, k2 = -INFINITY;
-    int i1 = 0x7fffffff;
-    const float sq = (MODE == SIM_I8 && q0 + tid < args.n_q) ? args.scale_q[q0 + tid] : 1.0f;
+    float k1 = -INFINITY, k2 = -INFINITY, m1 = -INFINITY, m2 = -INFINITY;
+    int i1 = 0x7fffffff, j1 = 0x7fffffff;
+    const float sq = (MODE == SIM_I8 && q0 + rloc < args.n_q) ? args.scale_q[q0 + rloc] : 1.0f;
     bool fail = false;
     int issued = 0;  // MMA groups committed
+    // per-column train values of this warp's chunks (|t|^2 or the int8 scale),
+    // loaded one tile before the tile is reduced
+    int nbv[NT / 64];
+    auto load_nb = [&](int tile) {
+#pragma unroll
+        for (int cc = 0; cc < NT / 64; ++cc) {
+            const int c = (t_begin + tile) * NT + (half * (NT / 64) + cc) * 32 + lane;
+            if (MODE == SIM_I8)
+                nbv[cc] = __float_as_int(c < args.n_t ? args.scale_t[c] : 1.0f);
+            else if (MODE != SIM_F16)
+                nbv[cc] = __float_as_int((float)(c < args.n_t ? args.norm_t[c] : 0));
+            else
+                nbv[cc] = 0;
+        }
+    };
+    load_nb(0);
     for (int it = 0; it <= nt; ++it) {
         // (1) the MMA of tile it-1 has finished: its train buffer and accumulator are free to read/reuse
         if (it >= 1) {
@@ -198,18 +248,20 @@ __global__ void __launch_bounds__(MATCH_THREADS) k_match_rows(const RowScanArgs 
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         }
-        // (2) prefetch train tile it+1 into the buffer tile it-1 used
-        if (it + 1 < nt) stage_rows<RB>(smem + (1 + ((it + 1) & 1)) * TILE_BYTES, args.t, (t_begin + it + 1) * NT, args.n_t);
+        // (2) prefetch train tile it+NB-1 into the buffer tile it-1 used
+        if (it + NB - 1 < nt)
+            stage_rows<RB>(smem + (1 + (it + NB - 1) % NB) * TILE_BYTES, args.t, (t_begin + it + NB - 1) * NT, args.n_t);
         asm volatile("cp.async.commit_group;" ::: "memory");
-        // (3) tile it is staged: issue its MMAs into accumulator it&1
+        // (3) tile it is staged (only the NB-1 newer groups may be pending):
+        // issue its MMAs into accumulator it&1
         if (it < nt) {
-            asm volatile("cp.async.wait_group 1;" ::: "memory");
+            asm volatile("cp.async.wait_group %0;" ::"n"(NB - 1) : "memory");
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncthreads();
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             if (tid == 0) {
-                const uint32_t a0 = smem_u32(sQ), b0 = smem_u32(smem + (1 + (it & 1)) * TILE_BYTES);
+                const uint32_t a0 = smem_u32(sQ), b0 = smem_u32(smem + (1 + it % NB) * TILE_BYTES);
                 const uint32_t d = tmem + (uint32_t)((it & 1) * NT);
                 // f16 / bf16 (kind::f16, format 0 / 1) or e4m3 (kind::f8f6f4, format 0);
                 // either way one MMA covers 32 bytes of K: two core matrices
@@ -249,18 +301,12 @@ __global__ void __launch_bounds__(MATCH_THREADS) k_match_rows(const RowScanArgs 
             const int tcol0 = (t_begin + it - 1) * NT;
             const int lim_tile = args.n_t - tcol0;
 #pragma unroll
-            for (int chunk = 0; chunk < NT / 32; ++chunk) {
-                int nb_lane = 0;
-                if (MODE == SIM_I8) {
-                    const int c = tcol0 + chunk * 32 + lane;
-                    nb_lane = __float_as_int(c < args.n_t ? args.scale_t[c] : 1.0f);
-                } else if (MODE != SIM_F16) {
-                    const int c = tcol0 + chunk * 32 + lane;
-                    nb_lane = __float_as_int((float)(c < args.n_t ? args.norm_t[c] : 0));
-                }
+            for (int cc = 0; cc < NT / 64; ++cc) {
+                const int chunk = half * (NT / 64) + cc;
+                const int nb_lane = nbv[cc];
                 uint32_t v[32];
                 const uint32_t taddr =
-                    tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(((it - 1) & 1) * NT + chunk * 32);
+                    tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(((it - 1) & 1) * NT + chunk * 32);
                 asm volatile(
                     "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
                     "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
@@ -272,8 +318,9 @@ __global__ void __launch_bounds__(MATCH_THREADS) k_match_rows(const RowScanArgs 
                       "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
                     : "r"(taddr));
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                scan_chunk<MODE>(v, tcol0 + chunk * 32, lim_tile - chunk * 32, nb_lane, sq, k1, k2, i1);
+                scan_chunk<MODE>(v, tcol0 + chunk * 32, lim_tile - chunk * 32, nb_lane, sq, k1, k2, i1, m1, m2, j1);
             }
+            if (it < nt) load_nb(it);  // for the reduction of tile it, one iteration from now
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         }
     }
@@ -284,8 +331,21 @@ __global__ void __launch_bounds__(MATCH_THREADS) k_match_rows(const RowScanArgs 
         for (int g = 0; g < issued; ++g) mbar_wait_bounded(&mbar[g & 1], (uint32_t)((g >> 1) & 1));
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
-    const int row = q0 + tid;
-    if (!fail && row < args.n_q) {
+    // even and odd columns of this thread, then the two column halves of the row
+    top2_merge(k1, k2, i1, m1, m2, j1);
+    if (half == 1) {
+        Top2 h;
+        h.k1 = k1;
+        h.k2 = k2;
+        h.i1 = i1;
+        h.pad = 0;
+        s_half[rloc] = h;
+    }
+    __syncthreads();
+    const int row = q0 + rloc;
+    if (half == 0 && !fail && row < args.n_q) {
+        const Top2 h = s_half[rloc];
+        top2_merge(k1, k2, i1, h.k1, h.k2, h.i1);
         Top2 r;
         r.k1 = k1;
         r.k2 = k2;
@@ -410,12 +470,27 @@ static int sm_count() {
     return n > 0 ? n : 148;
 }
 
-// Segments of the train side so that about two CTAs per SM are busy.
+// Segments of the train side.  Two CTAs fit on an SM (tensor memory), so a
+// grid of n_qb x nseg CTAs runs in ceil(n_qb nseg / (2 SMs)) waves of
+// ceil(n_tt / nseg) tiles each (+1 for a CTA's prologue): the segment count
+// with the fewest tile-steps is taken (the smaller one on ties), so that a
+// few CTAs past a full wave do not double the scan.
 static void scan_split(int n_q, int n_t, int& nseg, int& seg_tiles) {
     const int n_qb = ceil_div(n_q, MT), n_tt = ceil_div(n_t, NT);
-    int want = ceil_div(2 * sm_count(), n_qb);
-    want = std::max(1, std::min(want, n_tt));
-    seg_tiles = ceil_div(n_tt, want);
+    const long long slots = 2LL * sm_count();
+    long long best = -1;
+    nseg = 1;
+    for (int s_ = 1; s_ <= n_tt; ++s_) {
+        const int st_ = ceil_div(n_tt, s_);
+        if (ceil_div(n_tt, st_) != s_) continue;  // a segment count that leaves none empty
+        const long long waves = (n_qb * (long long)s_ + slots - 1) / slots;
+        const long long cost = waves * (st_ + 1);
+        if (best < 0 || cost < best) {
+            best = cost;
+            nseg = s_;
+        }
+    }
+    seg_tiles = ceil_div(n_tt, nseg);
     nseg = ceil_div(n_tt, seg_tiles);
 }
 
@@ -423,7 +498,7 @@ template <int MODE, int RB>
 static int launch_scan(const RowScanArgs& a, int nseg, cudaStream_t st) {
     // query block + two train buffers; at least 80 KB so that no more than two
     // CTAs (2 x 256 tensor-memory columns) share an SM
-    const size_t smem_launch = std::max((size_t)3 * MT * RB, (size_t)80 * 1024);
+    const size_t smem_launch = std::max((size_t)(RB <= 128 ? 4 : 3) * MT * RB, (size_t)80 * 1024);
     PYSIFT_CUDA_TRY(cudaFuncSetAttribute(k_match_rows<MODE, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem_launch));
     dim3 grid(ceil_div(a.n_q, MT), nseg);
