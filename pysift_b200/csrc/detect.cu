@@ -751,13 +751,13 @@ __device__ __forceinline__ unsigned long long pack2(float lo, float hi) {
 __device__ __forceinline__ float lo2(unsigned long long v) { return __uint_as_float((unsigned)(v & 0xffffffffull)); }
 __device__ __forceinline__ float hi2(unsigned long long v) { return __uint_as_float((unsigned)(v >> 32)); }
 
-// Tile geometry of k_blur<R>: input rows [r0-R, r0+TH+R) and columns
+// Tile geometry of k_blur<R, TH>: input rows [r0-R, r0+TH+R) and columns
 // [c0-R, c0+TW+R) at a row stride TS = 2 (mod 4) (8-byte aligned rows; lanes
 // that own consecutive rows read 8-byte pairs from distinct banks), then the
 // row-filtered rows at the stride HS = 66, also 2 (mod 4).
-template <int R>
+template <int R, int TH>
 struct BlurTile {
-    static constexpr int ROWS = BLUR_TH + 2 * R;
+    static constexpr int ROWS = TH + 2 * R;
     static constexpr int TWR = BLUR_TW + 2 * R;
     static constexpr int TS = (TWR % 4 == 2) ? TWR : TWR + 2;
     static constexpr int HS = BLUR_TW + 2;
@@ -794,17 +794,18 @@ __device__ __forceinline__ void blur_row_strip(const float* src, float* dst, con
 // warps), 8 outputs per lane.  Column pass: each thread filters a pair of
 // adjacent columns over 4 rows.  Both passes use packed fma pairs; each
 // output is the same fmaf chain over the taps in ascending order.
-template <int R>
-__global__ void __launch_bounds__(BLUR_NT) k_blur(const BlurArgs a) {
-    using T = BlurTile<R>;
-    constexpr int TW = BLUR_TW, TH = BLUR_TH, ROWS = T::ROWS, TWR = T::TWR, TS = T::TS, HS = T::HS;
+template <int R, int TH>
+__global__ void __launch_bounds__(BLUR_NT, TH == 40 ? 7 : 1) k_blur(const BlurArgs a) {
+    using T = BlurTile<R, TH>;
+    constexpr int TW = BLUR_TW, ROWS = T::ROWS, TWR = T::TWR, TS = T::TS, HS = T::HS;
+    constexpr int RP = TH / 8;  // column-pass rows per thread
     constexpr int CQ = (TWR + 31) / 32;
     static_assert(BLUR_NT / 32 == TW / 8, "one warp per 8-column strip in the row pass");
-    static_assert(BLUR_NT == (TW / 2) * (TH / 4), "one thread per column pair and 4 rows in the column pass");
+    static_assert(TH % 8 == 0 && BLUR_NT == (TW / 2) * 8, "one thread per column pair and TH / 8 rows in the column pass");
     extern __shared__ __align__(16) float smem[];
     float* tile = smem;
     float* hb = smem + ROWS * TS;
-    const int c0 = blockIdx.x * TW, r0 = blockIdx.y * TH;
+    const int c0 = blockIdx.x * TW, r0 = blockIdx.y * TH;  // TH: the template tile height
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     {
         long long gcs[CQ];
@@ -851,22 +852,24 @@ __global__ void __launch_bounds__(BLUR_NT) k_blur(const BlurArgs a) {
     }
     __syncthreads();
     {
-        const int cp = lane, y0 = warp * 4;
-        constexpr int NV = 4 + 2 * R;
+        const int cp = lane, y0 = warp * RP;
+        constexpr int NV = RP + 2 * R;
         unsigned long long V[NV];
 #pragma unroll
         for (int m = 0; m < NV; ++m) V[m] = reinterpret_cast<const unsigned long long*>(hb + (y0 + m) * HS)[cp];
-        unsigned long long A[4] = {0ull, 0ull, 0ull, 0ull};
+        unsigned long long A[RP];
+#pragma unroll
+        for (int j = 0; j < RP; ++j) A[j] = 0ull;
 #pragma unroll
         for (int k = 0; k <= 2 * R; ++k) {
             const unsigned long long wk = a.w2[k];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) A[j] = ffma2(V[j + k], wk, A[j]);
+            for (int j = 0; j < RP; ++j) A[j] = ffma2(V[j + k], wk, A[j]);
         }
         const int gc = c0 + 2 * cp;
         const bool vec = gc + 1 < a.W && (a.out_pitch & 1) == 0;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
+        for (int j = 0; j < RP; ++j) {
             const int gr = r0 + y0 + j;
             if (gr >= a.H || gc >= a.W) continue;
             const float v0 = lo2(A[j]), v1 = hi2(A[j]);
@@ -926,40 +929,83 @@ static size_t blur_smem_bytes(int R) {
 
 typedef void (*BlurKernel)(const BlurArgs);
 
-static size_t blur_fast_smem_bytes(int R) {
-    switch (R) {
-#define PYSIFT_BLUR_BYTES(r) \
-    case r: return BlurTile<r>::bytes;
-        PYSIFT_BLUR_BYTES(1) PYSIFT_BLUR_BYTES(2) PYSIFT_BLUR_BYTES(3) PYSIFT_BLUR_BYTES(4)
-        PYSIFT_BLUR_BYTES(5) PYSIFT_BLUR_BYTES(6) PYSIFT_BLUR_BYTES(7) PYSIFT_BLUR_BYTES(8)
-        PYSIFT_BLUR_BYTES(9) PYSIFT_BLUR_BYTES(10) PYSIFT_BLUR_BYTES(11) PYSIFT_BLUR_BYTES(12)
-        PYSIFT_BLUR_BYTES(13) PYSIFT_BLUR_BYTES(14) PYSIFT_BLUR_BYTES(15) PYSIFT_BLUR_BYTES(16)
-#undef PYSIFT_BLUR_BYTES
-        default: return 0;
+static int num_sms();
+
+// Register-blocked blur variants: radius 1..16 x tile height 16, 32, 40.
+constexpr int BLUR_NV = 3;
+constexpr int BLUR_THS[BLUR_NV] = {16, 32, 40};
+struct BlurVariant {
+    BlurKernel fn;
+    size_t smem;
+};
+static_assert(BlurTile<16, 40>::bytes <= 48 * 1024, "k_blur<R, TH> stays within the default dynamic shared memory");
+
+template <int R>
+static BlurVariant blur_variant_r(int v) {
+    switch (v) {
+        case 0: return {k_blur<R, 16>, BlurTile<R, 16>::bytes};
+        case 1: return {k_blur<R, 32>, BlurTile<R, 32>::bytes};
+        default: return {k_blur<R, 40>, BlurTile<R, 40>::bytes};
     }
 }
-static_assert(BlurTile<16>::bytes <= 48 * 1024, "k_blur<R> stays within the default dynamic shared memory");
 
-static BlurKernel blur_table(int R) {
+static BlurVariant blur_variant(int R, int v) {
     switch (R) {
-        case 1: return k_blur<1>;
-        case 2: return k_blur<2>;
-        case 3: return k_blur<3>;
-        case 4: return k_blur<4>;
-        case 5: return k_blur<5>;
-        case 6: return k_blur<6>;
-        case 7: return k_blur<7>;
-        case 8: return k_blur<8>;
-        case 9: return k_blur<9>;
-        case 10: return k_blur<10>;
-        case 11: return k_blur<11>;
-        case 12: return k_blur<12>;
-        case 13: return k_blur<13>;
-        case 14: return k_blur<14>;
-        case 15: return k_blur<15>;
-        case 16: return k_blur<16>;
-        default: return nullptr;
+        case 1: return blur_variant_r<1>(v);
+        case 2: return blur_variant_r<2>(v);
+        case 3: return blur_variant_r<3>(v);
+        case 4: return blur_variant_r<4>(v);
+        case 5: return blur_variant_r<5>(v);
+        case 6: return blur_variant_r<6>(v);
+        case 7: return blur_variant_r<7>(v);
+        case 8: return blur_variant_r<8>(v);
+        case 9: return blur_variant_r<9>(v);
+        case 10: return blur_variant_r<10>(v);
+        case 11: return blur_variant_r<11>(v);
+        case 12: return blur_variant_r<12>(v);
+        case 13: return blur_variant_r<13>(v);
+        case 14: return blur_variant_r<14>(v);
+        case 15: return blur_variant_r<15>(v);
+        case 16: return blur_variant_r<16>(v);
+        default: return {nullptr, 0};
     }
+}
+
+// Resident CTAs per SM of every variant, queried once per device.
+static int blur_occupancy(int R, int v) {
+    constexpr int MAXDEV = 64;
+    static std::once_flag once[MAXDEV];
+    static int occ[MAXDEV][BLUR_PAIR_MAX_R + 1][BLUR_NV];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAXDEV) return 1;
+    std::call_once(once[dev], [dev] {
+        for (int r = 1; r <= BLUR_PAIR_MAX_R; ++r)
+            for (int k = 0; k < BLUR_NV; ++k) {
+                const BlurVariant bv = blur_variant(r, k);
+                int n = 0;
+                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bv.fn, BLUR_NT, bv.smem) != cudaSuccess) n = 1;
+                occ[dev][r][k] = n > 0 ? n : 1;
+            }
+    });
+    return occ[dev][R][v];
+}
+
+// The tile height with the fewest (rounds of resident CTAs) x (tile rows +
+// halo): big levels avoid a short last round, small ones a long CTA.
+static int blur_pick(int R, int H, int W) {
+    int best = 1;
+    long long best_cost = -1;
+    for (int v = 0; v < BLUR_NV; ++v) {
+        const long long blocks = (long long)ceil_div(W, BLUR_TW) * ceil_div(H, BLUR_THS[v]);
+        const long long slots = (long long)num_sms() * blur_occupancy(R, v);
+        const long long rounds = (blocks + slots - 1) / slots;
+        const long long cost = rounds * (BLUR_THS[v] + 2 * R);
+        if (best_cost < 0 || cost < best_cost) {
+            best_cost = cost;
+            best = v;
+        }
+    }
+    return best;
 }
 
 static int ensure_blur_attrs() {
@@ -984,12 +1030,14 @@ static int launch_blur(BlurArgs& a, int R, const float* w, cudaStream_t st) {
         memcpy(&u, &w[k], sizeof(u));
         a.w2[k] = ((unsigned long long)u << 32) | u;
     }
-    dim3 grid(ceil_div(a.W, BLUR_TW), ceil_div(a.H, BLUR_TH));
-    BlurKernel kfn = (R >= 1) ? blur_table(R) : nullptr;
-    if (kfn) {
-        kfn<<<grid, BLUR_NT, blur_fast_smem_bytes(R), st>>>(a);
+    if (R >= 1 && R <= BLUR_PAIR_MAX_R) {
+        const int v = blur_pick(R, a.H, a.W);
+        const BlurVariant bv = blur_variant(R, v);
+        dim3 grid(ceil_div(a.W, BLUR_TW), ceil_div(a.H, BLUR_THS[v]));
+        bv.fn<<<grid, BLUR_NT, bv.smem, st>>>(a);
         PYSIFT_LAUNCH_CHECK("k_blur");
     } else {
+        dim3 grid(ceil_div(a.W, BLUR_TW), ceil_div(a.H, BLUR_TH));
         int rc = ensure_blur_attrs();
         if (rc) return rc;
         k_blur_generic<<<grid, BLUR_NT, blur_smem_bytes(R), st>>>(a, R);
