@@ -373,8 +373,17 @@ __global__ void k_blend_prepare(const Img1 w1, const uint8_t* __restrict__ m1,
         const float s0 = (g1[0] + g2[0]) * 0.5f, s1 = (g1[1] + g2[1]) * 0.5f, s2 = (g1[2] + g2[2]) * 0.5f;
         avg[p] = ((s0 + s1) + s2) / 3.0f;
     }
+    // one atomic per block on the single seam-RMSE counter (per-warp atomics
+    // on one address serialise in L2); a block's sum stays below 2^32
+    __shared__ unsigned int s_sq[32];
     sq = warp_sum(sq);
-    if ((threadIdx.x & 31) == 0 && sq) atomicAdd(&ctl->sq, (unsigned long long)sq);
+    if ((threadIdx.x & 31) == 0) s_sq[threadIdx.x >> 5] = sq;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned int t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_sq[w];
+        if (t) atomicAdd(&ctl->sq, (unsigned long long)t);
+    }
 }
 
 // scipy sobel of the average gray along both axes and the seam cost

@@ -215,10 +215,22 @@ __global__ void __launch_bounds__(256) k_warp_feather(const WarpArgs a) {
     }
     if (a.mask1) a.mask1[(long long)v * a.cw + u] = valid1;
     if (a.mask2) a.mask2[(long long)v * a.cw + u] = valid2;
-    if (valid1 || valid2) {
-        if (a.row_lo) {
-            atomicMin(&a.row_lo[v], u);
-            atomicMax(&a.row_hi[v], u);
+    if (a.row_lo) {
+        // the lanes of a warp share the row: one min / max per warp for the
+        // row extents (same-address atomics serialise), one per pixel for the
+        // columns (distinct addresses)
+        const bool cov = valid1 || valid2;
+        const unsigned am = __activemask();
+        const unsigned cm = __ballot_sync(am, cov);
+        if (cm) {
+            const int lo = __reduce_min_sync(am, cov ? u : 0x7fffffff);
+            const int hi = __reduce_max_sync(am, cov ? u : -1);
+            if ((int)(threadIdx.x & 31) == __ffs(cm) - 1) {
+                atomicMin(&a.row_lo[v], lo);
+                atomicMax(&a.row_hi[v], hi);
+            }
+        }
+        if (cov) {
             atomicMin(&a.col_lo[u], v);
             atomicMax(&a.col_hi[u], v);
         }
