@@ -679,21 +679,36 @@ __device__ __forceinline__ float seam_value(const uint8_t* __restrict__ m1, cons
 }
 
 // seam-mask blur (sigma 3, 25 taps, reflect-101, float64 sums in tap order):
-// the row pass over the mask values ...
-__global__ void __launch_bounds__(256) k_seam_rows(const uint8_t* __restrict__ m1, const uint8_t* __restrict__ m2,
-                                                   const int* __restrict__ seam, const BlendCtl* ctl,
-                                                   const SeamTaps k25, float* __restrict__ out, int W) {
-    __shared__ float sv[256 + 24];
-    const int y = blockIdx.y, x0 = blockIdx.x * 256;
-    for (int i = threadIdx.x; i < 256 + 24; i += 256)
-        sv[i] = seam_value(m1, m2, seam, ctl, refl_101(x0 + i - 12, W), y, W);
+// the row pass over the mask values ...  A block stages the mask values of
+// SR_T x SR_R outputs (+12 each side) in shared memory, one padding word per
+// 8 values so that lanes reading 8-value strips hit distinct banks; a thread
+// widens its SR_R + 24 inputs to float64 once and forms SR_R outputs, each
+// the same 25-tap sum in tap order.
+constexpr int SR_T = 64, SR_R = 8, SR_N = SR_T * SR_R + 24;
+__device__ __forceinline__ int sr_phys(int i) { return i + (i >> 3); }
+
+__global__ void __launch_bounds__(SR_T) k_seam_rows(const uint8_t* __restrict__ m1, const uint8_t* __restrict__ m2,
+                                                    const int* __restrict__ seam, const BlendCtl* ctl,
+                                                    const SeamTaps k25, float* __restrict__ out, int W) {
+    __shared__ float sv[SR_N + SR_N / 8 + 1];
+    const int y = blockIdx.y, x0 = blockIdx.x * SR_T * SR_R;
+    for (int i = threadIdx.x; i < SR_N; i += SR_T)
+        sv[sr_phys(i)] = seam_value(m1, m2, seam, ctl, refl_101(x0 + i - 12, W), y, W);
     __syncthreads();
-    const int x = x0 + threadIdx.x;
-    if (x >= W) return;
-    double s = 0.0;
+    const int b = threadIdx.x * SR_R;
+    if (x0 + b >= W) return;
+    double v[SR_R + 24];
 #pragma unroll
-    for (int t = 0; t < 25; ++t) s = s + (double)k25.k[t] * (double)sv[threadIdx.x + t];
-    out[(long long)y * W + x] = (float)s;
+    for (int m = 0; m < SR_R + 24; ++m) v[m] = (double)sv[sr_phys(b + m)];
+#pragma unroll
+    for (int j = 0; j < SR_R; ++j) {
+        const int x = x0 + b + j;
+        if (x >= W) break;
+        double s = 0.0;
+#pragma unroll
+        for (int t = 0; t < 25; ++t) s = s + (double)k25.k[t] * v[j + t];
+        out[(long long)y * W + x] = (float)s;
+    }
 }
 
 // ... then the column pass; the blurred value replaces the mask where both
@@ -1273,7 +1288,7 @@ int pysift_blend_multiband(const void* image1, int32_t image1_f32, const uint8_t
     // seam mask and its blur
     float* gm0 = bwp<float>(ws, l.off_gm[0]);
     float* srow = bwp<float>(ws, l.off_srow);
-    k_seam_rows<<<g2d, 256, 0, st>>>(mask1, mask2, seam, ctl, k25, srow, cw);
+    k_seam_rows<<<dim3(ceil_div(cw, SR_T * SR_R), ch), SR_T, 0, st>>>(mask1, mask2, seam, ctl, k25, srow, cw);
     PYSIFT_LAUNCH_CHECK("k_seam_rows");
     k_seam_cols<<<g2d, 256, 0, st>>>(srow, mask1, mask2, seam, ctl, k25, gm0, cw, ch);
     PYSIFT_LAUNCH_CHECK("k_seam_cols");
