@@ -284,6 +284,31 @@ def test_single_image_graph_replay(oracle_lib):
     assert np.array_equal(d2.cpu().numpy(), ref["desc"])
 
 
+def test_capture_on_a_stream_the_library_has_not_seen():
+    """A detection captured into a CUDA graph on a fresh stream with no eager
+    call on that stream first (the library then keeps all of its work on the
+    caller's stream instead of forking its side stream): the replay's rows
+    equal an eager detection's."""
+    import torch
+    from pysift_b200 import PySIFT, _lib
+    img = synthetic.scene(480, 640, seed=43)
+    k1, d1 = PySIFT(graphs=False).detectAndCompute(img, gpu_output=True)
+    sift = PySIFT(graphs=False)
+    H, W = img.shape
+    g_dev = torch.from_numpy(img).cuda()
+    b = sift._buffers(H, W)  # allocated outside the capture
+    torch.cuda.synchronize()
+    fresh = torch.cuda.Stream()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=fresh):
+        sift._launch(b, g_dev.data_ptr(), H, W, W, fresh.cuda_stream)
+    graph.replay()
+    torch.cuda.synchronize()
+    n = int(b.stats.cpu()[_lib.STAT_N_KEYPOINTS])
+    assert n == k1.shape[0] and n > 0
+    assert torch_equal(b.kpts[:n], k1) and torch_equal(b.desc[:n], d1)
+
+
 def torch_equal(x, y):
     import torch
     return x.shape == y.shape and bool(torch.equal(x, y))
