@@ -79,6 +79,18 @@ def test_odd_sizes(shape, oracle_lib):
     _compare(out, ref)
 
 
+def test_wide_image_bit_exact(oracle_lib):
+    """1024 x 2100: doubled (8.6 Mpix, under the cap), so the in-place row
+    prefilter walks each 2100-wide row in two chunks, and the blur tile
+    heights are picked for odd level sizes; pyramid and every output row
+    bit-exact against the oracle."""
+    img = synthetic.scene(1024, 2100, seed=9)
+    sift, out, ref = _run_both(img, oracle_lib)
+    assert sift.last_stats[5] == 1
+    assert not _pyramid_equal(sift, img, ref)
+    _compare(out, ref)
+
+
 def test_no_doubling(oracle_lib):
     img = synthetic.scene(480, 640, seed=3)
     sift, out, ref = _run_both(img, oracle_lib, double_image=False)
