@@ -39,7 +39,7 @@ def test_exact_u8_ties_go_to_lower_index():
     assert (out["fwd_best"][:100].cpu().numpy() == np.arange(100)).all()
 
 
-@pytest.mark.parametrize("n1,n2,D", [(700, 900, 64), (1200, 800, 128)])
+@pytest.mark.parametrize("n1,n2,D", [(700, 900, 64), (1200, 800, 128), (8000, 8000, 64)])
 def test_fp16_reference_mode(n1, n2, D):
     import torch
     from oracle import match_oracle as mo
