@@ -133,6 +133,12 @@ int pysift_detect_workspace_view(const pysift_detect_config* cfg, int32_t H, int
 int pysift_gauss_blur(const float* in, int32_t in_pitch, float* out, int32_t out_pitch, int32_t H, int32_t W,
                       const float* weights, int32_t radius, pysift_stream_t stream);
 
+/* Testing hook: the blur's tile height (16, 32 or 40 rows) is normally
+ * picked per launch from the level size and the device's occupancy;
+ * rows = 16, 32 or 40 forces it for every later launch in the process,
+ * rows = 0 restores the automatic choice.  Results do not depend on it. */
+int pysift_set_blur_tile_rows(int32_t rows);
+
 /* 2x cubic B-spline zoom of a uint8 image scaled by 1/255
  * (cupyx.scipy.ndimage.zoom(order=3) at pysift/core.py:1270-1275).
  * coef: caller scratch of H*W doubles; out: 2H x 2W floats, pitch in floats. */

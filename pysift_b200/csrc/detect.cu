@@ -990,9 +990,14 @@ static int blur_occupancy(int R, int v) {
     return occ[dev][R][v];
 }
 
+// pysift_set_blur_tile_rows: a forced variant (testing), -1 = automatic
+static std::atomic<int> g_blur_forced{-1};
+
 // The tile height with the fewest (rounds of resident CTAs) x (tile rows +
 // halo): big levels avoid a short last round, small ones a long CTA.
 static int blur_pick(int R, int H, int W) {
+    const int forced = g_blur_forced.load(std::memory_order_relaxed);
+    if (forced >= 0) return forced;
     int best = 1;
     long long best_cost = -1;
     for (int v = 0; v < BLUR_NV; ++v) {
@@ -2699,6 +2704,15 @@ int pysift_gauss_blur(const float* in, int32_t in_pitch, float* out, int32_t out
     a.H = H;
     a.W = W;
     return launch_blur(a, radius, weights, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int pysift_set_blur_tile_rows(int32_t rows) {
+    int v = -1;
+    for (int k = 0; k < BLUR_NV; ++k)
+        if (rows == BLUR_THS[k]) v = k;
+    PYSIFT_CHECK_ARG(rows == 0 || v >= 0, "tile rows %d: 0 (automatic), 16, 32 or 40", rows);
+    g_blur_forced.store(rows == 0 ? -1 : v, std::memory_order_relaxed);
+    return PYSIFT_OK;
 }
 
 int pysift_zoom2x_u8(const uint8_t* gray, int32_t H, int32_t W, int64_t pitch_bytes, int32_t fp16_round,

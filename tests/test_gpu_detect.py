@@ -203,6 +203,38 @@ def test_gauss_blur_entry_point(sigma, H, W, pitch, oracle_lib):
     assert np.array_equal(dst[:, :W].cpu().numpy(), ref)
 
 
+@pytest.mark.parametrize("rows", [16, 32, 40])
+def test_gauss_blur_every_tile_height(rows, oracle_lib):
+    """Each register-blocked blur variant (tile height forced through the
+    testing hook; normally picked per launch from the level size and the
+    occupancy) against the oracle's FMA-chain blur, bit for bit, for radii
+    1, 5, 12 and 16 and odd and even pitches."""
+    import torch
+    from oracle import oracle
+    from pysift_b200 import _lib
+    from pysift_b200.core import gaussian_weights
+    lib = _lib.load()
+    assert lib.pysift_set_blur_tile_rows(7) != 0  # only 0, 16, 32 and 40
+    try:
+        assert lib.pysift_set_blur_tile_rows(rows) == 0
+        for sigma, (H, W, pitch) in [(0.3, (75, 130, 131)), (1.25, (257, 301, 301)), (3.0, (130, 128, 160)),
+                                     (4.0, (90, 200, 203))]:
+            rng = np.random.default_rng(H * W + rows)
+            img = rng.random((H, W), dtype=np.float32)
+            src = torch.zeros((H, pitch), dtype=torch.float32, device="cuda")
+            src[:, :W] = torch.from_numpy(img).cuda()
+            dst = torch.full((H, pitch), float("nan"), dtype=torch.float32, device="cuda")
+            k, radius = gaussian_weights(sigma)
+            k = np.ascontiguousarray(k, dtype=np.float32)
+            rc = lib.pysift_gauss_blur(src.data_ptr(), pitch, dst.data_ptr(), pitch, H, W,
+                                       k.ctypes.data_as(ctypes.c_void_p), radius,
+                                       torch.cuda.current_stream().cuda_stream)
+            assert rc == 0, lib.pysift_last_error()
+            assert np.array_equal(dst[:, :W].cpu().numpy(), oracle.gauss_blur(img, sigma)), (sigma, radius)
+    finally:
+        lib.pysift_set_blur_tile_rows(0)
+
+
 def test_detect_batch_matches_single_image_calls():
     """detect_batch on uneven sizes over several streams returns, per image,
     exactly what detectAndCompute returns for that image alone."""
