@@ -65,7 +65,7 @@ struct Ctrl {
     int n_oriented;
     int overflow_octs;
     int desc_next;  // next oriented entry a descriptor block takes
-    int pad[1];
+    int ori_next;   // next kept keypoint an orientation block takes
 };
 
 // buckets of the exact rank kernels (k_br_*)
@@ -1637,13 +1637,20 @@ __device__ __forceinline__ float mod360(float x) { return x >= 360.0f ? x - 360.
 constexpr int ORI_T = 64;
 constexpr int ORI_W = ORI_T / 32;
 
-__global__ void __launch_bounds__(ORI_T) k_orientation(const OriArgs a, const Ctrl* ctrl) {
+// One ORI_T-thread block per kept keypoint at a time: the first is the
+// block index, later ones come from a counter (windows differ in size), the
+// next index requested when a keypoint starts and read when it ends.
+__global__ void __launch_bounds__(ORI_T) k_orientation(const OriArgs a, Ctrl* ctrl) {
     __shared__ unsigned int wlo[ORI_W][36], whi[ORI_W][36];
     __shared__ unsigned long long whist[ORI_W][36];
     __shared__ float h0[36], h1[36];
+    __shared__ int s_next[2];  // alternates, so a late reader never sees the next keypoint
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int n = ctrl->n_kept;
-    for (int i = blockIdx.x; i < n; i += gridDim.x) {
+    int i = blockIdx.x;
+    for (int it = 0; i < n; ++it) {
+        int next = 0;
+        if (tid == 0) next = (int)gridDim.x + atomicAdd(&ctrl->ori_next, 1);
         for (int b = tid; b < ORI_W * 36; b += ORI_T) {
             (&whist[0][0])[b] = 0ull;
             (&wlo[0][0])[b] = 0u;
@@ -1762,7 +1769,9 @@ __global__ void __launch_bounds__(ORI_T) k_orientation(const OriArgs a, const Ct
                 for (int k = cnt; k < 4; ++k) a.ang[i * 4 + k] = -1.0f;
             }
         }
+        if (tid == 0) s_next[it & 1] = next;
         __syncthreads();
+        i = s_next[it & 1];
     }
 }
 
