@@ -186,6 +186,15 @@ def dist_setup():
     return world, rank, local
 
 
+def all_ranks_max(t, world):
+    """Replace `t` in place by its element-wise maximum over all ranks, so a
+    step time is the slowest rank's; a no-op on one process."""
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t
+
+
 def run_reference(args, wl, world, rank):
     """--impl reference: the reference's path as the CPU oracle port, rank 0 only."""
     if rank != 0:
@@ -273,8 +282,7 @@ def run_match(args, wl, world, rank, local):
     launches = lib.pysift_launch_count() - launches0
     n_pairs = int(out["count"].item())
     t = torch.tensor([float(np.sum(step_ms))], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    all_ranks_max(t, world)
     total_ms = float(t.item())
     # end to end: pinned host sets -> device, match, pairs and count back to the host
     ha = torch.from_numpy(a).pin_memory()
@@ -292,8 +300,7 @@ def run_match(args, wl, world, rank, local):
         if i >= args.warmup:
             e2e_ms.append(dt * 1e3)
     e2e_t = torch.tensor([float(np.sum(e2e_ms))], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    all_ranks_max(e2e_t, world)
     if rank != 0:
         return 0
     step_s = total_ms / args.steps / 1e3
@@ -456,8 +463,7 @@ def run_batch_detect(args, wl, world, rank, local):
         step_ms = timed(lambda: sift.detect_batch(g, n_streams=ns), args.steps)
     launches = lib.pysift_launch_count() - launches0
     t = torch.tensor([float(np.sum(step_ms))], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    all_ranks_max(t, world)
     total_ms = float(t.item())
     # the same images, the plain way: one detectAndCompute call per image
     # (each comparison leg runs once untimed first, as the batched one did:
@@ -487,8 +493,7 @@ def run_batch_detect(args, wl, world, rank, local):
         if i >= args.warmup:
             e2e_ms.append(dt * 1e3)
     e2e_t = torch.tensor([float(np.sum(e2e_ms))], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    all_ranks_max(e2e_t, world)
     if rank != 0:
         return 0
     n_kp = int(sum(r[0].shape[0] for r in res))
@@ -585,8 +590,7 @@ def run_batch_stitch(args, wl, world, rank, local, pairs):
         step_ms = timed(lambda: st.stitch_batch(g, n_streams=ns), args.steps)
     launches = lib.pysift_launch_count() - launches0
     t = torch.tensor([float(np.sum(step_ms))], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    all_ranks_max(t, world)
     total_ms = float(t.item())
     metrics = st.last_batch_metrics
     plain_fn = lambda: [st.stitch(a, b) for a, b in g]
@@ -602,8 +606,7 @@ def run_batch_stitch(args, wl, world, rank, local, pairs):
         if i >= args.warmup:
             e2e_ms.append(dt * 1e3)
     e2e_t = torch.tensor([float(np.sum(e2e_ms))], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    all_ranks_max(e2e_t, world)
     if rank != 0:
         return 0
     P = len(pairs)
@@ -818,8 +821,7 @@ def run_detect(args, wl, world, rank, local):
         dist.barrier()
     total_ms = float(np.sum(step_ms))
     t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    all_ranks_max(t, world)
     total_ms = float(t.item())
 
     # end to end: pinned host image -> device -> pipeline -> host arrays
@@ -845,8 +847,7 @@ def run_detect(args, wl, world, rank, local):
             e2e_ms.append(dt * 1e3)
             d2h = b.stats.numel() * 4 + n * (4 * 4 + 4 + 4 + 128 * 4)
     e2e_tot = torch.tensor([float(np.sum(e2e_ms))], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(e2e_tot, op=dist.ReduceOp.MAX)
+    all_ranks_max(e2e_tot, world)
 
     if rank != 0:
         return 0
@@ -943,8 +944,7 @@ def run_stitch(args, wl, world, rank, local):
     if world > 1:
         dist.barrier()
     t = torch.tensor([float(np.sum(step_ms))], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    all_ranks_max(t, world)
     total_ms = float(t.item())
     m = dict(st.last_metrics)
     # end to end through the public API with host images
@@ -958,8 +958,7 @@ def run_stitch(args, wl, world, rank, local):
         if i >= args.warmup:
             e2e_ms.append(dt * 1e3)
     e2e_tot = torch.tensor([float(np.sum(e2e_ms))], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(e2e_tot, op=dist.ReduceOp.MAX)
+    all_ranks_max(e2e_tot, world)
     # stage breakdown of one more stitch (events on the stitch's stream)
     st.stage_events = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
     st.stitch(g1, g2)
