@@ -49,6 +49,23 @@ def gaussian_weights(sigma, truncate=4):
     return k.astype(np.float32), radius
 
 
+def check_detector_options(dsp_n_scales, orientation, descriptor):
+    """Reject the detector options this backend does not carry, before any
+    device work: the reference's DSP scale-count check
+    (pysift/core.py:1203-1204), and the learned orientation and descriptor
+    paths, which raise NotImplementedError instead of falling back."""
+    if dsp_n_scales not in DSP_PRESETS:
+        raise ValueError(f"dsp_n_scales must be 3, 4, or 5 (got {dsp_n_scales})")
+    if orientation != 'histogram':
+        raise NotImplementedError(
+            f"orientation={orientation!r}: only the histogram orientation is implemented on this backend "
+            "(the learned OriNet/AffNet paths are not part of it)")
+    if descriptor != 'sift':
+        raise NotImplementedError(
+            f"descriptor={descriptor!r}: only the SIFT descriptor is implemented on this backend "
+            "(the learned HardNet/HyNet paths are not part of it)")
+
+
 def build_detect_config(n_octaves, n_scales, sigma0, contrast_thresh, edge_thresh, dsp, dsp_n_scales,
                         fp16_pyramid, double_image, rootsift, high_vram):
     """Fill pysift_detect_config the way the reference's host code derives
@@ -162,16 +179,7 @@ class PySIFT:
                  dsp=False, dsp_n_scales=3, fp16_pyramid=None, orientation='histogram', descriptor='sift',
                  double_image=True, rootsift=True, *, device=None, high_vram=None, as_uint8=False,
                  graphs=True):
-        if dsp_n_scales not in DSP_PRESETS:
-            raise ValueError(f"dsp_n_scales must be 3, 4, or 5 (got {dsp_n_scales})")
-        if orientation != 'histogram':
-            raise NotImplementedError(
-                f"orientation={orientation!r}: only the histogram orientation is implemented on this backend "
-                "(the learned OriNet/AffNet paths are not part of it)")
-        if descriptor != 'sift':
-            raise NotImplementedError(
-                f"descriptor={descriptor!r}: only the SIFT descriptor is implemented on this backend "
-                "(the learned HardNet/HyNet paths are not part of it)")
+        check_detector_options(dsp_n_scales, orientation, descriptor)
         if as_uint8 and rootsift:
             raise ValueError("as_uint8 converts the L2 / clip / L2 descriptor as OpenCV does: "
                              "construct with rootsift=False")

@@ -20,7 +20,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .core import PySIFT
+from .core import PySIFT, check_detector_options
 
 
 def _ptr_aligned(t, align=256):
@@ -58,6 +58,7 @@ class GPUPyStitch:
                  clahe_clip=2.0, clahe_tile=8, output_max_dim=0, post_sharpen=False, output_format='png',
                  output_quality=90, *, device=None, save_output=True, verbose=True, high_vram=None,
                  blend='multiband'):
+        check_detector_options(3, orientation, descriptor)
         if matcher != 'ratio':
             raise NotImplementedError(f"matcher={matcher!r}: only the ratio-test matcher is implemented here")
         if pca_dims not in (0, 64, 128):

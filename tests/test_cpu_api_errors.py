@@ -31,6 +31,8 @@ def test_pysift_without_a_device_fails_loudly():
 
 @pytest.mark.parametrize("kw,exc", [
     (dict(matcher='lightglue'), NotImplementedError),
+    (dict(orientation='orinet'), NotImplementedError),
+    (dict(descriptor='hardnet'), NotImplementedError),
     (dict(pca_dims=32), NotImplementedError),
     (dict(blend='average'), ValueError),
     (dict(n_blend_levels=9), ValueError),
