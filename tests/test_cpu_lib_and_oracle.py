@@ -167,3 +167,24 @@ def test_as_uint8_requires_plain_sift():
     from pysift_b200 import PySIFT
     with pytest.raises(ValueError):
         PySIFT(as_uint8=True)
+
+
+def test_product_never_imports_the_oracle():
+    """The package is the product; the oracle is test infrastructure only.
+    No module of pysift_b200 imports, loads or executes anything under
+    oracle/, so a missing CUDA library can only fail, never fall back."""
+    import ast
+    import pathlib
+    pkg = pathlib.Path(__file__).resolve().parent.parent / "pysift_b200"
+    for py in sorted(pkg.rglob("*.py")):
+        tree = ast.parse(py.read_text(), str(py))
+        for node in ast.walk(tree):
+            if isinstance(node, ast.Import):
+                names = [a.name for a in node.names]
+            elif isinstance(node, ast.ImportFrom):
+                names = [node.module or ""]
+            else:
+                continue
+            assert not any(n == "oracle" or n.startswith("oracle.") for n in names), f"{py.name} imports the oracle"
+        src = py.read_text()
+        assert "liboracle" not in src and "oracle/" not in src, f"{py.name} names an oracle file"
