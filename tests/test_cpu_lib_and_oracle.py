@@ -188,3 +188,23 @@ def test_product_never_imports_the_oracle():
             assert not any(n == "oracle" or n.startswith("oracle.") for n in names), f"{py.name} imports the oracle"
         src = py.read_text()
         assert "liboracle" not in src and "oracle/" not in src, f"{py.name} names an oracle file"
+
+
+@pytest.mark.parametrize("n_points,n_hyp", [(4, 1), (5, 155), (157, 156), (1000, 2048), (65537, 700)])
+def test_ransac_samples_equal_torch_randint(n_points, n_hyp):
+    """The reference draws its 4-point samples as torch.randint(0, N, (B, 4))
+    from a CPU generator seeded with 42 (pysift/core.py:3011-3060).  The
+    library's host stream (pysift_mt19937_u32) and the oracle's, reduced
+    modulo N as the RANSAC kernels do, give the same indices; the lengths
+    cross the 624-word MT19937 regeneration."""
+    import torch
+    from oracle import stitch_oracle as so
+    from pysift_b200 import _lib
+    lib = _lib.load()
+    host = np.empty(4 * n_hyp, np.uint32)
+    lib.pysift_mt19937_u32(42, host.ctypes.data_as(ctypes.c_void_p), host.size)
+    assert np.array_equal(host, so.mt19937_u32(42, 4 * n_hyp))
+    gen = torch.Generator(device="cpu")
+    gen.manual_seed(42)
+    want = torch.randint(0, n_points, (n_hyp, 4), generator=gen).numpy().ravel()
+    assert np.array_equal((host % np.uint32(n_points)).astype(np.int64), want)
