@@ -155,13 +155,25 @@ int pysift_zoom2x_u8(const uint8_t* gray, int32_t H, int32_t W, int64_t pitch_by
  * 2 = pysift_match_u8_split_fp8. */
 int pysift_match_workspace_size(int32_t n1, int32_t n2, int32_t D, int32_t exact_u8, size_t* bytes);
 
-/* Reference semantics: fp16 operands (16-byte aligned rows), the fp32
- * tensor-core tile rounded to fp16, d^2 = max(0, 2 - 2 s), pass iff
- * d2^2 > 1e-10 and d1^2 < ratio^2 d2^2 (float32). pairs: int32[n1][2]. */
+/* Reference semantics: fp16 operands (16-byte aligned rows), the similarity
+ * s = the fp16 rounding (nearest, ties to even) of the exact dot product,
+ * d^2 = max(0, 2 - 2 s), pass iff d2^2 > 1e-10 and d1^2 < ratio^2 d2^2
+ * (float32). pairs: int32[n1][2].  The tensor-core scan keeps candidates on
+ * its fp32 values; the two candidates of each row are recomputed exactly and
+ * the rows they do not settle are recomputed over every column, so the result
+ * is the one the exact similarity matrix gives, for rows of L2 norm <= 1 (the
+ * stitch path's normalised descriptors; the float64 sums are exact there). */
 int pysift_match_fp16(const uint16_t* d1, int32_t n1, const uint16_t* d2, int32_t n2, int32_t D, float ratio,
                       void* workspace, size_t workspace_bytes, int32_t* fwd_best, int32_t* fwd_pass,
                       int32_t* bwd_best, int32_t* bwd_pass, int32_t* pairs, float* pair_dist, int32_t* pair_count,
                       pysift_stream_t stream);
+
+/* Rows of the last pysift_match_fp16 on this workspace that the candidate
+ * check left to the exact recomputation over every column, forward and
+ * backward: counts (device int32[2]) receives them, stream-ordered.  A
+ * diagnostic; no counterpart in the reference. */
+int pysift_match_fp16_recheck_counts(const void* workspace, int32_t n1, int32_t n2, int32_t D, int32_t* counts,
+                                     pysift_stream_t stream);
 
 /* Exact squared L2 of uint8-valued descriptors via bf16 products (exact for
  * D <= 128), pass iff d2^2 > 0 and d1^2 < ratio^2 d2^2. */
@@ -338,7 +350,11 @@ int pysift_mask_extents(const uint8_t* mask, int32_t cw, int32_t ch, int32_t* ro
  * (H*W > PYSIFT_ZOOM2X_NOALLOC_MAX_PIXELS) return PYSIFT_ERR_CAPACITY.
  * The first call on a device looks up the array's device address
  * (cudaGetSymbolAddress) with that device current; make that first call
- * before any stream capture.  All calls share the one array: calls that
+ * before any stream capture.  The address is cached per device ordinal for
+ * the process: it holds for the device's primary context (the one the CUDA
+ * runtime uses) and only until that context is destroyed, so the entry point
+ * is not for callers that make their own driver-API contexts current or call
+ * cudaDeviceReset between calls.  All calls share the one array: calls that
  * overlap on the GPU (other streams, other host threads) race and must be
  * serialised by the caller.  Allocates nothing. */
 #define PYSIFT_ZOOM2X_NOALLOC_MAX_PIXELS (1 << 20)

@@ -101,6 +101,7 @@ EXPORTS.update({
     "pysift_match_fp16": (ctypes.c_int, [c_void_p, c_int32, c_void_p, c_int32, c_int32, c_float, c_void_p, c_size_t,
                                          c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                          c_void_p]),
+    "pysift_match_fp16_recheck_counts": (ctypes.c_int, [c_void_p, c_int32, c_int32, c_int32, c_void_p, c_void_p]),
     "pysift_match_u8_exact": (ctypes.c_int, [c_void_p, c_int32, c_void_p, c_int32, c_int32, c_float, c_void_p,
                                              c_size_t, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                              c_void_p, c_void_p]),

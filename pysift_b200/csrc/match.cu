@@ -16,9 +16,20 @@
 // (pysift/core.py:2574-2701, 2840-2940).
 //
 // Two scoring modes share the kernels:
-//   SIM_F16   reference semantics: fp16 inputs, the fp32 tile rounded to fp16
+//   SIM_F16   reference semantics: fp16 inputs, the similarity rounded to fp16
 //             (torch.mm under fp16 autocast, core.py:2604-2605), larger is better,
 //             d^2 = max(0, 2 - 2 s), pass iff d2^2 > 1e-10 and d1^2 < r^2 d2^2 in float32.
+//             The canonical similarity is the fp16 rounding (nearest, ties to
+//             even) of the EXACT dot product.  The tensor cores' fp32
+//             accumulation is within e = D 2^-21 |a| max|b| of it, so the
+//             scan keeps, on the raw fp32 values, the best and second with
+//             their indices and the third value; k_match_merge_f16 recomputes
+//             the two candidates exactly (float64 sums of the exact fp16
+//             products: every partial sum is a multiple of 2^-48 below 2^5 in
+//             magnitude for rows of norm <= 1, hence exact in any order) and
+//             accepts the row when no other column can reach the exact
+//             second value (fp16(third + e) <= second, and < best); the other
+//             rows are recomputed over every column by k_match_recheck_f16.
 //   DIST_BF16 exact L2 on uint8-valued descriptors: bf16 holds 0..255 exactly and
 //             every partial sum of 128 products stays below 2^24, so the fp32
 //             accumulator is the exact integer dot product.  Rows rank train
@@ -48,6 +59,71 @@ struct Top2 {  // best key and index, second-best key
     float k1, k2;
     int i1, pad;
 };
+
+// SIM_F16 scan state of one row: the best and second raw keys with their
+// indices (order: larger key first, the lower index on equal keys) and the
+// third-largest key of the columns seen.
+struct Top3 {
+    float k1, k2, k3;
+    int i1, i2;
+    int pad[3];
+};
+
+__device__ __forceinline__ void top3_init(Top3& t) {
+    t.k1 = t.k2 = t.k3 = -INFINITY;
+    t.i1 = t.i2 = 0x7fffffff;
+}
+
+// Column c with key x, visited in increasing column order within the state.
+__device__ __forceinline__ void top3_push(Top3& t, float x, int c) {
+    t.k3 = fmaxf(t.k3, fminf(x, t.k2));
+    const bool g1 = x > t.k1, g2 = x > t.k2;
+    t.i2 = g2 ? (g1 ? t.i1 : c) : t.i2;
+    t.k2 = fmaxf(t.k2, fminf(x, t.k1));
+    t.i1 = g1 ? c : t.i1;
+    t.k1 = fmaxf(t.k1, x);
+}
+
+__device__ __forceinline__ bool key_before(float ka, int ia, float kb, int ib) {
+    return ka > kb || (ka == kb && ia < ib);
+}
+
+// Union of two states over disjoint column sets (in any index relation):
+// the two first entries in (key desc, index asc) order, and the third-largest
+// key of the union.
+__device__ __forceinline__ void top3_merge(Top3& a, const Top3& b) {
+    Top3 r;
+    if (key_before(a.k1, a.i1, b.k1, b.i1)) {
+        r.k1 = a.k1;
+        r.i1 = a.i1;
+        if (key_before(a.k2, a.i2, b.k1, b.i1)) {
+            r.k2 = a.k2;
+            r.i2 = a.i2;
+            r.k3 = fmaxf(a.k3, b.k1);
+        } else {
+            r.k2 = b.k1;
+            r.i2 = b.i1;
+            r.k3 = fmaxf(a.k2, b.k2);
+        }
+    } else {
+        r.k1 = b.k1;
+        r.i1 = b.i1;
+        if (key_before(b.k2, b.i2, a.k1, a.i1)) {
+            r.k2 = b.k2;
+            r.i2 = b.i2;
+            r.k3 = fmaxf(b.k3, a.k1);
+        } else {
+            r.k2 = a.k1;
+            r.i2 = a.i1;
+            r.k3 = fmaxf(a.k2, b.k2);
+        }
+    }
+    a.k1 = r.k1;
+    a.k2 = r.k2;
+    a.k3 = r.k3;
+    a.i1 = r.i1;
+    a.i2 = r.i2;
+}
 
 // byte offset of 16-byte chunk c (8 elements along K) of row r in the
 // no-swizzle K-major layout: core matrices of 8 rows x 16 bytes, adjacent
@@ -125,7 +201,7 @@ struct RowScanArgs {
     const float* scale_q;  // SIM_I8: quantisation scale per query row
     const float* scale_t;  //         and per train row
     int seg_tiles;       // train tiles per segment (blockIdx.y)
-    Top2* part;          // [n_q][gridDim.y]
+    void* part;          // [n_q][gridDim.y] Top3 (SIM_F16) or Top2
     int* error;          // set when an MMA wait gives up
 };
 
@@ -163,6 +239,19 @@ __device__ __forceinline__ void scan_chunk(const uint32_t (&v)[32], int col0, in
     }
 }
 
+// SIM_F16: the raw fp32 accumulator values, even columns into e, odd into o
+// (two independent chains, each visiting its columns in increasing order).
+__device__ __forceinline__ void scan_chunk_f16(const uint32_t (&v)[32], int col0, int lim, Top3& e, Top3& o) {
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+        const float key = j < lim ? __uint_as_float(v[j]) : -INFINITY;
+        if (j & 1)
+            top3_push(o, key, col0 + j);
+        else
+            top3_push(e, key, col0 + j);
+    }
+}
+
 // Top-2 of the union of two disjoint column sets: the best is the larger
 // best (the lower index on equal keys, i.e. its first occurrence in index
 // order), the second the largest of the smaller best and the two seconds --
@@ -188,7 +277,7 @@ __global__ void __launch_bounds__(MATCH_THREADS) k_match_rows(const RowScanArgs 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int quad = warp & 3, half = warp >> 2;  // TMEM lane quadrant, column half of each tile
     const int rloc = quad * 32 + lane;            // this thread's query row in the block
-    __shared__ Top2 s_half[MT];
+    __shared__ Top3 s_half[MT];  // Top2 in the first 16 bytes outside SIM_F16
     const int q0 = blockIdx.x * MT;
     const int n_tt = (args.n_t + NT - 1) / NT;
     const int t_begin = blockIdx.y * args.seg_tiles;
@@ -219,6 +308,9 @@ __global__ void __launch_bounds__(MATCH_THREADS) k_match_rows(const RowScanArgs 
 
     float k1 = -INFINITY, k2 = -INFINITY, m1 = -INFINITY, m2 = -INFINITY;
     int i1 = 0x7fffffff, j1 = 0x7fffffff;
+    Top3 te, to;  // SIM_F16: even and odd column chains
+    top3_init(te);
+    top3_init(to);
     const float sq = (MODE == SIM_I8 && q0 + rloc < args.n_q) ? args.scale_q[q0 + rloc] : 1.0f;
     bool fail = false;
     int issued = 0;  // MMA groups committed
@@ -318,7 +410,11 @@ __global__ void __launch_bounds__(MATCH_THREADS) k_match_rows(const RowScanArgs 
                       "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
                     : "r"(taddr));
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                scan_chunk<MODE>(v, tcol0 + chunk * 32, lim_tile - chunk * 32, nb_lane, sq, k1, k2, i1, m1, m2, j1);
+                if constexpr (MODE == SIM_F16)
+                    scan_chunk_f16(v, tcol0 + chunk * 32, lim_tile - chunk * 32, te, to);
+                else
+                    scan_chunk<MODE>(v, tcol0 + chunk * 32, lim_tile - chunk * 32, nb_lane, sq, k1, k2, i1, m1, m2,
+                                     j1);
             }
             if (it < nt) load_nb(it);  // for the reduction of tile it, one iteration from now
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -332,26 +428,38 @@ __global__ void __launch_bounds__(MATCH_THREADS) k_match_rows(const RowScanArgs 
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
     // even and odd columns of this thread, then the two column halves of the row
-    top2_merge(k1, k2, i1, m1, m2, j1);
-    if (half == 1) {
-        Top2 h;
-        h.k1 = k1;
-        h.k2 = k2;
-        h.i1 = i1;
-        h.pad = 0;
-        s_half[rloc] = h;
-    }
-    __syncthreads();
     const int row = q0 + rloc;
-    if (half == 0 && !fail && row < args.n_q) {
-        const Top2 h = s_half[rloc];
-        top2_merge(k1, k2, i1, h.k1, h.k2, h.i1);
-        Top2 r;
-        r.k1 = k1;
-        r.k2 = k2;
-        r.i1 = i1;
-        r.pad = 0;
-        args.part[(size_t)row * gridDim.y + blockIdx.y] = r;
+    if constexpr (MODE == SIM_F16) {
+        top3_merge(te, to);
+        if (half == 1) s_half[rloc] = te;
+        __syncthreads();
+        if (half == 0 && !fail && row < args.n_q) {
+            top3_merge(te, s_half[rloc]);
+            te.pad[0] = te.pad[1] = te.pad[2] = 0;
+            static_cast<Top3*>(args.part)[(size_t)row * gridDim.y + blockIdx.y] = te;
+        }
+    } else {
+        top2_merge(k1, k2, i1, m1, m2, j1);
+        Top2* sh2 = reinterpret_cast<Top2*>(&s_half[rloc]);
+        if (half == 1) {
+            Top2 h;
+            h.k1 = k1;
+            h.k2 = k2;
+            h.i1 = i1;
+            h.pad = 0;
+            *sh2 = h;
+        }
+        __syncthreads();
+        if (half == 0 && !fail && row < args.n_q) {
+            const Top2 h = *sh2;
+            top2_merge(k1, k2, i1, h.k1, h.k2, h.i1);
+            Top2 r;
+            r.k1 = k1;
+            r.k2 = k2;
+            r.i1 = i1;
+            r.pad = 0;
+            static_cast<Top2*>(args.part)[(size_t)row * gridDim.y + blockIdx.y] = r;
+        }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -394,6 +502,202 @@ __global__ void k_match_merge(const Top2* __restrict__ part, int n, int nseg, fl
     best[i] = (k1 > -INFINITY) ? i1 : -1;
     pass[i] = ok;
     if (dist) dist[i] = d;
+}
+
+// ---- SIM_F16: the canonical similarity fp16(exact a.b) ----
+
+// The binary16 value nearest to x (ties to even) as a float, +0 for zero:
+// x is scaled by a power of two to the integer grid of its binade (exact),
+// rounded with rint (nearest, ties to even) and scaled back.
+__device__ __forceinline__ float f16_round_f64(double x) {
+    const double ax = fabs(x);
+    if (!(ax < 65520.0)) return x < 0.0 ? -INFINITY : INFINITY;  // 65520: the tie that rounds up to 2^16
+    int shift = 24;                                               // subnormal quantum 2^-24
+    if (ax >= 6.103515625e-05) {                                  // 2^-14: normal, quantum 2^(E - 10)
+        const int E = (int)((__double_as_longlong(ax) >> 52) & 0x7FF) - 1023;
+        shift = 10 - E;
+    }
+    const double up = __longlong_as_double((long long)(1023 + shift) << 52);
+    const double dn = __longlong_as_double((long long)(1023 - shift) << 52);
+    return (float)(rint(x * up) * dn) + 0.0f;
+}
+
+// Exact dot product of two fp16 rows of D elements (16-byte aligned): each
+// product is exact in fp32 (11-bit significands), and for rows of norm <= 1
+// every float64 partial sum is exact (a multiple of 2^-48 below 2^5).
+__device__ __forceinline__ double dot_f16_exact(const __half* a, const __half* b, int D) {
+    double acc = 0.0;
+    const uint4* pa = reinterpret_cast<const uint4*>(a);
+    const uint4* pb = reinterpret_cast<const uint4*>(b);
+    for (int c = 0; c < D / 8; ++c) {
+        const uint4 x = pa[c], y = pb[c];
+        const __half2* hx = reinterpret_cast<const __half2*>(&x);
+        const __half2* hy = reinterpret_cast<const __half2*>(&y);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const float2 fx = __half22float2(hx[q]), fy = __half22float2(hy[q]);
+            acc += (double)__fmul_rn(fx.x, fy.x);
+            acc += (double)__fmul_rn(fx.y, fy.y);
+        }
+    }
+    return acc;
+}
+
+// Largest row L2 norm of each of the two fp16 sets, rounded up with a
+// relative margin of 2^-20, as float bits (non-negative floats order as
+// their bits, so the integer atomicMax is the float max: the result does not
+// depend on the order of the updates).  One warp per row.
+__global__ void k_f16_max_norms(const __half* __restrict__ a, int n1, const __half* __restrict__ b, int n2, int D,
+                                unsigned* __restrict__ out) {
+    const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (w >= n1 + n2) return;
+    const __half* row = w < n1 ? a + (size_t)w * D : b + (size_t)(w - n1) * D;
+    double s = 0.0;
+    for (int k = lane; k < D; k += 32) {
+        const float f = __half2float(row[k]);
+        s += (double)__fmul_rn(f, f);
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL_MASK, s, o);
+    if (lane == 0) {
+        const float nrm = __double2float_ru(sqrt(s) * (1.0 + 0x1p-20));
+        atomicMax(&out[w < n1 ? 0 : 1], __float_as_uint(nrm));
+    }
+}
+
+__device__ __forceinline__ void finish_f16_row(int i, float f1, float f2, int c1, float ratio_sq, int* best, int* pass,
+                                               float* dist) {
+    // pysift/core.py:2676-2680 (float32); no second column: no pass
+    int ok = 0;
+    float d = 0.0f;
+    if (f2 > -INFINITY) {
+        float db = 2.0f - 2.0f * f1;
+        float ds = 2.0f - 2.0f * f2;
+        db = db < 0.0f ? 0.0f : db;
+        ds = ds < 0.0f ? 0.0f : ds;
+        ok = (ds > 1e-10f) && (db < ratio_sq * ds);
+        d = sqrtf(db);
+    }
+    best[i] = c1;
+    pass[i] = ok;
+    if (dist) dist[i] = d;
+}
+
+// Merge the segments of one SIM_F16 scan (Top3 parts, in segment order),
+// recompute the two candidates exactly and accept the row when no other
+// column can reach them: every other column's fp32 value is <= k3, so its
+// exact value is <= k3 + e and its fp16 similarity <= U = fp16(k3 + e); the
+// row is settled when U <= F2 and U < F1 (a column tying F1 could have a
+// lower index).  Unsettled rows are appended to `recheck` (their order there
+// does not matter: each row's result is computed on its own).
+__global__ void k_match_merge_f16(const Top3* __restrict__ part, int n, int nseg, float ratio_sq,
+                                  const __half* __restrict__ q, const __half* __restrict__ t, int n_t, int D,
+                                  const unsigned* __restrict__ maxnorm_t, const int* __restrict__ error,
+                                  int* __restrict__ best, int* __restrict__ pass, float* __restrict__ dist,
+                                  int* __restrict__ recheck, int* __restrict__ n_recheck) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Top3 a;
+    top3_init(a);
+    for (int s_ = 0; s_ < nseg; ++s_) top3_merge(a, part[(size_t)i * nseg + s_]);
+    // a scan that gave up on its MMA barrier left its parts unwritten: no
+    // result, and no candidate index is trusted
+    const bool i2_ok = a.k2 > -INFINITY && a.i2 >= 0 && a.i2 < n_t;
+    if (*error || a.i1 < 0 || a.i1 >= n_t || (a.k2 > -INFINITY && !i2_ok)) {
+        best[i] = -1;
+        pass[i] = 0;
+        if (dist) dist[i] = 0.0f;
+        return;
+    }
+    const __half* qi = q + (size_t)i * D;
+    float f1 = f16_round_f64(dot_f16_exact(qi, t + (size_t)a.i1 * D, D));
+    int c1 = a.i1;
+    float f2 = -INFINITY;
+    if (a.k2 > -INFINITY) {
+        f2 = f16_round_f64(dot_f16_exact(qi, t + (size_t)a.i2 * D, D));
+        if (f2 > f1 || (f2 == f1 && a.i2 < a.i1)) {
+            const float tf = f1;
+            f1 = f2;
+            f2 = tf;
+            c1 = a.i2;
+        }
+    }
+    if (a.k3 > -INFINITY) {
+        double nq = 0.0;
+        for (int k = 0; k < D; ++k) {
+            const float f = __half2float(qi[k]);
+            nq += (double)__fmul_rn(f, f);
+        }
+        const double e = (double)D * 0x1p-21 * (sqrt(nq) * (1.0 + 0x1p-20)) * (double)__uint_as_float(*maxnorm_t);
+        const float u = f16_round_f64((double)a.k3 + e);
+        if (!(u <= f2 && u < f1)) {
+            recheck[atomicAdd(n_recheck, 1)] = i;
+            return;
+        }
+    }
+    finish_f16_row(i, f1, f2, c1, ratio_sq, best, pass, dist);
+}
+
+// Rows the merge could not settle: the exact fp16 similarity against every
+// column, top-2 by (similarity desc, index asc).  One CTA per row (grid
+// stride over both directions' lists); keys pack the order-preserving bits
+// of the similarity above the complemented column index, so the integer
+// maximum is the best with the lowest index.
+__global__ void __launch_bounds__(256) k_match_recheck_f16(const int* __restrict__ list0, const int* __restrict__ list1,
+                                                           const int* __restrict__ counts, const __half* __restrict__ a,
+                                                           int n1, const __half* __restrict__ b, int n2, int D,
+                                                           float ratio_sq, int* __restrict__ fbest,
+                                                           int* __restrict__ fpass, float* __restrict__ fdist,
+                                                           int* __restrict__ bbest, int* __restrict__ bpass,
+                                                           float* __restrict__ bdist) {
+    __shared__ __align__(16) __half qrow[128];
+    __shared__ unsigned long long s_b[8], s_s[8];
+    const int c0 = counts[0], call = c0 + counts[1];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int v = blockIdx.x; v < call; v += gridDim.x) {
+        const bool fwd = v < c0;
+        const int i = fwd ? list0[v] : list1[v - c0];
+        const __half* t = fwd ? b : a;
+        const int nt = fwd ? n2 : n1;
+        if ((int)threadIdx.x < D) qrow[threadIdx.x] = (fwd ? a : b)[(size_t)i * D + threadIdx.x];
+        __syncthreads();
+        unsigned long long kb = 0, ks = 0;  // best and second keys; 0 = none
+        for (int j = threadIdx.x; j < nt; j += blockDim.x) {
+            const float f = f16_round_f64(dot_f16_exact(qrow, t + (size_t)j * D, D));
+            const unsigned u = __float_as_uint(f);
+            const unsigned ord = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+            const unsigned long long key = ((unsigned long long)ord << 32) | (0xFFFFFFFFu - (unsigned)j);
+            ks = max(ks, min(kb, key));
+            kb = max(kb, key);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long ob = __shfl_xor_sync(FULL_MASK, kb, o), os = __shfl_xor_sync(FULL_MASK, ks, o);
+            ks = max(max(ks, os), min(kb, ob));
+            kb = max(kb, ob);
+        }
+        if (lane == 0) {
+            s_b[warp] = kb;
+            s_s[warp] = ks;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+                ks = max(max(ks, s_s[w]), min(kb, s_b[w]));
+                kb = max(kb, s_b[w]);
+            }
+            auto val = [](unsigned long long k) {
+                const unsigned o = (unsigned)(k >> 32);
+                return __uint_as_float((o & 0x80000000u) ? (o & 0x7FFFFFFFu) : ~o);
+            };
+            const float f1 = val(kb);
+            const float f2 = ks ? val(ks) : -INFINITY;
+            const int c1 = (int)(0xFFFFFFFFu - (unsigned)(kb & 0xFFFFFFFFu));
+            if (fwd)
+                finish_f16_row(i, f1, f2, c1, ratio_sq, fbest, fpass, fdist);
+            else
+                finish_f16_row(i, f1, f2, c1, ratio_sq, bbest, bpass, bdist);
+        }
+        __syncthreads();
+    }
 }
 
 // Mutual matches in query order: fwd[i] = j passes, bwd[j] = i passes.
@@ -517,7 +821,10 @@ static int launch_scan_mode(int mode, const RowScanArgs& a, int D, int nseg, cud
 }
 
 struct MatchLayout {
-    size_t off_fpart, off_bpart, off_fbest, off_fpass, off_fdist, off_bbest, off_bpass, off_bdist, off_err;
+    // off_ctl: int[8] = error flag, SIM_F16 recheck counts (forward, backward),
+    // max row norms (set 1, set 2) as float bits
+    size_t off_fpart, off_bpart, off_fbest, off_fpass, off_fdist, off_bbest, off_bpass, off_bdist, off_ctl;
+    size_t off_rl0, off_rl1;
     size_t off_na, off_nb, off_bfa, off_bfb, off_qa, off_ta, off_qb, off_tb;
     size_t total;
 };
@@ -532,15 +839,21 @@ static MatchLayout match_layout(int n1, int n2, int D, int exact) {
         return r;
     };
     // segments never exceed the tiles of the other side
-    l.off_fpart = take((size_t)n1 * ceil_div(n2, NT) * sizeof(Top2));
-    l.off_bpart = take((size_t)n2 * ceil_div(n1, MT) * sizeof(Top2));
+    const size_t part_bytes = exact ? sizeof(Top2) : sizeof(Top3);
+    l.off_fpart = take((size_t)n1 * ceil_div(n2, NT) * part_bytes);
+    l.off_bpart = take((size_t)n2 * ceil_div(n1, MT) * part_bytes);
     l.off_fbest = take((size_t)n1 * 4);
     l.off_fpass = take((size_t)n1 * 4);
     l.off_fdist = take((size_t)n1 * 4);
     l.off_bbest = take((size_t)n2 * 4);
     l.off_bpass = take((size_t)n2 * 4);
     l.off_bdist = take((size_t)n2 * 4);
-    l.off_err = take(4);
+    l.off_ctl = take(8 * sizeof(int));
+    l.off_rl0 = l.off_rl1 = 0;
+    if (!exact) {
+        l.off_rl0 = take((size_t)n1 * 4);
+        l.off_rl1 = take((size_t)n2 * 4);
+    }
     l.off_na = l.off_nb = l.off_bfa = l.off_bfb = l.off_qa = l.off_ta = l.off_qb = l.off_tb = 0;
     if (exact) {
         l.off_na = take((size_t)n1 * 4);
@@ -572,8 +885,16 @@ static int run_match(int mode, const uint8_t* a_q, const uint8_t* a_t, int n1, c
                      const MatchLayout& l, void* ws, int* fbest_out, int* fpass_out, int* bbest_out, int* bpass_out,
                      int32_t* pairs, float* pdist, int32_t* count, cudaStream_t st, const float* sa = nullptr,
                      const float* sb = nullptr) {
-    int* err = wsp<int>(ws, l.off_err);
-    PYSIFT_CUDA_TRY(cudaMemsetAsync(err, 0, 4, st));
+    int* ctl = wsp<int>(ws, l.off_ctl);
+    int* err = ctl;
+    PYSIFT_CUDA_TRY(cudaMemsetAsync(ctl, 0, 8 * sizeof(int), st));
+    const __half* ha = reinterpret_cast<const __half*>(a_q);
+    const __half* hb = reinterpret_cast<const __half*>(b_q);
+    unsigned* maxnorm = reinterpret_cast<unsigned*>(ctl + 3);
+    if (mode == SIM_F16) {
+        k_f16_max_norms<<<ceil_div(n1 + n2, 8), 256, 0, st>>>(ha, n1, hb, n2, D, maxnorm);
+        PYSIFT_LAUNCH_CHECK("k_f16_max_norms");
+    }
     const bool sim = mode == SIM_F16 || mode == SIM_I8;
     const int* na = !sim ? wsp<int>(ws, l.off_na) : nullptr;
     const int* nb = !sim ? wsp<int>(ws, l.off_nb) : nullptr;
@@ -592,7 +913,7 @@ static int run_match(int mode, const uint8_t* a_q, const uint8_t* a_t, int n1, c
         s.norm_t = dir == 0 ? nb : na;
         s.scale_q = dir == 0 ? sa : sb;
         s.scale_t = dir == 0 ? sb : sa;
-        s.part = wsp<Top2>(ws, dir == 0 ? l.off_fpart : l.off_bpart);
+        s.part = wsp<void>(ws, dir == 0 ? l.off_fpart : l.off_bpart);
         s.error = err;
         int nseg;
         scan_split(s.n_q, s.n_t, nseg, s.seg_tiles);
@@ -602,13 +923,28 @@ static int run_match(int mode, const uint8_t* a_q, const uint8_t* a_t, int n1, c
         int* best = dir == 0 ? fbest : bbest;
         int* pass = dir == 0 ? fpass : bpass;
         float* dist = dir == 0 ? fdist : bdist;
-        if (sim)
-            k_match_merge<SIM_F16><<<ceil_div(s.n_q, 256), 256, 0, st>>>(s.part, s.n_q, nseg, ratio_sq, nq, best, pass,
-                                                                       dist);
-        else
-            k_match_merge<DIST_BF16><<<ceil_div(s.n_q, 256), 256, 0, st>>>(s.part, s.n_q, nseg, ratio_sq, nq, best,
-                                                                         pass, dist);
-        PYSIFT_LAUNCH_CHECK("k_match_merge");
+        if (mode == SIM_F16) {
+            k_match_merge_f16<<<ceil_div(s.n_q, 128), 128, 0, st>>>(
+                static_cast<const Top3*>(s.part), s.n_q, nseg, ratio_sq, dir == 0 ? ha : hb, dir == 0 ? hb : ha,
+                s.n_t, D, maxnorm + (dir == 0 ? 1 : 0), err, best, pass, dist,
+                wsp<int>(ws, dir == 0 ? l.off_rl0 : l.off_rl1), ctl + 1 + dir);
+            PYSIFT_LAUNCH_CHECK("k_match_merge_f16");
+        } else {
+            const Top2* part = static_cast<const Top2*>(s.part);
+            if (sim)
+                k_match_merge<SIM_F16><<<ceil_div(s.n_q, 256), 256, 0, st>>>(part, s.n_q, nseg, ratio_sq, nq, best,
+                                                                           pass, dist);
+            else
+                k_match_merge<DIST_BF16><<<ceil_div(s.n_q, 256), 256, 0, st>>>(part, s.n_q, nseg, ratio_sq, nq, best,
+                                                                             pass, dist);
+            PYSIFT_LAUNCH_CHECK("k_match_merge");
+        }
+    }
+    if (mode == SIM_F16) {
+        k_match_recheck_f16<<<2 * sm_count(), 256, 0, st>>>(wsp<int>(ws, l.off_rl0), wsp<int>(ws, l.off_rl1), ctl + 1,
+                                                             ha, n1, hb, n2, D, ratio_sq, fbest, fpass, fdist, bbest,
+                                                             bpass, bdist);
+        PYSIFT_LAUNCH_CHECK("k_match_recheck_f16");
     }
     k_match_mutual<<<1, 1024, 0, st>>>(fbest, fpass, fdist, bbest, bpass, n1, reinterpret_cast<int2*>(pairs), pdist,
                                        count);
@@ -648,6 +984,16 @@ int pysift_match_fp16(const uint16_t* d1, int32_t n1, const uint16_t* d2, int32_
     const uint8_t* b = reinterpret_cast<const uint8_t*>(d2);
     return run_match(SIM_F16, a, a, n1, b, b, n2, D, ratio_sq, l, workspace, fwd_best, fwd_pass, bwd_best, bwd_pass,
                      pairs, pair_dist, pair_count, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int pysift_match_fp16_recheck_counts(const void* workspace, int32_t n1, int32_t n2, int32_t D, int32_t* counts,
+                                     pysift_stream_t stream) {
+    PYSIFT_CHECK_ARG(workspace && counts, "NULL pointer argument");
+    PYSIFT_CHECK_ARG(n1 >= 1 && n2 >= 1 && (D == 64 || D == 128), "bad sizes (D must be 64 or 128)");
+    const MatchLayout l = match_layout(n1, n2, D, 0);
+    PYSIFT_CUDA_TRY(cudaMemcpyAsync(counts, static_cast<const char*>(workspace) + l.off_ctl + sizeof(int),
+                                    2 * sizeof(int), cudaMemcpyDeviceToDevice, reinterpret_cast<cudaStream_t>(stream)));
+    return PYSIFT_OK;
 }
 
 int pysift_match_u8_exact(const uint8_t* d1, int32_t n1, const uint8_t* d2, int32_t n2, int32_t D, float ratio,

@@ -39,27 +39,84 @@ def test_exact_u8_ties_go_to_lower_index():
     assert (out["fwd_best"][:100].cpu().numpy() == np.arange(100)).all()
 
 
-@pytest.mark.parametrize("n1,n2,D", [(700, 900, 64), (1200, 800, 128), (8000, 8000, 64)])
-def test_fp16_reference_mode(n1, n2, D):
-    import torch
-    from oracle import match_oracle as mo
-    from pysift_b200 import match
-    rng = np.random.default_rng(n1)
+def _unit_f16_sets(n1, n2, D, seed, dup=0):
+    """Gaussian rows, L2-normalised, half of the second set noisy copies of
+    the first; `dup` rows of the second set repeated exactly (fp16 ties)."""
+    rng = np.random.default_rng(seed)
     x = rng.standard_normal((n1, D)).astype(np.float32)
-    y = np.concatenate([x[: n2 // 2] + 0.05 * rng.standard_normal((n2 // 2, D)).astype(np.float32),
-                        rng.standard_normal((n2 - n2 // 2, D)).astype(np.float32)])
+    k = min(n1, n2 // 2)
+    y = np.concatenate([x[:k] + 0.05 * rng.standard_normal((k, D)).astype(np.float32),
+                        rng.standard_normal((n2 - k, D)).astype(np.float32)])
     x /= np.linalg.norm(x, axis=1, keepdims=True)
     y /= np.linalg.norm(y, axis=1, keepdims=True)
     xh, yh = x.astype(np.float16), y.astype(np.float16)
+    if dup:  # two exact copies of the first `dup` rows at the end
+        yh[n2 - 2 * dup:n2 - dup] = yh[:dup]
+        yh[n2 - dup:] = yh[:dup]
+    return xh, yh
+
+
+def _fp16_match_and_check(xh, yh):
+    import torch
+    from oracle import match_oracle as mo
+    from pysift_b200 import _lib, match
     out = match.match_fp16(torch.from_numpy(xh).cuda(), torch.from_numpy(yh).cuda())
     ref = mo.match_fp16(xh, yh)
-    fb = out["fwd_best"].cpu().numpy()
-    agree = np.mean(fb == ref["fwd_best"])
-    # disagreements can only come from fp16 rounding ties of the fp32 accumulation
-    assert agree >= 0.995, agree
+    for k in ("fwd_best", "fwd_pass", "bwd_best", "bwd_pass"):
+        assert np.array_equal(out[k].cpu().numpy(), ref[k]), k
     n = int(out["count"].item())
-    assert abs(n - len(ref["pairs"])) <= max(2, 0.005 * len(ref["pairs"]))
-    assert n > n2 // 4
+    assert np.array_equal(out["pairs"][:n].cpu().numpy(), ref["pairs"])
+    assert np.array_equal(out["dist"][:n].cpu().numpy(), ref["dist"])
+    # rows the candidate check could not settle went through the exact full-row pass
+    cnt = torch.zeros(2, dtype=torch.int32, device="cuda")
+    ws = out["workspace"]
+    off = (-ws.data_ptr()) % 256
+    _lib.check(_lib.load().pysift_match_fp16_recheck_counts(ws.data_ptr() + off, xh.shape[0], yh.shape[0],
+                                                            xh.shape[1], cnt.data_ptr(),
+                                                            torch.cuda.current_stream().cuda_stream), "counts")
+    return out, ref, cnt.cpu().numpy()
+
+
+@pytest.mark.parametrize("n1,n2,D", [(700, 900, 64), (1200, 800, 128), (8000, 8000, 64), (1, 300, 64),
+                                     (300, 1, 64), (2, 2, 64), (3, 700, 128), (5000, 16000, 64)])
+def test_fp16_reference_mode_bit_exact(n1, n2, D):
+    """The stitch matcher's fp16 mode equals the oracle's exact-then-round
+    similarity in every output: best indices and pass flags both ways, the
+    mutual pairs and their distances."""
+    xh, yh = _unit_f16_sets(n1, n2, D, seed=n1 + 7 * n2)
+    out, ref, rechecked = _fp16_match_and_check(xh, yh)
+    assert rechecked[0] <= n1 and rechecked[1] <= n2
+    if n1 >= 300 and n2 >= 300:
+        assert int(out["count"].item()) > min(n1, n2 // 2) // 2
+
+
+def test_fp16_reference_mode_ties_and_rechecks():
+    """Train rows 0..299 repeated twice at 900.. and 1200..: for a query whose
+    best is one of them, the best, second and third similarities are equal,
+    so the candidate check cannot settle the row and it is recomputed over
+    every column; the lowest index wins the tie."""
+    xh, yh = _unit_f16_sets(1500, 1500, 64, seed=11, dup=300)
+    out, ref, rechecked = _fp16_match_and_check(xh, yh)
+    fb = out["fwd_best"].cpu().numpy()
+    assert (fb[:300] < 900).all()  # the copies never beat their originals
+    assert rechecked[0] >= np.count_nonzero(fb[:300] == np.arange(300))
+
+
+def test_fp16_reference_mode_near_ties_of_the_rounding():
+    """Rows built so that the best and second similarities sit within an
+    fp32 accumulation error of an fp16 rounding boundary (two train rows that
+    differ in one low-order element), which a rounding of the fp32 tile
+    alone can order differently from the exact similarity."""
+    rng = np.random.default_rng(5)
+    xh, yh = _unit_f16_sets(600, 900, 64, seed=5)
+    yh = yh.copy()
+    # perturb one element of a copy of each of the first 300 train rows by one fp16 ulp
+    for r in range(300):
+        k = int(rng.integers(64))
+        v = yh[r].copy()
+        v[k] = np.nextafter(v[k], np.float16(np.inf) if rng.random() < 0.5 else np.float16(-np.inf))
+        yh[600 + r] = v
+    _fp16_match_and_check(xh, yh)
 
 
 @pytest.mark.parametrize("n1,n2,D", [(1000, 1000, 128), (300, 517, 128), (129, 1, 128), (2000, 1500, 64),
