@@ -206,7 +206,8 @@ class OracleStitch:
             out, _ = blend_oracle.blend_pair(warped, m1, canvas2, m2, self.n_blend_levels,
                                              color_match=self.color_match)
         pano = autocrop(out, m1 | m2)
-        return dict(pano=pano, H=H, mask=mask, info=info, pairs=pairs, p1=p1, p2=p2, n1=len(pts1), n2=len(pts2))
+        return dict(pano=pano, H=H, mask=mask, info=info, pairs=pairs, p1=p1, p2=p2, n1=len(pts1), n2=len(pts2),
+                    canvas=out, canvas_size=(cw, ch), ox=ox, oy=oy)
 
     def stitch3(self, img1, img2, img3):
         """_stitch_triple (pysift/core.py:3820-3966) without depth: matches 1-2

@@ -345,9 +345,12 @@ class GPUPyStitch:
         col_lo, col_hi = e[2 * ch:2 * ch + cw], e[2 * ch + cw:]
         r0, r1, c0, c1, ir0, ir1, ic0, ic1, degenerate = self._autocrop_box(row_lo, row_hi, col_lo, col_hi)
         if r0 is None:
+            c["crop_box"] = (0, 0, cw, ch)
             return out
         if degenerate:
+            c["crop_box"] = (c0, r0, c1 - c0 + 1, r1 - r0 + 1)
             return out[r0:r1 + 1, c0:c1 + 1]
+        c["crop_box"] = (c0 + ic0, r0 + ir0, ic1 - ic0 + 1, ir1 - ir0 + 1)
         return out[r0 + ir0:r0 + ir1 + 1, c0 + ic0:c0 + ic1 + 1]
 
     def _compose(self, img1, img2, H, max_canvas_px=400_000_000):
@@ -356,7 +359,7 @@ class GPUPyStitch:
         pano = self._to_host(self._compose_crop(c))
         self._last_compose = c
         return pano, dict(canvas_w=c["canvas_w"], canvas_h=c["canvas_h"], ox=c["ox"], oy=c["oy"],
-                          seam_rmse=self._seam_rmse_of(c))
+                          seam_rmse=self._seam_rmse_of(c), crop_box=c.get("crop_box"))
 
     @staticmethod
     def _seam_rmse_of(c):
@@ -455,7 +458,8 @@ class GPUPyStitch:
             pano, cm = self._compose(g1, g2, H)
             self._mark(5)
             timings['st5'] = time.perf_counter() - t0
-            metrics.update(canvas_w=cm['canvas_w'], canvas_h=cm['canvas_h'], seam_rmse=cm['seam_rmse'])
+            metrics.update(canvas_w=cm['canvas_w'], canvas_h=cm['canvas_h'], seam_rmse=cm['seam_rmse'],
+                           crop_box=cm['crop_box'])
         self._last = dict(H=H, mask=mask_d, pairs=m["pairs"][:n_m], kp1=kp1, kp2=kp2, p1=p1, p2=p2, info=info)
         return pano, timings, metrics
 

@@ -198,11 +198,13 @@ def test_stitch_multiband_end_to_end():
     st = GPUPyStitch(ransac_iters=2048, inlier_thresh=4.0, save_output=False, verbose=False)
     pano = st.stitch(img1, img2)
     orc = so.OracleStitch(ransac_iters=2048, inlier_thresh=4.0).stitch(img1, img2)
-    Hg = st._last["H"]
-    assert np.max(np.abs(Hg - orc["H"]) / np.maximum(np.abs(orc["H"]), 1e-6)) < 1e-3
-    if pano.shape == orc["pano"].shape:
-        diff = np.abs(pano.astype(int) - orc["pano"].astype(int))
-        assert np.mean(diff <= 1) > 0.98
+    assert np.array_equal(st._last["pairs"].cpu().numpy(), orc["pairs"])
+    assert np.array_equal(st._last["mask"].cpu().numpy().astype(bool), orc["mask"])
+    assert np.array_equal(st._last["H"], orc["H"])
+    c = st._last_compose
+    assert (c["canvas_w"], c["canvas_h"]) == orc["canvas_size"]
+    assert np.array_equal(c["out"].cpu().numpy(), orc["canvas"])
+    assert pano.shape == orc["pano"].shape and np.array_equal(pano, orc["pano"])
 
 
 TRIPLES = os.path.join(os.path.dirname(__file__), "golden", "triple_cases.npz")
