@@ -119,6 +119,19 @@ def test_starvation_retry(oracle_lib):
     _compare(out, ref)
 
 
+def test_candidate_cap_overflow(oracle_lib):
+    """An octave with more than 25,000 extrema (pysift/core.py:1395, 209-214):
+    the first 25,000 in (scale, row, column) order are refined, the overflow
+    is reported in the stats, and every output row equals the oracle's."""
+    img = synthetic.dense_texture(900, 1200, seed=6, sigma=1.0)
+    sift, out, ref = _run_both(img, oracle_lib)
+    assert ref["n_cands"][0] > 25000
+    st = sift.last_stats
+    assert st[6] >= 1
+    assert list(st[8:8 + len(ref["n_cands"])]) == list(ref["n_cands"])
+    _compare(out, ref)
+
+
 def test_keypoint_cap(oracle_lib):
     """More than 8000 refined keypoints -> top-8000 by response (pysift/core.py:2078-2080)."""
     img = synthetic.dense_texture(800, 1000, seed=5, sigma=2.0)
