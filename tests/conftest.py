@@ -8,6 +8,14 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 
+def reference_root():
+    """The reference checkout (SivaIITM/PySIFT) named by the PYSIFT_REFERENCE
+    environment variable, or None: the tests that read the reference's own
+    source or golden dumps are skipped without it."""
+    root = os.environ.get("PYSIFT_REFERENCE")
+    return root if root and os.path.isdir(root) else None
+
+
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
 

@@ -7,6 +7,7 @@ copy of one of them: the decoded grayscale source image (lossless PNG), all
 keypoint rows (points, angles, sizes) and every 16th descriptor row.
 
     python tests/golden/make_golden.py /path/to/reference
+    (or with the path in PYSIFT_REFERENCE)
 """
 import os
 import sys
@@ -32,4 +33,7 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PYSIFT_REFERENCE")
+    if not root:
+        sys.exit("usage: make_golden.py /path/to/reference (or set PYSIFT_REFERENCE)")
+    main(root)

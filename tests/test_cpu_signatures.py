@@ -3,15 +3,18 @@ PySIFT.__init__ (pysift/core.py:1184-1188), PySIFT.detectAndCompute
 (pysift/core.py:2021), GPUPyStitch.__init__ (pysift/core.py:2429-2445) and
 GPUPyStitch.stitch (pysift/core.py:3972) exists here, in the same position,
 with the same default.  The reference's signatures are read from its source
-with `ast` (nothing of it is imported or run); the test is skipped where the
-reference tree is absent.  Extra parameters here are keyword-only."""
+with `ast` (nothing of it is imported or run); the test is skipped unless
+PYSIFT_REFERENCE names the reference checkout.  Extra parameters here are
+keyword-only."""
 import ast
 import inspect
 import os
 
 import pytest
 
-REF_CORE = "/root/reference/pysift/core.py"
+from conftest import reference_root
+
+REF_CORE = os.path.join(reference_root() or "", "pysift", "core.py")
 
 
 def _ref_signature(cls_name, fn_name):
@@ -27,7 +30,7 @@ def _ref_signature(cls_name, fn_name):
     raise LookupError(f"{cls_name}.{fn_name}")
 
 
-@pytest.mark.skipif(not os.path.isfile(REF_CORE), reason="reference tree absent")
+@pytest.mark.skipif(not os.path.isfile(REF_CORE), reason="PYSIFT_REFERENCE unset or not a reference checkout")
 @pytest.mark.parametrize("cls_name,fn_name", [("PySIFT", "__init__"), ("PySIFT", "detectAndCompute"),
                                               ("GPUPyStitch", "__init__"), ("GPUPyStitch", "stitch")])
 def test_signature_matches_reference(cls_name, fn_name):

@@ -14,7 +14,7 @@ cosine >= 0.999, and the keypoint counts agree within 0.5 %.  The
 remaining differences come from the reference's fast-math refinement and
 atomic-order float sums.  The compact committed copy of one dump
 (tests/golden/, made by tests/golden/make_golden.py) always runs; the full
-dumps run when the reference tree is available.
+dumps run when PYSIFT_REFERENCE names the reference checkout.
 """
 import json
 import os
@@ -22,8 +22,10 @@ import os
 import numpy as np
 import pytest
 
+from conftest import reference_root
+
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = "/root/reference"
+REF = reference_root() or os.path.join(HERE, "_no_reference_checkout")
 
 IMC_IMAGES = {
     "imc_british_museum": "british_museum/set_100/images/00350405_2611802704.jpg",
@@ -90,7 +92,7 @@ def test_pin_committed_fixture(oracle_lib):
     assert cos > 0.9999
 
 
-@pytest.mark.skipif(not os.path.isdir(os.path.join(REF, "determinism_reference")), reason="reference tree absent")
+@pytest.mark.skipif(not os.path.isdir(os.path.join(REF, "determinism_reference")), reason="PYSIFT_REFERENCE unset")
 @pytest.mark.parametrize("name", sorted(IMC_IMAGES))
 def test_pin_reference_dumps(name, oracle_lib):
     import cv2
@@ -126,7 +128,7 @@ def test_blend_oracle_matches_reference_composition(faithful):
             assert d.max() <= 1 and (d > 0).mean() < 1e-3, (name, int((d > 0).sum()))
 
 
-@pytest.mark.skipif(not os.path.isfile(os.path.join(REF, "pysift", "core.py")), reason="reference tree absent")
+@pytest.mark.skipif(not os.path.isfile(os.path.join(REF, "pysift", "core.py")), reason="PYSIFT_REFERENCE unset")
 def test_blend_fixture_regenerates():
     """The committed composition fixtures (two- and three-image) are what the
     reference produces now."""
