@@ -5,11 +5,12 @@ pysift_zoom2x_u8_noalloc serves callers that cannot allocate device memory
 where they call the library (for instance a plugin running inside a host
 application that owns the whole device heap): its scratch is a fixed
 file-scope device array instead of a caller buffer.  This test calls both
-entry points through the C ABI on two different images in a row (the
-second call must not see anything left behind by the first) and requires
-bit-identical outputs, the same bar as the other GPU parity tests.  It also
-checks that an input larger than the fixed scratch is refused.  The file is
-named so that pytest collects it last.
+entry points through the C ABI on images in a row, the larger first, so
+that a later, smaller call would read anything the earlier one left behind
+past its own pixels, and requires bit-identical outputs, the same bar as the
+other GPU parity tests.  It runs the largest accepted input (exactly the
+scratch's 2^20 pixels) and checks that one row more is refused.  The file
+is named so that pytest collects it last.
 """
 import ctypes
 
@@ -42,11 +43,26 @@ def test_noalloc_zoom_matches_caller_scratch_twice():
     from pysift_b200 import synthetic
     lib = _lib.load()
     dev = torch.device("cuda", 0)
-    imgs = [synthetic.scene(300, 400, seed=21), synthetic.scene(480, 640, seed=22)]
+    # larger first: a stale read past the smaller call's H*W would show
+    imgs = [synthetic.scene(480, 640, seed=22), synthetic.scene(300, 400, seed=21),
+            synthetic.scene(37, 53, seed=23)]
     for img in imgs:
         ref, out = _zoom_both(lib, img, dev)
         assert np.array_equal(ref, out)
         assert np.isfinite(out).all() and out.max() > 0.0
+
+
+def test_noalloc_zoom_largest_accepted_input():
+    """1024 x 1024 = 2^20 pixels, the whole fixed scratch, twice in a row."""
+    import torch
+    from pysift_b200 import _lib
+    from pysift_b200 import synthetic
+    lib = _lib.load()
+    dev = torch.device("cuda", 0)
+    assert 1024 * 1024 == _lib.ZOOM2X_NOALLOC_MAX_PIXELS
+    for seed in (24, 25):
+        ref, out = _zoom_both(lib, synthetic.scene(1024, 1024, seed=seed), dev)
+        assert np.array_equal(ref, out)
 
 
 def test_noalloc_zoom_rejects_oversized_input():
