@@ -112,7 +112,7 @@ class ClockSampler:
                 self.reasons |= nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
             except Exception:
                 pass
-            time.sleep(0.1)
+            time.sleep(0.025)
 
     def __enter__(self):
         if self._nv is not None:
@@ -163,12 +163,15 @@ def cpu_detect_baseline(img, budget_s=15.0):
     return med, len(times)
 
 
-def opencv_detect_baseline(img, runs=5):
+def opencv_detect_baseline(img, threads=None, runs=5):
+    """OpenCV's SIFT on the host cores, the reference's own CPU comparison
+    (examples/quick_test.py:71-80): cv2.SIFT_create() with its defaults,
+    detectAndCompute(img, None), median of `runs` after one warm-up call."""
     try:
         import cv2
     except Exception:
         return None
-    cv2.setNumThreads(os.cpu_count() or 1)
+    cv2.setNumThreads(threads or os.cpu_count() or 1)
     s = cv2.SIFT_create()
     s.detectAndCompute(img, None)
     t = []
@@ -176,7 +179,78 @@ def opencv_detect_baseline(img, runs=5):
         t0 = time.perf_counter()
         kps, _ = s.detectAndCompute(img, None)
         t.append(time.perf_counter() - t0)
+    cv2.setNumThreads(os.cpu_count() or 1)
     return float(np.median(t)), len(kps)
+
+
+def opencv_stitch_once(img1, img2, ratio=0.75, thresh=4.0):
+    """The two-image stitch with OpenCV on the host: SIFT on both gray views,
+    BFMatcher(NORM_L2).knnMatch(k=2) with the ratio test,
+    findHomography(USAC_MAGSAC, 4 px), warpPerspective of view 1 onto the
+    canvas that holds both views, and a linear feather (each view weighted by
+    its distance to its own border where both cover a pixel)."""
+    import cv2
+    sift = cv2.SIFT_create()
+    k1, d1 = sift.detectAndCompute(cv2.cvtColor(img1, cv2.COLOR_BGR2GRAY), None)
+    k2, d2 = sift.detectAndCompute(cv2.cvtColor(img2, cv2.COLOR_BGR2GRAY), None)
+    knn = cv2.BFMatcher(cv2.NORM_L2).knnMatch(d1, d2, k=2)
+    good = [p[0] for p in knn if len(p) == 2 and p[0].distance < ratio * p[1].distance]
+    src = np.float32([k1[m.queryIdx].pt for m in good]).reshape(-1, 1, 2)
+    dst = np.float32([k2[m.trainIdx].pt for m in good]).reshape(-1, 1, 2)
+    H, inl = cv2.findHomography(src, dst, cv2.USAC_MAGSAC, thresh)
+    h1, w1 = img1.shape[:2]
+    h2, w2 = img2.shape[:2]
+    c = cv2.perspectiveTransform(np.float32([[0, 0], [w1, 0], [w1, h1], [0, h1]]).reshape(-1, 1, 2), H).reshape(-1, 2)
+    xs = np.concatenate([c[:, 0], [0, w2]])
+    ys = np.concatenate([c[:, 1], [0, h2]])
+    ox, oy = max(0.0, -xs.min()), max(0.0, -ys.min())
+    cw, ch = int(np.ceil(xs.max() + ox)) + 1, int(np.ceil(ys.max() + oy)) + 1
+    T = np.array([[1, 0, ox], [0, 1, oy], [0, 0, 1]], np.float64)
+    warped = cv2.warpPerspective(img1, T @ H, (cw, ch))
+    wmask = cv2.warpPerspective(np.full((h1, w1), 255, np.uint8), T @ H, (cw, ch), flags=cv2.INTER_NEAREST)
+    canvas2 = np.zeros((ch, cw, 3), np.uint8)
+    m2 = np.zeros((ch, cw), np.uint8)
+    iox, ioy = int(round(ox)), int(round(oy))
+    ye, xe = min(ioy + h2, ch), min(iox + w2, cw)
+    canvas2[ioy:ye, iox:xe] = img2[:ye - ioy, :xe - iox]
+    m2[ioy:ye, iox:xe] = 255
+    f1 = cv2.distanceTransform(wmask, cv2.DIST_L2, 3)
+    f2 = cv2.distanceTransform(m2, cv2.DIST_L2, 3)
+    wsum = f1 + f2
+    wsum[wsum == 0] = 1.0
+    pano = (warped * (f1 / wsum)[..., None] + canvas2 * (f2 / wsum)[..., None]).clip(0, 255).astype(np.uint8)
+    return pano, len(good), int(inl.sum()) if inl is not None else 0
+
+
+def opencv_stitch_baseline(img1, img2, threads, runs=3):
+    """Median time of opencv_stitch_once over `runs` after one warm-up, with
+    OpenCV limited to `threads` threads."""
+    try:
+        import cv2
+    except Exception:
+        return None
+    cv2.setNumThreads(threads)
+    opencv_stitch_once(img1, img2)
+    t = []
+    for _ in range(runs):
+        t0 = time.perf_counter()
+        _, n_good, n_inl = opencv_stitch_once(img1, img2)
+        t.append(time.perf_counter() - t0)
+    cv2.setNumThreads(os.cpu_count() or 1)
+    return float(np.median(t)), n_good, n_inl
+
+
+def opencv_baselines(kind, *imgs, scale=1.0):
+    """OpenCV at one thread and at every host thread: {threads_1, threads_all}
+    in units per second (scale / median seconds)."""
+    n = os.cpu_count() or 1
+    out = {"cores": n, "kind": "opencv " + __import__("cv2").__version__}
+    for key, th in (("threads_1", 1), ("threads_all", n)):
+        r = opencv_detect_baseline(imgs[0], threads=th) if kind == "detect" else opencv_stitch_baseline(*imgs, th)
+        out[key] = None if r is None else scale / r[0]
+        if r is not None and kind == "stitch":
+            out["matches_inliers"] = [r[1], r[2]]
+    return out
 
 
 def dist_setup():
@@ -302,7 +376,7 @@ def run_match(args, wl, world, rank, local):
     e2e_t = torch.tensor([float(np.sum(e2e_ms))], dtype=torch.float64, device=dev)
     all_ranks_max(e2e_t, world)
     if rank != 0:
-        return 0
+        return None
     step_s = total_ms / args.steps / 1e3
     flops = 2.0 * N * M * D
     peak, peak_kind = measured_tensor_peak()
@@ -341,8 +415,7 @@ def run_match(args, wl, world, rank, local):
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 def run_reference_pairs(args, wl):
@@ -495,7 +568,7 @@ def run_batch_detect(args, wl, world, rank, local):
     e2e_t = torch.tensor([float(np.sum(e2e_ms))], dtype=torch.float64, device=dev)
     all_ranks_max(e2e_t, world)
     if rank != 0:
-        return 0
+        return None
     n_kp = int(sum(r[0].shape[0] for r in res))
     out_bytes = int(sum(r[0].nbytes + r[1].nbytes for r in res))
     step_s = total_ms / args.steps / 1e3
@@ -534,8 +607,7 @@ def run_batch_detect(args, wl, world, rank, local):
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 def _gen_pairs(n, seed):
@@ -608,7 +680,7 @@ def run_batch_stitch(args, wl, world, rank, local, pairs):
     e2e_t = torch.tensor([float(np.sum(e2e_ms))], dtype=torch.float64, device=dev)
     all_ranks_max(e2e_t, world)
     if rank != 0:
-        return 0
+        return None
     P = len(pairs)
     step_s = total_ms / args.steps / 1e3
     peak, peak_kind = measured_peaks()
@@ -648,8 +720,7 @@ def run_batch_stitch(args, wl, world, rank, local, pairs):
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 def run_grad(args, wl, world, rank, local):
@@ -719,7 +790,7 @@ def run_grad(args, wl, world, rank, local):
             tot += np.array(step())
     launches = lib.pysift_launch_count() - launches0
     if rank != 0:
-        return 0
+        return None
     df, db, wf, wb = (tot / args.steps).tolist()
     step_ms = df + db + wf + wb
     line = {
@@ -738,8 +809,7 @@ def run_grad(args, wl, world, rank, local):
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 def run_reference_stitch(args, wl):
@@ -850,7 +920,7 @@ def run_detect(args, wl, world, rank, local):
     all_ranks_max(e2e_tot, world)
 
     if rank != 0:
-        return 0
+        return None
     mpix = H * W / 1e6
     value = world * args.steps * mpix / (total_ms / 1e3)
     e2e_value = world * args.steps * mpix / (float(e2e_tot.item()) / 1e3)
@@ -862,7 +932,7 @@ def run_detect(args, wl, world, rank, local):
         cpu_med, cpu_n, ocv = float("nan"), 0, None
     else:
         cpu_med, cpu_n = cpu_detect_baseline(img)
-        ocv = opencv_detect_baseline(img)
+        ocv = opencv_baselines("detect", img, scale=mpix)
     line = {
         "metric": METRIC, "value": value, "unit": "Mpix/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -884,10 +954,10 @@ def run_detect(args, wl, world, rank, local):
                          total=round(float(np.mean(step_ms)), 4)),
     }
     if ocv:
-        line["opencv_cpu"] = {"value": mpix / ocv[0], "unit": "Mpix/s", "cores": os.cpu_count(),
-                              "keypoints": ocv[1]}
-    print(json.dumps(line), flush=True)
-    return 0
+        ocv.update(unit="Mpix/s", sample="cv2.SIFT_create().detectAndCompute(img, None) on the same image, "
+                   "median of 5 after a warm-up (the reference's examples/quick_test.py:71-80)")
+        line["opencv_cpu"] = ocv
+    return line
 
 
 def cpu_stitch_baseline(img1, img2, wl, budget_s=20.0):
@@ -977,7 +1047,7 @@ def run_stitch(args, wl, world, rank, local):
         ev[6].synchronize()
         pyr_ms.append(ev[0].elapsed_time(ev[3]))
     if rank != 0:
-        return 0
+        return None
     pairs_s = world * args.steps / (total_ms / 1e3)
     e2e_pairs_s = world * args.steps / (float(e2e_tot.item()) / 1e3)
     peak, peak_kind = measured_peaks()
@@ -985,9 +1055,10 @@ def run_stitch(args, wl, world, rank, local):
     pyr_s = float(np.median(pyr_ms)) / 1e3
     achieved = alg / pyr_s / 1e9
     if args.no_cpu_baseline:
-        cpu_s, cpu_n = float("nan"), 0
+        cpu_s, cpu_n, ocv = float("nan"), 0, None
     else:
         cpu_s, cpu_n = cpu_stitch_baseline(img1, img2, wl)
+        ocv = opencv_baselines("stitch", img1, img2)
     mpix = 2 * H * W / 1e6
     line = {
         "metric": METRIC, "value": pairs_s, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
@@ -999,6 +1070,7 @@ def run_stitch(args, wl, world, rank, local):
                    if st.blend == "multiband" else "linear feather",
                    "keypoints": [m["kp1"], m["kp2"]], "matches": m["matches"],
                    "inliers": m["inliers"], "canvas": [m["canvas_w"], m["canvas_h"]],
+                   "crop_xywh": list(m["crop_box"]) if m.get("crop_box") else None,
                    "l2": "flushed (256 MiB write) before every step", "parallelism": f"replicas{world}"},
         "mpix_per_s": pairs_s * mpix,
         "roofline": {"bound": "hbm", "kernel": "pyramid+DoG+extrema of one 1280x960 view (k_blur x%d + "
@@ -1015,18 +1087,66 @@ def run_stitch(args, wl, world, rank, local):
         "clocks": clk.summary(),
         "stage_ms": stage_ms,
     }
-    print(json.dumps(line), flush=True)
-    return 0
+    if ocv:
+        ocv.update(unit="pairs/s", sample="3 stitches of the same pair after a warm-up: cv2 SIFT on both gray "
+                   "views, BFMatcher(NORM_L2).knnMatch(k=2) + ratio 0.75, findHomography(USAC_MAGSAC, 4 px), "
+                   "warpPerspective, linear feather")
+        line["opencv_cpu"] = ocv
+    return line
+
+
+EXTRA_WORKLOADS = (("detect_640x480", None), ("match_u8_8192", None), ("batch96_detect", 3),
+                   ("batch32_stitch", 2))
+
+
+def run_extras(args, world, rank, local):
+    """The other configurations of the metric, measured after the default
+    stitch line on every rank (each takes the same collective steps there):
+    plain detection of one 640x480 image (Mpix/s), exact 8192 x 8192 matching
+    through the bf16 tensor-core GEMM (match-pairs/s, tensor roofline), and
+    the batched forms against their plain per-image / per-pair loops.
+    Returns {workload: summary} on rank 0, None elsewhere."""
+    out = {}
+    for name, steps in EXTRA_WORKLOADS:
+        wl = WORKLOADS[name]
+        sub = argparse.Namespace(**vars(args))
+        sub.workload = name
+        if steps is not None:
+            sub.steps, sub.warmup = min(args.steps, steps), 3
+        if wl["kind"] == "detect":
+            line = run_detect(sub, wl, world, rank, local)
+        elif wl["kind"] == "match":
+            line = run_match(sub, wl, world, rank, local)
+        elif wl["kind"] == "batch_detect":
+            line = run_batch_detect(sub, wl, world, rank, local)
+        else:
+            line = run_batch_stitch(sub, wl, world, rank, local, _gen_pairs(wl["n"], wl["seed"] + rank))
+        if line is None:
+            continue
+        keep = {k: line.get(k) for k in ("value", "unit", "ms_per_step", "steps", "dtype", "roofline",
+                                           "cpu_baseline", "opencv_cpu", "e2e", "gpu_launches", "clocks")}
+        keep["config"] = line["config"]
+        if wl["kind"] == "batch_detect":
+            keep["plain_mpix_per_s"] = line["plain_mpix_per_s"]
+            keep["graph_mpix_per_s"] = line["graph_mpix_per_s"]
+            keep["batched_over_plain"] = line["value"] / line["plain_mpix_per_s"]
+        if wl["kind"] == "batch_stitch":
+            keep["plain_pairs_per_s"] = line["plain_pairs_per_s"]
+            keep["batched_over_plain"] = line["value"] / line["plain_pairs_per_s"]
+        out[name] = keep
+    return out if rank == 0 else None
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU baseline legs (profiling runs)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="default workload only: skip the other configurations embedded in its line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup()
@@ -1041,16 +1161,24 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
         if wl["kind"] == "stitch":
-            return run_stitch(args, wl, world, rank, local)
-        if wl["kind"] == "match":
-            return run_match(args, wl, world, rank, local)
-        if wl["kind"] == "batch_detect":
-            return run_batch_detect(args, wl, world, rank, local)
-        if wl["kind"] == "batch_stitch":
-            return run_batch_stitch(args, wl, world, rank, local, pairs)
-        if wl["kind"] == "grad":
-            return run_grad(args, wl, world, rank, local)
-        return run_detect(args, wl, world, rank, local)
+            line = run_stitch(args, wl, world, rank, local)
+            if args.workload == DEFAULT_WORKLOAD and not args.no_extras:
+                extras = run_extras(args, world, rank, local)
+                if line is not None:
+                    line["workloads"] = extras
+        elif wl["kind"] == "match":
+            line = run_match(args, wl, world, rank, local)
+        elif wl["kind"] == "batch_detect":
+            line = run_batch_detect(args, wl, world, rank, local)
+        elif wl["kind"] == "batch_stitch":
+            line = run_batch_stitch(args, wl, world, rank, local, pairs)
+        elif wl["kind"] == "grad":
+            line = run_grad(args, wl, world, rank, local)
+        else:
+            line = run_detect(args, wl, world, rank, local)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return 0
     finally:
         if world > 1:
             import torch.distributed as dist
