@@ -23,6 +23,7 @@
 //                        and the output-limit order, exactly, through buckets
 //   k_descriptor         4x4x8 descriptor (+DSP) + L2/clip/L2 + RootSIFT, written at its
 //                        output row (pysift/core.py:693-997, 1870-1873)
+#include <algorithm>
 #include <cstdarg>
 #include <cstring>
 #include <atomic>
@@ -768,8 +769,8 @@ struct BlurTile {
 // dst[0..7]: 4 output pairs, one packed fma per pair and tap, taps in
 // ascending order.  Pairs at even offsets are loaded as 8-byte words; the
 // pairs at odd offsets are formed from their neighbours.
-template <int R>
-__device__ __forceinline__ void blur_row_strip(const float* src, float* dst, const unsigned long long* w2) {
+template <int R, typename WF>
+__device__ __forceinline__ void blur_row_strip(const float* src, float* dst, const WF& w2) {
     constexpr int NP = 4 + R;
     unsigned long long E[NP], O[NP - 1];
 #pragma unroll
@@ -779,7 +780,7 @@ __device__ __forceinline__ void blur_row_strip(const float* src, float* dst, con
     unsigned long long A[4] = {0ull, 0ull, 0ull, 0ull};
 #pragma unroll
     for (int k = 0; k <= 2 * R; ++k) {
-        const unsigned long long wk = w2[k];
+        const unsigned long long wk = w2(k);
 #pragma unroll
         for (int p = 0; p < 4; ++p) A[p] = ffma2((k & 1) ? O[p + (k >> 1)] : E[p + (k >> 1)], wk, A[p]);
     }
@@ -787,25 +788,40 @@ __device__ __forceinline__ void blur_row_strip(const float* src, float* dst, con
     for (int p = 0; p < 4; ++p) reinterpret_cast<unsigned long long*>(dst)[p] = A[p];
 }
 
-// Fused H+V separable blur of one 64x32 output tile.  The tile and its
-// reflected halo are filled with cp.async (every load in flight at once;
-// reflection computed once per row and once per column).  Row pass: a lane
-// per tile row (the rows past the first 32 packed densely onto the first
-// warps), 8 outputs per lane.  Column pass: each thread filters a pair of
-// adjacent columns over 4 rows.  Both passes use packed fma pairs; each
-// output is the same fmaf chain over the taps in ascending order.
-template <int R, int TH>
-__global__ void __launch_bounds__(BLUR_NT, TH == 40 ? 7 : 1) k_blur(const BlurArgs a) {
+// The source, destination and geometry of one blurred level, as a tile of
+// it sees them (the fields of BlurArgs without the weights).
+struct TileIO {
+    const float* in;
+    long long in_pitch;
+    int step;
+    float* out;
+    float* out_r;
+    float* copy0;
+    float* copy0_r;
+    int out_pitch;
+    int H, W;
+};
+
+// Fused H+V separable blur of one 64 x TH output tile (tile column bx, tile
+// row by).  The tile and its reflected halo are filled with cp.async (every
+// load in flight at once; reflection computed once per row and once per
+// column).  Row pass: a lane per tile row (the rows past the first 32 packed
+// densely onto the first warps), 8 outputs per lane.  Column pass: each
+// thread filters a pair of adjacent columns over TH / 8 rows.  Both passes
+// use packed fma pairs; each output is the same fmaf chain over the taps in
+// ascending order.  w2(k) is tap k's weight packed twice.  The caller
+// synchronises the block before smem is reused.
+template <int R, int TH, typename WF>
+__device__ __forceinline__ void blur_tile(const TileIO& a, int bx, int by, float* smem, const WF& w2) {
     using T = BlurTile<R, TH>;
     constexpr int TW = BLUR_TW, ROWS = T::ROWS, TWR = T::TWR, TS = T::TS, HS = T::HS;
     constexpr int RP = TH / 8;  // column-pass rows per thread
     constexpr int CQ = (TWR + 31) / 32;
     static_assert(BLUR_NT / 32 == TW / 8, "one warp per 8-column strip in the row pass");
     static_assert(TH % 8 == 0 && BLUR_NT == (TW / 2) * 8, "one thread per column pair and TH / 8 rows in the column pass");
-    extern __shared__ __align__(16) float smem[];
     float* tile = smem;
     float* hb = smem + ROWS * TS;
-    const int c0 = blockIdx.x * TW, r0 = blockIdx.y * TH;  // TH: the template tile height
+    const int c0 = bx * TW, r0 = by * TH;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     {
         long long gcs[CQ];
@@ -841,12 +857,12 @@ __global__ void __launch_bounds__(BLUR_NT, TH == 40 ? 7 : 1) k_blur(const BlurAr
 #pragma unroll
         for (int round = 0; round < NF; ++round) {
             const int rr = round * 32 + lane;
-            blur_row_strip<R>(tile + rr * TS + warp * 8, hb + rr * HS + warp * 8, a.w2);
+            blur_row_strip<R>(tile + rr * TS + warp * 8, hb + rr * HS + warp * 8, w2);
         }
         if constexpr (N2 > 0) {
             if (threadIdx.x < N2 * 8) {
                 const int rr = NF * 32 + threadIdx.x % N2, x0 = (threadIdx.x / N2) * 8;
-                blur_row_strip<R>(tile + rr * TS + x0, hb + rr * HS + x0, a.w2);
+                blur_row_strip<R>(tile + rr * TS + x0, hb + rr * HS + x0, w2);
             }
         }
     }
@@ -862,7 +878,7 @@ __global__ void __launch_bounds__(BLUR_NT, TH == 40 ? 7 : 1) k_blur(const BlurAr
         for (int j = 0; j < RP; ++j) A[j] = 0ull;
 #pragma unroll
         for (int k = 0; k <= 2 * R; ++k) {
-            const unsigned long long wk = a.w2[k];
+            const unsigned long long wk = w2(k);
 #pragma unroll
             for (int j = 0; j < RP; ++j) A[j] = ffma2(V[j + k], wk, A[j]);
         }
@@ -887,6 +903,151 @@ __global__ void __launch_bounds__(BLUR_NT, TH == 40 ? 7 : 1) k_blur(const BlurAr
             }
         }
     }
+}
+
+// Interior tiles: the window [r0-R, r0+TH+R) x [c0-RA, c0+64+RA) (RA = R
+// rounded up to 4) lies inside the level, the source is read with stride 1
+// from 16-byte aligned rows and no copy of the input is stored.  Then the
+// fill is one 16-byte cp.async per 4 floats, a warp per row, with no
+// reflection; the row stride TSF = 4 (mod 8) lets the lane-per-row row pass
+// read 16-byte words without bank conflicts; the stores need no bounds
+// checks.  Same arithmetic as blur_tile, so the same results.
+template <int R>
+struct BlurFast {
+    static constexpr int RA = (R + 3) / 4 * 4;
+    static constexpr int D = RA - R;                          // first needed column of a strip, within its quad
+    static constexpr int TWF = BLUR_TW + 2 * RA;              // floats per tile row
+    static constexpr int TSF = (TWF % 8 == 4) ? TWF : TWF + 4;  // row stride = 4 (mod 8)
+    static constexpr int NQ = (D + 8 + 2 * R + 3) / 4;        // 16-byte words a strip reads
+    static_assert(TWF / 4 <= 32, "one warp fills a tile row");
+};
+
+template <int R, int TH>
+__host__ __device__ constexpr size_t blur_fast_bytes() {
+    return (size_t)((TH + 2 * R) * BlurFast<R>::TSF + (TH + 2 * R) * (BLUR_TW + 2)) * sizeof(float);
+}
+
+__device__ __forceinline__ void cp_async16(float* dst, const float* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+
+__device__ __forceinline__ bool blur_tile_is_fast(const TileIO& a, int R, int RA, int TH, int bx, int by) {
+    const int c0 = bx * BLUR_TW, r0 = by * TH;
+    return a.step == 1 && !a.copy0 && r0 - R >= 0 && r0 + TH + R <= a.H && c0 - RA >= 0 &&
+           c0 + BLUR_TW + RA <= a.W && (a.in_pitch & 3) == 0 && (reinterpret_cast<uintptr_t>(a.in) & 15) == 0 &&
+           (a.out_pitch & 1) == 0 && (reinterpret_cast<uintptr_t>(a.out) & 7) == 0 &&
+           (reinterpret_cast<uintptr_t>(a.out_r) & 7) == 0;
+}
+
+// Row filter of one strip from 16-byte words q[0..NQ): output pair p, tap k
+// reads floats D + 2p + k and D + 2p + k + 1 of the strip's words.
+template <int R, typename WF>
+__device__ __forceinline__ void blur_row_strip_q(const float* src, float* dst, const WF& w2) {
+    using F = BlurFast<R>;
+    constexpr int NF = 4 * F::NQ;
+    float v[NF];
+#pragma unroll
+    for (int i = 0; i < F::NQ; ++i) {
+        const float4 t = reinterpret_cast<const float4*>(src)[i];
+        v[4 * i] = t.x;
+        v[4 * i + 1] = t.y;
+        v[4 * i + 2] = t.z;
+        v[4 * i + 3] = t.w;
+    }
+    unsigned long long A[4] = {0ull, 0ull, 0ull, 0ull};
+#pragma unroll
+    for (int k = 0; k <= 2 * R; ++k) {
+        const unsigned long long wk = w2(k);
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            const int e = F::D + 2 * p + k;
+            A[p] = ffma2(pack2(v[e], v[e + 1]), wk, A[p]);
+        }
+    }
+#pragma unroll
+    for (int p = 0; p < 4; ++p) reinterpret_cast<unsigned long long*>(dst)[p] = A[p];
+}
+
+template <int R, int TH, typename WF>
+__device__ __forceinline__ void blur_tile_fast(const TileIO& a, int bx, int by, float* smem, const WF& w2) {
+    using F = BlurFast<R>;
+    constexpr int TW = BLUR_TW, ROWS = TH + 2 * R, TSF = F::TSF, HS = BLUR_TW + 2;
+    constexpr int RP = TH / 8;
+    float* tile = smem;
+    float* hb = smem + ROWS * TSF;
+    const int c0 = bx * TW, r0 = by * TH;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    {
+        const bool act = lane < F::TWF / 4;
+        const float* src = a.in + (long long)(r0 - R + warp) * a.in_pitch + (c0 - F::RA) + 4 * lane;
+        float* dst = tile + warp * TSF + 4 * lane;
+        const long long gstep = 8 * a.in_pitch;
+        for (int rr = warp; rr < ROWS; rr += BLUR_NT / 32) {
+            if (act) cp_async16(dst, src);
+            src += gstep;
+            dst += 8 * TSF;
+        }
+        asm volatile("cp.async.wait_all;" ::: "memory");
+    }
+    __syncthreads();
+    {
+        constexpr int NR = ROWS / 32, N2 = ROWS % 32;
+#pragma unroll
+        for (int round = 0; round < NR; ++round) {
+            const int rr = round * 32 + lane;
+            blur_row_strip_q<R>(tile + rr * TSF + warp * 8, hb + rr * HS + warp * 8, w2);
+        }
+        if constexpr (N2 > 0) {
+            if (threadIdx.x < N2 * 8) {
+                const int rr = NR * 32 + threadIdx.x % N2, x0 = (threadIdx.x / N2) * 8;
+                blur_row_strip_q<R>(tile + rr * TSF + x0, hb + rr * HS + x0, w2);
+            }
+        }
+    }
+    __syncthreads();
+    {
+        const int cp = lane, y0 = warp * RP;
+        constexpr int NV = RP + 2 * R;
+        unsigned long long V[NV];
+#pragma unroll
+        for (int m = 0; m < NV; ++m) V[m] = reinterpret_cast<const unsigned long long*>(hb + (y0 + m) * HS)[cp];
+        unsigned long long A[RP];
+#pragma unroll
+        for (int j = 0; j < RP; ++j) A[j] = 0ull;
+#pragma unroll
+        for (int k = 0; k <= 2 * R; ++k) {
+            const unsigned long long wk = w2(k);
+#pragma unroll
+            for (int j = 0; j < RP; ++j) A[j] = ffma2(V[j + k], wk, A[j]);
+        }
+        const long long off = (long long)(r0 + y0) * a.out_pitch + c0 + 2 * cp;
+        unsigned long long* o = reinterpret_cast<unsigned long long*>(a.out + off);
+        const int op2 = a.out_pitch >> 1;
+#pragma unroll
+        for (int j = 0; j < RP; ++j) o[j * op2] = A[j];
+        if (a.out_r) {
+            float2* orr = reinterpret_cast<float2*>(a.out_r + off);
+#pragma unroll
+            for (int j = 0; j < RP; ++j) orr[j * op2] = make_float2(round_half(lo2(A[j])), round_half(hi2(A[j])));
+        }
+    }
+}
+
+template <int R, int TH>
+__host__ __device__ constexpr size_t blur_smem_bytes_rt() {
+    return BlurTile<R, TH>::bytes > blur_fast_bytes<R, TH>() ? BlurTile<R, TH>::bytes : blur_fast_bytes<R, TH>();
+}
+
+template <int R, int TH>
+__global__ void __launch_bounds__(BLUR_NT, TH == 40 ? 7 : 1) k_blur(const BlurArgs a) {
+    extern __shared__ __align__(16) float smem[];
+    const TileIO io{a.in, a.in_pitch, a.step, a.out, a.out_r, a.copy0, a.copy0_r, a.out_pitch, a.H, a.W};
+    auto w = [&](int k) { return a.w2[k]; };
+    if (blur_tile_is_fast(io, R, BlurFast<R>::RA, TH, blockIdx.x, blockIdx.y))
+        blur_tile_fast<R, TH>(io, blockIdx.x, blockIdx.y, smem, w);
+    else
+        blur_tile<R, TH>(io, blockIdx.x, blockIdx.y, smem, w);
 }
 
 // Any radius up to PYSIFT_MAX_RADIUS (no register blocking); radius 0 copies.
@@ -938,14 +1099,15 @@ struct BlurVariant {
     BlurKernel fn;
     size_t smem;
 };
-static_assert(BlurTile<16, 40>::bytes <= 48 * 1024, "k_blur<R, TH> stays within the default dynamic shared memory");
+static_assert(BlurTile<16, 40>::bytes <= 48 * 1024 && blur_fast_bytes<16, 40>() <= 48 * 1024,
+              "k_blur<R, TH> stays within the default dynamic shared memory");
 
 template <int R>
 static BlurVariant blur_variant_r(int v) {
     switch (v) {
-        case 0: return {k_blur<R, 16>, BlurTile<R, 16>::bytes};
-        case 1: return {k_blur<R, 32>, BlurTile<R, 32>::bytes};
-        default: return {k_blur<R, 40>, BlurTile<R, 40>::bytes};
+        case 0: return {k_blur<R, 16>, blur_smem_bytes_rt<R, 16>()};
+        case 1: return {k_blur<R, 32>, blur_smem_bytes_rt<R, 32>()};
+        default: return {k_blur<R, 40>, blur_smem_bytes_rt<R, 40>()};
     }
 }
 
