@@ -1238,30 +1238,21 @@ __device__ __forceinline__ int find_octave(const int* blk_off, int n_oct, int b)
     return o;
 }
 
-// One block = 32 (16 for 7 or 8 levels) rows x 64 columns of one octave (a
-// warp per 4 or 2 rows, two mask words per row and scale).  The block stages the DoG levels of its
-// tile and a one-pixel halo in shared memory (D_s = G_{s+1} - G_s, computed
-// once per position from the NL Gaussian levels): columns c0-4 .. c0+67 are
-// read as 16-byte quads, every quad's loads of all NL levels issued before
-// the first subtraction; a quad that is not wholly inside the level is read
-// element by element, with zeros outside it.  Then each pixel is tested:
-// |D| > threshold inside the border and D >= all 26 neighbours or D <= all
-// 26 neighbours.  Lane k < (rows / 8) * 2 * S of a warp finally writes one
-// mask word (its row, 32-column half and scale) and adds its population to
-// the row's count.
-constexpr int EX_COLS = 64;
-constexpr int EX_Q = (EX_COLS + 8) / 4;       // 16-byte quads per staged row (columns c0-4 .. c0+67)
-constexpr int EX_SC = EX_COLS + 3;            // smem stride; smem column j holds image column c0-1+j
-// tile rows: 32, or 16 for 7 and 8 levels (the staged DoG stays within 48 KB)
-__host__ __device__ constexpr int ex_rows(int nl) { return nl <= 6 ? 32 : 16; }
+// One block = 32 rows x 32 columns of one octave (a warp per 4 rows, a mask
+// word per row and scale).  The block stages the DoG levels of its tile and
+// a one-pixel halo in shared memory (D_s = G_{s+1} - G_s, computed once per
+// position from the NL Gaussian levels, every load of the tile issued before
+// the first subtraction), then tests its pixels: |D| > threshold inside the
+// border and D >= all 26 neighbours or D <= all 26 neighbours.  Each lane k
+// < 4*S of a warp finally writes the mask word (row k / S, scale k % S + 1)
+// and adds its population to the row's count.
+constexpr int EX_ROWS = 32;
+constexpr int EX_SR = EX_ROWS + 2, EX_SW = 34, EX_SC = 35;  // staged rows, columns, padded stride
 
 template <int NL>
 __global__ void __launch_bounds__(256) k_extrema_mask(const ExtArgs a, Ctrl* ctrl) {
     constexpr int S = NL - 3, ND = NL - 1;
-    constexpr int EX_ROWS = ex_rows(NL), EX_SR = EX_ROWS + 2;
-    static_assert((EX_ROWS / 8) * 2 * S <= 32, "a warp's mask words fit its lanes");
-    constexpr int NQT = EX_SR * EX_Q;            // quads per level
-    constexpr int NIT = (NQT + 255) / 256;
+    constexpr int NQ = (EX_SR * EX_SW + 255) / 256;
     __shared__ float sDm[ND * EX_SR * EX_SC];
     if (a.retry_mode && !ctrl->retried) return;
     auto sD = [&](int s, int rr, int cc) -> float& { return sDm[(s * EX_SR + rr) * EX_SC + cc]; };
@@ -1269,93 +1260,69 @@ __global__ void __launch_bounds__(256) k_extrema_mask(const ExtArgs a, Ctrl* ctr
     const int o = find_octave(a.blk_off, a.n_oct, blockIdx.x);
     const OctView& v = a.oct[o];
     const int wpr = a.wpr[o];
-    const int nbx = (v.W + EX_COLS - 1) / EX_COLS;
     const int bl = blockIdx.x - a.blk_off[o];
-    const int by = bl / nbx, bx = bl - by * nbx;
-    const int r0 = by * EX_ROWS, c0 = bx * EX_COLS;
-    const bool aligned = (v.pitch & 3) == 0;
+    const int by = bl / wpr, wc = bl - by * wpr;
+    const int r0 = by * EX_ROWS, c0 = wc * 32;
+    {
+        float g[NQ][NL];
 #pragma unroll
-    for (int it = 0; it < NIT; ++it) {
-        const int q = threadIdx.x + 256 * it;
-        if (q < NQT) {
-            const int rr = q / EX_Q, qq = q - rr * EX_Q;
-            const int r = r0 - 1 + rr, cq = c0 - 4 + 4 * qq;  // image row, first column of the quad
-            float4 g[NL];
-            const bool rin = r >= 0 && r < v.H;
-            if (rin && aligned && cq >= 0 && cq + 3 < v.W) {
-                const long long off = (long long)r * v.pitch + cq;
+        for (int k = 0; k < NQ; ++k) {
+            const int q = threadIdx.x + 256 * k;
+            const int rr = q / EX_SW, cc = q - rr * EX_SW;
+            const int r = r0 - 1 + rr, c = c0 - 1 + cc;
+            const bool in = q < EX_SR * EX_SW && r >= 0 && r < v.H && c >= 0 && c < v.W;
+            const long long off = in ? (long long)r * v.pitch + c : 0;
 #pragma unroll
-                for (int l = 0; l < NL; ++l) g[l] = *reinterpret_cast<const float4*>(v.lev[l] + off);
-            } else {
+            for (int l = 0; l < NL; ++l) g[k][l] = in ? v.lev[l][off] : 0.0f;
+        }
 #pragma unroll
-                for (int l = 0; l < NL; ++l) {
-                    float e[4];
+        for (int k = 0; k < NQ; ++k) {
+            const int q = threadIdx.x + 256 * k;
+            if (q >= EX_SR * EX_SW) break;
+            const int rr = q / EX_SW, cc = q - rr * EX_SW;
 #pragma unroll
-                    for (int t = 0; t < 4; ++t) {
-                        const int c = cq + t;
-                        e[t] = (rin && c >= 0 && c < v.W) ? v.lev[l][(long long)r * v.pitch + c] : 0.0f;
-                    }
-                    g[l] = make_float4(e[0], e[1], e[2], e[3]);
-                }
-            }
-            // staged columns: image column c -> smem column c - (c0 - 1), kept for 0 .. EX_COLS + 1
-#pragma unroll
-            for (int t = 0; t < 4; ++t) {
-                const int j = 4 * qq - 3 + t;
-                if (j >= 0 && j < EX_COLS + 2) {
-#pragma unroll
-                    for (int s_ = 0; s_ < ND; ++s_) {
-                        const float hi = t == 0 ? g[s_ + 1].x : t == 1 ? g[s_ + 1].y : t == 2 ? g[s_ + 1].z : g[s_ + 1].w;
-                        const float lo = t == 0 ? g[s_].x : t == 1 ? g[s_].y : t == 2 ? g[s_].z : g[s_].w;
-                        sD(s_, rr, j) = hi - lo;
-                    }
-                }
-            }
+            for (int s = 0; s < ND; ++s) sD(s, rr, cc) = g[k][s + 1] - g[k][s];
         }
     }
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int c = c0 + lane;
     const int B = a.border;
     unsigned mine = 0;  // the mask word this lane writes
 #pragma unroll
     for (int i = 0; i < EX_ROWS / 8; ++i) {
         const int lr = warp + 8 * i, r = r0 + lr;
+        const bool inb = (r >= B && r < v.H - B && c >= B && c < v.W - B);
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int lc = 32 * h + lane, c = c0 + lc;
-            const bool inb = (r >= B && r < v.H - B && c >= B && c < v.W - B);
+        for (int s = 1; s <= S; ++s) {
+            bool ext = false;
+            if (inb) {
+                const float val = sD(s, lr + 1, lane + 1);
+                if (fabsf(val) > thr) {
+                    bool is_max = true, is_min = true;
 #pragma unroll
-            for (int s = 1; s <= S; ++s) {
-                bool ext = false;
-                if (inb) {
-                    const float val = sD(s, lr + 1, lc + 1);
-                    if (fabsf(val) > thr) {
-                        bool is_max = true, is_min = true;
+                    for (int ds = -1; ds <= 1; ++ds)
 #pragma unroll
-                        for (int ds = -1; ds <= 1; ++ds)
+                        for (int dr = 0; dr < 3; ++dr)
 #pragma unroll
-                            for (int dr = 0; dr < 3; ++dr)
-#pragma unroll
-                                for (int dc = 0; dc < 3; ++dc) {
-                                    if (ds == 0 && dr == 1 && dc == 1) continue;
-                                    const float nb = sD(s + ds, lr + dr, lc + dc);
-                                    is_max = is_max && (val >= nb);
-                                    is_min = is_min && (val <= nb);
-                                }
-                        ext = is_max || is_min;
-                    }
+                            for (int dc = 0; dc < 3; ++dc) {
+                                if (ds == 0 && dr == 1 && dc == 1) continue;
+                                const float nb = sD(s + ds, lr + dr, lane + dc);
+                                is_max = is_max && (val >= nb);
+                                is_min = is_min && (val <= nb);
+                            }
+                    ext = is_max || is_min;
                 }
-                const unsigned m = __ballot_sync(FULL_MASK, ext);
-                if (lane == (i * 2 + h) * S + (s - 1)) mine = m;
             }
+            const unsigned m = __ballot_sync(FULL_MASK, ext);
+            if (lane == i * S + (s - 1)) mine = m;
         }
     }
-    if (lane < (EX_ROWS / 8) * 2 * S) {
-        const int k = lane / S, s = lane - k * S + 1;
-        const int i = k >> 1, h = k & 1;
-        const int r = r0 + warp + 8 * i, w = 2 * bx + h;
-        if (r < v.H && w < wpr) {
-            a.mask[o][((long long)(s - 1) * v.H + r) * wpr + w] = mine;
+    if (lane < (EX_ROWS / 8) * S) {
+        const int i = lane / S, s = lane - i * S + 1;
+        const int r = r0 + warp + 8 * i;
+        if (r < v.H) {
+            a.mask[o][((long long)(s - 1) * v.H + r) * wpr + wc] = mine;
             if (mine) atomicAdd(&a.rowcnt[o][(s - 1) * v.H + r], __popc(mine));
         }
     }
@@ -2639,7 +2606,7 @@ static int run_detect(const pysift_detect_config* cfg, const uint8_t* gray, int 
     int row_off[PYSIFT_MAX_OCTAVES + 1];
     for (int o = 0; o < n_oct; ++o) {
         ea.blk_off[o] = mask_blocks;
-        mask_blocks += ceil_div(l.H[o], ex_rows(S + 3)) * ceil_div(l.W[o], EX_COLS);
+        mask_blocks += ceil_div(l.H[o], EX_ROWS) * l.wpr[o];
         row_off[o] = row_blocks;
         row_blocks += ceil_div(S * l.H[o], 8);
         ea.mask[o] = at<uint32_t>(ws, l.off_mask[o]);
