@@ -139,6 +139,17 @@ int pysift_gauss_blur(const float* in, int32_t in_pitch, float* out, int32_t out
  * rows = 0 restores the automatic choice.  Results do not depend on it. */
 int pysift_set_blur_tile_rows(int32_t rows);
 
+/* Tile heights measured by an autotuner (pysift_b200/autotune.py), used
+ * when no height is forced: rows[r * 16 + c] for radius r = 0 .. 16 (row 0
+ * unused) and level size class c = pysift_blur_size_class(H, W) (floor of
+ * log2 of the level's pixel count, minus 10, clamped to 0 .. 15): 16, 32 or
+ * 40, or 0 for the built-in rule.  n = 17 * 16 entries, or 0 to clear the
+ * table.  Applies to later calls in the process; results do not depend on
+ * it.  No counterpart in the reference (its blur launches have one shape,
+ * pysift/core.py:583-602). */
+int pysift_blur_size_class(int32_t H, int32_t W);
+int pysift_set_blur_tile_table(const int32_t* rows, int32_t n);
+
 /* 2x cubic B-spline zoom of a uint8 image scaled by 1/255
  * (cupyx.scipy.ndimage.zoom(order=3) at pysift/core.py:1270-1275).
  * coef: caller scratch of H*W doubles; out: 2H x 2W floats, pitch in floats. */

@@ -89,6 +89,8 @@ EXPORTS = {
     "pysift_gauss_blur": (ctypes.c_int, [c_void_p, c_int32, c_void_p, c_int32, c_int32, c_int32, c_void_p, c_int32,
                                          c_void_p]),
     "pysift_set_blur_tile_rows": (ctypes.c_int, [c_int32]),
+    "pysift_blur_size_class": (ctypes.c_int, [c_int32, c_int32]),
+    "pysift_set_blur_tile_table": (ctypes.c_int, [c_void_p, c_int32]),
     "pysift_zoom2x_u8": (ctypes.c_int, [c_void_p, c_int32, c_int32, c_int64, c_int32, c_void_p, c_void_p, c_int32,
                                         c_void_p]),
     "pysift_zoom2x_u8_noalloc": (ctypes.c_int, [c_void_p, c_int32, c_int32, c_int64, c_int32, c_void_p, c_int32,

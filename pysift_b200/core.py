@@ -211,6 +211,13 @@ class PySIFT:
         self._last_stats = None
         self._graphs = {}
 
+    def autotune(self, H, W, path=None):
+        """Measure (or load from the per-GPU JSON cache) the blur tile heights
+        for detections of H x W images with this configuration and hand them
+        to the library (pysift_b200.autotune); results do not change."""
+        from . import autotune as _autotune
+        return _autotune.autotune(self, H, W, path=path)
+
     # -- plumbing ---------------------------------------------------------
     def _buffers(self, H, W, slot=0):
         """Buffer set for one image size; distinct slots let detections of

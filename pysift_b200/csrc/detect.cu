@@ -1155,11 +1155,36 @@ static int blur_occupancy(int R, int v) {
 // pysift_set_blur_tile_rows: a forced variant (testing), -1 = automatic
 static std::atomic<int> g_blur_forced{-1};
 
-// The tile height with the fewest (rounds of resident CTAs) x (tile rows +
-// halo): big levels avoid a short last round, small ones a long CTA.
+// pysift_set_blur_tile_table: a measured variant per (radius, level size
+// class), -1 = the cost rule below.  Size class: floor(log2(H W)) - 10,
+// clamped to 0 .. BLUR_SIZE_CLASSES - 1.
+constexpr int BLUR_SIZE_CLASSES = 16;
+static std::atomic<int> g_blur_table[BLUR_PAIR_MAX_R + 1][BLUR_SIZE_CLASSES];
+static std::once_flag g_blur_table_once;
+
+static int blur_size_class(int H, int W) {
+    const long long px = (long long)H * W;
+    int lg = 0;
+    while (lg < 62 && (2LL << lg) <= px) ++lg;
+    return std::max(0, std::min(BLUR_SIZE_CLASSES - 1, lg - 10));
+}
+
+static void blur_table_init() {
+    std::call_once(g_blur_table_once, [] {
+        for (auto& row : g_blur_table)
+            for (auto& e : row) e.store(-1, std::memory_order_relaxed);
+    });
+}
+
+// The tile height: forced, else tuned, else the one with the fewest (rounds
+// of resident CTAs) x (tile rows + halo): big levels avoid a short last
+// round, small ones a long CTA.
 static int blur_pick(int R, int H, int W) {
     const int forced = g_blur_forced.load(std::memory_order_relaxed);
     if (forced >= 0) return forced;
+    blur_table_init();
+    const int tuned = g_blur_table[R][blur_size_class(H, W)].load(std::memory_order_relaxed);
+    if (tuned >= 0) return tuned;
     int best = 1;
     long long best_cost = -1;
     for (int v = 0; v < BLUR_NV; ++v) {
@@ -2883,6 +2908,24 @@ int pysift_set_blur_tile_rows(int32_t rows) {
         if (rows == BLUR_THS[k]) v = k;
     PYSIFT_CHECK_ARG(rows == 0 || v >= 0, "tile rows %d: 0 (automatic), 16, 32 or 40", rows);
     g_blur_forced.store(rows == 0 ? -1 : v, std::memory_order_relaxed);
+    return PYSIFT_OK;
+}
+
+int pysift_blur_size_class(int32_t H, int32_t W) { return (H > 0 && W > 0) ? blur_size_class(H, W) : -1; }
+
+int pysift_set_blur_tile_table(const int32_t* rows, int32_t n) {
+    constexpr int N = (BLUR_PAIR_MAX_R + 1) * BLUR_SIZE_CLASSES;
+    PYSIFT_CHECK_ARG(n == 0 || (rows && n == N), "the table has %d entries (0 clears it)", N);
+    int v[N];
+    for (int i = 0; i < n; ++i) {
+        v[i] = -1;
+        for (int k = 0; k < BLUR_NV; ++k)
+            if (rows[i] == BLUR_THS[k]) v[i] = k;
+        PYSIFT_CHECK_ARG(rows[i] == 0 || v[i] >= 0, "entry %d: tile rows %d: 0 (rule), 16, 32 or 40", i, rows[i]);
+    }
+    blur_table_init();
+    for (int i = 0; i < N; ++i)
+        g_blur_table[i / BLUR_SIZE_CLASSES][i % BLUR_SIZE_CLASSES].store(n ? v[i] : -1, std::memory_order_relaxed);
     return PYSIFT_OK;
 }
 
