@@ -525,30 +525,36 @@ __device__ __forceinline__ float f16_round_f64(double x) {
 // Exact dot product of two fp16 rows of D elements (16-byte aligned): each
 // product is exact in fp32 (11-bit significands), and for rows of norm <= 1
 // every float64 partial sum is exact (a multiple of 2^-48 below 2^5).
+// Four partial sums (one per 16-byte word position mod 4) added at the end:
+// exact in any order, so the result is the same as one running sum.
 __device__ __forceinline__ double dot_f16_exact(const __half* a, const __half* b, int D) {
-    double acc = 0.0;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
     const uint4* pa = reinterpret_cast<const uint4*>(a);
     const uint4* pb = reinterpret_cast<const uint4*>(b);
-    for (int c = 0; c < D / 8; ++c) {
-        const uint4 x = pa[c], y = pb[c];
-        const __half2* hx = reinterpret_cast<const __half2*>(&x);
-        const __half2* hy = reinterpret_cast<const __half2*>(&y);
+    for (int c = 0; c < D / 8; c += 4) {  // D / 8 is 8 or 16
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const float2 fx = __half22float2(hx[q]), fy = __half22float2(hy[q]);
-            acc += (double)__fmul_rn(fx.x, fy.x);
-            acc += (double)__fmul_rn(fx.y, fy.y);
+        for (int w = 0; w < 4; ++w) {
+            const uint4 x = pa[c + w], y = pb[c + w];
+            const __half2* hx = reinterpret_cast<const __half2*>(&x);
+            const __half2* hy = reinterpret_cast<const __half2*>(&y);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float2 fx = __half22float2(hx[q]), fy = __half22float2(hy[q]);
+                acc[w] += (double)__fmul_rn(fx.x, fy.x);
+                acc[w] += (double)__fmul_rn(fx.y, fy.y);
+            }
         }
     }
-    return acc;
+    return (acc[0] + acc[1]) + (acc[2] + acc[3]);
 }
 
-// Largest row L2 norm of each of the two fp16 sets, rounded up with a
-// relative margin of 2^-20, as float bits (non-negative floats order as
+// Row L2 norms of the two fp16 sets (set 1's rows, then set 2's) and the
+// largest of each set, rounded up with a relative margin of 2^-20, the
+// largest as float bits (non-negative floats order as
 // their bits, so the integer atomicMax is the float max: the result does not
 // depend on the order of the updates).  One warp per row.
 __global__ void k_f16_max_norms(const __half* __restrict__ a, int n1, const __half* __restrict__ b, int n2, int D,
-                                unsigned* __restrict__ out) {
+                                unsigned* __restrict__ out, float* __restrict__ row_norm) {
     const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
     if (w >= n1 + n2) return;
     const __half* row = w < n1 ? a + (size_t)w * D : b + (size_t)(w - n1) * D;
@@ -560,6 +566,7 @@ __global__ void k_f16_max_norms(const __half* __restrict__ a, int n1, const __ha
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL_MASK, s, o);
     if (lane == 0) {
         const float nrm = __double2float_ru(sqrt(s) * (1.0 + 0x1p-20));
+        row_norm[w] = nrm;
         atomicMax(&out[w < n1 ? 0 : 1], __float_as_uint(nrm));
     }
 }
@@ -591,7 +598,8 @@ __device__ __forceinline__ void finish_f16_row(int i, float f1, float f2, int c1
 // does not matter: each row's result is computed on its own).
 __global__ void k_match_merge_f16(const Top3* __restrict__ part, int n, int nseg, float ratio_sq,
                                   const __half* __restrict__ q, const __half* __restrict__ t, int n_t, int D,
-                                  const unsigned* __restrict__ maxnorm_t, const int* __restrict__ error,
+                                  const float* __restrict__ norm_q, const unsigned* __restrict__ maxnorm_t,
+                                  const int* __restrict__ error,
                                   int* __restrict__ best, int* __restrict__ pass, float* __restrict__ dist,
                                   int* __restrict__ recheck, int* __restrict__ n_recheck) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -622,12 +630,7 @@ __global__ void k_match_merge_f16(const Top3* __restrict__ part, int n, int nseg
         }
     }
     if (a.k3 > -INFINITY) {
-        double nq = 0.0;
-        for (int k = 0; k < D; ++k) {
-            const float f = __half2float(qi[k]);
-            nq += (double)__fmul_rn(f, f);
-        }
-        const double e = (double)D * 0x1p-21 * (sqrt(nq) * (1.0 + 0x1p-20)) * (double)__uint_as_float(*maxnorm_t);
+        const double e = (double)D * 0x1p-21 * (double)norm_q[i] * (double)__uint_as_float(*maxnorm_t);
         const float u = f16_round_f64((double)a.k3 + e);
         if (!(u <= f2 && u < f1)) {
             recheck[atomicAdd(n_recheck, 1)] = i;
@@ -642,7 +645,9 @@ __global__ void k_match_merge_f16(const Top3* __restrict__ part, int n, int nseg
 // stride over both directions' lists); keys pack the order-preserving bits
 // of the similarity above the complemented column index, so the integer
 // maximum is the best with the lowest index.
-__global__ void __launch_bounds__(256) k_match_recheck_f16(const int* __restrict__ list0, const int* __restrict__ list1,
+constexpr int RECHECK_T = 1024;
+
+__global__ void __launch_bounds__(RECHECK_T) k_match_recheck_f16(const int* __restrict__ list0, const int* __restrict__ list1,
                                                            const int* __restrict__ counts, const __half* __restrict__ a,
                                                            int n1, const __half* __restrict__ b, int n2, int D,
                                                            float ratio_sq, int* __restrict__ fbest,
@@ -650,7 +655,7 @@ __global__ void __launch_bounds__(256) k_match_recheck_f16(const int* __restrict
                                                            int* __restrict__ bbest, int* __restrict__ bpass,
                                                            float* __restrict__ bdist) {
     __shared__ __align__(16) __half qrow[128];
-    __shared__ unsigned long long s_b[8], s_s[8];
+    __shared__ unsigned long long s_b[RECHECK_T / 32], s_s[RECHECK_T / 32];
     const int c0 = counts[0], call = c0 + counts[1];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int v = blockIdx.x; v < call; v += gridDim.x) {
@@ -824,7 +829,7 @@ struct MatchLayout {
     // off_ctl: int[8] = error flag, SIM_F16 recheck counts (forward, backward),
     // max row norms (set 1, set 2) as float bits
     size_t off_fpart, off_bpart, off_fbest, off_fpass, off_fdist, off_bbest, off_bpass, off_bdist, off_ctl;
-    size_t off_rl0, off_rl1;
+    size_t off_rl0, off_rl1, off_nrm;
     size_t off_na, off_nb, off_bfa, off_bfb, off_qa, off_ta, off_qb, off_tb;
     size_t total;
 };
@@ -849,10 +854,11 @@ static MatchLayout match_layout(int n1, int n2, int D, int exact) {
     l.off_bpass = take((size_t)n2 * 4);
     l.off_bdist = take((size_t)n2 * 4);
     l.off_ctl = take(8 * sizeof(int));
-    l.off_rl0 = l.off_rl1 = 0;
+    l.off_rl0 = l.off_rl1 = l.off_nrm = 0;
     if (!exact) {
         l.off_rl0 = take((size_t)n1 * 4);
         l.off_rl1 = take((size_t)n2 * 4);
+        l.off_nrm = take(((size_t)n1 + n2) * 4);
     }
     l.off_na = l.off_nb = l.off_bfa = l.off_bfb = l.off_qa = l.off_ta = l.off_qb = l.off_tb = 0;
     if (exact) {
@@ -892,7 +898,7 @@ static int run_match(int mode, const uint8_t* a_q, const uint8_t* a_t, int n1, c
     const __half* hb = reinterpret_cast<const __half*>(b_q);
     unsigned* maxnorm = reinterpret_cast<unsigned*>(ctl + 3);
     if (mode == SIM_F16) {
-        k_f16_max_norms<<<ceil_div(n1 + n2, 8), 256, 0, st>>>(ha, n1, hb, n2, D, maxnorm);
+        k_f16_max_norms<<<ceil_div(n1 + n2, 8), 256, 0, st>>>(ha, n1, hb, n2, D, maxnorm, wsp<float>(ws, l.off_nrm));
         PYSIFT_LAUNCH_CHECK("k_f16_max_norms");
     }
     const bool sim = mode == SIM_F16 || mode == SIM_I8;
@@ -926,7 +932,8 @@ static int run_match(int mode, const uint8_t* a_q, const uint8_t* a_t, int n1, c
         if (mode == SIM_F16) {
             k_match_merge_f16<<<ceil_div(s.n_q, 128), 128, 0, st>>>(
                 static_cast<const Top3*>(s.part), s.n_q, nseg, ratio_sq, dir == 0 ? ha : hb, dir == 0 ? hb : ha,
-                s.n_t, D, maxnorm + (dir == 0 ? 1 : 0), err, best, pass, dist,
+                s.n_t, D, wsp<float>(ws, l.off_nrm) + (dir == 0 ? 0 : n1), maxnorm + (dir == 0 ? 1 : 0), err, best,
+                pass, dist,
                 wsp<int>(ws, dir == 0 ? l.off_rl0 : l.off_rl1), ctl + 1 + dir);
             PYSIFT_LAUNCH_CHECK("k_match_merge_f16");
         } else {
@@ -941,7 +948,7 @@ static int run_match(int mode, const uint8_t* a_q, const uint8_t* a_t, int n1, c
         }
     }
     if (mode == SIM_F16) {
-        k_match_recheck_f16<<<2 * sm_count(), 256, 0, st>>>(wsp<int>(ws, l.off_rl0), wsp<int>(ws, l.off_rl1), ctl + 1,
+        k_match_recheck_f16<<<sm_count(), RECHECK_T, 0, st>>>(wsp<int>(ws, l.off_rl0), wsp<int>(ws, l.off_rl1), ctl + 1,
                                                              ha, n1, hb, n2, D, ratio_sq, fbest, fpass, fdist, bbest,
                                                              bpass, bdist);
         PYSIFT_LAUNCH_CHECK("k_match_recheck_f16");
