@@ -340,10 +340,16 @@ EXPORT void orc_refine(const float* dog, int S2, int H, int W, const int* cands,
 /* Exact, order-independent histogram accumulation: every non-negative
  * float32 contribution is rounded to a multiple of 2^-40 (round to nearest
  * even) and summed as a 64-bit integer; the bin value is the sum rounded to
- * float32 and scaled back.  Contributions are <= sqrt(2), so the sums stay
- * far below 2^63 for any patch these kernels visit. */
+ * float32 and scaled back.  Contributions are below 2.2 (gradient
+ * magnitudes of pyramid values in [-0.28, 1.28]), so the sums stay far below
+ * 2^63 for any patch these kernels visit. */
 static inline long long orc_fix(float c) { return llrintf(c * 0x1p40f); }
 static inline float orc_unfix(long long s) { return (float)s * 0x1p-40f; }
+/* The descriptor's bins use a quantum of 2^-24 (same rounding, same
+ * integer sum): the kernel keeps them in 32-bit shared words folded into
+ * 64-bit totals, so the sum is the same exact integer. */
+static inline long long orc_fix24(float c) { return llrintf(c * 0x1p24f); }
+static inline float orc_unfix24(long long s) { return (float)s * 0x1p-24f; }
 
 static float tree32(const float* v, int stride) {
     float a[32];
@@ -422,7 +428,7 @@ EXPORT void orc_orientation(const float* gauss, int H, int W, const float* kpts,
 /* (N,5) = [ri, ci, ang_rad, ph, si]; dsp_scales NULL/n_dsp=0 for the   */
 /* single-scale descriptor.  Output: L2 -> clip 0.2 -> L2 vector (the   */
 /* kernel output before RootSIFT).                                      */
-/* Canonical: exact fixed-point histogram (orc_fix) instead of shared-  */
+/* Canonical: exact fixed-point histogram (orc_fix24) instead of shared-*/
 /* memory float atomics; norms by the reference's warp tree then warp   */
 /* partials 0..3 in order; 1/sqrtf instead of rsqrtf; orc_* math.        */
 /* ------------------------------------------------------------------ */
@@ -465,14 +471,14 @@ static void desc_accumulate(const float* g, int H, int W, float ri, float ci, fl
         float w_y0 = 1.0f - dy_b, w_y1 = dy_b;
         float w_x0 = 1.0f - dx_b, w_x1 = dx_b;
         float w_o0 = 1.0f - df, w_o1 = df;
-        acc[yi0c * 32 + xi0c * 8 + oi0w] += orc_fix(w_y0 * w_x0 * w_o0 * wmag);
-        acc[yi0c * 32 + xi0c * 8 + oi1w] += orc_fix(w_y0 * w_x0 * w_o1 * wmag);
-        acc[yi0c * 32 + xi1c * 8 + oi0w] += orc_fix(w_y0 * w_x1 * w_o0 * wmag);
-        acc[yi0c * 32 + xi1c * 8 + oi1w] += orc_fix(w_y0 * w_x1 * w_o1 * wmag);
-        acc[yi1c * 32 + xi0c * 8 + oi0w] += orc_fix(w_y1 * w_x0 * w_o0 * wmag);
-        acc[yi1c * 32 + xi0c * 8 + oi1w] += orc_fix(w_y1 * w_x0 * w_o1 * wmag);
-        acc[yi1c * 32 + xi1c * 8 + oi0w] += orc_fix(w_y1 * w_x1 * w_o0 * wmag);
-        acc[yi1c * 32 + xi1c * 8 + oi1w] += orc_fix(w_y1 * w_x1 * w_o1 * wmag);
+        acc[yi0c * 32 + xi0c * 8 + oi0w] += orc_fix24(w_y0 * w_x0 * w_o0 * wmag);
+        acc[yi0c * 32 + xi0c * 8 + oi1w] += orc_fix24(w_y0 * w_x0 * w_o1 * wmag);
+        acc[yi0c * 32 + xi1c * 8 + oi0w] += orc_fix24(w_y0 * w_x1 * w_o0 * wmag);
+        acc[yi0c * 32 + xi1c * 8 + oi1w] += orc_fix24(w_y0 * w_x1 * w_o1 * wmag);
+        acc[yi1c * 32 + xi0c * 8 + oi0w] += orc_fix24(w_y1 * w_x0 * w_o0 * wmag);
+        acc[yi1c * 32 + xi0c * 8 + oi1w] += orc_fix24(w_y1 * w_x0 * w_o1 * wmag);
+        acc[yi1c * 32 + xi1c * 8 + oi0w] += orc_fix24(w_y1 * w_x1 * w_o0 * wmag);
+        acc[yi1c * 32 + xi1c * 8 + oi1w] += orc_fix24(w_y1 * w_x1 * w_o1 * wmag);
     }
 }
 
@@ -513,7 +519,7 @@ EXPORT void orc_descriptor(const float* gauss, int n_slices, int H, int W, const
             desc_accumulate(g, H, W, ri, ci, cos_a, sin_a, ang, (int)phf, acc);
         }
         float v[128];
-        for (int b = 0; b < 128; ++b) v[b] = orc_unfix(acc[b]);
+        for (int b = 0; b < 128; ++b) v[b] = orc_unfix24(acc[b]);
         if (n_dsp > 0) {
             float inv_n = 1.0f / (float)n_dsp;
             for (int b = 0; b < 128; ++b) v[b] = v[b] * inv_n;

@@ -1770,23 +1770,23 @@ struct OriArgs {
     int* angcnt;
 };
 
-// Exact, order-independent histogram accumulation: each non-negative float32
+// Exact, order-independent orientation histograms: each non-negative float32
 // contribution is rounded to a multiple of 2^-40 (round to nearest even) and
 // added as a 64-bit integer; a bin's value is the integer sum rounded to
-// float32 and scaled back.  Contributions are <= sqrt(2), so sums stay far
-// below 2^63.  This makes the histograms independent of which thread adds
+// float32 and scaled back.  Contributions are below 2.2 (gradient magnitudes
+// of pyramid values in [-0.28, 1.28]), so sums stay far below 2^63.  This makes the histograms independent of which thread adds
 // what when, so any number of threads can share a keypoint.
 __device__ __forceinline__ unsigned long long fix40(float c) {
     return (unsigned long long)__float2ll_rn(c * 0x1p40f);
 }
 __device__ __forceinline__ float unfix40(unsigned long long s) { return __ll2float_rn((long long)s) * 0x1p-40f; }
 
-// Warp-private fixed-point histograms with native 32-bit shared atomics.
-// A value q < 2^42 is added as two limbs, q mod 2^21 into lo[bin] and
-// q >> 21 into hi[bin]; every FOLD_STEPS warp steps (at most 4 values per
-// lane and bin per step) the limbs are folded into a 64-bit total and
-// cleared, so neither limb can overflow.  Integer sums keep the totals exact
-// and independent of the order of the atomics.
+// Warp-private fixed-point orientation histograms with native 32-bit
+// shared atomics.  A value q < 2^42 is added as two limbs, q mod 2^21 into
+// lo[bin] and q >> 21 into hi[bin]; every FOLD_STEPS warp steps (at most 4
+// values per lane and bin per step) the limbs are folded into a 64-bit total
+// and cleared, so neither limb can overflow.  Integer sums keep the totals
+// exact and independent of the order of the atomics.
 constexpr int FOLD_STEPS = 8;
 
 struct WarpHist {
@@ -1794,10 +1794,7 @@ struct WarpHist {
     unsigned int* hi;
     unsigned long long* tot;
     int nbins;
-    // Descriptor histograms (128 bins = 4 y-cells x 4 x-cells x 8 orientations)
-    // store bin b at b ^ (ycell << 3), so that the y-cell moves a bin to
-    // another shared-memory bank; other sizes are stored in order.
-    __device__ __forceinline__ int phys(int bin) const { return nbins == 128 ? bin ^ (((bin >> 5) & 3) << 3) : bin; }
+    __device__ __forceinline__ int phys(int bin) const { return bin; }
     __device__ __forceinline__ void add(int bin, unsigned long long q) const {
         const int p = phys(bin);
         atomicAdd(lo + p, (unsigned int)(q & 0x1fffffull));
@@ -2204,9 +2201,39 @@ constexpr int DESC_W = DESC_T / 32;
 constexpr int DESC_L = 32 / (DESC_GR * DESC_GC);
 static_assert(DESC_GR * DESC_GC * DESC_L == 32, "descriptor lane groups must tile a warp");
 
+// Descriptor histograms: exact fixed point at a quantum of 2^-24, one 32-bit
+// shared word per bin and warp (one atomic per corner).  Pyramid values lie
+// in [-0.28, 1.28] (u8/255, widened by the cubic spline of the 2x base), so
+// a gradient magnitude is below 2.2 and a pixel's eight corner weights sum
+// to at most that; a warp step adds at most 32 * 2.2 * 2^24 + 64 < 1.19e9 to
+// one bin, and folding the words into 64-bit totals every DESC_FOLD_STEPS = 3
+// steps keeps them below 2^32.  Bin b sits at b ^ (ycell << 3), so the
+// y-cell moves a bin to another bank.
+constexpr int DESC_FOLD_STEPS = 3;
+__device__ __forceinline__ unsigned fix24(float c) { return __float2uint_rn(c * 0x1p24f); }
+__device__ __forceinline__ float unfix24(unsigned long long s) { return __ull2float_rn(s) * 0x1p-24f; }
+
+struct DescHist {
+    unsigned* h;               // [128] words of this warp
+    unsigned long long* tot;   // [128] totals of this warp
+    __device__ static __forceinline__ int phys(int bin) { return bin ^ (((bin >> 5) & 3) << 3); }
+    // all lanes of the warp call fold() together
+    __device__ __forceinline__ void fold() const {
+        __syncwarp();
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int b = (int)(threadIdx.x & 31) + 32 * i;
+            const int p = phys(b);
+            tot[b] += (unsigned long long)h[p];
+            h[p] = 0u;
+        }
+        __syncwarp();
+    }
+};
+
 __device__ __forceinline__ void desc_accumulate(const float* __restrict__ g, long long P, int H, int W, float ri,
                                                 float ci, float cos_a, float sin_a, float ang_rad, int ph,
-                                                const WarpHist& hw, int tid) {
+                                                const DescHist& hw, int tid) {
     const float scale_sp = 4.0f / (2.0f * (float)ph);
     const float sigma_d = (float)ph * 0.5657f;
     const float inv_2s2 = 1.0f / (2.0f * sigma_d * sigma_d + 1e-12f);
@@ -2224,8 +2251,7 @@ __device__ __forceinline__ void desc_accumulate(const float* __restrict__ g, lon
     const int du = DESC_W / runs, dv = DESC_W - du * runs;
     int u = warp / runs, v = warp - u * runs;
     const int pr0 = gi * band_r, pc0 = gj * band_c + k;
-    unsigned* const lo = hw.lo;
-    unsigned* const hi = hw.hi;
+    unsigned* const hb = hw.h;
     int steps = 0;
     for (int t = warp; t < nsteps; t += DESC_W) {
         const int pr = pr0 + u, pcb = v * DESC_L + k, pc = pc0 + v * DESC_L;
@@ -2271,20 +2297,17 @@ __device__ __forceinline__ void desc_accumulate(const float* __restrict__ g, lon
             // histograms store it at y*32 + ((x ^ y) << 3) + o
             const int b00 = yi0c * 32 + ((xi0c ^ yi0c) << 3), b01 = yi0c * 32 + ((xi1c ^ yi0c) << 3);
             const int b10 = yi1c * 32 + ((xi0c ^ yi1c) << 3), b11 = yi1c * 32 + ((xi1c ^ yi1c) << 3);
-            const unsigned long long q[8] = {
-                fix40(w_y0 * w_x0 * w_o0 * wmag), fix40(w_y0 * w_x0 * w_o1 * wmag),
-                fix40(w_y0 * w_x1 * w_o0 * wmag), fix40(w_y0 * w_x1 * w_o1 * wmag),
-                fix40(w_y1 * w_x0 * w_o0 * wmag), fix40(w_y1 * w_x0 * w_o1 * wmag),
-                fix40(w_y1 * w_x1 * w_o0 * wmag), fix40(w_y1 * w_x1 * w_o1 * wmag)};
+            const unsigned q[8] = {
+                fix24(w_y0 * w_x0 * w_o0 * wmag), fix24(w_y0 * w_x0 * w_o1 * wmag),
+                fix24(w_y0 * w_x1 * w_o0 * wmag), fix24(w_y0 * w_x1 * w_o1 * wmag),
+                fix24(w_y1 * w_x0 * w_o0 * wmag), fix24(w_y1 * w_x0 * w_o1 * wmag),
+                fix24(w_y1 * w_x1 * w_o0 * wmag), fix24(w_y1 * w_x1 * w_o1 * wmag)};
             const int pb[8] = {b00 + oi0w, b00 + oi1w, b01 + oi0w, b01 + oi1w,
                                b10 + oi0w, b10 + oi1w, b11 + oi0w, b11 + oi1w};
 #pragma unroll
-            for (int c = 0; c < 8; ++c) {
-                atomicAdd(lo + pb[c], (unsigned)q[c] & 0x1fffffu);
-                atomicAdd(hi + pb[c], (unsigned)(q[c] >> 21));
-            }
+            for (int c = 0; c < 8; ++c) atomicAdd(hb + pb[c], q[c]);
         }
-        if (++steps == FOLD_STEPS) {
+        if (++steps == DESC_FOLD_STEPS) {
             hw.fold();
             steps = 0;
         }
@@ -2320,7 +2343,7 @@ __device__ __forceinline__ float bins_sum(float x, float* part) {
 // Warps accumulate into private fixed-point histograms; threads 0..127 then
 // own one bin each for the merge, normalisation and RootSIFT.
 __global__ void __launch_bounds__(DESC_T, 5) k_descriptor(const DescArgs a, Ctrl* ctrl) {
-    __shared__ unsigned int wlo[DESC_W][128], whi[DESC_W][128];
+    __shared__ unsigned int wh32[DESC_W][128];
     __shared__ unsigned long long whist[DESC_W][128];
     __shared__ float part[4];
     __shared__ int s_entry[2];  // alternates, so a late reader never sees the next entry
@@ -2334,8 +2357,7 @@ __global__ void __launch_bounds__(DESC_T, 5) k_descriptor(const DescArgs a, Ctrl
         if (tid == 0) next = (int)gridDim.x + atomicAdd(&ctrl->desc_next, 1);
         for (int b = tid; b < DESC_W * 128; b += DESC_T) {
             (&whist[0][0])[b] = 0ull;
-            (&wlo[0][0])[b] = 0u;
-            (&whi[0][0])[b] = 0u;
+            (&wh32[0][0])[b] = 0u;
         }
         __syncthreads();
         int row = a.rank[e];
@@ -2351,7 +2373,7 @@ __global__ void __launch_bounds__(DESC_T, 5) k_descriptor(const DescArgs a, Ctrl
             float sin_a, cos_a;
             sm::sincosf_(ang_rad, &sin_a, &cos_a);
             const float* g = v.lev[si];
-            const WarpHist hw{wlo[warp], whi[warp], whist[warp], 128};
+            const DescHist hw{wh32[warp], whist[warp]};
             if (a.n_dsp > 0) {
                 for (int dd = 0; dd < a.n_dsp; ++dd) {
                     int ph = (int)(phf * a.dsp_scales[dd] + 0.5f);
@@ -2366,7 +2388,7 @@ __global__ void __launch_bounds__(DESC_T, 5) k_descriptor(const DescArgs a, Ctrl
                 unsigned long long s = 0ull;
     #pragma unroll
                 for (int w = 0; w < DESC_W; ++w) s += whist[w][tid];
-                float val = unfix40(s);
+                float val = unfix24(s);
                 if (a.n_dsp > 0) val = val * (1.0f / (float)a.n_dsp);
                 float inv = 1.0f / sqrtf(bins_sum(val * val, part) + 1e-14f);
                 float t = val * inv;
