@@ -169,11 +169,12 @@ int pysift_match_workspace_size(int32_t n1, int32_t n2, int32_t D, int32_t exact
 /* Reference semantics: fp16 operands (16-byte aligned rows), the similarity
  * s = the fp16 rounding (nearest, ties to even) of the exact dot product,
  * d^2 = max(0, 2 - 2 s), pass iff d2^2 > 1e-10 and d1^2 < ratio^2 d2^2
- * (float32). pairs: int32[n1][2].  The tensor-core scan keeps candidates on
- * its fp32 values; the two candidates of each row are recomputed exactly and
- * the rows they do not settle are recomputed over every column, so the result
- * is the one the exact similarity matrix gives, for rows of L2 norm <= 1 (the
- * stitch path's normalised descriptors; the float64 sums are exact there). */
+ * (float32). pairs: int32[n1][2].  The tensor-core scan keeps, per row, the
+ * three 32-column chunks with the largest fp32 values; the columns of the two
+ * best chunks are recomputed exactly and the rows they do not settle are
+ * recomputed over every column, so the result is the one the exact
+ * similarity matrix gives, for rows of L2 norm <= 1 (the stitch path's
+ * normalised descriptors; the float64 sums are exact there). */
 int pysift_match_fp16(const uint16_t* d1, int32_t n1, const uint16_t* d2, int32_t n2, int32_t D, float ratio,
                       void* workspace, size_t workspace_bytes, int32_t* fwd_best, int32_t* fwd_pass,
                       int32_t* bwd_best, int32_t* bwd_pass, int32_t* pairs, float* pair_dist, int32_t* pair_count,
@@ -186,8 +187,9 @@ int pysift_match_fp16(const uint16_t* d1, int32_t n1, const uint16_t* d2, int32_
 int pysift_match_fp16_recheck_counts(const void* workspace, int32_t n1, int32_t n2, int32_t D, int32_t* counts,
                                      pysift_stream_t stream);
 
-/* Exact squared L2 of uint8-valued descriptors via bf16 products (exact for
- * D <= 128), pass iff d2^2 > 0 and d1^2 < ratio^2 d2^2. */
+/* Exact squared L2 of uint8-valued descriptors (16-byte aligned rows) via
+ * bf16 products (exact for D <= 128), pass iff d2^2 > 0 and
+ * d1^2 < ratio^2 d2^2. */
 int pysift_match_u8_exact(const uint8_t* d1, int32_t n1, const uint8_t* d2, int32_t n2, int32_t D, float ratio,
                           void* workspace, size_t workspace_bytes, int32_t* fwd_best, int32_t* fwd_pass,
                           int32_t* bwd_best, int32_t* bwd_pass, int32_t* pairs, float* pair_dist,
@@ -197,7 +199,8 @@ int pysift_match_u8_exact(const uint8_t* d1, int32_t n1, const uint8_t* d2, int3
  * into e4m3 planes (16h, h, 16l, l all exact in e4m3) and one kind::f8f6f4
  * tcgen05 GEMM over the 4D concatenated planes forms 256 h.h' + 16 h.l' +
  * 16 l.h' + l.l' = v.v' (the four nibble GEMMs in one accumulation).
- * Workspace from pysift_match_workspace_size(..., exact_u8 = 2, ...). */
+ * Rows 16-byte aligned.  Workspace from
+ * pysift_match_workspace_size(..., exact_u8 = 2, ...). */
 int pysift_match_u8_split_fp8(const uint8_t* d1, int32_t n1, const uint8_t* d2, int32_t n2, int32_t D, float ratio,
                               void* workspace, size_t workspace_bytes, int32_t* fwd_best, int32_t* fwd_pass,
                               int32_t* bwd_best, int32_t* bwd_pass, int32_t* pairs, float* pair_dist,

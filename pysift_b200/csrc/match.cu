@@ -6,36 +6,44 @@
 // streams 128-row train tiles through a ring of cp.async buffers (three for
 // 128-byte rows, two for 256-byte rows; no-swizzle
 // K-major core-matrix layout); one thread issues the tcgen05.mma of tile t+1
-// (kind::f16, fp32 accumulator in tensor memory, two accumulators of 128
-// columns) while eight warps reduce tile t, read back with tcgen05.ld, to
-// running per-row top-2s in registers (two warps per TMEM lane quadrant, each
-// half of the tile's columns, even and odd columns in separate chains; the
-// partials merge exactly at the end).  Train tiles are split into
-// segments so that the grid fills the SMs; k_match_merge combines the
-// segments and applies the ratio test; k_match_mutual keeps mutual matches
-// (pysift/core.py:2574-2701, 2840-2940).
+// (kind::f16 / f8f6f4 / i8, fp32 or s32 accumulator in tensor memory, two
+// accumulators of 128 columns) while eight warps reduce tile t, read back with
+// tcgen05.ld (two warps per TMEM lane quadrant, each half of the tile's
+// columns).  Train tiles are split into segments so that the grid fills the
+// SMs; a merge kernel combines the segments of each row and applies the ratio
+// test; k_match_mutual keeps mutual matches (pysift/core.py:2574-2701,
+// 2840-2940).
 //
-// Two scoring modes share the kernels:
+// The reduction works on 32-column chunks: a chunk's key is its largest
+// column key (a tree of 31 max operations, no per-column index), and each
+// row keeps the three best chunks in (key desc, first column asc) order with
+// the first two chunks' positions (Top3 at chunk level).  The merge then
+// recomputes the candidate chunks' columns exactly, one warp per row:
 //   SIM_F16   reference semantics: fp16 inputs, the similarity rounded to fp16
 //             (torch.mm under fp16 autocast, core.py:2604-2605), larger is better,
 //             d^2 = max(0, 2 - 2 s), pass iff d2^2 > 1e-10 and d1^2 < r^2 d2^2 in float32.
 //             The canonical similarity is the fp16 rounding (nearest, ties to
 //             even) of the EXACT dot product.  The tensor cores' fp32
-//             accumulation is within e = D 2^-21 |a| max|b| of it, so the
-//             scan keeps, on the raw fp32 values, the best and second with
-//             their indices and the third value; k_match_merge_f16 recomputes
-//             the two candidates exactly (float64 sums of the exact fp16
-//             products: every partial sum is a multiple of 2^-48 below 2^5 in
-//             magnitude for rows of norm <= 1, hence exact in any order) and
-//             accepts the row when no other column can reach the exact
-//             second value (fp16(third + e) <= second, and < best); the other
-//             rows are recomputed over every column by k_match_recheck_f16.
+//             accumulation is within e = D 2^-21 |a| max|b| of it.  The merge
+//             recomputes every column of the two best chunks exactly (float64
+//             sums of the exact fp16 products: every partial sum is a multiple
+//             of 2^-48 below 2^5 in magnitude for rows of norm <= 1, hence
+//             exact in any order) and accepts the row when no column of the
+//             other chunks can reach the exact second value
+//             (fp16(third chunk key + e) <= second, and < best); the other rows
+//             are recomputed over every column by k_match_recheck_f16.
 //   DIST_BF16 exact L2 on uint8-valued descriptors: bf16 holds 0..255 exactly and
 //             every partial sum of 128 products stays below 2^24, so the fp32
 //             accumulator is the exact integer dot product.  Rows rank train
 //             entries by 2 a.b - |b|^2 (exact in fp32: |2 a.b| < 2^24), which orders
 //             them as -|a - b|^2; d^2 = |a|^2 - key, pass iff d2^2 > 0 and
-//             d1^2 < r^2 d2^2 (exact).
+//             d1^2 < r^2 d2^2 (exact).  The merge recomputes the best chunk
+//             from the uint8 rows (integer dot products): the first column
+//             with the chunk's key is the best, the second key the larger of
+//             the chunk's second and the next chunk's key.
+//   SPLIT_FP8 the same keys through split-nibble e4m3 planes.
+//   SIM_I8    int8 similarities divided by the row scales, per column (the
+//             division does not commute with the maximum): column-level top-2.
 // Ties are broken towards the lower index in every direction: a scan visits
 // train entries in increasing index order and replaces the best only on a
 // strictly larger key; segments merge in index order.
@@ -197,35 +205,26 @@ struct RowScanArgs {
     const uint8_t* q;    // n_q rows of RB bytes (fp16 / bf16 / e4m3 codes)
     const uint8_t* t;    // n_t rows of RB bytes
     int n_q, n_t;
-    const int* norm_t;   // DIST_BF16: |t|^2 per train row
+    const float* norm_t;   // DIST_BF16 / SPLIT_FP8: |t|^2 per train row (exact in float32)
     const float* scale_q;  // SIM_I8: quantisation scale per query row
     const float* scale_t;  //         and per train row
     int seg_tiles;       // train tiles per segment (blockIdx.y)
-    void* part;          // [n_q][gridDim.y] Top3 (SIM_F16) or Top2
+    void* part;          // [n_q][gridDim.y] Top3 (chunk level; SIM_I8: Top2 of columns)
     int* error;          // set when an MMA wait gives up
 };
 
-// Running top-2 of one 32-column chunk: even columns into (k1, k2, i1), odd
-// columns into (m1, m2, j1) (two independent chains); each partial visits
-// its columns in increasing index order and replaces its best only on a
-// strictly larger key.
-template <int MODE>
-__device__ __forceinline__ void scan_chunk(const uint32_t (&v)[32], int col0, int lim, int nb_lane, float sq,
-                                           float& k1, float& k2, int& i1, float& m1, float& m2, int& j1) {
+// SIM_I8 running top-2 of one 32-column chunk: even columns into (k1, k2,
+// i1), odd columns into (m1, m2, j1) (two independent chains); each partial
+// visits its columns in increasing index order and replaces its best only
+// on a strictly larger key.
+__device__ __forceinline__ void scan_chunk_i8(const uint32_t (&v)[32], int col0, int lim, int nb_lane, float sq,
+                                              float& k1, float& k2, int& i1, float& m1, float& m2, int& j1) {
 #pragma unroll
     for (int j = 0; j < 32; ++j) {
-        float key;
-        if (MODE == SIM_F16) {
-            key = __half2float(__float2half_rn(__uint_as_float(v[j])));
-        } else if (MODE == SIM_I8) {
-            // torch._int_mm(...).float() / (s1 * s2.T) (pysift/core.py:2908-2910):
-            // the int32 dot product is exact (|.| < 2^24, so exact in float32)
-            const float st = __int_as_float(__shfl_sync(FULL_MASK, nb_lane, j));
-            key = __fdiv_rn((float)(int)v[j], __fmul_rn(sq, st));
-        } else {
-            const float nb = __int_as_float(__shfl_sync(FULL_MASK, nb_lane, j));
-            key = __fsub_rn(2.0f * __uint_as_float(v[j]), nb);
-        }
+        // torch._int_mm(...).float() / (s1 * s2.T) (pysift/core.py:2908-2910):
+        // the int32 dot product is exact (|.| < 2^24, so exact in float32)
+        const float st = __int_as_float(__shfl_sync(FULL_MASK, nb_lane, j));
+        float key = __fdiv_rn((float)(int)v[j], __fmul_rn(sq, st));
         if (j >= lim) key = -INFINITY;
         if (j & 1) {
             m2 = fmaxf(m2, fminf(key, m1));
@@ -239,17 +238,39 @@ __device__ __forceinline__ void scan_chunk(const uint32_t (&v)[32], int col0, in
     }
 }
 
-// SIM_F16: the raw fp32 accumulator values, even columns into e, odd into o
-// (two independent chains, each visiting its columns in increasing order).
-__device__ __forceinline__ void scan_chunk_f16(const uint32_t (&v)[32], int col0, int lim, Top3& e, Top3& o) {
+// Largest key of a 32-column chunk (SIM_F16: the raw fp32 accumulator;
+// DIST_BF16 / SPLIT_FP8: 2 a.b - |b|^2, exact), columns >= lim excluded.
+// A pairwise tree of 31 max operations; the chunk's position in the row is
+// kept by the caller, so no per-column index is tracked.
+template <int MODE>
+__device__ __forceinline__ float chunk_max(uint32_t (&v)[32], int lim, const float* __restrict__ nb) {
+    float x[32];
+    if constexpr (MODE == SIM_F16) {
 #pragma unroll
-    for (int j = 0; j < 32; ++j) {
-        const float key = j < lim ? __uint_as_float(v[j]) : -INFINITY;
-        if (j & 1)
-            top3_push(o, key, col0 + j);
-        else
-            top3_push(e, key, col0 + j);
+        for (int j = 0; j < 32; ++j) x[j] = __uint_as_float(v[j]);
+    } else {
+        const float4* n4 = reinterpret_cast<const float4*>(nb);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const float4 n = n4[q];  // the same address in every lane: one broadcast
+            // 2 a.b and |b|^2 are integers below 2^24: the fused result is exact
+            x[4 * q + 0] = __fmaf_rn(2.0f, __uint_as_float(v[4 * q + 0]), -n.x);
+            x[4 * q + 1] = __fmaf_rn(2.0f, __uint_as_float(v[4 * q + 1]), -n.y);
+            x[4 * q + 2] = __fmaf_rn(2.0f, __uint_as_float(v[4 * q + 2]), -n.z);
+            x[4 * q + 3] = __fmaf_rn(2.0f, __uint_as_float(v[4 * q + 3]), -n.w);
+        }
     }
+    if (lim < 32) {  // the last tile only; the same in every lane
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+            if (j >= lim) x[j] = -INFINITY;
+    }
+#pragma unroll
+    for (int w = 16; w > 0; w >>= 1) {
+#pragma unroll
+        for (int j = 0; j < w; ++j) x[j] = fmaxf(x[j], x[j + w]);
+    }
+    return x[0];
 }
 
 // Top-2 of the union of two disjoint column sets: the best is the larger
@@ -262,6 +283,19 @@ __device__ __forceinline__ void top2_merge(float& k1, float& k2, int& i1, float 
     k1 = fmaxf(k1, bk1);
 }
 
+// 128 train norms (float) of tile `col0` into a shared slot by cp.async;
+// columns >= n are zero-filled (their keys are excluded anyway).
+__device__ __forceinline__ void stage_norms(float* dst, const float* src, int col0, int n) {
+    const int t = threadIdx.x;
+    if (t < NT / 4) {
+        const int c = col0 + 4 * t;
+        const int valid = c < n ? min(16, (n - c) * 4) : 0;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst + 4 * t)),
+                     "l"(valid ? src + c : src), "r"(valid)
+                     : "memory");
+    }
+}
+
 template <int MODE, int RB>
 __global__ void __launch_bounds__(MATCH_THREADS) k_match_rows(const RowScanArgs args) {
     constexpr int KC = RB / 16;
@@ -269,15 +303,23 @@ __global__ void __launch_bounds__(MATCH_THREADS) k_match_rows(const RowScanArgs 
     // train tiles in flight: a 3-deep ring for 128-byte rows (4 tiles in the
     // 80 KB a CTA is given), 2 for 256-byte rows
     constexpr int NB = RB <= 128 ? 3 : 2;
+    // SIM_F16, DIST_BF16, SPLIT_FP8: chunk-level state (the key of each
+    // 32-column chunk is its largest); SIM_I8: column-level top-2
+    constexpr bool CHUNKED = MODE != SIM_I8;
+    constexpr bool NORMS = MODE == DIST_BF16 || MODE == SPLIT_FP8;
+    // train norms of a tile are read one iteration after the tile's slot in
+    // the train ring is refilled, so their ring has one slot more
+    constexpr int NBN = NB + 1;
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t* sQ = smem;
+    float* sNorm = reinterpret_cast<float*>(smem + (1 + NB) * TILE_BYTES);  // [NBN][NT]
     __shared__ __align__(8) uint64_t mbar[2];
     __shared__ uint32_t tmem_base;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int quad = warp & 3, half = warp >> 2;  // TMEM lane quadrant, column half of each tile
     const int rloc = quad * 32 + lane;            // this thread's query row in the block
-    __shared__ Top3 s_half[MT];  // Top2 in the first 16 bytes outside SIM_F16
+    __shared__ Top3 s_half[MT];  // Top2 in the first 16 bytes for SIM_I8
     const int q0 = blockIdx.x * MT;
     const int n_tt = (args.n_t + NT - 1) / NT;
     const int t_begin = blockIdx.y * args.seg_tiles;
@@ -295,10 +337,14 @@ __global__ void __launch_bounds__(MATCH_THREADS) k_match_rows(const RowScanArgs 
     }
     stage_rows<RB>(sQ, args.q, q0, args.n_q);
     stage_rows<RB>(smem + TILE_BYTES, args.t, t_begin * NT, args.n_t);
+    if (NORMS) stage_norms(sNorm, args.norm_t, t_begin * NT, args.n_t);
     asm volatile("cp.async.commit_group;" ::: "memory");
 #pragma unroll
     for (int p = 1; p < NB - 1; ++p) {  // tiles 1 .. NB-2, one commit group each
-        if (p < nt) stage_rows<RB>(smem + (1 + p) * TILE_BYTES, args.t, (t_begin + p) * NT, args.n_t);
+        if (p < nt) {
+            stage_rows<RB>(smem + (1 + p) * TILE_BYTES, args.t, (t_begin + p) * NT, args.n_t);
+            if (NORMS) stage_norms(sNorm + p * NT, args.norm_t, (t_begin + p) * NT, args.n_t);
+        }
         asm volatile("cp.async.commit_group;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -308,28 +354,22 @@ __global__ void __launch_bounds__(MATCH_THREADS) k_match_rows(const RowScanArgs 
 
     float k1 = -INFINITY, k2 = -INFINITY, m1 = -INFINITY, m2 = -INFINITY;
     int i1 = 0x7fffffff, j1 = 0x7fffffff;
-    Top3 te, to;  // SIM_F16: even and odd column chains
-    top3_init(te);
-    top3_init(to);
+    Top3 tc;  // chunk-level state (CHUNKED)
+    top3_init(tc);
     const float sq = (MODE == SIM_I8 && q0 + rloc < args.n_q) ? args.scale_q[q0 + rloc] : 1.0f;
     bool fail = false;
     int issued = 0;  // MMA groups committed
-    // per-column train values of this warp's chunks (|t|^2 or the int8 scale),
-    // loaded one tile before the tile is reduced
+    // SIM_I8: the int8 scale of this warp's columns, loaded one tile before
+    // the tile is reduced
     int nbv[NT / 64];
-    auto load_nb = [&](int tile) {
+    auto load_scales = [&](int tile) {
 #pragma unroll
         for (int cc = 0; cc < NT / 64; ++cc) {
             const int c = (t_begin + tile) * NT + (half * (NT / 64) + cc) * 32 + lane;
-            if (MODE == SIM_I8)
-                nbv[cc] = __float_as_int(c < args.n_t ? args.scale_t[c] : 1.0f);
-            else if (MODE != SIM_F16)
-                nbv[cc] = __float_as_int((float)(c < args.n_t ? args.norm_t[c] : 0));
-            else
-                nbv[cc] = 0;
+            nbv[cc] = MODE == SIM_I8 ? __float_as_int(c < args.n_t ? args.scale_t[c] : 1.0f) : 0;
         }
     };
-    load_nb(0);
+    if (MODE == SIM_I8) load_scales(0);
     for (int it = 0; it <= nt; ++it) {
         // (1) the MMA of tile it-1 has finished: its train buffer and accumulator are free to read/reuse
         if (it >= 1) {
@@ -341,8 +381,12 @@ __global__ void __launch_bounds__(MATCH_THREADS) k_match_rows(const RowScanArgs 
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         }
         // (2) prefetch train tile it+NB-1 into the buffer tile it-1 used
-        if (it + NB - 1 < nt)
-            stage_rows<RB>(smem + (1 + (it + NB - 1) % NB) * TILE_BYTES, args.t, (t_begin + it + NB - 1) * NT, args.n_t);
+        if (it + NB - 1 < nt) {
+            stage_rows<RB>(smem + (1 + (it + NB - 1) % NB) * TILE_BYTES, args.t, (t_begin + it + NB - 1) * NT,
+                           args.n_t);
+            if (NORMS)
+                stage_norms(sNorm + ((it + NB - 1) % NBN) * NT, args.norm_t, (t_begin + it + NB - 1) * NT, args.n_t);
+        }
         asm volatile("cp.async.commit_group;" ::: "memory");
         // (3) tile it is staged (only the NB-1 newer groups may be pending):
         // issue its MMAs into accumulator it&1
@@ -392,10 +436,10 @@ __global__ void __launch_bounds__(MATCH_THREADS) k_match_rows(const RowScanArgs 
         if (it >= 1) {
             const int tcol0 = (t_begin + it - 1) * NT;
             const int lim_tile = args.n_t - tcol0;
+            const float* nrm = sNorm + ((it - 1) % NBN) * NT;
 #pragma unroll
             for (int cc = 0; cc < NT / 64; ++cc) {
                 const int chunk = half * (NT / 64) + cc;
-                const int nb_lane = nbv[cc];
                 uint32_t v[32];
                 const uint32_t taddr =
                     tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(((it - 1) & 1) * NT + chunk * 32);
@@ -410,13 +454,12 @@ __global__ void __launch_bounds__(MATCH_THREADS) k_match_rows(const RowScanArgs 
                       "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
                     : "r"(taddr));
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                if constexpr (MODE == SIM_F16)
-                    scan_chunk_f16(v, tcol0 + chunk * 32, lim_tile - chunk * 32, te, to);
+                if constexpr (CHUNKED)
+                    top3_push(tc, chunk_max<MODE>(v, lim_tile - chunk * 32, nrm + chunk * 32), tcol0 + chunk * 32);
                 else
-                    scan_chunk<MODE>(v, tcol0 + chunk * 32, lim_tile - chunk * 32, nb_lane, sq, k1, k2, i1, m1, m2,
-                                     j1);
+                    scan_chunk_i8(v, tcol0 + chunk * 32, lim_tile - chunk * 32, nbv[cc], sq, k1, k2, i1, m1, m2, j1);
             }
-            if (it < nt) load_nb(it);  // for the reduction of tile it, one iteration from now
+            if (MODE == SIM_I8 && it < nt) load_scales(it);  // for the reduction of tile it, one iteration from now
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         }
     }
@@ -427,16 +470,15 @@ __global__ void __launch_bounds__(MATCH_THREADS) k_match_rows(const RowScanArgs 
         for (int g = 0; g < issued; ++g) mbar_wait_bounded(&mbar[g & 1], (uint32_t)((g >> 1) & 1));
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
-    // even and odd columns of this thread, then the two column halves of the row
+    // the two column halves of the row
     const int row = q0 + rloc;
-    if constexpr (MODE == SIM_F16) {
-        top3_merge(te, to);
-        if (half == 1) s_half[rloc] = te;
+    if constexpr (CHUNKED) {
+        if (half == 1) s_half[rloc] = tc;
         __syncthreads();
         if (half == 0 && !fail && row < args.n_q) {
-            top3_merge(te, s_half[rloc]);
-            te.pad[0] = te.pad[1] = te.pad[2] = 0;
-            static_cast<Top3*>(args.part)[(size_t)row * gridDim.y + blockIdx.y] = te;
+            top3_merge(tc, s_half[rloc]);
+            tc.pad[0] = tc.pad[1] = tc.pad[2] = 0;
+            static_cast<Top3*>(args.part)[(size_t)row * gridDim.y + blockIdx.y] = tc;
         }
     } else {
         top2_merge(k1, k2, i1, m1, m2, j1);
@@ -466,11 +508,10 @@ __global__ void __launch_bounds__(MATCH_THREADS) k_match_rows(const RowScanArgs 
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * NT));
 }
 
-// Merge the segments of one scan (in index order), ratio test.
-template <int MODE>
-__global__ void k_match_merge(const Top2* __restrict__ part, int n, int nseg, float ratio_sq,
-                              const int* __restrict__ norm_q, int* __restrict__ best, int* __restrict__ pass,
-                              float* __restrict__ dist) {
+// SIM_I8: merge the column-level segments of one scan (in index order),
+// ratio test on the similarities (pysift/core.py:2676-2680, float32).
+__global__ void k_match_merge_i8(const Top2* __restrict__ part, int n, int nseg, float ratio_sq,
+                                 int* __restrict__ best, int* __restrict__ pass, float* __restrict__ dist) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float k1 = -INFINITY, k2 = -INFINITY;
@@ -484,22 +525,89 @@ __global__ void k_match_merge(const Top2* __restrict__ part, int n, int nseg, fl
     int ok = 0;
     float d = 0.0f;
     if (k2 > -INFINITY) {
-        if (MODE == SIM_F16) {
-            // pysift/core.py:2676-2680 (float32)
-            float db = 2.0f - 2.0f * k1;
-            float ds = 2.0f - 2.0f * k2;
-            db = db < 0.0f ? 0.0f : db;
-            ds = ds < 0.0f ? 0.0f : ds;
-            ok = (ds > 1e-10f) && (db < ratio_sq * ds);
-            d = sqrtf(db);
-        } else {
+        float db = 2.0f - 2.0f * k1;
+        float ds = 2.0f - 2.0f * k2;
+        db = db < 0.0f ? 0.0f : db;
+        ds = ds < 0.0f ? 0.0f : ds;
+        ok = (ds > 1e-10f) && (db < ratio_sq * ds);
+        d = sqrtf(db);
+    }
+    best[i] = (k1 > -INFINITY) ? i1 : -1;
+    pass[i] = ok;
+    if (dist) dist[i] = d;
+}
+
+// Warp-wide top-2 of 64-bit keys (larger first): the best and the second
+// (a second copy of the best counts), 0 = none.
+__device__ __forceinline__ void warp_top2_u64(unsigned long long& kb, unsigned long long& ks) {
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long ob = __shfl_xor_sync(FULL_MASK, kb, o), os = __shfl_xor_sync(FULL_MASK, ks, o);
+        ks = max(max(ks, os), min(kb, ob));
+        kb = max(kb, ob);
+    }
+}
+
+// Segments of one chunk-level scan, merged in segment order (every lane
+// reads the same parts).
+__device__ __forceinline__ Top3 merge_parts(const Top3* __restrict__ part, int i, int nseg) {
+    Top3 a;
+    top3_init(a);
+    for (int s_ = 0; s_ < nseg; ++s_) top3_merge(a, part[(size_t)i * nseg + s_]);
+    return a;
+}
+
+// DIST_BF16 / SPLIT_FP8: the best chunk of row i (the first chunk holding
+// the row's largest key) recomputed exactly from the uint8 rows, one warp per
+// row and one column per lane: the best column is the first in that chunk
+// with the chunk's key, and the second key the larger of the chunk's second
+// and the other chunks' largest (a.k2).  Keys 2 a.b - |b|^2 are exact
+// integers on both sides, so the recomputed maximum equals a.k1; a mismatch
+// (or a scan that gave up) leaves the row without a match.
+__global__ void k_match_merge_u8(const Top3* __restrict__ part, int n, int nseg, float ratio_sq,
+                                 const uint8_t* __restrict__ q, const uint8_t* __restrict__ t, int n_t, int D,
+                                 const int* __restrict__ norm_q, const int* __restrict__ norm_t,
+                                 const int* __restrict__ error, int* __restrict__ best, int* __restrict__ pass,
+                                 float* __restrict__ dist) {
+    const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (i >= n) return;
+    const Top3 a = merge_parts(part, i, nseg);
+    const bool bad = *error || !(a.k1 > -INFINITY) || a.i1 < 0 || a.i1 >= n_t;
+    unsigned long long kb = 0, ks = 0;
+    if (!bad) {
+        const int c = a.i1 + lane;
+        if (c < n_t) {
+            const uint4* pq = reinterpret_cast<const uint4*>(q + (size_t)i * D);
+            const uint4* pt = reinterpret_cast<const uint4*>(t + (size_t)c * D);
+            unsigned acc = 0;
+            for (int w = 0; w < D / 16; ++w) {
+                const uint4 x = pq[w], y = pt[w];
+                acc = __dp4a(x.x, y.x, acc);
+                acc = __dp4a(x.y, y.y, acc);
+                acc = __dp4a(x.z, y.z, acc);
+                acc = __dp4a(x.w, y.w, acc);
+            }
+            const int key = 2 * (int)acc - norm_t[c];  // > -2^24
+            // order-preserving bits of the key above the complemented column
+            kb = ((unsigned long long)((unsigned)key ^ 0x80000000u) << 32) | (0xFFFFFFFFu - (unsigned)c);
+        }
+    }
+    warp_top2_u64(kb, ks);
+    if (lane != 0) return;
+    auto key_of = [](unsigned long long k) { return (int)((unsigned)(k >> 32) ^ 0x80000000u); };
+    int ok = 0, b = -1;
+    float d = 0.0f;
+    if (!bad && kb && (float)key_of(kb) == a.k1) {
+        b = (int)(0xFFFFFFFFu - (unsigned)(kb & 0xFFFFFFFFu));
+        float k2 = a.k2;  // the other chunks' largest key (exact)
+        if (ks) k2 = fmaxf(k2, (float)key_of(ks));
+        if (k2 > -INFINITY) {
             const double na = (double)norm_q[i];
-            const double d1 = na - (double)k1, d2 = na - (double)k2;  // exact integers
+            const double d1 = na - (double)a.k1, d2 = na - (double)k2;  // exact integers
             ok = (d2 > 0.0) && (d1 < (double)ratio_sq * d2);
             d = sqrtf((float)d1);
         }
     }
-    best[i] = (k1 > -INFINITY) ? i1 : -1;
+    best[i] = b;
     pass[i] = ok;
     if (dist) dist[i] = d;
 }
@@ -589,46 +697,64 @@ __device__ __forceinline__ void finish_f16_row(int i, float f1, float f2, int c1
     if (dist) dist[i] = d;
 }
 
-// Merge the segments of one SIM_F16 scan (Top3 parts, in segment order),
-// recompute the two candidates exactly and accept the row when no other
-// column can reach them: every other column's fp32 value is <= k3, so its
-// exact value is <= k3 + e and its fp16 similarity <= U = fp16(k3 + e); the
-// row is settled when U <= F2 and U < F1 (a column tying F1 could have a
-// lower index).  Unsettled rows are appended to `recheck` (their order there
-// does not matter: each row's result is computed on its own).
+// Order-preserving bits of a float above the complemented column index: the
+// integer maximum is the largest value with the lowest index.
+__device__ __forceinline__ unsigned long long sim_key(float f, int c) {
+    const unsigned u = __float_as_uint(f);
+    const unsigned ord = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+    return ((unsigned long long)ord << 32) | (0xFFFFFFFFu - (unsigned)c);
+}
+__device__ __forceinline__ float sim_key_value(unsigned long long k) {
+    const unsigned o = (unsigned)(k >> 32);
+    return __uint_as_float((o & 0x80000000u) ? (o & 0x7FFFFFFFu) : ~o);
+}
+__device__ __forceinline__ int sim_key_column(unsigned long long k) {
+    return (int)(0xFFFFFFFFu - (unsigned)(k & 0xFFFFFFFFu));
+}
+
+// Merge the chunk-level segments of one SIM_F16 scan (in segment order) and
+// settle the row from its two best chunks: every column of both is
+// recomputed exactly (one warp per row, a column of each chunk per lane),
+// giving the exact best F1 (lowest index on ties) and second F2 among them.
+// Every column of the other chunks has an fp32 value <= k3 (the third chunk's
+// largest), so its exact value is <= k3 + e and its fp16 similarity
+// <= U = fp16(k3 + e); the row is settled when U <= F2 and U < F1 (a column
+// tying F1 could have a lower index).  Unsettled rows are appended to
+// `recheck` (their order there does not matter: each row's result is
+// computed on its own).
 __global__ void k_match_merge_f16(const Top3* __restrict__ part, int n, int nseg, float ratio_sq,
                                   const __half* __restrict__ q, const __half* __restrict__ t, int n_t, int D,
                                   const float* __restrict__ norm_q, const unsigned* __restrict__ maxnorm_t,
                                   const int* __restrict__ error,
                                   int* __restrict__ best, int* __restrict__ pass, float* __restrict__ dist,
                                   int* __restrict__ recheck, int* __restrict__ n_recheck) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
     if (i >= n) return;
-    Top3 a;
-    top3_init(a);
-    for (int s_ = 0; s_ < nseg; ++s_) top3_merge(a, part[(size_t)i * nseg + s_]);
+    const Top3 a = merge_parts(part, i, nseg);
     // a scan that gave up on its MMA barrier left its parts unwritten: no
-    // result, and no candidate index is trusted
-    const bool i2_ok = a.k2 > -INFINITY && a.i2 >= 0 && a.i2 < n_t;
-    if (*error || a.i1 < 0 || a.i1 >= n_t || (a.k2 > -INFINITY && !i2_ok)) {
-        best[i] = -1;
-        pass[i] = 0;
-        if (dist) dist[i] = 0.0f;
+    // result, and no candidate chunk is trusted
+    const bool c2 = a.k2 > -INFINITY;
+    if (*error || !(a.k1 > -INFINITY) || a.i1 < 0 || a.i1 >= n_t || (c2 && (a.i2 < 0 || a.i2 >= n_t))) {
+        if (lane == 0) {
+            best[i] = -1;
+            pass[i] = 0;
+            if (dist) dist[i] = 0.0f;
+        }
         return;
     }
     const __half* qi = q + (size_t)i * D;
-    float f1 = f16_round_f64(dot_f16_exact(qi, t + (size_t)a.i1 * D, D));
-    int c1 = a.i1;
-    float f2 = -INFINITY;
-    if (a.k2 > -INFINITY) {
-        f2 = f16_round_f64(dot_f16_exact(qi, t + (size_t)a.i2 * D, D));
-        if (f2 > f1 || (f2 == f1 && a.i2 < a.i1)) {
-            const float tf = f1;
-            f1 = f2;
-            f2 = tf;
-            c1 = a.i2;
-        }
+    unsigned long long kb = 0, ks = 0;
+    const int ca = a.i1 + lane, cb = a.i2 + lane;
+    if (ca < n_t) kb = sim_key(f16_round_f64(dot_f16_exact(qi, t + (size_t)ca * D, D)), ca);
+    if (c2 && cb < n_t) {
+        const unsigned long long k = sim_key(f16_round_f64(dot_f16_exact(qi, t + (size_t)cb * D, D)), cb);
+        ks = min(kb, k);
+        kb = max(kb, k);
     }
+    warp_top2_u64(kb, ks);
+    if (lane != 0) return;
+    const float f1 = sim_key_value(kb);
+    const float f2 = ks ? sim_key_value(ks) : -INFINITY;
     if (a.k3 > -INFINITY) {
         const double e = (double)D * 0x1p-21 * (double)norm_q[i] * (double)__uint_as_float(*maxnorm_t);
         const float u = f16_round_f64((double)a.k3 + e);
@@ -637,7 +763,7 @@ __global__ void k_match_merge_f16(const Top3* __restrict__ part, int n, int nseg
             return;
         }
     }
-    finish_f16_row(i, f1, f2, c1, ratio_sq, best, pass, dist);
+    finish_f16_row(i, f1, f2, sim_key_column(kb), ratio_sq, best, pass, dist);
 }
 
 // Rows the merge could not settle: the exact fp16 similarity against every
@@ -667,18 +793,11 @@ __global__ void __launch_bounds__(RECHECK_T) k_match_recheck_f16(const int* __re
         __syncthreads();
         unsigned long long kb = 0, ks = 0;  // best and second keys; 0 = none
         for (int j = threadIdx.x; j < nt; j += blockDim.x) {
-            const float f = f16_round_f64(dot_f16_exact(qrow, t + (size_t)j * D, D));
-            const unsigned u = __float_as_uint(f);
-            const unsigned ord = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
-            const unsigned long long key = ((unsigned long long)ord << 32) | (0xFFFFFFFFu - (unsigned)j);
+            const unsigned long long key = sim_key(f16_round_f64(dot_f16_exact(qrow, t + (size_t)j * D, D)), j);
             ks = max(ks, min(kb, key));
             kb = max(kb, key);
         }
-        for (int o = 16; o > 0; o >>= 1) {
-            const unsigned long long ob = __shfl_xor_sync(FULL_MASK, kb, o), os = __shfl_xor_sync(FULL_MASK, ks, o);
-            ks = max(max(ks, os), min(kb, ob));
-            kb = max(kb, ob);
-        }
+        warp_top2_u64(kb, ks);
         if (lane == 0) {
             s_b[warp] = kb;
             s_s[warp] = ks;
@@ -689,13 +808,9 @@ __global__ void __launch_bounds__(RECHECK_T) k_match_recheck_f16(const int* __re
                 ks = max(max(ks, s_s[w]), min(kb, s_b[w]));
                 kb = max(kb, s_b[w]);
             }
-            auto val = [](unsigned long long k) {
-                const unsigned o = (unsigned)(k >> 32);
-                return __uint_as_float((o & 0x80000000u) ? (o & 0x7FFFFFFFu) : ~o);
-            };
-            const float f1 = val(kb);
-            const float f2 = ks ? val(ks) : -INFINITY;
-            const int c1 = (int)(0xFFFFFFFFu - (unsigned)(kb & 0xFFFFFFFFu));
+            const float f1 = sim_key_value(kb);
+            const float f2 = ks ? sim_key_value(ks) : -INFINITY;
+            const int c1 = sim_key_column(kb);
             if (fwd)
                 finish_f16_row(i, f1, f2, c1, ratio_sq, fbest, fpass, fdist);
             else
@@ -706,24 +821,43 @@ __global__ void __launch_bounds__(RECHECK_T) k_match_recheck_f16(const int* __re
 }
 
 // Mutual matches in query order: fwd[i] = j passes, bwd[j] = i passes.
+// One CTA; each thread owns a run of up to 32 consecutive rows (so the pairs
+// of a thread are consecutive in the output), tests them with its loads
+// issued eight rows at a time, and one block scan of the per-thread counts
+// places them; more than 32 x blockDim rows take several rounds.
 __global__ void __launch_bounds__(1024) k_match_mutual(const int* __restrict__ fbest, const int* __restrict__ fpass,
                                                        const float* __restrict__ fdist, const int* __restrict__ bbest,
                                                        const int* __restrict__ bpass, int n1, int2* __restrict__ pairs,
                                                        float* __restrict__ pdist, int* __restrict__ count) {
     __shared__ int sh[33];
+    const int span = (int)blockDim.x * 32;
     int base = 0;
-    for (int c0 = 0; c0 < n1; c0 += blockDim.x) {
-        const int i = c0 + threadIdx.x;
-        int keep = 0, j = -1;
-        if (i < n1 && fpass[i]) {
-            j = fbest[i];
-            keep = (j >= 0 && bpass[j] && bbest[j] == i) ? 1 : 0;
+    for (int c0 = 0; c0 < n1; c0 += span) {
+        const int per = min(32, ceil_div(min(span, n1 - c0), (int)blockDim.x));
+        const int r0 = c0 + (int)threadIdx.x * per;
+        unsigned mask = 0;
+        for (int k0 = 0; k0 < per; k0 += 8) {
+            int j[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int i = r0 + k0 + u;
+                j[u] = (k0 + u < per && i < n1 && fpass[i]) ? fbest[i] : -1;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int i = r0 + k0 + u;
+                if (j[u] >= 0 && bpass[j[u]] && bbest[j[u]] == i) mask |= 1u << (k0 + u);
+            }
         }
         int tot;
-        const int pos = base + block_excl_scan(keep, &tot, sh);
-        if (keep) {
-            pairs[pos] = make_int2(i, j);
+        int pos = base + block_excl_scan(__popc(mask), &tot, sh);
+        while (mask) {
+            const int k = __ffs(mask) - 1;
+            mask &= mask - 1;
+            const int i = r0 + k;
+            pairs[pos] = make_int2(i, fbest[i]);
             pdist[pos] = fdist[i];
+            ++pos;
         }
         base += tot;
     }
@@ -731,7 +865,7 @@ __global__ void __launch_bounds__(1024) k_match_mutual(const int* __restrict__ f
 }
 
 __global__ void k_row_norms_u8(const uint8_t* __restrict__ d, int n, int D, int* __restrict__ norms,
-                               uint16_t* __restrict__ bf) {
+                               float* __restrict__ fnorms, uint16_t* __restrict__ bf) {
     const int i = blockIdx.x * blockDim.y + threadIdx.y;
     if (i >= n) return;
     int s = 0;
@@ -741,7 +875,10 @@ __global__ void k_row_norms_u8(const uint8_t* __restrict__ d, int n, int D, int*
         if (bf) bf[(size_t)i * D + k] = __bfloat16_as_ushort(__float2bfloat16_rn((float)v));
     }
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(FULL_MASK, s, o);
-    if (threadIdx.x == 0) norms[i] = s;
+    if (threadIdx.x == 0) {
+        norms[i] = s;
+        fnorms[i] = (float)s;  // exact: s < 2^24
+    }
 }
 
 // Split-nibble e4m3 planes of uint8-valued rows, v = 16 h + l with h, l in
@@ -805,9 +942,12 @@ static void scan_split(int n_q, int n_t, int& nseg, int& seg_tiles) {
 
 template <int MODE, int RB>
 static int launch_scan(const RowScanArgs& a, int nseg, cudaStream_t st) {
-    // query block + two train buffers; at least 80 KB so that no more than two
-    // CTAs (2 x 256 tensor-memory columns) share an SM
-    const size_t smem_launch = std::max((size_t)(RB <= 128 ? 4 : 3) * MT * RB, (size_t)80 * 1024);
+    // query block + the train ring + its norms ring (one slot more); at least
+    // 80 KB so that no more than two CTAs (2 x 256 tensor-memory columns)
+    // share an SM
+    constexpr int NB = RB <= 128 ? 3 : 2;
+    const size_t smem_launch =
+        std::max((size_t)(1 + NB) * MT * RB + (size_t)(NB + 1) * NT * sizeof(float), (size_t)80 * 1024);
     PYSIFT_CUDA_TRY(cudaFuncSetAttribute(k_match_rows<MODE, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem_launch));
     dim3 grid(ceil_div(a.n_q, MT), nseg);
@@ -830,7 +970,7 @@ struct MatchLayout {
     // max row norms (set 1, set 2) as float bits
     size_t off_fpart, off_bpart, off_fbest, off_fpass, off_fdist, off_bbest, off_bpass, off_bdist, off_ctl;
     size_t off_rl0, off_rl1, off_nrm;
-    size_t off_na, off_nb, off_bfa, off_bfb, off_qa, off_ta, off_qb, off_tb;
+    size_t off_na, off_nb, off_fna, off_fnb, off_bfa, off_bfb, off_qa, off_ta, off_qb, off_tb;
     size_t total;
 };
 
@@ -844,7 +984,7 @@ static MatchLayout match_layout(int n1, int n2, int D, int exact) {
         return r;
     };
     // segments never exceed the tiles of the other side
-    const size_t part_bytes = exact ? sizeof(Top2) : sizeof(Top3);
+    const size_t part_bytes = sizeof(Top3);
     l.off_fpart = take((size_t)n1 * ceil_div(n2, NT) * part_bytes);
     l.off_bpart = take((size_t)n2 * ceil_div(n1, MT) * part_bytes);
     l.off_fbest = take((size_t)n1 * 4);
@@ -860,10 +1000,13 @@ static MatchLayout match_layout(int n1, int n2, int D, int exact) {
         l.off_rl1 = take((size_t)n2 * 4);
         l.off_nrm = take(((size_t)n1 + n2) * 4);
     }
-    l.off_na = l.off_nb = l.off_bfa = l.off_bfb = l.off_qa = l.off_ta = l.off_qb = l.off_tb = 0;
-    if (exact) {
+    l.off_na = l.off_nb = l.off_fna = l.off_fnb = 0;
+    l.off_bfa = l.off_bfb = l.off_qa = l.off_ta = l.off_qb = l.off_tb = 0;
+    if (exact) {  // |row|^2 as int32 and as float32 (exact: below 2^24)
         l.off_na = take((size_t)n1 * 4);
         l.off_nb = take((size_t)n2 * 4);
+        l.off_fna = take((size_t)n1 * 4);
+        l.off_fnb = take((size_t)n2 * 4);
     }
     if (exact == 1) {
         l.off_bfa = take((size_t)n1 * D * 2);
@@ -886,11 +1029,12 @@ static T* wsp(void* ws, size_t off) {
 
 // a / b: the query-side and train-side rows of each set (the same rows
 // except for the split e4m3 planes, whose two sides differ)
+// (u8a, u8b: the uint8 rows of the exact modes, for the merge's recompute)
 static int run_match(int mode, const uint8_t* a_q, const uint8_t* a_t, int n1, const uint8_t* b_q,
                      const uint8_t* b_t, int n2, int D, float ratio_sq,
                      const MatchLayout& l, void* ws, int* fbest_out, int* fpass_out, int* bbest_out, int* bpass_out,
                      int32_t* pairs, float* pdist, int32_t* count, cudaStream_t st, const float* sa = nullptr,
-                     const float* sb = nullptr) {
+                     const float* sb = nullptr, const uint8_t* u8a = nullptr, const uint8_t* u8b = nullptr) {
     int* ctl = wsp<int>(ws, l.off_ctl);
     int* err = ctl;
     PYSIFT_CUDA_TRY(cudaMemsetAsync(ctl, 0, 8 * sizeof(int), st));
@@ -904,6 +1048,8 @@ static int run_match(int mode, const uint8_t* a_q, const uint8_t* a_t, int n1, c
     const bool sim = mode == SIM_F16 || mode == SIM_I8;
     const int* na = !sim ? wsp<int>(ws, l.off_na) : nullptr;
     const int* nb = !sim ? wsp<int>(ws, l.off_nb) : nullptr;
+    const float* fna = !sim ? wsp<float>(ws, l.off_fna) : nullptr;
+    const float* fnb = !sim ? wsp<float>(ws, l.off_fnb) : nullptr;
     int* fbest = fbest_out ? fbest_out : wsp<int>(ws, l.off_fbest);
     int* fpass = fpass_out ? fpass_out : wsp<int>(ws, l.off_fpass);
     int* bbest = bbest_out ? bbest_out : wsp<int>(ws, l.off_bbest);
@@ -916,7 +1062,7 @@ static int run_match(int mode, const uint8_t* a_q, const uint8_t* a_t, int n1, c
         s.t = dir == 0 ? b_t : a_t;
         s.n_q = dir == 0 ? n1 : n2;
         s.n_t = dir == 0 ? n2 : n1;
-        s.norm_t = dir == 0 ? nb : na;
+        s.norm_t = dir == 0 ? fnb : fna;
         s.scale_q = dir == 0 ? sa : sb;
         s.scale_t = dir == 0 ? sb : sa;
         s.part = wsp<void>(ws, dir == 0 ? l.off_fpart : l.off_bpart);
@@ -925,26 +1071,25 @@ static int run_match(int mode, const uint8_t* a_q, const uint8_t* a_t, int n1, c
         scan_split(s.n_q, s.n_t, nseg, s.seg_tiles);
         const int rc = launch_scan_mode(mode, s, D, nseg, st);
         if (rc) return rc;
-        const int* nq = dir == 0 ? na : nb;
         int* best = dir == 0 ? fbest : bbest;
         int* pass = dir == 0 ? fpass : bpass;
         float* dist = dir == 0 ? fdist : bdist;
         if (mode == SIM_F16) {
-            k_match_merge_f16<<<ceil_div(s.n_q, 128), 128, 0, st>>>(
+            k_match_merge_f16<<<ceil_div(s.n_q, 8), 256, 0, st>>>(
                 static_cast<const Top3*>(s.part), s.n_q, nseg, ratio_sq, dir == 0 ? ha : hb, dir == 0 ? hb : ha,
                 s.n_t, D, wsp<float>(ws, l.off_nrm) + (dir == 0 ? 0 : n1), maxnorm + (dir == 0 ? 1 : 0), err, best,
                 pass, dist,
                 wsp<int>(ws, dir == 0 ? l.off_rl0 : l.off_rl1), ctl + 1 + dir);
             PYSIFT_LAUNCH_CHECK("k_match_merge_f16");
+        } else if (mode == SIM_I8) {
+            k_match_merge_i8<<<ceil_div(s.n_q, 256), 256, 0, st>>>(static_cast<const Top2*>(s.part), s.n_q, nseg,
+                                                                   ratio_sq, best, pass, dist);
+            PYSIFT_LAUNCH_CHECK("k_match_merge_i8");
         } else {
-            const Top2* part = static_cast<const Top2*>(s.part);
-            if (sim)
-                k_match_merge<SIM_F16><<<ceil_div(s.n_q, 256), 256, 0, st>>>(part, s.n_q, nseg, ratio_sq, nq, best,
-                                                                           pass, dist);
-            else
-                k_match_merge<DIST_BF16><<<ceil_div(s.n_q, 256), 256, 0, st>>>(part, s.n_q, nseg, ratio_sq, nq, best,
-                                                                             pass, dist);
-            PYSIFT_LAUNCH_CHECK("k_match_merge");
+            k_match_merge_u8<<<ceil_div(s.n_q, 8), 256, 0, st>>>(
+                static_cast<const Top3*>(s.part), s.n_q, nseg, ratio_sq, dir == 0 ? u8a : u8b, dir == 0 ? u8b : u8a,
+                s.n_t, D, dir == 0 ? na : nb, dir == 0 ? nb : na, err, best, pass, dist);
+            PYSIFT_LAUNCH_CHECK("k_match_merge_u8");
         }
     }
     if (mode == SIM_F16) {
@@ -1009,6 +1154,8 @@ int pysift_match_u8_exact(const uint8_t* d1, int32_t n1, const uint8_t* d2, int3
                           int32_t* pair_count, pysift_stream_t stream) {
     PYSIFT_CHECK_ARG(d1 && d2 && workspace && pairs && pair_dist && pair_count, "NULL pointer argument");
     PYSIFT_CHECK_ARG(n1 >= 1 && n2 >= 1 && (D == 64 || D == 128), "bad sizes (D must be 64 or 128)");
+    PYSIFT_CHECK_ARG((reinterpret_cast<uintptr_t>(d1) & 15) == 0 && (reinterpret_cast<uintptr_t>(d2) & 15) == 0,
+                     "descriptor arrays must be 16-byte aligned");
     MatchLayout l = match_layout(n1, n2, D, 1);
     if (workspace_bytes < l.total) {
         set_error("workspace %zu bytes < required %zu", workspace_bytes, l.total);
@@ -1017,15 +1164,17 @@ int pysift_match_u8_exact(const uint8_t* d1, int32_t n1, const uint8_t* d2, int3
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     uint16_t* bfa = wsp<uint16_t>(workspace, l.off_bfa);
     uint16_t* bfb = wsp<uint16_t>(workspace, l.off_bfb);
-    k_row_norms_u8<<<ceil_div(n1, 8), dim3(32, 8), 0, st>>>(d1, n1, D, wsp<int>(workspace, l.off_na), bfa);
+    k_row_norms_u8<<<ceil_div(n1, 8), dim3(32, 8), 0, st>>>(d1, n1, D, wsp<int>(workspace, l.off_na),
+                                                             wsp<float>(workspace, l.off_fna), bfa);
     PYSIFT_LAUNCH_CHECK("k_row_norms_u8");
-    k_row_norms_u8<<<ceil_div(n2, 8), dim3(32, 8), 0, st>>>(d2, n2, D, wsp<int>(workspace, l.off_nb), bfb);
+    k_row_norms_u8<<<ceil_div(n2, 8), dim3(32, 8), 0, st>>>(d2, n2, D, wsp<int>(workspace, l.off_nb),
+                                                             wsp<float>(workspace, l.off_fnb), bfb);
     PYSIFT_LAUNCH_CHECK("k_row_norms_u8");
     const float ratio_sq = (float)((double)ratio * (double)ratio);
     const uint8_t* a = reinterpret_cast<const uint8_t*>(bfa);
     const uint8_t* b = reinterpret_cast<const uint8_t*>(bfb);
     return run_match(DIST_BF16, a, a, n1, b, b, n2, D, ratio_sq, l, workspace, fwd_best, fwd_pass, bwd_best, bwd_pass,
-                     pairs, pair_dist, pair_count, st);
+                     pairs, pair_dist, pair_count, st, nullptr, nullptr, d1, d2);
 }
 
 int pysift_match_u8_split_fp8(const uint8_t* d1, int32_t n1, const uint8_t* d2, int32_t n2, int32_t D, float ratio,
@@ -1034,15 +1183,19 @@ int pysift_match_u8_split_fp8(const uint8_t* d1, int32_t n1, const uint8_t* d2, 
                               int32_t* pair_count, pysift_stream_t stream) {
     PYSIFT_CHECK_ARG(d1 && d2 && workspace && pairs && pair_dist && pair_count, "NULL pointer argument");
     PYSIFT_CHECK_ARG(n1 >= 1 && n2 >= 1 && (D == 64 || D == 128), "bad sizes (D must be 64 or 128)");
+    PYSIFT_CHECK_ARG((reinterpret_cast<uintptr_t>(d1) & 15) == 0 && (reinterpret_cast<uintptr_t>(d2) & 15) == 0,
+                     "descriptor arrays must be 16-byte aligned");
     MatchLayout l = match_layout(n1, n2, D, 2);
     if (workspace_bytes < l.total) {
         set_error("workspace %zu bytes < required %zu", workspace_bytes, l.total);
         return PYSIFT_ERR_WORKSPACE;
     }
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    k_row_norms_u8<<<ceil_div(n1, 8), dim3(32, 8), 0, st>>>(d1, n1, D, wsp<int>(workspace, l.off_na), nullptr);
+    k_row_norms_u8<<<ceil_div(n1, 8), dim3(32, 8), 0, st>>>(d1, n1, D, wsp<int>(workspace, l.off_na),
+                                                             wsp<float>(workspace, l.off_fna), nullptr);
     PYSIFT_LAUNCH_CHECK("k_row_norms_u8");
-    k_row_norms_u8<<<ceil_div(n2, 8), dim3(32, 8), 0, st>>>(d2, n2, D, wsp<int>(workspace, l.off_nb), nullptr);
+    k_row_norms_u8<<<ceil_div(n2, 8), dim3(32, 8), 0, st>>>(d2, n2, D, wsp<int>(workspace, l.off_nb),
+                                                             wsp<float>(workspace, l.off_fnb), nullptr);
     PYSIFT_LAUNCH_CHECK("k_row_norms_u8");
     uint8_t* qa = wsp<uint8_t>(workspace, l.off_qa);
     uint8_t* ta = wsp<uint8_t>(workspace, l.off_ta);
@@ -1054,7 +1207,7 @@ int pysift_match_u8_split_fp8(const uint8_t* d1, int32_t n1, const uint8_t* d2, 
     PYSIFT_LAUNCH_CHECK("k_split_nibbles_u8");
     const float ratio_sq = (float)((double)ratio * (double)ratio);
     return run_match(SPLIT_FP8, qa, ta, n1, qb, tb, n2, D, ratio_sq, l, workspace, fwd_best, fwd_pass, bwd_best,
-                     bwd_pass, pairs, pair_dist, pair_count, st);
+                     bwd_pass, pairs, pair_dist, pair_count, st, nullptr, nullptr, d1, d2);
 }
 
 int pysift_match_i8(const int8_t* d1, const float* s1, int32_t n1, const int8_t* d2, const float* s2, int32_t n2,
