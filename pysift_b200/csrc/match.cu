@@ -1,15 +1,15 @@
 // match.cu -- brute-force ratio-test matching on the 5th-generation tensor cores.
 //
 // Matching runs as two row scans: queries against the train set (forward
-// top-2) and the train set against the queries (backward top-2).  Each CTA of
-// k_match_rows keeps a 128-row query block resident in shared memory and
-// streams 128-row train tiles through a ring of cp.async buffers (three for
-// 128-byte rows, two for 256-byte rows; no-swizzle
-// K-major core-matrix layout); one thread issues the tcgen05.mma of tile t+1
-// (kind::f16 / f8f6f4 / i8, fp32 or s32 accumulator in tensor memory, two
-// accumulators of 128 columns) while eight warps reduce tile t, read back with
-// tcgen05.ld (two warps per TMEM lane quadrant, each half of the tile's
-// columns).  Train tiles are split into segments so that the grid fills the
+// top-2) and the train set against the queries (backward top-2).  Both sets
+// are first written in a tiled operand layout (128-row tiles of 16 KB slabs
+// in the no-swizzle K-major core-matrix layout).  Each CTA of k_match_rows
+// keeps a 128-row query tile resident in shared memory; a loader thread
+// streams the train slabs into a ring with one bulk copy each, an MMA thread
+// issues tcgen05.mma (kind::f16 / f8f6f4 / i8, fp32 or s32 accumulator in
+// tensor memory, two accumulators of 128 columns) and eight warps reduce the
+// finished accumulator, read back with tcgen05.ld (two warps per TMEM lane
+// quadrant, each half of the tile's columns); mbarriers link the three roles.  Train tiles are split into segments so that the grid fills the
 // SMs; a merge kernel combines the segments of each row and applies the ratio
 // test; k_match_mutual keeps mutual matches (pysift/core.py:2574-2701,
 // 2840-2940).
@@ -59,7 +59,7 @@ namespace pysift {
 constexpr int MT = 128;           // query rows per CTA = UMMA M = TMEM lanes
 constexpr int NT = 128;           // train rows per tile = UMMA N
 constexpr int MATCH_THREADS = 256;  // 2 warps per TMEM lane quadrant, each half the tile's columns
-constexpr unsigned SPIN_LIMIT = 1u << 26;  // bounded waits on the MMA barriers
+constexpr unsigned SPIN_LIMIT = 1u << 22;  // bounded waits on the pipeline barriers
 
 enum MatchMode { SIM_F16 = 0, DIST_BF16 = 1, SPLIT_FP8 = 2, SIM_I8 = 3 };
 
@@ -133,13 +133,6 @@ __device__ __forceinline__ void top3_merge(Top3& a, const Top3& b) {
     a.i2 = r.i2;
 }
 
-// byte offset of 16-byte chunk c (8 elements along K) of row r in the
-// no-swizzle K-major layout: core matrices of 8 rows x 16 bytes, adjacent
-// along K at 128 bytes (LBO), 8-row groups at K/8 * 128 bytes (SBO).
-__device__ __forceinline__ uint32_t core_off(int r, int c, int kchunks) {
-    return (uint32_t)(((r >> 3) * kchunks + c) * 128 + (r & 7) * 16);
-}
-
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
     uint64_t d = 0;
     d |= (uint64_t)((saddr & 0x3FFFF) >> 4);
@@ -167,26 +160,46 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-// Stage rows [row0, row0 + 128) of a row-major matrix of RB-byte rows into
-// the core-matrix layout with cp.async; rows >= n are zero-filled.  A warp
-// moves 8 rows x 4 chunks per instruction: 64 contiguous bytes per row in
-// global memory, 512 contiguous bytes in shared memory.
+// Tiled operand layout (global memory and shared memory alike).  A tile is
+// 128 rows of RB bytes; it is stored as RB / (16 SW) slabs of SW 16-byte
+// chunks along K (SW = min(RB / 16, 8)), each slab in the no-swizzle K-major
+// core-matrix layout: core matrices of 8 rows x 16 bytes, adjacent along K
+// at 128 bytes (LBO), 8-row groups at SW * 128 bytes (SBO).  A slab is one
+// contiguous block, so one bulk copy moves it; rows past the set are zero.
 template <int RB>
-__device__ __forceinline__ void stage_rows(uint8_t* dst, const uint8_t* src, int row0, int n) {
-    constexpr int KC = RB / 16, G = KC / 4;
-    for (int q = threadIdx.x; q < MT * KC; q += MATCH_THREADS) {
-        const int lane = q & 31, blk = q >> 5;
-        const int r = (blk / G) * 8 + (lane & 7), c = (blk % G) * 4 + (lane >> 3);
-        const int gr = row0 + r;
-        const bool valid = gr < n;
-        const uint8_t* s = valid ? src + (size_t)gr * RB + c * 16 : src;
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst + core_off(r, c, KC))),
-                     "l"(s), "r"(valid ? 16 : 0)
-                     : "memory");
-    }
+struct TileGeom {
+    static constexpr int KC = RB / 16;              // 16-byte chunks per row
+    static constexpr int SW = KC < 8 ? KC : 8;      // chunks per slab
+    static constexpr int NSL = KC / SW;             // slabs per tile
+    static constexpr uint32_t SLAB = MT * SW * 16;  // bytes per slab
+    static constexpr uint32_t TILE = MT * RB;       // bytes per tile
+    // slabs in the shared-memory ring: query tile + ring within 96 KB
+    static constexpr int NS = (96 * 1024 - (int)TILE) / (int)SLAB;
+    static_assert(NS >= 2, "ring too small");
+};
+
+// Byte offset of 16-byte chunk c of row r (RB-byte rows) in the tiled layout.
+__host__ __device__ __forceinline__ size_t tiled_off(int r, int c, int RB) {
+    const int KC = RB / 16, SW = KC < 8 ? KC : 8;
+    const int rr = r & (MT - 1), slab = c / SW, cs = c - slab * SW;
+    return (size_t)(r / MT) * MT * RB + (size_t)slab * MT * SW * 16 + (size_t)(((rr >> 3) * SW + cs) * 128 + (rr & 7) * 16);
 }
 
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+// Row-major rows of RB bytes (16-byte aligned) into the tiled layout, rows
+// n .. n_pad-1 zero.  One thread per 16-byte chunk.
+__global__ void k_tile_rows(const uint8_t* __restrict__ src, int n, int n_pad, int RB, uint8_t* __restrict__ dst) {
+    const int KC = RB / 16;
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= (long long)n_pad * KC) return;
+    const int r = (int)(q / KC), c = (int)(q - (long long)r * KC);
+    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+    if (r < n) v = *reinterpret_cast<const uint4*>(src + (size_t)r * RB + (size_t)c * 16);
+    *reinterpret_cast<uint4*>(dst + tiled_off(r, c, RB)) = v;
+}
+
+// Bounded mbarrier wait that also gives up once another role of the CTA has
+// raised the abort flag.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, const volatile int* abort_flag) {
     uint32_t done = 0;
     for (unsigned spins = 0; spins < SPIN_LIMIT; ++spins) {
         asm volatile(
@@ -197,8 +210,31 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
             : "r"(smem_u32(bar)), "r"(parity)
             : "memory");
         if (done) return true;
+        if (abort_flag && *abort_flag) return false;
     }
     return false;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// One contiguous global -> shared bulk copy (no multicast) completing on bar.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+// Arrives on bar once every tcgen05.mma this thread issued before has completed.
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
 }
 
 struct RowScanArgs {
@@ -283,44 +319,34 @@ __device__ __forceinline__ void top2_merge(float& k1, float& k2, int& i1, float 
     k1 = fmaxf(k1, bk1);
 }
 
-// 128 train norms (float) of tile `col0` into a shared slot by cp.async;
-// columns >= n are zero-filled (their keys are excluded anyway).
-__device__ __forceinline__ void stage_norms(float* dst, const float* src, int col0, int n) {
-    const int t = threadIdx.x;
-    if (t < NT / 4) {
-        const int c = col0 + 4 * t;
-        const int valid = c < n ? min(16, (n - c) * 4) : 0;
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst + 4 * t)),
-                     "l"(valid ? src + c : src), "r"(valid)
-                     : "memory");
-    }
-}
+// Warp roles of k_match_rows: warps 0..7 reduce (two per TMEM lane
+// quadrant, each half of a tile's columns), warp 8 lane 0 loads (bulk
+// copies of the query tile and of the train slabs into a ring of NS slabs),
+// warp 9 lane 0 issues the MMAs.  Barriers: full[s] (slab landed), empty[s]
+// (the MMAs reading slab s completed), acc_full[a] (accumulator a holds a
+// finished tile), acc_empty[a] (the reducers have read accumulator a).  No
+// block-wide barrier in the loop; every wait is bounded and gives up once a
+// role raised the abort flag (the scan then reports an error).
+constexpr int EPI_WARPS = MATCH_THREADS / 32;
+constexpr int SCAN_THREADS = MATCH_THREADS + 64;
 
 template <int MODE, int RB>
-__global__ void __launch_bounds__(MATCH_THREADS) k_match_rows(const RowScanArgs args) {
-    constexpr int KC = RB / 16;
-    constexpr uint32_t TILE_BYTES = MT * RB;
-    // train tiles in flight: a 3-deep ring for 128-byte rows (4 tiles in the
-    // 80 KB a CTA is given), 2 for 256-byte rows
-    constexpr int NB = RB <= 128 ? 3 : 2;
+__global__ void __launch_bounds__(SCAN_THREADS, 2) k_match_rows(const RowScanArgs args) {
+    using G = TileGeom<RB>;
+    constexpr int NS = G::NS;
     // SIM_F16, DIST_BF16, SPLIT_FP8: chunk-level state (the key of each
     // 32-column chunk is its largest); SIM_I8: column-level top-2
     constexpr bool CHUNKED = MODE != SIM_I8;
     constexpr bool NORMS = MODE == DIST_BF16 || MODE == SPLIT_FP8;
-    // train norms of a tile are read one iteration after the tile's slot in
-    // the train ring is refilled, so their ring has one slot more
-    constexpr int NBN = NB + 1;
     extern __shared__ __align__(1024) uint8_t smem[];
-    uint8_t* sQ = smem;
-    float* sNorm = reinterpret_cast<float*>(smem + (1 + NB) * TILE_BYTES);  // [NBN][NT]
-    __shared__ __align__(8) uint64_t mbar[2];
+    uint8_t* sQ = smem;                // the query tile (NSL slabs)
+    uint8_t* sRing = smem + G::TILE;   // NS train slabs
+    __shared__ __align__(8) uint64_t bar_full[NS], bar_empty[NS], bar_acc_full[2], bar_acc_empty[2], bar_q, bar_done;
     __shared__ uint32_t tmem_base;
+    __shared__ volatile int s_abort;
+    __shared__ Top3 s_half[MT];  // Top2 in the first 16 bytes for SIM_I8
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int quad = warp & 3, half = warp >> 2;  // TMEM lane quadrant, column half of each tile
-    const int rloc = quad * 32 + lane;            // this thread's query row in the block
-    __shared__ Top3 s_half[MT];  // Top2 in the first 16 bytes for SIM_I8
-    const int q0 = blockIdx.x * MT;
     const int n_tt = (args.n_t + NT - 1) / NT;
     const int t_begin = blockIdx.y * args.seg_tiles;
     const int nt = min(n_tt, t_begin + args.seg_tiles) - t_begin;  // >= 1 by construction
@@ -331,176 +357,197 @@ __global__ void __launch_bounds__(MATCH_THREADS) k_match_rows(const RowScanArgs 
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mbar[0])), "r"(1));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mbar[1])), "r"(1));
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    stage_rows<RB>(sQ, args.q, q0, args.n_q);
-    stage_rows<RB>(smem + TILE_BYTES, args.t, t_begin * NT, args.n_t);
-    if (NORMS) stage_norms(sNorm, args.norm_t, t_begin * NT, args.n_t);
-    asm volatile("cp.async.commit_group;" ::: "memory");
-#pragma unroll
-    for (int p = 1; p < NB - 1; ++p) {  // tiles 1 .. NB-2, one commit group each
-        if (p < nt) {
-            stage_rows<RB>(smem + (1 + p) * TILE_BYTES, args.t, (t_begin + p) * NT, args.n_t);
-            if (NORMS) stage_norms(sNorm + p * NT, args.norm_t, (t_begin + p) * NT, args.n_t);
+        for (int k = 0; k < NS; ++k) {
+            mbar_init(&bar_full[k], 1);
+            mbar_init(&bar_empty[k], 1);
         }
-        asm volatile("cp.async.commit_group;" ::: "memory");
+        for (int k = 0; k < 2; ++k) {
+            mbar_init(&bar_acc_full[k], 1);
+            mbar_init(&bar_acc_empty[k], EPI_WARPS);
+        }
+        mbar_init(&bar_q, 1);
+        mbar_init(&bar_done, 1);
+        s_abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_base;
-
-    float k1 = -INFINITY, k2 = -INFINITY, m1 = -INFINITY, m2 = -INFINITY;
-    int i1 = 0x7fffffff, j1 = 0x7fffffff;
-    Top3 tc;  // chunk-level state (CHUNKED)
-    top3_init(tc);
-    const float sq = (MODE == SIM_I8 && q0 + rloc < args.n_q) ? args.scale_q[q0 + rloc] : 1.0f;
-    bool fail = false;
-    int issued = 0;  // MMA groups committed
-    // SIM_I8: the int8 scale of this warp's columns, loaded one tile before
-    // the tile is reduced
-    int nbv[NT / 64];
-    auto load_scales = [&](int tile) {
-#pragma unroll
-        for (int cc = 0; cc < NT / 64; ++cc) {
-            const int c = (t_begin + tile) * NT + (half * (NT / 64) + cc) * 32 + lane;
-            nbv[cc] = MODE == SIM_I8 ? __float_as_int(c < args.n_t ? args.scale_t[c] : 1.0f) : 0;
-        }
+    auto give_up = [&]() {
+        s_abort = 1;
+        atomicExch(args.error, 1);
     };
-    if (MODE == SIM_I8) load_scales(0);
-    for (int it = 0; it <= nt; ++it) {
-        // (1) the MMA of tile it-1 has finished: its train buffer and accumulator are free to read/reuse
-        if (it >= 1) {
-            const bool ok = mbar_wait_bounded(&mbar[(it - 1) & 1], (uint32_t)(((it - 1) >> 1) & 1));
-            if (__syncthreads_or(!ok)) {
+
+    if (warp == EPI_WARPS) {
+        // ---- loader ----
+        if (lane == 0) {
+            mbar_expect_tx(&bar_q, G::TILE);
+            bulk_load(sQ, args.q + (size_t)blockIdx.x * G::TILE, G::TILE, &bar_q);
+            int issued = 0;  // slabs
+            const int total = nt * G::NSL;
+            for (int k = 0; k < total; ++k) {
+                const int sl = k % NS;
+                if (k >= NS && !mbar_wait_bounded(&bar_empty[sl], (uint32_t)(((k / NS) - 1) & 1), &s_abort)) {
+                    give_up();
+                    break;
+                }
+                const int p = k / G::NSL, j = k - p * G::NSL;
+                mbar_expect_tx(&bar_full[sl], G::SLAB);
+                bulk_load(sRing + (size_t)sl * G::SLAB, args.t + (size_t)(t_begin + p) * G::TILE + (size_t)j * G::SLAB,
+                          G::SLAB, &bar_full[sl]);
+                ++issued;
+            }
+            // the copies in flight land in this CTA's shared memory: let the
+            // last NS of them finish (bounded) before the CTA can exit
+            mbar_wait_bounded(&bar_q, 0u, nullptr);
+            for (int k = max(0, issued - NS); k < issued; ++k)
+                mbar_wait_bounded(&bar_full[k % NS], (uint32_t)((k / NS) & 1), nullptr);
+        }
+    } else if (warp == EPI_WARPS + 1) {
+        // ---- MMA issuer ----
+        if (lane == 0) {
+            constexpr uint32_t idesc = MODE == SIM_I8 ? umma_idesc_s8() : umma_idesc(MODE == DIST_BF16 ? 1 : 0);
+            bool ok = mbar_wait_bounded(&bar_q, 0u, &s_abort);
+            int k = 0;  // slabs consumed
+            for (int p = 0; ok && p < nt; ++p) {
+                const int a = p & 1;
+                if (p >= 2 && !mbar_wait_bounded(&bar_acc_empty[a], (uint32_t)(((p - 2) >> 1) & 1), &s_abort)) {
+                    ok = false;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t d = tmem + (uint32_t)(a * NT);
+                for (int j = 0; j < G::NSL; ++j, ++k) {
+                    const int sl = k % NS;
+                    if (!mbar_wait_bounded(&bar_full[sl], (uint32_t)((k / NS) & 1), &s_abort)) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t a0 = smem_u32(sQ + (size_t)j * G::SLAB), b0 = smem_u32(sRing + (size_t)sl * G::SLAB);
+                    // one MMA covers 32 bytes of K: two core matrices
+#pragma unroll
+                    for (int u = 0; u < G::SW / 2; ++u) {
+                        const uint64_t da = umma_desc(a0 + u * 256, 128, G::SW * 128);
+                        const uint64_t db = umma_desc(b0 + u * 256, 128, G::SW * 128);
+                        const uint32_t acc = (j > 0 || u > 0) ? 1u : 0u;
+                        if (MODE == SIM_I8)
+                            asm volatile(
+                                "{\n\t.reg .pred p;\n\t"
+                                "setp.ne.b32 p, %4, 0;\n\t"
+                                "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+                                "l"(da), "l"(db), "r"(idesc), "r"(acc));
+                        else if (MODE == SPLIT_FP8)
+                            asm volatile(
+                                "{\n\t.reg .pred p;\n\t"
+                                "setp.ne.b32 p, %4, 0;\n\t"
+                                "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+                                "l"(da), "l"(db), "r"(idesc), "r"(acc));
+                        else
+                            asm volatile(
+                                "{\n\t.reg .pred p;\n\t"
+                                "setp.ne.b32 p, %4, 0;\n\t"
+                                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+                                "l"(da), "l"(db), "r"(idesc), "r"(acc));
+                    }
+                    umma_commit(&bar_empty[sl]);  // the slab is free once these MMAs complete
+                }
+                if (!ok) break;
+                umma_commit(&bar_acc_full[a]);
+            }
+            if (!ok) give_up();
+            // every MMA issued has completed before the tensor memory is released
+            umma_commit(&bar_done);
+            mbar_wait_bounded(&bar_done, 0u, nullptr);
+        }
+    } else {
+        // ---- reducers ----
+        const int quad = warp & 3, half = warp >> 2;  // TMEM lane quadrant, column half of each tile
+        const int rloc = quad * 32 + lane;            // this thread's query row in the block
+        const int q0 = blockIdx.x * MT;
+        const float sq = (MODE == SIM_I8 && q0 + rloc < args.n_q) ? args.scale_q[q0 + rloc] : 1.0f;
+        float k1 = -INFINITY, k2 = -INFINITY, m1 = -INFINITY, m2 = -INFINITY;
+        int i1 = 0x7fffffff, j1 = 0x7fffffff;
+        Top3 tc;  // chunk-level state (CHUNKED)
+        top3_init(tc);
+        bool fail = false;
+        for (int p = 0; p < nt; ++p) {
+            const int a = p & 1;
+            if (!mbar_wait_bounded(&bar_acc_full[a], (uint32_t)((p >> 1) & 1), &s_abort)) {
                 fail = true;
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        }
-        // (2) prefetch train tile it+NB-1 into the buffer tile it-1 used
-        if (it + NB - 1 < nt) {
-            stage_rows<RB>(smem + (1 + (it + NB - 1) % NB) * TILE_BYTES, args.t, (t_begin + it + NB - 1) * NT,
-                           args.n_t);
-            if (NORMS)
-                stage_norms(sNorm + ((it + NB - 1) % NBN) * NT, args.norm_t, (t_begin + it + NB - 1) * NT, args.n_t);
-        }
-        asm volatile("cp.async.commit_group;" ::: "memory");
-        // (3) tile it is staged (only the NB-1 newer groups may be pending):
-        // issue its MMAs into accumulator it&1
-        if (it < nt) {
-            asm volatile("cp.async.wait_group %0;" ::"n"(NB - 1) : "memory");
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-            __syncthreads();
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            if (tid == 0) {
-                const uint32_t a0 = smem_u32(sQ), b0 = smem_u32(smem + (1 + it % NB) * TILE_BYTES);
-                const uint32_t d = tmem + (uint32_t)((it & 1) * NT);
-                // f16 / bf16 (kind::f16, format 0 / 1) or e4m3 (kind::f8f6f4, format 0);
-                // either way one MMA covers 32 bytes of K: two core matrices
-                constexpr uint32_t idesc = MODE == SIM_I8 ? umma_idesc_s8() : umma_idesc(MODE == DIST_BF16 ? 1 : 0);
-#pragma unroll
-                for (int s = 0; s < RB / 32; ++s) {
-                    const uint64_t da = umma_desc(a0 + s * 256, 128, KC * 128);
-                    const uint64_t db = umma_desc(b0 + s * 256, 128, KC * 128);
-                    const uint32_t acc = s > 0 ? 1u : 0u;
-                    if (MODE == SIM_I8)
-                        asm volatile(
-                            "{\n\t.reg .pred p;\n\t"
-                            "setp.ne.b32 p, %4, 0;\n\t"
-                            "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
-                            "l"(da), "l"(db), "r"(idesc), "r"(acc));
-                    else if (MODE == SPLIT_FP8)
-                        asm volatile(
-                            "{\n\t.reg .pred p;\n\t"
-                            "setp.ne.b32 p, %4, 0;\n\t"
-                            "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
-                            "l"(da), "l"(db), "r"(idesc), "r"(acc));
-                    else
-                        asm volatile(
-                            "{\n\t.reg .pred p;\n\t"
-                            "setp.ne.b32 p, %4, 0;\n\t"
-                            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
-                            "l"(da), "l"(db), "r"(idesc), "r"(acc));
-                }
-                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                                 smem_u32(&mbar[it & 1]))
-                             : "memory");
-            }
-            ++issued;
-        }
-        // (4) reduce tile it-1 (overlaps the MMA of tile it)
-        if (it >= 1) {
-            const int tcol0 = (t_begin + it - 1) * NT;
+            const int tcol0 = (t_begin + p) * NT;
             const int lim_tile = args.n_t - tcol0;
-            const float* nrm = sNorm + ((it - 1) % NBN) * NT;
-#pragma unroll
-            for (int cc = 0; cc < NT / 64; ++cc) {
-                const int chunk = half * (NT / 64) + cc;
-                uint32_t v[32];
-                const uint32_t taddr =
-                    tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(((it - 1) & 1) * NT + chunk * 32);
-                asm volatile(
-                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-                    "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-                    "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-                      "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
-                      "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]),
-                      "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]),
-                      "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-                    : "r"(taddr));
-                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                if constexpr (CHUNKED)
-                    top3_push(tc, chunk_max<MODE>(v, lim_tile - chunk * 32, nrm + chunk * 32), tcol0 + chunk * 32);
-                else
-                    scan_chunk_i8(v, tcol0 + chunk * 32, lim_tile - chunk * 32, nbv[cc], sq, k1, k2, i1, m1, m2, j1);
-            }
-            if (MODE == SIM_I8 && it < nt) load_scales(it);  // for the reduction of tile it, one iteration from now
+            uint32_t v0[32], v1[32];
+            const uint32_t taddr = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * NT + half * 64);
+#define PYSIFT_TMEM_LD32(V, ADDR)                                                                                 \
+    asm volatile(                                                                                                 \
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "                                                                 \
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"                                                 \
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"                                \
+        : "=r"(V[0]), "=r"(V[1]), "=r"(V[2]), "=r"(V[3]), "=r"(V[4]), "=r"(V[5]), "=r"(V[6]), "=r"(V[7]),        \
+          "=r"(V[8]), "=r"(V[9]), "=r"(V[10]), "=r"(V[11]), "=r"(V[12]), "=r"(V[13]), "=r"(V[14]), "=r"(V[15]), \
+          "=r"(V[16]), "=r"(V[17]), "=r"(V[18]), "=r"(V[19]), "=r"(V[20]), "=r"(V[21]), "=r"(V[22]),           \
+          "=r"(V[23]), "=r"(V[24]), "=r"(V[25]), "=r"(V[26]), "=r"(V[27]), "=r"(V[28]), "=r"(V[29]),           \
+          "=r"(V[30]), "=r"(V[31])                                                                                \
+        : "r"(ADDR))
+            PYSIFT_TMEM_LD32(v0, taddr);
+            PYSIFT_TMEM_LD32(v1, taddr + 32u);
+#undef PYSIFT_TMEM_LD32
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            // the accumulator is read: hand it back to the MMA issuer
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&bar_acc_empty[a]);
+            const int c0 = tcol0 + half * 64;
+            if constexpr (CHUNKED) {
+                const float* nrm = NORMS ? args.norm_t + c0 : nullptr;
+                top3_push(tc, chunk_max<MODE>(v0, lim_tile - half * 64, nrm), c0);
+                top3_push(tc, chunk_max<MODE>(v1, lim_tile - half * 64 - 32, NORMS ? nrm + 32 : nullptr), c0 + 32);
+            } else {
+                const int ca = c0 + lane, cb = c0 + 32 + lane;
+                const int sa = __float_as_int(ca < args.n_t ? args.scale_t[ca] : 1.0f);
+                const int sb = __float_as_int(cb < args.n_t ? args.scale_t[cb] : 1.0f);
+                scan_chunk_i8(v0, c0, lim_tile - half * 64, sa, sq, k1, k2, i1, m1, m2, j1);
+                scan_chunk_i8(v1, c0 + 32, lim_tile - half * 64 - 32, sb, sq, k1, k2, i1, m1, m2, j1);
+            }
         }
-    }
-    if (fail) {
-        // give the MMAs still in flight a bounded chance to finish before the
-        // shared memory and tensor memory they use are released
-        if (tid == 0) atomicExch(args.error, 1);
-        for (int g = 0; g < issued; ++g) mbar_wait_bounded(&mbar[g & 1], (uint32_t)((g >> 1) & 1));
-    }
-    asm volatile("cp.async.wait_all;" ::: "memory");
-    // the two column halves of the row
-    const int row = q0 + rloc;
-    if constexpr (CHUNKED) {
-        if (half == 1) s_half[rloc] = tc;
-        __syncthreads();
-        if (half == 0 && !fail && row < args.n_q) {
-            top3_merge(tc, s_half[rloc]);
-            tc.pad[0] = tc.pad[1] = tc.pad[2] = 0;
-            static_cast<Top3*>(args.part)[(size_t)row * gridDim.y + blockIdx.y] = tc;
-        }
-    } else {
-        top2_merge(k1, k2, i1, m1, m2, j1);
-        Top2* sh2 = reinterpret_cast<Top2*>(&s_half[rloc]);
-        if (half == 1) {
-            Top2 h;
-            h.k1 = k1;
-            h.k2 = k2;
-            h.i1 = i1;
-            h.pad = 0;
-            *sh2 = h;
-        }
-        __syncthreads();
-        if (half == 0 && !fail && row < args.n_q) {
-            const Top2 h = *sh2;
-            top2_merge(k1, k2, i1, h.k1, h.k2, h.i1);
-            Top2 r;
-            r.k1 = k1;
-            r.k2 = k2;
-            r.i1 = i1;
-            r.pad = 0;
-            static_cast<Top2*>(args.part)[(size_t)row * gridDim.y + blockIdx.y] = r;
+        if (fail) give_up();
+        // the two column halves of the row (named barrier over the reducers)
+        const int row = q0 + rloc;
+        if constexpr (CHUNKED) {
+            if (half == 1) s_half[rloc] = tc;
+            asm volatile("bar.sync 1, %0;" ::"n"(MATCH_THREADS) : "memory");
+            if (half == 0 && !s_abort && row < args.n_q) {
+                top3_merge(tc, s_half[rloc]);
+                tc.pad[0] = tc.pad[1] = tc.pad[2] = 0;
+                static_cast<Top3*>(args.part)[(size_t)row * gridDim.y + blockIdx.y] = tc;
+            }
+        } else {
+            top2_merge(k1, k2, i1, m1, m2, j1);
+            Top2* sh2 = reinterpret_cast<Top2*>(&s_half[rloc]);
+            if (half == 1) {
+                Top2 h;
+                h.k1 = k1;
+                h.k2 = k2;
+                h.i1 = i1;
+                h.pad = 0;
+                *sh2 = h;
+            }
+            asm volatile("bar.sync 1, %0;" ::"n"(MATCH_THREADS) : "memory");
+            if (half == 0 && !s_abort && row < args.n_q) {
+                const Top2 h = *sh2;
+                top2_merge(k1, k2, i1, h.k1, h.k2, h.i1);
+                Top2 r;
+                r.k1 = k1;
+                r.k2 = k2;
+                r.i1 = i1;
+                r.pad = 0;
+                static_cast<Top2*>(args.part)[(size_t)row * gridDim.y + blockIdx.y] = r;
+            }
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -864,20 +911,25 @@ __global__ void __launch_bounds__(1024) k_match_mutual(const int* __restrict__ f
     if (threadIdx.x == 0) *count = base;
 }
 
-__global__ void k_row_norms_u8(const uint8_t* __restrict__ d, int n, int D, int* __restrict__ norms,
-                               float* __restrict__ fnorms, uint16_t* __restrict__ bf) {
+// |row|^2 of uint8 rows (int32 for the merge, float32 for the scan; exact:
+// below 2^24) and, with bf, the rows as bf16 in the tiled layout.  Rows
+// n .. n_pad-1 get a zero float norm and zero bf16 rows.
+__global__ void k_row_norms_u8(const uint8_t* __restrict__ d, int n, int n_pad, int D, int* __restrict__ norms,
+                               float* __restrict__ fnorms, uint8_t* __restrict__ bf) {
     const int i = blockIdx.x * blockDim.y + threadIdx.y;
-    if (i >= n) return;
+    if (i >= n_pad) return;
     int s = 0;
     for (int k = threadIdx.x; k < D; k += 32) {
-        const int v = d[(size_t)i * D + k];
+        const int v = i < n ? d[(size_t)i * D + k] : 0;
         s += v * v;
-        if (bf) bf[(size_t)i * D + k] = __bfloat16_as_ushort(__float2bfloat16_rn((float)v));
+        if (bf)
+            *reinterpret_cast<uint16_t*>(bf + tiled_off(i, k >> 3, 2 * D) + ((2 * k) & 15)) =
+                __bfloat16_as_ushort(__float2bfloat16_rn((float)v));
     }
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(FULL_MASK, s, o);
     if (threadIdx.x == 0) {
-        norms[i] = s;
-        fnorms[i] = (float)s;  // exact: s < 2^24
+        if (i < n) norms[i] = s;
+        fnorms[i] = (float)s;
     }
 }
 
@@ -886,27 +938,29 @@ __global__ void k_row_norms_u8(const uint8_t* __restrict__ d, int n, int D, int*
 // [16h | h | 16l | l], the train-side row [16h | 16l | h | l], each plane D
 // bytes, so that the 4D-long dot product of the two is
 // 256 h.h' + 16 h.l' + 16 l.h' + l.l' = v.v', the four nibble GEMMs in one.
-__global__ void k_split_nibbles_u8(const uint8_t* __restrict__ d, int n, int D, uint8_t* __restrict__ qside,
-                                   uint8_t* __restrict__ tside) {
+// Both sides are written in the tiled layout of 4D-byte rows; rows
+// n .. n_pad-1 are zero.
+__global__ void k_split_nibbles_u8(const uint8_t* __restrict__ d, int n, int n_pad, int D,
+                                   uint8_t* __restrict__ qside, uint8_t* __restrict__ tside) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (size_t)n * D) return;
-    const size_t r = i / D, k = i - r * D;
-    const int v = d[i];
+    if (i >= (size_t)n_pad * D) return;
+    const int r = (int)(i / D), k = (int)(i - (size_t)r * D);
+    const int v = r < n ? d[i] : 0;
     const float h = (float)(v >> 4), l = (float)(v & 15);
     const uint8_t e16h = __nv_cvt_float_to_fp8(16.0f * h, __NV_SATFINITE, __NV_E4M3);
     const uint8_t eh = __nv_cvt_float_to_fp8(h, __NV_SATFINITE, __NV_E4M3);
     const uint8_t e16l = __nv_cvt_float_to_fp8(16.0f * l, __NV_SATFINITE, __NV_E4M3);
     const uint8_t el = __nv_cvt_float_to_fp8(l, __NV_SATFINITE, __NV_E4M3);
-    uint8_t* q = qside + r * 4 * D;
-    uint8_t* t = tside + r * 4 * D;
-    q[k] = e16h;
-    q[D + k] = eh;
-    q[2 * D + k] = e16l;
-    q[3 * D + k] = el;
-    t[k] = e16h;
-    t[D + k] = e16l;
-    t[2 * D + k] = eh;
-    t[3 * D + k] = el;
+    const int RB = 4 * D;
+    auto at = [&](int byte) { return tiled_off(r, byte >> 4, RB) + (byte & 15); };
+    qside[at(k)] = e16h;
+    qside[at(D + k)] = eh;
+    qside[at(2 * D + k)] = e16l;
+    qside[at(3 * D + k)] = el;
+    tside[at(k)] = e16h;
+    tside[at(D + k)] = e16l;
+    tside[at(2 * D + k)] = eh;
+    tside[at(3 * D + k)] = el;
 }
 
 static int sm_count() {
@@ -942,16 +996,14 @@ static void scan_split(int n_q, int n_t, int& nseg, int& seg_tiles) {
 
 template <int MODE, int RB>
 static int launch_scan(const RowScanArgs& a, int nseg, cudaStream_t st) {
-    // query block + the train ring + its norms ring (one slot more); at least
-    // 80 KB so that no more than two CTAs (2 x 256 tensor-memory columns)
-    // share an SM
-    constexpr int NB = RB <= 128 ? 3 : 2;
-    const size_t smem_launch =
-        std::max((size_t)(1 + NB) * MT * RB + (size_t)(NB + 1) * NT * sizeof(float), (size_t)80 * 1024);
+    // query tile + the slab ring: about 96 KB, so that no more than two CTAs
+    // (2 x 256 tensor-memory columns) share an SM
+    using G = TileGeom<RB>;
+    const size_t smem_launch = std::max((size_t)G::TILE + (size_t)G::NS * G::SLAB, (size_t)80 * 1024);
     PYSIFT_CUDA_TRY(cudaFuncSetAttribute(k_match_rows<MODE, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem_launch));
     dim3 grid(ceil_div(a.n_q, MT), nseg);
-    k_match_rows<MODE, RB><<<grid, MATCH_THREADS, smem_launch, st>>>(a);
+    k_match_rows<MODE, RB><<<grid, SCAN_THREADS, smem_launch, st>>>(a);
     PYSIFT_LAUNCH_CHECK("k_match_rows");
     return PYSIFT_OK;
 }
@@ -970,11 +1022,19 @@ struct MatchLayout {
     // max row norms (set 1, set 2) as float bits
     size_t off_fpart, off_bpart, off_fbest, off_fpass, off_fdist, off_bbest, off_bpass, off_bdist, off_ctl;
     size_t off_rl0, off_rl1, off_nrm;
-    size_t off_na, off_nb, off_fna, off_fnb, off_bfa, off_bfb, off_qa, off_ta, off_qb, off_tb;
+    size_t off_na, off_nb, off_fna, off_fnb;
+    // the scan operands in the tiled layout (rows padded to whole tiles):
+    // query side and train side of each set (the same buffer except for the
+    // split e4m3 planes)
+    size_t off_qa, off_ta, off_qb, off_tb;
     size_t total;
 };
 
-// exact: 0 = fp16 similarity, 1 = exact via bf16, 2 = exact via split e4m3
+static int pad_rows(int n) { return ceil_div(n, MT) * MT; }
+
+// exact: 0 = fp16 similarity (and int8 similarity, whose D-byte rows fit in
+// its buffers), 1 = exact via bf16, 2 = exact via split e4m3 (scan row
+// bytes: 2 D, 2 D, 4 D)
 static MatchLayout match_layout(int n1, int n2, int D, int exact) {
     MatchLayout l;
     size_t off = 0;
@@ -995,28 +1055,26 @@ static MatchLayout match_layout(int n1, int n2, int D, int exact) {
     l.off_bdist = take((size_t)n2 * 4);
     l.off_ctl = take(8 * sizeof(int));
     l.off_rl0 = l.off_rl1 = l.off_nrm = 0;
-    if (!exact) {
+    if (exact == 0) {
         l.off_rl0 = take((size_t)n1 * 4);
         l.off_rl1 = take((size_t)n2 * 4);
         l.off_nrm = take(((size_t)n1 + n2) * 4);
     }
     l.off_na = l.off_nb = l.off_fna = l.off_fnb = 0;
-    l.off_bfa = l.off_bfb = l.off_qa = l.off_ta = l.off_qb = l.off_tb = 0;
-    if (exact) {  // |row|^2 as int32 and as float32 (exact: below 2^24)
+    if (exact == 1 || exact == 2) {  // |row|^2 as int32 and (padded) as float32
         l.off_na = take((size_t)n1 * 4);
         l.off_nb = take((size_t)n2 * 4);
-        l.off_fna = take((size_t)n1 * 4);
-        l.off_fnb = take((size_t)n2 * 4);
+        l.off_fna = take((size_t)pad_rows(n1) * 4);
+        l.off_fnb = take((size_t)pad_rows(n2) * 4);
     }
-    if (exact == 1) {
-        l.off_bfa = take((size_t)n1 * D * 2);
-        l.off_bfb = take((size_t)n2 * D * 2);
-    }
+    const size_t rb = exact == 2 ? 4 * (size_t)D : 2 * (size_t)D;
+    l.off_qa = take((size_t)pad_rows(n1) * rb);
+    l.off_qb = take((size_t)pad_rows(n2) * rb);
+    l.off_ta = l.off_qa;
+    l.off_tb = l.off_qb;
     if (exact == 2) {
-        l.off_qa = take((size_t)n1 * D * 4);
-        l.off_ta = take((size_t)n1 * D * 4);
-        l.off_qb = take((size_t)n2 * D * 4);
-        l.off_tb = take((size_t)n2 * D * 4);
+        l.off_ta = take((size_t)pad_rows(n1) * rb);
+        l.off_tb = take((size_t)pad_rows(n2) * rb);
     }
     l.total = off;
     return l;
@@ -1029,27 +1087,53 @@ static T* wsp(void* ws, size_t off) {
 
 // a / b: the query-side and train-side rows of each set (the same rows
 // except for the split e4m3 planes, whose two sides differ)
-// (u8a, u8b: the uint8 rows of the exact modes, for the merge's recompute)
-static int run_match(int mode, const uint8_t* a_q, const uint8_t* a_t, int n1, const uint8_t* b_q,
-                     const uint8_t* b_t, int n2, int D, float ratio_sq,
+// rows_a, rows_b: the row-major descriptor sets as the caller passed them
+// (fp16, uint8 or int8 rows, 16-byte aligned); the scan operands are built
+// from them in the workspace in the tiled layout.
+static int run_match(int mode, const uint8_t* rows_a, int n1, const uint8_t* rows_b, int n2, int D, float ratio_sq,
                      const MatchLayout& l, void* ws, int* fbest_out, int* fpass_out, int* bbest_out, int* bpass_out,
                      int32_t* pairs, float* pdist, int32_t* count, cudaStream_t st, const float* sa = nullptr,
-                     const float* sb = nullptr, const uint8_t* u8a = nullptr, const uint8_t* u8b = nullptr) {
+                     const float* sb = nullptr) {
     int* ctl = wsp<int>(ws, l.off_ctl);
     int* err = ctl;
     PYSIFT_CUDA_TRY(cudaMemsetAsync(ctl, 0, 8 * sizeof(int), st));
-    const __half* ha = reinterpret_cast<const __half*>(a_q);
-    const __half* hb = reinterpret_cast<const __half*>(b_q);
+    const __half* ha = reinterpret_cast<const __half*>(rows_a);
+    const __half* hb = reinterpret_cast<const __half*>(rows_b);
     unsigned* maxnorm = reinterpret_cast<unsigned*>(ctl + 3);
+    uint8_t* qa = wsp<uint8_t>(ws, l.off_qa);
+    uint8_t* ta = wsp<uint8_t>(ws, l.off_ta);
+    uint8_t* qb = wsp<uint8_t>(ws, l.off_qb);
+    uint8_t* tb = wsp<uint8_t>(ws, l.off_tb);
+    const int p1 = pad_rows(n1), p2 = pad_rows(n2);
+    const bool sim = mode == SIM_F16 || mode == SIM_I8;
+    int* na = !sim ? wsp<int>(ws, l.off_na) : nullptr;
+    int* nb = !sim ? wsp<int>(ws, l.off_nb) : nullptr;
+    float* fna = !sim ? wsp<float>(ws, l.off_fna) : nullptr;
+    float* fnb = !sim ? wsp<float>(ws, l.off_fnb) : nullptr;
+    if (sim) {
+        const int rb = mode == SIM_F16 ? 2 * D : D;
+        k_tile_rows<<<(unsigned)ceil_div_ll((long long)p1 * (rb / 16), 256), 256, 0, st>>>(rows_a, n1, p1, rb, qa);
+        PYSIFT_LAUNCH_CHECK("k_tile_rows");
+        k_tile_rows<<<(unsigned)ceil_div_ll((long long)p2 * (rb / 16), 256), 256, 0, st>>>(rows_b, n2, p2, rb, qb);
+        PYSIFT_LAUNCH_CHECK("k_tile_rows");
+    } else {
+        k_row_norms_u8<<<ceil_div(p1, 8), dim3(32, 8), 0, st>>>(rows_a, n1, p1, D, na, fna,
+                                                                 mode == DIST_BF16 ? qa : nullptr);
+        PYSIFT_LAUNCH_CHECK("k_row_norms_u8");
+        k_row_norms_u8<<<ceil_div(p2, 8), dim3(32, 8), 0, st>>>(rows_b, n2, p2, D, nb, fnb,
+                                                                 mode == DIST_BF16 ? qb : nullptr);
+        PYSIFT_LAUNCH_CHECK("k_row_norms_u8");
+        if (mode == SPLIT_FP8) {
+            k_split_nibbles_u8<<<(unsigned)ceil_div_ll((long long)p1 * D, 256), 256, 0, st>>>(rows_a, n1, p1, D, qa, ta);
+            PYSIFT_LAUNCH_CHECK("k_split_nibbles_u8");
+            k_split_nibbles_u8<<<(unsigned)ceil_div_ll((long long)p2 * D, 256), 256, 0, st>>>(rows_b, n2, p2, D, qb, tb);
+            PYSIFT_LAUNCH_CHECK("k_split_nibbles_u8");
+        }
+    }
     if (mode == SIM_F16) {
         k_f16_max_norms<<<ceil_div(n1 + n2, 8), 256, 0, st>>>(ha, n1, hb, n2, D, maxnorm, wsp<float>(ws, l.off_nrm));
         PYSIFT_LAUNCH_CHECK("k_f16_max_norms");
     }
-    const bool sim = mode == SIM_F16 || mode == SIM_I8;
-    const int* na = !sim ? wsp<int>(ws, l.off_na) : nullptr;
-    const int* nb = !sim ? wsp<int>(ws, l.off_nb) : nullptr;
-    const float* fna = !sim ? wsp<float>(ws, l.off_fna) : nullptr;
-    const float* fnb = !sim ? wsp<float>(ws, l.off_fnb) : nullptr;
     int* fbest = fbest_out ? fbest_out : wsp<int>(ws, l.off_fbest);
     int* fpass = fpass_out ? fpass_out : wsp<int>(ws, l.off_fpass);
     int* bbest = bbest_out ? bbest_out : wsp<int>(ws, l.off_bbest);
@@ -1058,8 +1142,8 @@ static int run_match(int mode, const uint8_t* a_q, const uint8_t* a_t, int n1, c
     float* bdist = wsp<float>(ws, l.off_bdist);
     for (int dir = 0; dir < 2; ++dir) {
         RowScanArgs s;
-        s.q = dir == 0 ? a_q : b_q;
-        s.t = dir == 0 ? b_t : a_t;
+        s.q = dir == 0 ? qa : qb;
+        s.t = dir == 0 ? tb : ta;
         s.n_q = dir == 0 ? n1 : n2;
         s.n_t = dir == 0 ? n2 : n1;
         s.norm_t = dir == 0 ? fnb : fna;
@@ -1087,8 +1171,8 @@ static int run_match(int mode, const uint8_t* a_q, const uint8_t* a_t, int n1, c
             PYSIFT_LAUNCH_CHECK("k_match_merge_i8");
         } else {
             k_match_merge_u8<<<ceil_div(s.n_q, 8), 256, 0, st>>>(
-                static_cast<const Top3*>(s.part), s.n_q, nseg, ratio_sq, dir == 0 ? u8a : u8b, dir == 0 ? u8b : u8a,
-                s.n_t, D, dir == 0 ? na : nb, dir == 0 ? nb : na, err, best, pass, dist);
+                static_cast<const Top3*>(s.part), s.n_q, nseg, ratio_sq, dir == 0 ? rows_a : rows_b,
+                dir == 0 ? rows_b : rows_a, s.n_t, D, dir == 0 ? na : nb, dir == 0 ? nb : na, err, best, pass, dist);
             PYSIFT_LAUNCH_CHECK("k_match_merge_u8");
         }
     }
@@ -1134,8 +1218,8 @@ int pysift_match_fp16(const uint16_t* d1, int32_t n1, const uint16_t* d2, int32_
     const float ratio_sq = (float)((double)ratio * (double)ratio);
     const uint8_t* a = reinterpret_cast<const uint8_t*>(d1);
     const uint8_t* b = reinterpret_cast<const uint8_t*>(d2);
-    return run_match(SIM_F16, a, a, n1, b, b, n2, D, ratio_sq, l, workspace, fwd_best, fwd_pass, bwd_best, bwd_pass,
-                     pairs, pair_dist, pair_count, reinterpret_cast<cudaStream_t>(stream));
+    return run_match(SIM_F16, a, n1, b, n2, D, ratio_sq, l, workspace, fwd_best, fwd_pass, bwd_best, bwd_pass, pairs,
+                     pair_dist, pair_count, reinterpret_cast<cudaStream_t>(stream));
 }
 
 int pysift_match_fp16_recheck_counts(const void* workspace, int32_t n1, int32_t n2, int32_t D, int32_t* counts,
@@ -1161,20 +1245,9 @@ int pysift_match_u8_exact(const uint8_t* d1, int32_t n1, const uint8_t* d2, int3
         set_error("workspace %zu bytes < required %zu", workspace_bytes, l.total);
         return PYSIFT_ERR_WORKSPACE;
     }
-    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    uint16_t* bfa = wsp<uint16_t>(workspace, l.off_bfa);
-    uint16_t* bfb = wsp<uint16_t>(workspace, l.off_bfb);
-    k_row_norms_u8<<<ceil_div(n1, 8), dim3(32, 8), 0, st>>>(d1, n1, D, wsp<int>(workspace, l.off_na),
-                                                             wsp<float>(workspace, l.off_fna), bfa);
-    PYSIFT_LAUNCH_CHECK("k_row_norms_u8");
-    k_row_norms_u8<<<ceil_div(n2, 8), dim3(32, 8), 0, st>>>(d2, n2, D, wsp<int>(workspace, l.off_nb),
-                                                             wsp<float>(workspace, l.off_fnb), bfb);
-    PYSIFT_LAUNCH_CHECK("k_row_norms_u8");
     const float ratio_sq = (float)((double)ratio * (double)ratio);
-    const uint8_t* a = reinterpret_cast<const uint8_t*>(bfa);
-    const uint8_t* b = reinterpret_cast<const uint8_t*>(bfb);
-    return run_match(DIST_BF16, a, a, n1, b, b, n2, D, ratio_sq, l, workspace, fwd_best, fwd_pass, bwd_best, bwd_pass,
-                     pairs, pair_dist, pair_count, st, nullptr, nullptr, d1, d2);
+    return run_match(DIST_BF16, d1, n1, d2, n2, D, ratio_sq, l, workspace, fwd_best, fwd_pass, bwd_best, bwd_pass,
+                     pairs, pair_dist, pair_count, reinterpret_cast<cudaStream_t>(stream));
 }
 
 int pysift_match_u8_split_fp8(const uint8_t* d1, int32_t n1, const uint8_t* d2, int32_t n2, int32_t D, float ratio,
@@ -1190,24 +1263,9 @@ int pysift_match_u8_split_fp8(const uint8_t* d1, int32_t n1, const uint8_t* d2, 
         set_error("workspace %zu bytes < required %zu", workspace_bytes, l.total);
         return PYSIFT_ERR_WORKSPACE;
     }
-    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    k_row_norms_u8<<<ceil_div(n1, 8), dim3(32, 8), 0, st>>>(d1, n1, D, wsp<int>(workspace, l.off_na),
-                                                             wsp<float>(workspace, l.off_fna), nullptr);
-    PYSIFT_LAUNCH_CHECK("k_row_norms_u8");
-    k_row_norms_u8<<<ceil_div(n2, 8), dim3(32, 8), 0, st>>>(d2, n2, D, wsp<int>(workspace, l.off_nb),
-                                                             wsp<float>(workspace, l.off_fnb), nullptr);
-    PYSIFT_LAUNCH_CHECK("k_row_norms_u8");
-    uint8_t* qa = wsp<uint8_t>(workspace, l.off_qa);
-    uint8_t* ta = wsp<uint8_t>(workspace, l.off_ta);
-    uint8_t* qb = wsp<uint8_t>(workspace, l.off_qb);
-    uint8_t* tb = wsp<uint8_t>(workspace, l.off_tb);
-    k_split_nibbles_u8<<<(unsigned)ceil_div_ll((long long)n1 * D, 256), 256, 0, st>>>(d1, n1, D, qa, ta);
-    PYSIFT_LAUNCH_CHECK("k_split_nibbles_u8");
-    k_split_nibbles_u8<<<(unsigned)ceil_div_ll((long long)n2 * D, 256), 256, 0, st>>>(d2, n2, D, qb, tb);
-    PYSIFT_LAUNCH_CHECK("k_split_nibbles_u8");
     const float ratio_sq = (float)((double)ratio * (double)ratio);
-    return run_match(SPLIT_FP8, qa, ta, n1, qb, tb, n2, D, ratio_sq, l, workspace, fwd_best, fwd_pass, bwd_best,
-                     bwd_pass, pairs, pair_dist, pair_count, st, nullptr, nullptr, d1, d2);
+    return run_match(SPLIT_FP8, d1, n1, d2, n2, D, ratio_sq, l, workspace, fwd_best, fwd_pass, bwd_best, bwd_pass,
+                     pairs, pair_dist, pair_count, reinterpret_cast<cudaStream_t>(stream));
 }
 
 int pysift_match_i8(const int8_t* d1, const float* s1, int32_t n1, const int8_t* d2, const float* s2, int32_t n2,
@@ -1226,8 +1284,8 @@ int pysift_match_i8(const int8_t* d1, const float* s1, int32_t n1, const int8_t*
     const float ratio_sq = (float)((double)ratio * (double)ratio);
     const uint8_t* a = reinterpret_cast<const uint8_t*>(d1);
     const uint8_t* b = reinterpret_cast<const uint8_t*>(d2);
-    return run_match(SIM_I8, a, a, n1, b, b, n2, D, ratio_sq, l, workspace, fwd_best, fwd_pass, bwd_best, bwd_pass,
-                     pairs, pair_dist, pair_count, reinterpret_cast<cudaStream_t>(stream), s1, s2);
+    return run_match(SIM_I8, a, n1, b, n2, D, ratio_sq, l, workspace, fwd_best, fwd_pass, bwd_best, bwd_pass, pairs,
+                     pair_dist, pair_count, reinterpret_cast<cudaStream_t>(stream), s1, s2);
 }
 
 }  // extern "C"
