@@ -596,10 +596,27 @@ __device__ __forceinline__ void warp_top2_u64(unsigned long long& kb, unsigned l
 
 // Segments of one chunk-level scan, merged in segment order (every lane
 // reads the same parts).
+__device__ __forceinline__ Top3 shfl_xor_top3(const Top3& t, int o) {
+    Top3 r;
+    r.k1 = __shfl_xor_sync(FULL_MASK, t.k1, o);
+    r.k2 = __shfl_xor_sync(FULL_MASK, t.k2, o);
+    r.k3 = __shfl_xor_sync(FULL_MASK, t.k3, o);
+    r.i1 = __shfl_xor_sync(FULL_MASK, t.i1, o);
+    r.i2 = __shfl_xor_sync(FULL_MASK, t.i2, o);
+    return r;
+}
+
+// The segments of one row merged by the whole warp: lane s loads parts s,
+// s + 32, ... (all loads in flight at once), then a butterfly of top3_merge
+// leaves the union in every lane.  The union's two first entries in
+// (key desc, first column asc) order and its third key do not depend on the
+// order of the merges.
 __device__ __forceinline__ Top3 merge_parts(const Top3* __restrict__ part, int i, int nseg) {
+    const int lane = threadIdx.x & 31;
     Top3 a;
     top3_init(a);
-    for (int s_ = 0; s_ < nseg; ++s_) top3_merge(a, part[(size_t)i * nseg + s_]);
+    for (int s_ = lane; s_ < nseg; s_ += 32) top3_merge(a, part[(size_t)i * nseg + s_]);
+    for (int o = 16; o > 0; o >>= 1) top3_merge(a, shfl_xor_top3(a, o));
     return a;
 }
 
