@@ -242,6 +242,16 @@ int pysift_l2_normalize_rows(const float* in, int32_t n, int32_t D, float* out, 
 int pysift_pca_workspace_size(int32_t n, int32_t D, size_t* bytes);
 int pysift_pca_stats(const float* x, int32_t n, int32_t D, void* workspace, size_t workspace_bytes, float* mean,
                      double* cov, pysift_stream_t stream);
+/* PCA basis from a D x D float64 covariance (D even, <= 128), replacing the
+ * reference's cp.linalg.eigh (pysift/core.py:2729-2736): proj (device,
+ * float32 D x P, row-major) receives the eigenvectors of the P largest
+ * eigenvalues in ascending eigenvalue order (as eigh's v[:, -P:]), found by
+ * a round-robin parallel Jacobi in float64 on the device (sweeps until no
+ * off-diagonal element exceeds 2^-60 trace; sweeps, if not NULL, a device
+ * int32 receiving their count).  Workspace: pysift_pca_basis_workspace_size. */
+int pysift_pca_basis_workspace_size(int32_t D, size_t* bytes);
+int pysift_pca_basis(const double* cov, int32_t D, int32_t P, void* workspace, size_t workspace_bytes, float* proj,
+                     int32_t* sweeps, pysift_stream_t stream);
 int pysift_pca_project_f16(const float* x, int32_t n, int32_t D, const float* mean, const float* proj, int32_t P,
                            uint16_t* out, pysift_stream_t stream);
 int pysift_to_f16(const float* in, int64_t n, uint16_t* out, pysift_stream_t stream);

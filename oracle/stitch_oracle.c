@@ -435,6 +435,114 @@ EXPORT void orc_pca_stats(const float* x, long n, int D, float* mean, double* co
 }
 
 /* projection + normalisation; output float32 (the caller rounds to fp16) */
+/* ------------------------------------------------------------------ */
+/* PCA basis (pysift/core.py:2729-2736 takes cp.linalg.eigh of the      */
+/* covariance and keeps the eigenvectors of the P largest eigenvalues). */
+/* Canonical: round-robin parallel cyclic Jacobi on the D x D float64    */
+/* covariance (D even).  Round r = 0..D-2 rotates the D/2 disjoint      */
+/* pairs {D-1, r} and {(r+i) mod (D-1), (r-i) mod (D-1)}, i = 1..D/2-1  */
+/* (p < q); every angle comes from the matrix at the start of the round */
+/* and only pairs with |a_pq| > tol rotate, tol = 2^-60 trace (the       */
+/* trace summed in index order): all column rotations, then all row     */
+/* rotations and the eigenvector columns.  Sweeps stop once no upper    */
+/* off-diagonal element exceeds tol (60 at most).  The basis is the      */
+/* eigenvectors of the last P indices in (eigenvalue asc, index asc)    */
+/* order, in that order (as eigh's v[:, -P:]), rounded to float32.      */
+/* The device kernel k_pca_basis performs the same operations.          */
+/* ------------------------------------------------------------------ */
+static void pca_pair(int D, int rnd, int i, int* p, int* q) {
+    int a, b;
+    if (i == 0) {
+        a = D - 1;
+        b = rnd;
+    } else {
+        a = (rnd + i) % (D - 1);
+        b = (rnd - i + (D - 1)) % (D - 1);
+    }
+    *p = a < b ? a : b;
+    *q = a < b ? b : a;
+}
+
+EXPORT int orc_pca_basis(const double* cov, int D, int P, float* proj, int* sweeps_out) {
+    if (D < 2 || D > 128 || (D & 1) || P < 1 || P > D) return -1;
+    static double A[128][128], V[128][128];
+    double cs[64][2];
+    int act[64], pq[64][2];
+    for (int r = 0; r < D; ++r)
+        for (int c = 0; c < D; ++c) {
+            A[r][c] = cov[(long)r * D + c];
+            V[r][c] = r == c ? 1.0 : 0.0;
+        }
+    double tr = 0.0;
+    for (int k = 0; k < D; ++k) tr = tr + A[k][k];
+    const double tol = tr * 0x1p-60;
+    int sweep = 0;
+    for (; sweep < 60; ++sweep) {
+        int any = 0;
+        for (int r = 0; r < D && !any; ++r)
+            for (int c = r + 1; c < D; ++c)
+                if (fabs(A[r][c]) > tol) {
+                    any = 1;
+                    break;
+                }
+        if (!any) break;
+        for (int rnd = 0; rnd < D - 1; ++rnd) {
+            for (int j = 0; j < D / 2; ++j) {
+                int p, q;
+                pca_pair(D, rnd, j, &p, &q);
+                pq[j][0] = p;
+                pq[j][1] = q;
+                const double apq = A[p][q];
+                act[j] = 0;
+                if (fabs(apq) > tol) {
+                    const double app = A[p][p], aqq = A[q][q];
+                    const double theta = (aqq - app) / (2.0 * apq);
+                    const double tt = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                    const double c = 1.0 / sqrt(tt * tt + 1.0);
+                    cs[j][0] = c;
+                    cs[j][1] = tt * c;
+                    act[j] = 1;
+                }
+            }
+            for (int j = 0; j < D / 2; ++j) {
+                if (!act[j]) continue;
+                const int p = pq[j][0], q = pq[j][1];
+                const double c = cs[j][0], s = cs[j][1];
+                for (int k = 0; k < D; ++k) {
+                    const double mkp = A[k][p], mkq = A[k][q];
+                    A[k][p] = c * mkp - s * mkq;
+                    A[k][q] = s * mkp + c * mkq;
+                }
+            }
+            for (int j = 0; j < D / 2; ++j) {
+                if (!act[j]) continue;
+                const int p = pq[j][0], q = pq[j][1];
+                const double c = cs[j][0], s = cs[j][1];
+                for (int k = 0; k < D; ++k) {
+                    const double mpk = A[p][k], mqk = A[q][k];
+                    A[p][k] = c * mpk - s * mqk;
+                    A[q][k] = s * mpk + c * mqk;
+                    const double vkp = V[k][p], vkq = V[k][q];
+                    V[k][p] = c * vkp - s * vkq;
+                    V[k][q] = s * vkp + c * vkq;
+                }
+            }
+        }
+    }
+    /* rank of each index in (eigenvalue asc, index asc) order */
+    int order[128];
+    for (int i = 0; i < D; ++i) {
+        int rk = 0;
+        for (int j = 0; j < D; ++j)
+            if (A[j][j] < A[i][i] || (A[j][j] == A[i][i] && j < i)) ++rk;
+        order[rk] = i;
+    }
+    for (int k = 0; k < D; ++k)
+        for (int c = 0; c < P; ++c) proj[(long)k * P + c] = (float)V[k][order[D - P + c]];
+    if (sweeps_out) *sweeps_out = sweep;
+    return 0;
+}
+
 EXPORT void orc_pca_project(const float* x, long n, int D, const float* mean, const float* proj, int P, float* out) {
     #pragma omp parallel for schedule(static)
     for (long r = 0; r < n; ++r) {

@@ -24,6 +24,8 @@ def _setup():
     L.orc_dlt.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
     L.orc_l2_normalize.argtypes = [ctypes.c_void_p, ctypes.c_long, ctypes.c_int, ctypes.c_void_p]
     L.orc_pca_stats.argtypes = [ctypes.c_void_p, ctypes.c_long, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    L.orc_pca_basis.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    L.orc_pca_basis.restype = ctypes.c_int
     L.orc_pca_project.argtypes = [ctypes.c_void_p, ctypes.c_long, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                   ctypes.c_int, ctypes.c_void_p]
     L.orc_warp_feather.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
@@ -81,6 +83,20 @@ def pca_stats(x):
     cov = np.empty((D, D), np.float64)
     L.orc_pca_stats(_p(x), x.shape[0], D, _p(mean), _p(cov))
     return mean, cov
+
+
+def pca_basis(cov, P, return_sweeps=False):
+    """(D, P) float32 basis of the P largest eigenvalues of the float64
+    covariance by the canonical parallel Jacobi (stitch_oracle.c:
+    orc_pca_basis; the reference takes cp.linalg.eigh, pysift/core.py:2734)."""
+    L = _setup()
+    cov = np.ascontiguousarray(cov, np.float64)
+    D = cov.shape[0]
+    out = np.empty((D, P), np.float32)
+    sw = ctypes.c_int(0)
+    if L.orc_pca_basis(_p(cov), D, P, _p(out), ctypes.byref(sw)) != 0:
+        raise ValueError("pca_basis: D must be even and <= 128, 1 <= P <= D")
+    return (out, sw.value) if return_sweeps else out
 
 
 def pca_project(x, mean, proj):
@@ -175,8 +191,7 @@ class OracleStitch:
         both = np.concatenate([l2_normalize(d1), l2_normalize(d2)])
         if self.pca is None:
             mean, cov = pca_stats(both)
-            w, v = np.linalg.eigh(cov)
-            self.pca = (mean, np.ascontiguousarray(v[:, -self.pca_dims:].astype(np.float32)))
+            self.pca = (mean, pca_basis(cov, self.pca_dims))
         p = pca_project(both, *self.pca)
         if not self.int8_matching:
             p = p.astype(np.float16)

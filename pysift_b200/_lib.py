@@ -166,6 +166,8 @@ EXPORTS.update({
     "pysift_gather_points": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_void_p, c_void_p]),
     "pysift_l2_normalize_rows": (ctypes.c_int, [c_void_p, c_int32, c_int32, c_void_p, c_void_p]),
     "pysift_pca_workspace_size": (ctypes.c_int, [c_int32, c_int32, ctypes.POINTER(c_size_t)]),
+    "pysift_pca_basis_workspace_size": (ctypes.c_int, [c_int32, ctypes.POINTER(c_size_t)]),
+    "pysift_pca_basis": (ctypes.c_int, [c_void_p, c_int32, c_int32, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p]),
     "pysift_pca_stats": (ctypes.c_int, [c_void_p, c_int32, c_int32, c_void_p, c_size_t, c_void_p, c_void_p,
                                         c_void_p]),
     "pysift_pca_project_f16": (ctypes.c_int, [c_void_p, c_int32, c_int32, c_void_p, c_void_p, c_int32, c_void_p,

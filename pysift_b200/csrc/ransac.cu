@@ -510,8 +510,8 @@ __global__ void __launch_bounds__(RT) k_ransac_select(const RansacArgs a) {
     __shared__ double s_M[45];
     __shared__ double s_H[9], s_Hi[9], s_H1[9];
     __shared__ int s_best;
-    __shared__ double s_bscore[RT];
-    __shared__ int s_bidx[RT];
+    __shared__ double s_bscore[RT / 32];
+    __shared__ int s_bidx[RT / 32];
     // argmax, lowest index on ties
     double bs = -INFINITY;
     int bi = 0x7fffffff;
@@ -522,13 +522,25 @@ __global__ void __launch_bounds__(RT) k_ransac_select(const RansacArgs a) {
             bi = h;
         }
     }
-    s_bscore[threadIdx.x] = bs;
-    s_bidx[threadIdx.x] = bi;
+    // (score desc, index asc) is a total order on the non-NaN candidates the
+    // threads kept, so a shuffle tree gives the serial scan's choice
+    for (int o = 16; o > 0; o >>= 1) {
+        const double ov = __shfl_xor_sync(FULL_MASK, bs, o);
+        const int oi = __shfl_xor_sync(FULL_MASK, bi, o);
+        if (ov > bs || (ov == bs && oi < bi)) {
+            bs = ov;
+            bi = oi;
+        }
+    }
+    if ((threadIdx.x & 31) == 0) {
+        s_bscore[threadIdx.x >> 5] = bs;
+        s_bidx[threadIdx.x >> 5] = bi;
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
         double B = s_bscore[0];
         int I = s_bidx[0];
-        for (int t = 1; t < RT; ++t)
+        for (int t = 1; t < RT / 32; ++t)
             if (s_bscore[t] > B || (s_bscore[t] == B && s_bidx[t] < I)) {
                 B = s_bscore[t];
                 I = s_bidx[t];
@@ -772,6 +784,134 @@ struct RansacLayout {
     size_t off_prep, off_p1n, off_p2n, off_hyp, off_score, off_idx, total;
 };
 
+// PCA basis (pysift/core.py:2729-2736: cp.linalg.eigh of the covariance,
+// the eigenvectors of the P largest eigenvalues).  Round-robin parallel
+// cyclic Jacobi on the D x D float64 covariance in one CTA (D even, <= 128):
+// round r = 0..D-2 rotates the D/2 disjoint pairs {D-1, r} and
+// {(r+i) mod (D-1), (r-i) mod (D-1)}, i = 1..D/2-1 (p < q); every angle comes
+// from the matrix at the start of the round and only pairs with
+// |a_pq| > tol = 2^-60 trace rotate; all column rotations, then all row
+// rotations and the eigenvector columns.  Sweeps stop once no upper
+// off-diagonal element exceeds tol (60 at most).  The basis is the
+// eigenvectors of the last P indices in (eigenvalue asc, index asc) order,
+// in that order (as eigh's v[:, -P:]), rounded to float32.  A lives in
+// shared memory, V in the caller's workspace.
+__device__ __forceinline__ void pca_pair(int D, int rnd, int i, int* p, int* q) {
+    int a, b;
+    if (i == 0) {
+        a = D - 1;
+        b = rnd;
+    } else {
+        a = (rnd + i) % (D - 1);
+        b = (rnd - i + (D - 1)) % (D - 1);
+    }
+    *p = a < b ? a : b;
+    *q = a < b ? b : a;
+}
+
+constexpr int PCA_BT = 1024;
+
+__global__ void __launch_bounds__(PCA_BT) k_pca_basis(const double* __restrict__ cov, int D, int P,
+                                                       double* __restrict__ V, float* __restrict__ proj,
+                                                       int* __restrict__ sweeps_out) {
+    extern __shared__ __align__(16) double A[];  // D x D
+    __shared__ double s_cs[64][2];
+    __shared__ int s_pq[64][2];
+    __shared__ int s_act[64];
+    __shared__ int s_order[128];
+    __shared__ double s_tol;
+    const int tid = threadIdx.x, nt = blockDim.x, npair = D / 2;
+    for (int it = tid; it < D * D; it += nt) {
+        A[it] = cov[it];
+        V[it] = (it / D == it % D) ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double tr = 0.0;
+        for (int k = 0; k < D; ++k) tr = tr + A[k * D + k];
+        s_tol = tr * 0x1p-60;
+    }
+    __syncthreads();
+    const double tol = s_tol;
+    int sweep = 0;
+    for (; sweep < 60; ++sweep) {
+        int any = 0;
+        for (int it = tid; it < D * D; it += nt) {
+            const int r = it / D, c = it - r * D;
+            if (c > r && fabs(A[it]) > tol) any = 1;
+        }
+        if (!__syncthreads_or(any)) break;
+        for (int rnd = 0; rnd < D - 1; ++rnd) {
+            if (tid < npair) {
+                int p, q;
+                pca_pair(D, rnd, tid, &p, &q);
+                s_pq[tid][0] = p;
+                s_pq[tid][1] = q;
+                const double apq = A[p * D + q];
+                int act = 0;
+                if (fabs(apq) > tol) {
+                    const double app = A[p * D + p], aqq = A[q * D + q];
+                    const double theta = (aqq - app) / (2.0 * apq);
+                    const double tt = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                    const double c = 1.0 / sqrt(tt * tt + 1.0);
+                    s_cs[tid][0] = c;
+                    s_cs[tid][1] = tt * c;
+                    act = 1;
+                }
+                s_act[tid] = act;
+            }
+            __syncthreads();
+            // column rotations: item = (row k, pair j), pairs adjacent
+            for (int it = tid; it < D * npair; it += nt) {
+                const int k = it / npair, j = it - k * npair;
+                if (!s_act[j]) continue;
+                const int p = s_pq[j][0], q = s_pq[j][1];
+                const double c = s_cs[j][0], s = s_cs[j][1];
+                const double mkp = A[k * D + p], mkq = A[k * D + q];
+                A[k * D + p] = c * mkp - s * mkq;
+                A[k * D + q] = s * mkp + c * mkq;
+            }
+            __syncthreads();
+            // row rotations: item = (pair j, column k), columns adjacent
+            for (int it = tid; it < npair * D; it += nt) {
+                const int j = it / D, k = it - j * D;
+                if (!s_act[j]) continue;
+                const int p = s_pq[j][0], q = s_pq[j][1];
+                const double c = s_cs[j][0], s = s_cs[j][1];
+                const double mpk = A[p * D + k], mqk = A[q * D + k];
+                A[p * D + k] = c * mpk - s * mqk;
+                A[q * D + k] = s * mpk + c * mqk;
+            }
+            // eigenvector columns: item = (row k, pair j)
+            for (int it = tid; it < D * npair; it += nt) {
+                const int k = it / npair, j = it - k * npair;
+                if (!s_act[j]) continue;
+                const int p = s_pq[j][0], q = s_pq[j][1];
+                const double c = s_cs[j][0], s = s_cs[j][1];
+                const double vkp = V[k * D + p], vkq = V[k * D + q];
+                V[k * D + p] = c * vkp - s * vkq;
+                V[k * D + q] = s * vkp + c * vkq;
+            }
+            __syncthreads();
+        }
+    }
+    if (tid < D) {
+        const double v = A[tid * D + tid];
+        int rk = 0;
+        for (int j = 0; j < D; ++j) {
+            const double w = A[j * D + j];
+            if (w < v || (w == v && j < tid)) ++rk;
+        }
+        s_order[rk] = tid;
+    }
+    __syncthreads();
+    for (int it = tid; it < D * P; it += nt) {
+        const int k = it / P, c = it - k * P;
+        proj[it] = (float)V[k * D + s_order[D - P + c]];
+    }
+    if (tid == 0 && sweeps_out) *sweeps_out = sweep;
+}
+
 static RansacLayout ransac_layout(int n, int n_hyp) {
     RansacLayout l;
     size_t off = 0;
@@ -958,6 +1098,34 @@ int pysift_pca_stats(const float* x, int32_t n, int32_t D, void* workspace, size
     PYSIFT_LAUNCH_CHECK("k_pca_cov_part");
     k_pca_cov_final<<<ceil_div(D * D, 256), 256, 0, st>>>(cpart, nchunks, n, D, cov);
     PYSIFT_LAUNCH_CHECK("k_pca_cov_final");
+    return PYSIFT_OK;
+}
+
+int pysift_pca_basis_workspace_size(int32_t D, size_t* bytes) {
+    PYSIFT_CHECK_ARG(bytes != nullptr, "bytes is NULL");
+    PYSIFT_CHECK_ARG(D >= 2 && D <= 128 && (D & 1) == 0, "D must be even and <= 128");
+    *bytes = align_up((size_t)D * D * sizeof(double), 256) + 256;
+    return PYSIFT_OK;
+}
+
+int pysift_pca_basis(const double* cov, int32_t D, int32_t P, void* workspace, size_t workspace_bytes, float* proj,
+                     int32_t* sweeps, pysift_stream_t stream) {
+    PYSIFT_CHECK_ARG(cov && workspace && proj, "NULL pointer argument");
+    PYSIFT_CHECK_ARG(D >= 2 && D <= 128 && (D & 1) == 0, "D must be even and <= 128");
+    PYSIFT_CHECK_ARG(P >= 1 && P <= D, "P must be in 1..D");
+    size_t need = 0;
+    pysift_pca_basis_workspace_size(D, &need);
+    if (workspace_bytes < need) {
+        set_error("workspace %zu bytes < required %zu", workspace_bytes, need);
+        return PYSIFT_ERR_WORKSPACE;
+    }
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const size_t smem = (size_t)D * D * sizeof(double);
+    PYSIFT_CUDA_TRY(cudaFuncSetAttribute(k_pca_basis, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int* sw = reinterpret_cast<int*>(static_cast<char*>(workspace) + align_up((size_t)D * D * sizeof(double), 256));
+    k_pca_basis<<<1, PCA_BT, smem, st>>>(cov, D, P, static_cast<double*>(workspace), proj, sw);
+    PYSIFT_LAUNCH_CHECK("k_pca_basis");
+    if (sweeps) PYSIFT_CUDA_TRY(cudaMemcpyAsync(sweeps, sw, sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
     return PYSIFT_OK;
 }
 

@@ -210,11 +210,15 @@ class GPUPyStitch:
             ws = torch.empty(int(sz.value), dtype=torch.uint8, device=self.device)
             _lib.check(lib.pysift_pca_stats(both.data_ptr(), n1 + n2, D, ws.data_ptr(), ws.numel(), mean.data_ptr(),
                                             cov.data_ptr(), st), "pysift_pca_stats")
-            # one 128x128 symmetric eigendecomposition per instance (LAPACK),
-            # the basis cached like the reference's (pysift/core.py:2729-2736)
-            w, v = np.linalg.eigh(cov.cpu().numpy())
-            proj = np.ascontiguousarray(v[:, -P:].astype(np.float32))
-            self._pca_matrix = torch.from_numpy(proj).to(self.device)
+            # one 128x128 symmetric eigendecomposition per instance (parallel
+            # Jacobi on the device), the basis cached like the reference's
+            # (pysift/core.py:2729-2736)
+            proj = torch.empty((D, P), dtype=torch.float32, device=self.device)
+            _lib.check(lib.pysift_pca_basis_workspace_size(D, ctypes.byref(sz)), "pysift_pca_basis_workspace_size")
+            wsb = torch.empty(int(sz.value), dtype=torch.uint8, device=self.device)
+            _lib.check(lib.pysift_pca_basis(cov.data_ptr(), D, P, wsb.data_ptr(), wsb.numel(), proj.data_ptr(), None,
+                                            st), "pysift_pca_basis")
+            self._pca_matrix = proj
             self._pca_mean = mean
         if self.int8_matching:
             outf = torch.empty((n1 + n2, P), dtype=torch.float32, device=self.device)

@@ -73,9 +73,16 @@ def test_matcher_preparation_bit_exact():
     rmean, rcov = so.pca_stats(ref)
     assert np.array_equal(mean.cpu().numpy(), rmean)
     assert np.array_equal(cov.cpu().numpy(), rcov)
-    w, v = np.linalg.eigh(rcov)
-    proj = np.ascontiguousarray(v[:, -64:].astype(np.float32))
-    pj = torch.from_numpy(proj).cuda()
+    # the basis: the device Jacobi equals the oracle's bit for bit
+    proj = so.pca_basis(rcov, 64)
+    pj = torch.empty((128, 64), dtype=torch.float32, device="cuda")
+    assert lib.pysift_pca_basis_workspace_size(128, ctypes.byref(sz)) == 0
+    wsb = torch.empty(sz.value, dtype=torch.uint8, device="cuda")
+    sweeps = torch.zeros(1, dtype=torch.int32, device="cuda")
+    assert lib.pysift_pca_basis(cov.data_ptr(), 128, 64, wsb.data_ptr(), wsb.numel(), pj.data_ptr(),
+                                sweeps.data_ptr(), _st()) == 0
+    assert np.array_equal(pj.cpu().numpy(), proj)
+    assert so.pca_basis(rcov, 64, return_sweeps=True)[1] == int(sweeps.item())
     o16 = torch.empty((3000, 64), dtype=torch.float16, device="cuda")
     assert lib.pysift_pca_project_f16(out.data_ptr(), 3000, 128, mean.data_ptr(), pj.data_ptr(), 64, o16.data_ptr(),
                                       _st()) == 0

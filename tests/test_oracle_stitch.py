@@ -7,6 +7,9 @@
 * RANSAC (pysift/core.py:3011-3097, MAGSAC++ and classic scores): on
   correspondences with a known homography, sub-pixel noise and planted
   outliers, the oracle recovers the homography and keeps no planted outlier.
+* PCA basis (pysift/core.py:2729-2736 takes cp.linalg.eigh): the oracle's
+  parallel Jacobi spans the same top-P eigenvectors as LAPACK's eigh, in the
+  same order, to float32 rounding.
 """
 import numpy as np
 import pytest
@@ -67,3 +70,20 @@ def test_ransac_oracle_recovers_the_homography(seed, magsac):
     corners = np.array([[0, 0, 1], [1280, 0, 1], [1280, 960, 1], [0, 960, 1]], np.float64).T
     pa, pb = H @ corners, Ht @ corners
     assert np.max(np.abs(pa[:2] / pa[2] - pb[:2] / pb[2])) < 2.0
+
+
+@pytest.mark.parametrize("seed,n,D,P", [(0, 16000, 128, 64), (1, 3000, 128, 32), (2, 500, 64, 64)])
+def test_pca_basis_spans_the_eigh_subspace(seed, n, D, P):
+    rng = np.random.default_rng(seed)
+    x = np.abs(rng.standard_normal((n, D))).astype(np.float32) ** 2
+    x /= np.linalg.norm(x, axis=1, keepdims=True)
+    _, cov = so.pca_stats(x)
+    basis, sweeps = so.pca_basis(cov, P, return_sweeps=True)
+    assert basis.shape == (D, P) and basis.dtype == np.float32 and 0 < sweeps < 60
+    w, v = np.linalg.eigh(cov)
+    m = np.abs(basis.astype(np.float64).T @ v[:, -P:])
+    # unit columns, orthogonal, each the eigh eigenvector of the same rank (up to sign)
+    assert np.abs(np.diag(m) - 1.0).max() < 1e-6
+    assert (m - np.diag(np.diag(m))).max() < 1e-5
+    # and the projections the matcher uses agree to float32 rounding
+    assert np.abs(x @ basis - x @ v[:, -P:].astype(np.float32) * np.sign(np.diag(basis.T @ v[:, -P:]))).max() < 1e-5
