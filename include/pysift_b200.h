@@ -187,9 +187,9 @@ int pysift_match_fp16(const uint16_t* d1, int32_t n1, const uint16_t* d2, int32_
 int pysift_match_fp16_recheck_counts(const void* workspace, int32_t n1, int32_t n2, int32_t D, int32_t* counts,
                                      pysift_stream_t stream);
 
-/* Exact squared L2 of uint8-valued descriptors (16-byte aligned rows) via
- * bf16 products (exact for D <= 128), pass iff d2^2 > 0 and
- * d1^2 < ratio^2 d2^2. */
+/* Exact squared L2 of uint8 descriptors (16-byte aligned rows) via unsigned
+ * 8-bit tensor-core products with 32-bit integer accumulation (exact for
+ * D <= 128), pass iff d2^2 > 0 and d1^2 < ratio^2 d2^2. */
 int pysift_match_u8_exact(const uint8_t* d1, int32_t n1, const uint8_t* d2, int32_t n2, int32_t D, float ratio,
                           void* workspace, size_t workspace_bytes, int32_t* fwd_best, int32_t* fwd_pass,
                           int32_t* bwd_best, int32_t* bwd_pass, int32_t* pairs, float* pair_dist,

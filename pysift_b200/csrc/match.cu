@@ -32,9 +32,9 @@
 //             other chunks can reach the exact second value
 //             (fp16(third chunk key + e) <= second, and < best); the other rows
 //             are recomputed over every column by k_match_recheck_f16.
-//   DIST_BF16 exact L2 on uint8-valued descriptors: bf16 holds 0..255 exactly and
-//             every partial sum of 128 products stays below 2^24, so the fp32
-//             accumulator is the exact integer dot product.  Rows rank train
+//   DIST_U8   exact L2 on uint8 descriptors: kind::i8 with unsigned 8-bit
+//             operands and an s32 accumulator gives the exact integer dot
+//             product (below 128 * 255^2 < 2^24).  Rows rank train
 //             entries by 2 a.b - |b|^2 (exact in fp32: |2 a.b| < 2^24), which orders
 //             them as -|a - b|^2; d^2 = |a|^2 - key, pass iff d2^2 > 0 and
 //             d1^2 < r^2 d2^2 (exact).  The merge recomputes the best chunk
@@ -48,6 +48,7 @@
 // train entries in increasing index order and replaces the best only on a
 // strictly larger key; segments merge in index order.
 #include <algorithm>
+#include <climits>
 #include <cstdint>
 
 #include "common.cuh"
@@ -61,7 +62,7 @@ constexpr int NT = 128;           // train rows per tile = UMMA N
 constexpr int MATCH_THREADS = 256;  // 2 warps per TMEM lane quadrant, each half the tile's columns
 constexpr unsigned SPIN_LIMIT = 1u << 22;  // bounded waits on the pipeline barriers
 
-enum MatchMode { SIM_F16 = 0, DIST_BF16 = 1, SPLIT_FP8 = 2, SIM_I8 = 3 };
+enum MatchMode { SIM_F16 = 0, DIST_U8 = 1, SPLIT_FP8 = 2, SIM_I8 = 3 };
 
 struct Top2 {  // best key and index, second-best key
     float k1, k2;
@@ -150,10 +151,11 @@ __host__ __device__ constexpr uint32_t umma_idesc(int ab_format) {
            ((uint32_t)(MT >> 4) << 24);
 }
 
-// kind::i8 instruction descriptor: D = s32 (2), A/B = signed 8-bit (1),
-// both K-major, N = 128, M = 128.
-__host__ __device__ constexpr uint32_t umma_idesc_s8() {
-    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NT >> 3) << 17) | ((uint32_t)(MT >> 4) << 24);
+// kind::i8 instruction descriptor: D = s32 (2), A/B = signed (1) or
+// unsigned (0) 8-bit, both K-major, N = 128, M = 128.
+__host__ __device__ constexpr uint32_t umma_idesc_i8(bool is_signed) {
+    return (2u << 4) | ((is_signed ? 1u : 0u) << 7) | ((is_signed ? 1u : 0u) << 10) | ((uint32_t)(NT >> 3) << 17) |
+           ((uint32_t)(MT >> 4) << 24);
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -238,10 +240,11 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
 }
 
 struct RowScanArgs {
-    const uint8_t* q;    // n_q rows of RB bytes (fp16 / bf16 / e4m3 codes)
+    const uint8_t* q;    // n_q rows of RB bytes (fp16 / uint8 / int8 / e4m3 codes), tiled
     const uint8_t* t;    // n_t rows of RB bytes
     int n_q, n_t;
-    const float* norm_t;   // DIST_BF16 / SPLIT_FP8: |t|^2 per train row (exact in float32)
+    const float* norm_t;   // SPLIT_FP8: |t|^2 per train row (exact in float32), padded to whole tiles
+    const int* norm_ti;    // DIST_U8: |t|^2 per train row as int32, padded to whole tiles
     const float* scale_q;  // SIM_I8: quantisation scale per query row
     const float* scale_t;  //         and per train row
     int seg_tiles;       // train tiles per segment (blockIdx.y)
@@ -275,11 +278,37 @@ __device__ __forceinline__ void scan_chunk_i8(const uint32_t (&v)[32], int col0,
 }
 
 // Largest key of a 32-column chunk (SIM_F16: the raw fp32 accumulator;
-// DIST_BF16 / SPLIT_FP8: 2 a.b - |b|^2, exact), columns >= lim excluded.
+// DIST_U8 / SPLIT_FP8: 2 a.b - |b|^2, exact), columns >= lim excluded.
 // A pairwise tree of 31 max operations; the chunk's position in the row is
 // kept by the caller, so no per-column index is tracked.
 template <int MODE>
-__device__ __forceinline__ float chunk_max(uint32_t (&v)[32], int lim, const float* __restrict__ nb) {
+__device__ __forceinline__ float chunk_max(uint32_t (&v)[32], int lim, const float* __restrict__ nb,
+                                           const int* __restrict__ nbi) {
+    if constexpr (MODE == DIST_U8) {
+        // integer keys 2 a.b - |b|^2 from the s32 accumulator (|key| < 2^24):
+        // an integer max tree, one conversion per chunk (exact)
+        int y[32];
+        const int4* n4 = reinterpret_cast<const int4*>(nbi);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int4 n = n4[q];  // the same address in every lane: one broadcast
+            y[4 * q + 0] = 2 * (int)v[4 * q + 0] - n.x;
+            y[4 * q + 1] = 2 * (int)v[4 * q + 1] - n.y;
+            y[4 * q + 2] = 2 * (int)v[4 * q + 2] - n.z;
+            y[4 * q + 3] = 2 * (int)v[4 * q + 3] - n.w;
+        }
+        if (lim < 32) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+                if (j >= lim) y[j] = INT_MIN;
+        }
+#pragma unroll
+        for (int w = 16; w > 0; w >>= 1) {
+#pragma unroll
+            for (int j = 0; j < w; ++j) y[j] = max(y[j], y[j + w]);
+        }
+        return y[0] == INT_MIN ? -INFINITY : (float)y[0];
+    }
     float x[32];
     if constexpr (MODE == SIM_F16) {
 #pragma unroll
@@ -334,10 +363,10 @@ template <int MODE, int RB>
 __global__ void __launch_bounds__(SCAN_THREADS, 2) k_match_rows(const RowScanArgs args) {
     using G = TileGeom<RB>;
     constexpr int NS = G::NS;
-    // SIM_F16, DIST_BF16, SPLIT_FP8: chunk-level state (the key of each
+    // SIM_F16, DIST_U8, SPLIT_FP8: chunk-level state (the key of each
     // 32-column chunk is its largest); SIM_I8: column-level top-2
     constexpr bool CHUNKED = MODE != SIM_I8;
-    constexpr bool NORMS = MODE == DIST_BF16 || MODE == SPLIT_FP8;
+    constexpr bool NORMS = MODE == DIST_U8 || MODE == SPLIT_FP8;
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t* sQ = smem;                // the query tile (NSL slabs)
     uint8_t* sRing = smem + G::TILE;   // NS train slabs
@@ -407,7 +436,8 @@ __global__ void __launch_bounds__(SCAN_THREADS, 2) k_match_rows(const RowScanArg
     } else if (warp == EPI_WARPS + 1) {
         // ---- MMA issuer ----
         if (lane == 0) {
-            constexpr uint32_t idesc = MODE == SIM_I8 ? umma_idesc_s8() : umma_idesc(MODE == DIST_BF16 ? 1 : 0);
+            constexpr uint32_t idesc =
+                MODE == SIM_I8 ? umma_idesc_i8(true) : MODE == DIST_U8 ? umma_idesc_i8(false) : umma_idesc(0);
             bool ok = mbar_wait_bounded(&bar_q, 0u, &s_abort);
             int k = 0;  // slabs consumed
             for (int p = 0; ok && p < nt; ++p) {
@@ -432,7 +462,7 @@ __global__ void __launch_bounds__(SCAN_THREADS, 2) k_match_rows(const RowScanArg
                         const uint64_t da = umma_desc(a0 + u * 256, 128, G::SW * 128);
                         const uint64_t db = umma_desc(b0 + u * 256, 128, G::SW * 128);
                         const uint32_t acc = (j > 0 || u > 0) ? 1u : 0u;
-                        if (MODE == SIM_I8)
+                        if (MODE == SIM_I8 || MODE == DIST_U8)
                             asm volatile(
                                 "{\n\t.reg .pred p;\n\t"
                                 "setp.ne.b32 p, %4, 0;\n\t"
@@ -504,9 +534,12 @@ __global__ void __launch_bounds__(SCAN_THREADS, 2) k_match_rows(const RowScanArg
             if (lane == 0) mbar_arrive(&bar_acc_empty[a]);
             const int c0 = tcol0 + half * 64;
             if constexpr (CHUNKED) {
-                const float* nrm = NORMS ? args.norm_t + c0 : nullptr;
-                top3_push(tc, chunk_max<MODE>(v0, lim_tile - half * 64, nrm), c0);
-                top3_push(tc, chunk_max<MODE>(v1, lim_tile - half * 64 - 32, NORMS ? nrm + 32 : nullptr), c0 + 32);
+                const float* nrm = MODE == SPLIT_FP8 ? args.norm_t + c0 : nullptr;
+                const int* nri = MODE == DIST_U8 ? args.norm_ti + c0 : nullptr;
+                top3_push(tc, chunk_max<MODE>(v0, lim_tile - half * 64, nrm, nri), c0);
+                top3_push(tc, chunk_max<MODE>(v1, lim_tile - half * 64 - 32, nrm ? nrm + 32 : nullptr,
+                                              nri ? nri + 32 : nullptr),
+                          c0 + 32);
             } else {
                 const int ca = c0 + lane, cb = c0 + 32 + lane;
                 const int sa = __float_as_int(ca < args.n_t ? args.scale_t[ca] : 1.0f);
@@ -620,7 +653,7 @@ __device__ __forceinline__ Top3 merge_parts(const Top3* __restrict__ part, int i
     return a;
 }
 
-// DIST_BF16 / SPLIT_FP8: the best chunk of row i (the first chunk holding
+// DIST_U8 / SPLIT_FP8: the best chunk of row i (the first chunk holding
 // the row's largest key) recomputed exactly from the uint8 rows, one warp per
 // row and one column per lane: the best column is the first in that chunk
 // with the chunk's key, and the second key the larger of the chunk's second
@@ -928,24 +961,20 @@ __global__ void __launch_bounds__(1024) k_match_mutual(const int* __restrict__ f
     if (threadIdx.x == 0) *count = base;
 }
 
-// |row|^2 of uint8 rows (int32 for the merge, float32 for the scan; exact:
-// below 2^24) and, with bf, the rows as bf16 in the tiled layout.  Rows
-// n .. n_pad-1 get a zero float norm and zero bf16 rows.
+// |row|^2 of uint8 rows as int32 and float32 (exact: below 2^24).  Rows
+// n .. n_pad-1 get zero norms.
 __global__ void k_row_norms_u8(const uint8_t* __restrict__ d, int n, int n_pad, int D, int* __restrict__ norms,
-                               float* __restrict__ fnorms, uint8_t* __restrict__ bf) {
+                               float* __restrict__ fnorms) {
     const int i = blockIdx.x * blockDim.y + threadIdx.y;
     if (i >= n_pad) return;
     int s = 0;
     for (int k = threadIdx.x; k < D; k += 32) {
         const int v = i < n ? d[(size_t)i * D + k] : 0;
         s += v * v;
-        if (bf)
-            *reinterpret_cast<uint16_t*>(bf + tiled_off(i, k >> 3, 2 * D) + ((2 * k) & 15)) =
-                __bfloat16_as_ushort(__float2bfloat16_rn((float)v));
     }
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(FULL_MASK, s, o);
     if (threadIdx.x == 0) {
-        if (i < n) norms[i] = s;
+        norms[i] = s;
         fnorms[i] = (float)s;
     }
 }
@@ -1025,12 +1054,11 @@ static int launch_scan(const RowScanArgs& a, int nseg, cudaStream_t st) {
     return PYSIFT_OK;
 }
 
-// row bytes: 2 D for fp16 / bf16 rows, 4 D for the split e4m3 planes, D for int8
+// row bytes: 2 D for fp16 rows, 4 D for the split e4m3 planes, D for uint8 / int8
 static int launch_scan_mode(int mode, const RowScanArgs& a, int D, int nseg, cudaStream_t st) {
     if (mode == SIM_I8) return D == 64 ? launch_scan<SIM_I8, 64>(a, nseg, st) : launch_scan<SIM_I8, 128>(a, nseg, st);
     if (mode == SIM_F16) return D == 64 ? launch_scan<SIM_F16, 128>(a, nseg, st) : launch_scan<SIM_F16, 256>(a, nseg, st);
-    if (mode == DIST_BF16)
-        return D == 64 ? launch_scan<DIST_BF16, 128>(a, nseg, st) : launch_scan<DIST_BF16, 256>(a, nseg, st);
+    if (mode == DIST_U8) return D == 64 ? launch_scan<DIST_U8, 64>(a, nseg, st) : launch_scan<DIST_U8, 128>(a, nseg, st);
     return D == 64 ? launch_scan<SPLIT_FP8, 256>(a, nseg, st) : launch_scan<SPLIT_FP8, 512>(a, nseg, st);
 }
 
@@ -1050,8 +1078,8 @@ struct MatchLayout {
 static int pad_rows(int n) { return ceil_div(n, MT) * MT; }
 
 // exact: 0 = fp16 similarity (and int8 similarity, whose D-byte rows fit in
-// its buffers), 1 = exact via bf16, 2 = exact via split e4m3 (scan row
-// bytes: 2 D, 2 D, 4 D)
+// its buffers), 1 = exact via unsigned 8-bit MMAs, 2 = exact via split e4m3
+// (scan row bytes: 2 D, D, 4 D)
 static MatchLayout match_layout(int n1, int n2, int D, int exact) {
     MatchLayout l;
     size_t off = 0;
@@ -1078,13 +1106,13 @@ static MatchLayout match_layout(int n1, int n2, int D, int exact) {
         l.off_nrm = take(((size_t)n1 + n2) * 4);
     }
     l.off_na = l.off_nb = l.off_fna = l.off_fnb = 0;
-    if (exact == 1 || exact == 2) {  // |row|^2 as int32 and (padded) as float32
-        l.off_na = take((size_t)n1 * 4);
-        l.off_nb = take((size_t)n2 * 4);
+    if (exact == 1 || exact == 2) {  // |row|^2 as int32 and as float32, padded to whole tiles
+        l.off_na = take((size_t)pad_rows(n1) * 4);
+        l.off_nb = take((size_t)pad_rows(n2) * 4);
         l.off_fna = take((size_t)pad_rows(n1) * 4);
         l.off_fnb = take((size_t)pad_rows(n2) * 4);
     }
-    const size_t rb = exact == 2 ? 4 * (size_t)D : 2 * (size_t)D;
+    const size_t rb = exact == 2 ? 4 * (size_t)D : exact == 1 ? (size_t)D : 2 * (size_t)D;
     l.off_qa = take((size_t)pad_rows(n1) * rb);
     l.off_qb = take((size_t)pad_rows(n2) * rb);
     l.off_ta = l.off_qa;
@@ -1134,12 +1162,16 @@ static int run_match(int mode, const uint8_t* rows_a, int n1, const uint8_t* row
         k_tile_rows<<<(unsigned)ceil_div_ll((long long)p2 * (rb / 16), 256), 256, 0, st>>>(rows_b, n2, p2, rb, qb);
         PYSIFT_LAUNCH_CHECK("k_tile_rows");
     } else {
-        k_row_norms_u8<<<ceil_div(p1, 8), dim3(32, 8), 0, st>>>(rows_a, n1, p1, D, na, fna,
-                                                                 mode == DIST_BF16 ? qa : nullptr);
+        k_row_norms_u8<<<ceil_div(p1, 8), dim3(32, 8), 0, st>>>(rows_a, n1, p1, D, na, fna);
         PYSIFT_LAUNCH_CHECK("k_row_norms_u8");
-        k_row_norms_u8<<<ceil_div(p2, 8), dim3(32, 8), 0, st>>>(rows_b, n2, p2, D, nb, fnb,
-                                                                 mode == DIST_BF16 ? qb : nullptr);
+        k_row_norms_u8<<<ceil_div(p2, 8), dim3(32, 8), 0, st>>>(rows_b, n2, p2, D, nb, fnb);
         PYSIFT_LAUNCH_CHECK("k_row_norms_u8");
+        if (mode == DIST_U8) {
+            k_tile_rows<<<(unsigned)ceil_div_ll((long long)p1 * (D / 16), 256), 256, 0, st>>>(rows_a, n1, p1, D, qa);
+            PYSIFT_LAUNCH_CHECK("k_tile_rows");
+            k_tile_rows<<<(unsigned)ceil_div_ll((long long)p2 * (D / 16), 256), 256, 0, st>>>(rows_b, n2, p2, D, qb);
+            PYSIFT_LAUNCH_CHECK("k_tile_rows");
+        }
         if (mode == SPLIT_FP8) {
             k_split_nibbles_u8<<<(unsigned)ceil_div_ll((long long)p1 * D, 256), 256, 0, st>>>(rows_a, n1, p1, D, qa, ta);
             PYSIFT_LAUNCH_CHECK("k_split_nibbles_u8");
@@ -1164,6 +1196,7 @@ static int run_match(int mode, const uint8_t* rows_a, int n1, const uint8_t* row
         s.n_q = dir == 0 ? n1 : n2;
         s.n_t = dir == 0 ? n2 : n1;
         s.norm_t = dir == 0 ? fnb : fna;
+        s.norm_ti = dir == 0 ? nb : na;
         s.scale_q = dir == 0 ? sa : sb;
         s.scale_t = dir == 0 ? sb : sa;
         s.part = wsp<void>(ws, dir == 0 ? l.off_fpart : l.off_bpart);
@@ -1263,7 +1296,7 @@ int pysift_match_u8_exact(const uint8_t* d1, int32_t n1, const uint8_t* d2, int3
         return PYSIFT_ERR_WORKSPACE;
     }
     const float ratio_sq = (float)((double)ratio * (double)ratio);
-    return run_match(DIST_BF16, d1, n1, d2, n2, D, ratio_sq, l, workspace, fwd_best, fwd_pass, bwd_best, bwd_pass,
+    return run_match(DIST_U8, d1, n1, d2, n2, D, ratio_sq, l, workspace, fwd_best, fwd_pass, bwd_best, bwd_pass,
                      pairs, pair_dist, pair_count, reinterpret_cast<cudaStream_t>(stream));
 }
 
