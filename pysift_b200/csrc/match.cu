@@ -755,25 +755,32 @@ __device__ __forceinline__ double dot_f16_exact(const __half* a, const __half* b
 
 // Row L2 norms of the two fp16 sets (set 1's rows, then set 2's) and the
 // largest of each set, rounded up with a relative margin of 2^-20, the
-// largest as float bits (non-negative floats order as
-// their bits, so the integer atomicMax is the float max: the result does not
-// depend on the order of the updates).  One warp per row.
+// largest as float bits (non-negative floats order as their bits, so the
+// integer maximum is the float maximum and the result does not depend on the
+// order of the updates).  One warp per row; the block's largest per set
+// goes to one atomicMax each.
 __global__ void k_f16_max_norms(const __half* __restrict__ a, int n1, const __half* __restrict__ b, int n2, int D,
                                 unsigned* __restrict__ out, float* __restrict__ row_norm) {
+    __shared__ unsigned s_max[2];
+    if (threadIdx.x < 2) s_max[threadIdx.x] = 0u;
+    __syncthreads();
     const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-    if (w >= n1 + n2) return;
-    const __half* row = w < n1 ? a + (size_t)w * D : b + (size_t)(w - n1) * D;
-    double s = 0.0;
-    for (int k = lane; k < D; k += 32) {
-        const float f = __half2float(row[k]);
-        s += (double)__fmul_rn(f, f);
+    if (w < n1 + n2) {
+        const __half* row = w < n1 ? a + (size_t)w * D : b + (size_t)(w - n1) * D;
+        double s = 0.0;
+        for (int k = lane; k < D; k += 32) {
+            const float f = __half2float(row[k]);
+            s += (double)__fmul_rn(f, f);
+        }
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL_MASK, s, o);
+        if (lane == 0) {
+            const float nrm = __double2float_ru(sqrt(s) * (1.0 + 0x1p-20));
+            row_norm[w] = nrm;
+            atomicMax(&s_max[w < n1 ? 0 : 1], __float_as_uint(nrm));
+        }
     }
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL_MASK, s, o);
-    if (lane == 0) {
-        const float nrm = __double2float_ru(sqrt(s) * (1.0 + 0x1p-20));
-        row_norm[w] = nrm;
-        atomicMax(&out[w < n1 ? 0 : 1], __float_as_uint(nrm));
-    }
+    __syncthreads();
+    if (threadIdx.x < 2 && s_max[threadIdx.x]) atomicMax(&out[threadIdx.x], s_max[threadIdx.x]);
 }
 
 __device__ __forceinline__ void finish_f16_row(int i, float f1, float f2, int c1, float ratio_sq, int* best, int* pass,
