@@ -795,7 +795,8 @@ struct RansacLayout {
 // off-diagonal element exceeds tol (60 at most).  The basis is the
 // eigenvectors of the last P indices in (eigenvalue asc, index asc) order,
 // in that order (as eigh's v[:, -P:]), rounded to float32.  A lives in
-// shared memory, V in the caller's workspace.
+// shared memory, V (stored transposed, so that its column rotations are
+// coalesced row rotations) in the caller's workspace.
 __device__ __forceinline__ void pca_pair(int D, int rnd, int i, int* p, int* q) {
     int a, b;
     if (i == 0) {
@@ -810,10 +811,15 @@ __device__ __forceinline__ void pca_pair(int D, int rnd, int i, int* p, int* q) 
 }
 
 constexpr int PCA_BT = 1024;
+constexpr int PCA_IT = 4;  // items per thread loaded together (a pass has 128 x 64 / 1024 = 8)
 
-__global__ void __launch_bounds__(PCA_BT) k_pca_basis(const double* __restrict__ cov, int D, int P,
+// DC: the dimension as a compile-time constant (64, 128), or 0 for any even
+// D <= 128 given at run time (the same operations either way).
+template <int DC>
+__global__ void __launch_bounds__(PCA_BT) k_pca_basis(const double* __restrict__ cov, int D_rt, int P,
                                                        double* __restrict__ V, float* __restrict__ proj,
                                                        int* __restrict__ sweeps_out) {
+    const int D = DC ? DC : D_rt;
     extern __shared__ __align__(16) double A[];  // D x D
     __shared__ double s_cs[64][2];
     __shared__ int s_pq[64][2];
@@ -861,36 +867,70 @@ __global__ void __launch_bounds__(PCA_BT) k_pca_basis(const double* __restrict__
                 s_act[tid] = act;
             }
             __syncthreads();
+            // each pass: a thread's items it = tid + (g + m) nt, PCA_IT at a
+            // time, load all of a group first, then rotate and store, so a
+            // pass costs two memory round trips
             // column rotations: item = (row k, pair j), pairs adjacent
-            for (int it = tid; it < D * npair; it += nt) {
-                const int k = it / npair, j = it - k * npair;
-                if (!s_act[j]) continue;
-                const int p = s_pq[j][0], q = s_pq[j][1];
-                const double c = s_cs[j][0], s = s_cs[j][1];
-                const double mkp = A[k * D + p], mkq = A[k * D + q];
-                A[k * D + p] = c * mkp - s * mkq;
-                A[k * D + q] = s * mkp + c * mkq;
+            for (int g = 0; g * nt < D * npair; g += PCA_IT) {
+                double x0[PCA_IT], x1[PCA_IT];
+#pragma unroll
+                for (int m = 0; m < PCA_IT; ++m) {
+                    const int it = tid + (g + m) * nt, k = it / npair, j = it - k * npair;
+                    if (it < D * npair && s_act[j]) {
+                        x0[m] = A[k * D + s_pq[j][0]];
+                        x1[m] = A[k * D + s_pq[j][1]];
+                    }
+                }
+#pragma unroll
+                for (int m = 0; m < PCA_IT; ++m) {
+                    const int it = tid + (g + m) * nt, k = it / npair, j = it - k * npair;
+                    if (it < D * npair && s_act[j]) {
+                        const double c = s_cs[j][0], s = s_cs[j][1];
+                        const double mkp = x0[m], mkq = x1[m];
+                        A[k * D + s_pq[j][0]] = c * mkp - s * mkq;
+                        A[k * D + s_pq[j][1]] = s * mkp + c * mkq;
+                    }
+                }
             }
             __syncthreads();
-            // row rotations: item = (pair j, column k), columns adjacent
-            for (int it = tid; it < npair * D; it += nt) {
-                const int j = it / D, k = it - j * D;
-                if (!s_act[j]) continue;
-                const int p = s_pq[j][0], q = s_pq[j][1];
-                const double c = s_cs[j][0], s = s_cs[j][1];
-                const double mpk = A[p * D + k], mqk = A[q * D + k];
-                A[p * D + k] = c * mpk - s * mqk;
-                A[q * D + k] = s * mpk + c * mqk;
-            }
-            // eigenvector columns: item = (row k, pair j)
-            for (int it = tid; it < D * npair; it += nt) {
-                const int k = it / npair, j = it - k * npair;
-                if (!s_act[j]) continue;
-                const int p = s_pq[j][0], q = s_pq[j][1];
-                const double c = s_cs[j][0], s = s_cs[j][1];
-                const double vkp = V[k * D + p], vkq = V[k * D + q];
-                V[k * D + p] = c * vkp - s * vkq;
-                V[k * D + q] = s * vkp + c * vkq;
+            // row rotations and eigenvector columns: item = (pair j, column k),
+            // columns adjacent (V^T[p][k] is V[k][p])
+            for (int g = 0; g * nt < D * npair; g += PCA_IT) {
+                double x0[PCA_IT], x1[PCA_IT], y0[PCA_IT], y1[PCA_IT];
+#pragma unroll
+                for (int m = 0; m < PCA_IT; ++m) {
+                    const int it = tid + (g + m) * nt;
+                    if (it < npair * D) {
+                        const int j = it / D, k = it - j * D;
+                        if (s_act[j]) {
+                            x0[m] = A[s_pq[j][0] * D + k];
+                            x1[m] = A[s_pq[j][1] * D + k];
+                        }
+                        if (s_act[j]) {  // V is kept transposed: rows p, q of V^T, columns adjacent
+                            y0[m] = V[s_pq[j][0] * D + k];
+                            y1[m] = V[s_pq[j][1] * D + k];
+                        }
+                    }
+                }
+#pragma unroll
+                for (int m = 0; m < PCA_IT; ++m) {
+                    const int it = tid + (g + m) * nt;
+                    if (it < npair * D) {
+                        const int j = it / D, k = it - j * D;
+                        if (s_act[j]) {
+                            const double c = s_cs[j][0], s = s_cs[j][1];
+                            const double mpk = x0[m], mqk = x1[m];
+                            A[s_pq[j][0] * D + k] = c * mpk - s * mqk;
+                            A[s_pq[j][1] * D + k] = s * mpk + c * mqk;
+                        }
+                        if (s_act[j]) {
+                            const double c = s_cs[j][0], s = s_cs[j][1];
+                            const double vkp = y0[m], vkq = y1[m];
+                            V[s_pq[j][0] * D + k] = c * vkp - s * vkq;
+                            V[s_pq[j][1] * D + k] = s * vkp + c * vkq;
+                        }
+                    }
+                }
             }
             __syncthreads();
         }
@@ -907,7 +947,7 @@ __global__ void __launch_bounds__(PCA_BT) k_pca_basis(const double* __restrict__
     __syncthreads();
     for (int it = tid; it < D * P; it += nt) {
         const int k = it / P, c = it - k * P;
-        proj[it] = (float)V[k * D + s_order[D - P + c]];
+        proj[it] = (float)V[s_order[D - P + c] * D + k];
     }
     if (tid == 0 && sweeps_out) *sweeps_out = sweep;
 }
@@ -1121,9 +1161,18 @@ int pysift_pca_basis(const double* cov, int32_t D, int32_t P, void* workspace, s
     }
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     const size_t smem = (size_t)D * D * sizeof(double);
-    PYSIFT_CUDA_TRY(cudaFuncSetAttribute(k_pca_basis, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int* sw = reinterpret_cast<int*>(static_cast<char*>(workspace) + align_up((size_t)D * D * sizeof(double), 256));
-    k_pca_basis<<<1, PCA_BT, smem, st>>>(cov, D, P, static_cast<double*>(workspace), proj, sw);
+    double* V = static_cast<double*>(workspace);
+    if (D == 128) {
+        PYSIFT_CUDA_TRY(cudaFuncSetAttribute(k_pca_basis<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_pca_basis<128><<<1, PCA_BT, smem, st>>>(cov, D, P, V, proj, sw);
+    } else if (D == 64) {
+        PYSIFT_CUDA_TRY(cudaFuncSetAttribute(k_pca_basis<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_pca_basis<64><<<1, PCA_BT, smem, st>>>(cov, D, P, V, proj, sw);
+    } else {
+        PYSIFT_CUDA_TRY(cudaFuncSetAttribute(k_pca_basis<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_pca_basis<0><<<1, PCA_BT, smem, st>>>(cov, D, P, V, proj, sw);
+    }
     PYSIFT_LAUNCH_CHECK("k_pca_basis");
     if (sweeps) PYSIFT_CUDA_TRY(cudaMemcpyAsync(sweeps, sw, sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
     return PYSIFT_OK;
