@@ -297,10 +297,10 @@ class RefSchedule:
 
 def run_reference(args, wl, world, rank):
     """--impl reference: the reference's path as the CPU oracle port, rank 0
-    only; at most two warm-up steps and REF_BUDGET_S of timed steps."""
+    only; three warm-up steps and at most REF_BUDGET_S of timed steps."""
     if rank != 0:
         return 0
-    args.warmup = min(args.warmup, 2)
+    args.warmup = min(args.warmup, 3)
     from pysift_b200 import synthetic
     if wl["kind"] == "stitch":
         return run_reference_stitch(args, wl)
