@@ -33,3 +33,19 @@ def test_reference_arm_detect_line():
 def test_reference_arm_unavailable_line():
     d = _run("--workload", "grad_16x1024x768")
     assert d["impl"] == "reference" and "unavailable" in d
+
+
+def test_reference_schedule_stops_at_the_budget():
+    """The reference arm's steps: all warm-up steps, then timed steps until the
+    requested count or the wall-time budget (after at least one timed step)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    assert list(bench.RefSchedule(3, 4)) == [0, 1, 2, 3, 4, 5, 6]
+    old = bench.REF_BUDGET_S
+    try:
+        bench.REF_BUDGET_S = -1.0  # already spent: one timed step, then stop
+        assert list(bench.RefSchedule(3, 200)) == [0, 1, 2, 3]
+    finally:
+        bench.REF_BUDGET_S = old

@@ -325,3 +325,26 @@ def test_pre_and_post_processing_options(tmp_path, monkeypatch):
         exp = cv2.resize(exp, (int(w * 300 / max(h, w)), int(h * 300 / max(h, w))), interpolation=cv2.INTER_AREA)
     exp = cv2.addWeighted(exp, 1.5, cv2.GaussianBlur(exp, (0, 0), sigmaX=2.0), -0.5, 0)
     assert np.array_equal(saved, exp)
+
+
+@pytest.mark.parametrize("D,P", [(64, 32), (128, 128)])
+def test_pca_basis_other_shapes_bit_exact(D, P):
+    """The device Jacobi at the other compile-time dimension and all columns."""
+    import torch
+    from oracle import stitch_oracle as so
+    L, lib = _lib()
+    rng = np.random.default_rng(D + P)
+    x = np.abs(rng.standard_normal((2000, D))).astype(np.float32) ** 2
+    x /= np.linalg.norm(x, axis=1, keepdims=True)
+    _, cov = so.pca_stats(x)
+    want, sweeps = so.pca_basis(cov, P, return_sweeps=True)
+    c = torch.from_numpy(cov).cuda()
+    sz = ctypes.c_size_t()
+    assert lib.pysift_pca_basis_workspace_size(D, ctypes.byref(sz)) == 0
+    ws = torch.empty(sz.value, dtype=torch.uint8, device="cuda")
+    got = torch.empty((D, P), dtype=torch.float32, device="cuda")
+    sw = torch.zeros(1, dtype=torch.int32, device="cuda")
+    assert lib.pysift_pca_basis(c.data_ptr(), D, P, ws.data_ptr(), ws.numel(), got.data_ptr(), sw.data_ptr(),
+                                _st()) == 0
+    assert np.array_equal(got.cpu().numpy(), want)
+    assert int(sw.item()) == sweeps
