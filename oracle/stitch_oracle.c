@@ -214,14 +214,17 @@ static void dlt_refit(const double* p1, const double* p2, const int* idx, int m,
         for (int c = 0; c < 9; ++c) V[r][c] = (r == c) ? 1.0 : 0.0;
     /* parallel (round-robin) Jacobi: round r rotates the disjoint pairs
      * {(r+i) mod 9, (r-i) mod 9}, i = 1..4; angles from the start-of-round
-     * matrix, then all column rotations, then all row rotations; after sweep
-     * 3 negligible elements are zeroed instead of rotated; stop when every
-     * off-diagonal element is 0 (15 sweeps at most). */
+     * matrix, then all column rotations, then all row rotations; only pairs
+     * with |a_pq| > tol = 2^-52 trace rotate; stop when no upper
+     * off-diagonal element exceeds tol (15 sweeps at most). */
+    double tr = 0.0;
+    for (int k = 0; k < 9; ++k) tr = tr + M[k][k];
+    const double tol = tr * 0x1p-52;
     for (int sweep = 0; sweep < 15; ++sweep) {
         int nz = 0;
         for (int r = 0; r < 9; ++r)
             for (int c = r + 1; c < 9; ++c)
-                if (M[r][c] != 0.0) nz = 1;
+                if (fabs(M[r][c]) > tol) nz = 1;
         if (!nz) break;
         for (int rnd = 0; rnd < 9; ++rnd) {
             int P[4], Q[4], act[4];
@@ -233,14 +236,8 @@ static void dlt_refit(const double* p1, const double* p2, const int* idx, int m,
                 Q[j] = qq;
                 act[j] = 0;
                 double apq = M[p][qq];
-                if (apq == 0.0) continue;
+                if (!(fabs(apq) > tol)) continue;
                 double app = M[p][p], aqq = M[qq][qq];
-                double g = 100.0 * fabs(apq);
-                if (sweep > 3 && fabs(app) + g == fabs(app) && fabs(aqq) + g == fabs(aqq)) {
-                    M[p][qq] = 0.0;
-                    M[qq][p] = 0.0;
-                    continue;
-                }
                 double theta = (aqq - app) / (2.0 * apq);
                 double tt = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
                 double c = 1.0 / sqrt(tt * tt + 1.0);

@@ -12,7 +12,8 @@
 //     pivoting on its 8x9 system (the reference takes the last right singular
 //     vector of a batched SVD); degenerate samples get score -inf;
 //   * the least-squares refit takes the eigenvector of A^T A for the smallest
-//     eigenvalue by cyclic Jacobi (15 sweeps) instead of the SVD of A;
+//     eigenvalue by cyclic Jacobi (until no off-diagonal element exceeds
+//     2^-52 trace, 15 sweeps at most) instead of the SVD of A;
 //   * T2^-1 is formed analytically, H^-1 by the adjugate; 3x3 products sum
 //     k = 0, 1, 2 in order; exp is computed by ransac_exp (below);
 //   * RANSAC samples are the reference's: torch.randint on a CPU generator
@@ -341,10 +342,10 @@ __global__ void __launch_bounds__(256) k_ransac_hyp(const RansacArgs a) {
 // disjoint pairs {(r+i) mod 9, (r-i) mod 9}, i = 1..4 (p < q); index r rests.
 // The 4 angles of a round come from the matrix at the start of the round,
 // then all column rotations are applied, then all row rotations (exact, as
-// the pairs are disjoint).  After sweep 3 a rotation whose off-diagonal
-// element is negligible (|a_pp| + 100|a_pq| == |a_pp| and the same for a_qq)
-// zeroes it instead; sweeps stop once every off-diagonal element is 0, at 15
-// at most.  Returns the index of the smallest diagonal element (lowest on ties).
+// the pairs are disjoint).  Only pairs with |a_pq| > tol = 2^-52 trace
+// (the trace summed in index order) rotate; sweeps stop once no upper
+// off-diagonal element exceeds tol, at 15 at most.  Returns the index of the
+// smallest diagonal element (lowest on ties).
 __device__ int jacobi9_smallest(double (*M)[9], double (*V)[9]) {
     __shared__ double s_cs[4][2];
     __shared__ int s_pq[4][2];
@@ -353,13 +354,16 @@ __device__ int jacobi9_smallest(double (*M)[9], double (*V)[9]) {
     const int lane = threadIdx.x & 31;
     if (threadIdx.x < 32) {
         for (int it = lane; it < 81; it += 32) V[it / 9][it % 9] = (it / 9 == it % 9) ? 1.0 : 0.0;
+        double tr = 0.0;
+        for (int k = 0; k < 9; ++k) tr = tr + M[k][k];
+        const double tol = tr * 0x1p-52;
         __syncwarp();
         for (int sweep = 0; sweep < 15; ++sweep) {
-            // every upper off-diagonal element exactly zero -> converged
+            // no upper off-diagonal element above tol -> converged
             bool nz = false;
             for (int it = lane; it < 81; it += 32) {
                 const int r = it / 9, c = it % 9;
-                if (c > r && M[r][c] != 0.0) nz = true;
+                if (c > r && fabs(M[r][c]) > tol) nz = true;
             }
             if (!__any_sync(FULL_MASK, nz)) break;
             for (int rnd = 0; rnd < 9; ++rnd) {
@@ -370,20 +374,14 @@ __device__ int jacobi9_smallest(double (*M)[9], double (*V)[9]) {
                     s_pq[lane][1] = q;
                     const double apq = M[p][q];
                     int act = 0;
-                    if (apq != 0.0) {
+                    if (fabs(apq) > tol) {
                         const double app = M[p][p], aqq = M[q][q];
-                        const double g = 100.0 * fabs(apq);
-                        if (sweep > 3 && fabs(app) + g == fabs(app) && fabs(aqq) + g == fabs(aqq)) {
-                            M[p][q] = 0.0;
-                            M[q][p] = 0.0;
-                        } else {
-                            const double theta = (aqq - app) / (2.0 * apq);
-                            const double tt = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
-                            const double c = 1.0 / sqrt(tt * tt + 1.0);
-                            s_cs[lane][0] = c;
-                            s_cs[lane][1] = tt * c;
-                            act = 1;
-                        }
+                        const double theta = (aqq - app) / (2.0 * apq);
+                        const double tt = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                        const double c = 1.0 / sqrt(tt * tt + 1.0);
+                        s_cs[lane][0] = c;
+                        s_cs[lane][1] = tt * c;
+                        act = 1;
                     }
                     s_act[lane] = act;
                 }
