@@ -52,14 +52,13 @@
 #include <cstdint>
 
 #include "common.cuh"
-#include <cuda_bf16.h>
 #include <cuda_fp8.h>
 
 namespace pysift {
 
 constexpr int MT = 128;           // query rows per CTA = UMMA M = TMEM lanes
 constexpr int NT = 128;           // train rows per tile = UMMA N
-constexpr int MATCH_THREADS = 256;  // 2 warps per TMEM lane quadrant, each half the tile's columns
+constexpr int MATCH_THREADS = 256;  // the scan's reducer threads: 2 warps per TMEM lane quadrant, each half the tile's columns
 constexpr unsigned SPIN_LIMIT = 1u << 22;  // bounded waits on the pipeline barriers
 
 enum MatchMode { SIM_F16 = 0, DIST_U8 = 1, SPLIT_FP8 = 2, SIM_I8 = 3 };
