@@ -63,3 +63,25 @@ def test_detect_config_ranges():
         build_detect_config(5, _lib.MAX_LEVELS, 1.6, 0.04, 10.0, False, 3, False, True, True, True)
     with pytest.raises(ValueError, match="n_octaves"):
         build_detect_config(_lib.MAX_OCTAVES + 1, 3, 1.6, 0.04, 10.0, False, 3, False, True, True, True)
+
+
+def test_c_abi_argument_checks_without_a_device():
+    """The new C entry points reject bad sizes and misaligned rows before any
+    CUDA call (so these run on a host without a GPU)."""
+    import ctypes
+    from pysift_b200 import _lib
+    lib = _lib.load()
+    sz = ctypes.c_size_t()
+    assert lib.pysift_pca_basis_workspace_size(128, ctypes.byref(sz)) == 0 and sz.value >= 128 * 128 * 8
+    assert lib.pysift_pca_basis_workspace_size(65, ctypes.byref(sz)) == -1       # odd D
+    assert lib.pysift_pca_basis_workspace_size(130, ctypes.byref(sz)) == -1      # D > 128
+    fake = ctypes.c_void_p(256)  # never dereferenced: the checks fail first
+    assert lib.pysift_pca_basis(fake, 64, 65, fake, 1 << 20, fake, None, None) == -1   # P > D
+    assert lib.pysift_pca_basis(fake, 64, 0, fake, 1 << 20, fake, None, None) == -1    # P < 1
+    assert lib.pysift_pca_basis(fake, 64, 32, fake, 16, fake, None, None) == -2        # workspace too small
+    # exact uint8 matching wants 16-byte aligned rows
+    odd = ctypes.c_void_p(256 + 8)
+    args = (0.75, fake, 1 << 30, fake, fake, fake, fake, fake, fake, fake, None)
+    assert lib.pysift_match_u8_exact(odd, 10, fake, 10, 128, *args) == -1
+    assert lib.pysift_match_u8_split_fp8(fake, 10, odd, 10, 128, *args) == -1
+    assert "aligned" in lib.pysift_last_error().decode()
