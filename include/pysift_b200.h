@@ -284,6 +284,16 @@ int pysift_ransac_workspace_size(int32_t n, int32_t n_hyp, size_t* bytes);
 int pysift_ransac(const double* pts1, const double* pts2, int32_t n, const uint32_t* rand_u32, int32_t n_hyp,
                   double inlier_thresh, double sigma_max, int32_t magsac, int32_t min_inliers, void* workspace,
                   size_t workspace_bytes, double* H_out, uint8_t* mask_out, int32_t* info, pysift_stream_t stream);
+/* The same with the point count on the device (n_dev, e.g. the match count
+ * pysift_match_* wrote), so that matching, point gathering and RANSAC run
+ * without the host reading the count in between: pts hold up to n_cap
+ * points, the workspace is sized for n_cap, and a count below 4 yields
+ * info = {0, 0, 0} (the caller reports the shortage after reading info).
+ * No counterpart in the reference (its RANSAC takes host arrays). */
+int pysift_ransac_count(const double* pts1, const double* pts2, const int32_t* n_dev, int32_t n_cap,
+                        const uint32_t* rand_u32, int32_t n_hyp, double inlier_thresh, double sigma_max,
+                        int32_t magsac, int32_t min_inliers, void* workspace, size_t workspace_bytes, double* H_out,
+                        uint8_t* mask_out, int32_t* info, pysift_stream_t stream);
 
 /* Normalised DLT homography of all n correspondences (pysift/core.py:2959-2981). */
 int pysift_dlt_homography(const double* pts1, const double* pts2, int32_t n, int32_t* idx_scratch, double* H_out,

@@ -177,6 +177,9 @@ EXPORTS.update({
     "pysift_ransac_workspace_size": (ctypes.c_int, [c_int32, c_int32, ctypes.POINTER(c_size_t)]),
     "pysift_ransac": (ctypes.c_int, [c_void_p, c_void_p, c_int32, c_void_p, c_int32, c_double, c_double, c_int32,
                                      c_int32, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "pysift_ransac_count": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_int32, c_void_p, c_int32, c_double,
+                                           c_double, c_int32, c_int32, c_void_p, c_size_t, c_void_p, c_void_p,
+                                           c_void_p, c_void_p]),
     "pysift_dlt_homography": (ctypes.c_int, [c_void_p, c_void_p, c_int32, c_void_p, c_void_p, c_void_p]),
     "pysift_warp_feather": (ctypes.c_int, [c_void_p, c_int32, c_int32, c_int32, c_void_p, c_int32, c_int32, c_int32,
                                            c_int32, c_int32, c_void_p, c_float, c_float, c_int32, c_int32, c_int32,

@@ -280,11 +280,24 @@ struct RansacArgs {
     uint8_t* mask;    // n output
     double* H_out;    // 9
     int* info;        // [n_inliers, best_i, stage]
+    const int* n_dev; // if set: the point count on the device (n is then the capacity)
 };
 
-__global__ void __launch_bounds__(RT) k_ransac_prep(const RansacArgs a) {
+// The point count of a launch: n, or the device count clamped to 0..n.
+// Fewer than 4 points leave no homography to fit: the kernels then write an
+// empty result (info = 0, 0, 0) instead of sampling.
+__device__ __forceinline__ int ransac_count(const RansacArgs& a) {
+    if (!a.n_dev) return a.n;
+    const int c = *a.n_dev;
+    return c < 0 ? 0 : (c > a.n ? a.n : c);
+}
+
+__global__ void __launch_bounds__(RT) k_ransac_prep(const RansacArgs args) {
     __shared__ double sh[4][RT];
     __shared__ double red[4];
+    RansacArgs a = args;
+    a.n = ransac_count(args);
+    if (a.n < 4) return;
     Norm n1, n2;
     hartley2(a.p1, a.p2, nullptr, a.n, sh, red, n1, n2);
     for (int i = threadIdx.x; i < a.n; i += RT) {
@@ -302,9 +315,15 @@ __global__ void __launch_bounds__(RT) k_ransac_prep(const RansacArgs a) {
 
 // One warp per hypothesis: solve, denormalise, score all points
 // (lane-strided partial sums, then the warp tree 16, 8, 4, 2, 1).
-__global__ void __launch_bounds__(256) k_ransac_hyp(const RansacArgs a) {
+__global__ void __launch_bounds__(256) k_ransac_hyp(const RansacArgs args) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    RansacArgs a = args;
+    a.n = ransac_count(args);
     if (warp >= a.n_hyp) return;
+    if (a.n < 4) {
+        if (lane == 0) a.score[warp] = -INFINITY;
+        return;
+    }
     double x1 = 0.0, y1 = 0.0, x2 = 0.0, y2 = 0.0;
     if (lane < 8) {
         const int i = (int)(a.rnd[4 * warp + (lane >> 1)] % (uint32_t)a.n);
@@ -502,7 +521,14 @@ __device__ int compact_mask(const uint8_t* flags, int n, int* idx, int* shi) {
 }
 
 // Best hypothesis (first maximum), its inlier set, LO refits (pysift/core.py:3060-3092).
-__global__ void __launch_bounds__(RT) k_ransac_select(const RansacArgs a) {
+__global__ void __launch_bounds__(RT) k_ransac_select(const RansacArgs args) {
+    RansacArgs a = args;
+    a.n = ransac_count(args);
+    if (a.n < 4) {
+        if (threadIdx.x < 9) a.H_out[threadIdx.x] = 0.0;
+        if (threadIdx.x < 3) a.info[threadIdx.x] = 0;
+        return;
+    }
     __shared__ double sh[RT];
     __shared__ int shi[33];
     __shared__ double s_M[45];
@@ -1048,11 +1074,11 @@ int pysift_ransac_workspace_size(int32_t n, int32_t n_hyp, size_t* bytes) {
     return PYSIFT_OK;
 }
 
-int pysift_ransac(const double* pts1, const double* pts2, int32_t n, const uint32_t* rand_u32, int32_t n_hyp,
-                  double inlier_thresh, double sigma_max, int32_t magsac, int32_t min_inliers, void* workspace,
-                  size_t workspace_bytes, double* H_out, uint8_t* mask_out, int32_t* info, pysift_stream_t stream) {
+static int run_ransac(const double* pts1, const double* pts2, int32_t n, const int32_t* n_dev,
+                      const uint32_t* rand_u32, int32_t n_hyp, double inlier_thresh, double sigma_max,
+                      int32_t magsac, int32_t min_inliers, void* workspace, size_t workspace_bytes, double* H_out,
+                      uint8_t* mask_out, int32_t* info, pysift_stream_t stream) {
     PYSIFT_CHECK_ARG(pts1 && pts2 && rand_u32 && workspace && H_out && mask_out && info, "NULL pointer argument");
-    PYSIFT_CHECK_ARG(n >= 4, "Need >= 4 correspondences, got %d", n);
     PYSIFT_CHECK_ARG(n_hyp >= 1 && inlier_thresh > 0.0 && sigma_max > 0.0, "bad RANSAC parameters");
     RansacLayout l = ransac_layout(n, n_hyp);
     if (workspace_bytes < l.total) {
@@ -1063,6 +1089,7 @@ int pysift_ransac(const double* pts1, const double* pts2, int32_t n, const uint3
     a.p1 = pts1;
     a.p2 = pts2;
     a.n = n;
+    a.n_dev = n_dev;
     a.n_hyp = n_hyp;
     a.rnd = rand_u32;
     a.tq = inlier_thresh * inlier_thresh;
@@ -1087,6 +1114,24 @@ int pysift_ransac(const double* pts1, const double* pts2, int32_t n, const uint3
     k_ransac_select<<<1, RT, 0, st>>>(a);
     PYSIFT_LAUNCH_CHECK("k_ransac_select");
     return PYSIFT_OK;
+}
+
+int pysift_ransac(const double* pts1, const double* pts2, int32_t n, const uint32_t* rand_u32, int32_t n_hyp,
+                  double inlier_thresh, double sigma_max, int32_t magsac, int32_t min_inliers, void* workspace,
+                  size_t workspace_bytes, double* H_out, uint8_t* mask_out, int32_t* info, pysift_stream_t stream) {
+    PYSIFT_CHECK_ARG(n >= 4, "Need >= 4 correspondences, got %d", n);
+    return run_ransac(pts1, pts2, n, nullptr, rand_u32, n_hyp, inlier_thresh, sigma_max, magsac, min_inliers,
+                      workspace, workspace_bytes, H_out, mask_out, info, stream);
+}
+
+int pysift_ransac_count(const double* pts1, const double* pts2, const int32_t* n_dev, int32_t n_cap,
+                        const uint32_t* rand_u32, int32_t n_hyp, double inlier_thresh, double sigma_max,
+                        int32_t magsac, int32_t min_inliers, void* workspace, size_t workspace_bytes, double* H_out,
+                        uint8_t* mask_out, int32_t* info, pysift_stream_t stream) {
+    PYSIFT_CHECK_ARG(n_dev != nullptr, "NULL pointer argument");
+    PYSIFT_CHECK_ARG(n_cap >= 1, "bad capacity %d", n_cap);
+    return run_ransac(pts1, pts2, n_cap, n_dev, rand_u32, n_hyp, inlier_thresh, sigma_max, magsac, min_inliers,
+                      workspace, workspace_bytes, H_out, mask_out, info, stream);
 }
 
 int pysift_dlt_homography(const double* pts1, const double* pts2, int32_t n, int32_t* idx_scratch, double* H_out,

@@ -276,6 +276,33 @@ class GPUPyStitch:
                                            mask.data_ptr(), info.data_ptr(), st), "pysift_ransac")
         return H, mask[:n], info
 
+    def _ransac_count(self, p1, p2, count, cap):
+        """_ransac with the point count on the device (up to `cap` points)."""
+        st = self._stream()
+        n_hyp = int(self.ransac_iters)
+        sz = ctypes.c_size_t()
+        _lib.check(self._lib.pysift_ransac_workspace_size(cap, n_hyp, ctypes.byref(sz)), "ransac ws")
+        ws = self._dev.get("ransac_ws", (int(sz.value) + 256,), torch.uint8, self.device)
+        wp, wn = _ptr_aligned(ws)
+        H = self._dev.get("ransac_H", (9,), torch.float64, self.device)
+        mask = self._dev.get("ransac_mask", (cap,), torch.uint8, self.device)
+        info = self._dev.get("ransac_info", (4,), torch.int32, self.device)
+        rnd = self._random_stream(n_hyp)
+        _lib.check(self._lib.pysift_ransac_count(p1.data_ptr(), p2.data_ptr(), count.data_ptr(), cap, rnd.data_ptr(),
+                                                 n_hyp, float(self.inlier_thresh), float(self.sigma_max),
+                                                 1 if self.ransac_method == 'magsac' else 0, 10, wp, wn,
+                                                 H.data_ptr(), mask.data_ptr(), info.data_ptr(), st),
+                   "pysift_ransac_count")
+        return H, mask, info
+
+    def _pinned(self, key, shape, dtype):
+        """A cached page-locked host buffer."""
+        t = self._dev.bufs.get(key)
+        if t is None or tuple(t.shape) != tuple(shape) or t.dtype != dtype:
+            t = torch.empty(shape, dtype=dtype, pin_memory=True)
+            self._dev.bufs[key] = t
+        return t
+
     @staticmethod
     def _compute_canvas_size(img1_shape, img2_shape, H):
         """pysift/core.py:3171-3187 (float64, host)."""
@@ -433,26 +460,38 @@ class GPUPyStitch:
             self._mark(2)
             m = self._match_prepared(prep)
             self._mark(3)
-            n_m = int(m["count"].item())
-            metrics.update(matches=n_m)
             timings['st1'] = time.perf_counter() - t0
-            if n_m < 4:
-                raise RuntimeError(f"Insufficient matches ({n_m}), need >= 4")
+            # the match count stays on the device: the points are gathered and
+            # RANSAC runs on it (capacity: the smaller keypoint count), and the
+            # host reads the count with RANSAC's result, one sync for both
             st = self._stream()
-            p1 = torch.empty((n_m, 2), dtype=torch.float64, device=self.device)
-            p2 = torch.empty((n_m, 2), dtype=torch.float64, device=self.device)
+            cap = max(min(n1, n2), 1)
+            p1 = self._dev.get("pts1", (cap, 2), torch.float64, self.device)
+            p2 = self._dev.get("pts2", (cap, 2), torch.float64, self.device)
             _lib.check(self._lib.pysift_gather_points(kp1.data_ptr(), m["pairs"].data_ptr(), m["count"].data_ptr(),
-                                                      n_m, 0, p1.data_ptr(), st), "gather")
+                                                      cap, 0, p1.data_ptr(), st), "gather")
             _lib.check(self._lib.pysift_gather_points(kp2.data_ptr(), m["pairs"].data_ptr(), m["count"].data_ptr(),
-                                                      n_m, 1, p2.data_ptr(), st), "gather")
+                                                      cap, 1, p2.data_ptr(), st), "gather")
             timings['st2'] = 0.0
             t0 = time.perf_counter()
-            H_d, mask_d, info_d = self._ransac(p1, p2, n_m)
+            H_d, mask_d, info_d = self._ransac_count(p1, p2, m["count"], cap)
             self._mark(4)
-            H = H_d.cpu().numpy().reshape(3, 3).copy()
-            info = info_d.cpu().numpy()
-            n_in = int(info[0])
+            hh = self._pinned("ransac_H_host", (9,), torch.float64)
+            ih = self._pinned("ransac_info_host", (4,), torch.int32)
+            ch = self._pinned("match_count_host", (1,), torch.int32)
+            hh.copy_(H_d, non_blocking=True)
+            ih.copy_(info_d, non_blocking=True)
+            ch.copy_(m["count"][:1], non_blocking=True)
+            torch.cuda.current_stream(self.device).synchronize()
+            H = hh.numpy().reshape(3, 3).copy()
+            info = ih.numpy()[:3].copy()
+            n_m, n_in = int(ch.numpy()[0]), int(info[0])
+            metrics.update(matches=n_m)
             timings['st3'] = time.perf_counter() - t0
+            if n_m < 4:
+                raise RuntimeError(f"Insufficient matches ({n_m}), need >= 4")
+            mask_d = mask_d[:n_m]
+            p1, p2 = p1[:n_m], p2[:n_m]
             metrics.update(inliers=n_in, inlier_ratio=n_in / max(n_m, 1))
             if n_in < 4:
                 raise RuntimeError(f"Only {n_in} inliers after RANSAC, need >= 4")

@@ -348,3 +348,49 @@ def test_pca_basis_other_shapes_bit_exact(D, P):
                                 _st()) == 0
     assert np.array_equal(got.cpu().numpy(), want)
     assert int(sw.item()) == sweeps
+
+
+def test_ransac_with_device_count_equals_host_count():
+    """pysift_ransac_count (the count read on the device, a larger capacity)
+    gives pysift_ransac's H, mask and info bit for bit; a count below 4 gives
+    the empty result without sampling."""
+    import torch
+    from oracle import stitch_oracle as so
+    L, lib = _lib()
+    p1, p2, _ = _correspondences(3)
+    n, n_hyp, cap = len(p1), 1024, len(p1) + 37
+    rnd = torch.from_numpy(so.mt19937_u32(42, 4 * n_hyp)).cuda()
+    pad = lambda p: torch.from_numpy(np.vstack([p, np.full((cap - n, 2), 1e30)])).cuda()  # rows past n ignored
+    d1, d2 = pad(p1), pad(p2)
+    sz = ctypes.c_size_t()
+    lib.pysift_ransac_workspace_size(cap, n_hyp, ctypes.byref(sz))
+    ws = torch.empty(sz.value + 256, dtype=torch.uint8, device="cuda")
+    off = (-ws.data_ptr()) % 256
+    outs = []
+    for dev_count in (False, True):
+        H = torch.empty(9, dtype=torch.float64, device="cuda")
+        mask = torch.zeros(cap, dtype=torch.uint8, device="cuda")
+        info = torch.empty(3, dtype=torch.int32, device="cuda")
+        if dev_count:
+            cnt = torch.tensor([n], dtype=torch.int32, device="cuda")
+            rc = lib.pysift_ransac_count(d1.data_ptr(), d2.data_ptr(), cnt.data_ptr(), cap, rnd.data_ptr(), n_hyp,
+                                         4.0, 4.0, 1, 10, ws.data_ptr() + off, sz.value, H.data_ptr(),
+                                         mask.data_ptr(), info.data_ptr(), _st())
+        else:
+            rc = lib.pysift_ransac(d1.data_ptr(), d2.data_ptr(), n, rnd.data_ptr(), n_hyp, 4.0, 4.0, 1, 10,
+                                   ws.data_ptr() + off, sz.value, H.data_ptr(), mask.data_ptr(), info.data_ptr(),
+                                   _st())
+        assert rc == 0
+        outs.append((H.cpu().numpy(), mask[:n].cpu().numpy(), info.cpu().numpy()))
+    for a, b in zip(*outs):
+        assert np.array_equal(a, b)
+    assert outs[1][2][0] > 0.6 * n
+    # three points on the device: the empty result
+    cnt = torch.tensor([3], dtype=torch.int32, device="cuda")
+    H = torch.ones(9, dtype=torch.float64, device="cuda")
+    info = torch.full((3,), 7, dtype=torch.int32, device="cuda")
+    mask = torch.zeros(cap, dtype=torch.uint8, device="cuda")
+    assert lib.pysift_ransac_count(d1.data_ptr(), d2.data_ptr(), cnt.data_ptr(), cap, rnd.data_ptr(), n_hyp, 4.0,
+                                   4.0, 1, 10, ws.data_ptr() + off, sz.value, H.data_ptr(), mask.data_ptr(),
+                                   info.data_ptr(), _st()) == 0
+    assert np.array_equal(info.cpu().numpy(), [0, 0, 0]) and not H.cpu().numpy().any()
