@@ -112,6 +112,7 @@ class GPUPyStitch:
         self.last_timings = None
         self.stage_events = None  # optional list of 6 torch.cuda.Event(enable_timing=True)
         self._side = None         # two side streams, one per view
+        self._graphs = {}         # captured match + RANSAC launches per (counts, buffers)
 
     # ------------------------------------------------------------------
     #: stage names of the events recorded when ``stage_events`` holds six
@@ -275,6 +276,63 @@ class GPUPyStitch:
                                            1 if self.ransac_method == 'magsac' else 0, 10, wp, wn, H.data_ptr(),
                                            mask.data_ptr(), info.data_ptr(), st), "pysift_ransac")
         return H, mask[:n], info
+
+    def _match_and_ransac_launches(self, kp1, d1, n1, kp2, d2, n2):
+        """Matcher preparation, matching, point gather and RANSAC of a pair,
+        enqueued on the current stream with no host read: the match count
+        stays on the device (RANSAC capacity: the smaller keypoint count)."""
+        prep = self._prepare(d1, d2)
+        self._mark(2)
+        m = self._match_prepared(prep)
+        self._mark(3)
+        st = self._stream()
+        cap = max(min(n1, n2), 1)
+        p1 = self._dev.get("pts1", (cap, 2), torch.float64, self.device)
+        p2 = self._dev.get("pts2", (cap, 2), torch.float64, self.device)
+        _lib.check(self._lib.pysift_gather_points(kp1.data_ptr(), m["pairs"].data_ptr(), m["count"].data_ptr(),
+                                                  cap, 0, p1.data_ptr(), st), "gather")
+        _lib.check(self._lib.pysift_gather_points(kp2.data_ptr(), m["pairs"].data_ptr(), m["count"].data_ptr(),
+                                                  cap, 1, p2.data_ptr(), st), "gather")
+        H_d, mask_d, info_d = self._ransac_count(p1, p2, m["count"], cap)
+        self._mark(4)
+        return m, p1, p2, H_d, mask_d, info_d
+
+    def _match_and_ransac(self, kp1, d1, n1, kp2, d2, n2):
+        """_match_and_ransac_launches as a CUDA graph replay: the first call
+        for the keypoint counts and buffers runs eagerly (and fits the PCA
+        basis on an instance's first pair), then the same launches are
+        captured; later calls replay them in one launch.  Eager with
+        stage_events (their records sit between the stages) or when the
+        detector was built with graphs=False."""
+        if not self._detector._use_graphs or self.stage_events is not None:
+            return self._match_and_ransac_launches(kp1, d1, n1, kp2, d2, n2)
+        key = ("pair", n1, n2, kp1.data_ptr(), d1.data_ptr(), kp2.data_ptr(), d2.data_ptr(), tuple(d1.shape[1:]),
+               d1.dtype, self.pca_dims, self.int8_matching, self.ransac_iters, self.ransac_method,
+               self.inlier_thresh, self.sigma_max, self.match_ratio)
+        main = torch.cuda.current_stream(self.device)
+        ent = self._graphs.get(key)
+        if ent is None:
+            out = self._match_and_ransac_launches(kp1, d1, n1, kp2, d2, n2)
+            cap = self._capture_stream()
+            cap.wait_stream(main)
+            n0 = self._lib.pysift_launch_count()
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=cap):
+                outg = self._match_and_ransac_launches(kp1, d1, n1, kp2, d2, n2)
+            n = self._lib.pysift_launch_count() - n0
+            self._lib.pysift_count_launches(-n)  # captured, not run
+            self._graphs[key] = (g, outg, n)
+            return out
+        g, outg, n = ent
+        with torch.cuda.stream(main):
+            g.replay()
+        self._lib.pysift_count_launches(n)
+        return outg
+
+    def _capture_stream(self):
+        if getattr(self, "_cap_stream", None) is None:
+            self._cap_stream = torch.cuda.Stream(self.device)
+        return self._cap_stream
 
     def _ransac_count(self, p1, p2, count, cap):
         """_ransac with the point count on the device (up to `cap` points)."""
@@ -455,27 +513,10 @@ class GPUPyStitch:
             metrics.update(kp1=n1, kp2=n2)
             if n1 == 0 or n2 < 2:
                 raise RuntimeError(f"Insufficient matches (0), need >= 4")
-            from . import match as _match_mod
-            prep = self._prepare(d1, d2)
-            self._mark(2)
-            m = self._match_prepared(prep)
-            self._mark(3)
+            m, p1, p2, H_d, mask_d, info_d = self._match_and_ransac(kp1, d1, n1, kp2, d2, n2)
             timings['st1'] = time.perf_counter() - t0
-            # the match count stays on the device: the points are gathered and
-            # RANSAC runs on it (capacity: the smaller keypoint count), and the
-            # host reads the count with RANSAC's result, one sync for both
-            st = self._stream()
-            cap = max(min(n1, n2), 1)
-            p1 = self._dev.get("pts1", (cap, 2), torch.float64, self.device)
-            p2 = self._dev.get("pts2", (cap, 2), torch.float64, self.device)
-            _lib.check(self._lib.pysift_gather_points(kp1.data_ptr(), m["pairs"].data_ptr(), m["count"].data_ptr(),
-                                                      cap, 0, p1.data_ptr(), st), "gather")
-            _lib.check(self._lib.pysift_gather_points(kp2.data_ptr(), m["pairs"].data_ptr(), m["count"].data_ptr(),
-                                                      cap, 1, p2.data_ptr(), st), "gather")
             timings['st2'] = 0.0
             t0 = time.perf_counter()
-            H_d, mask_d, info_d = self._ransac_count(p1, p2, m["count"], cap)
-            self._mark(4)
             hh = self._pinned("ransac_H_host", (9,), torch.float64)
             ih = self._pinned("ransac_info_host", (4,), torch.int32)
             ch = self._pinned("match_count_host", (1,), torch.int32)

@@ -394,3 +394,22 @@ def test_ransac_with_device_count_equals_host_count():
                                    4.0, 1, 10, ws.data_ptr() + off, sz.value, H.data_ptr(), mask.data_ptr(),
                                    info.data_ptr(), _st()) == 0
     assert np.array_equal(info.cpu().numpy(), [0, 0, 0]) and not H.cpu().numpy().any()
+
+
+def test_stitch_replay_equals_eager():
+    """The second call for the same keypoint counts captures the matcher +
+    RANSAC launches and the third replays them: all three give the same
+    panorama, homography and inlier mask, and the replay equals the oracle."""
+    from oracle import stitch_oracle as so
+    from pysift_b200.stitch import GPUPyStitch
+    img1, img2, _ = synthetic.stitch_pair(480, 640, seed=4)
+    st = GPUPyStitch(ransac_iters=2048, inlier_thresh=4.0, save_output=False, verbose=False)
+    runs = []
+    for _ in range(3):
+        pano = st.stitch(img1, img2)
+        runs.append((pano.copy(), st._last["H"].copy(), st._last["mask"].cpu().numpy().copy()))
+    assert len(st._graphs) == 1
+    for pano, H, mask in runs[1:]:
+        assert np.array_equal(pano, runs[0][0]) and np.array_equal(H, runs[0][1]) and np.array_equal(mask, runs[0][2])
+    orc = so.OracleStitch(ransac_iters=2048, inlier_thresh=4.0).stitch(img1, img2)
+    _assert_stitch_equals_oracle(st, runs[2][0], orc)
