@@ -113,6 +113,7 @@ class GPUPyStitch:
         self.stage_events = None  # optional list of 6 torch.cuda.Event(enable_timing=True)
         self._side = None         # two side streams, one per view
         self._graphs = {}         # captured match + RANSAC launches per (counts, buffers)
+        self._graph_seen = {}     # how often each key was met
 
     # ------------------------------------------------------------------
     #: stage names of the events recorded when ``stage_events`` holds six
@@ -297,13 +298,16 @@ class GPUPyStitch:
         self._mark(4)
         return m, p1, p2, H_d, mask_d, info_d
 
+    #: graphs of the matcher + RANSAC stage kept per instance
+    GRAPH_CACHE = 8
+
     def _match_and_ransac(self, kp1, d1, n1, kp2, d2, n2):
         """_match_and_ransac_launches as a CUDA graph replay: the first call
         for the keypoint counts and buffers runs eagerly (and fits the PCA
-        basis on an instance's first pair), then the same launches are
-        captured; later calls replay them in one launch.  Eager with
-        stage_events (their records sit between the stages) or when the
-        detector was built with graphs=False."""
+        basis on an instance's first pair), the second runs eagerly and
+        captures the same launches, later calls replay them in one launch.
+        Eager with stage_events (their records sit between the stages) or
+        when the detector was built with graphs=False."""
         if not self._detector._use_graphs or self.stage_events is not None:
             return self._match_and_ransac_launches(kp1, d1, n1, kp2, d2, n2)
         key = ("pair", n1, n2, kp1.data_ptr(), d1.data_ptr(), kp2.data_ptr(), d2.data_ptr(), tuple(d1.shape[1:]),
@@ -313,6 +317,17 @@ class GPUPyStitch:
         ent = self._graphs.get(key)
         if ent is None:
             out = self._match_and_ransac_launches(kp1, d1, n1, kp2, d2, n2)
+            # capture on a key's second sighting only (one-off counts stay
+            # eager), and keep the last GRAPH_CACHE graphs (each holds its
+            # buffers in its own memory pool)
+            seen = self._graph_seen.get(key, 0)
+            if len(self._graph_seen) > 64:
+                self._graph_seen.clear()
+            self._graph_seen[key] = seen + 1
+            if seen == 0:
+                return out
+            if len(self._graphs) >= self.GRAPH_CACHE:
+                self._graphs.pop(next(iter(self._graphs)))
             cap = self._capture_stream()
             cap.wait_stream(main)
             n0 = self._lib.pysift_launch_count()
