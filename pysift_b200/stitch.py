@@ -113,7 +113,6 @@ class GPUPyStitch:
         self.stage_events = None  # optional list of 6 torch.cuda.Event(enable_timing=True)
         self._side = None         # two side streams, one per view
         self._graphs = {}         # captured match + RANSAC launches per (counts, buffers)
-        self._graph_seen = {}     # how often each key was met
 
     # ------------------------------------------------------------------
     #: stage names of the events recorded when ``stage_events`` holds six
@@ -304,8 +303,8 @@ class GPUPyStitch:
     def _match_and_ransac(self, kp1, d1, n1, kp2, d2, n2):
         """_match_and_ransac_launches as a CUDA graph replay: the first call
         for the keypoint counts and buffers runs eagerly (and fits the PCA
-        basis on an instance's first pair), the second runs eagerly and
-        captures the same launches, later calls replay them in one launch.
+        basis on an instance's first pair) and captures the same launches,
+        later calls replay them in one launch.
         Eager with stage_events (their records sit between the stages) or
         when the detector was built with graphs=False."""
         if not self._detector._use_graphs or self.stage_events is not None:
@@ -317,17 +316,11 @@ class GPUPyStitch:
         ent = self._graphs.get(key)
         if ent is None:
             out = self._match_and_ransac_launches(kp1, d1, n1, kp2, d2, n2)
-            # capture on a key's second sighting only (one-off counts stay
-            # eager), and keep the last GRAPH_CACHE graphs (each holds its
-            # buffers in its own memory pool)
-            seen = self._graph_seen.get(key, 0)
-            if len(self._graph_seen) > 64:
-                self._graph_seen.clear()
-            self._graph_seen[key] = seen + 1
-            if seen == 0:
-                return out
+            # at most GRAPH_CACHE graphs per instance (each holds its buffers
+            # in its own memory pool); keys past that stay eager, so pairs of
+            # many different sizes never recapture
             if len(self._graphs) >= self.GRAPH_CACHE:
-                self._graphs.pop(next(iter(self._graphs)))
+                return out
             cap = self._capture_stream()
             cap.wait_stream(main)
             n0 = self._lib.pysift_launch_count()

@@ -397,9 +397,10 @@ def test_ransac_with_device_count_equals_host_count():
 
 
 def test_stitch_replay_equals_eager():
-    """The second call for the same keypoint counts captures the matcher +
-    RANSAC launches and the third replays them: all three give the same
-    panorama, homography and inlier mask, and the replay equals the oracle."""
+    """The first call for the keypoint counts runs eagerly and captures the
+    matcher + RANSAC launches, the next two replay them: all three give the
+    same panorama, homography and inlier mask, and the replay equals the
+    oracle."""
     from oracle import stitch_oracle as so
     from pysift_b200.stitch import GPUPyStitch
     img1, img2, _ = synthetic.stitch_pair(480, 640, seed=4)
