@@ -37,6 +37,20 @@ def _device_high_vram(device):
     return props.total_memory / _GIB >= 12
 
 
+def capture_graph(g, stream, fn):
+    """Capture the launches fn() enqueues on `stream` into CUDA graph `g` and
+    return fn()'s result.  Unlike the torch.cuda.graph context manager this
+    neither synchronizes nor empties the device and pinned-host allocator
+    caches, so a capture in the middle of a run of varying image sizes does
+    not send the calls after it back to cudaMalloc and cudaHostAlloc."""
+    with torch.cuda.stream(stream):
+        g.capture_begin()
+        try:
+            return fn()
+        finally:
+            g.capture_end()
+
+
 def gaussian_weights(sigma, truncate=4):
     """1-D Gaussian weights exactly as pysift/core.py:563-577 computes them
     (numpy float32); radius 0 when sigma < 0.01 (no blur)."""
@@ -290,8 +304,7 @@ class PySIFT:
             st.wait_stream(cap)
             n0 = self._lib.pysift_launch_count()
             g = torch.cuda.CUDAGraph()
-            with torch.cuda.graph(g, stream=cap):
-                self._launch(b, b.gray.data_ptr(), H, W, W, cap.cuda_stream)
+            capture_graph(g, cap, lambda: self._launch(b, b.gray.data_ptr(), H, W, W, cap.cuda_stream))
             n = self._lib.pysift_launch_count() - n0
             self._lib.pysift_count_launches(-n)  # captured, not run
             self._graphs[key] = (g, n)

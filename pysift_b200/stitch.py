@@ -20,7 +20,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .core import PySIFT, check_detector_options
+from .core import PySIFT, capture_graph, check_detector_options
 
 
 def _ptr_aligned(t, align=256):
@@ -287,8 +287,11 @@ class GPUPyStitch:
         self._mark(3)
         st = self._stream()
         cap = max(min(n1, n2), 1)
-        p1 = self._dev.get("pts1", (cap, 2), torch.float64, self.device)
-        p2 = self._dev.get("pts2", (cap, 2), torch.float64, self.device)
+        # fresh buffers, not the instance's cached ones: under capture they
+        # come from the graph's own memory pool, so a graph never writes
+        # into a buffer that a later pair of another size replaced
+        p1 = torch.empty((cap, 2), dtype=torch.float64, device=self.device)
+        p2 = torch.empty((cap, 2), dtype=torch.float64, device=self.device)
         _lib.check(self._lib.pysift_gather_points(kp1.data_ptr(), m["pairs"].data_ptr(), m["count"].data_ptr(),
                                                   cap, 0, p1.data_ptr(), st), "gather")
         _lib.check(self._lib.pysift_gather_points(kp2.data_ptr(), m["pairs"].data_ptr(), m["count"].data_ptr(),
@@ -325,8 +328,7 @@ class GPUPyStitch:
             cap.wait_stream(main)
             n0 = self._lib.pysift_launch_count()
             g = torch.cuda.CUDAGraph()
-            with torch.cuda.graph(g, stream=cap):
-                outg = self._match_and_ransac_launches(kp1, d1, n1, kp2, d2, n2)
+            outg = capture_graph(g, cap, lambda: self._match_and_ransac_launches(kp1, d1, n1, kp2, d2, n2))
             n = self._lib.pysift_launch_count() - n0
             self._lib.pysift_count_launches(-n)  # captured, not run
             self._graphs[key] = (g, outg, n)
@@ -348,11 +350,14 @@ class GPUPyStitch:
         n_hyp = int(self.ransac_iters)
         sz = ctypes.c_size_t()
         _lib.check(self._lib.pysift_ransac_workspace_size(cap, n_hyp, ctypes.byref(sz)), "ransac ws")
-        ws = self._dev.get("ransac_ws", (int(sz.value) + 256,), torch.uint8, self.device)
+        # fresh buffers (see _match_and_ransac_launches): a workspace freed
+        # after a capture stays in that graph's private pool, which nothing
+        # outside the capture allocates from
+        ws = torch.empty((int(sz.value) + 256,), dtype=torch.uint8, device=self.device)
         wp, wn = _ptr_aligned(ws)
-        H = self._dev.get("ransac_H", (9,), torch.float64, self.device)
-        mask = self._dev.get("ransac_mask", (cap,), torch.uint8, self.device)
-        info = self._dev.get("ransac_info", (4,), torch.int32, self.device)
+        H = torch.empty((9,), dtype=torch.float64, device=self.device)
+        mask = torch.empty((cap,), dtype=torch.uint8, device=self.device)
+        info = torch.empty((4,), dtype=torch.int32, device=self.device)
         rnd = self._random_stream(n_hyp)
         _lib.check(self._lib.pysift_ransac_count(p1.data_ptr(), p2.data_ptr(), count.data_ptr(), cap, rnd.data_ptr(),
                                                  n_hyp, float(self.inlier_thresh), float(self.sigma_max),

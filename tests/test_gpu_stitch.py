@@ -414,3 +414,23 @@ def test_stitch_replay_equals_eager():
         assert np.array_equal(pano, runs[0][0]) and np.array_equal(H, runs[0][1]) and np.array_equal(mask, runs[0][2])
     orc = so.OracleStitch(ransac_iters=2048, inlier_thresh=4.0).stitch(img1, img2)
     _assert_stitch_equals_oracle(st, runs[2][0], orc)
+
+
+def test_stitch_replays_across_sizes_keep_their_buffers():
+    """Pairs of two sizes, interleaved: each size's first call captures its
+    own graph and later calls replay it after the other size ran (and
+    allocated its own buffers) in between; every replay gives the result of
+    that size's eager call."""
+    from pysift_b200.stitch import GPUPyStitch
+    pairs = [synthetic.stitch_pair(480, 640, seed=4)[:2], synthetic.stitch_pair(600, 800, seed=9)[:2]]
+    st = GPUPyStitch(ransac_iters=2048, inlier_thresh=4.0, save_output=False, verbose=False)
+    first = {}
+    for rep in range(3):
+        for i, (a, b) in enumerate(pairs):
+            pano = st.stitch(a, b)
+            got = (pano.copy(), st._last["H"].copy(), st._last["mask"].cpu().numpy().copy())
+            if rep == 0:
+                first[i] = got
+            else:
+                assert all(np.array_equal(x, y) for x, y in zip(got, first[i])), (rep, i)
+    assert len(st._graphs) == 2
