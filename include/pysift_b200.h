@@ -374,6 +374,20 @@ int pysift_blend_multiband(const void* image1, int32_t image1_f32, const uint8_t
  * crop (pysift/core.py:3627-3684). */
 int pysift_mask_extents(const uint8_t* mask, int32_t cw, int32_t ch, int32_t* row_lo, int32_t* row_hi,
                         int32_t* col_lo, int32_t* col_hi, pysift_stream_t stream);
+/* The inner-rectangle crop (pysift/core.py:3627-3684) from the four extents
+ * arrays of pysift_mask_extents, computed on the HOST (all pointers are host
+ * memory; no stream).  box[0..3] = x, y, width, height of the crop in the
+ * canvas; box[4] = 0 when no pixel is covered (the whole canvas), 1 when the
+ * coverage has no inner rectangle (its bounding box), 2 for the inner
+ * rectangle. */
+int pysift_autocrop_box(const int32_t* row_lo, const int32_t* row_hi, const int32_t* col_lo, const int32_t* col_hi,
+                        int32_t cw, int32_t ch, int32_t* box);
+/* height rows of width_bytes from src (row pitch src_pitch) to dst (row pitch
+ * dst_pitch), asynchronously on the stream; either side may be device or
+ * page-locked host memory (the copy direction follows the pointers).  Used to
+ * read a crop of a device canvas into host memory in one copy. */
+int pysift_copy2d(void* dst, size_t dst_pitch, const void* src, size_t src_pitch, size_t width_bytes, size_t height,
+                  pysift_stream_t stream);
 
 /* Allocation-free 2x zoom (no counterpart in the reference; it exists for
  * callers that cannot allocate device memory at the call site, such as a

@@ -199,4 +199,6 @@ EXPORTS.update({
                                               c_void_p, c_void_p, c_void_p, c_void_p]),
     "pysift_mask_extents": (ctypes.c_int, [c_void_p, c_int32, c_int32, c_void_p, c_void_p, c_void_p, c_void_p,
                                            c_void_p]),
+    "pysift_autocrop_box": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_void_p]),
+    "pysift_copy2d": (ctypes.c_int, [c_void_p, c_size_t, c_void_p, c_size_t, c_size_t, c_size_t, c_void_p]),
 })

@@ -15,6 +15,7 @@
 // exact (int64 sums / count); the seam-mask blur (cv2.GaussianBlur, sigma 3)
 // is separable with the 25 float32 taps the caller passes (exp(-x^2 / 18)
 // normalised), reflect-101, rows then columns, float64 sums.
+#include <algorithm>
 #include <cstdint>
 
 #include "common.cuh"
@@ -1154,6 +1155,57 @@ int pysift_mask_extents(const uint8_t* mask, int32_t cw, int32_t ch, int32_t* ro
     PYSIFT_CUDA_TRY(cudaMemsetAsync(col_hi, 0xff, (size_t)cw * 4, st));
     k_mask_extents<<<dim3(1, ch), 256, 0, st>>>(mask, cw, row_lo, row_hi, col_lo, col_hi);
     PYSIFT_LAUNCH_CHECK("k_mask_extents");
+    return PYSIFT_OK;
+}
+
+int pysift_autocrop_box(const int32_t* row_lo, const int32_t* row_hi, const int32_t* col_lo, const int32_t* col_hi,
+                        int32_t cw, int32_t ch, int32_t* box) {
+    PYSIFT_CHECK_ARG(row_lo && row_hi && col_lo && col_hi && box, "NULL pointer argument");
+    PYSIFT_CHECK_ARG(cw > 0 && ch > 0, "bad sizes");
+    int r0 = -1, r1 = -1, c0 = -1, c1 = -1;
+    for (int r = 0; r < ch; ++r)
+        if (row_hi[r] >= 0) {
+            if (r0 < 0) r0 = r;
+            r1 = r;
+        }
+    for (int c = 0; c < cw; ++c)
+        if (col_hi[c] >= 0) {
+            if (c0 < 0) c0 = c;
+            c1 = c;
+        }
+    if (r0 < 0 || c0 < 0) {  // nothing covered: the whole canvas
+        box[0] = 0, box[1] = 0, box[2] = cw, box[3] = ch, box[4] = 0;
+        return PYSIFT_OK;
+    }
+    const int nr = r1 - r0 + 1, nc = c1 - c0 + 1;
+    // the largest left / top edge and the smallest right / bottom edge over
+    // the covered lines of the bounding box (uncovered lines do not bind)
+    int left = INT32_MIN, right = INT32_MAX, top = INT32_MIN, bot = INT32_MAX;
+    for (int r = r0; r <= r1; ++r) {
+        const bool cov = row_hi[r] >= 0;
+        left = std::max(left, cov ? row_lo[r] - c0 : 0);
+        right = std::min(right, cov ? row_hi[r] - c0 : nc - 1);
+    }
+    for (int c = c0; c <= c1; ++c) {
+        const bool cov = col_hi[c] >= 0;
+        top = std::max(top, cov ? col_lo[c] - r0 : 0);
+        bot = std::min(bot, cov ? col_hi[c] - r0 : nr - 1);
+    }
+    if (left >= right || top >= bot) {  // no inner rectangle: the bounding box
+        box[0] = c0, box[1] = r0, box[2] = nc, box[3] = nr, box[4] = 1;
+        return PYSIFT_OK;
+    }
+    box[0] = c0 + left, box[1] = r0 + top, box[2] = right - left + 1, box[3] = bot - top + 1, box[4] = 2;
+    return PYSIFT_OK;
+}
+
+int pysift_copy2d(void* dst, size_t dst_pitch, const void* src, size_t src_pitch, size_t width_bytes, size_t height,
+                  pysift_stream_t stream) {
+    PYSIFT_CHECK_ARG(dst && src, "NULL pointer argument");
+    PYSIFT_CHECK_ARG(width_bytes <= dst_pitch && width_bytes <= src_pitch, "bad pitches");
+    if (width_bytes == 0 || height == 0) return PYSIFT_OK;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    PYSIFT_CUDA_TRY(cudaMemcpy2DAsync(dst, dst_pitch, src, src_pitch, width_bytes, height, cudaMemcpyDefault, st));
     return PYSIFT_OK;
 }
 

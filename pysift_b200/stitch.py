@@ -440,20 +440,17 @@ class GPUPyStitch:
         return res
 
     def _compose_crop(self, c):
-        """The inner-rectangle crop of a composed canvas (its extents on the host)."""
+        """The inner-rectangle crop of a composed canvas (its extents on the
+        host; pysift_autocrop_box): a device view of the canvas."""
         cw, ch, out = c["canvas_w"], c["canvas_h"], c["out"]
-        e = c["ext_host"].numpy()
-        row_lo, row_hi = e[:ch], e[ch:2 * ch]
-        col_lo, col_hi = e[2 * ch:2 * ch + cw], e[2 * ch + cw:]
-        r0, r1, c0, c1, ir0, ir1, ic0, ic1, degenerate = self._autocrop_box(row_lo, row_hi, col_lo, col_hi)
-        if r0 is None:
-            c["crop_box"] = (0, 0, cw, ch)
-            return out
-        if degenerate:
-            c["crop_box"] = (c0, r0, c1 - c0 + 1, r1 - r0 + 1)
-            return out[r0:r1 + 1, c0:c1 + 1]
-        c["crop_box"] = (c0 + ic0, r0 + ir0, ic1 - ic0 + 1, ir1 - ir0 + 1)
-        return out[r0 + ir0:r0 + ir1 + 1, c0 + ic0:c0 + ic1 + 1]
+        e = np.ascontiguousarray(c["ext_host"].numpy(), dtype=np.int32)
+        box = np.empty(5, dtype=np.int32)
+        p = e.ctypes.data
+        _lib.check(self._lib.pysift_autocrop_box(p, p + 4 * ch, p + 8 * ch, p + 8 * ch + 4 * cw, cw, ch,
+                                                 box.ctypes.data), "pysift_autocrop_box")
+        x, y, w, h = (int(v) for v in box[:4])
+        c["crop_box"] = (x, y, w, h)
+        return out[y:y + h, x:x + w]
 
     def _compose(self, img1, img2, H, max_canvas_px=400_000_000):
         c = self._compose_enqueue(img1, img2, H, max_canvas_px=max_canvas_px)
@@ -472,33 +469,16 @@ class GPUPyStitch:
         """Device tensor -> numpy array in page-locked memory from torch's
         caching host allocator (the array keeps its block alive; a freed
         block is reused by a later call)."""
-        t = t.contiguous()
         host = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
-        host.copy_(t, non_blocking=True)
+        if t.dim() >= 2 and not t.is_contiguous() and t[0].is_contiguous() and t.numel() > 0:
+            # rows of a crop: one strided copy, no packing launch
+            rb = t[0].numel() * t.element_size()
+            _lib.check(self._lib.pysift_copy2d(host.data_ptr(), rb, t.data_ptr(), t.stride(0) * t.element_size(),
+                                               rb, t.shape[0], self._stream()), "pysift_copy2d")
+        else:
+            host.copy_(t.contiguous(), non_blocking=True)
         torch.cuda.current_stream(self.device).synchronize()
         return host.numpy()
-
-    @staticmethod
-    def _autocrop_box(row_lo, row_hi, col_lo, col_hi):
-        """The reference's inner-rectangle crop (pysift/core.py:3627-3684)
-        from per-row/column coverage extents."""
-        rows = np.nonzero(row_hi >= 0)[0]
-        cols = np.nonzero(col_hi >= 0)[0]
-        if rows.size == 0:
-            return (None,) * 8 + (False,)
-        r0, r1 = int(rows[0]), int(rows[-1])
-        c0, c1 = int(cols[0]), int(cols[-1])
-        nr, nc = r1 - r0 + 1, c1 - c0 + 1
-        rl, rh = row_lo[r0:r1 + 1], row_hi[r0:r1 + 1]
-        cl, chh = col_lo[c0:c1 + 1], col_hi[c0:c1 + 1]
-        left = np.where(rh >= 0, rl - c0, 0)
-        right = np.where(rh >= 0, rh - c0, nc - 1)
-        top = np.where(chh >= 0, cl - r0, 0)
-        bot = np.where(chh >= 0, chh - r0, nr - 1)
-        ic0, ic1 = int(left.max()), int(right.min())
-        ir0, ir1 = int(top.max()), int(bot.min())
-        degenerate = ic0 >= ic1 or ir0 >= ir1
-        return r0, r1, c0, c1, ir0, ir1, ic0, ic1, degenerate
 
     # ------------------------------------------------------------------
     def _stitch_pair(self, img1, img2):
