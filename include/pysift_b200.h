@@ -417,6 +417,13 @@ int pysift_zoom2x_u8_noalloc(const uint8_t* gray, int32_t H, int32_t W, int64_t 
 int64_t pysift_launch_count(void);
 void pysift_count_launches(int64_t n);
 
+/* memcpy of `bytes` host bytes split over up to n_threads host threads (the
+ * caller and a persistent pool of at most 7 workers; below 1 MiB, or with
+ * n_threads = 1, one plain memcpy).  Used for the staging copy of a host image
+ * into page-locked memory ahead of its upload.  Synchronous; concurrent
+ * callers are served one after another. */
+int pysift_host_copy(void* dst, const void* src, size_t bytes, int32_t n_threads);
+
 const char* pysift_last_error(void);
 const char* pysift_b200_version(void);
 

@@ -77,6 +77,7 @@ EXPORTS = {
     "pysift_b200_version": (ctypes.c_char_p, []),
     "pysift_launch_count": (c_int64, []),
     "pysift_count_launches": (None, [c_int64]),
+    "pysift_host_copy": (ctypes.c_int, [c_void_p, c_void_p, c_size_t, c_int32]),
     "pysift_detect_config_size": (c_size_t, []),
     "pysift_detect_workspace_size": (ctypes.c_int, [c_void_p, c_int32, c_int32, ctypes.POINTER(c_size_t)]),
     "pysift_detect_max_keypoints": (c_int32, [c_void_p]),

@@ -366,7 +366,6 @@ __global__ void __launch_bounds__(SCAN_THREADS, 2) k_match_rows(const RowScanArg
     // SIM_F16, DIST_U8, SPLIT_FP8: chunk-level state (the key of each
     // 32-column chunk is its largest); SIM_I8: column-level top-2
     constexpr bool CHUNKED = MODE != SIM_I8;
-    constexpr bool NORMS = MODE == DIST_U8 || MODE == SPLIT_FP8;
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t* sQ = smem;                // the query tile (NSL slabs)
     uint8_t* sRing = smem + G::TILE;   // NS train slabs
